@@ -1,0 +1,289 @@
+#!/usr/bin/env python
+"""Benchmark: CP steps/s of the Gamma-point CP electronic step on B200.
+
+Workload (default): 32 H2O (96 atoms) in an 18.6 bohr cubic box, 80 Ry state
+cutoff, 108^3 grid, 128 doubly occupied states, dt = 5 a.u., fictitious mass
+400 a.u. (mass cutoff 2 on g^2), synthetic seeded coefficients.  The random
+start is quenched (damped CP, untimed) before the timed dynamics steps.
+
+A "step" is one CP dynamics step: state FFTs + density, V_KS (XC, Hartree,
+local), V_KS psi back to forces + EKE, Lambda / Gamma constraint force,
+Verlet integration, S, Newton-Schulz S^-1/2 and Psi T.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  N > 1 runs independent replicas (one system
+per rank, no data-path collective): scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "CP steps/s at 128 states: mixed vs FP64 on 1 B200, |dE|<=1e-6 Ha/atom"
+UNIT = "CP steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="w32")
+    ap.add_argument("--quench", type=int, default=60)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--seed", type=int, default=2024)
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rk = int(os.environ.get("RANK", "0"))
+    lr = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rk, lr
+
+
+def make_sys(cfg, seed):
+    from openatom_b200.system import make_system
+    return make_system(cfg, seed=seed, ecut_mass=2.0, cmass0=400.0, dt=5.0)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, idx):
+        self.idx = idx
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                f = [x.strip() for x in out.stdout.strip().split(",")]
+                if len(f) >= 7:
+                    self.samples.append(f)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def total_energy(en):
+    return en["EKE"] + en["EHART"] + en["EEXT"] + en["EEXC"]
+
+
+# ----------------------------------------------------------------------------
+# CPU arm: the oracle port on the host cores (only here and in the reference
+# arm does bench.py execute oracle code)
+# ----------------------------------------------------------------------------
+
+def cpu_step_rate(sysm, nsteps, warm):
+    from oracle import cp_oracle as O
+    O.set_fft_workers(os.cpu_count() or 1)
+    st = O.CPState(sysm)
+    for _ in range(warm):
+        O.cp_step(st, sysm)
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        O.cp_step(st, sysm)
+    dt = time.perf_counter() - t0
+    return nsteps / dt, dt
+
+
+def run_reference(args):
+    ws, rk, lr = dist_env()
+    if rk != 0:
+        return 0
+    sysm = make_sys(args.config, args.seed)
+    k = max(1, min(args.steps, 3))
+    w = min(args.warmup, 1)
+    rate, dt = cpu_step_rate(sysm, k, w)
+    cores = os.cpu_count() or 1
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": k, "warmup": w, "ms_per_step": 1e3 * dt / k, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water box, random Loewdin-orthonormal start)",
+        "config": {"workload": f"{args.config}: 32 H2O, 128 states, 80 Ry, 108^3, ng={sysm.ng}",
+                   "nstate": sysm.nstate, "grid": list(sysm.nfft)},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{k} full CP steps of the FP64 oracle (numpy/scipy FFT, {cores} FFT workers)"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------
+
+def time_steps(torch, drv, k, before=None):
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    ens = []
+    for _ in range(k):
+        if before:
+            before()
+        ens.append(drv.step())
+    ev1.record()
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1) / k, ens
+
+
+def run_ours(args):
+    import torch
+    from openatom_b200.gpu import CPDriver
+    ws, rk, lr = dist_env()
+    torch.cuda.set_device(lr)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    sysm = make_sys(args.config, args.seed + rk)
+    natm = sysm.natm
+
+    # quench the random start (untimed), FP64
+    d64 = CPDriver(sysm, "fp64")
+    d64.quench(args.quench)
+    psi0 = d64.psi.cpu().numpy()
+    # two drivers from the same quenched state
+    d64 = CPDriver(sysm, "fp64", psi0=psi0)
+    dmx = CPDriver(sysm, "mixed", psi0=psi0)
+    for _ in range(args.warmup):
+        d64.step()
+        dmx.step()
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    with ClockSampler(lr) as clk:
+        barrier()
+        ms_mx, en_mx = time_steps(torch, dmx, args.steps)
+        barrier()
+        ms_64, en_64 = time_steps(torch, d64, args.steps)
+        barrier()
+        # end-to-end through the public API: host atom positions in, energies out
+        pos_host = torch.from_numpy(np.ascontiguousarray(sysm.pos)).pin_memory().numpy()
+        ms_e2e, _ = time_steps(torch, dmx, args.steps, before=lambda: dmx.ctx.set_atoms(pos_host))
+        barrier()
+    if ws > 1:
+        t = torch.tensor([ms_mx, ms_64, ms_e2e], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_mx, ms_64, ms_e2e = [float(x) for x in t.tolist()]
+
+    # accuracy of the mixed form against FP64 on the same trajectory start
+    de = max(abs(total_energy(a) - total_energy(b)) for a, b in zip(en_mx, en_64)) / natm
+    s_err = dmx.last_ortho
+
+    # per-kernel timing (CUDA events on the launch stream) for the roofline
+    kt = dmx.ctx.time_kernels(dmx.psi, reps=5)
+    kt64 = d64.ctx.time_kernels(d64.psi, reps=5)
+    roof = roofline(sysm, dmx, kt)
+
+    cpu = None
+    if rk == 0 and not args.no_cpu:
+        rate, dt = cpu_step_rate(sysm, 1, 0)
+        cpu = {"value": rate, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"1 full CP step of the FP64 oracle on this workload ({dt:.1f} s, scipy FFT workers={os.cpu_count()})"}
+
+    if rk == 0:
+        launches_per_step = dmx.launches_per_step()
+        line = {
+            "metric": METRIC, "value": ws * 1e3 / ms_mx, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_mx, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 FFT path + f64 GEMM/ortho/energies (mixed form)",
+            "data": "synthetic (seeded water box, random Loewdin start quenched by damped CP)",
+            "config": {"workload": f"{args.config}: 32 H2O, 128 states, 80 Ry, 108^3, ng={sysm.ng}",
+                       "nstate": sysm.nstate, "grid": list(sysm.nfft), "dt": sysm.dt, "quench_steps": args.quench,
+                       "l2": "per-step working set > 126 MB L2 (z-line buffer alone "
+                             f"{dmx.ctx.scratch_bytes() / 1e6:.0f} MB); no explicit flush",
+                       "parallelism": f"replicas x{ws}"},
+            "fp64": {"value": ws * 1e3 / ms_64, "ms_per_step": ms_64},
+            "mixed_over_fp64": ms_64 / ms_mx,
+            "dE_per_atom_max": de,
+            "ortho": {"iters": s_err[0], "residual": s_err[1]},
+            "kernel_ms": kt, "kernel_ms_fp64": kt64,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": {"value": ws * 1e3 / ms_e2e, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * natm,
+                    "d2h_bytes_per_step": 2 * 16 * 8},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def roofline(sysm, drv, kt):
+    """Roofline of the dominant kernel from its algorithmic bytes and its
+    CUDA-event time (see DESIGN.md for the per-kernel byte formulas)."""
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    src = "measured" if "hbm_gbs" in peaks else "fallback"
+    bytes_per = drv.ctx.algorithmic_bytes()
+    name = max(kt, key=lambda k: kt[k])
+    b = bytes_per.get(name)
+    if b is None:
+        return {"kernel": name, "bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
+                "traffic": None, "peak_source": src}
+    ach = b / (kt[name] * 1e-3) / 1e9
+    return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+            "traffic": None, "algorithmic_bytes": b, "peak_source": src}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

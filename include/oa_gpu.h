@@ -1,0 +1,183 @@
+/*
+ * liboa_gpu — C ABI of the B200 (sm_100a) Car-Parrinello electronic step.
+ *
+ * Each entry point does, for all states of one system on one GPU, the work of
+ * one OpenAtom chare entry method (or PINY physics routine) named beside it.
+ * Plain pointers and sizes only.  Arrays called "device" are caller-owned
+ * device memory; the context owns its own scratch.  Every call is
+ * asynchronous on the given stream unless it says it synchronises.
+ *
+ * Coefficient layout: double complex AoS (re, im), state-major:
+ *   psi[state * ng + ig], the reference's `complex` of ckcomplex.h, with the
+ *   g-points ordered as OpenAtom's doublePack state planes (kx = 0 first,
+ *   its redundant half first; z-line runs negative kz then non-negative kz),
+ *   src_charm_driver/fft_slab_ctrl/stateSlab.C:299-370 and
+ *   src_charm_driver/utility/util.C:936-990.
+ */
+#ifndef OA_GPU_H
+#define OA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  OA_OK = 0,
+  OA_ERR_BAD_ARG = 1,
+  OA_ERR_CUDA = 2,
+  OA_ERR_NOT_CONVERGED = 3,
+  OA_ERR_NONFINITE = 4,
+  OA_ERR_UNSUPPORTED = 5
+} oa_status;
+
+typedef enum { OA_FP64 = 0, OA_MIXED = 1 } oa_precision;
+
+typedef struct oa_ctx oa_ctx;
+
+/* Host-side description of one Gamma-point system (read during oa_gpu_init,
+ * not retained).  Mirrors what CPcharmParaInfo / the PINY CP singletons hold
+ * for the state step (src_piny_physics_v1.0/include/class_defs/allclass_cp.h). */
+typedef struct {
+  int nx, ny, nz;              /* FFT grid (sizeX, sizeY, sizeZ) */
+  int nstate;
+  int ng;                      /* half-sphere g-points per state (numPoints) */
+  int nlines;                  /* z-lines (numRuns / 2) */
+  const int *line_kx, *line_ky;      /* [nlines] */
+  const int *line_off;               /* [nlines] packed offset of the line */
+  const int *line_nneg, *line_npos;  /* [nlines] run lengths, kz<0 and kz>=0 */
+  const int *kx, *ky, *kz;           /* [ng] */
+  int nkx0, nkx0_red, nkx0_uni, nkx0_zero;
+  const int *red_partner;            /* [nkx0_red] index of -g of each redundant point */
+  double box;                  /* cubic cell edge, bohr */
+  double ecut_psi;             /* state cutoff on g^2 (Ry), cp_eke.C:50 */
+  double ecut_rho;             /* density cutoff on g^2, cp_hart_ext.C:113 */
+  const double *occ;           /* [nstate] occupations (1.0 closed shell) */
+  const double *cmass;         /* [ng] fictitious masses, cp_control_integrate.C:136 */
+  int natm, ntype;
+  const double *pos;           /* [natm][3] bohr */
+  const int *atm_type;         /* [natm] 0..ntype-1 */
+  const double *q_type;        /* [ntype] valence charges */
+  const double *gzvps;         /* [ntype] g = 0 local term */
+  double alp_ewd;
+  int nspl;                    /* local pseudopotential spline (CP_get_vpsnow) */
+  double spl_gmin, spl_dg;
+  const double *spl;           /* [ntype][nspl][4] */
+} oa_system_desc;
+
+/* Create a context on the current CUDA device.  precision = OA_FP64 (plain
+ * form) or OA_MIXED (FP32 state FFT path).  Allocates all scratch. */
+oa_status oa_gpu_init(const oa_system_desc *desc, int precision, oa_ctx **out);
+oa_status oa_gpu_destroy(oa_ctx *ctx);
+const char *oa_gpu_last_error(void);
+/* Bytes of device scratch the context holds. */
+size_t oa_gpu_scratch_bytes(const oa_ctx *ctx);
+
+/* State FFT g -> r and density.
+ * Replaces CP_State_GSpacePlane::doFFT (CP_State_GSpacePlane.C:1377-1445),
+ * sendFFTData (:1448), CP_State_RealSpacePlane::unpackFFT/doFFT/doReduction
+ * (CP_State_RealSpacePlane.C:186-517) and the density sum of
+ * CP_Rho_RealSpacePlane::acceptDensity (CP_Rho_RealSpacePlane.C:398-500).
+ * psi: device [nstate][ng] complex.  rho_out (optional, device [nz][ny][nx]
+ * doubles) receives rho(r) = sum_s occ_s psi_s(r)^2 / V after the call. */
+oa_status oa_gpu_state_fft_fwd(oa_ctx *ctx, void *stream, const double *psi, double *rho_out);
+
+/* V_KS(r) = V_xc + V_H + V_loc from the density of the last state_fft_fwd.
+ * Replaces CP_Rho_RealSpacePlane::energyComputation -> CPXCFNCTS::CP_exc_calc
+ * (cp_pz_lda.C:23-175), fftRhoRtoRhoG, CP_Rho_GHartExt::HartExtVksG ->
+ * CPLOCAL::CP_hart_eext_calc (cp_hart_ext.C:56-431), FFTVks, acceptHartVks.
+ * vks_out (optional, device [nz][ny][nx] doubles). */
+oa_status oa_gpu_vks_build(oa_ctx *ctx, void *stream, double *vks_out);
+
+/* Set V_KS(r) directly (device doubles [nz][ny][nx]); for callers that build
+ * the potential themselves (CP_State_RealSpacePlane::acceptVks). */
+oa_status oa_gpu_set_vks(oa_ctx *ctx, void *stream, const double *vks);
+
+/* psi(r) V_KS(r) occ -> back to g-space -> coefficient forces and EKE.
+ * Replaces CP_State_RealSpacePlane::unpackVks/doVksFFT/sendFPsiToGSP
+ * (:530-725), CP_State_GSpacePlane::unpackIFFT/doIFFT (:1530-1626),
+ * combineForcesGetEke (:1634-1746) with GStateSlab::addForces
+ * (stateSlab.C:239-268) and CPNONLOCAL::CP_eke_calc (cp_eke.C:30-140).
+ * recompute_fwd = 1 redoes the z pass from psi (needed unless the previous
+ * call on this context was oa_gpu_state_fft_fwd on the same psi).
+ * fnl: optional device [nstate][ng] nonlocal forces added after the x2.
+ * force: device [nstate][ng] output.  eke_out: optional device [nstate]. */
+oa_status oa_gpu_vks_apply_fft_bwd(oa_ctx *ctx, void *stream, const double *psi, int recompute_fwd,
+                                   const double *fnl, double *force, double *eke_out);
+
+/* PairCalculator forward (ckPairCalculator.C:821-893 + the tile reduction
+ * to Ortho, :938-1016): C[x][y] = alpha * sum_k w(k) left_x(k) right_y(k)
+ * over the real view (2*ng doubles per state); w = w_kx0 on the first
+ * 2*nkx0 doubles (kx = 0 plane) and 1 elsewhere.  S: alpha = 2,
+ * w_kx0 = 1/2 (sendPsi 1/sqrt2 on both sides); Lambda: alpha = 1, w_kx0 = 1.
+ * left, right: device [nstate][ng] complex; C: device [nstate][nstate]. */
+oa_status oa_gpu_pc_forward(oa_ctx *ctx, void *stream, const double *left, const double *right,
+                            double alpha, double w_kx0, double *C);
+
+/* Ortho S -> T = (S/2)^(-1/2) by Newton-Schulz (ortho.C:109-146, 153-266,
+ * 848-971; same iteration as CPORTHOG::get_iter_Tmat, cp_lowdin.C:180-265).
+ * S, T: device [n][n].  Synchronises the stream to return iterations and
+ * residual; returns OA_ERR_NOT_CONVERGED when max_iter is reached. */
+oa_status oa_gpu_ortho_invsqrt(oa_ctx *ctx, void *stream, const double *S, double *T, double tol,
+                               int max_iter, int *iters_out, double *err_out);
+
+/* PairCalculator backward (multiplyResult / bwMultiplyHelper /
+ * bwMultiplyDynOrthoT, ckPairCalculator.C:1201-2031), state-row form:
+ *   out_j = a1(c) sum_k M1[k][j] X1_k + a2 sum_k M2[k][j] X2_k
+ * a1(c) = a1_kx0 on the kx = 0 plane, a1_rest elsewhere.  M2/X2 may be NULL.
+ * Orthonormalisation psi = Psi T: M1 = T, a1 = 1.  Dynamics constraint
+ * force F' = F T - Psi Gamma (kx=0 Psi term halved by the 1/sqrt2
+ * scalings of sendLambda + doLambda): M1 = Gamma, X1 = psi,
+ * a1_kx0 = -1/2, a1_rest = -1, M2 = T, X2 = F, a2 = 1.
+ * out must not alias X1 or X2. */
+oa_status oa_gpu_pc_backward(oa_ctx *ctx, void *stream, const double *M1, const double *X1,
+                             double a1_kx0, double a1_rest, const double *M2, const double *X2, double a2,
+                             double *out);
+
+/* Small dense C = alpha A B (N x N), e.g. Gamma = T Lambda (ortho.C:565-570). */
+oa_status oa_gpu_small_gemm(oa_ctx *ctx, void *stream, const double *A, const double *B, double alpha,
+                            double *C);
+
+/* Velocity Verlet on the coefficients (CPINTEGRATE::CP_integrate_dyn,
+ * cp_dynamics.C:29-88, cp_evolve_vel :97-210, get_fictKE :218-254) and the
+ * Gamma redundancy sync (CP_State_GSpacePlane.C:2829-2970).  complete_prev = 1
+ * first completes the previous half kick (iteration > 1).  fict_ke_out:
+ * optional device double. */
+oa_status oa_gpu_integrate(oa_ctx *ctx, void *stream, const double *force, double *vpsi, double *psi,
+                           double dt, int complete_prev, double *fict_ke_out);
+
+/* PsiV tolerance reset (Ortho::maxCheck, ortho.C:455-475, and the
+ * "replace non-ortho psi by ortho" copies of CP_State_GSpacePlane.C:3590-3600,
+ * 3750-3760): psi_t <- psi and the velocities projected onto the
+ * orthonormality constraint, v_j <- v_j - sum_k psi_k X_kj,
+ * X = (A + A^T)/4, A_ij = <psi_i|v_j> in the S metric.  The caller resets
+ * its T to the identity. */
+oa_status oa_gpu_psiv_reset(oa_ctx *ctx, void *stream, const double *psi, double *psi_t, double *vpsi);
+
+/* Copy new atom positions (host [natm][3], bohr) for the next vks_build
+ * (the structure-factor phases are rebuilt from them every call). */
+oa_status oa_gpu_set_atoms(oa_ctx *ctx, void *stream, const double *pos_host);
+
+/* Average device time (ms, CUDA events on `stream`) of each kernel of the
+ * step over `reps` launches on the given orthonormal psi: ms_out[0..8] =
+ * state z pass fwd, state plane pass + density, density sum + XC, V_KS build
+ * (density FFT, Hartree/local, inverse), state plane pass with V_KS,
+ * state z pass bwd + EKE, PairCalculator forward (S), PairCalculator
+ * backward (two-term), Newton-Schulz.  Clobbers the context's scratch.
+ * No reference counterpart (it replaces the Projections user events of
+ * e.g. CP_State_GSpacePlane.C:1407-1409). */
+oa_status oa_gpu_time_kernels(oa_ctx *ctx, void *stream, const double *psi, int reps, double *ms_out);
+
+/* Sizes for byte/flop accounting (see oa_abi.cu): out[0..9]. */
+oa_status oa_gpu_sizes(const oa_ctx *ctx, long *out);
+
+/* Energies of the last vks_build / vks_apply_fft_bwd (synchronises):
+ * out[0..6] = EKE, EHART, EEXT, EWALD_RECIP, EEXC, MUXC, FICT_KE. */
+oa_status oa_gpu_energies(oa_ctx *ctx, void *stream, double *out7);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,516 @@
+// C ABI of liboa_gpu: context setup and the per-chare-work entry points.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+#include "oa_internal.h"
+
+// launchers from the other translation units
+size_t oa_plane_smem_bytes(int precision, int nx, int ny, int nkx, int npair, int ychunk, bool tile);
+size_t oa_rho_plane_smem_bytes(int nx, int ny, int nkx, int npair, int ychunk);
+int oa_rho_xc_nblk();
+int oa_rho_z_nblk(const oa_ctx* c);
+cudaError_t oa_launch_pc_fwd(cudaStream_t s, const double* A, const double* B, int n, long K, long kx0_cols,
+                             double w_kx0, double alpha, double* part, int nkb, double* C);
+cudaError_t oa_launch_pc_bwd(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
+                             const double* M2, const double* X2, double a2, int n, long ncol, long kx0_cols,
+                             double* out);
+cudaError_t oa_launch_small_gemm(cudaStream_t s, const double* A, const double* B, int n, double alpha, double* C);
+int oa_ns_grid(int n, int device);
+cudaError_t oa_launch_ortho_ns(cudaStream_t s, const double* S, int n, double bscale, double tol, int max_iter,
+                               double* work, double* T, int* status, double* errv, int grid);
+cudaError_t oa_launch_integrate(cudaStream_t s, const double2* F, double2* V, double2* P, const double* cmass,
+                                int ng, int nstate, int r0, int r1, int iend, double dt, int complete_prev,
+                                double* kepart, int nblk);
+cudaError_t oa_launch_sync_redundant(cudaStream_t s, double2* P, double2* V, const int* partner, int nred, int ng,
+                                     int nstate);
+cudaError_t oa_launch_sum_partials(cudaStream_t s, const double* part, int n, int stride, int off, double scale,
+                                   double* out);
+
+static thread_local char g_err[512] = "";
+
+void oa_set_error(const char* msg, const char* file, int line) {
+  snprintf(g_err, sizeof(g_err), "%s (%s:%d)", msg, file, line);
+}
+
+extern "C" const char* oa_gpu_last_error(void) { return g_err; }
+
+#define OA_ARG_CHECK(cond, msg)                         \
+  do {                                                  \
+    if (!(cond)) { oa_set_error(msg, __FILE__, __LINE__); return OA_ERR_BAD_ARG; } \
+  } while (0)
+
+// extra per-context PC/Ortho/integrator scratch lives behind the struct
+struct oa_ctx_pc {
+  double* part;      // split-K partials
+  int nkb;
+  double* ns_work;   // 5 n^2 + grid
+  int ns_grid;
+  int* ns_status;    // [2] device
+  double* ns_err;    // [1] device
+  int* partner;      // [nkx0_red]
+  double* cmass;     // [ng]
+  double* ke_part;   // integrate partials
+  int ke_nblk;
+  double* dev_e;     // [8] device energies
+  int* h_status;     // pinned
+  double* h_vals;    // pinned [16]
+  double* mat_a;     // [n][n] scratch
+  double* mat_x;     // [n][n] scratch
+  double* eye;       // [n][n] identity
+  double* vtmp;      // [nstate][ng] complex scratch
+};
+
+static oa_ctx_pc* pcx(oa_ctx* c);
+
+struct oa_ctx_full {
+  oa_ctx c;
+  oa_ctx_pc pc;
+};
+
+static oa_ctx_pc* pcx(oa_ctx* c) { return &reinterpret_cast<oa_ctx_full*>(c)->pc; }
+
+static bool make_plan(int n, OaFftPlan* p) {
+  p->n = n;
+  p->nst = 0;
+  int m = n;
+  while (m % 4 == 0 && m > 0) { if (p->nst >= OA_FFT_MAXST) return false; p->rad[p->nst++] = 4; m /= 4; }
+  const int prim[3] = {2, 3, 5};
+  for (int q = 0; q < 3; ++q)
+    while (m % prim[q] == 0) { if (p->nst >= OA_FFT_MAXST) return false; p->rad[p->nst++] = prim[q]; m /= prim[q]; }
+  return m == 1 && p->nst >= 2 && n <= OA_FFT_MAXN;
+}
+
+static double2* make_twiddles(int n) {
+  std::vector<double2> h(n);
+  for (int k = 0; k < n; ++k) {
+    const double a = -2.0 * M_PI * (double)k / (double)n;
+    h[k] = make_double2(cos(a), sin(a));
+  }
+  double2* d = nullptr;
+  if (cudaMalloc(&d, n * sizeof(double2)) != cudaSuccess) return nullptr;
+  cudaMemcpy(d, h.data(), n * sizeof(double2), cudaMemcpyHostToDevice);
+  return d;
+}
+
+template <typename T>
+static cudaError_t upload(T** dst, const T* src, size_t n) {
+  cudaError_t e = cudaMalloc(dst, (n ? n : 1) * sizeof(T));
+  if (e != cudaSuccess) return e;
+  if (n) e = cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+  return e;
+}
+
+static int pick_groups(int nz, int nstate, int bps, int nsm) {
+  // minimise ceil(nz g / (nsm bps)) * ceil(nstate / g)
+  int best = 1;
+  long bestc = -1;
+  for (int g = 1; g <= 32 && g <= nstate; ++g) {
+    const long waves = (nz * (long)g + (long)nsm * bps - 1) / ((long)nsm * bps);
+    const long cost = waves * ((nstate + g - 1) / g);
+    if (bestc < 0 || cost < bestc) { bestc = cost; best = g; }
+  }
+  return best;
+}
+
+extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx** out) {
+  OA_ARG_CHECK(d && out, "null argument");
+  OA_ARG_CHECK(precision == OA_FP64 || precision == OA_MIXED, "precision must be OA_FP64 or OA_MIXED");
+  OA_ARG_CHECK(d->nx > 0 && d->ny > 0 && d->nz > 0 && d->nstate > 0 && d->ng > 0 && d->nlines > 0, "bad sizes");
+  OA_ARG_CHECK(d->ntype >= 1 && d->ntype <= 4, "ntype must be 1..4");
+  *out = nullptr;
+  oa_ctx_full* F = (oa_ctx_full*)calloc(1, sizeof(oa_ctx_full));
+  if (!F) return OA_ERR_CUDA;
+  oa_ctx* c = &F->c;
+  oa_ctx_pc* p = &F->pc;
+  cudaGetDevice(&c->device);
+  c->precision = precision;
+  c->nx = d->nx; c->ny = d->ny; c->nz = d->nz; c->npts = d->nx * d->ny * d->nz;
+  c->ng = d->ng; c->nlines = d->nlines; c->nstate = d->nstate;
+  c->ldl = (d->nlines + 31) / 32 * 32;
+  c->nkx0 = d->nkx0; c->nkx0_red = d->nkx0_red; c->nkx0_uni = d->nkx0_uni; c->nkx0_zero = d->nkx0_zero;
+  c->natm = d->natm; c->ntype = d->ntype;
+  c->box = d->box; c->vol = d->box * d->box * d->box;
+  c->ecut_psi = d->ecut_psi; c->ecut_rho = d->ecut_rho; c->alp_ewd = d->alp_ewd;
+  c->nspl = d->nspl; c->spl_gmin = d->spl_gmin; c->spl_dg = d->spl_dg;
+  int mkx = 0;
+  for (int l = 0; l < d->nlines; ++l) mkx = d->line_kx[l] > mkx ? d->line_kx[l] : mkx;
+  c->nkx_s = mkx + 1;
+  c->nkx_d = d->nx / 2 + 1;
+  c->nlines_d = c->nkx_d * d->ny;
+  c->ldl_d = (c->nlines_d + 31) / 32 * 32;
+  const double f = 2.0 * M_PI / d->box;
+  c->kmax_tab = (int)floor(sqrt(d->ecut_rho) / f) + 1;
+  double gz = 0.0;
+  for (int a = 0; a < d->natm; ++a) gz += d->gzvps[d->atm_type[a]];
+  c->gzvps_sum = gz;
+  if (!make_plan(d->nx, &c->plan_x) || !make_plan(d->ny, &c->plan_y) || !make_plan(d->nz, &c->plan_z)) {
+    oa_set_error("FFT length must be 2^a 3^b 5^c with at least two radix stages and <= 512", __FILE__, __LINE__);
+    free(F);
+    return OA_ERR_UNSUPPORTED;
+  }
+  // plane kernel chunking to fit shared memory
+  c->npair_s = 16; c->ychunk_s = 16;
+  while (oa_plane_smem_bytes(precision, d->nx, d->ny, c->nkx_s, c->npair_s, c->ychunk_s, true) > OA_MAX_SMEM &&
+         c->npair_s > 1) { c->npair_s /= 2; c->ychunk_s = c->npair_s; }
+  c->npair_d = 16; c->ychunk_d = 16;
+  while (oa_rho_plane_smem_bytes(d->nx, d->ny, c->nkx_d, c->npair_d, c->ychunk_d) > OA_MAX_SMEM && c->npair_d > 1) {
+    c->npair_d /= 2; c->ychunk_d = c->npair_d;
+  }
+  c->smem_plane = oa_plane_smem_bytes(precision, d->nx, d->ny, c->nkx_s, c->npair_s, c->ychunk_s, true);
+  c->smem_rho_plane = oa_rho_plane_smem_bytes(d->nx, d->ny, c->nkx_d, c->npair_d, c->ychunk_d);
+  if (c->smem_plane > OA_MAX_SMEM || c->smem_rho_plane > OA_MAX_SMEM) {
+    oa_set_error("grid too large for the shared-memory plane kernels at this precision", __FILE__, __LINE__);
+    free(F);
+    return OA_ERR_UNSUPPORTED;
+  }
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  const int bps = (int)(228 * 1024 / (c->smem_plane + 1024)) > 0 ? (int)(228 * 1024 / (c->smem_plane + 1024)) : 1;
+  c->ngroup = pick_groups(d->nz, d->nstate, bps, nsm);
+  c->nblk_z = (d->nlines + OA_LB - 1) / OA_LB;
+
+  const size_t csz = precision == OA_FP64 ? sizeof(double2) : sizeof(float2);
+  const size_t rsz = precision == OA_FP64 ? sizeof(double) : sizeof(float);
+  cudaError_t e = cudaSuccess;
+#define TRY(x) do { e = (x); if (e != cudaSuccess) goto fail; } while (0)
+  {
+    std::vector<double> g2(d->ng);
+    std::vector<int> kxv(d->kx, d->kx + d->ng);
+    for (int i = 0; i < d->ng; ++i) {
+      const double gx = f * d->kx[i], gy = f * d->ky[i], gzz = f * d->kz[i];
+      g2[i] = gx * gx + gy * gy + gzz * gzz;
+    }
+    TRY(upload(&c->line_kx, d->line_kx, d->nlines));
+    TRY(upload(&c->line_ky, d->line_ky, d->nlines));
+    TRY(upload(&c->line_off, d->line_off, d->nlines));
+    TRY(upload(&c->line_nneg, d->line_nneg, d->nlines));
+    TRY(upload(&c->line_npos, d->line_npos, d->nlines));
+    TRY(upload(&c->kx, kxv.data(), d->ng));
+    TRY(upload(&c->g2, g2.data(), d->ng));
+    TRY(upload(&c->occ, d->occ, d->nstate));
+    TRY(upload(&c->spl, d->spl, (size_t)d->ntype * d->nspl * 4));
+    TRY(upload(&c->q_type, d->q_type, d->ntype));
+    TRY(upload(&c->atm_type, d->atm_type, d->natm));
+    TRY(upload(&c->pos, d->pos, (size_t)3 * d->natm));
+    TRY(upload(&p->partner, d->red_partner, d->nkx0_red));
+    TRY(upload(&p->cmass, d->cmass, d->ng));
+    c->tw_x = make_twiddles(d->nx);
+    c->tw_y = make_twiddles(d->ny);
+    c->tw_z = make_twiddles(d->nz);
+    if (!c->tw_x || !c->tw_y || !c->tw_z) { e = cudaErrorMemoryAllocation; goto fail; }
+    TRY(cudaMalloc(&c->phase, (size_t)d->natm * 3 * (2 * c->kmax_tab + 1) * sizeof(double2)));
+    c->zbuf_bytes = (size_t)d->nstate * d->nz * c->ldl * csz;
+    TRY(cudaMalloc(&c->zbuf, c->zbuf_bytes));
+    TRY(cudaMalloc(&c->rho_part, (size_t)c->ngroup * c->npts * sizeof(double)));
+    TRY(cudaMalloc(&c->rho, (size_t)c->npts * sizeof(double)));
+    TRY(cudaMalloc(&c->vxc, (size_t)c->npts * sizeof(double)));
+    TRY(cudaMalloc(&c->vks, (size_t)c->npts * rsz));
+    TRY(cudaMalloc(&c->dz, (size_t)d->nz * c->ldl_d * sizeof(double2)));
+    c->red_len = (size_t)3 * oa_rho_xc_nblk() + 3 * (size_t)oa_rho_z_nblk(c) + 64;
+    TRY(cudaMalloc(&c->red, c->red_len * sizeof(double)));
+    TRY(cudaMalloc(&c->eke_part, (size_t)d->nstate * c->nblk_z * sizeof(double)));
+    p->nkb = 64;
+    TRY(cudaMalloc(&p->part, (size_t)p->nkb * d->nstate * d->nstate * sizeof(double)));
+    p->ns_grid = oa_ns_grid(d->nstate, c->device);
+    TRY(cudaMalloc(&p->ns_work, ((size_t)5 * d->nstate * d->nstate + p->ns_grid + 8) * sizeof(double)));
+    TRY(cudaMalloc(&p->ns_status, 4 * sizeof(int)));
+    TRY(cudaMalloc(&p->ns_err, 2 * sizeof(double)));
+    p->ke_nblk = 2 * nsm;
+    TRY(cudaMalloc(&p->ke_part, p->ke_nblk * sizeof(double)));
+    TRY(cudaMalloc(&p->dev_e, 16 * sizeof(double)));
+    TRY(cudaMemset(p->dev_e, 0, 16 * sizeof(double)));
+    TRY(cudaMalloc(&p->mat_a, (size_t)d->nstate * d->nstate * sizeof(double)));
+    TRY(cudaMalloc(&p->mat_x, (size_t)d->nstate * d->nstate * sizeof(double)));
+    {
+      std::vector<double> eye((size_t)d->nstate * d->nstate, 0.0);
+      for (int i = 0; i < d->nstate; ++i) eye[(size_t)i * d->nstate + i] = 1.0;
+      TRY(upload(&p->eye, eye.data(), eye.size()));
+    }
+    TRY(cudaMalloc(&p->vtmp, (size_t)d->nstate * d->ng * sizeof(double2)));
+    TRY(cudaMallocHost(&p->h_status, 4 * sizeof(int)));
+    TRY(cudaMallocHost(&p->h_vals, 16 * sizeof(double)));
+    TRY(cudaDeviceSynchronize());
+  }
+#undef TRY
+  *out = c;
+  return OA_OK;
+fail:
+  oa_set_error(cudaGetErrorString(e), __FILE__, __LINE__);
+  oa_gpu_destroy(c);
+  return OA_ERR_CUDA;
+}
+
+extern "C" oa_status oa_gpu_destroy(oa_ctx* c) {
+  if (!c) return OA_OK;
+  oa_ctx_pc* p = pcx(c);
+  void* dev[] = {c->line_kx, c->line_ky, c->line_off, c->line_nneg, c->line_npos, c->kx, c->g2, c->tw_x, c->tw_y,
+                 c->tw_z, c->spl, c->q_type, c->atm_type, c->pos, c->phase, c->occ, c->zbuf, c->rho_part, c->rho,
+                 c->vks, c->vxc, c->dz, c->red, c->eke_part, p->part, p->ns_work, p->ns_status, p->ns_err,
+                 p->partner, p->cmass, p->ke_part, p->dev_e, p->mat_a, p->mat_x, p->eye, p->vtmp};
+  for (void* q : dev) if (q) cudaFree(q);
+  if (p->h_status) cudaFreeHost(p->h_status);
+  if (p->h_vals) cudaFreeHost(p->h_vals);
+  free(reinterpret_cast<oa_ctx_full*>(c));
+  return OA_OK;
+}
+
+extern "C" size_t oa_gpu_scratch_bytes(const oa_ctx* c) {
+  if (!c) return 0;
+  const size_t rsz = c->precision == OA_FP64 ? 8 : 4;
+  return c->zbuf_bytes + (size_t)c->ngroup * c->npts * 8 + (size_t)c->npts * (16 + rsz) +
+         (size_t)c->nz * c->ldl_d * 16;
+}
+
+extern "C" oa_status oa_gpu_state_fft_fwd(oa_ctx* c, void* stream, const double* psi, double* rho_out) {
+  OA_ARG_CHECK(c && psi, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  OA_CUDA_TRY(oa_launch_state_zfwd(c, s, (const double2*)psi, 0, c->nstate));
+  OA_CUDA_TRY(oa_launch_state_plane_density(c, s));
+  OA_CUDA_TRY(oa_launch_rho_xc(c, s));
+  if (rho_out) OA_CUDA_TRY(cudaMemcpyAsync(rho_out, c->rho, (size_t)c->npts * 8, cudaMemcpyDeviceToDevice, s));
+  return OA_OK;
+}
+
+__global__ void k_to_double(const float* a, double* b, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) b[i] = a[i];
+}
+__global__ void k_to_float(const double* a, float* b, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) b[i] = (float)a[i];
+}
+
+extern "C" oa_status oa_gpu_vks_build(oa_ctx* c, void* stream, double* vks_out) {
+  OA_ARG_CHECK(c, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  oa_ctx_pc* p = pcx(c);
+  OA_CUDA_TRY(oa_launch_rho_fft_hart(c, s));
+  const int nx = oa_rho_xc_nblk(), nzb = oa_rho_z_nblk(c);
+  const double vs = c->vol / (double)c->npts;
+  // EEXC = (0.75 ex + ec) V/N ; MUXC = sum vxc rho V/N
+  OA_CUDA_TRY(oa_launch_sum_partials(s, c->red, nx, 3, 0, 0.75 * vs, p->dev_e + 8));
+  OA_CUDA_TRY(oa_launch_sum_partials(s, c->red, nx, 3, 1, vs, p->dev_e + 9));
+  OA_CUDA_TRY(oa_launch_sum_partials(s, c->red, nx, 3, 2, vs, p->dev_e + OA_E_MUXC));
+  OA_CUDA_TRY(oa_launch_sum_partials(s, c->red + 3 * nx, nzb, 3, 0, 0.5, p->dev_e + OA_E_EHART));
+  OA_CUDA_TRY(oa_launch_sum_partials(s, c->red + 3 * nx, nzb, 3, 1, 1.0, p->dev_e + OA_E_EEXT));
+  OA_CUDA_TRY(oa_launch_sum_partials(s, c->red + 3 * nx, nzb, 3, 2, 0.5, p->dev_e + OA_E_EWALD));
+  if (vks_out) {
+    if (c->precision == OA_FP64)
+      OA_CUDA_TRY(cudaMemcpyAsync(vks_out, c->vks, (size_t)c->npts * 8, cudaMemcpyDeviceToDevice, s));
+    else {
+      k_to_double<<<592, 256, 0, s>>>((const float*)c->vks, vks_out, (size_t)c->npts);
+      OA_CUDA_TRY(cudaGetLastError());
+    }
+  }
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_set_vks(oa_ctx* c, void* stream, const double* vks) {
+  OA_ARG_CHECK(c && vks, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (c->precision == OA_FP64)
+    OA_CUDA_TRY(cudaMemcpyAsync(c->vks, vks, (size_t)c->npts * 8, cudaMemcpyDeviceToDevice, s));
+  else {
+    k_to_float<<<592, 256, 0, s>>>(vks, (float*)c->vks, (size_t)c->npts);
+    OA_CUDA_TRY(cudaGetLastError());
+  }
+  return OA_OK;
+}
+
+__global__ void k_eke_states(const double* part, int nblk, int nstate, double* eke_state, double* total) {
+  __shared__ double sh[32];
+  double tsum = 0.0;
+  for (int st = 0; st < nstate; ++st) {
+    double sv = 0.0;
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) sv += part[(size_t)st * nblk + i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sv += __shfl_xor_sync(0xffffffffu, sv, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = sv;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+      if (eke_state) eke_state[st] = 0.5 * t;
+      tsum += 0.5 * t;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) total[0] = tsum;
+}
+
+extern "C" oa_status oa_gpu_vks_apply_fft_bwd(oa_ctx* c, void* stream, const double* psi, int recompute_fwd,
+                                              const double* fnl, double* force, double* eke_out) {
+  OA_ARG_CHECK(c && psi && force, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (recompute_fwd) OA_CUDA_TRY(oa_launch_state_zfwd(c, s, (const double2*)psi, 0, c->nstate));
+  OA_CUDA_TRY(oa_launch_state_plane_vks(c, s));
+  OA_CUDA_TRY(oa_launch_state_zbwd(c, s, (const double2*)psi, (const double2*)fnl, (double2*)force, 0, c->nstate));
+  k_eke_states<<<1, 256, 0, s>>>(c->eke_part, c->nblk_z, c->nstate, eke_out, pcx(c)->dev_e + OA_E_EKE);
+  OA_CUDA_TRY(cudaGetLastError());
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_pc_forward(oa_ctx* c, void* stream, const double* left, const double* right,
+                                       double alpha, double w_kx0, double* C) {
+  OA_ARG_CHECK(c && left && right && C, "null argument");
+  oa_ctx_pc* p = pcx(c);
+  OA_CUDA_TRY(oa_launch_pc_fwd((cudaStream_t)stream, left, right, c->nstate, 2L * c->ng, 2L * c->nkx0, w_kx0, alpha,
+                               p->part, p->nkb, C));
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_ortho_invsqrt(oa_ctx* c, void* stream, const double* S, double* T, double tol,
+                                          int max_iter, int* iters_out, double* err_out) {
+  OA_ARG_CHECK(c && S && T && max_iter > 0, "bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  oa_ctx_pc* p = pcx(c);
+  OA_CUDA_TRY(oa_launch_ortho_ns(s, S, c->nstate, 0.5, tol, max_iter, p->ns_work, T, p->ns_status, p->ns_err,
+                                 p->ns_grid));
+  OA_CUDA_TRY(cudaMemcpyAsync(p->h_status, p->ns_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  OA_CUDA_TRY(cudaMemcpyAsync(p->h_vals, p->ns_err, sizeof(double), cudaMemcpyDeviceToHost, s));
+  OA_CUDA_TRY(cudaStreamSynchronize(s));
+  if (iters_out) *iters_out = p->h_status[0];
+  if (err_out) *err_out = p->h_vals[0];
+  if (!isfinite(p->h_vals[0])) { oa_set_error("Newton-Schulz residual is not finite", __FILE__, __LINE__); return OA_ERR_NONFINITE; }
+  if (!p->h_status[1]) { oa_set_error("Newton-Schulz reached max_iter", __FILE__, __LINE__); return OA_ERR_NOT_CONVERGED; }
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_pc_backward(oa_ctx* c, void* stream, const double* M1, const double* X1,
+                                        double a1_kx0, double a1_rest, const double* M2, const double* X2, double a2,
+                                        double* out) {
+  OA_ARG_CHECK(c && M1 && X1 && out, "null argument");
+  OA_ARG_CHECK((M2 == nullptr) == (X2 == nullptr), "M2 and X2 must both be given or both be NULL");
+  OA_ARG_CHECK(out != X1 && out != X2, "out must not alias an input");
+  OA_CUDA_TRY(oa_launch_pc_bwd((cudaStream_t)stream, M1, X1, a1_kx0, a1_rest, M2, X2, a2, c->nstate, 2L * c->ng,
+                               2L * c->nkx0, out));
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_small_gemm(oa_ctx* c, void* stream, const double* A, const double* B, double alpha,
+                                       double* C) {
+  OA_ARG_CHECK(c && A && B && C, "null argument");
+  OA_CUDA_TRY(oa_launch_small_gemm((cudaStream_t)stream, A, B, c->nstate, alpha, C));
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_integrate(oa_ctx* c, void* stream, const double* force, double* vpsi, double* psi,
+                                      double dt, int complete_prev, double* fict_ke_out) {
+  OA_ARG_CHECK(c && force && vpsi && psi, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  oa_ctx_pc* p = pcx(c);
+  const int r0 = c->nkx0_red, r1 = c->nkx0_red + c->nkx0_zero, iend = c->nkx0_red + c->nkx0_uni;
+  OA_CUDA_TRY(oa_launch_integrate(s, (const double2*)force, (double2*)vpsi, (double2*)psi, p->cmass, c->ng,
+                                  c->nstate, r0, r1, iend, dt, complete_prev, p->ke_part, p->ke_nblk));
+  OA_CUDA_TRY(oa_launch_sum_partials(s, p->ke_part, p->ke_nblk, 1, 0, 1.0, p->dev_e + OA_E_FICT));
+  if (fict_ke_out)
+    OA_CUDA_TRY(cudaMemcpyAsync(fict_ke_out, p->dev_e + OA_E_FICT, sizeof(double), cudaMemcpyDeviceToDevice, s));
+  OA_CUDA_TRY(oa_launch_sync_redundant(s, (double2*)psi, (double2*)vpsi, p->partner, c->nkx0_red, c->ng, c->nstate));
+  return OA_OK;
+}
+
+__global__ void k_energy_combine(double* e) {
+  // EEXC = 0.75 ex V/N + ec V/N was stored split at [8] and [9]
+  e[OA_E_EEXC] = e[8] + e[9];
+}
+
+extern "C" oa_status oa_gpu_energies(oa_ctx* c, void* stream, double* out7) {
+  OA_ARG_CHECK(c && out7, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  oa_ctx_pc* p = pcx(c);
+  k_energy_combine<<<1, 1, 0, s>>>(p->dev_e);
+  OA_CUDA_TRY(cudaGetLastError());
+  OA_CUDA_TRY(cudaMemcpyAsync(p->h_vals, p->dev_e, 16 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  OA_CUDA_TRY(cudaStreamSynchronize(s));
+  out7[0] = p->h_vals[OA_E_EKE];
+  out7[1] = p->h_vals[OA_E_EHART];
+  out7[2] = p->h_vals[OA_E_EEXT];
+  out7[3] = p->h_vals[OA_E_EWALD];
+  out7[4] = p->h_vals[OA_E_EEXC];
+  out7[5] = p->h_vals[OA_E_MUXC];
+  out7[6] = p->h_vals[OA_E_FICT];
+  return OA_OK;
+}
+
+__global__ void k_sym_quarter(const double* A, int n, double* X) {
+  const int i = blockIdx.y * 16 + threadIdx.y, j = blockIdx.x * 16 + threadIdx.x;
+  if (i < n && j < n) X[(size_t)i * n + j] = 0.25 * (A[(size_t)i * n + j] + A[(size_t)j * n + i]);
+}
+
+extern "C" oa_status oa_gpu_psiv_reset(oa_ctx* c, void* stream, const double* psi, double* psi_t, double* vpsi) {
+  OA_ARG_CHECK(c && psi && psi_t && vpsi, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  oa_ctx_pc* p = pcx(c);
+  const int n = c->nstate;
+  OA_CUDA_TRY(oa_launch_pc_fwd(s, psi, vpsi, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, p->mat_a));
+  dim3 grid((n + 15) / 16, (n + 15) / 16), blk(16, 16);
+  k_sym_quarter<<<grid, blk, 0, s>>>(p->mat_a, n, p->mat_x);
+  OA_CUDA_TRY(cudaGetLastError());
+  OA_CUDA_TRY(oa_launch_pc_bwd(s, p->mat_x, psi, -1.0, -1.0, p->eye, vpsi, 1.0, n, 2L * c->ng, 2L * c->nkx0,
+                               p->vtmp));
+  const size_t bytes = (size_t)n * c->ng * sizeof(double2);
+  OA_CUDA_TRY(cudaMemcpyAsync(vpsi, p->vtmp, bytes, cudaMemcpyDeviceToDevice, s));
+  OA_CUDA_TRY(cudaMemcpyAsync(psi_t, psi, bytes, cudaMemcpyDeviceToDevice, s));
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_set_atoms(oa_ctx* c, void* stream, const double* pos_host) {
+  OA_ARG_CHECK(c && pos_host, "null argument");
+  OA_CUDA_TRY(cudaMemcpyAsync(c->pos, pos_host, (size_t)3 * c->natm * sizeof(double), cudaMemcpyHostToDevice,
+                              (cudaStream_t)stream));
+  return OA_OK;
+}
+
+// Average device time of each kernel of the step (CUDA events on `stream`),
+// for the roofline: ms_out[0..8] = state_zfwd, state_plane_density, rho_xc,
+// vks_build (density FFT + Hartree/local + inverse), state_plane_vks,
+// state_zbwd, pc_forward (S), pc_backward (two-term), ortho_ns.
+extern "C" oa_status oa_gpu_time_kernels(oa_ctx* c, void* stream, const double* psi, int reps, double* ms_out) {
+  OA_ARG_CHECK(c && psi && ms_out && reps > 0, "bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  oa_ctx_pc* p = pcx(c);
+  cudaEvent_t e0, e1;
+  OA_CUDA_TRY(cudaEventCreate(&e0));
+  OA_CUDA_TRY(cudaEventCreate(&e1));
+  float ms = 0.f;
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const int n = c->nstate;
+  double* S = p->mat_a;
+  double* T = p->mat_x;
+  for (int r = 0; r < reps; ++r) {
+#define OA_TIME(slot, call)                                   \
+    OA_CUDA_TRY(cudaEventRecord(e0, s));                      \
+    OA_CUDA_TRY(call);                                        \
+    OA_CUDA_TRY(cudaEventRecord(e1, s));                      \
+    OA_CUDA_TRY(cudaEventSynchronize(e1));                    \
+    OA_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));           \
+    acc[slot] += ms;
+    OA_TIME(0, oa_launch_state_zfwd(c, s, (const double2*)psi, 0, n));
+    OA_TIME(1, oa_launch_state_plane_density(c, s));
+    OA_TIME(2, oa_launch_rho_xc(c, s));
+    OA_TIME(3, oa_launch_rho_fft_hart(c, s));
+    OA_TIME(4, oa_launch_state_plane_vks(c, s));
+    OA_TIME(5, oa_launch_state_zbwd(c, s, (const double2*)psi, nullptr, (double2*)p->vtmp, 0, n));
+    OA_TIME(6, oa_launch_pc_fwd(s, psi, psi, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, S));
+    OA_TIME(7, oa_launch_pc_bwd(s, p->eye, psi, -0.5, -1.0, p->eye, psi, 1.0, n, 2L * c->ng, 2L * c->nkx0,
+                                p->vtmp));
+    OA_TIME(8, oa_launch_ortho_ns(s, S, n, 0.5, 1e-15, 1000, p->ns_work, T, p->ns_status, p->ns_err, p->ns_grid));
+#undef OA_TIME
+  }
+  for (int k = 0; k < 9; ++k) ms_out[k] = acc[k] / reps;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return OA_OK;
+}
+
+// Problem sizes a caller needs for byte/flop accounting: out[0..9] =
+// nstate, ng, nlines, nz, ldl, ngroup, npts, compute-precision bytes per
+// real, nlines_d, kernel launches per CP step of the host runner.
+extern "C" oa_status oa_gpu_sizes(const oa_ctx* c, long* out) {
+  OA_ARG_CHECK(c && out, "null argument");
+  out[0] = c->nstate; out[1] = c->ng; out[2] = c->nlines; out[3] = c->nz; out[4] = c->ldl;
+  out[5] = c->ngroup; out[6] = c->npts; out[7] = c->precision == OA_FP64 ? 8 : 4; out[8] = c->nlines_d;
+  // state_fft_fwd 3 + vks_build 10 + vks_apply 3 + lambda (2+1+1+1) + integrate 3 + S (2) + NS 1 + Psi T 1
+  out[9] = 3 + 10 + 3 + 5 + 3 + 2 + 1 + 1;
+  return OA_OK;
+}

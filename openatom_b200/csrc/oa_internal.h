@@ -1,0 +1,74 @@
+// Internal context of liboa_gpu: device tables, plans and scratch for one
+// Gamma-point system on one GPU.  Not part of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "oa_fft.cuh"
+#include "../../include/oa_gpu.h"
+
+#define OA_NTHREADS 256
+#define OA_LB 16          // z-lines per block in the z passes
+#define OA_MAX_SMEM (227 * 1024)
+
+struct oa_ctx {
+  int device;
+  int precision;          // OA_FP64 or OA_MIXED
+  int nx, ny, nz, npts;
+  int ng, nlines, ldl;    // g-points, state z-lines, padded line stride
+  int nstate, natm, ntype;
+  int nkx0, nkx0_red, nkx0_uni, nkx0_zero;
+  int nkx_s;              // state sphere x-columns (max line kx + 1)
+  int nkx_d;              // density half-spectrum columns (nx/2 + 1)
+  int nlines_d, ldl_d;    // density z-lines (nkx_d * ny) and padded stride
+  int ngroup;             // state groups in the plane kernels
+  double box, vol, ecut_psi, ecut_rho, alp_ewd;
+  double gzvps_sum;
+  int nspl; double spl_gmin, spl_dg;
+  int kmax_tab;           // phase table half-width
+  OaFftPlan plan_x, plan_y, plan_z;
+  // device tables
+  int *line_kx, *line_ky, *line_off, *line_nneg, *line_npos;
+  int *kx;                // per g-point
+  double *g2;             // per g-point
+  double2 *tw_x, *tw_y, *tw_z;
+  double *spl;            // [ntype][nspl][4]
+  double *q_type;         // [ntype]
+  int *atm_type;          // [natm]
+  double *pos;            // [natm][3]
+  double2 *phase;         // [natm][3][2*kmax_tab+1] exp(i 2 pi k x / L)
+  double *occ;            // [nstate]
+  // scratch (FFT path precision R; byte sizes)
+  void *zbuf;             // [nstate][nz][ldl] C
+  size_t zbuf_bytes;
+  double *rho_part;       // [ngroup][nz][ny][nx] double (FP64 accumulate)
+  double *rho;            // [nz][ny][nx]
+  void *vks;              // [nz][ny][nx] R
+  double *vxc;            // [nz][ny][nx]
+  void *dz;               // [nz][ldl_d] C  (density z-lines)
+  double *red;            // reduction partials
+  size_t red_len;
+  double *eke_part;       // [nstate][nblk_z]
+  int nblk_z;
+  double energies[8];
+  size_t smem_plane, smem_rho_plane;
+  int npair_s, npair_d, ychunk_s, ychunk_d;
+};
+
+enum { OA_E_EKE = 0, OA_E_EHART, OA_E_EEXT, OA_E_EWALD, OA_E_EEXC, OA_E_MUXC, OA_E_ENL, OA_E_FICT };
+
+#define OA_CUDA_TRY(x)                                  \
+  do {                                                  \
+    cudaError_t e_ = (x);                               \
+    if (e_ != cudaSuccess) { oa_set_error(cudaGetErrorString(e_), __FILE__, __LINE__); return OA_ERR_CUDA; } \
+  } while (0)
+
+void oa_set_error(const char* msg, const char* file, int line);
+
+// stage launchers (return cudaError_t)
+cudaError_t oa_launch_state_zfwd(oa_ctx* c, cudaStream_t s, const double2* psi, int s0, int ns);
+cudaError_t oa_launch_state_plane_density(oa_ctx* c, cudaStream_t s);
+cudaError_t oa_launch_state_plane_vks(oa_ctx* c, cudaStream_t s);
+cudaError_t oa_launch_state_zbwd(oa_ctx* c, cudaStream_t s, const double2* psi, const double2* fnl,
+                                 double2* force, int s0, int ns);
+cudaError_t oa_launch_rho_xc(oa_ctx* c, cudaStream_t s);
+cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s);

@@ -1,0 +1,448 @@
+// PairCalculator, Ortho and CP integrator work on one GPU, FP64 form.
+//
+//   PairCalculator::multiplyForward (ckPairCalculator.C:821-893), tile reduce
+//     contributeSubTiles + sumMatrixDouble (:938-1016, :20-53)        -> k_pc_fwd_f64 + k_pc_fwd_reduce
+//   Ortho::start_calc/do_iteration/step_2/step_3/tolerance_check/collect_error
+//     (ortho.C:109-146, 153-266, 848-971)                             -> k_ortho_ns (cooperative)
+//   Ortho::acceptSectionLambda Gamma = T Lambda (ortho.C:565-570)     -> k_small_gemm_tn
+//   PairCalculator::multiplyResult/bwMultiplyHelper/bwMultiplyDynOrthoT
+//     (ckPairCalculator.C:1201-1468, 1710-2031)                       -> k_pc_bwd_f64
+//   CPINTEGRATE::CP_integrate_dyn/cp_evolve_vel/get_fictKE (cp_dynamics.C:29-270)
+//     + Gamma redundancy sync (CP_State_GSpacePlane.C:2829-2970)     -> k_integrate + k_sync_redundant
+//
+// Operand layout: every state row is its coefficients as 2*ng contiguous
+// doubles (the DGEMM real view).  kx = 0 rows of the reference's 1/sqrt(2),
+// sqrt(2) pre-scalings become per-column weights on the first 2*nkx0 doubles.
+#include <cooperative_groups.h>
+#include "oa_internal.h"
+
+namespace cg = cooperative_groups;
+
+// D = A(8x4, row) * B(4x8, col) + C, FP64 tensor core (DMMA)
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
+// ---------------------------------------------------------------------------
+// forward: part[kb][i][j] = sum_{k in chunk kb} w(k) A[i][k] B[j][k]
+//   64x64 output tile per block, 4 warps each 32x32 (4x4 DMMA tiles),
+//   K staged through shared memory in slabs of 32.
+// ---------------------------------------------------------------------------
+#define PC_TM 64
+#define PC_KS 32
+#define PC_LDS (PC_KS + 4)
+
+__global__ void __launch_bounds__(128)
+k_pc_fwd_f64(const double* __restrict__ A, const double* __restrict__ B, int n, long K, long kchunk,
+             long kx0_cols, double w_kx0, double* __restrict__ part) {
+  __shared__ double As[PC_TM * PC_LDS];
+  __shared__ double Bs[PC_TM * PC_LDS];
+  const int ti = blockIdx.x, tj = blockIdx.y, kb = blockIdx.z;
+  const int i0 = ti * PC_TM, j0 = tj * PC_TM;
+  const long kbeg = (long)kb * kchunk;
+  const long kend = min(K, kbeg + kchunk);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wi = (warp >> 1) * 32, wj = (warp & 1) * 32;
+  double acc[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) { acc[a][b][0] = 0.0; acc[a][b][1] = 0.0; }
+  for (long k0 = kbeg; k0 < kend; k0 += PC_KS) {
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < PC_TM * PC_KS; idx += blockDim.x) {
+      const int r = idx / PC_KS, kk = idx - r * PC_KS;
+      const long k = k0 + kk;
+      double va = 0.0, vb = 0.0;
+      if (k < kend) {
+        const double w = (k < kx0_cols) ? w_kx0 : 1.0;
+        if (i0 + r < n) va = A[(size_t)(i0 + r) * K + k] * w;
+        if (j0 + r < n) vb = B[(size_t)(j0 + r) * K + k];
+      }
+      As[r * PC_LDS + kk] = va;
+      Bs[r * PC_LDS + kk] = vb;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k4 = 0; k4 < PC_KS; k4 += 4) {
+      double af[4], bf[4];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) af[m] = As[(wi + m * 8 + (lane >> 2)) * PC_LDS + k4 + (lane & 3)];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) bf[m] = Bs[(wj + m * 8 + (lane >> 2)) * PC_LDS + k4 + (lane & 3)];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) dmma_8x8x4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+    }
+  }
+  double* out = part + (size_t)kb * n * n;
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = i0 + wi + a * 8 + (lane >> 2);
+      const int j = j0 + wj + b * 8 + 2 * (lane & 3);
+      if (i < n && j < n) out[(size_t)i * n + j] = acc[a][b][0];
+      if (i < n && j + 1 < n) out[(size_t)i * n + j + 1] = acc[a][b][1];
+    }
+}
+
+__global__ void k_pc_fwd_reduce(const double* __restrict__ part, int nkb, int n, double alpha, double* __restrict__ C) {
+  const size_t nn = (size_t)n * n;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (size_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < nkb; ++k) s += part[(size_t)k * nn + i];
+    C[i] = alpha * s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// backward: out[j][c] = a1(c) sum_k M1[k][j] X1[k][c] + a2 sum_k M2[k][j] X2[k][c]
+//   a1(c) = a1_kx0 for c < kx0_cols else a1_rest.  Tile: 64 states x 64 cols,
+//   4 warps each 32x32; K = n (states) staged in slabs of 32.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+k_pc_bwd_f64(const double* __restrict__ M1, const double* __restrict__ X1, double a1_kx0, double a1_rest,
+             const double* __restrict__ M2, const double* __restrict__ X2, double a2,
+             int n, long ncol, long kx0_cols, double* __restrict__ out) {
+  __shared__ double Ms[PC_KS * (PC_TM + 4)];   // [k][j]
+  __shared__ double Xs[PC_KS * (PC_TM + 4)];   // [k][c]
+  const int LDT = PC_TM + 4;
+  const int tj = blockIdx.y;
+  const long c0 = (long)blockIdx.x * PC_TM;
+  const int j0 = tj * PC_TM;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wj = (warp >> 1) * 32, wc = (warp & 1) * 32;
+  double acc1[4][4][2], acc2[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) { acc1[a][b][0] = acc1[a][b][1] = 0.0; acc2[a][b][0] = acc2[a][b][1] = 0.0; }
+  for (int term = 0; term < (M2 ? 2 : 1); ++term) {
+    const double* M = term ? M2 : M1;
+    const double* X = term ? X2 : X1;
+    for (int k0 = 0; k0 < n; k0 += PC_KS) {
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < PC_KS * PC_TM; idx += blockDim.x) {
+        const int kk = idx / PC_TM, r = idx - kk * PC_TM;
+        const int k = k0 + kk;
+        double vm = 0.0, vx = 0.0;
+        if (k < n) {
+          if (j0 + r < n) vm = M[(size_t)k * n + j0 + r];
+          if (c0 + r < ncol) vx = X[(size_t)k * ncol + c0 + r];
+        }
+        Ms[kk * LDT + r] = vm;
+        Xs[kk * LDT + r] = vx;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k4 = 0; k4 < PC_KS; k4 += 4) {
+        double af[4], bf[4];
+        // A fragment (row-major 8x4): A[j][k] = M[k][j]
+#pragma unroll
+        for (int m = 0; m < 4; ++m) af[m] = Ms[(k4 + (lane & 3)) * LDT + wj + m * 8 + (lane >> 2)];
+        // B fragment (col-major 4x8): B[k][c] = X[k][c]
+#pragma unroll
+        for (int m = 0; m < 4; ++m) bf[m] = Xs[(k4 + (lane & 3)) * LDT + wc + m * 8 + (lane >> 2)];
+        if (term == 0) {
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) dmma_8x8x4(acc1[a][b][0], acc1[a][b][1], af[a], bf[b]);
+        } else {
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) dmma_8x8x4(acc2[a][b][0], acc2[a][b][1], af[a], bf[b]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int j = j0 + wj + a * 8 + (lane >> 2);
+      const long c = c0 + wc + b * 8 + 2 * (lane & 3);
+      if (j >= n) continue;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const long cc = c + e;
+        if (cc < ncol) {
+          const double a1 = (cc < kx0_cols) ? a1_kx0 : a1_rest;
+          out[(size_t)j * ncol + cc] = a1 * acc1[a][b][e] + a2 * acc2[a][b][e];
+        }
+      }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// small N x N: C = alpha * A^op B  (op = none), FP64, one output per thread
+// ---------------------------------------------------------------------------
+__global__ void k_small_gemm(const double* __restrict__ A, const double* __restrict__ B, int n, double alpha,
+                             double* __restrict__ C) {
+  const int i = blockIdx.y * 16 + threadIdx.y, j = blockIdx.x * 16 + threadIdx.x;
+  if (i >= n || j >= n) return;
+  double s = 0.0;
+  for (int k = 0; k < n; ++k) s += A[(size_t)i * n + k] * B[(size_t)k * n + j];
+  C[(size_t)i * n + j] = alpha * s;
+}
+
+// ---------------------------------------------------------------------------
+// Newton-Schulz S^-1/2 (ortho.C), one cooperative kernel, bounded iterations.
+//   B = S/2 (or S for lsda); A = I; repeat:
+//     C = 3I - A B;  B <- B C / 2;  A <- C A / 2;
+//     err = sqrt(sum (A_old - A_new)^2 / N^2)
+//   until err <= tol or iter == max_iter.  status[0] = iterations,
+//   status[1] = 1 if converged; errv[0] = err.
+// ---------------------------------------------------------------------------
+#define NS_TS 32
+
+__device__ void ns_tile_gemm(const double* __restrict__ X, const double* __restrict__ Y, int n, double alpha,
+                             double diag, double* __restrict__ Z, int tile, double* sX, double* sY,
+                             const double* __restrict__ Aold, double* err_acc) {
+  // Z[tile] = alpha * X Y + diag * I ; optional err += (Aold - Z)^2 on the tile
+  const int nt = (n + NS_TS - 1) / NS_TS;
+  const int ti = tile / nt, tj = tile - ti * nt;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int k0 = 0; k0 < n; k0 += NS_TS) {
+    __syncthreads();
+    for (int r = ty; r < NS_TS; r += 8) {
+      const int i = ti * NS_TS + r, k = k0 + tx;
+      sX[r * (NS_TS + 1) + tx] = (i < n && k < n) ? X[(size_t)i * n + k] : 0.0;
+      const int kk = k0 + r, j = tj * NS_TS + tx;
+      sY[r * (NS_TS + 1) + tx] = (kk < n && j < n) ? Y[(size_t)kk * n + j] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int k = 0; k < NS_TS; ++k) {
+      const double y = sY[k * (NS_TS + 1) + tx];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] += sX[(ty + 8 * q) * (NS_TS + 1) + k] * y;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int i = ti * NS_TS + ty + 8 * q, j = tj * NS_TS + tx;
+    if (i < n && j < n) {
+      double v = alpha * acc[q] + ((i == j) ? diag : 0.0);
+      Z[(size_t)i * n + j] = v;
+      if (Aold) { const double d = Aold[(size_t)i * n + j] - v; *err_acc += d * d; }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256)
+k_ortho_ns(const double* __restrict__ S, int n, double bscale, double tol, int max_iter,
+           double* __restrict__ A0, double* __restrict__ A1, double* __restrict__ B0, double* __restrict__ B1,
+           double* __restrict__ Cm, double* __restrict__ errpart, double* __restrict__ T,
+           int* __restrict__ status, double* __restrict__ errv) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sX[NS_TS * (NS_TS + 1)];
+  __shared__ double sY[NS_TS * (NS_TS + 1)];
+  __shared__ double sred[32];
+  __shared__ int sdone;
+  const int nt = (n + NS_TS - 1) / NS_TS;
+  const int ntiles = nt * nt;
+  const size_t nn = (size_t)n * n;
+  // init: A = I, B = S * bscale
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i / n), c = (int)(i - (size_t)r * n);
+    A0[i] = (r == c) ? 1.0 : 0.0;
+    B0[i] = S[i] * bscale;
+  }
+  grid.sync();
+  double* A = A0; double* An = A1; double* B = B0; double* Bn = B1;
+  int it = 0;
+  double err = 1.0;
+  while (true) {
+    // C = 3I - A B
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
+      ns_tile_gemm(A, B, n, -1.0, 3.0, Cm, t, sX, sY, nullptr, nullptr);
+    grid.sync();
+    // Bn = B C / 2 ; An = C A / 2 with error partials
+    double e_loc = 0.0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      ns_tile_gemm(B, Cm, n, 0.5, 0.0, Bn, t, sX, sY, nullptr, nullptr);
+      ns_tile_gemm(Cm, A, n, 0.5, 0.0, An, t, sX, sY, A, &e_loc);
+    }
+    // deterministic per-block partial
+    double v = e_loc;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sred[w];
+      errpart[blockIdx.x] = s;
+    }
+    grid.sync();
+    ++it;
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int b = 0; b < (int)gridDim.x; ++b) s += errpart[b];
+      err = sqrt(s / (double)nn);
+      sdone = !(err > tol && it < max_iter);
+      sred[0] = err;
+    }
+    __syncthreads();
+    err = sred[0];
+    const int done = sdone;
+    { double* t = A; A = An; An = t; t = B; B = Bn; Bn = t; }
+    if (done) break;
+    // errpart is rewritten next iteration only after the next grid.sync
+    grid.sync();
+  }
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (size_t)gridDim.x * blockDim.x) T[i] = A[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    status[0] = it;
+    status[1] = (err <= tol) ? 1 : 0;
+    errv[0] = err;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// integrator
+// ---------------------------------------------------------------------------
+__global__ void k_integrate(const double2* __restrict__ F, double2* __restrict__ V, double2* __restrict__ P,
+                            const double* __restrict__ cmass, int ng, int nstate, int r0, int r1, int iend,
+                            double dt, int complete_prev, double* __restrict__ kepart) {
+  __shared__ double sh[32];
+  const size_t total = (size_t)nstate * ng;
+  const double dt2 = 0.5 * dt;
+  double ke = 0.0;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % ng);
+    if (i < r0) continue;
+    double2 f = F[t], v = V[t];
+    const double m = cmass[i];
+    const bool g0 = (i < r1);
+    if (g0) { f.y = 0.0; v.y = 0.0; }
+    if (complete_prev) { v.x += f.x * (dt2 / m); v.y += f.y * (dt2 / m); if (g0) v.y = 0.0; }
+    const double mk = (i >= r1 && i < iend) ? 2.0 * m : m;
+    ke += mk * (v.x * v.x + v.y * v.y);
+    v.x += f.x * (dt2 / m); v.y += f.y * (dt2 / m);
+    if (g0) v.y = 0.0;
+    V[t] = v;
+    double2 p = P[t];
+    p.x += v.x * dt; p.y += v.y * dt;
+    P[t] = p;
+  }
+  double w = ke;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = w;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += sh[k];
+    kepart[blockIdx.x] = 0.5 * s;
+  }
+}
+
+__global__ void k_sync_redundant(double2* __restrict__ P, double2* __restrict__ V, const int* __restrict__ partner,
+                                 int nred, int ng, int nstate) {
+  const size_t total = (size_t)nstate * nred;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int s = (int)(t / nred), i = (int)(t - (size_t)s * nred);
+    const size_t src = (size_t)s * ng + partner[i];
+    const size_t dst = (size_t)s * ng + i;
+    double2 p = P[src]; p.y = -p.y; P[dst] = p;
+    if (V) { double2 v = V[src]; v.y = -v.y; V[dst] = v; }
+  }
+}
+
+__global__ void k_sum_partials(const double* __restrict__ part, int n, int stride, int off, double scale,
+                               double* __restrict__ out) {
+  // one block: out[0] = scale * sum_i part[i*stride + off]
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += part[(size_t)i * stride + off];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+    out[0] = scale * t;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+cudaError_t oa_launch_pc_fwd(cudaStream_t s, const double* A, const double* B, int n, long K, long kx0_cols,
+                             double w_kx0, double alpha, double* part, int nkb, double* C) {
+  const long kchunk = ((K + nkb - 1) / nkb + PC_KS - 1) / PC_KS * PC_KS;
+  const int nkb_eff = (int)((K + kchunk - 1) / kchunk);
+  dim3 grid((n + PC_TM - 1) / PC_TM, (n + PC_TM - 1) / PC_TM, nkb_eff);
+  k_pc_fwd_f64<<<grid, 128, 0, s>>>(A, B, n, K, kchunk, kx0_cols, w_kx0, part);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_pc_fwd_reduce<<<(n * n + 255) / 256, 256, 0, s>>>(part, nkb_eff, n, alpha, C);
+  return cudaGetLastError();
+}
+
+cudaError_t oa_launch_pc_bwd(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
+                             const double* M2, const double* X2, double a2, int n, long ncol, long kx0_cols,
+                             double* out) {
+  dim3 grid((unsigned)((ncol + PC_TM - 1) / PC_TM), (n + PC_TM - 1) / PC_TM);
+  k_pc_bwd_f64<<<grid, 128, 0, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, n, ncol, kx0_cols, out);
+  return cudaGetLastError();
+}
+
+cudaError_t oa_launch_small_gemm(cudaStream_t s, const double* A, const double* B, int n, double alpha, double* C) {
+  dim3 grid((n + 15) / 16, (n + 15) / 16), blk(16, 16);
+  k_small_gemm<<<grid, blk, 0, s>>>(A, B, n, alpha, C);
+  return cudaGetLastError();
+}
+
+int oa_ns_grid(int n, int device) {
+  const int nt = (n + NS_TS - 1) / NS_TS;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ortho_ns, 256, 0);
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  int g = nt * nt;
+  const int cap = per_sm * nsm;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return g;
+}
+
+cudaError_t oa_launch_ortho_ns(cudaStream_t s, const double* S, int n, double bscale, double tol, int max_iter,
+                               double* work /* 5 n^2 + grid */, double* T, int* status, double* errv, int grid) {
+  const size_t nn = (size_t)n * n;
+  double* A0 = work; double* A1 = A0 + nn; double* B0 = A1 + nn; double* B1 = B0 + nn; double* Cm = B1 + nn;
+  double* errpart = Cm + nn;
+  void* args[] = {(void*)&S, (void*)&n, (void*)&bscale, (void*)&tol, (void*)&max_iter, (void*)&A0, (void*)&A1,
+                  (void*)&B0, (void*)&B1, (void*)&Cm, (void*)&errpart, (void*)&T, (void*)&status, (void*)&errv};
+  return cudaLaunchCooperativeKernel((void*)k_ortho_ns, dim3(grid), dim3(256), args, 0, s);
+}
+
+cudaError_t oa_launch_integrate(cudaStream_t s, const double2* F, double2* V, double2* P, const double* cmass,
+                                int ng, int nstate, int r0, int r1, int iend, double dt, int complete_prev,
+                                double* kepart, int nblk) {
+  k_integrate<<<nblk, 256, 0, s>>>(F, V, P, cmass, ng, nstate, r0, r1, iend, dt, complete_prev, kepart);
+  return cudaGetLastError();
+}
+
+cudaError_t oa_launch_sync_redundant(cudaStream_t s, double2* P, double2* V, const int* partner, int nred, int ng,
+                                     int nstate) {
+  if (nred == 0) return cudaSuccess;
+  const size_t total = (size_t)nstate * nred;
+  const int nb = (int)((total + 255) / 256 < 4096 ? (total + 255) / 256 : 4096);
+  k_sync_redundant<<<nb, 256, 0, s>>>(P, V, partner, nred, ng, nstate);
+  return cudaGetLastError();
+}
+
+cudaError_t oa_launch_sum_partials(cudaStream_t s, const double* part, int n, int stride, int off, double scale,
+                                   double* out) {
+  k_sum_partials<<<1, 256, 0, s>>>(part, n, stride, off, scale, out);
+  return cudaGetLastError();
+}

@@ -1,0 +1,346 @@
+"""ctypes binding of liboa_gpu and the host-side CP step driver.
+
+``CPContext`` exposes one method per C-ABI entry point (include/oa_gpu.h);
+``CPDriver`` sequences one Car-Parrinello dynamics step the way
+``GSpaceDriver::computeDynamics`` does (src_charm_driver/cp_state_ctrl/gspace.ci:199-324):
+forces on the orthonormal states (computePsiFandVKS + combineForcesGetEke),
+the constraint force (computeLambdaAndCg), integration (integrateModForce)
+and orthonormalisation (computeNewPsi).
+
+Device memory and streams come from torch; there is no CPU fallback: every
+method raises if the CUDA library or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liboa_gpu.so")
+
+OA_OK, OA_ERR_BAD_ARG, OA_ERR_CUDA, OA_ERR_NOT_CONVERGED, OA_ERR_NONFINITE, OA_ERR_UNSUPPORTED = range(6)
+OA_FP64, OA_MIXED = 0, 1
+
+_ip = C.POINTER(C.c_int)
+_dp = C.POINTER(C.c_double)
+
+
+class SystemDesc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("nstate", C.c_int), ("ng", C.c_int), ("nlines", C.c_int),
+        ("line_kx", _ip), ("line_ky", _ip), ("line_off", _ip), ("line_nneg", _ip), ("line_npos", _ip),
+        ("kx", _ip), ("ky", _ip), ("kz", _ip),
+        ("nkx0", C.c_int), ("nkx0_red", C.c_int), ("nkx0_uni", C.c_int), ("nkx0_zero", C.c_int),
+        ("red_partner", _ip),
+        ("box", C.c_double), ("ecut_psi", C.c_double), ("ecut_rho", C.c_double),
+        ("occ", _dp), ("cmass", _dp),
+        ("natm", C.c_int), ("ntype", C.c_int),
+        ("pos", _dp), ("atm_type", _ip), ("q_type", _dp), ("gzvps", _dp),
+        ("alp_ewd", C.c_double),
+        ("nspl", C.c_int), ("spl_gmin", C.c_double), ("spl_dg", C.c_double), ("spl", _dp),
+    ]
+
+
+# name -> (restype, argtypes); the exported surface of include/oa_gpu.h
+_vp = C.c_void_p
+SIGNATURES = {
+    "oa_gpu_init": (C.c_int, [C.POINTER(SystemDesc), C.c_int, C.POINTER(_vp)]),
+    "oa_gpu_destroy": (C.c_int, [_vp]),
+    "oa_gpu_last_error": (C.c_char_p, []),
+    "oa_gpu_scratch_bytes": (C.c_size_t, [_vp]),
+    "oa_gpu_state_fft_fwd": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "oa_gpu_vks_build": (C.c_int, [_vp, _vp, _vp]),
+    "oa_gpu_set_vks": (C.c_int, [_vp, _vp, _vp]),
+    "oa_gpu_vks_apply_fft_bwd": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp, _vp]),
+    "oa_gpu_pc_forward": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_double, _vp]),
+    "oa_gpu_ortho_invsqrt": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_int, _ip, _dp]),
+    "oa_gpu_pc_backward": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_double, _vp, _vp, C.c_double, _vp]),
+    "oa_gpu_small_gemm": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, _vp]),
+    "oa_gpu_integrate": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_double, C.c_int, _vp]),
+    "oa_gpu_energies": (C.c_int, [_vp, _vp, _dp]),
+    "oa_gpu_psiv_reset": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "oa_gpu_set_atoms": (C.c_int, [_vp, _vp, _dp]),
+    "oa_gpu_time_kernels": (C.c_int, [_vp, _vp, _vp, C.c_int, _dp]),
+    "oa_gpu_sizes": (C.c_int, [_vp, C.POINTER(C.c_long)]),
+}
+
+KERNEL_NAMES = ("state_zfwd", "state_plane_density", "rho_xc", "vks_build", "state_plane_vks",
+                "state_zbwd", "pc_forward_S", "pc_backward", "ortho_ns")
+
+_lib = None
+
+
+class OaError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"liboa_gpu status {status}: {msg}")
+        self.status = status
+
+
+def load_library(path: str = LIB_PATH):
+    """Load liboa_gpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError(f"{path} not found: build it with `python -m openatom_b200.build`")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(st):
+    if st != OA_OK:
+        raise OaError(st, _lib.oa_gpu_last_error().decode())
+
+
+def _ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def _iarr(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _darr(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def redundant_partner(sysm) -> np.ndarray:
+    key = {(int(sysm.ky[i]), int(sysm.kz[i])): i for i in range(sysm.nkx0)}
+    return np.array([key[(-int(sysm.ky[i]), -int(sysm.kz[i]))] for i in range(sysm.nkx0_red)], dtype=np.int32)
+
+
+class CPContext:
+    """One system on the current CUDA device (one ``oa_ctx``)."""
+
+    def __init__(self, sysm, precision: str = "fp64"):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("CPContext needs a CUDA device; there is no CPU path")
+        lib = load_library()
+        self.sys = sysm
+        self.precision = OA_FP64 if precision == "fp64" else OA_MIXED
+        keep = dict(
+            line_kx=_iarr(sysm.line_kx), line_ky=_iarr(sysm.line_ky), line_off=_iarr(sysm.line_off),
+            line_nneg=_iarr(sysm.line_nneg), line_npos=_iarr(sysm.line_npos),
+            kx=_iarr(sysm.kx), ky=_iarr(sysm.ky), kz=_iarr(sysm.kz), red=_iarr(redundant_partner(sysm)),
+            occ=_darr(sysm.occ), cmass=_darr(sysm.cmass), pos=_darr(sysm.pos), atm_type=_iarr(sysm.atm_type),
+            q_type=_darr([6.0, 1.0][: len(sysm.type_names)]), gzvps=_darr(sysm.gzvps),
+            spl=_darr(sysm.vloc.coef))
+        # per-type valence charge from the atoms
+        qt = np.zeros(len(sysm.type_names))
+        for t in range(len(sysm.type_names)):
+            m = sysm.atm_type == t
+            if m.any():
+                qt[t] = sysm.q[m][0]
+        keep["q_type"] = _darr(qt)
+
+        def ip(a):
+            return a.ctypes.data_as(_ip)
+
+        def dp(a):
+            return a.ctypes.data_as(_dp)
+
+        d = SystemDesc()
+        d.nx, d.ny, d.nz = sysm.nfft
+        d.nstate, d.ng, d.nlines = sysm.nstate, sysm.ng, sysm.nlines
+        d.line_kx, d.line_ky, d.line_off = ip(keep["line_kx"]), ip(keep["line_ky"]), ip(keep["line_off"])
+        d.line_nneg, d.line_npos = ip(keep["line_nneg"]), ip(keep["line_npos"])
+        d.kx, d.ky, d.kz = ip(keep["kx"]), ip(keep["ky"]), ip(keep["kz"])
+        d.nkx0, d.nkx0_red, d.nkx0_uni, d.nkx0_zero = sysm.nkx0, sysm.nkx0_red, sysm.nkx0_uni, sysm.nkx0_zero
+        d.red_partner = ip(keep["red"])
+        d.box, d.ecut_psi, d.ecut_rho = sysm.box, sysm.ecut_ry, sysm.ecut_rho_g2
+        d.occ, d.cmass = dp(keep["occ"]), dp(keep["cmass"])
+        d.natm, d.ntype = sysm.natm, len(sysm.type_names)
+        d.pos, d.atm_type, d.q_type, d.gzvps = dp(keep["pos"]), ip(keep["atm_type"]), dp(keep["q_type"]), dp(keep["gzvps"])
+        d.alp_ewd = sysm.alp_ewd
+        d.nspl, d.spl_gmin, d.spl_dg, d.spl = sysm.vloc.n, sysm.vloc.gmin, sysm.vloc.dg, dp(keep["spl"])
+        h = C.c_void_p()
+        _check(lib.oa_gpu_init(C.byref(d), self.precision, C.byref(h)))
+        self._h = h
+        self._lib = lib
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.oa_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _stream():
+        import torch
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def scratch_bytes(self) -> int:
+        return int(self._lib.oa_gpu_scratch_bytes(self._h))
+
+    # -- entry points -------------------------------------------------------
+    def state_fft_fwd(self, psi, rho_out=None):
+        _check(self._lib.oa_gpu_state_fft_fwd(self._h, self._stream(), _ptr(psi), _ptr(rho_out)))
+
+    def vks_build(self, vks_out=None):
+        _check(self._lib.oa_gpu_vks_build(self._h, self._stream(), _ptr(vks_out)))
+
+    def set_vks(self, vks):
+        _check(self._lib.oa_gpu_set_vks(self._h, self._stream(), _ptr(vks)))
+
+    def vks_apply_fft_bwd(self, psi, force, fnl=None, recompute_fwd=False, eke_out=None):
+        _check(self._lib.oa_gpu_vks_apply_fft_bwd(self._h, self._stream(), _ptr(psi), int(recompute_fwd),
+                                                  _ptr(fnl), _ptr(force), _ptr(eke_out)))
+
+    def pc_forward(self, left, right, alpha, w_kx0, out):
+        _check(self._lib.oa_gpu_pc_forward(self._h, self._stream(), _ptr(left), _ptr(right),
+                                           float(alpha), float(w_kx0), _ptr(out)))
+
+    def ortho_invsqrt(self, S, T, tol=1e-15, max_iter=1000):
+        it = C.c_int(0)
+        err = C.c_double(0.0)
+        st = self._lib.oa_gpu_ortho_invsqrt(self._h, self._stream(), _ptr(S), _ptr(T), float(tol), int(max_iter),
+                                            C.byref(it), C.byref(err))
+        if st not in (OA_OK, OA_ERR_NOT_CONVERGED):
+            _check(st)
+        return it.value, err.value, st == OA_OK
+
+    def pc_backward(self, M1, X1, a1_kx0, a1_rest, out, M2=None, X2=None, a2=0.0):
+        _check(self._lib.oa_gpu_pc_backward(self._h, self._stream(), _ptr(M1), _ptr(X1), float(a1_kx0),
+                                            float(a1_rest), _ptr(M2), _ptr(X2), float(a2), _ptr(out)))
+
+    def small_gemm(self, A, B, alpha, out):
+        _check(self._lib.oa_gpu_small_gemm(self._h, self._stream(), _ptr(A), _ptr(B), float(alpha), _ptr(out)))
+
+    def integrate(self, force, vpsi, psi, dt, complete_prev, fict_out=None):
+        _check(self._lib.oa_gpu_integrate(self._h, self._stream(), _ptr(force), _ptr(vpsi), _ptr(psi), float(dt),
+                                          int(complete_prev), _ptr(fict_out)))
+
+    def psiv_reset(self, psi, psi_t, vpsi):
+        _check(self._lib.oa_gpu_psiv_reset(self._h, self._stream(), _ptr(psi), _ptr(psi_t), _ptr(vpsi)))
+
+    def set_atoms(self, pos_host: np.ndarray):
+        a = np.ascontiguousarray(pos_host, dtype=np.float64)
+        _check(self._lib.oa_gpu_set_atoms(self._h, self._stream(), a.ctypes.data_as(_dp)))
+
+    def sizes(self) -> dict:
+        out = (C.c_long * 10)()
+        _check(self._lib.oa_gpu_sizes(self._h, out))
+        keys = ("nstate", "ng", "nlines", "nz", "ldl", "ngroup", "npts", "rbytes", "nlines_d", "launches_per_step")
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def time_kernels(self, psi, reps: int = 5) -> dict:
+        out = (C.c_double * 9)()
+        _check(self._lib.oa_gpu_time_kernels(self._h, self._stream(), _ptr(psi), int(reps), out))
+        return {k: float(v) for k, v in zip(KERNEL_NAMES, out)}
+
+    def algorithmic_bytes(self) -> dict:
+        """Compulsory HBM bytes per launch of each kernel (inputs read once,
+        outputs written once) -- the numerator of the roofline."""
+        z = self.sizes()
+        n, ng, nl, nz, npts, g = z["nstate"], z["ng"], z["nlines"], z["nz"], z["npts"], z["ngroup"]
+        cb = 2 * z["rbytes"]
+        zrow = n * nz * nl * cb          # the z-line buffer
+        coef = n * ng * 16               # one coefficient array
+        return {
+            "state_zfwd": coef + zrow,
+            "state_plane_density": zrow + g * npts * 8,
+            "rho_xc": g * npts * 8 + 2 * npts * 8,
+            "vks_build": npts * 8 * 2 + npts * z["rbytes"],
+            "state_plane_vks": 2 * zrow + g * npts * z["rbytes"],
+            "state_zbwd": zrow + 2 * coef + ng * 8,
+            "pc_forward_S": coef + n * n * 8,
+            "pc_backward": 3 * coef,
+            "ortho_ns": 2 * n * n * 8,
+        }
+
+    def energies(self) -> dict:
+        out = (C.c_double * 7)()
+        _check(self._lib.oa_gpu_energies(self._h, self._stream(), out))
+        keys = ("EKE", "EHART", "EEXT", "EWALD_RECIP", "EEXC", "MUXC", "FICT_KE")
+        return {k: float(v) for k, v in zip(keys, out)}
+
+
+class CPDriver:
+    """Host runner of the CP dynamics step on one GPU (electrons; ions fixed)."""
+
+    def __init__(self, sysm, precision: str = "fp64", tol: float = 1e-15, max_iter: int = 1000,
+                 psi0=None):
+        import torch
+        self.torch = torch
+        self.sys = sysm
+        self.ctx = CPContext(sysm, precision)
+        dev = torch.device("cuda")
+        n, ng = sysm.nstate, sysm.ng
+        p0 = sysm.psi if psi0 is None else psi0
+        self.psi_t = torch.from_numpy(np.ascontiguousarray(p0)).to(dev)   # non-orthogonal, integrated
+        self.psi = self.psi_t.clone()                                     # orthonormal psi_t T
+        self.v = torch.zeros_like(self.psi)
+        self.F = torch.zeros_like(self.psi)
+        self.F2 = torch.zeros_like(self.psi)
+        self.T = torch.eye(n, dtype=torch.float64, device=dev)
+        self.S = torch.zeros(n, n, dtype=torch.float64, device=dev)
+        self.lam = torch.zeros_like(self.S)
+        self.gam = torch.zeros_like(self.S)
+        self.tol, self.max_iter = tol, max_iter
+        self.iteration = 0
+        self.last_ortho = (0, 0.0, True)
+
+    def forces(self):
+        """computePsiFandVKS + combineForcesGetEke on the orthonormal psi."""
+        c = self.ctx
+        c.state_fft_fwd(self.psi)
+        c.vks_build()
+        c.vks_apply_fft_bwd(self.psi, self.F)
+
+    def launches_per_step(self) -> int:
+        return self.ctx.sizes()["launches_per_step"]
+
+    def psiv_reset(self):
+        """PsiV tolerance reset (oracle.psiv_reset restates the reference)."""
+        self.ctx.psiv_reset(self.psi, self.psi_t, self.v)
+        self.T.copy_(self.torch.eye(self.sys.nstate, dtype=self.torch.float64, device=self.T.device))
+
+    def quench(self, nsteps: int, dt: float | None = None):
+        """Damped CP (steepest descent on the orthonormal states): each step
+        zeroes the velocities and resets psi_t to psi.  Used to bring a random
+        start near the Born-Oppenheimer surface before dynamics."""
+        out = []
+        for _ in range(nsteps):
+            out.append(self.step(damp_velocity=True, dt=dt))
+            self.psiv_reset()
+            self.iteration = 0
+        return out
+
+    def step(self, damp_velocity: bool = False, dt: float | None = None) -> dict:
+        c, s = self.ctx, self.sys
+        dt = s.dt if dt is None else dt
+        self.iteration += 1
+        self.forces()
+        en = c.energies()
+        # Lambda = <psi_x | F_y>, Gamma = T Lambda, F' = F T - Psi Gamma (kx0 psi term halved)
+        c.pc_forward(self.psi, self.F, 1.0, 1.0, self.lam)
+        c.small_gemm(self.T, self.lam, 1.0, self.gam)
+        c.pc_backward(self.gam, self.psi, -0.5, -1.0, self.F2, M2=self.T, X2=self.F, a2=1.0)
+        # integrate psi_t
+        c.integrate(self.F2, self.v, self.psi_t, dt, self.iteration > 1)
+        en["FICT_KE"] = c.energies()["FICT_KE"]
+        if damp_velocity:
+            self.v.zero_()
+        # orthonormalise: S = 2 sum w psi psi (kx0 weight 1/2), T = (S/2)^-1/2, psi = psi_t T
+        c.pc_forward(self.psi_t, self.psi_t, 2.0, 0.5, self.S)
+        it, err, ok = c.ortho_invsqrt(self.S, self.T, self.tol, self.max_iter)
+        self.last_ortho = (it, err, ok)
+        c.pc_backward(self.T, self.psi_t, 1.0, 1.0, self.psi)
+        en["ORTHO_ITERS"] = it
+        en["ORTHO_ERR"] = err
+        return en

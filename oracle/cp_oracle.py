@@ -1,0 +1,470 @@
+"""CPU oracle for the OpenAtom Gamma-point CP electronic step (FP64, numpy).
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker: only the tests, the
+smoke check in ``__graft_entry__`` and the ``cpu_baseline`` / ``--impl
+reference`` legs of ``bench.py`` may import it.  The product path
+(``openatom_b200``) never calls it and fails loudly without its CUDA library.
+
+Each function restates one reference routine and cites it.  FFTs use numpy's
+pocketfft, GEMMs use numpy BLAS: FFTW2 / Fortran BLAS / the Charm-FFT library
+of the reference are not present, so parity at those boundaries is pinned by
+mathematics (any correct FP64 FFT/GEMM), while the physics kernels
+(cp_eke, cp_pz_lda, cp_hart_ext, Newton-Schulz, cp_dynamics) are pinned
+against the reference's own source compiled into ``oracle/_ref`` (see
+``oracle/build_ref.sh`` and ``tests/test_oracle_pin.py``).
+
+Sign conventions (``src_charm_driver/fft_slab_ctrl/fftCache.C:100-160``):
+state "forward" plans are FFTW_FORWARD (exp(-i g.r)) and the c2r x-transform
+is preceded by conjugation (``fftCache.C:1206-1212``), so
+psi(r) = sum_{full sphere} c(g) exp(-i g.r); the backward path uses
+exp(+i g.r).  The density forward transform is exp(-i g.r) with the V/N
+volume factor (``CP_Rho_RealSpacePlane.C:846-851``).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+TWO_PI = 2.0 * math.pi
+
+_FFT_WORKERS = 1
+
+
+def set_fft_workers(n: int):
+    """Threads for the oracle's FFTs (scipy.fft workers); 1 = numpy."""
+    global _FFT_WORKERS
+    _FFT_WORKERS = max(1, int(n))
+
+
+def _fftn(a, axes=None):
+    if _FFT_WORKERS > 1:
+        import scipy.fft as sf
+        return sf.fftn(a, axes=axes, workers=_FFT_WORKERS)
+    return np.fft.fftn(a, axes=axes)
+
+
+def _ifftn(a, axes=None):
+    if _FFT_WORKERS > 1:
+        import scipy.fft as sf
+        return sf.ifftn(a, axes=axes, workers=_FFT_WORKERS)
+    return np.fft.ifftn(a, axes=axes)
+
+
+# ----------------------------------------------------------------------------
+# sphere <-> grid
+# ----------------------------------------------------------------------------
+
+def expand_gspace(packed, sysm):
+    """``FFTcache::expandGSpace`` (``fftCache.C:460-507``): packed runs ->
+    zero-filled z-lines [.., nlines, nz]; kz < 0 goes to index kz + nz."""
+    nz = sysm.nfft[2]
+    out = np.zeros(packed.shape[:-1] + (sysm.nlines, nz), dtype=packed.dtype)
+    line = np.repeat(np.arange(sysm.nlines), sysm.line_nneg + sysm.line_npos)
+    out[..., line, sysm.kz % nz] = packed
+    return out
+
+
+def pack_gspace(lines, sysm):
+    """``FFTcache::packGSpace`` (``fftCache.C:517-553``)."""
+    nz = sysm.nfft[2]
+    line = np.repeat(np.arange(sysm.nlines), sysm.line_nneg + sysm.line_npos)
+    return lines[..., line, sysm.kz % nz]
+
+
+def _full_grid(coef, kx, ky, kz, nfft, hermitian_partner=True):
+    """Scatter half-sphere coefficients onto a full [.., nz, ny, nx] grid and
+    add the Hermitian partner c(-g) = conj(c(g)) for kx > 0."""
+    nx, ny, nz = nfft
+    out = np.zeros(coef.shape[:-1] + (nz, ny, nx), dtype=np.complex128)
+    out[..., kz % nz, ky % ny, kx % nx] = coef
+    if hermitian_partner:
+        m = kx > 0
+        out[..., (-kz[m]) % nz, (-ky[m]) % ny, (-kx[m]) % nx] = np.conj(coef[..., m])
+    return out
+
+
+def state_g_to_r(psi, sysm):
+    """G-sphere -> real space for each state: the composition of
+    ``doStpFFTGtoR_Gchare`` (expand + z FFT, ``fftCache.C:1133-1159``), the
+    z->R transpose (``CP_State_GSpacePlane.C:1448-1517``,
+    ``CP_State_RealSpacePlane.C:186-271``) and ``doStpFFTGtoR_Rchare``
+    (y FFT, conjugate, c2r x FFT, ``fftCache.C:1167-1243``).
+    Returns psi(r) as float64 [nstate, nz, ny, nx]."""
+    nx, ny, nz = sysm.nfft
+    out = np.empty(psi.shape[:-1] + (nz, ny, nx))
+    flat_in = psi.reshape(-1, psi.shape[-1])
+    flat_out = out.reshape(-1, nz, ny, nx)
+    for c0 in range(0, flat_in.shape[0], 16):
+        full = _full_grid(flat_in[c0:c0 + 16], sysm.kx, sysm.ky, sysm.kz, sysm.nfft)
+        flat_out[c0:c0 + 16] = _fftn(full, axes=(-3, -2, -1)).real
+    return out
+
+
+def state_r_to_g(fr, sysm):
+    """Real space -> g-sphere, unnormalised exp(+i g.r): ``doStpFFTRtoG_Rchare``
+    (r2c x, conjugate, y FFT, ``fftCache.C:1252-1319``), transpose back, and
+    ``doStpFFTRtoG_Gchare`` (z FFT + pack, ``fftCache.C:1099-1123``)."""
+    n = fr.shape[-1] * fr.shape[-2] * fr.shape[-3]
+    nx, ny, nz = sysm.nfft
+    flat = fr.reshape(-1, nz, ny, nx)
+    out = np.empty((flat.shape[0], sysm.ng), dtype=np.complex128)
+    for c0 in range(0, flat.shape[0], 16):
+        full = _ifftn(flat[c0:c0 + 16], axes=(-3, -2, -1)) * n
+        out[c0:c0 + 16] = full[:, sysm.kz % nz, sysm.ky % ny, sysm.kx % nx]
+    return out.reshape(fr.shape[:-3] + (sysm.ng,))
+
+
+# ----------------------------------------------------------------------------
+# density, XC, Hartree + local
+# ----------------------------------------------------------------------------
+
+def density(psir, sysm):
+    """rho(r) = sum_s occ_s w_k psi_s(r)^2 / V
+    (``CP_State_RealSpacePlane.C:349-363`` then the probScale = 1/V scaling
+    of ``CP_Rho_RealSpacePlane.C:136-138,500``)."""
+    return np.einsum("s,szyx->zyx", sysm.occ, psir * psir) / sysm.vol
+
+
+def pz_lda(rho, vol, npts):
+    """``CPXCFNCTS::CP_exc_calc`` (``abinito_physics/cp_xc_fnctl/cp_pz_lda.C:23-175``):
+    Perdew-Zunger LDA.  Returns (vxc(r), exc, muxc)."""
+    gamma, beta1, beta2 = -0.14230, 1.05290, 0.33340
+    au, bu, cu, du = 0.03110, -0.0480, 0.00200, -0.01160
+    power = 1.0 / 3.0
+    rat1 = (7.0 / 6.0) * beta1
+    rat2 = (4.0 / 3.0) * beta2
+    fpin = 4.0 * math.pi * rho
+    rs = np.power(3.0 / fpin, power)
+    sqtrs = np.sqrt(rs)
+    xfact = -np.power(3.0 * rho / math.pi, power)
+    hi = rs >= 1.0
+    cf1 = 1.0 + beta1 * sqtrs + beta2 * rs
+    cf2 = 1.0 + rat1 * sqtrs + rat2 * rs
+    c_hi = gamma / cf1
+    m_hi = c_hi * (cf2 / cf1)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        lnrs = np.log(rs)
+    c_lo = au * lnrs + bu + cu * rs * lnrs + du * rs
+    m_lo = (au * lnrs + (bu - power * au) + 2.0 * power * cu * rs * lnrs
+            + power * (2.0 * du - cu) * rs)
+    cfact = np.where(hi, c_hi, c_lo)
+    mufact = np.where(hi, m_hi, m_lo)
+    ex = float(np.sum(xfact * rho)) * 0.75
+    ec = float(np.sum(cfact * rho))
+    v = xfact + mufact
+    vxc_sum = float(np.sum(v * rho))
+    vscale = vol / npts
+    return v, (ex + ec) * vscale, vxc_sum * vscale
+
+
+def rho_sphere(sysm):
+    """Density g-points: kx >= 0 half of g^2 <= 4 Ecut with the whole kx = 0
+    plane (weight 1 on kx = 0, 2 elsewhere, ``cp_hart_ext.C:196-205``)."""
+    nx, ny, nz = sysm.nfft
+    f = TWO_PI / sysm.box
+    kxs = np.arange(0, nx // 2 + 1)
+    kys = np.arange(-(ny // 2), ny - ny // 2)
+    kzs = np.arange(-(nz // 2), nz - nz // 2)
+    KX, KY, KZ = np.meshgrid(kxs, kys, kzs, indexing="ij")
+    g2 = f * f * (KX ** 2 + KY ** 2 + KZ ** 2)
+    m = (g2 <= sysm.ecut_rho_g2)
+    return KX[m], KY[m], KZ[m], g2[m]
+
+
+def hart_eext(rho_r, sysm, want_forces=False):
+    """``CPLOCAL::CP_hart_eext_calc`` (``abinito_physics/cp_local/cp_hart_ext.C:56-431``)
+    on rho(g) = FFT_-[rho(r) V/N] (``CP_Rho_RealSpacePlane.C:846-851``).
+    Returns (vks_hart_ext(r), ehart, eext, ewald_recip[, fatm])."""
+    nx, ny, nz = sysm.nfft
+    n = nx * ny * nz
+    vol = sysm.vol
+    rhog_full = _fftn(rho_r * (vol / n))
+    kx, ky, kz, g2 = rho_sphere(sysm)
+    rho = rhog_full[kz % nz, ky % ny, kx % nx]
+    f = TWO_PI / sysm.box
+    gx, gy, gz = f * kx, f * ky, f * kz
+    nz0 = g2 != 0
+    w = np.where(kx == 0, 1.0, 2.0)
+    # Hartree
+    hf = np.zeros_like(g2)
+    hf[nz0] = 4.0 * math.pi / (g2[nz0] * vol)
+    ehart = float(np.sum(hf * np.abs(rho) ** 2 * w)) / 2.0
+    vks = rho * hf
+    # structure factor h = exp(i g.R) and local pseudopotential
+    arg = np.outer(gx, sysm.pos[:, 0]) + np.outer(gy, sysm.pos[:, 1]) + np.outer(gz, sysm.pos[:, 2])
+    h = np.exp(1j * arg)                                  # [ng, natm]
+    g = np.sqrt(g2)
+    vtyp = np.stack([sysm.vloc.eval(np.full(g.shape, t), g) for t in range(len(sysm.type_names))], axis=1) / vol
+    vtemp = vtyp[:, sysm.atm_type]                        # [ng, natm]
+    vext = np.sum(h * vtemp, axis=1)
+    sewd = h @ sysm.q
+    falp2 = 4.0 * sysm.alp_ewd ** 2
+    ewf = np.zeros_like(g2)
+    ewf[nz0] = 4.0 * math.pi * np.exp(-g2[nz0] / falp2) / (g2[nz0] * vol)
+    ewald = float(np.sum(ewf * np.abs(sewd) ** 2 * w)) / 2.0
+    vks = np.where(nz0, vks + np.conj(vext), 0.0)
+    eext = float(np.sum(np.where(nz0, (rho * vext).real * w, 0.0)))
+    fatm = None
+    if want_forces:
+        rr = (rho.real * w)[:, None] * vtemp + ((sewd.real * ewf * w)[:, None] * sysm.q[None, :])
+        ri = (-rho.imag * w)[:, None] * vtemp + ((sewd.imag * ewf * w)[:, None] * sysm.q[None, :])
+        comp = rr * h.imag - ri * h.real
+        fatm = np.stack([(gx[:, None] * comp).sum(0), (gy[:, None] * comp).sum(0), (gz[:, None] * comp).sum(0)], axis=1)
+    # g = 0 term (cp_hart_ext.C:366-395)
+    iz = np.nonzero(~nz0)[0]
+    if iz.size:
+        v0 = float(np.sum(sysm.gzvps[sysm.atm_type])) / vol
+        vks[iz[0]] = v0
+        eext += v0 * rho[iz[0]].real
+    # V(r) = sum_{full sphere} vks(g) exp(+i g.r)
+    full = np.zeros((nz, ny, nx), dtype=np.complex128)
+    full[kz % nz, ky % ny, kx % nx] = vks
+    m = kx > 0
+    full[(-kz[m]) % nz, (-ky[m]) % ny, (-kx[m]) % nx] = np.conj(vks[m])
+    vr = (_ifftn(full) * n).real
+    out = (vr, ehart, eext, ewald)
+    return out + (fatm,) if want_forces else out
+
+
+def vks_build(psir, sysm):
+    """Density -> V_KS(r) = V_xc + V_H + V_loc with the energy terms
+    (``CP_Rho_RealSpacePlane::energyComputation`` 739-800, ``HartExtVksG``
+    ``CP_Rho_GHartExt.C:461-510``, ``acceptHartVks`` 1365-1390)."""
+    rho = density(psir, sysm)
+    vxc, exc, muxc = pz_lda(rho, sysm.vol, sysm.npts)
+    vh, ehart, eext, ewald = hart_eext(rho, sysm)
+    return rho, vxc + vh, dict(EEXC=exc, MUXC=muxc, EHART=ehart, EEXT=eext, EWALD_RECIP=ewald)
+
+
+# ----------------------------------------------------------------------------
+# forces, EKE
+# ----------------------------------------------------------------------------
+
+def vks_forces(psir, vks, sysm):
+    """psi(r) *= V_KS(r) occ w_k (``CP_State_RealSpacePlane::unpackVks`` 580-596),
+    back-transform, F = -2/N * result (``CP_State_GSpacePlane::doIFFT``
+    1581-1612)."""
+    prod = psir * (vks[None] * sysm.occ[:, None, None, None])
+    g = state_r_to_g(prod, sysm)
+    return g * (-2.0 / sysm.npts)
+
+
+def add_forces(fks, fnl, sysm):
+    """``GStateSlab::addForces`` (``fft_slab_ctrl/stateSlab.C:239-268``):
+    kx > 0 FFT forces are doubled before the nonlocal forces are added."""
+    f = np.where(sysm.kx == 0, 1.0, 2.0) * fks
+    return f + fnl if fnl is not None else f
+
+
+def eke(psi, forces, sysm, kpt_weight=1.0):
+    """``CPNONLOCAL::CP_eke_calc`` (``abinito_physics/cp_nonlocal/cp_eke.C:30-140``).
+    Returns (new forces, per-state EKE)."""
+    g2 = sysm.g2()
+    ecut = sysm.ecut_ry
+    w = np.where(sysm.kx == 0, 1.0, 2.0)
+    wt = (sysm.occ * kpt_weight)[:, None] * w[None, :]
+    inside = g2 <= ecut
+    f = np.where(inside[None, :], forces - psi * (wt * g2[None, :]), 0.0)
+    e = np.sum(np.where(inside[None, :], wt * g2[None, :] * np.abs(psi) ** 2, 0.0), axis=1) / 2.0
+    return f, e
+
+
+# ----------------------------------------------------------------------------
+# PairCalculator / Ortho
+# ----------------------------------------------------------------------------
+
+def real_view(a):
+    """complex [nstate, ng] -> real [nstate, 2 ng] (re, im interleaved),
+    the DGEMM view of ``ckPairCalculator.C:866-871``."""
+    return a.view(np.float64).reshape(a.shape[0], -1)
+
+
+def kx0_scale(a, sysm, s):
+    out = a.copy()
+    out[:, :sysm.nkx0] *= s
+    return out
+
+
+def pc_forward(left, right, sysm, alpha):
+    """``PairCalculator::multiplyForward`` (``ckPairCalculator.C:821-893``):
+    DGEMM('T','N') over the real view; C[x][y] = alpha * <left_x | right_y>."""
+    return alpha * (real_view(left) @ real_view(right).T)
+
+
+def newton_schulz(S, tol=1e-15, max_iter=1000, lsda=False):
+    """``Ortho::start_calc``/``do_iteration``/``step_2``/``step_3``/
+    ``tolerance_check``/``collect_error`` (``orthog_ctrl/ortho.C:109-146,
+    233-262, 848-971``); same iteration as ``CPORTHOG::get_iter_Tmat``
+    (``cp_orthog/cp_lowdin.C:180-265``):
+    A = I, B = S/2; loop C = 3I - A B; B <- B C / 2; A <- C A / 2;
+    err = sqrt(sum((A_old - A)^2) / N^2) until err <= tol.
+    Returns (T, iterations, err)."""
+    n = S.shape[0]
+    B = S.copy() if lsda else S / 2.0
+    A = np.eye(n)
+    it = 0
+    err = 1.0
+    while True:
+        C = 3.0 * np.eye(n) - A @ B
+        Bn = 0.5 * (B @ C)
+        An = 0.5 * (C @ A)
+        err = math.sqrt(float(np.sum((A - An) ** 2)) / (n * n))
+        A, B = An, Bn
+        it += 1
+        if not (err > tol and it < max_iter):
+            break
+    return A, it, err
+
+
+def ortho_psi(psi_nonorth, sysm, tol=1e-15, max_iter=1000):
+    """Orthonormalisation step (``computeNewPsi``, ``gspace.ci:710-730``):
+    kx=0 rows scaled by 1/sqrt(2) (``CP_State_GSpacePlane::sendPsi``
+    2975-3070), S = 2 Psi^T Psi (symmetric PC, alpha = 2), T by
+    Newton-Schulz, Psi_new = Psi T (``bwMultiplyHelper``, 'N','N'), kx=0
+    rows rescaled by sqrt(2) (``doNewPsi`` 3232-3281).  Returns
+    (psi_orth, T, S, iters, err)."""
+    r2i = 1.0 / math.sqrt(2.0)
+    ps = kx0_scale(psi_nonorth, sysm, r2i)
+    S = pc_forward(ps, ps, sysm, 2.0)
+    T, it, err = newton_schulz(S, tol, max_iter)
+    new = T.T @ ps
+    new = kx0_scale(new, sysm, math.sqrt(2.0))
+    return new, T, S, it, err
+
+
+def lambda_step(psi, force, T, sysm):
+    """Constraint force in dynamics (``computeLambdaAndCg``, ``gspace.ci:667-690``):
+    kx=0: psi/sqrt2, F*sqrt2 (``sendLambda`` 1817-2007); Lambda[x][y] =
+    <psi_x|F_y> (asymmetric PC, alpha = 1); Gamma = T Lambda
+    (``ortho.C:565-570``); PC backward R = Psi Gamma^T - F T
+    (``bwMultiplyHelper`` 1842 + ``bwMultiplyDynOrthoT`` 1965-2031);
+    F = -R (``unpackLambda`` 2067-2072); kx=0 F/sqrt2 (``doLambda`` 2237-2242).
+    Returns (F_new, Lambda)."""
+    r2 = math.sqrt(2.0)
+    ps = kx0_scale(psi, sysm, 1.0 / r2)
+    fs = kx0_scale(force, sysm, r2)
+    lam = pc_forward(ps, fs, sysm, 1.0)
+    gam = T @ lam
+    # Column-major (state = column) R = Psi Gamma - F T; as state rows:
+    # R_j = sum_k Gamma[k][j] psi_k - sum_k T[k][j] F_k
+    r = gam.T @ ps - T.T @ fs
+    fnew = -r
+    fnew = kx0_scale(fnew, sysm, 1.0 / r2)
+    return fnew, lam
+
+
+# ----------------------------------------------------------------------------
+# integrator
+# ----------------------------------------------------------------------------
+
+def evolve_vel(force, vpsi, cmass, dt, sysm):
+    """``CPINTEGRATE::cp_evolve_vel`` without NHC (``cp_dynamics.C:97-210``):
+    on [nkx0_red, ng): g=0 imaginary parts zeroed, kx=0 unique points use
+    F*2 / m*2, v += F dt/2 / m."""
+    v = vpsi.copy()
+    f = force.copy()
+    r0 = sysm.nkx0_red
+    r1 = r0 + sysm.nkx0_zero
+    f[:, r0:r1] = f[:, r0:r1].real
+    v[:, r0:r1] = v[:, r0:r1].real
+    v[:, r0:] += f[:, r0:] * (0.5 * dt / cmass[None, r0:])
+    v[:, r0:r1] = v[:, r0:r1].real
+    return v
+
+
+def fict_ke(vpsi, cmass, sysm):
+    """``CPINTEGRATE::get_fictKE`` (``cp_dynamics.C:218-270``): sum m|v|^2 / 2
+    over kx>0 plus the unique kx=0 points with mass doubled, g=0 real part."""
+    r0 = sysm.nkx0_red
+    r1 = r0 + sysm.nkx0_zero
+    iend = sysm.nkx0_red + sysm.nkx0_uni
+    m = cmass.copy()
+    m[r1:iend] *= 2.0
+    e = np.sum(m[None, r0:] * np.abs(vpsi[:, r0:]) ** 2, axis=1)
+    return 0.5 * e
+
+
+def sync_redundant(a, sysm):
+    """Gamma redundancy sync (``gspace.ci:692-708``, ``CP_State_GSpacePlane.C:2829-2970``):
+    the redundant kx=0 half is the conjugate of the unique half."""
+    idx = redundant_partner(sysm)
+    out = a.copy()
+    out[:, :sysm.nkx0_red] = np.conj(a[:, idx])
+    return out
+
+
+def redundant_partner(sysm):
+    k0 = np.arange(sysm.nkx0)
+    key = {(int(sysm.ky[i]), int(sysm.kz[i])): i for i in k0}
+    return np.array([key[(-int(sysm.ky[i]), -int(sysm.kz[i]))] for i in range(sysm.nkx0_red)], dtype=np.int64)
+
+
+# ----------------------------------------------------------------------------
+# one CP dynamics step (gspace.ci:199-324), electrons only, ions fixed
+# ----------------------------------------------------------------------------
+
+class CPState:
+    """psi_t: non-orthogonal coefficients integrated by Verlet; psi: the
+    orthonormal set psi_t T; T: last Newton-Schulz result; v: velocities."""
+
+    def __init__(self, sysm):
+        self.psi_t = sysm.psi.copy()
+        self.psi = sysm.psi.copy()
+        self.T = np.eye(sysm.nstate)
+        self.v = np.zeros_like(sysm.psi)
+        self.iteration = 0
+
+
+def electronic_forces(psi, sysm, fnl=None, enl=0.0):
+    psir = state_g_to_r(psi, sysm)
+    rho, vks, en = vks_build(psir, sysm)
+    fks = vks_forces(psir, vks, sysm)
+    f = add_forces(fks, fnl, sysm)
+    f, ek = eke(psi, f, sysm)
+    en = dict(en)
+    en["EKE"] = float(ek.sum())
+    en["ENL"] = enl
+    return f, en
+
+
+def psiv_reset(st, sysm):
+    """PsiV tolerance reset (``Ortho::maxCheck``, ``ortho.C:455-475``; the
+    "replace non-ortho psi by ortho" copies of ``CP_State_GSpacePlane.C:3590-3600,
+    3750-3760``): psi_t <- psi, T <- I, and the velocities projected onto the
+    orthonormality constraint, v_j <- v_j - sum_k psi_k X_kj with
+    X = (A + A^T)/4, A = <psi_i|v_j> in the S metric (alpha = 2)."""
+    r2i = 1.0 / math.sqrt(2.0)
+    ps = kx0_scale(st.psi, sysm, r2i)
+    vs = kx0_scale(st.v, sysm, r2i)
+    A = pc_forward(ps, vs, sysm, 2.0)
+    X = 0.25 * (A + A.T)
+    st.v = st.v - X.T @ st.psi
+    st.psi_t = st.psi.copy()
+    st.T = np.eye(sysm.nstate)
+
+
+def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl=None):
+    """One CPAIMD electronic step.  Order: forces on the orthonormal psi
+    (computePsiFandVKS + NL, combineForcesGetEke), constraint force
+    (computeLambdaAndCg), integrate (integrateModForce ->
+    CPINTEGRATE::CP_integrate_dyn, cp_dynamics.C:29-88), orthonormalise
+    (computeNewPsi).  Returns the energy record of the psi the forces were
+    evaluated on."""
+    st.iteration += 1
+    fnl, enl = (None, 0.0) if nl is None else nl(st.psi, sysm)
+    f, en = electronic_forces(st.psi, sysm, fnl, enl)
+    f, lam = lambda_step(st.psi, f, st.T, sysm)
+    dt = sysm.dt
+    if st.iteration > 1:
+        st.v = evolve_vel(f, st.v, sysm.cmass, dt, sysm)
+    en["FICT_KE"] = float(fict_ke(st.v, sysm.cmass, sysm).sum())
+    st.v = evolve_vel(f, st.v, sysm.cmass, dt, sysm)
+    r0 = sysm.nkx0_red
+    st.psi_t[:, r0:] = st.psi_t[:, r0:] + st.v[:, r0:] * dt
+    st.psi_t = sync_redundant(st.psi_t, sysm)
+    st.v = sync_redundant(st.v, sysm)
+    st.psi, st.T, S, it, err = ortho_psi(st.psi_t, sysm, tol, max_iter)
+    en["ORTHO_ITERS"] = it
+    en["ORTHO_ERR"] = err
+    return en

@@ -1,0 +1,113 @@
+"""CPU checks of the oracle itself (no GPU): transforms, physics identities and
+energy conservation of the CP dynamics it restates."""
+import math
+
+import numpy as np
+import pytest
+
+from openatom_b200.system import gamma_overlap, make_system
+from oracle import cp_oracle as O
+
+
+@pytest.fixture(scope="module")
+def w2():
+    return make_system("w2", seed=3, dt=0.25)
+
+
+def test_layout(w2):
+    s = w2
+    assert np.all(s.kx[:s.nkx0] == 0)
+    assert s.nkx0 == s.nkx0_red + s.nkx0_uni and s.nkx0_zero == 1
+    assert int(np.sum(s.line_nneg + s.line_npos)) == s.ng
+    assert np.all(np.diff(s.line_off) == (s.line_nneg + s.line_npos)[:-1])
+
+
+def test_orthonormal_start(w2):
+    S = gamma_overlap(w2.psi, w2.kx)
+    assert np.max(np.abs(S - 2 * np.eye(w2.nstate))) < 1e-12
+
+
+def test_expand_pack_roundtrip(w2):
+    z = O.expand_gspace(w2.psi, w2)
+    assert np.array_equal(O.pack_gspace(z, w2), w2.psi)
+
+
+def test_psi_r_real_and_parseval(w2):
+    s = w2
+    full = O._full_grid(s.psi, s.kx, s.ky, s.kz, s.nfft)
+    pr = np.fft.fftn(full, axes=(-3, -2, -1))
+    assert np.max(np.abs(pr.imag)) < 1e-12 * np.max(np.abs(pr.real))
+    psir = O.state_g_to_r(s.psi, s)
+    # sum_r psi^2 = N * sum_full |c|^2 = 2 N
+    assert np.allclose((psir ** 2).sum(axis=(1, 2, 3)), 2.0 * s.npts, rtol=1e-12)
+
+
+def test_round_trip_r_to_g(w2):
+    s = w2
+    psir = O.state_g_to_r(s.psi, s)
+    back = O.state_r_to_g(psir, s) / s.npts
+    assert np.max(np.abs(back - s.psi)) < 1e-13
+
+
+def test_hartree_real_space(w2):
+    s = w2
+    rho = O.density(O.state_g_to_r(s.psi, s), s)
+    vr, eh, ee, ew = O.hart_eext(rho, s)
+    assert eh > 0 and ew > 0
+    # E_H + E_ext = integral of rho * (V_H + V_loc) minus E_H (V_H counted twice)
+    tot = float(np.sum(rho * vr)) * s.vol / s.npts
+    assert abs(tot - (2 * eh + ee)) < 1e-9 * max(1.0, abs(tot))
+
+
+def test_eke_direct(w2):
+    s = w2
+    f, e = O.eke(s.psi, np.zeros_like(s.psi), s)
+    g2 = s.g2()
+    w = np.where(s.kx == 0, 1.0, 2.0)
+    assert np.allclose(e, 0.5 * (w * g2 * np.abs(s.psi) ** 2).sum(1), rtol=1e-13)
+
+
+def test_newton_schulz_vs_eigen():
+    rng = np.random.default_rng(1)
+    n = 24
+    a = rng.standard_normal((n, n)) * 0.05
+    S = 2 * np.eye(n) + a + a.T
+    T, it, err = O.newton_schulz(S, tol=1e-15, max_iter=100)
+    w, v = np.linalg.eigh(S / 2)
+    Tex = (v / np.sqrt(w)) @ v.T
+    assert np.max(np.abs(T - Tex)) < 1e-13 and err <= 1e-15
+
+
+def test_newton_schulz_reports_non_convergence():
+    S = 2 * np.diag([3.5, 0.5, 1.0, 1.2])  # an eigenvalue of S/2 above 3: no convergence
+    T, it, err = O.newton_schulz(S, tol=1e-15, max_iter=7)
+    assert it == 7 and not (err <= 1e-15)
+
+
+def test_energy_conservation(w2):
+    """E_KS + fictitious KE is conserved to O(dt^2) by the restated dynamics."""
+    drifts = []
+    for dt in (0.25, 0.125):
+        s = make_system("w2", seed=3, dt=dt)
+        st = O.CPState(s)
+        tot = []
+        for _ in range(int(round(1.0 / dt))):
+            en = O.cp_step(st, s)
+            tot.append(en["EKE"] + en["EHART"] + en["EEXC"] + en["EEXT"] + en["FICT_KE"])
+        drifts.append(abs(tot[-1] - tot[0]))
+    assert drifts[0] < 1e-3
+    assert drifts[1] < drifts[0] / 2.5  # second order in dt
+
+
+def test_psiv_reset_restores_orthonormal_frame(w2):
+    s = make_system("w2", seed=3, dt=0.5)
+    st = O.CPState(s)
+    for _ in range(3):
+        O.cp_step(st, s)
+    O.psiv_reset(st, s)
+    S = gamma_overlap(st.psi_t, s.kx)
+    assert np.max(np.abs(S - 2 * np.eye(s.nstate))) < 1e-12
+    # velocities satisfy the linearised constraint <psi_i|v_j> + <v_i|psi_j> = 0
+    r2i = 1 / math.sqrt(2)
+    A = O.pc_forward(O.kx0_scale(st.psi, s, r2i), O.kx0_scale(st.v, s, r2i), s, 2.0)
+    assert np.max(np.abs(A + A.T)) < 1e-12
