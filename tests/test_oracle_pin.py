@@ -1,0 +1,129 @@
+"""Pin the numpy oracle against the reference's own PINY physics routines,
+compiled from the reference sources into oracle/_ref/libpiny_ref.so by
+oracle/build_ref.sh (CPU only).
+
+Pinned: CPNONLOCAL::CP_eke_calc (cp_eke.C), CPXCFNCTS::CP_exc_calc
+(cp_pz_lda.C), CPLOCAL::CP_hart_eext_calc (cp_hart_ext.C) and
+CPORTHOG::get_iter_Tmat (cp_lowdin.C).  The FFT and GEMM boundaries have no
+reference implementation here (FFTW2 / Fortran BLAS are absent) and are
+pinned by mathematics in test_oracle_cpu.py.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from openatom_b200.system import make_system
+from oracle import cp_oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "oracle", "_ref", "libpiny_ref.so")
+
+dp = C.POINTER(C.c_double)
+ip = C.POINTER(C.c_int)
+
+
+@pytest.fixture(scope="module")
+def ref():
+    if not os.path.exists(LIB) and os.path.isdir("/root/reference"):
+        subprocess.run(["bash", os.path.join(ROOT, "oracle", "build_ref.sh")], check=True,
+                       capture_output=True)
+    if not os.path.exists(LIB):
+        pytest.skip("oracle/_ref not built (reference sources absent)")
+    lib = C.CDLL(LIB)
+    lib.ref_eke.argtypes = [C.c_int, dp, dp, ip, ip, ip, dp, C.c_double, C.c_double, C.c_int, C.c_double, dp]
+    lib.ref_pz_lda.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp, C.c_double, dp, dp]
+    lib.ref_hart_eext.argtypes = [C.c_int, ip, ip, ip, dp, dp, C.c_int, dp, ip, dp, C.c_int, C.c_int, C.c_double,
+                                  C.c_double, dp, dp, C.c_double, C.c_double, C.c_double, dp, dp, dp, dp]
+    lib.ref_iter_tmat.argtypes = [dp, dp, C.c_int]
+    return lib
+
+
+def _d(a):
+    return a.ctypes.data_as(dp)
+
+
+def _i(a):
+    return a.ctypes.data_as(ip)
+
+
+@pytest.fixture(scope="module")
+def sysm():
+    return make_system("w4", seed=21)
+
+
+def test_eke_pinned(ref, sysm):
+    s = sysm
+    rng = np.random.default_rng(0)
+    f0 = (rng.standard_normal(s.psi.shape) + 1j * rng.standard_normal(s.psi.shape)) * 0.1
+    f_or, e_or = O.eke(s.psi, f0, s)
+    kx, ky, kz = (np.ascontiguousarray(a, dtype=np.int32) for a in (s.kx, s.ky, s.kz))
+    f = 2.0 * np.pi / s.box
+    g2 = np.ascontiguousarray((f * kx) ** 2 + (f * ky) ** 2 + (f * kz) ** 2, dtype=np.float64)
+    for st in range(s.nstate):
+        psi = np.ascontiguousarray(s.psi[st])
+        fr = np.ascontiguousarray(f0[st].copy())
+        e = C.c_double(0.0)
+        ref.ref_eke(s.ng, _d(psi.view(np.float64)), _d(fr.view(np.float64)), _i(kx), _i(ky), _i(kz), _d(g2),
+                    s.ecut_ry, float(s.occ[st]), s.nkx0, s.box, C.byref(e))
+        assert abs(e.value - e_or[st]) <= 1e-12 * abs(e_or[st])
+        assert np.max(np.abs(fr - f_or[st])) <= 1e-12 * np.max(np.abs(f_or[st]))
+
+
+def test_pz_lda_pinned(ref, sysm):
+    s = sysm
+    nx, ny, nz = s.nfft
+    rho = O.density(O.state_g_to_r(s.psi, s), s)
+    v_or, exc_or, muxc_or = O.pz_lda(rho, s.vol, s.npts)
+    xl = 2 * (nx // 2 + 1)
+    pad = np.zeros((nz, ny, xl))
+    pad[:, :, :nx] = rho
+    res = np.zeros_like(pad)
+    exc, muxc = C.c_double(), C.c_double()
+    ref.ref_pz_lda(nx, ny, nz, _d(pad), _d(res), s.box, C.byref(exc), C.byref(muxc))
+    assert abs(exc.value - exc_or) <= 1e-12 * abs(exc_or)
+    assert abs(muxc.value - muxc_or) <= 1e-12 * abs(muxc_or)
+    assert np.max(np.abs(res[:, :, :nx] - v_or)) <= 1e-13 * np.max(np.abs(v_or))
+
+
+def test_hart_eext_pinned(ref, sysm):
+    s = sysm
+    nx, ny, nz = s.nfft
+    rho_r = O.density(O.state_g_to_r(s.psi, s), s)
+    _, eh_or, ee_or, ew_or, f_or = O.hart_eext(rho_r, s, want_forces=True)
+    kx, ky, kz, g2 = O.rho_sphere(s)
+    # order points as z-lines (kz fastest) so the reference's incremental phases apply
+    order = np.lexsort((kz, ky, kx))
+    kx, ky, kz = kx[order], ky[order], kz[order]
+    rhog = np.fft.fftn(rho_r * (s.vol / s.npts))[kz % nz, ky % ny, kx % nx]
+    rhog = np.ascontiguousarray(rhog)
+    vks = np.zeros_like(rhog)
+    kx_, ky_, kz_ = (np.ascontiguousarray(a, dtype=np.int32) for a in (kx, ky, kz))
+    typ = np.ascontiguousarray(s.atm_type, dtype=np.int32)
+    pos = np.ascontiguousarray(s.pos)
+    q = np.ascontiguousarray(s.q)
+    spl = np.ascontiguousarray(s.vloc.coef)
+    gz = np.ascontiguousarray(s.gzvps)
+    fatm = np.zeros((s.natm, 3))
+    eh, ee, ew = C.c_double(), C.c_double(), C.c_double()
+    ref.ref_hart_eext(len(kx), _i(kx_), _i(ky_), _i(kz_), _d(rhog.view(np.float64)), _d(vks.view(np.float64)),
+                      s.natm, _d(pos), _i(typ), _d(q), len(s.type_names), s.vloc.n, s.vloc.gmin, s.vloc.dg,
+                      _d(spl), _d(gz), s.alp_ewd, s.ecut_ry, s.box, C.byref(eh), C.byref(ee), C.byref(ew),
+                      _d(fatm))
+    assert abs(eh.value - eh_or) <= 1e-11 * abs(eh_or)
+    assert abs(ee.value - ee_or) <= 1e-11 * abs(ee_or)
+    assert abs(ew.value - ew_or) <= 1e-11 * abs(ew_or)
+    assert np.max(np.abs(fatm - f_or)) <= 1e-10 * np.max(np.abs(f_or))
+
+
+def test_iter_tmat_pinned(ref):
+    rng = np.random.default_rng(2)
+    n = 16
+    a = rng.standard_normal((n, n)) * 0.02
+    S = np.ascontiguousarray(2 * np.eye(n) + a + a.T)
+    T = np.zeros_like(S)
+    ref.ref_iter_tmat(_d(S), _d(T), n)
+    T_or, it, err = O.newton_schulz(S, tol=1e-15, max_iter=10)
+    assert np.max(np.abs(T - T_or)) < 1e-14
