@@ -65,6 +65,12 @@ typedef struct {
   int nspl;                    /* local pseudopotential spline (CP_get_vpsnow) */
   double spl_gmin, spl_dg;
   const double *spl;           /* [ntype][nspl][4] */
+  /* nonlocal l = 0 KB channel (cppseudo->nonlocal); same spline grid */
+  int natm_nl;
+  const int *nl_atm;           /* [natm_nl] atom index of each nonlocal atom (map_nl) */
+  const double *nl_spl;        /* [ntype][nspl][4] projector spline */
+  const double *nl_vnorm;      /* [ntype] vnorm_0 */
+  const double *nl_gz0;        /* [ntype] projector at g = 0 (gzvps0) */
 } oa_system_desc;
 
 /* Create a context on the current CUDA device.  precision = OA_FP64 (plain
@@ -118,10 +124,12 @@ oa_status oa_gpu_pc_forward(oa_ctx *ctx, void *stream, const double *left, const
 
 /* Ortho S -> T = (S/2)^(-1/2) by Newton-Schulz (ortho.C:109-146, 153-266,
  * 848-971; same iteration as CPORTHOG::get_iter_Tmat, cp_lowdin.C:180-265).
- * S, T: device [n][n].  Synchronises the stream to return iterations and
- * residual; returns OA_ERR_NOT_CONVERGED when max_iter is reached. */
+ * S, T: device [n][n].  Synchronises the stream to return iterations,
+ * residual and smax = max |S - 2I| (Ortho::array_diag_max, ortho.h:282, the
+ * quantity Ortho::maxCheck compares with cp_norb_tol); returns
+ * OA_ERR_NOT_CONVERGED when max_iter is reached. */
 oa_status oa_gpu_ortho_invsqrt(oa_ctx *ctx, void *stream, const double *S, double *T, double tol,
-                               int max_iter, int *iters_out, double *err_out);
+                               int max_iter, int *iters_out, double *err_out, double *smax_out);
 
 /* PairCalculator backward (multiplyResult / bwMultiplyHelper /
  * bwMultiplyDynOrthoT, ckPairCalculator.C:1201-2031), state-row form:
@@ -135,6 +143,23 @@ oa_status oa_gpu_ortho_invsqrt(oa_ctx *ctx, void *stream, const double *S, doubl
 oa_status oa_gpu_pc_backward(oa_ctx *ctx, void *stream, const double *M1, const double *X1,
                              double a1_kx0, double a1_rest, const double *M2, const double *X2, double a2,
                              double *out);
+
+/* Mixed-precision PairCalculator forward on the tcgen05 tensor cores: same
+ * contract as oa_gpu_pc_forward, operands split into nterm bf16 terms
+ * (nterm = 2: 3 products, ~2^-16 relative; nterm = 3: 6 products, ~2^-24),
+ * FP32 accumulation per K block, FP64 reduction over K blocks. */
+oa_status oa_gpu_pc_forward_mixed(oa_ctx *ctx, void *stream, const double *left, const double *right,
+                                  double alpha, double w_kx0, int nterm, double *C);
+
+/* Mixed-precision PairCalculator backward on the tcgen05 tensor cores; same
+ * contract as oa_gpu_pc_backward, split as oa_gpu_pc_forward_mixed. */
+oa_status oa_gpu_pc_backward_mixed(oa_ctx *ctx, void *stream, const double *M1, const double *X1,
+                                   double a1_kx0, double a1_rest, const double *M2, const double *X2, double a2,
+                                   int nterm, double *out);
+
+/* Synchronise the stream and report whether any kernel's bounded wait ran
+ * out (OA_ERR_CUDA with a message) since the context was created. */
+oa_status oa_gpu_check(oa_ctx *ctx, void *stream);
 
 /* Small dense C = alpha A B (N x N), e.g. Gamma = T Lambda (ortho.C:565-570). */
 oa_status oa_gpu_small_gemm(oa_ctx *ctx, void *stream, const double *A, const double *B, double alpha,
@@ -173,9 +198,21 @@ oa_status oa_gpu_time_kernels(oa_ctx *ctx, void *stream, const double *psi, int 
 /* Sizes for byte/flop accounting (see oa_abi.cu): out[0..9]. */
 oa_status oa_gpu_sizes(const oa_ctx *ctx, long *out);
 
+/* Nonlocal energy and coefficient forces by the structure-factor method
+ * (StructureFactor::computeSF -> CPNONLOCAL::CP_calc_Struct_Fact,
+ * cp_struct_fact.C:37-255; CP_State_ParticlePlane::computeZ/reduceZ/getForces,
+ * CP_State_ParticlePlane.C:500-760 -> CP_enl_matrix_calc cp_nlmat.C:24-100,
+ * CP_enl_atm_forc_calc and CP_enl_force_calc cp_nl_energy_forc.C:29-235).
+ * psi: device [nstate][ng]; fnl_out: device [nstate][ng] (the
+ * ParticlePlane forces that addForces adds); enl_out: optional device
+ * [nstate].  nterm = 0 uses FP64 tensor-core GEMMs, 2 or 3 the split-BF16
+ * tcgen05 GEMMs.  The structure factor (FP64) is rebuilt from the current
+ * atom positions on every call. */
+oa_status oa_gpu_nl_sf(oa_ctx *ctx, void *stream, const double *psi, int nterm, double *fnl_out, double *enl_out);
+
 /* Energies of the last vks_build / vks_apply_fft_bwd (synchronises):
- * out[0..6] = EKE, EHART, EEXT, EWALD_RECIP, EEXC, MUXC, FICT_KE. */
-oa_status oa_gpu_energies(oa_ctx *ctx, void *stream, double *out7);
+ * out[0..7] = EKE, EHART, EEXT, EWALD_RECIP, EEXC, MUXC, FICT_KE, ENL. */
+oa_status oa_gpu_energies(oa_ctx *ctx, void *stream, double *out8);
 
 #ifdef __cplusplus
 }

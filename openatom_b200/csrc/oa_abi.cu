@@ -27,6 +27,24 @@ cudaError_t oa_launch_sync_redundant(cudaStream_t s, double2* P, double2* V, con
                                      int nstate);
 cudaError_t oa_launch_sum_partials(cudaStream_t s, const double* part, int n, int stride, int off, double scale,
                                    double* out);
+cudaError_t oa_launch_umma_fwd(cudaStream_t s, int nterm, const double* A, const double* B, int m, int n, long K,
+                               long kx0_cols, double w_kx0, double alpha, float* part, int max_kb, double* C,
+                               int* err_flag, int nsm);
+cudaError_t oa_launch_umma_bwd(cudaStream_t s, int nterm, const double* M1, const double* X1, double a1_kx0,
+                               double a1_rest, const double* M2, const double* X2, double a2, int nj, int nk,
+                               long ncol, long kx0_cols, double* out, int* err_flag);
+int oa_umma_max_kb(int m, int n, int nsm);
+cudaError_t oa_launch_pc_fwd_mn(cudaStream_t s, const double* A, const double* B, int m, int n, long K,
+                                long kx0_cols, double w_kx0, double alpha, double* part, int nkb, double* C);
+cudaError_t oa_launch_pc_bwd_jk(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
+                                const double* M2, const double* X2, double a2, int nj, int nk, long ncol,
+                                long kx0_cols, double* out);
+cudaError_t oa_launch_nl_sf(cudaStream_t s, const int* kx, const int* ky, const int* kz, int ng, const int* nl_atm,
+                            int natm_nl, const int* atm_type, const double2* phase, int ktab, const double* spl,
+                            int nspl, double gmin, double dg, const double* gz0, double tpi_l, double2* sf);
+cudaError_t oa_launch_nl_zscale(cudaStream_t s, const double* Z, int nstate, int natm_nl, const int* nl_atm,
+                                const int* atm_type, const double* vnorm, double rvol, const double* occ, double* zt,
+                                double* enl);
 
 static thread_local char g_err[512] = "";
 
@@ -60,6 +78,10 @@ struct oa_ctx_pc {
   double* mat_x;     // [n][n] scratch
   double* eye;       // [n][n] identity
   double* vtmp;      // [nstate][ng] complex scratch
+  float* upart;      // split-K FP32 partials of the tensor-core forward GEMM
+  int umax_kb;
+  int* err_flag;     // device: set by a kernel whose bounded wait ran out
+  int nsm;
 };
 
 static oa_ctx_pc* pcx(oa_ctx* c);
@@ -195,6 +217,17 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     TRY(upload(&c->atm_type, d->atm_type, d->natm));
     TRY(upload(&c->pos, d->pos, (size_t)3 * d->natm));
     TRY(upload(&p->partner, d->red_partner, d->nkx0_red));
+    TRY(upload(&c->ky, d->ky, d->ng));
+    TRY(upload(&c->kz, d->kz, d->ng));
+    c->natm_nl = d->natm_nl;
+    TRY(upload(&c->nl_atm, d->nl_atm, d->natm_nl));
+    TRY(upload(&c->nl_spl, d->nl_spl, d->natm_nl ? (size_t)d->ntype * d->nspl * 4 : 0));
+    TRY(upload(&c->nl_vnorm, d->nl_vnorm, d->natm_nl ? d->ntype : 0));
+    TRY(upload(&c->nl_gz0, d->nl_gz0, d->natm_nl ? d->ntype : 0));
+    TRY(cudaMalloc(&c->sf, ((size_t)d->natm_nl * d->ng + 1) * sizeof(double2)));
+    TRY(cudaMalloc(&c->zmat, ((size_t)d->natm_nl * d->nstate + 1) * sizeof(double)));
+    TRY(cudaMalloc(&c->zt, ((size_t)d->natm_nl * d->nstate + 1) * sizeof(double)));
+    TRY(cudaMalloc(&c->enl, (size_t)d->nstate * sizeof(double)));
     TRY(upload(&p->cmass, d->cmass, d->ng));
     c->tw_x = make_twiddles(d->nx);
     c->tw_y = make_twiddles(d->ny);
@@ -229,6 +262,17 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
       TRY(upload(&p->eye, eye.data(), eye.size()));
     }
     TRY(cudaMalloc(&p->vtmp, (size_t)d->nstate * d->ng * sizeof(double2)));
+    p->nsm = nsm;
+    p->umax_kb = oa_umma_max_kb(d->nstate, d->nstate, nsm);
+    {
+      const int mx = d->nstate > d->natm_nl ? d->nstate : d->natm_nl;
+      const int kbz = oa_umma_max_kb(d->nstate, d->natm_nl > 0 ? d->natm_nl : 1, nsm);
+      const size_t need = (size_t)(p->umax_kb > kbz ? p->umax_kb : kbz) * d->nstate * mx;
+      TRY(cudaMalloc(&p->upart, need * sizeof(float)));
+      p->umax_kb = p->umax_kb > kbz ? p->umax_kb : kbz;
+    }
+    TRY(cudaMalloc(&p->err_flag, sizeof(int)));
+    TRY(cudaMemset(p->err_flag, 0, sizeof(int)));
     TRY(cudaMallocHost(&p->h_status, 4 * sizeof(int)));
     TRY(cudaMallocHost(&p->h_vals, 16 * sizeof(double)));
     TRY(cudaDeviceSynchronize());
@@ -248,7 +292,9 @@ extern "C" oa_status oa_gpu_destroy(oa_ctx* c) {
   void* dev[] = {c->line_kx, c->line_ky, c->line_off, c->line_nneg, c->line_npos, c->kx, c->g2, c->tw_x, c->tw_y,
                  c->tw_z, c->spl, c->q_type, c->atm_type, c->pos, c->phase, c->occ, c->zbuf, c->rho_part, c->rho,
                  c->vks, c->vxc, c->dz, c->red, c->eke_part, p->part, p->ns_work, p->ns_status, p->ns_err,
-                 p->partner, p->cmass, p->ke_part, p->dev_e, p->mat_a, p->mat_x, p->eye, p->vtmp};
+                 p->partner, p->cmass, p->ke_part, p->dev_e, p->mat_a, p->mat_x, p->eye, p->vtmp, p->upart,
+                 p->err_flag, c->ky, c->kz, c->nl_atm, c->nl_spl, c->nl_vnorm, c->nl_gz0, c->sf, c->zmat, c->zt,
+                 c->enl};
   for (void* q : dev) if (q) cudaFree(q);
   if (p->h_status) cudaFreeHost(p->h_status);
   if (p->h_vals) cudaFreeHost(p->h_vals);
@@ -360,17 +406,18 @@ extern "C" oa_status oa_gpu_pc_forward(oa_ctx* c, void* stream, const double* le
 }
 
 extern "C" oa_status oa_gpu_ortho_invsqrt(oa_ctx* c, void* stream, const double* S, double* T, double tol,
-                                          int max_iter, int* iters_out, double* err_out) {
+                                          int max_iter, int* iters_out, double* err_out, double* smax_out) {
   OA_ARG_CHECK(c && S && T && max_iter > 0, "bad argument");
   cudaStream_t s = (cudaStream_t)stream;
   oa_ctx_pc* p = pcx(c);
   OA_CUDA_TRY(oa_launch_ortho_ns(s, S, c->nstate, 0.5, tol, max_iter, p->ns_work, T, p->ns_status, p->ns_err,
                                  p->ns_grid));
   OA_CUDA_TRY(cudaMemcpyAsync(p->h_status, p->ns_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-  OA_CUDA_TRY(cudaMemcpyAsync(p->h_vals, p->ns_err, sizeof(double), cudaMemcpyDeviceToHost, s));
+  OA_CUDA_TRY(cudaMemcpyAsync(p->h_vals, p->ns_err, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
   OA_CUDA_TRY(cudaStreamSynchronize(s));
   if (iters_out) *iters_out = p->h_status[0];
   if (err_out) *err_out = p->h_vals[0];
+  if (smax_out) *smax_out = p->h_vals[1];
   if (!isfinite(p->h_vals[0])) { oa_set_error("Newton-Schulz residual is not finite", __FILE__, __LINE__); return OA_ERR_NONFINITE; }
   if (!p->h_status[1]) { oa_set_error("Newton-Schulz reached max_iter", __FILE__, __LINE__); return OA_ERR_NOT_CONVERGED; }
   return OA_OK;
@@ -429,6 +476,7 @@ extern "C" oa_status oa_gpu_energies(oa_ctx* c, void* stream, double* out7) {
   out7[4] = p->h_vals[OA_E_EEXC];
   out7[5] = p->h_vals[OA_E_MUXC];
   out7[6] = p->h_vals[OA_E_FICT];
+  out7[7] = p->h_vals[OA_E_ENL];
   return OA_OK;
 }
 
@@ -512,5 +560,76 @@ extern "C" oa_status oa_gpu_sizes(const oa_ctx* c, long* out) {
   out[5] = c->ngroup; out[6] = c->npts; out[7] = c->precision == OA_FP64 ? 8 : 4; out[8] = c->nlines_d;
   // state_fft_fwd 3 + vks_build 10 + vks_apply 3 + lambda (2+1+1+1) + integrate 3 + S (2) + NS 1 + Psi T 1
   out[9] = 3 + 10 + 3 + 5 + 3 + 2 + 1 + 1;
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_pc_forward_mixed(oa_ctx* c, void* stream, const double* left, const double* right,
+                                             double alpha, double w_kx0, int nterm, double* C) {
+  OA_ARG_CHECK(c && left && right && C, "null argument");
+  OA_ARG_CHECK(nterm == 2 || nterm == 3, "nterm must be 2 or 3");
+  oa_ctx_pc* p = pcx(c);
+  OA_CUDA_TRY(oa_launch_umma_fwd((cudaStream_t)stream, nterm, left, right, c->nstate, c->nstate, 2L * c->ng,
+                                 2L * c->nkx0, w_kx0, alpha, p->upart, p->umax_kb, C, p->err_flag, p->nsm));
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_pc_backward_mixed(oa_ctx* c, void* stream, const double* M1, const double* X1,
+                                              double a1_kx0, double a1_rest, const double* M2, const double* X2,
+                                              double a2, int nterm, double* out) {
+  OA_ARG_CHECK(c && M1 && X1 && out, "null argument");
+  OA_ARG_CHECK((M2 == nullptr) == (X2 == nullptr), "M2 and X2 must both be given or both be NULL");
+  OA_ARG_CHECK(out != X1 && out != X2, "out must not alias an input");
+  OA_ARG_CHECK(nterm == 2 || nterm == 3, "nterm must be 2 or 3");
+  OA_CUDA_TRY(oa_launch_umma_bwd((cudaStream_t)stream, nterm, M1, X1, a1_kx0, a1_rest, M2, X2, a2, c->nstate,
+                                 c->nstate, 2L * c->ng, 2L * c->nkx0, out, pcx(c)->err_flag));
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_check(oa_ctx* c, void* stream) {
+  OA_ARG_CHECK(c, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  oa_ctx_pc* p = pcx(c);
+  OA_CUDA_TRY(cudaMemcpyAsync(p->h_status + 2, p->err_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  OA_CUDA_TRY(cudaStreamSynchronize(s));
+  if (p->h_status[2]) {
+    oa_set_error("a device wait reached its iteration limit", __FILE__, __LINE__);
+    return OA_ERR_CUDA;
+  }
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_nl_sf(oa_ctx* c, void* stream, const double* psi, int nterm, double* fnl_out,
+                                  double* enl_out) {
+  OA_ARG_CHECK(c && psi && fnl_out, "null argument");
+  OA_ARG_CHECK(nterm == 0 || nterm == 2 || nterm == 3, "nterm must be 0, 2 or 3");
+  cudaStream_t s = (cudaStream_t)stream;
+  oa_ctx_pc* p = pcx(c);
+  const int n = c->nstate, na = c->natm_nl;
+  if (na == 0) {
+    OA_CUDA_TRY(cudaMemsetAsync(fnl_out, 0, (size_t)n * c->ng * sizeof(double2), s));
+    OA_CUDA_TRY(cudaMemsetAsync(p->dev_e + OA_E_ENL, 0, sizeof(double), s));
+    if (enl_out) OA_CUDA_TRY(cudaMemsetAsync(enl_out, 0, (size_t)n * sizeof(double), s));
+    return OA_OK;
+  }
+  const double tpi_l = 2.0 * M_PI / c->box;
+  OA_CUDA_TRY(oa_launch_phase_tables(c, s));
+  OA_CUDA_TRY(oa_launch_nl_sf(s, c->kx, c->ky, c->kz, c->ng, c->nl_atm, na, c->atm_type, c->phase, c->kmax_tab,
+                              c->nl_spl, c->nspl, c->spl_gmin, c->spl_dg, c->nl_gz0, tpi_l, c->sf));
+  const long K = 2L * c->ng;
+  if (nterm == 0)
+    OA_CUDA_TRY(oa_launch_pc_fwd_mn(s, psi, (const double*)c->sf, n, na, K, 0, 1.0, 1.0, p->part, p->nkb, c->zmat));
+  else
+    OA_CUDA_TRY(oa_launch_umma_fwd(s, nterm, psi, (const double*)c->sf, n, na, K, 0, 1.0, 1.0, p->upart, p->umax_kb,
+                                   c->zmat, p->err_flag, p->nsm));
+  OA_CUDA_TRY(oa_launch_nl_zscale(s, c->zmat, n, na, c->nl_atm, c->atm_type, c->nl_vnorm, 1.0 / c->vol, c->occ,
+                                  c->zt, c->enl));
+  if (nterm == 0)
+    OA_CUDA_TRY(oa_launch_pc_bwd_jk(s, c->zt, (const double*)c->sf, 1.0, 1.0, nullptr, nullptr, 0.0, n, na, K, 0,
+                                    fnl_out));
+  else
+    OA_CUDA_TRY(oa_launch_umma_bwd(s, nterm, c->zt, (const double*)c->sf, 1.0, 1.0, nullptr, nullptr, 0.0, n, na, K,
+                                   0, fnl_out, p->err_flag));
+  OA_CUDA_TRY(oa_launch_sum_partials(s, c->enl, n, 1, 0, 1.0, p->dev_e + OA_E_ENL));
+  if (enl_out) OA_CUDA_TRY(cudaMemcpyAsync(enl_out, c->enl, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   return OA_OK;
 }

@@ -37,6 +37,12 @@ struct oa_ctx {
   double *pos;            // [natm][3]
   double2 *phase;         // [natm][3][2*kmax_tab+1] exp(i 2 pi k x / L)
   double *occ;            // [nstate]
+  int *ky, *kz;           // per g-point
+  int natm_nl;
+  int *nl_atm;            // [natm_nl]
+  double *nl_spl, *nl_vnorm, *nl_gz0;
+  double2 *sf;            // [natm_nl][ng] structure factor x projector
+  double *zmat, *zt, *enl;
   // scratch (FFT path precision R; byte sizes)
   void *zbuf;             // [nstate][nz][ldl] C
   size_t zbuf_bytes;
@@ -55,6 +61,7 @@ struct oa_ctx {
 };
 
 enum { OA_E_EKE = 0, OA_E_EHART, OA_E_EEXT, OA_E_EWALD, OA_E_EEXC, OA_E_MUXC, OA_E_ENL, OA_E_FICT };
+cudaError_t oa_launch_phase_tables(oa_ctx* c, cudaStream_t s);
 
 #define OA_CUDA_TRY(x)                                  \
   do {                                                  \

@@ -34,7 +34,7 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 #define PC_LDS (PC_KS + 4)
 
 __global__ void __launch_bounds__(128)
-k_pc_fwd_f64(const double* __restrict__ A, const double* __restrict__ B, int n, long K, long kchunk,
+k_pc_fwd_f64(const double* __restrict__ A, const double* __restrict__ B, int m, int n, long K, long kchunk,
              long kx0_cols, double w_kx0, double* __restrict__ part) {
   __shared__ double As[PC_TM * PC_LDS];
   __shared__ double Bs[PC_TM * PC_LDS];
@@ -57,7 +57,7 @@ k_pc_fwd_f64(const double* __restrict__ A, const double* __restrict__ B, int n, 
       double va = 0.0, vb = 0.0;
       if (k < kend) {
         const double w = (k < kx0_cols) ? w_kx0 : 1.0;
-        if (i0 + r < n) va = A[(size_t)(i0 + r) * K + k] * w;
+        if (i0 + r < m) va = A[(size_t)(i0 + r) * K + k] * w;
         if (j0 + r < n) vb = B[(size_t)(j0 + r) * K + k];
       }
       As[r * PC_LDS + kk] = va;
@@ -68,29 +68,29 @@ k_pc_fwd_f64(const double* __restrict__ A, const double* __restrict__ B, int n, 
     for (int k4 = 0; k4 < PC_KS; k4 += 4) {
       double af[4], bf[4];
 #pragma unroll
-      for (int m = 0; m < 4; ++m) af[m] = As[(wi + m * 8 + (lane >> 2)) * PC_LDS + k4 + (lane & 3)];
+      for (int q = 0; q < 4; ++q) af[q] = As[(wi + q * 8 + (lane >> 2)) * PC_LDS + k4 + (lane & 3)];
 #pragma unroll
-      for (int m = 0; m < 4; ++m) bf[m] = Bs[(wj + m * 8 + (lane >> 2)) * PC_LDS + k4 + (lane & 3)];
+      for (int q = 0; q < 4; ++q) bf[q] = Bs[(wj + q * 8 + (lane >> 2)) * PC_LDS + k4 + (lane & 3)];
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) dmma_8x8x4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
     }
   }
-  double* out = part + (size_t)kb * n * n;
+  double* out = part + (size_t)kb * m * n;
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
       const int i = i0 + wi + a * 8 + (lane >> 2);
       const int j = j0 + wj + b * 8 + 2 * (lane & 3);
-      if (i < n && j < n) out[(size_t)i * n + j] = acc[a][b][0];
-      if (i < n && j + 1 < n) out[(size_t)i * n + j + 1] = acc[a][b][1];
+      if (i < m && j < n) out[(size_t)i * n + j] = acc[a][b][0];
+      if (i < m && j + 1 < n) out[(size_t)i * n + j + 1] = acc[a][b][1];
     }
 }
 
-__global__ void k_pc_fwd_reduce(const double* __restrict__ part, int nkb, int n, double alpha, double* __restrict__ C) {
-  const size_t nn = (size_t)n * n;
+__global__ void k_pc_fwd_reduce(const double* __restrict__ part, int nkb, size_t nn, double alpha,
+                                double* __restrict__ C) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (size_t)gridDim.x * blockDim.x) {
     double s = 0.0;
     for (int k = 0; k < nkb; ++k) s += part[(size_t)k * nn + i];
@@ -106,7 +106,7 @@ __global__ void k_pc_fwd_reduce(const double* __restrict__ part, int nkb, int n,
 __global__ void __launch_bounds__(128)
 k_pc_bwd_f64(const double* __restrict__ M1, const double* __restrict__ X1, double a1_kx0, double a1_rest,
              const double* __restrict__ M2, const double* __restrict__ X2, double a2,
-             int n, long ncol, long kx0_cols, double* __restrict__ out) {
+             int nj, int nk, long ncol, long kx0_cols, double* __restrict__ out) {
   __shared__ double Ms[PC_KS * (PC_TM + 4)];   // [k][j]
   __shared__ double Xs[PC_KS * (PC_TM + 4)];   // [k][c]
   const int LDT = PC_TM + 4;
@@ -123,14 +123,14 @@ k_pc_bwd_f64(const double* __restrict__ M1, const double* __restrict__ X1, doubl
   for (int term = 0; term < (M2 ? 2 : 1); ++term) {
     const double* M = term ? M2 : M1;
     const double* X = term ? X2 : X1;
-    for (int k0 = 0; k0 < n; k0 += PC_KS) {
+    for (int k0 = 0; k0 < nk; k0 += PC_KS) {
       __syncthreads();
       for (int idx = threadIdx.x; idx < PC_KS * PC_TM; idx += blockDim.x) {
         const int kk = idx / PC_TM, r = idx - kk * PC_TM;
         const int k = k0 + kk;
         double vm = 0.0, vx = 0.0;
-        if (k < n) {
-          if (j0 + r < n) vm = M[(size_t)k * n + j0 + r];
+        if (k < nk) {
+          if (j0 + r < nj) vm = M[(size_t)k * nj + j0 + r];
           if (c0 + r < ncol) vx = X[(size_t)k * ncol + c0 + r];
         }
         Ms[kk * LDT + r] = vm;
@@ -166,7 +166,7 @@ k_pc_bwd_f64(const double* __restrict__ M1, const double* __restrict__ X1, doubl
     for (int b = 0; b < 4; ++b) {
       const int j = j0 + wj + a * 8 + (lane >> 2);
       const long c = c0 + wc + b * 8 + 2 * (lane & 3);
-      if (j >= n) continue;
+      if (j >= nj) continue;
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const long cc = c + e;
@@ -248,11 +248,30 @@ k_ortho_ns(const double* __restrict__ S, int n, double bscale, double tol, int m
   const int nt = (n + NS_TS - 1) / NS_TS;
   const int ntiles = nt * nt;
   const size_t nn = (size_t)n * n;
-  // init: A = I, B = S * bscale
+  // init: A = I, B = S * bscale; max |S - I/bscale| (Ortho::array_diag_max,
+  // ortho.h:282-310) for the PsiV tolerance check
+  double dmax = 0.0;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (size_t)gridDim.x * blockDim.x) {
     const int r = (int)(i / n), c = (int)(i - (size_t)r * n);
     A0[i] = (r == c) ? 1.0 : 0.0;
     B0[i] = S[i] * bscale;
+    const double dv = fabs(S[i] - ((r == c) ? 1.0 / bscale : 0.0));
+    dmax = dv > dmax ? dv : dmax;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+  if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = dmax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, sred[w]);
+    errpart[blockIdx.x] = m;
+  }
+  grid.sync();
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double m = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) m = fmax(m, errpart[b]);
+    errv[1] = m;
   }
   grid.sync();
   double* A = A0; double* An = A1; double* B = B0; double* Bn = B1;
@@ -376,24 +395,36 @@ __global__ void k_sum_partials(const double* __restrict__ part, int n, int strid
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-cudaError_t oa_launch_pc_fwd(cudaStream_t s, const double* A, const double* B, int n, long K, long kx0_cols,
-                             double w_kx0, double alpha, double* part, int nkb, double* C) {
+cudaError_t oa_launch_pc_fwd_mn(cudaStream_t s, const double* A, const double* B, int m, int n, long K,
+                                long kx0_cols, double w_kx0, double alpha, double* part, int nkb, double* C) {
   const long kchunk = ((K + nkb - 1) / nkb + PC_KS - 1) / PC_KS * PC_KS;
   const int nkb_eff = (int)((K + kchunk - 1) / kchunk);
-  dim3 grid((n + PC_TM - 1) / PC_TM, (n + PC_TM - 1) / PC_TM, nkb_eff);
-  k_pc_fwd_f64<<<grid, 128, 0, s>>>(A, B, n, K, kchunk, kx0_cols, w_kx0, part);
+  dim3 grid((m + PC_TM - 1) / PC_TM, (n + PC_TM - 1) / PC_TM, nkb_eff);
+  k_pc_fwd_f64<<<grid, 128, 0, s>>>(A, B, m, n, K, kchunk, kx0_cols, w_kx0, part);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_pc_fwd_reduce<<<(n * n + 255) / 256, 256, 0, s>>>(part, nkb_eff, n, alpha, C);
+  const size_t mn = (size_t)m * n;
+  k_pc_fwd_reduce<<<(unsigned)((mn + 255) / 256), 256, 0, s>>>(part, nkb_eff, mn, alpha, C);
+  return cudaGetLastError();
+}
+
+cudaError_t oa_launch_pc_fwd(cudaStream_t s, const double* A, const double* B, int n, long K, long kx0_cols,
+                             double w_kx0, double alpha, double* part, int nkb, double* C) {
+  return oa_launch_pc_fwd_mn(s, A, B, n, n, K, kx0_cols, w_kx0, alpha, part, nkb, C);
+}
+
+cudaError_t oa_launch_pc_bwd_jk(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
+                                const double* M2, const double* X2, double a2, int nj, int nk, long ncol,
+                                long kx0_cols, double* out) {
+  dim3 grid((unsigned)((ncol + PC_TM - 1) / PC_TM), (nj + PC_TM - 1) / PC_TM);
+  k_pc_bwd_f64<<<grid, 128, 0, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out);
   return cudaGetLastError();
 }
 
 cudaError_t oa_launch_pc_bwd(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
                              const double* M2, const double* X2, double a2, int n, long ncol, long kx0_cols,
                              double* out) {
-  dim3 grid((unsigned)((ncol + PC_TM - 1) / PC_TM), (n + PC_TM - 1) / PC_TM);
-  k_pc_bwd_f64<<<grid, 128, 0, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, n, ncol, kx0_cols, out);
-  return cudaGetLastError();
+  return oa_launch_pc_bwd_jk(s, M1, X1, a1_kx0, a1_rest, M2, X2, a2, n, n, ncol, kx0_cols, out);
 }
 
 cudaError_t oa_launch_small_gemm(cudaStream_t s, const double* A, const double* B, int n, double alpha, double* C) {

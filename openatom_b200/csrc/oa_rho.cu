@@ -342,15 +342,18 @@ cudaError_t oa_launch_rho_xc(oa_ctx* c, cudaStream_t s) {
 int oa_rho_xc_nblk() { return 4 * 148; }
 int oa_rho_z_nblk(const oa_ctx* c) { return (c->nlines_d + OA_LB - 1) / OA_LB; }
 
+cudaError_t oa_launch_phase_tables(oa_ctx* c, cudaStream_t s) {
+  const double tpi_l = 2.0 * 3.14159265358979323846 / c->box;
+  const int total = c->natm * 3 * (2 * c->kmax_tab + 1);
+  k_phase_tables<<<(total + 255) / 256, 256, 0, s>>>(c->pos, c->natm, c->kmax_tab, tpi_l, c->phase);
+  return cudaGetLastError();
+}
+
 cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
   const double tpi_l = 2.0 * 3.14159265358979323846 / c->box;
   cudaError_t e;
   // phase tables exp(i 2 pi k x / L)
-  {
-    const int total = c->natm * 3 * (2 * c->kmax_tab + 1);
-    k_phase_tables<<<(total + 255) / 256, 256, 0, s>>>(c->pos, c->natm, c->kmax_tab, tpi_l, c->phase);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  }
+  if ((e = oa_launch_phase_tables(c, s)) != cudaSuccess) return e;
   RhoPlaneSmem L = rho_plane_layout(c->nx, c->ny, c->nkx_d, c->npair_d, c->ychunk_d);
   e = cudaFuncSetAttribute(k_rho_plane_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
   if (e != cudaSuccess) return e;

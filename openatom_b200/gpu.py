@@ -42,6 +42,7 @@ class SystemDesc(C.Structure):
         ("pos", _dp), ("atm_type", _ip), ("q_type", _dp), ("gzvps", _dp),
         ("alp_ewd", C.c_double),
         ("nspl", C.c_int), ("spl_gmin", C.c_double), ("spl_dg", C.c_double), ("spl", _dp),
+        ("natm_nl", C.c_int), ("nl_atm", _ip), ("nl_spl", _dp), ("nl_vnorm", _dp), ("nl_gz0", _dp),
     ]
 
 
@@ -57,7 +58,7 @@ SIGNATURES = {
     "oa_gpu_set_vks": (C.c_int, [_vp, _vp, _vp]),
     "oa_gpu_vks_apply_fft_bwd": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp, _vp]),
     "oa_gpu_pc_forward": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_double, _vp]),
-    "oa_gpu_ortho_invsqrt": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_int, _ip, _dp]),
+    "oa_gpu_ortho_invsqrt": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_int, _ip, _dp, _dp]),
     "oa_gpu_pc_backward": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_double, _vp, _vp, C.c_double, _vp]),
     "oa_gpu_small_gemm": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, _vp]),
     "oa_gpu_integrate": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_double, C.c_int, _vp]),
@@ -66,6 +67,11 @@ SIGNATURES = {
     "oa_gpu_set_atoms": (C.c_int, [_vp, _vp, _dp]),
     "oa_gpu_time_kernels": (C.c_int, [_vp, _vp, _vp, C.c_int, _dp]),
     "oa_gpu_sizes": (C.c_int, [_vp, C.POINTER(C.c_long)]),
+    "oa_gpu_pc_forward_mixed": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_double, C.c_int, _vp]),
+    "oa_gpu_pc_backward_mixed": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_double, _vp, _vp, C.c_double,
+                                           C.c_int, _vp]),
+    "oa_gpu_check": (C.c_int, [_vp, _vp]),
+    "oa_gpu_nl_sf": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp]),
 }
 
 KERNEL_NAMES = ("state_zfwd", "state_plane_density", "rho_xc", "vks_build", "state_plane_vks",
@@ -142,6 +148,15 @@ class CPContext:
             if m.any():
                 qt[t] = sysm.q[m][0]
         keep["q_type"] = _darr(qt)
+        nl = sysm.nl_atoms()
+        keep["nl_atm"] = _iarr(nl)
+        ntyp = len(sysm.type_names)
+        keep["nl_spl"] = _darr(sysm.nl_proj.coef if sysm.nl_proj is not None else np.zeros((ntyp, sysm.vloc.n, 4)))
+        keep["nl_vnorm"] = _darr(sysm.nl_vnorm if sysm.nl_vnorm is not None else np.zeros(ntyp))
+        keep["nl_gz0"] = _darr(sysm.nl_gz0 if sysm.nl_gz0 is not None else np.zeros(ntyp))
+        if sysm.nl_proj is not None and (sysm.nl_proj.n != sysm.vloc.n or sysm.nl_proj.dg != sysm.vloc.dg
+                                         or sysm.nl_proj.gmin != sysm.vloc.gmin):
+            raise ValueError("nonlocal and local spline tables must share one g grid")
 
         def ip(a):
             return a.ctypes.data_as(_ip)
@@ -163,6 +178,8 @@ class CPContext:
         d.pos, d.atm_type, d.q_type, d.gzvps = dp(keep["pos"]), ip(keep["atm_type"]), dp(keep["q_type"]), dp(keep["gzvps"])
         d.alp_ewd = sysm.alp_ewd
         d.nspl, d.spl_gmin, d.spl_dg, d.spl = sysm.vloc.n, sysm.vloc.gmin, sysm.vloc.dg, dp(keep["spl"])
+        d.natm_nl, d.nl_atm = len(nl), ip(keep["nl_atm"])
+        d.nl_spl, d.nl_vnorm, d.nl_gz0 = dp(keep["nl_spl"]), dp(keep["nl_vnorm"]), dp(keep["nl_gz0"])
         h = C.c_void_p()
         _check(lib.oa_gpu_init(C.byref(d), self.precision, C.byref(h)))
         self._h = h
@@ -205,18 +222,33 @@ class CPContext:
         _check(self._lib.oa_gpu_pc_forward(self._h, self._stream(), _ptr(left), _ptr(right),
                                            float(alpha), float(w_kx0), _ptr(out)))
 
-    def ortho_invsqrt(self, S, T, tol=1e-15, max_iter=1000):
+    def ortho_invsqrt(self, S, T, tol=1e-15, max_iter=1000, with_smax=False):
         it = C.c_int(0)
         err = C.c_double(0.0)
+        smax = C.c_double(0.0)
         st = self._lib.oa_gpu_ortho_invsqrt(self._h, self._stream(), _ptr(S), _ptr(T), float(tol), int(max_iter),
-                                            C.byref(it), C.byref(err))
+                                            C.byref(it), C.byref(err), C.byref(smax))
         if st not in (OA_OK, OA_ERR_NOT_CONVERGED):
             _check(st)
+        if with_smax:
+            return it.value, err.value, st == OA_OK, smax.value
         return it.value, err.value, st == OA_OK
 
     def pc_backward(self, M1, X1, a1_kx0, a1_rest, out, M2=None, X2=None, a2=0.0):
         _check(self._lib.oa_gpu_pc_backward(self._h, self._stream(), _ptr(M1), _ptr(X1), float(a1_kx0),
                                             float(a1_rest), _ptr(M2), _ptr(X2), float(a2), _ptr(out)))
+
+    def pc_forward_mixed(self, left, right, alpha, w_kx0, out, nterm=3):
+        _check(self._lib.oa_gpu_pc_forward_mixed(self._h, self._stream(), _ptr(left), _ptr(right), float(alpha),
+                                                 float(w_kx0), int(nterm), _ptr(out)))
+
+    def pc_backward_mixed(self, M1, X1, a1_kx0, a1_rest, out, M2=None, X2=None, a2=0.0, nterm=3):
+        _check(self._lib.oa_gpu_pc_backward_mixed(self._h, self._stream(), _ptr(M1), _ptr(X1), float(a1_kx0),
+                                                  float(a1_rest), _ptr(M2), _ptr(X2), float(a2), int(nterm),
+                                                  _ptr(out)))
+
+    def check(self):
+        _check(self._lib.oa_gpu_check(self._h, self._stream()))
 
     def small_gemm(self, A, B, alpha, out):
         _check(self._lib.oa_gpu_small_gemm(self._h, self._stream(), _ptr(A), _ptr(B), float(alpha), _ptr(out)))
@@ -263,10 +295,14 @@ class CPContext:
             "ortho_ns": 2 * n * n * 8,
         }
 
+    def nl_sf(self, psi, fnl_out, nterm=0, enl_out=None):
+        _check(self._lib.oa_gpu_nl_sf(self._h, self._stream(), _ptr(psi), int(nterm), _ptr(fnl_out),
+                                      _ptr(enl_out)))
+
     def energies(self) -> dict:
-        out = (C.c_double * 7)()
+        out = (C.c_double * 8)()
         _check(self._lib.oa_gpu_energies(self._h, self._stream(), out))
-        keys = ("EKE", "EHART", "EEXT", "EWALD_RECIP", "EEXC", "MUXC", "FICT_KE")
+        keys = ("EKE", "EHART", "EEXT", "EWALD_RECIP", "EEXC", "MUXC", "FICT_KE", "ENL")
         return {k: float(v) for k, v in zip(keys, out)}
 
 
@@ -274,7 +310,7 @@ class CPDriver:
     """Host runner of the CP dynamics step on one GPU (electrons; ions fixed)."""
 
     def __init__(self, sysm, precision: str = "fp64", tol: float = 1e-15, max_iter: int = 1000,
-                 psi0=None):
+                 psi0=None, norb_tol: float = 0.003):
         import torch
         self.torch = torch
         self.sys = sysm
@@ -287,20 +323,30 @@ class CPDriver:
         self.v = torch.zeros_like(self.psi)
         self.F = torch.zeros_like(self.psi)
         self.F2 = torch.zeros_like(self.psi)
+        self.Fnl = torch.zeros_like(self.psi)
+        # mixed form: split-BF16 tcgen05 GEMMs for Lambda, the constraint
+        # force and the nonlocal Z / force products; FP64 for S and Psi T
+        self.mixed = precision != "fp64"
+        self.nterm_nl = 3 if self.mixed else 0
         self.T = torch.eye(n, dtype=torch.float64, device=dev)
         self.S = torch.zeros(n, n, dtype=torch.float64, device=dev)
         self.lam = torch.zeros_like(self.S)
         self.gam = torch.zeros_like(self.S)
         self.tol, self.max_iter = tol, max_iter
+        # PsiV tolerance (cp_norb_tol, default 0.003; Ortho::maxCheck every step)
+        self.norb_tol = norb_tol
+        self.n_psiv = 0
         self.iteration = 0
         self.last_ortho = (0, 0.0, True)
 
     def forces(self):
-        """computePsiFandVKS + combineForcesGetEke on the orthonormal psi."""
+        """computePsiFandVKS + nonlocal forces + combineForcesGetEke on the
+        orthonormal psi."""
         c = self.ctx
         c.state_fft_fwd(self.psi)
         c.vks_build()
-        c.vks_apply_fft_bwd(self.psi, self.F)
+        c.nl_sf(self.psi, self.Fnl, nterm=self.nterm_nl)
+        c.vks_apply_fft_bwd(self.psi, self.F, fnl=self.Fnl)
 
     def launches_per_step(self) -> int:
         return self.ctx.sizes()["launches_per_step"]
@@ -328,9 +374,14 @@ class CPDriver:
         self.forces()
         en = c.energies()
         # Lambda = <psi_x | F_y>, Gamma = T Lambda, F' = F T - Psi Gamma (kx0 psi term halved)
-        c.pc_forward(self.psi, self.F, 1.0, 1.0, self.lam)
-        c.small_gemm(self.T, self.lam, 1.0, self.gam)
-        c.pc_backward(self.gam, self.psi, -0.5, -1.0, self.F2, M2=self.T, X2=self.F, a2=1.0)
+        if self.mixed:
+            c.pc_forward_mixed(self.psi, self.F, 1.0, 1.0, self.lam)
+            c.small_gemm(self.T, self.lam, 1.0, self.gam)
+            c.pc_backward_mixed(self.gam, self.psi, -0.5, -1.0, self.F2, M2=self.T, X2=self.F, a2=1.0)
+        else:
+            c.pc_forward(self.psi, self.F, 1.0, 1.0, self.lam)
+            c.small_gemm(self.T, self.lam, 1.0, self.gam)
+            c.pc_backward(self.gam, self.psi, -0.5, -1.0, self.F2, M2=self.T, X2=self.F, a2=1.0)
         # integrate psi_t
         c.integrate(self.F2, self.v, self.psi_t, dt, self.iteration > 1)
         en["FICT_KE"] = c.energies()["FICT_KE"]
@@ -338,9 +389,16 @@ class CPDriver:
             self.v.zero_()
         # orthonormalise: S = 2 sum w psi psi (kx0 weight 1/2), T = (S/2)^-1/2, psi = psi_t T
         c.pc_forward(self.psi_t, self.psi_t, 2.0, 0.5, self.S)
-        it, err, ok = c.ortho_invsqrt(self.S, self.T, self.tol, self.max_iter)
+        it, err, ok, smax = c.ortho_invsqrt(self.S, self.T, self.tol, self.max_iter, with_smax=True)
         self.last_ortho = (it, err, ok)
+        if not ok:
+            raise RuntimeError(f"Newton-Schulz did not converge: {it} iterations, residual {err:g}")
         c.pc_backward(self.T, self.psi_t, 1.0, 1.0, self.psi)
+        if smax > self.norb_tol and not damp_velocity:
+            # Ortho::maxCheck -> PsiV: restart the non-orthogonal set from psi
+            self.psiv_reset()
+            self.n_psiv += 1
         en["ORTHO_ITERS"] = it
         en["ORTHO_ERR"] = err
+        en["SMAX"] = smax
         return en

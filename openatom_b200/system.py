@@ -91,6 +91,11 @@ class CPSystem:
     psi: np.ndarray                 # [nstate, ng] complex128, S = 2 I
     dt: float = 5.0
     cmass0: float = 400.0
+    # nonlocal (Kleinman-Bylander, l = 0) projector per type; vnorm = 0 for
+    # types without a nonlocal channel (H in the shipped tables: local only)
+    nl_proj: SplineTable | None = None
+    nl_vnorm: np.ndarray | None = None
+    nl_gz0: np.ndarray | None = None
 
     @property
     def vol(self) -> float:
@@ -124,6 +129,14 @@ class CPSystem:
 
     def kx_weight(self) -> np.ndarray:
         return np.where(self.kx == 0, 1.0, 2.0)
+
+    def nl_atoms(self) -> np.ndarray:
+        """Atoms with a nonlocal channel, grouped by type in type order (the
+        order of cppseudo->nonlocal.map_nl)."""
+        if self.nl_vnorm is None:
+            return np.zeros(0, dtype=np.int64)
+        out = [np.nonzero(self.atm_type == t)[0] for t in range(len(self.type_names)) if self.nl_vnorm[t] != 0.0]
+        return np.concatenate(out) if out else np.zeros(0, dtype=np.int64)
 
 
 # ----------------------------------------------------------------------------
@@ -255,6 +268,19 @@ def _cubic_coeffs(x: np.ndarray, y: np.ndarray) -> np.ndarray:
     return out
 
 
+def gaussian_nl_table(amp, rnl, gmax: float, nspl: int = 4000):
+    """l = 0 KB projector p(g) = amp exp(-g^2 rnl^2 / 2) per type on the same
+    kind of grid as the local table; p(0) = amp is the gzvps0 term
+    (cp_struct_fact.C:get_rad_proj)."""
+    gmin = gmax / nspl
+    g = gmin + np.arange(nspl) * ((gmax - gmin) / (nspl - 1))
+    dg = g[1] - g[0]
+    coef = np.zeros((len(amp), nspl, 4))
+    for t, (a, r) in enumerate(zip(amp, rnl)):
+        coef[t] = _cubic_coeffs(g, a * np.exp(-0.5 * (g * r) ** 2))
+    return SplineTable(gmin=float(gmin), dg=float(dg), coef=coef), np.array(amp, dtype=np.float64)
+
+
 def gaussian_vloc_table(zval, rloc, gmax: float, nspl: int = 4000):
     """Local pseudopotential v(g) = -4 pi Z exp(-g^2 rloc^2 / 2) / g^2 per type
     (a Goedecker-style Gaussian-smeared ion core), tabulated on a uniform grid
@@ -356,6 +382,9 @@ def make_system(preset: str = "w8", seed: int = 1234, nstate: int | None = None,
     g2 = f * f * (kx.astype(np.float64) ** 2 + ky ** 2 + kz ** 2)
     gmax = math.sqrt(4.0 * ecut_ry) * 1.05 + 0.5
     vloc, gz = gaussian_vloc_table([6.0, 1.0], [0.247, 0.2], gmax)
+    # O: one s-channel KB projector; H: local only (data/DATABASE/pi_md.vps)
+    nl_proj, nl_gz0 = gaussian_nl_table([12.0, 0.0], [0.35, 0.35], gmax)
+    nl_vnorm = np.array([0.9, 0.0])
     psi = random_coefficients(nstate, kx, ky, kz, g2, rng)
     cmass = create_mass(kx, g2, cmass0, ecut_mass)
     # Ewald splitting parameter: alpha = 3.5 / (L/2) style default (screening
@@ -366,4 +395,5 @@ def make_system(preset: str = "w8", seed: int = 1234, nstate: int | None = None,
                     gzvps=gz, vloc=vloc, alp_ewd=alp_ewd, kx=kx, ky=ky, kz=kz,
                     line_kx=lkx, line_ky=lky, line_off=loff, line_nneg=lneg, line_npos=lpos,
                     nkx0=nkx0, nkx0_red=nred, nkx0_uni=nuni, nkx0_zero=nzero,
-                    occ=np.ones(nstate), cmass=cmass, psi=psi, dt=dt, cmass0=cmass0)
+                    occ=np.ones(nstate), cmass=cmass, psi=psi, dt=dt, cmass0=cmass0,
+                    nl_proj=nl_proj, nl_vnorm=nl_vnorm, nl_gz0=nl_gz0)

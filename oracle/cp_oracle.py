@@ -271,6 +271,52 @@ def eke(psi, forces, sysm, kpt_weight=1.0):
 
 
 # ----------------------------------------------------------------------------
+# nonlocal pseudopotential, structure-factor (N^2) method, l = 0 KB
+# ----------------------------------------------------------------------------
+
+def struct_fact(sysm):
+    """``CPNONLOCAL::CP_calc_Struct_Fact`` (``cp_nonlocal/cp_struct_fact.C:37-255``)
+    for l = 0: SF[a][g] = w_g p_t(|g|) y00 conj(exp(i g.R_a)), w_g = 1 on
+    kx = 0 and 2 elsewhere, y00 = 1/sqrt(4 pi), p_t(0) = gzvps0
+    (``get_rad_proj`` 260-285); the conjugation is the doublePack im flip
+    at the end of the routine.  Returns ([natm_nl, ng] complex, atom list)."""
+    nl = sysm.nl_atoms()
+    f = TWO_PI / sysm.box
+    gx, gy, gz = f * sysm.kx, f * sysm.ky, f * sysm.kz
+    g = np.sqrt(gx * gx + gy * gy + gz * gz)
+    w = np.where(sysm.kx == 0, 1.0, 2.0)
+    y00 = 1.0 / math.sqrt(4.0 * math.pi)
+    out = np.zeros((len(nl), sysm.ng), dtype=np.complex128)
+    for ia, a in enumerate(nl):
+        t = int(sysm.atm_type[a])
+        p = sysm.nl_proj.eval(np.full(g.shape, t), np.where(g == 0, 1.0, g))
+        p = np.where(g == 0, sysm.nl_gz0[t], p)
+        x, y, z = sysm.pos[a]
+        arg = x * gx + y * gy + z * gz
+        out[ia] = np.conj(np.exp(1j * arg)) * (w * p * y00)
+    return out, nl
+
+
+def nl_energy_forces(psi, sysm, sf=None):
+    """Z matrix, ENL and the nonlocal coefficient forces of the N^2 method:
+    ``CPNONLOCAL::CP_enl_matrix_calc`` (``cp_nlmat.C:24-100``, DGEMV over the
+    2 ng real view), ``CP_enl_atm_forc_calc`` (``cp_nl_energy_forc.C:178-235``,
+    ENL = occ sum_a Z^2 vnorm / V, Z <- 2 vnorm / V Z) and
+    ``CP_enl_force_calc`` (``cp_nl_energy_forc.C:29-110``, F -= sum_a Z SF_a).
+    Returns (F_nl [nstate, ng] complex, per-state ENL, Z)."""
+    if sf is None:
+        sf, nl = struct_fact(sysm)
+    else:
+        nl = sysm.nl_atoms()
+    vn = sysm.nl_vnorm[sysm.atm_type[nl]] / sysm.vol
+    Z = real_view(psi) @ real_view(sf).T                 # [nstate, natm_nl]
+    enl = sysm.occ * np.sum(Z * Z * vn[None, :], axis=1)
+    Zp = 2.0 * vn[None, :] * Z
+    f = -(Zp @ sf)
+    return f, enl, Z
+
+
+# ----------------------------------------------------------------------------
 # PairCalculator / Ortho
 # ----------------------------------------------------------------------------
 
@@ -444,7 +490,12 @@ def psiv_reset(st, sysm):
     st.T = np.eye(sysm.nstate)
 
 
-def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl=None):
+def _nl_default(psi, sysm):
+    f, enl, _ = nl_energy_forces(psi, sysm)
+    return f, float(enl.sum())
+
+
+def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl="auto", norb_tol=None):
     """One CPAIMD electronic step.  Order: forces on the orthonormal psi
     (computePsiFandVKS + NL, combineForcesGetEke), constraint force
     (computeLambdaAndCg), integrate (integrateModForce ->
@@ -452,6 +503,8 @@ def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl=None):
     (computeNewPsi).  Returns the energy record of the psi the forces were
     evaluated on."""
     st.iteration += 1
+    if nl == "auto":
+        nl = _nl_default if len(sysm.nl_atoms()) else None
     fnl, enl = (None, 0.0) if nl is None else nl(st.psi, sysm)
     f, en = electronic_forces(st.psi, sysm, fnl, enl)
     f, lam = lambda_step(st.psi, f, st.T, sysm)
@@ -467,4 +520,7 @@ def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl=None):
     st.psi, st.T, S, it, err = ortho_psi(st.psi_t, sysm, tol, max_iter)
     en["ORTHO_ITERS"] = it
     en["ORTHO_ERR"] = err
+    en["SMAX"] = float(np.max(np.abs(S - 2.0 * np.eye(sysm.nstate))))
+    if norb_tol is not None and en["SMAX"] > norb_tol:
+        psiv_reset(st, sysm)
     return en

@@ -116,7 +116,8 @@ def test_pc_forward_and_ortho(case):
     torch.cuda.synchronize()
     o = out.cpu().numpy()
     assert rel(o, new_ref) < 1e-12
-    Snew = O.gamma_overlap(o, s.kx)
+    from openatom_b200.system import gamma_overlap
+    Snew = gamma_overlap(o, s.kx)
     assert np.max(np.abs(Snew - 2 * np.eye(n))) < 1e-12
 
 
@@ -162,3 +163,16 @@ def test_integrate(case):
     assert rel(Vg.cpu().numpy(), v2) < 1e-13
     assert rel(Pg.cpu().numpy(), p2) < 1e-13
     assert abs(en["FICT_KE"] - ke) <= 1e-12 * max(ke, 1e-30)
+
+
+def test_nonlocal_structure_factor(case):
+    import torch
+    s, ctx, psi = case
+    f = torch.zeros_like(psi)
+    enl = torch.zeros(s.nstate, dtype=torch.float64, device="cuda")
+    ctx.nl_sf(psi, f, nterm=0, enl_out=enl)
+    torch.cuda.synchronize()
+    fr, er, _ = O.nl_energy_forces(s.psi, s)
+    assert rel(f.cpu().numpy(), fr) < 1e-12
+    assert rel(enl.cpu().numpy(), er) < 1e-12
+    assert abs(ctx.energies()["ENL"] - er.sum()) <= 1e-12 * abs(er.sum())

@@ -93,7 +93,7 @@ def test_energy_conservation(w2):
         tot = []
         for _ in range(int(round(1.0 / dt))):
             en = O.cp_step(st, s)
-            tot.append(en["EKE"] + en["EHART"] + en["EEXC"] + en["EEXT"] + en["FICT_KE"])
+            tot.append(en["EKE"] + en["EHART"] + en["EEXC"] + en["EEXT"] + en["ENL"] + en["FICT_KE"])
         drifts.append(abs(tot[-1] - tot[0]))
     assert drifts[0] < 1e-3
     assert drifts[1] < drifts[0] / 2.5  # second order in dt
@@ -111,3 +111,16 @@ def test_psiv_reset_restores_orthonormal_frame(w2):
     r2i = 1 / math.sqrt(2)
     A = O.pc_forward(O.kx0_scale(st.psi, s, r2i), O.kx0_scale(st.v, s, r2i), s, 2.0)
     assert np.max(np.abs(A + A.T)) < 1e-12
+
+
+def test_nonlocal_force_is_energy_gradient(w2):
+    """F_nl = -dE_nl/d(Re c, Im c) (kx > 0) checked by finite differences."""
+    s = w2
+    f, enl, _ = O.nl_energy_forces(s.psi, s)
+    rng = np.random.default_rng(4)
+    d = (rng.standard_normal(s.psi.shape) + 1j * rng.standard_normal(s.psi.shape)) * 1e-6
+    d[:, :s.nkx0] = 0.0
+    e1 = O.nl_energy_forces(s.psi + d, s)[1].sum()
+    e0 = O.nl_energy_forces(s.psi - d, s)[1].sum()
+    pred = -2.0 * np.sum(f.real * d.real + f.imag * d.imag)
+    assert abs((e1 - e0) - pred) < 1e-6 * abs(pred)
