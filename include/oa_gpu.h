@@ -210,6 +210,49 @@ oa_status oa_gpu_sizes(const oa_ctx *ctx, long *out);
  * atom positions on every call. */
 oa_status oa_gpu_nl_sf(oa_ctx *ctx, void *stream, const double *psi, int nterm, double *fnl_out, double *enl_out);
 
+/* State of one CP dynamics run (caller-owned device buffers). */
+typedef struct {
+  double *psi_t;        /* [nstate][ng] non-orthogonal coefficients (integrated) */
+  double *psi;          /* [nstate][ng] orthonormal coefficients psi_t T */
+  double *vpsi;         /* [nstate][ng] coefficient velocities */
+  double *T;            /* [nstate][nstate] last Newton-Schulz result */
+  int iteration;        /* steps done; the call increments it */
+  double dt;            /* time step (a.u.) */
+  double ns_tol;        /* invsqr_tolerance (default 1e-15) */
+  double norb_tol;      /* cp_norb_tol for the PsiV reset (default 0.003) */
+  int ns_max_iter;      /* invsqr_max_iter */
+  int mixed_nterm;      /* 0: FP64 GEMMs; 2 or 3: split-BF16 tcgen05 for Lambda, F', nonlocal */
+  int use_graph;        /* replay the steady-state step as one CUDA graph */
+  int last_ns_iters;    /* out */
+  double last_ns_err;   /* out */
+  double last_smax;     /* out: max |S - 2I| of this step */
+} oa_cp_state;
+
+/* One whole CP dynamics step (GSpaceDriver::computeDynamics,
+ * cp_state_ctrl/gspace.ci:199-324): forces, constraint force, Verlet
+ * integration, orthonormalisation, in native code with one host
+ * synchronisation at the end.  A PsiV reset triggered by max|S - 2I| >
+ * norb_tol runs at the start of the next call.  energies_out (optional,
+ * host [11]): EKE EHART EEXT EWALD_RECIP EEXC MUXC FICT_KE ENL, Newton-Schulz
+ * iterations, residual, max|S - 2I|. */
+oa_status oa_gpu_cp_step(oa_ctx *ctx, void *stream, oa_cp_state *state, double *energies_out);
+
+
+/* Set up the EES nonlocal path (cp_nonloc_ees_opt on): nonlocal grid
+ * na x nb x nc (2^a 3^b 5^c, each >= order), B-spline order (even, 4..16),
+ * and the per-g projector factor dyp(g) = d(g) y00 p(|g|) (host
+ * [ng][2] doubles; eesSetEesWghtGgrp cp_ees_nonlocal.C:60-160 and
+ * eesProjGchare 594-727).  Allocates the nonlocal-grid scratch. */
+oa_status oa_gpu_ees_init(oa_ctx *ctx, int na, int nb, int nc, int order, const double *dyp);
+
+/* Nonlocal energy and coefficient forces by the EES method:
+ * eesAtmBsplineRgrp (cp_ees_nonlocal.C:256-593), eesProjGchare + the
+ * nonlocal-grid FFT (CP_State_ParticlePlane.C:867-1136), eesZmatRchare
+ * (1238-1352) and its plane reduction, eesEnergyAtmForcRchare (1480-1720),
+ * the inverse FFT and eesPsiForcGspace (2000-2079).  Same outputs as
+ * oa_gpu_nl_sf. */
+oa_status oa_gpu_nl_ees(oa_ctx *ctx, void *stream, const double *psi, double *fnl_out, double *enl_out);
+
 /* Energies of the last vks_build / vks_apply_fft_bwd (synchronises):
  * out[0..7] = EKE, EHART, EEXT, EWALD_RECIP, EEXC, MUXC, FICT_KE, ENL. */
 oa_status oa_gpu_energies(oa_ctx *ctx, void *stream, double *out8);

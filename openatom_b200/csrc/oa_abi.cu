@@ -7,7 +7,8 @@
 #include "oa_internal.h"
 
 // launchers from the other translation units
-size_t oa_plane_smem_bytes(int precision, int nx, int ny, int nkx, int npair, int ychunk, bool tile);
+size_t oa_plane_smem_bytes(int precision, int nx, int ny, int nkx);
+int oa_plane_blocks_per_sm(int precision);
 size_t oa_rho_plane_smem_bytes(int nx, int ny, int nkx, int npair, int ychunk);
 int oa_rho_xc_nblk();
 int oa_rho_z_nblk(const oa_ctx* c);
@@ -172,15 +173,11 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     free(F);
     return OA_ERR_UNSUPPORTED;
   }
-  // plane kernel chunking to fit shared memory
-  c->npair_s = 16; c->ychunk_s = 16;
-  while (oa_plane_smem_bytes(precision, d->nx, d->ny, c->nkx_s, c->npair_s, c->ychunk_s, true) > OA_MAX_SMEM &&
-         c->npair_s > 1) { c->npair_s /= 2; c->ychunk_s = c->npair_s; }
   c->npair_d = 16; c->ychunk_d = 16;
   while (oa_rho_plane_smem_bytes(d->nx, d->ny, c->nkx_d, c->npair_d, c->ychunk_d) > OA_MAX_SMEM && c->npair_d > 1) {
     c->npair_d /= 2; c->ychunk_d = c->npair_d;
   }
-  c->smem_plane = oa_plane_smem_bytes(precision, d->nx, d->ny, c->nkx_s, c->npair_s, c->ychunk_s, true);
+  c->smem_plane = oa_plane_smem_bytes(precision, d->nx, d->ny, c->nkx_s);
   c->smem_rho_plane = oa_rho_plane_smem_bytes(d->nx, d->ny, c->nkx_d, c->npair_d, c->ychunk_d);
   if (c->smem_plane > OA_MAX_SMEM || c->smem_rho_plane > OA_MAX_SMEM) {
     oa_set_error("grid too large for the shared-memory plane kernels at this precision", __FILE__, __LINE__);
@@ -189,7 +186,12 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
   }
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-  const int bps = (int)(228 * 1024 / (c->smem_plane + 1024)) > 0 ? (int)(228 * 1024 / (c->smem_plane + 1024)) : 1;
+  int bps = (int)(228 * 1024 / (c->smem_plane + 1024));
+  {
+    const int occ_bps = oa_plane_blocks_per_sm(precision);
+    if (occ_bps > 0 && occ_bps < bps) bps = occ_bps;
+    if (bps < 1) bps = 1;
+  }
   c->ngroup = pick_groups(d->nz, d->nstate, bps, nsm);
   c->nblk_z = (d->nlines + OA_LB - 1) / OA_LB;
 
@@ -228,6 +230,7 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     TRY(cudaMalloc(&c->zmat, ((size_t)d->natm_nl * d->nstate + 1) * sizeof(double)));
     TRY(cudaMalloc(&c->zt, ((size_t)d->natm_nl * d->nstate + 1) * sizeof(double)));
     TRY(cudaMalloc(&c->enl, (size_t)d->nstate * sizeof(double)));
+    TRY(cudaMalloc(&c->enl_eke, (size_t)d->nstate * sizeof(double)));
     TRY(upload(&p->cmass, d->cmass, d->ng));
     c->tw_x = make_twiddles(d->nx);
     c->tw_y = make_twiddles(d->ny);
@@ -286,15 +289,20 @@ fail:
   return OA_ERR_CUDA;
 }
 
+void oa_step_free(oa_ctx* c);
+static void ees_free(oa_ctx* c);
+
 extern "C" oa_status oa_gpu_destroy(oa_ctx* c) {
   if (!c) return OA_OK;
+  oa_step_free(c);
+  ees_free(c);
   oa_ctx_pc* p = pcx(c);
   void* dev[] = {c->line_kx, c->line_ky, c->line_off, c->line_nneg, c->line_npos, c->kx, c->g2, c->tw_x, c->tw_y,
                  c->tw_z, c->spl, c->q_type, c->atm_type, c->pos, c->phase, c->occ, c->zbuf, c->rho_part, c->rho,
                  c->vks, c->vxc, c->dz, c->red, c->eke_part, p->part, p->ns_work, p->ns_status, p->ns_err,
                  p->partner, p->cmass, p->ke_part, p->dev_e, p->mat_a, p->mat_x, p->eye, p->vtmp, p->upart,
                  p->err_flag, c->ky, c->kz, c->nl_atm, c->nl_spl, c->nl_vnorm, c->nl_gz0, c->sf, c->zmat, c->zt,
-                 c->enl};
+                 c->enl, c->enl_eke};
   for (void* q : dev) if (q) cudaFree(q);
   if (p->h_status) cudaFreeHost(p->h_status);
   if (p->h_vals) cudaFreeHost(p->h_vals);
@@ -363,25 +371,21 @@ extern "C" oa_status oa_gpu_set_vks(oa_ctx* c, void* stream, const double* vks) 
   return OA_OK;
 }
 
-__global__ void k_eke_states(const double* part, int nblk, int nstate, double* eke_state, double* total) {
+// EKE per state (one block per state, deterministic) = half the weighted sum
+__global__ void k_eke_states(const double* part, int nblk, double* eke_state) {
   __shared__ double sh[32];
-  double tsum = 0.0;
-  for (int st = 0; st < nstate; ++st) {
-    double sv = 0.0;
-    for (int i = threadIdx.x; i < nblk; i += blockDim.x) sv += part[(size_t)st * nblk + i];
+  const int st = blockIdx.x;
+  double sv = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) sv += part[(size_t)st * nblk + i];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) sv += __shfl_xor_sync(0xffffffffu, sv, o);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = sv;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
-      if (eke_state) eke_state[st] = 0.5 * t;
-      tsum += 0.5 * t;
-    }
-    __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) sv += __shfl_xor_sync(0xffffffffu, sv, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = sv;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+    eke_state[st] = 0.5 * t;
   }
-  if (threadIdx.x == 0) total[0] = tsum;
 }
 
 extern "C" oa_status oa_gpu_vks_apply_fft_bwd(oa_ctx* c, void* stream, const double* psi, int recompute_fwd,
@@ -391,8 +395,10 @@ extern "C" oa_status oa_gpu_vks_apply_fft_bwd(oa_ctx* c, void* stream, const dou
   if (recompute_fwd) OA_CUDA_TRY(oa_launch_state_zfwd(c, s, (const double2*)psi, 0, c->nstate));
   OA_CUDA_TRY(oa_launch_state_plane_vks(c, s));
   OA_CUDA_TRY(oa_launch_state_zbwd(c, s, (const double2*)psi, (const double2*)fnl, (double2*)force, 0, c->nstate));
-  k_eke_states<<<1, 256, 0, s>>>(c->eke_part, c->nblk_z, c->nstate, eke_out, pcx(c)->dev_e + OA_E_EKE);
+  double* es = eke_out ? eke_out : c->enl_eke;
+  k_eke_states<<<c->nstate, 128, 0, s>>>(c->eke_part, c->nblk_z, es);
   OA_CUDA_TRY(cudaGetLastError());
+  OA_CUDA_TRY(oa_launch_sum_partials(s, es, c->nstate, 1, 0, 1.0, pcx(c)->dev_e + OA_E_EKE));
   return OA_OK;
 }
 
@@ -558,8 +564,9 @@ extern "C" oa_status oa_gpu_sizes(const oa_ctx* c, long* out) {
   OA_ARG_CHECK(c && out, "null argument");
   out[0] = c->nstate; out[1] = c->ng; out[2] = c->nlines; out[3] = c->nz; out[4] = c->ldl;
   out[5] = c->ngroup; out[6] = c->npts; out[7] = c->precision == OA_FP64 ? 8 : 4; out[8] = c->nlines_d;
-  // state_fft_fwd 3 + vks_build 10 + vks_apply 3 + lambda (2+1+1+1) + integrate 3 + S (2) + NS 1 + Psi T 1
-  out[9] = 3 + 10 + 3 + 5 + 3 + 2 + 1 + 1;
+  // kernels of oa_gpu_cp_step: state_fft_fwd 3 + vks_build 10 + nl_sf 7 + vks_apply 4 + lambda 4 +
+  // integrate 3 + S 2 + Newton-Schulz 1 + Psi T 1
+  out[9] = 3 + 10 + 7 + 4 + 4 + 3 + 2 + 1 + 1;
   return OA_OK;
 }
 
@@ -631,5 +638,84 @@ extern "C" oa_status oa_gpu_nl_sf(oa_ctx* c, void* stream, const double* psi, in
                                    0, fnl_out, p->err_flag));
   OA_CUDA_TRY(oa_launch_sum_partials(s, c->enl, n, 1, 0, 1.0, p->dev_e + OA_E_ENL));
   if (enl_out) OA_CUDA_TRY(cudaMemcpyAsync(enl_out, c->enl, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  return OA_OK;
+}
+
+cudaError_t oa_step_ortho_args(oa_ctx* c, double** work, int** status, double** errv, int* grid, double** dev_e,
+                               int** h_status, double** h_vals, double** eye) {
+  oa_ctx_pc* p = pcx(c);
+  *work = p->ns_work; *status = p->ns_status; *errv = p->ns_err; *grid = p->ns_grid; *dev_e = p->dev_e;
+  *h_status = p->h_status; *h_vals = p->h_vals; *eye = p->eye;
+  return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// EES nonlocal path
+// ---------------------------------------------------------------------------
+static void ees_free(oa_ctx* c) {
+  oa_ees* e = c->ees;
+  if (!e) return;
+  void* dev[] = {e->tw_a, e->tw_b, e->tw_c, e->zbuf, e->dyp, e->idx, e->mn, e->zpart, e->zmat, e->zs, e->enl};
+  for (void* q : dev) if (q) cudaFree(q);
+  free(e);
+  c->ees = nullptr;
+}
+
+int oa_plane_blocks_per_sm(int precision);
+
+extern "C" oa_status oa_gpu_ees_init(oa_ctx* c, int na, int nb, int nc, int order, const double* dyp_host) {
+  OA_ARG_CHECK(c && dyp_host, "null argument");
+  OA_ARG_CHECK(order >= 4 && order <= 16 && order % 2 == 0, "EES order must be even, 4..16 (cp_pseudo_ees_order)");
+  OA_ARG_CHECK(na >= order && nb >= order && nc >= order, "EES grid smaller than the interpolation order");
+  OA_ARG_CHECK(c->natm_nl > 0, "no nonlocal atoms");
+  ees_free(c);
+  oa_ees* e = (oa_ees*)calloc(1, sizeof(oa_ees));
+  if (!e) return OA_ERR_CUDA;
+  c->ees = e;
+  e->na = na; e->nb = nb; e->nc = nc; e->order = order;
+  if (!make_plan(na, &e->pa) || !make_plan(nb, &e->pb) || !make_plan(nc, &e->pc)) {
+    ees_free(c);
+    oa_set_error("EES grid size must be 2^a 3^b 5^c with at least two radix stages", __FILE__, __LINE__);
+    return OA_ERR_UNSUPPORTED;
+  }
+  int mkx = 0, mky = 0, mkz = 0;
+  (void)mky; (void)mkz;
+  mkx = c->nkx_s - 1;
+  if (2 * mkx + 1 > na) { ees_free(c); oa_set_error("EES grid too small for the state sphere", __FILE__, __LINE__); return OA_ERR_BAD_ARG; }
+  const size_t smem = oa_plane_smem_bytes(c->precision, na, nb, c->nkx_s);
+  if (smem > OA_MAX_SMEM) { ees_free(c); oa_set_error("EES grid too large for the plane kernel", __FILE__, __LINE__); return OA_ERR_UNSUPPORTED; }
+  int bps = (int)(228 * 1024 / (smem + 1024));
+  const int occ_bps = oa_plane_blocks_per_sm(c->precision);
+  if (occ_bps > 0 && occ_bps < bps) bps = occ_bps;
+  if (bps < 1) bps = 1;
+  e->ngroup = pick_groups(nc, c->nstate, bps, pcx(c)->nsm);
+  cudaError_t err = cudaSuccess;
+  const size_t csz = c->precision == OA_FP64 ? sizeof(double2) : sizeof(float2);
+#define TRYE(x) do { err = (x); if (err != cudaSuccess) { ees_free(c); oa_set_error(cudaGetErrorString(err), __FILE__, __LINE__); return OA_ERR_CUDA; } } while (0)
+  e->tw_a = make_twiddles(na);
+  e->tw_b = make_twiddles(nb);
+  e->tw_c = make_twiddles(nc);
+  if (!e->tw_a || !e->tw_b || !e->tw_c) { ees_free(c); oa_set_error("twiddle allocation failed", __FILE__, __LINE__); return OA_ERR_CUDA; }
+  TRYE(cudaMalloc(&e->zbuf, (size_t)c->nstate * nc * c->ldl * csz));
+  TRYE(upload(&e->dyp, (const double2*)dyp_host, (size_t)c->ng));
+  TRYE(cudaMalloc(&e->idx, (size_t)c->natm_nl * 3 * order * sizeof(int)));
+  TRYE(cudaMalloc(&e->mn, (size_t)c->natm_nl * 3 * order * sizeof(double)));
+  TRYE(cudaMalloc(&e->zpart, (size_t)c->nstate * c->natm_nl * order * sizeof(double)));
+  TRYE(cudaMalloc(&e->zmat, (size_t)c->nstate * c->natm_nl * sizeof(double)));
+  TRYE(cudaMalloc(&e->zs, (size_t)c->nstate * c->natm_nl * sizeof(double)));
+  TRYE(cudaMalloc(&e->enl, (size_t)c->nstate * sizeof(double)));
+#undef TRYE
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_nl_ees(oa_ctx* c, void* stream, const double* psi, double* fnl_out, double* enl_out) {
+  OA_ARG_CHECK(c && psi && fnl_out, "null argument");
+  if (!c->ees) { oa_set_error("oa_gpu_ees_init has not been called", __FILE__, __LINE__); return OA_ERR_BAD_ARG; }
+  cudaStream_t s = (cudaStream_t)stream;
+  oa_ees* e = c->ees;
+  OA_CUDA_TRY(oa_launch_ees_bspline(c, s));
+  OA_CUDA_TRY(oa_launch_ees(c, s, (const double2*)psi, (double2*)fnl_out));
+  OA_CUDA_TRY(oa_launch_sum_partials(s, e->enl, c->nstate, 1, 0, 1.0, pcx(c)->dev_e + OA_E_ENL));
+  if (enl_out) OA_CUDA_TRY(cudaMemcpyAsync(enl_out, e->enl, (size_t)c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, s));
   return OA_OK;
 }

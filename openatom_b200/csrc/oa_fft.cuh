@@ -93,11 +93,12 @@ template <int SIGN, typename C> __device__ __forceinline__ void dft5(C* v) {
 template <int RAD, int SIGN, typename C>
 __device__ __forceinline__ void stockham_stage(const C* __restrict__ src, int ld_src,
                                                C* __restrict__ dst, int ld_dst,
-                                               int n, int Ns, int nb, const C* __restrict__ tw) {
+                                               int n, int Ns, int nb, const C* __restrict__ tw,
+                                               int t0, int tstep) {
   const int m = n / RAD;
   const int tstride = n / (Ns * RAD);
   const int total = nb * m;
-  for (int w = threadIdx.x; w < total; w += blockDim.x) {
+  for (int w = t0; w < total; w += tstep) {
     const int s = w / m;
     const int j = w - s * m;
     const int k = j % Ns;
@@ -126,12 +127,12 @@ __device__ __forceinline__ void stockham_stage(const C* __restrict__ src, int ld
 
 template <int SIGN, typename C>
 __device__ __forceinline__ void fft_stage_dispatch(int rad, const C* src, int lds, C* dst, int ldd,
-                                                   int n, int Ns, int nb, const C* tw) {
+                                                   int n, int Ns, int nb, const C* tw, int t0, int tstep) {
   switch (rad) {
-    case 2: stockham_stage<2, SIGN>(src, lds, dst, ldd, n, Ns, nb, tw); break;
-    case 3: stockham_stage<3, SIGN>(src, lds, dst, ldd, n, Ns, nb, tw); break;
-    case 4: stockham_stage<4, SIGN>(src, lds, dst, ldd, n, Ns, nb, tw); break;
-    default: stockham_stage<5, SIGN>(src, lds, dst, ldd, n, Ns, nb, tw); break;
+    case 2: stockham_stage<2, SIGN>(src, lds, dst, ldd, n, Ns, nb, tw, t0, tstep); break;
+    case 3: stockham_stage<3, SIGN>(src, lds, dst, ldd, n, Ns, nb, tw, t0, tstep); break;
+    case 4: stockham_stage<4, SIGN>(src, lds, dst, ldd, n, Ns, nb, tw, t0, tstep); break;
+    default: stockham_stage<5, SIGN>(src, lds, dst, ldd, n, Ns, nb, tw, t0, tstep); break;
   }
 }
 
@@ -145,12 +146,47 @@ __device__ C* fft_pingpong(C* a, C* b, int ld, int nb, const OaFftPlan& p, const
   C* src = a;
   C* dst = b;
   for (int st = 0; st < p.nst; ++st) {
-    fft_stage_dispatch<SIGN>(p.rad[st], src, ld, dst, ld, p.n, Ns, nb, tw);
+    fft_stage_dispatch<SIGN>(p.rad[st], src, ld, dst, ld, p.n, Ns, nb, tw, threadIdx.x, blockDim.x);
     __syncthreads();
     Ns *= p.rad[st];
     C* t = src; src = dst; dst = t;
   }
   return src;
+}
+
+// Warp-cooperative variants: one warp owns the nb sequences, stages are
+// separated by __syncwarp() only.
+template <int SIGN, typename C>
+__device__ C* warp_fft_pingpong(C* a, C* b, int ld, int nb, const OaFftPlan& p, const C* tw, int lane) {
+  int Ns = 1;
+  C* src = a;
+  C* dst = b;
+  for (int st = 0; st < p.nst; ++st) {
+    fft_stage_dispatch<SIGN>(p.rad[st], src, ld, dst, ld, p.n, Ns, nb, tw, lane, 32);
+    __syncwarp();
+    Ns *= p.rad[st];
+    C* t = src; src = dst; dst = t;
+  }
+  return src;
+}
+
+template <int SIGN, typename C>
+__device__ void warp_fft_inout(const C* in, int ld_in, C* out, int ld_out, C* w1, C* w2, int ldw,
+                               int nb, const OaFftPlan& p, const C* tw, int lane) {
+  int Ns = 1;
+  const C* src = in;
+  int lds = ld_in;
+  C* bufs[2] = {w1, w2};
+  for (int st = 0; st < p.nst; ++st) {
+    const bool last = (st == p.nst - 1);
+    C* dst = last ? out : bufs[st & 1];
+    const int ldd = last ? ld_out : ldw;
+    fft_stage_dispatch<SIGN>(p.rad[st], src, lds, dst, ldd, p.n, Ns, nb, tw, lane, 32);
+    __syncwarp();
+    Ns *= p.rad[st];
+    src = dst;
+    lds = ldd;
+  }
 }
 
 // FFT from `in` (stride ld_in) to `out` (stride ld_out) with two scratch
@@ -166,7 +202,7 @@ __device__ void fft_inout(const C* in, int ld_in, C* out, int ld_out, C* w1, C* 
     const bool last = (st == p.nst - 1);
     C* dst = last ? out : bufs[st & 1];
     const int ldd = last ? ld_out : ldw;
-    fft_stage_dispatch<SIGN>(p.rad[st], src, lds, dst, ldd, p.n, Ns, nb, tw);
+    fft_stage_dispatch<SIGN>(p.rad[st], src, lds, dst, ldd, p.n, Ns, nb, tw, threadIdx.x, blockDim.x);
     __syncthreads();
     Ns *= p.rad[st];
     src = dst;

@@ -10,6 +10,21 @@
 #define OA_LB 16          // z-lines per block in the z passes
 #define OA_MAX_SMEM (227 * 1024)
 
+// EES nonlocal path (nonlocal grid na x nb x nc, B-spline order)
+struct oa_ees {
+  int na, nb, nc, order, ngroup;
+  OaFftPlan pa, pb, pc;
+  double2 *tw_a, *tw_b, *tw_c;
+  void* zbuf;          // [nstate][nc][ldl] compute precision
+  double2* dyp;        // [ng] d(g) y00 p(|g|)
+  int* idx;            // [natm_nl][3][order]
+  double* mn;          // [natm_nl][3][order]
+  double* zpart;       // [nstate][natm_nl][order]
+  double* zmat;        // [nstate][natm_nl]
+  double* zs;          // [nstate][natm_nl]
+  double* enl;         // [nstate]
+};
+
 struct oa_ctx {
   int device;
   int precision;          // OA_FP64 or OA_MIXED
@@ -43,6 +58,7 @@ struct oa_ctx {
   double *nl_spl, *nl_vnorm, *nl_gz0;
   double2 *sf;            // [natm_nl][ng] structure factor x projector
   double *zmat, *zt, *enl;
+  double *enl_eke;        // [nstate] per-state EKE scratch
   // scratch (FFT path precision R; byte sizes)
   void *zbuf;             // [nstate][nz][ldl] C
   size_t zbuf_bytes;
@@ -56,8 +72,10 @@ struct oa_ctx {
   double *eke_part;       // [nstate][nblk_z]
   int nblk_z;
   double energies[8];
+  void *step;             // native-step scratch and captured graph (oa_step.cu)
+  oa_ees *ees;            // EES nonlocal path, after oa_gpu_ees_init
   size_t smem_plane, smem_rho_plane;
-  int npair_s, npair_d, ychunk_s, ychunk_d;
+  int npair_d, ychunk_d;
 };
 
 enum { OA_E_EKE = 0, OA_E_EHART, OA_E_EEXT, OA_E_EWALD, OA_E_EEXC, OA_E_MUXC, OA_E_ENL, OA_E_FICT };
@@ -79,3 +97,7 @@ cudaError_t oa_launch_state_zbwd(oa_ctx* c, cudaStream_t s, const double2* psi, 
                                  double2* force, int s0, int ns);
 cudaError_t oa_launch_rho_xc(oa_ctx* c, cudaStream_t s);
 cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s);
+cudaError_t oa_launch_ees(oa_ctx* c, cudaStream_t s, const double2* psi, double2* fnl);
+cudaError_t oa_launch_ees_zreduce(oa_ctx* c, cudaStream_t s);
+cudaError_t oa_launch_ees_bspline(oa_ctx* c, cudaStream_t s);
+size_t oa_plane_smem_bytes(int precision, int nx, int ny, int nkx);

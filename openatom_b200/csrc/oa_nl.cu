@@ -78,3 +78,79 @@ cudaError_t oa_launch_nl_zscale(cudaStream_t s, const double* Z, int nstate, int
   k_nl_zscale<<<(nstate + 127) / 128, 128, 0, s>>>(Z, nstate, natm_nl, nl_atm, atm_type, vnorm, rvol, occ, zt, enl);
   return cudaGetLastError();
 }
+
+// ---------------------------------------------------------------------------
+// EES: atom B-splines on the nonlocal grid and the Z reduction
+// ---------------------------------------------------------------------------
+
+// CPNONLOCAL::eesAtmBsplineRgrp (cp_ees_nonlocal.C:256-593): cardinal
+// B-spline of order n at the fractional grid coordinate of each nonlocal atom,
+// per axis; stencil index it - (j - 2) wrapped onto [0, ngrid).
+__global__ void k_ees_bspline(const double* __restrict__ pos, const int* __restrict__ nl_atm, int natm_nl, double box,
+                              int na, int nb, int nc, int order, int* __restrict__ idx, double* __restrict__ mn) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= natm_nl * 3) return;
+  const int a = t / 3, ax = t - a * 3;
+  const int ngrid = ax == 0 ? na : (ax == 1 ? nb : nc);
+  double u0 = pos[nl_atm[a] * 3 + ax] / box;
+  u0 -= rint(u0 - 0.5);
+  if (u0 == 1.0) u0 = 0.0;
+  u0 *= (double)ngrid;
+  const int it = (int)u0;
+  const double frac = u0 - (double)it;
+  double m[17];
+  for (int j = 0; j <= order; ++j) m[j] = 0.0;
+  m[1] = 1.0 - fabs(frac - 1.0);
+  m[2] = 1.0 - fabs(frac + 1.0 - 1.0);
+  for (int n = 3; n <= order; ++n) {
+    const double rn1 = 1.0 / (double)(n - 1);
+    for (int j = n; j >= 2; --j) {
+      const double u = frac + (double)(j - 1);
+      m[j] = (u * m[j] + ((double)n - u) * m[j - 1]) * rn1;
+    }
+    m[1] = frac * m[1] * rn1;
+  }
+  for (int j = 1; j <= order; ++j) {
+    int g = it - (j - 2);
+    g = g > 0 ? g : ngrid + g;
+    g = g <= ngrid ? g : g - ngrid;
+    idx[((size_t)a * 3 + ax) * order + (j - 1)] = g - 1;
+    mn[((size_t)a * 3 + ax) * order + (j - 1)] = m[j];
+  }
+}
+
+// Z = sum over stencil planes; ENL = occ vnorm/V sum Z^2; zs = 2 vnorm/V occ Z
+// (eesEnergyAtmForcRchare, cp_ees_nonlocal.C:1480-1560)
+__global__ void k_ees_zreduce(const double* __restrict__ zpart, int nstate, int natm_nl, int order,
+                              const int* __restrict__ nl_atm, const int* __restrict__ atm_type,
+                              const double* __restrict__ vnorm, double rvol, const double* __restrict__ occ,
+                              double* __restrict__ zmat, double* __restrict__ zs, double* __restrict__ enl) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nstate) return;
+  double e = 0.0;
+  for (int a = 0; a < natm_nl; ++a) {
+    double z = 0.0;
+    for (int j = 0; j < order; ++j) z += zpart[((size_t)s * natm_nl + a) * order + j];
+    const double vn = vnorm[atm_type[nl_atm[a]]] * rvol;
+    zmat[(size_t)s * natm_nl + a] = z;
+    e += z * z * vn;
+    zs[(size_t)s * natm_nl + a] = 2.0 * vn * occ[s] * z;
+  }
+  enl[s] = e * occ[s];
+}
+
+cudaError_t oa_launch_ees_bspline(oa_ctx* c, cudaStream_t s) {
+  oa_ees* e = c->ees;
+  const int n = c->natm_nl * 3;
+  k_ees_bspline<<<(n + 127) / 128, 128, 0, s>>>(c->pos, c->nl_atm, c->natm_nl, c->box, e->na, e->nb, e->nc, e->order,
+                                                 e->idx, e->mn);
+  return cudaGetLastError();
+}
+
+cudaError_t oa_launch_ees_zreduce(oa_ctx* c, cudaStream_t s) {
+  oa_ees* e = c->ees;
+  k_ees_zreduce<<<(c->nstate + 127) / 128, 128, 0, s>>>(e->zpart, c->nstate, c->natm_nl, e->order, c->nl_atm,
+                                                        c->atm_type, c->nl_vnorm, 1.0 / c->vol, c->occ, e->zmat, e->zs,
+                                                        e->enl);
+  return cudaGetLastError();
+}

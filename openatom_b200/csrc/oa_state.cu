@@ -52,7 +52,7 @@ k_state_zfwd(const double2* __restrict__ psi, int ng, int s0,
              const int* __restrict__ line_off, const int* __restrict__ line_nneg,
              const int* __restrict__ line_npos, int nlines,
              typename CplxOf<R>::T* __restrict__ zbuf, int nz, int ldl,
-             OaFftPlan pz, const double2* __restrict__ twz) {
+             OaFftPlan pz, const double2* __restrict__ twz, const double2* __restrict__ dyp) {
   typedef typename CplxOf<R>::T C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ldz = nz + 1;
@@ -72,12 +72,18 @@ k_state_zfwd(const double2* __restrict__ psi, int ng, int s0,
     const int off = line_off[l], nn = line_nneg[l], np = line_npos[l];
     for (int i = lane; i < nn + np; i += 32) {
       const int kzi = (i < nn) ? (nz - nn + i) : (i - nn);
-      const double2 v = ps[off + i];
+      double2 v = ps[off + i];
+      if (dyp) {  // EES projector: projPsiG = conj(dyp psi) (eesProjGchare)
+        const double2 d = dyp[off + i];
+        v = make_double2(d.x * v.x - d.y * v.y, -(d.y * v.x + d.x * v.y));
+      }
       a[lb * ldz + kzi] = cmk<C>(v.x, v.y);
     }
   }
   __syncthreads();
-  C* r = fft_pingpong<-1>(a, b, ldz, nb, pz, tw);
+  C* r = (pz.nst & 1) ? b : a;
+  for (int lb = warp; lb < nb; lb += nwarp) warp_fft_pingpong<-1>(a + lb * ldz, b + lb * ldz, ldz, 1, pz, tw, lane);
+  __syncthreads();
   C* out = zbuf + (size_t)s * nz * ldl + l0;
   for (int idx = threadIdx.x; idx < nz * OA_LB; idx += blockDim.x) {
     const int z = idx / OA_LB, lb = idx - z * OA_LB;
@@ -104,193 +110,211 @@ __device__ __forceinline__ C herm_x(const C* P, int ldy, int nkx, int nx, int k,
   return v;
 }
 
-// Build W[p][k] = X_{y1}(k) + i X_{y2}(k) for row pairs p in [0, np).
-template <typename C>
-__device__ void build_pairs(C* W, int ldx, const C* P, int ldy, int nkx, int nx, int ny, int p0, int np) {
-  for (int idx = threadIdx.x; idx < np * nx; idx += blockDim.x) {
-    const int p = idx / nx, k = idx - p * nx;
-    const int y1 = 2 * (p0 + p), y2 = y1 + 1;
-    const C a = herm_x(P, ldy, nkx, nx, k, y1);
-    C b = cmk<C>(0.0, 0.0);
-    if (y2 < ny) b = herm_x(P, ldy, nkx, nx, k, y2);
-    C z; z.x = a.x - b.y; z.y = a.y + b.x;
-    W[p * ldx + k] = z;
-  }
-}
+#define OA_PLANE_THREADS 512
+#define OA_PLANE_WARPS (OA_PLANE_THREADS / 32)
 
-// Split W[p][k] = F1(k) + i F2(k) of two real sequences, store k < nkx into P.
-template <typename C>
-__device__ void split_pairs(const C* W, int ldx, C* P, int ldy, int nkx, int nx, int ny, int p0, int np) {
-  typedef decltype(W[0].x) R;
-  for (int idx = threadIdx.x; idx < np * nkx; idx += blockDim.x) {
-    const int p = idx / nkx, k = idx - p * nkx;
-    const int y1 = 2 * (p0 + p), y2 = y1 + 1;
-    const C a = W[p * ldx + k];
-    const C b = cconj(W[p * ldx + (k == 0 ? 0 : nx - k)]);
-    C f1, f2;
-    f1.x = (a.x + b.x) * (R)0.5; f1.y = (a.y + b.y) * (R)0.5;
-    const R dx = a.x - b.x, dy = a.y - b.y;
-    f2.x = dy * (R)0.5; f2.y = -dx * (R)0.5;
-    P[k * ldy + y1] = f1;
-    if (y2 < ny) P[k * ldy + y2] = f2;
-  }
-}
+// EES stencil data for the nonlocal-grid plane modes
+struct EesArgs {
+  const int* idx;       // [natm][3][order] grid index per axis (a, b, c)
+  const double* mn;     // [natm][3][order] B-spline weight per axis
+  double* zpart;        // [nstate][natm][order] MODE 2: per-plane Z contributions
+  const double* zs;     // [nstate][natm]        MODE 3: scaled Z to scatter
+  int natm, order;
+};
 
 struct PlaneSmem {
-  size_t tw_x, tw_y, P, W1, W2, tile, red, total;
+  size_t tw_x, tw_y, P, tile, wbuf, total;
+  int ldw;  // per-warp buffer length (complex elements)
 };
 
 template <typename C, typename T>
-static PlaneSmem plane_smem_layout(int nx, int ny, int nkx, int npair, int ychunk, bool tile) {
+static PlaneSmem plane_smem_layout(int nx, int ny, int nkx) {
   PlaneSmem L;
-  const int ldx = nx + 1, ldy = ny + 1;
+  const int ldy = ny + 1;
+  L.ldw = (nx > ny ? nx : ny) + 1;
   size_t o = 0;
   L.tw_x = o; o += align_up(nx * sizeof(C), 16);
   L.tw_y = o; o += align_up(ny * sizeof(C), 16);
   L.P = o; o += align_up((size_t)nkx * ldy * sizeof(C), 16);
-  size_t wsz = (size_t)npair * ldx;
-  if ((size_t)ychunk * ldy > wsz) wsz = (size_t)ychunk * ldy;
-  L.W1 = o; o += align_up(wsz * sizeof(C), 16);
-  L.W2 = o; o += align_up(wsz * sizeof(C), 16);
-  L.tile = o; if (tile) o += align_up((size_t)nx * ny * sizeof(T), 16);
-  L.red = o; o += 64 * sizeof(double);
+  L.tile = o; o += align_up((size_t)nx * ny * sizeof(T), 16);
+  L.wbuf = o; o += align_up((size_t)OA_PLANE_WARPS * 2 * L.ldw * sizeof(C), 16);
   L.total = o;
   return L;
 }
 
-// y FFT of all nkx columns of P, in place, in chunks through W1/W2.
-template <int SIGN, typename C>
-__device__ void plane_yfft(C* P, int ldy, int nkx, int ychunk, C* W1, C* W2, const OaFftPlan& py, const C* twy) {
-  for (int c0 = 0; c0 < nkx; c0 += ychunk) {
-    const int nb = min(ychunk, nkx - c0);
-    fft_inout<SIGN>(P + c0 * ldy, ldy, P + c0 * ldy, ldy, W1, W2, ldy, nb, py, twy);
-  }
-}
-
 // ---------------------------------------------------------------------------
-// plane pass, forward + density: zbuf row (s, z) -> P[kx][y] -> y FFT(-) ->
-// c2r x FFT(-) by row pairs -> rho tile += occ psi(r)^2
+// plane pass for one z-plane and a group of states.  MODE 0 (density):
+// zbuf row -> P[kx][y] -> y FFT(-) -> c2r x FFT(-) by row pairs -> tile +=
+// occ psi(r)^2.  MODE 1 (V_KS): ... -> psi(r) * V_KS occ -> r2c x FFT(+) ->
+// y FFT(+) -> zbuf row (in place).  Every pencil (a y column or an x row
+// pair) is owned by one warp; stages synchronise with __syncwarp, the block
+// synchronises only between the gather / y / x / y / scatter phases.
 // ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(OA_NTHREADS)
-k_state_plane_density(const typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlines,
-                      const int* __restrict__ line_kx, const int* __restrict__ line_ky,
-                      int nx, int ny, int nz, int nkx,
-                      OaFftPlan px, OaFftPlan py, const double2* __restrict__ twx, const double2* __restrict__ twy,
-                      const double* __restrict__ occ, double* __restrict__ rho_part,
-                      int ngroup, int npair, int ychunk, PlaneSmem L) {
+template <typename R, int MODE>
+__global__ void __launch_bounds__(OA_PLANE_THREADS)
+k_state_plane(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlines,
+              const int* __restrict__ line_kx, const int* __restrict__ line_ky,
+              int nx, int ny, int nz, int nkx,
+              OaFftPlan px, OaFftPlan py, const double2* __restrict__ twx, const double2* __restrict__ twy,
+              const double* __restrict__ occ, const R* __restrict__ vks, double* __restrict__ rho_part,
+              int ngroup, PlaneSmem L, EesArgs E) {
   typedef typename CplxOf<R>::T C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* stwx = (C*)(smem_raw + L.tw_x);
   C* stwy = (C*)(smem_raw + L.tw_y);
   C* P = (C*)(smem_raw + L.P);
-  C* W1 = (C*)(smem_raw + L.W1);
-  C* W2 = (C*)(smem_raw + L.W2);
   R* tile = (R*)(smem_raw + L.tile);
-  const int ldx = nx + 1, ldy = ny + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C* wa = (C*)(smem_raw + L.wbuf) + (size_t)warp * 2 * L.ldw;
+  C* wb = wa + L.ldw;
+  const int ldy = ny + 1, ldw = L.ldw;
   const int z = blockIdx.x, g = blockIdx.y;
   const int nper = (nstate + ngroup - 1) / ngroup;
   const int sb = g * nper, se = min(nstate, sb + nper);
   const int npairs = (ny + 1) / 2;
   load_twiddles(stwx, twx, nx);
   load_twiddles(stwy, twy, ny);
-  for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) tile[i] = (R)0;
-  for (int s = sb; s < se; ++s) {
-    for (int i = threadIdx.x; i < nkx * ldy; i += blockDim.x) P[i] = cmk<C>(0.0, 0.0);
-    __syncthreads();
-    const C* row = zbuf + ((size_t)s * nz + z) * ldl;
-    for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
-      int ky = line_ky[l]; if (ky < 0) ky += ny;
-      P[line_kx[l] * ldy + ky] = row[l];
-    }
-    __syncthreads();
-    plane_yfft<-1>(P, ldy, nkx, ychunk, W1, W2, py, stwy);
-    const R o = (R)occ[s];
-    for (int p0 = 0; p0 < npairs; p0 += npair) {
-      const int np = min(npair, npairs - p0);
-      build_pairs(W1, ldx, P, ldy, nkx, nx, ny, p0, np);
-      __syncthreads();
-      C* r = fft_pingpong<-1>(W1, W2, ldx, np, px, stwx);
-      for (int idx = threadIdx.x; idx < np * nx; idx += blockDim.x) {
-        const int p = idx / nx, x = idx - p * nx;
-        const int y1 = 2 * (p0 + p);
-        const C v = r[p * ldx + x];
-        tile[y1 * nx + x] += o * v.x * v.x;
-        if (y1 + 1 < ny) tile[(y1 + 1) * nx + x] += o * v.y * v.y;
-      }
-      __syncthreads();
-    }
+  if (MODE == 0) {
+    for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) tile[i] = (R)0;
+  } else if (MODE == 1) {
+    const R* vz = vks + (size_t)z * nx * ny;
+    for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) tile[i] = vz[i];
   }
-  __syncthreads();
-  double* out = rho_part + ((size_t)g * nz + z) * (size_t)nx * ny;
-  for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) out[i] = (double)tile[i];
-}
-
-// ---------------------------------------------------------------------------
-// plane pass, V_KS: zbuf row -> psi(r) by row pairs -> * V_KS occ -> r2c x
-// FFT(+) -> y FFT(+) -> zbuf row (in place)
-// ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(OA_NTHREADS)
-k_state_plane_vks(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlines,
-                  const int* __restrict__ line_kx, const int* __restrict__ line_ky,
-                  int nx, int ny, int nz, int nkx,
-                  OaFftPlan px, OaFftPlan py, const double2* __restrict__ twx, const double2* __restrict__ twy,
-                  const double* __restrict__ occ, const R* __restrict__ vks,
-                  int ngroup, int npair, int ychunk, PlaneSmem L) {
-  typedef typename CplxOf<R>::T C;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* stwx = (C*)(smem_raw + L.tw_x);
-  C* stwy = (C*)(smem_raw + L.tw_y);
-  C* P = (C*)(smem_raw + L.P);
-  C* W1 = (C*)(smem_raw + L.W1);
-  C* W2 = (C*)(smem_raw + L.W2);
-  R* tile = (R*)(smem_raw + L.tile);
-  const int ldx = nx + 1, ldy = ny + 1;
-  const int z = blockIdx.x, g = blockIdx.y;
-  const int nper = (nstate + ngroup - 1) / ngroup;
-  const int sb = g * nper, se = min(nstate, sb + nper);
-  const int npairs = (ny + 1) / 2;
-  load_twiddles(stwx, twx, nx);
-  load_twiddles(stwy, twy, ny);
-  const R* vz = vks + (size_t)z * nx * ny;
-  for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) tile[i] = vz[i];
   for (int s = sb; s < se; ++s) {
-    for (int i = threadIdx.x; i < nkx * ldy; i += blockDim.x) P[i] = cmk<C>(0.0, 0.0);
-    __syncthreads();
     C* row = zbuf + ((size_t)s * nz + z) * ldl;
-    for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
-      int ky = line_ky[l]; if (ky < 0) ky += ny;
-      P[line_kx[l] * ldy + ky] = row[l];
-    }
-    __syncthreads();
-    plane_yfft<-1>(P, ldy, nkx, ychunk, W1, W2, py, stwy);
-    const R o = (R)occ[s];
-    for (int p0 = 0; p0 < npairs; p0 += npair) {
-      const int np = min(npair, npairs - p0);
-      build_pairs(W1, ldx, P, ldy, nkx, nx, ny, p0, np);
+    if (MODE == 3) {
+      // scatter Z M onto this plane (eesEnergyAtmForcRchare: projPsiRScr[igrid] += z Mn)
+      for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) tile[i] = (R)0;
       __syncthreads();
-      C* r = fft_pingpong<-1>(W1, W2, ldx, np, px, stwx);
-      for (int idx = threadIdx.x; idx < np * nx; idx += blockDim.x) {
-        const int p = idx / nx, x = idx - p * nx;
-        const int y1 = 2 * (p0 + p);
-        C v = r[p * ldx + x];
-        v.x *= tile[y1 * nx + x] * o;
-        v.y = (y1 + 1 < ny) ? v.y * tile[(y1 + 1) * nx + x] * o : (R)0;
-        r[p * ldx + x] = v;
+      const int o2 = E.order * E.order;
+      for (int a = warp; a < E.natm; a += OA_PLANE_WARPS) {
+        const int* ia = E.idx + (size_t)a * 3 * E.order;
+        const double* ma = E.mn + (size_t)a * 3 * E.order;
+        int jc = -1;
+        for (int j = 0; j < E.order; ++j) if (ia[2 * E.order + j] == z) jc = j;
+        if (jc < 0) continue;
+        const double zc = E.zs[(size_t)s * E.natm + a] * ma[2 * E.order + jc];
+        for (int q = lane; q < o2; q += 32) {
+          const int jb = q / E.order, ja = q - jb * E.order;
+          atomicAdd(&tile[ia[E.order + jb] * nx + ia[ja]], (R)(zc * ma[E.order + jb] * ma[ja]));
+        }
       }
       __syncthreads();
-      C* other = (r == W1) ? W2 : W1;
-      C* r2 = fft_pingpong<+1>(r, other, ldx, np, px, stwx);
-      split_pairs(r2, ldx, P, ldy, nkx, nx, ny, p0, np);
+    } else {
+      for (int i = threadIdx.x; i < nkx * ldy; i += blockDim.x) P[i] = cmk<C>(0.0, 0.0);
+      __syncthreads();
+      for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
+        int ky = line_ky[l]; if (ky < 0) ky += ny;
+        P[line_kx[l] * ldy + ky] = row[l];
+      }
+      __syncthreads();
+      for (int c = warp; c < nkx; c += OA_PLANE_WARPS)
+        warp_fft_inout<-1>(P + c * ldy, ldy, P + c * ldy, ldy, wa, wb, ldw, 1, py, stwy, lane);
       __syncthreads();
     }
-    plane_yfft<+1>(P, ldy, nkx, ychunk, W1, W2, py, stwy);
-    for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
-      int ky = line_ky[l]; if (ky < 0) ky += ny;
-      row[l] = P[line_kx[l] * ldy + ky];
+    const R o = (R)occ[s];
+    for (int p = warp; p < npairs; p += OA_PLANE_WARPS) {
+      const int y1 = 2 * p, y2 = y1 + 1;
+      if (MODE == 3) {
+        for (int x = lane; x < nx; x += 32) {
+          C zz; zz.x = tile[y1 * nx + x]; zz.y = (y2 < ny) ? tile[y2 * nx + x] : (R)0;
+          wa[x] = zz;
+        }
+        __syncwarp();
+        C* r2 = warp_fft_pingpong<+1>(wa, wb, ldw, 1, px, stwx, lane);
+        for (int k = lane; k < nkx; k += 32) {
+          const C a = r2[k];
+          const C b = cconj(r2[k == 0 ? 0 : nx - k]);
+          C f1, f2;
+          f1.x = (a.x + b.x) * (R)0.5; f1.y = (a.y + b.y) * (R)0.5;
+          f2.x = (a.y - b.y) * (R)0.5; f2.y = -(a.x - b.x) * (R)0.5;
+          P[k * ldy + y1] = f1;
+          if (y2 < ny) P[k * ldy + y2] = f2;
+        }
+        __syncwarp();
+        continue;
+      }
+      for (int k = lane; k < nx; k += 32) {
+        const C a = herm_x(P, ldy, nkx, nx, k, y1);
+        C b = cmk<C>(0.0, 0.0);
+        if (y2 < ny) b = herm_x(P, ldy, nkx, nx, k, y2);
+        C zz; zz.x = a.x - b.y; zz.y = a.y + b.x;
+        wa[k] = zz;
+      }
+      __syncwarp();
+      C* r = warp_fft_pingpong<-1>(wa, wb, ldw, 1, px, stwx, lane);
+      if (MODE == 0) {
+        for (int x = lane; x < nx; x += 32) {
+          const C v = r[x];
+          tile[y1 * nx + x] += o * v.x * v.x;
+          if (y2 < ny) tile[y2 * nx + x] += o * v.y * v.y;
+        }
+        __syncwarp();
+      } else if (MODE == 2) {
+        for (int x = lane; x < nx; x += 32) {
+          const C v = r[x];
+          tile[y1 * nx + x] = v.x;
+          if (y2 < ny) tile[y2 * nx + x] = v.y;
+        }
+        __syncwarp();
+      } else {
+        for (int x = lane; x < nx; x += 32) {
+          C v = r[x];
+          v.x *= tile[y1 * nx + x] * o;
+          v.y = (y2 < ny) ? v.y * tile[y2 * nx + x] * o : (R)0;
+          r[x] = v;
+        }
+        __syncwarp();
+        C* other = (r == wa) ? wb : wa;
+        C* r2 = warp_fft_pingpong<+1>(r, other, ldw, 1, px, stwx, lane);
+        for (int k = lane; k < nkx; k += 32) {
+          const C a = r2[k];
+          const C b = cconj(r2[k == 0 ? 0 : nx - k]);
+          C f1, f2;
+          f1.x = (a.x + b.x) * (R)0.5; f1.y = (a.y + b.y) * (R)0.5;
+          f2.x = (a.y - b.y) * (R)0.5; f2.y = -(a.x - b.x) * (R)0.5;
+          P[k * ldy + y1] = f1;
+          if (y2 < ny) P[k * ldy + y2] = f2;
+        }
+        __syncwarp();
+      }
     }
     __syncthreads();
+    if (MODE == 2) {
+      // Z gather over the stencil points of this plane (eesZmatRchare)
+      const int o2 = E.order * E.order;
+      for (int a = warp; a < E.natm; a += OA_PLANE_WARPS) {
+        const int* ia = E.idx + (size_t)a * 3 * E.order;
+        const double* ma = E.mn + (size_t)a * 3 * E.order;
+        int jc = -1;
+        for (int j = 0; j < E.order; ++j) if (ia[2 * E.order + j] == z) jc = j;
+        if (jc < 0) continue;
+        double acc = 0.0;
+        for (int q = lane; q < o2; q += 32) {
+          const int jb = q / E.order, ja = q - jb * E.order;
+          acc += (double)tile[ia[E.order + jb] * nx + ia[ja]] * ma[E.order + jb] * ma[ja];
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (lane == 0) E.zpart[((size_t)s * E.natm + a) * E.order + jc] = acc * ma[2 * E.order + jc];
+      }
+      __syncthreads();
+    }
+    if (MODE == 1 || MODE == 3) {
+      for (int c = warp; c < nkx; c += OA_PLANE_WARPS)
+        warp_fft_inout<+1>(P + c * ldy, ldy, P + c * ldy, ldy, wa, wb, ldw, 1, py, stwy, lane);
+      __syncthreads();
+      for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
+        int ky = line_ky[l]; if (ky < 0) ky += ny;
+        row[l] = P[line_kx[l] * ldy + ky];
+      }
+      __syncthreads();
+    }
+  }
+  if (MODE == 0) {
+    __syncthreads();
+    double* out = rho_part + ((size_t)g * nz + z) * (size_t)nx * ny;
+    for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) out[i] = (double)tile[i];
   }
 }
 
@@ -306,7 +330,8 @@ k_state_zbwd(const typename CplxOf<R>::T* __restrict__ zbuf, int nz, int ldl, in
              OaFftPlan pz, const double2* __restrict__ twz,
              const double2* __restrict__ psi, const double2* __restrict__ fnl, double2* __restrict__ force,
              const double* __restrict__ g2, const double* __restrict__ occ, int ng, int s0,
-             double scale, double ecut, double* __restrict__ eke_part, int nblk) {
+             double scale, double ecut, double* __restrict__ eke_part, int nblk,
+             const double2* __restrict__ dyp) {
   typedef typename CplxOf<R>::T C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ldz = nz + 1;
@@ -324,8 +349,10 @@ k_state_zbwd(const typename CplxOf<R>::T* __restrict__ zbuf, int nz, int ldl, in
     if (lb < nb) a[lb * ldz + z] = in[(size_t)z * ldl + lb];
   }
   __syncthreads();
-  C* r = fft_pingpong<+1>(a, b, ldz, nb, pz, tw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  C* r = (pz.nst & 1) ? b : a;
+  for (int lb = warp; lb < nb; lb += nwarp) warp_fft_pingpong<+1>(a + lb * ldz, b + lb * ldz, ldz, 1, pz, tw, lane);
+  __syncthreads();
   const double2* ps = psi + (size_t)s * ng;
   double2* fs = force + (size_t)s * ng;
   const double2* fn = fnl ? fnl + (size_t)s * ng : nullptr;
@@ -341,6 +368,13 @@ k_state_zbwd(const typename CplxOf<R>::T* __restrict__ zbuf, int nz, int ldl, in
       const int kzi = (i < nn) ? (nz - nn + i) : (i - nn);
       const C v = r[lb * ldz + kzi];
       const int idx = off + i;
+      if (dyp) {  // EES psi force (eesPsiForcGspace): F = -w conj(dyp P), Im P = 0 at g = 0
+        const double2 d = dyp[idx];
+        const double px = (double)v.x;
+        const double py = (g2[idx] == 0.0) ? 0.0 : (double)v.y;
+        fs[idx] = make_double2(-w * (d.x * px - d.y * py), w * (d.y * px + d.x * py));
+        continue;
+      }
       double2 f = make_double2((double)v.x * sc, (double)v.y * sc);
       if (fn) { const double2 q = fn[idx]; f.x += q.x; f.y += q.y; }
       const double gg = g2[idx];
@@ -376,33 +410,21 @@ static cudaError_t launch_zfwd(oa_ctx* c, cudaStream_t st, const double2* psi, i
   if (e != cudaSuccess) return e;
   dim3 grid((c->nlines + OA_LB - 1) / OA_LB, ns);
   k_state_zfwd<R><<<grid, OA_NTHREADS, sm, st>>>(psi, c->ng, s0, c->line_off, c->line_nneg, c->line_npos,
-                                                  c->nlines, (C*)c->zbuf, c->nz, c->ldl, c->plan_z, c->tw_z);
+                                                  c->nlines, (C*)c->zbuf, c->nz, c->ldl, c->plan_z, c->tw_z, nullptr);
   return cudaGetLastError();
 }
 
-template <typename R>
-static cudaError_t launch_plane_density(oa_ctx* c, cudaStream_t st) {
+template <typename R, int MODE>
+static cudaError_t launch_plane(oa_ctx* c, cudaStream_t st) {
   typedef typename CplxOf<R>::T C;
-  PlaneSmem L = plane_smem_layout<C, R>(c->nx, c->ny, c->nkx_s, c->npair_s, c->ychunk_s, true);
-  cudaError_t e = cudaFuncSetAttribute(k_state_plane_density<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+  PlaneSmem L = plane_smem_layout<C, R>(c->nx, c->ny, c->nkx_s);
+  cudaError_t e = cudaFuncSetAttribute(k_state_plane<R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
   if (e != cudaSuccess) return e;
   dim3 grid(c->nz, c->ngroup);
-  k_state_plane_density<R><<<grid, OA_NTHREADS, L.total, st>>>(
-      (const C*)c->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky, c->nx, c->ny, c->nz, c->nkx_s,
-      c->plan_x, c->plan_y, c->tw_x, c->tw_y, c->occ, c->rho_part, c->ngroup, c->npair_s, c->ychunk_s, L);
-  return cudaGetLastError();
-}
-
-template <typename R>
-static cudaError_t launch_plane_vks(oa_ctx* c, cudaStream_t st) {
-  typedef typename CplxOf<R>::T C;
-  PlaneSmem L = plane_smem_layout<C, R>(c->nx, c->ny, c->nkx_s, c->npair_s, c->ychunk_s, true);
-  cudaError_t e = cudaFuncSetAttribute(k_state_plane_vks<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
-  if (e != cudaSuccess) return e;
-  dim3 grid(c->nz, c->ngroup);
-  k_state_plane_vks<R><<<grid, OA_NTHREADS, L.total, st>>>(
+  EesArgs E = {nullptr, nullptr, nullptr, nullptr, 0, 0};
+  k_state_plane<R, MODE><<<grid, OA_PLANE_THREADS, L.total, st>>>(
       (C*)c->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky, c->nx, c->ny, c->nz, c->nkx_s,
-      c->plan_x, c->plan_y, c->tw_x, c->tw_y, c->occ, (const R*)c->vks, c->ngroup, c->npair_s, c->ychunk_s, L);
+      c->plan_x, c->plan_y, c->tw_x, c->tw_y, c->occ, (const R*)c->vks, c->rho_part, c->ngroup, L, E);
   return cudaGetLastError();
 }
 
@@ -417,26 +439,86 @@ static cudaError_t launch_zbwd(oa_ctx* c, cudaStream_t st, const double2* psi, c
   k_state_zbwd<R><<<grid, OA_NTHREADS, sm, st>>>(
       (const C*)c->zbuf, c->nz, c->ldl, c->nlines, c->line_kx, c->line_off, c->line_nneg, c->line_npos,
       c->plan_z, c->tw_z, psi, fnl, force, c->g2, c->occ, c->ng, s0, -2.0 / (double)c->npts,
-      c->ecut_psi, c->eke_part, c->nblk_z);
+      c->ecut_psi, c->eke_part, c->nblk_z, nullptr);
   return cudaGetLastError();
 }
 
-size_t oa_plane_smem_bytes(int precision, int nx, int ny, int nkx, int npair, int ychunk, bool tile) {
-  if (precision == OA_FP64) return plane_smem_layout<double2, double>(nx, ny, nkx, npair, ychunk, tile).total;
-  return plane_smem_layout<float2, float>(nx, ny, nkx, npair, ychunk, tile).total;
+size_t oa_plane_smem_bytes(int precision, int nx, int ny, int nkx) {
+  if (precision == OA_FP64) return plane_smem_layout<double2, double>(nx, ny, nkx).total;
+  return plane_smem_layout<float2, float>(nx, ny, nkx).total;
+}
+
+int oa_plane_blocks_per_sm(int precision) {
+  int n = 0;
+  if (precision == OA_FP64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_state_plane<double, 1>, OA_PLANE_THREADS, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_state_plane<float, 1>, OA_PLANE_THREADS, 0);
+  return n;
 }
 
 cudaError_t oa_launch_state_zfwd(oa_ctx* c, cudaStream_t s, const double2* psi, int s0, int ns) {
   return c->precision == OA_FP64 ? launch_zfwd<double>(c, s, psi, s0, ns) : launch_zfwd<float>(c, s, psi, s0, ns);
 }
 cudaError_t oa_launch_state_plane_density(oa_ctx* c, cudaStream_t s) {
-  return c->precision == OA_FP64 ? launch_plane_density<double>(c, s) : launch_plane_density<float>(c, s);
+  return c->precision == OA_FP64 ? launch_plane<double, 0>(c, s) : launch_plane<float, 0>(c, s);
 }
 cudaError_t oa_launch_state_plane_vks(oa_ctx* c, cudaStream_t s) {
-  return c->precision == OA_FP64 ? launch_plane_vks<double>(c, s) : launch_plane_vks<float>(c, s);
+  return c->precision == OA_FP64 ? launch_plane<double, 1>(c, s) : launch_plane<float, 1>(c, s);
 }
 cudaError_t oa_launch_state_zbwd(oa_ctx* c, cudaStream_t s, const double2* psi, const double2* fnl,
                                  double2* force, int s0, int ns) {
   return c->precision == OA_FP64 ? launch_zbwd<double>(c, s, psi, fnl, force, s0, ns)
                                  : launch_zbwd<float>(c, s, psi, fnl, force, s0, ns);
 }
+
+// ---------------------------------------------------------------------------
+// EES nonlocal path on the nonlocal grid (na, nb, nc)
+// ---------------------------------------------------------------------------
+template <typename R>
+static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, double2* fnl) {
+  typedef typename CplxOf<R>::T C;
+  oa_ees* e = c->ees;
+  cudaError_t err;
+  // z pass forward with conj(dyp psi)
+  {
+    size_t sm = zpass_smem<R>(e->nc);
+    err = cudaFuncSetAttribute(k_state_zfwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (err != cudaSuccess) return err;
+    dim3 grid((c->nlines + OA_LB - 1) / OA_LB, c->nstate);
+    k_state_zfwd<R><<<grid, OA_NTHREADS, sm, st>>>(psi, c->ng, 0, c->line_off, c->line_nneg, c->line_npos, c->nlines,
+                                                    (C*)e->zbuf, e->nc, c->ldl, e->pc, e->tw_c, e->dyp);
+    if ((err = cudaGetLastError()) != cudaSuccess) return err;
+  }
+  PlaneSmem L = plane_smem_layout<C, R>(e->na, e->nb, c->nkx_s);
+  EesArgs E = {e->idx, e->mn, e->zpart, e->zs, c->natm_nl, e->order};
+  dim3 pgrid(e->nc, e->ngroup);
+  err = cudaFuncSetAttribute(k_state_plane<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+  if (err != cudaSuccess) return err;
+  k_state_plane<R, 2><<<pgrid, OA_PLANE_THREADS, L.total, st>>>(
+      (C*)e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky, e->na, e->nb, e->nc, c->nkx_s, e->pa, e->pb,
+      e->tw_a, e->tw_b, c->occ, nullptr, nullptr, e->ngroup, L, E);
+  if ((err = cudaGetLastError()) != cudaSuccess) return err;
+  err = oa_launch_ees_zreduce(c, st);
+  if (err != cudaSuccess) return err;
+  err = cudaFuncSetAttribute(k_state_plane<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+  if (err != cudaSuccess) return err;
+  k_state_plane<R, 3><<<pgrid, OA_PLANE_THREADS, L.total, st>>>(
+      (C*)e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky, e->na, e->nb, e->nc, c->nkx_s, e->pa, e->pb,
+      e->tw_a, e->tw_b, c->occ, nullptr, nullptr, e->ngroup, L, E);
+  if ((err = cudaGetLastError()) != cudaSuccess) return err;
+  {
+    size_t sm = zpass_smem<R>(e->nc);
+    err = cudaFuncSetAttribute(k_state_zbwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (err != cudaSuccess) return err;
+    dim3 grid(c->nblk_z, c->nstate);
+    k_state_zbwd<R><<<grid, OA_NTHREADS, sm, st>>>(
+        (const C*)e->zbuf, e->nc, c->ldl, c->nlines, c->line_kx, c->line_off, c->line_nneg, c->line_npos, e->pc,
+        e->tw_c, psi, nullptr, fnl, c->g2, c->occ, c->ng, 0, 1.0, c->ecut_psi, c->eke_part, c->nblk_z, e->dyp);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t oa_launch_ees(oa_ctx* c, cudaStream_t s, const double2* psi, double2* fnl) {
+  return c->precision == OA_FP64 ? launch_ees<double>(c, s, psi, fnl) : launch_ees<float>(c, s, psi, fnl);
+}
+
+size_t oa_ees_plane_smem(int precision, int na, int nb, int nkx) { return oa_plane_smem_bytes(precision, na, nb, nkx); }

@@ -23,7 +23,8 @@
 
 #define UM_KT 64          // K elements per pipeline stage
 #define UM_M 128          // MMA M (rows per CTA tile)
-#define UM_THREADS 128
+#define UM_THREADS 512
+#define UM_ITEMS_MAX 4   // staged 8-element chunks per thread per stage (nb <= 128)
 #define UM_SPIN_LIMIT (1u << 28)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -192,6 +193,55 @@ k_umma_fwd(const double* __restrict__ A, const double* __restrict__ B, int m, in
   uint32_t phase[2] = {0, 0};
   bool ok = true;
   int nst = 0;
+  const int items = (UM_M + nb) * (UM_KT / 8);
+  double pre[UM_ITEMS_MAX][8];
+  auto load_item = [&](int item, long kt, double* x) {
+    const long k0 = kt * UM_KT;
+    const bool isA = item < UM_M * (UM_KT / 8);
+    const int it2 = isA ? item : item - UM_M * (UM_KT / 8);
+    const int rows = isA ? UM_M : nb;
+    const int r = it2 % rows, kc = it2 / rows;
+    const int grow = (isA ? m0 : n0) + r;
+    const double* src = isA ? A : B;
+    const long kb0 = k0 + kc * 8;
+    if (grow < (isA ? m : n) && kb0 + 8 <= K) {
+      const double2* p2 = reinterpret_cast<const double2*>(src + (size_t)grow * K + kb0);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) { const double2 v = p2[e]; x[2 * e] = v.x; x[2 * e + 1] = v.y; }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const long k = kb0 + e;
+        x[e] = (grow < (isA ? m : n) && k < K) ? src[(size_t)grow * K + k] : 0.0;
+      }
+    }
+    if (isA && kb0 < kx0_cols) {
+#pragma unroll
+      for (int e = 0; e < 8; ++e) if (kb0 + e < kx0_cols) x[e] *= w_kx0;
+    }
+  };
+  auto store_item = [&](int item, unsigned char* sb, const double* x) {
+    const bool isA = item < UM_M * (UM_KT / 8);
+    const int it2 = isA ? item : item - UM_M * (UM_KT / 8);
+    const int rows = isA ? UM_M : nb;
+    const int r = it2 % rows, kc = it2 / rows;
+    uint4 t[NT];
+    split8<NT>(x, t);
+    const uint32_t off = canon_off(r, kc, rows);
+#pragma unroll
+    for (int qq = 0; qq < NT; ++qq) {
+      unsigned char* dst = sb + (isA ? qq * L.a_bytes : NT * L.a_bytes + qq * L.b_bytes) + off;
+      *reinterpret_cast<uint4*>(dst) = t[qq];
+    }
+  };
+  auto prefetch = [&](long kt) {
+#pragma unroll
+    for (int q = 0; q < UM_ITEMS_MAX; ++q) {
+      const int item = tid + q * UM_THREADS;
+      if (item < items) load_item(item, kt, pre[q]);
+    }
+  };
+  if (kt0 < kt1) prefetch(kt0);
   for (long kt = kt0; kt < kt1; ++kt, ++nst) {
     const int s = nst & 1;
     if (nst >= 2) {  // wait until the MMAs that read this buffer are done
@@ -200,34 +250,15 @@ k_umma_fwd(const double* __restrict__ A, const double* __restrict__ B, int m, in
       phase[s] ^= 1;
     }
     unsigned char* sb = base + s * L.stage_bytes;
-    const long k0 = kt * UM_KT;
-    // stage A rows (m-tile) and B rows (n-tile): thread -> row, loop over K core columns
-    for (int item = tid; item < (UM_M + nb) * (UM_KT / 8); item += UM_THREADS) {
-      const bool isA = item < UM_M * (UM_KT / 8);
-      const int it2 = isA ? item : item - UM_M * (UM_KT / 8);
-      const int rows = isA ? UM_M : nb;
-      const int r = it2 % rows, kc = it2 / rows;
-      const int grow = (isA ? m0 : n0) + r;
-      const double* src = isA ? A : B;
+#pragma unroll
+    for (int q = 0; q < UM_ITEMS_MAX; ++q) {
+      const int item = tid + q * UM_THREADS;
+      if (item < items) store_item(item, sb, pre[q]);
+    }
+    for (int item = tid + UM_ITEMS_MAX * UM_THREADS; item < items; item += UM_THREADS) {
       double x[8];
-#pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        const long k = k0 + kc * 8 + e;
-        double v = 0.0;
-        if (grow < (isA ? m : n) && k < K) {
-          v = src[(size_t)grow * K + k];
-          if (isA && k < kx0_cols) v *= w_kx0;
-        }
-        x[e] = v;
-      }
-      uint4 t[NT];
-      split8<NT>(x, t);
-      const uint32_t off = canon_off(r, kc, rows);
-#pragma unroll
-      for (int q = 0; q < NT; ++q) {
-        unsigned char* dst = sb + (isA ? q * L.a_bytes : NT * L.a_bytes + q * L.b_bytes) + off;
-        *reinterpret_cast<uint4*>(dst) = t[q];
-      }
+      load_item(item, kt, x);
+      store_item(item, sb, x);
     }
     fence_async_smem();
     __syncthreads();
@@ -236,7 +267,7 @@ k_umma_fwd(const double* __restrict__ A, const double* __restrict__ B, int m, in
       issue_stage<NT>(tmem, smem_u32(sb), L, nb, idesc, nst == 0);
       umma_commit(&bars[s]);
     }
-    __syncthreads();
+    if (kt + 1 < kt1) prefetch(kt + 1);
   }
   // drain: wait for the last (up to two) committed stages
   if (ok) {
@@ -249,8 +280,8 @@ k_umma_fwd(const double* __restrict__ A, const double* __restrict__ B, int m, in
   ok = __syncthreads_and(ok);
   tc_fence_after();
   float* out = part + ((size_t)blockIdx.x * m + m0) * (size_t)n + n0;
-  const int row = warp * 32 + (tid & 31);
-  if (ok && nst > 0) {
+  const int row = (warp & 3) * 32 + (tid & 31);
+  if (warp < 4 && ok && nst > 0) {
     for (int c0 = 0; c0 < nb; c0 += 16) {
       float v[16];
       tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
@@ -260,7 +291,7 @@ k_umma_fwd(const double* __restrict__ A, const double* __restrict__ B, int m, in
           if (n0 + c0 + e < n) out[(size_t)row * n + c0 + e] = v[e];
       }
     }
-  } else if (m0 + row < m) {
+  } else if (warp < 4 && m0 + row < m) {
     for (int c = 0; c < nb && n0 + c < n; ++c) out[(size_t)row * n + c] = 0.0f;
   }
   if (!ok && tid == 0) atomicExch(err_flag, 1);
@@ -308,61 +339,87 @@ k_umma_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double 
   bool ok = true;
   const int nterm = M2 ? 2 : 1;
   const int kch = (nk + UM_KT - 1) / UM_KT;
-  int nst = 0;
-  for (int term = 0; term < nterm; ++term) {
+  const int nstage = nterm * kch;
+  const int items = (UM_M + nb) * (UM_KT / 8);
+  double pre[UM_ITEMS_MAX][8];
+  auto load_item = [&](int item, int stg, double* x) {
+    const int term = stg / kch;
+    const int k0 = (stg - term * kch) * UM_KT;
     const double* Mm = term ? M2 : M1;
     const double* Xm = term ? X2 : X1;
-    for (int kc0 = 0; kc0 < kch; ++kc0, ++nst) {
-      const int s = nst & 1;
-      if (nst >= 2) {
-        const bool w = mbar_wait(&bars[s], phase[s]);
-        if (!__syncthreads_and(w)) { ok = false; break; }
-        phase[s] ^= 1;
-      }
-      unsigned char* sb = base + s * L.stage_bytes;
-      const int k0 = kc0 * UM_KT;
-      for (int item = tid; item < (UM_M + nb) * (UM_KT / 8); item += UM_THREADS) {
-        const bool isA = item < UM_M * (UM_KT / 8);
-        const int it2 = isA ? item : item - UM_M * (UM_KT / 8);
-        const int rows = isA ? UM_M : nb;
-        const int r = it2 % rows, kc = it2 / rows;
-        double x[8];
-        if (isA) {
-          const long c = c0 + r;
-          const double sc = term ? 1.0 : ((c < kx0_cols) ? a1_kx0 : a1_rest);
+    {
+      const bool isA = item < UM_M * (UM_KT / 8);
+      const int it2 = isA ? item : item - UM_M * (UM_KT / 8);
+      const int rows = isA ? UM_M : nb;
+      const int r = it2 % rows, kc = it2 / rows;
+      if (isA) {
+        const long c = c0 + r;
+        const double sc = term ? 1.0 : ((c < kx0_cols) ? a1_kx0 : a1_rest);
 #pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const int k = k0 + kc * 8 + e;
-            x[e] = (c < ncol && k < nk) ? Xm[(size_t)k * ncol + c] * sc : 0.0;
-          }
-        } else {
-          const int j = j0 + r;
-          const double sc = term ? a2 : 1.0;
-#pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const int k = k0 + kc * 8 + e;
-            x[e] = (j < nj && k < nk) ? Mm[(size_t)k * nj + j] * sc : 0.0;
-          }
+        for (int e = 0; e < 8; ++e) {
+          const int k = k0 + kc * 8 + e;
+          x[e] = (c < ncol && k < nk) ? Xm[(size_t)k * ncol + c] * sc : 0.0;
         }
-        uint4 t[NT];
-        split8<NT>(x, t);
-        const uint32_t off = canon_off(r, kc, rows);
+      } else {
+        const int j = j0 + r;
+        const double sc = term ? a2 : 1.0;
 #pragma unroll
-        for (int q = 0; q < NT; ++q) {
-          unsigned char* dst = sb + (isA ? q * L.a_bytes : NT * L.a_bytes + q * L.b_bytes) + off;
-          *reinterpret_cast<uint4*>(dst) = t[q];
+        for (int e = 0; e < 8; ++e) {
+          const int k = k0 + kc * 8 + e;
+          x[e] = (j < nj && k < nk) ? Mm[(size_t)k * nj + j] * sc : 0.0;
         }
       }
-      fence_async_smem();
-      __syncthreads();
-      if (tid == 0) {
-        tc_fence_after();
-        issue_stage<NT>(tmem, smem_u32(sb), L, nb, idesc, nst == 0);
-        umma_commit(&bars[s]);
-      }
-      __syncthreads();
     }
-    if (!ok) break;
+  };
+  auto store_item = [&](int item, unsigned char* sb, const double* x) {
+    const bool isA = item < UM_M * (UM_KT / 8);
+    const int it2 = isA ? item : item - UM_M * (UM_KT / 8);
+    const int rows = isA ? UM_M : nb;
+    const int r = it2 % rows, kc = it2 / rows;
+    uint4 t[NT];
+    split8<NT>(x, t);
+    const uint32_t off = canon_off(r, kc, rows);
+#pragma unroll
+    for (int qq = 0; qq < NT; ++qq) {
+      unsigned char* dst = sb + (isA ? qq * L.a_bytes : NT * L.a_bytes + qq * L.b_bytes) + off;
+      *reinterpret_cast<uint4*>(dst) = t[qq];
+    }
+  };
+  auto prefetch = [&](int stg) {
+#pragma unroll
+    for (int q = 0; q < UM_ITEMS_MAX; ++q) {
+      const int item = tid + q * UM_THREADS;
+      if (item < items) load_item(item, stg, pre[q]);
+    }
+  };
+  int nst = 0;
+  if (nstage > 0) prefetch(0);
+  for (int stg = 0; stg < nstage; ++stg, ++nst) {
+    const int s = nst & 1;
+    if (nst >= 2) {
+      const bool w = mbar_wait(&bars[s], phase[s]);
+      if (!__syncthreads_and(w)) { ok = false; break; }
+      phase[s] ^= 1;
+    }
+    unsigned char* sb = base + s * L.stage_bytes;
+#pragma unroll
+    for (int q = 0; q < UM_ITEMS_MAX; ++q) {
+      const int item = tid + q * UM_THREADS;
+      if (item < items) store_item(item, sb, pre[q]);
+    }
+    for (int item = tid + UM_ITEMS_MAX * UM_THREADS; item < items; item += UM_THREADS) {
+      double x[8];
+      load_item(item, stg, x);
+      store_item(item, sb, x);
+    }
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      issue_stage<NT>(tmem, smem_u32(sb), L, nb, idesc, nst == 0);
+      umma_commit(&bars[s]);
+    }
+    if (stg + 1 < nstage) prefetch(stg + 1);
   }
   if (ok) {
     for (int d = (nst >= 2 ? nst - 2 : 0); d < nst; ++d) {
@@ -373,9 +430,9 @@ k_umma_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double 
   }
   ok = __syncthreads_and(ok);
   tc_fence_after();
-  const int row = warp * 32 + (tid & 31);
+  const int row = (warp & 3) * 32 + (tid & 31);
   const long c = c0 + row;
-  if (ok) {
+  if (warp < 4 && ok) {
     for (int q0 = 0; q0 < nb; q0 += 16) {
       float v[16];
       tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)q0, v);

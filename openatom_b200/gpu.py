@@ -46,6 +46,15 @@ class SystemDesc(C.Structure):
     ]
 
 
+class CPState(C.Structure):
+    _fields_ = [
+        ("psi_t", _dp), ("psi", _dp), ("vpsi", _dp), ("T", _dp),
+        ("iteration", C.c_int), ("dt", C.c_double), ("ns_tol", C.c_double), ("norb_tol", C.c_double),
+        ("ns_max_iter", C.c_int), ("mixed_nterm", C.c_int), ("use_graph", C.c_int),
+        ("last_ns_iters", C.c_int), ("last_ns_err", C.c_double), ("last_smax", C.c_double),
+    ]
+
+
 # name -> (restype, argtypes); the exported surface of include/oa_gpu.h
 _vp = C.c_void_p
 SIGNATURES = {
@@ -72,6 +81,9 @@ SIGNATURES = {
                                            C.c_int, _vp]),
     "oa_gpu_check": (C.c_int, [_vp, _vp]),
     "oa_gpu_nl_sf": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp]),
+    "oa_gpu_cp_step": (C.c_int, [_vp, _vp, C.POINTER(CPState), _dp]),
+    "oa_gpu_ees_init": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp]),
+    "oa_gpu_nl_ees": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
 }
 
 KERNEL_NAMES = ("state_zfwd", "state_plane_density", "rho_xc", "vks_build", "state_plane_vks",
@@ -299,6 +311,26 @@ class CPContext:
         _check(self._lib.oa_gpu_nl_sf(self._h, self._stream(), _ptr(psi), int(nterm), _ptr(fnl_out),
                                       _ptr(enl_out)))
 
+    def cp_step(self, state: CPState) -> dict:
+        out = (C.c_double * 11)()
+        _check(self._lib.oa_gpu_cp_step(self._h, self._stream(), C.byref(state), out))
+        keys = ("EKE", "EHART", "EEXT", "EWALD_RECIP", "EEXC", "MUXC", "FICT_KE", "ENL", "ORTHO_ITERS",
+                "ORTHO_ERR", "SMAX")
+        return {k: float(v) for k, v in zip(keys, out)}
+
+    def ees_init(self, scale: float = 1.2, order: int = 6):
+        """Enable the EES nonlocal path (grid and dyp from openatom_b200.ees)."""
+        from . import ees
+        grid = ees.nonlocal_grid(self.sys, scale, order)
+        dyp = np.ascontiguousarray(ees.projector_factor(self.sys, grid, order))
+        _check(self._lib.oa_gpu_ees_init(self._h, grid[0], grid[1], grid[2], int(order),
+                                         dyp.view(np.float64).ctypes.data_as(_dp)))
+        self.ees_grid = grid
+        return grid
+
+    def nl_ees(self, psi, fnl_out, enl_out=None):
+        _check(self._lib.oa_gpu_nl_ees(self._h, self._stream(), _ptr(psi), _ptr(fnl_out), _ptr(enl_out)))
+
     def energies(self) -> dict:
         out = (C.c_double * 8)()
         _check(self._lib.oa_gpu_energies(self._h, self._stream(), out))
@@ -333,6 +365,9 @@ class CPDriver:
         self.lam = torch.zeros_like(self.S)
         self.gam = torch.zeros_like(self.S)
         self.tol, self.max_iter = tol, max_iter
+        # native steps run on their own stream (the legacy default stream
+        # cannot be captured into a CUDA graph)
+        self.stream = torch.cuda.Stream()
         # PsiV tolerance (cp_norb_tol, default 0.003; Ortho::maxCheck every step)
         self.norb_tol = norb_tol
         self.n_psiv = 0
@@ -347,6 +382,30 @@ class CPDriver:
         c.vks_build()
         c.nl_sf(self.psi, self.Fnl, nterm=self.nterm_nl)
         c.vks_apply_fft_bwd(self.psi, self.F, fnl=self.Fnl)
+
+    def native_state(self, use_graph: bool = True) -> CPState:
+        """The C-ABI run state pointing at this driver's device buffers."""
+        self.torch.cuda.synchronize()
+        st = CPState()
+        st.psi_t = C.cast(C.c_void_p(self.psi_t.data_ptr()), _dp)
+        st.psi = C.cast(C.c_void_p(self.psi.data_ptr()), _dp)
+        st.vpsi = C.cast(C.c_void_p(self.v.data_ptr()), _dp)
+        st.T = C.cast(C.c_void_p(self.T.data_ptr()), _dp)
+        st.iteration = self.iteration
+        st.dt = self.sys.dt
+        st.ns_tol, st.norb_tol, st.ns_max_iter = self.tol, self.norb_tol, self.max_iter
+        st.mixed_nterm = self.nterm_nl
+        st.use_graph = int(use_graph)
+        return st
+
+    def step_native(self, state: CPState) -> dict:
+        """One CP step through oa_gpu_cp_step (native sequencing, one sync),
+        on the driver's own stream."""
+        with self.torch.cuda.stream(self.stream):
+            en = self.ctx.cp_step(state)
+        self.iteration = state.iteration
+        self.last_ortho = (int(en["ORTHO_ITERS"]), en["ORTHO_ERR"], True)
+        return en
 
     def launches_per_step(self) -> int:
         return self.ctx.sizes()["launches_per_step"]

@@ -317,6 +317,175 @@ def nl_energy_forces(psi, sysm, sf=None):
 
 
 # ----------------------------------------------------------------------------
+# nonlocal pseudopotential, EES (Euler exponential spline) method, l = 0
+# ----------------------------------------------------------------------------
+
+def _smooth235(n):
+    while True:
+        m = n
+        for p in (2, 3, 5):
+            while m % p == 0:
+                m //= p
+        if m == 1:
+            return n
+        n += 1
+
+
+def ees_grid(sysm, scale=1.2, order=6):
+    """Nonlocal EES grid (``init_nonlocal_ees``, ``interface/cp_ewald/set_cp_ewald.C:1329-1410``):
+    n = int(2 scale (kmax+1)), at least 2 (kmax+1), rounded up to an FFT size
+    (here: the next 2^a 3^b 5^c)."""
+    kmax = [int(np.max(np.abs(k))) for k in (sysm.kx, sysm.ky, sysm.kz)]
+    out = []
+    for km in kmax:
+        nk = km + 1
+        n = int(2.0 * scale * nk)
+        if n < 2 * nk:
+            n += 1
+        out.append(_smooth235(n))
+    if min(out) < order:
+        raise ValueError("EES grid smaller than the interpolation order")
+    return tuple(out)
+
+
+def bspline_weight_1d(order, ngrid):
+    """``get_bspline_wght1d`` (``set_cp_ewald.C:1237-1325``): the complex
+    Euler-exponential-spline factor 1/b(m) for m = 0..ngrid-1."""
+    mn = np.zeros(order + 1)
+    uk = np.zeros(order + 1)
+    mn[1] = 1.0
+    uk[1] = 1.0
+    for k in range(2, order + 1):
+        uk[k] = float(k)
+    for n in range(3, order + 1):
+        for k in range(n, 1, -1):
+            mn[k] = (uk[k] * mn[k] + (n - uk[k]) * mn[k - 1]) / (n - 1)
+        mn[1] = uk[1] * mn[1] / (n - 1)
+    m = np.arange(ngrid)
+    k = np.arange(1, order)
+    arg = (2.0 * math.pi / ngrid) * np.outer(m, k - 1)
+    den = (np.cos(arg) * mn[k]).sum(1) + 1j * (np.sin(arg) * mn[k]).sum(1)
+    num = np.exp(1j * (2.0 * math.pi * (order - 1) / ngrid) * m)
+    return num / den
+
+
+def ees_dfactor(sysm, grid, order):
+    """``eesSetEesWghtGgrp`` (``cp_ees_nonlocal.C:60-160``): d(g) = b_a(kx) b_b(ky) b_c(kz),
+    negative k at index k + n; g = 0 keeps the real part."""
+    na, nb, nc = grid
+    ba, bb, bc = (bspline_weight_1d(order, n) for n in grid)
+    d = ba[sysm.kx % na] * bb[sysm.ky % nb] * bc[sysm.kz % nc]
+    g0 = (sysm.kx == 0) & (sysm.ky == 0) & (sysm.kz == 0)
+    d[g0] = (ba[0] * bb[0] * bc[0]).real
+    return d
+
+
+def ees_bsplines(sysm, grid, order):
+    """``eesAtmBsplineRgrp`` (``cp_ees_nonlocal.C:256-593``): for each nonlocal
+    atom the order^3 grid points (ia, ib, ic) and weights M_a M_b M_c of its
+    cardinal B-spline.  Returns (idx [natm_nl, 3, order] int, mn [natm_nl, 3, order])."""
+    nl = sysm.nl_atoms()
+    idx = np.zeros((len(nl), 3, order), dtype=np.int64)
+    mn = np.zeros((len(nl), 3, order))
+    for ia_, a in enumerate(nl):
+        for ax in range(3):
+            ng = grid[ax]
+            t = sysm.pos[a, ax] / sysm.box
+            t -= round(t - 0.5)
+            if t == 1.0:
+                t = 0.0
+            t *= ng
+            it = int(t)
+            frac = t - it
+            u = frac + np.arange(order, dtype=np.float64)          # ua[j], j = 1..order
+            m = np.zeros(order + 1)
+            m[1] = 1.0 - abs(u[0] - 1.0)
+            m[2] = 1.0 - abs(u[1] - 1.0)
+            for n in range(3, order + 1):
+                for j in range(n, 1, -1):
+                    m[j] = (u[j - 1] * m[j] + (n - u[j - 1]) * m[j - 1]) / (n - 1)
+                m[1] = u[0] * m[1] / (n - 1)
+            for j in range(1, order + 1):
+                g = it - (j - 2)
+                g = g if g > 0 else ng + g
+                g = g if g <= ng else g - ng
+                idx[ia_, ax, j - 1] = g - 1
+                mn[ia_, ax, j - 1] = m[j]
+    return idx, mn
+
+
+def ees_setup(sysm, scale=1.2, order=6):
+    grid = ees_grid(sysm, scale, order)
+    return dict(grid=grid, order=order, d=ees_dfactor(sysm, grid, order),
+                bspl=ees_bsplines(sysm, grid, order))
+
+
+def _nl_grid_g_to_r(coef, sysm, grid):
+    """State-convention transform on the nonlocal grid: sum over the full
+    sphere of coef(g) exp(-i g.r) (``doNlFFTGtoR_Gchare``/``_Rchare``,
+    ``fftCache.C:562-700``, same plans and signs as the state transforms)."""
+    full = _full_grid(coef, sysm.kx, sysm.ky, sysm.kz, grid)
+    return _fftn(full, axes=(-3, -2, -1)).real
+
+
+def _nl_grid_r_to_g(fr, sysm, grid):
+    na, nb, nc = grid
+    full = _ifftn(fr, axes=(-3, -2, -1)) * (na * nb * nc)
+    return full[..., sysm.kz % nc, sysm.ky % nb, sysm.kx % na]
+
+
+def nl_ees_energy_forces(psi, sysm, ees):
+    """EES nonlocal energy and coefficient forces, l = 0 channel:
+    ``eesProjGchare`` (``cp_ees_nonlocal.C:594-727``: dyp = d y00 p(|g|),
+    projPsiG = conj(dyp psi)), the nonlocal-grid FFT, ``eesZmatRchare``
+    (1238-1352: zmat = sum projPsiR M over the B-spline stencil),
+    ``eesEnergyAtmForcRchare`` (1480-1720: ENL = occ vnorm/V sum zmat^2,
+    zmat <- 2 vnorm/V occ zmat, scatter zmat M onto the grid), the inverse
+    nonlocal-grid FFT and ``eesPsiForcGspace`` (2000-2079:
+    F -= w conj(dyp P), w = 1 on kx = 0, 2 elsewhere; at g = 0 the
+    imaginary parts of P and dyp are dropped).  Returns (F_nl, per-state ENL, zmat)."""
+    grid, order, d = ees["grid"], ees["order"], ees["d"]
+    idx, mn = ees["bspl"]
+    na, nb, nc = grid
+    nl = sysm.nl_atoms()
+    f = TWO_PI / sysm.box
+    g = f * np.sqrt(sysm.kx.astype(np.float64) ** 2 + sysm.ky ** 2 + sysm.kz ** 2)
+    y00 = 1.0 / math.sqrt(4.0 * math.pi)
+    t = int(sysm.atm_type[nl[0]]) if len(nl) else 0
+    p = sysm.nl_proj.eval(np.full(g.shape, t), np.where(g == 0, 1.0, g))
+    p = np.where(g == 0, sysm.nl_gz0[t], p)
+    dyp = d * y00 * p
+    g0 = g == 0
+    dyp = np.where(g0, dyp.real, dyp)
+    vn = sysm.nl_vnorm[t] / sysm.vol
+    proj = np.conj(dyp[None, :] * psi)
+    pr = _nl_grid_g_to_r(proj, sysm, grid)                     # [nstate, nc, nb, na]
+    # stencil gather: zmat[s, a] = sum_{ja, jb, jc} pr[s, ic, ib, ia] Ma Mb Mc
+    nst = psi.shape[0]
+    zmat = np.zeros((nst, len(nl)))
+    scr = np.zeros_like(pr)
+    w3 = []
+    for a in range(len(nl)):
+        ia, ib, ic = idx[a]
+        ma, mb, mc = mn[a]
+        W = np.einsum("i,j,k->kji", ma, mb, mc)                 # [jc, jb, ja]
+        sub = pr[:, ic][:, :, ib][:, :, :, ia]                   # [s, jc, jb, ja]
+        zmat[:, a] = np.einsum("skji,kji->s", sub, W)
+        w3.append(W)
+    enl = sysm.occ * vn * np.sum(zmat * zmat, axis=1)
+    zs = zmat * (2.0 * vn) * sysm.occ[:, None]
+    for a in range(len(nl)):
+        ia, ib, ic = idx[a]
+        contrib = zs[:, a][:, None, None, None] * w3[a][None]
+        np.add.at(scr, (slice(None), ic[:, None, None], ib[None, :, None], ia[None, None, :]), contrib)
+    P = _nl_grid_r_to_g(scr, sysm, grid)
+    P = np.where(g0[None, :], P.real, P)
+    w = np.where(sysm.kx == 0, 1.0, 2.0)
+    fnl = -w[None, :] * np.conj(dyp[None, :] * P)
+    return fnl, enl, zmat
+
+
+# ----------------------------------------------------------------------------
 # PairCalculator / Ortho
 # ----------------------------------------------------------------------------
 

@@ -176,3 +176,21 @@ def test_nonlocal_structure_factor(case):
     assert rel(f.cpu().numpy(), fr) < 1e-12
     assert rel(enl.cpu().numpy(), er) < 1e-12
     assert abs(ctx.energies()["ENL"] - er.sum()) <= 1e-12 * abs(er.sum())
+
+
+@pytest.mark.parametrize("order,scale", [(6, 1.2), (4, 1.6)])
+def test_nonlocal_ees(case, order, scale):
+    """EES nonlocal path on the GPU against the oracle's EES restatement
+    (FP64: energies 1e-10, forces 1e-9)."""
+    import torch
+    s, ctx, psi = case
+    grid = ctx.ees_init(scale, order)
+    ees = O.ees_setup(s, scale, order)
+    assert tuple(grid) == tuple(ees["grid"])
+    f = torch.zeros_like(psi)
+    enl = torch.zeros(s.nstate, dtype=torch.float64, device="cuda")
+    ctx.nl_ees(psi, f, enl_out=enl)
+    torch.cuda.synchronize()
+    fr, er, _ = O.nl_ees_energy_forces(s.psi, s, ees)
+    assert rel(enl.cpu().numpy(), er) < 1e-10
+    assert rel(f.cpu().numpy(), fr) < 1e-9

@@ -24,3 +24,20 @@ def test_cp_steps_match_oracle(preset, nst, nsteps):
         assert got["ORTHO_ITERS"] == ref["ORTHO_ITERS"]
         psi = drv.psi.cpu().numpy()
         assert np.max(np.abs(psi - st.psi)) / np.max(np.abs(st.psi)) < 1e-9
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_native_step_matches_host_runner(use_graph):
+    """oa_gpu_cp_step (native sequencing, optional CUDA graph) reproduces the
+    host-sequenced step bit for bit in the FP64 form."""
+    from openatom_b200.gpu import CPDriver
+    s = make_system("w8", nstate=16, seed=12, dt=0.5)
+    a = CPDriver(s, "fp64")
+    b = CPDriver(s, "fp64")
+    st = b.native_state(use_graph=use_graph)
+    for _ in range(4):
+        ea = a.step()
+        eb = b.step_native(st)
+        for k in ("EKE", "EHART", "EEXT", "EEXC", "ENL", "FICT_KE"):
+            assert eb[k] == ea[k], (k, ea[k], eb[k])
+        assert np.array_equal(a.psi.cpu().numpy(), b.psi.cpu().numpy())

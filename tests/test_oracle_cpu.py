@@ -124,3 +124,18 @@ def test_nonlocal_force_is_energy_gradient(w2):
     e0 = O.nl_energy_forces(s.psi - d, s)[1].sum()
     pred = -2.0 * np.sum(f.real * d.real + f.imag * d.imag)
     assert abs((e1 - e0) - pred) < 1e-6 * abs(pred)
+
+
+def test_ees_nonlocal_matches_structure_factor():
+    """The EES interpolation (cp_ees_nonlocal.C) converges to the
+    structure-factor result (cp_struct_fact.C / cp_nlmat.C) as the spline
+    order and grid grow: an independent check of the EES conventions."""
+    s = make_system("w4", seed=3)
+    f1, e1, z1 = O.nl_energy_forces(s.psi, s)
+    errs = []
+    for order, scale in ((4, 1.2), (6, 1.2), (8, 2.0)):
+        ees = O.ees_setup(s, scale, order)
+        f2, e2, z2 = O.nl_ees_energy_forces(s.psi, s, ees)
+        errs.append(abs(e2.sum() - e1.sum()) / abs(e1.sum()))
+    assert errs[0] > errs[1] > errs[2]
+    assert errs[2] < 1e-5
