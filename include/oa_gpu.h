@@ -237,6 +237,21 @@ typedef struct {
  * iterations, residual, max|S - 2I|. */
 oa_status oa_gpu_cp_step(oa_ctx *ctx, void *stream, oa_cp_state *state, double *energies_out);
 
+/* Allocation-free PairCalculator forward product, for callers that cannot
+ * call cudaMalloc (code running during CUDA stream capture, or inside a host
+ * framework whose memory pool already holds the device memory).  Same
+ * result as oa_gpu_pc_forward, but it needs no context: the caller passes
+ * the sizes (nstate <= 128, ng g-points, nkx0 points on the kx = 0 plane),
+ * the device inputs left/right [nstate][ng] complex and the device output
+ * C [nstate][nstate].  Its split-K scratch is a fixed 4 MiB device array
+ * held by every GPU that loads the library until the process exits; calls
+ * whose kernels overlap on one GPU race on it (calls on one stream are
+ * ordered).  Larger nstate returns OA_ERR_BAD_ARG.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  No counterpart in the
+ * reference. */
+oa_status oa_gpu_pc_forward_noalloc(void *stream, const double *left, const double *right, int nstate, int ng,
+                                    int nkx0, double alpha, double w_kx0, double *C);
 
 /* Set up the EES nonlocal path (cp_nonloc_ees_opt on): nonlocal grid
  * na x nb x nc (2^a 3^b 5^c, each >= order), B-spline order (even, 4..16),

@@ -84,6 +84,8 @@ SIGNATURES = {
     "oa_gpu_cp_step": (C.c_int, [_vp, _vp, C.POINTER(CPState), _dp]),
     "oa_gpu_ees_init": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp]),
     "oa_gpu_nl_ees": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "oa_gpu_pc_forward_noalloc": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                            _vp]),
 }
 
 KERNEL_NAMES = ("state_zfwd", "state_plane_density", "rho_xc", "vks_build", "state_plane_vks",
