@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#define OA_HD __host__ __device__ __forceinline__
 #define OA_FFT_MAXST 8
 #define OA_FFT_MAXN 512
 
@@ -29,38 +30,38 @@ template <typename R> struct OaCplx;
 template <> struct OaCplx<double> { typedef double2 T; };
 template <> struct OaCplx<float> { typedef float2 T; };
 
-template <typename C> __device__ __forceinline__ C cmk(double x, double y);
-template <> __device__ __forceinline__ double2 cmk<double2>(double x, double y) { return make_double2(x, y); }
-template <> __device__ __forceinline__ float2 cmk<float2>(double x, double y) { return make_float2((float)x, (float)y); }
+template <typename C> OA_HD C cmk(double x, double y);
+template <> OA_HD double2 cmk<double2>(double x, double y) { return make_double2(x, y); }
+template <> OA_HD float2 cmk<float2>(double x, double y) { return make_float2((float)x, (float)y); }
 
-template <typename C> __device__ __forceinline__ C cadd(C a, C b) { a.x += b.x; a.y += b.y; return a; }
-template <typename C> __device__ __forceinline__ C csub(C a, C b) { a.x -= b.x; a.y -= b.y; return a; }
-template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+template <typename C> OA_HD C cadd(C a, C b) { a.x += b.x; a.y += b.y; return a; }
+template <typename C> OA_HD C csub(C a, C b) { a.x -= b.x; a.y -= b.y; return a; }
+template <typename C> OA_HD C cmul(C a, C b) {
   C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
 }
-template <typename C> __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
+template <typename C> OA_HD C cconj(C a) { a.y = -a.y; return a; }
 // multiply by sign*i
-template <int SIGN, typename C> __device__ __forceinline__ C cmul_si(C a) {
+template <int SIGN, typename C> OA_HD C cmul_si(C a) {
   C r;
   if (SIGN < 0) { r.x = a.y; r.y = -a.x; } else { r.x = -a.y; r.y = a.x; }
   return r;
 }
-template <typename C> __device__ __forceinline__ C cscale(C a, decltype(a.x) s) { a.x *= s; a.y *= s; return a; }
+template <typename C> OA_HD C cscale(C a, decltype(a.x) s) { a.x *= s; a.y *= s; return a; }
 
 // ---------------------------------------------------------------------------
 // small DFTs: y_k = sum_r v_r exp(SIGN 2 pi i r k / R)
 // ---------------------------------------------------------------------------
-template <int SIGN, typename C> __device__ __forceinline__ void dft2(C* v) {
+template <int SIGN, typename C> OA_HD void dft2(C* v) {
   C a = v[0], b = v[1];
   v[0] = cadd(a, b); v[1] = csub(a, b);
 }
-template <int SIGN, typename C> __device__ __forceinline__ void dft4(C* v) {
+template <int SIGN, typename C> OA_HD void dft4(C* v) {
   C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
   C t2 = cadd(v[1], v[3]), t3 = cmul_si<SIGN>(csub(v[1], v[3]));
   v[0] = cadd(t0, t2); v[2] = csub(t0, t2);
   v[1] = cadd(t1, t3); v[3] = csub(t1, t3);
 }
-template <int SIGN, typename C> __device__ __forceinline__ void dft3(C* v) {
+template <int SIGN, typename C> OA_HD void dft3(C* v) {
   typedef decltype(v[0].x) R;
   const R c1 = (R)-0.5;
   const R s1 = (R)0.86602540378443864676372317075294;  // sin(2 pi / 3)
@@ -71,7 +72,7 @@ template <int SIGN, typename C> __device__ __forceinline__ void dft3(C* v) {
   v[1] = cadd(m, u);
   v[2] = csub(m, u);
 }
-template <int SIGN, typename C> __device__ __forceinline__ void dft5(C* v) {
+template <int SIGN, typename C> OA_HD void dft5(C* v) {
   typedef decltype(v[0].x) R;
   const R c1 = (R)0.30901699437494742410229341718282;   // cos(2 pi / 5)
   const R c2 = (R)-0.80901699437494742410229341718282;  // cos(4 pi / 5)

@@ -1,0 +1,596 @@
+// Two-pass pencil kernels of the state FFT path, for the grid lengths with a
+// compile-time factorisation N = N1 * N2 (oa_rdft.cuh).  Same work and same
+// results as the runtime-plan kernels in oa_state.cu (which cover every
+// 2-3-5 length), with every pencil transformed as
+//   pass A: DFT_N1 in registers + twiddle -> shared memory
+//   pass B: DFT_N2 in registers -> destination
+// so each pencil makes two shared-memory round trips, all index arithmetic
+// is by constants and the small DFTs have constant twiddles.
+//
+// Reference work replaced (as the oa_state.cu kernels):
+//   FFTcache::expandGSpace + doStpFFTGtoR_Gchare (fftCache.C:460, 1133)     -> k_zfwd2
+//   FFTcache::doStpFFTGtoR_Rchare (fftCache.C:1167) + density part of
+//     CP_State_RealSpacePlane::doFFT/doReduction (:349-363, 450-517)      -> k_plane2<MODE 0>
+//   CP_State_RealSpacePlane::unpackVks (:530-597) + doStpFFTRtoG_Rchare
+//     (fftCache.C:1252-1319)                                              -> k_plane2<MODE 1>
+//   EES eesZmatRchare / eesEnergyAtmForcRchare on the nonlocal grid
+//     (cp_ees_nonlocal.C:1238-1352, 1480-1720)                            -> k_plane2<MODE 2, 3>
+//   CP_State_GSpacePlane::doIFFT (:1581) + packGSpace (fftCache.C:517) +
+//     GStateSlab::addForces (stateSlab.C:239) + CP_eke_calc (cp_eke.C:30)  -> k_zbwd2
+#include "oa_rdft.cuh"
+#include "oa_state_common.cuh"
+
+// shared-memory strides (complex elements) of the pass-A -> pass-B buffer
+// ([k1][n2] per pencil) and of the inverse B' -> A' buffer ([m2][k1])
+template <int N1, int N2> struct PencilLd {
+  static constexpr int ls1 = odd_ld(N2);
+  static constexpr int ps1 = odd_ld(N1 * ls1);
+  static constexpr int ls2 = odd_ld(N1);
+  static constexpr int ps2 = odd_ld(N2 * ls2);
+};
+
+// packed index of z-slot z on a line with nn negative and np non-negative kz
+// (negative kz first, as the reference's run pairs); -1 outside the sphere
+__device__ __forceinline__ int line_slot(int z, int n, int nn, int np) {
+  if (z < np) return nn + z;
+  if (z >= n - nn) return z - (n - nn);
+  return -1;
+}
+
+// ---------------------------------------------------------------------------
+// z pass forward: packed sphere (optionally conj(dyp psi)) -> FFT(-) of the
+// zero-filled z-line -> zbuf[s][z][line].  Block = OA_LB lines of one state.
+// ---------------------------------------------------------------------------
+template <typename R, int N1, int N2>
+__global__ void __launch_bounds__(OA_NTHREADS)
+k_zfwd2(const double2* __restrict__ psi, int ng, int s0, const int* __restrict__ line_off,
+        const int* __restrict__ line_nneg, const int* __restrict__ line_npos, int nlines,
+        typename CplxOf<R>::T* __restrict__ zbuf, int ldl, const double2* __restrict__ twz,
+        const double2* __restrict__ dyp) {
+  typedef typename CplxOf<R>::T C;
+  constexpr int N = N1 * N2;
+  typedef PencilLd<N1, N2> L;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = (C*)smem_raw;
+  C* s1 = tw + align_up(N, 2);
+  const int s = s0 + blockIdx.y;
+  const int l0 = blockIdx.x * OA_LB;
+  const int nb = min(OA_LB, nlines - l0);
+  load_twiddles(tw, twz, N);
+  __syncthreads();
+  const double2* ps = psi + (size_t)s * ng;
+  for (int it = threadIdx.x; it < nb * N2; it += blockDim.x) {
+    const int lb = it / N2, n2 = it - lb * N2;
+    const int l = l0 + lb;
+    const int off = line_off[l], nn = line_nneg[l], np = line_npos[l];
+    C u[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int i = line_slot(N2 * n1 + n2, N, nn, np);
+      double2 v = make_double2(0.0, 0.0);
+      if (i >= 0) {
+        v = ps[off + i];
+        if (dyp) {  // EES projector: projPsiG = conj(dyp psi) (eesProjGchare)
+          const double2 d = dyp[off + i];
+          v = make_double2(d.x * v.x - d.y * v.y, -(d.y * v.x + d.x * v.y));
+        }
+      }
+      u[n1] = cmk<C>(v.x, v.y);
+    }
+    pass_a<N1, N2, -1>(u, n2, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) s1[lb * L::ps1 + k1 * L::ls1 + n2] = u[k1];
+  }
+  __syncthreads();
+  C* out = zbuf + (size_t)s * N * ldl + l0;
+  for (int it = threadIdx.x; it < N1 * OA_LB; it += blockDim.x) {
+    const int k1 = it / OA_LB, lb = it - k1 * OA_LB;
+    if (lb >= nb) continue;
+    C w[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) w[n2] = s1[lb * L::ps1 + k1 * L::ls1 + n2];
+    RDft<N2, -1>::run(w);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) out[(size_t)(k1 + N1 * k2) * ldl + lb] = w[k2];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z pass backward: zbuf -> FFT(+) -> pack; F = scale w v (+ F_NL), then
+// CP_eke_calc: F -= occ w g2 psi (g2 <= ecut, else F = 0), EKE partials.
+// With dyp (EES): F = -w conj(dyp P) instead (eesPsiForcGspace).
+// ---------------------------------------------------------------------------
+template <typename R, int N1, int N2>
+__global__ void __launch_bounds__(OA_NTHREADS)
+k_zbwd2(const typename CplxOf<R>::T* __restrict__ zbuf, int ldl, int nlines, const int* __restrict__ line_kx,
+        const int* __restrict__ line_off, const int* __restrict__ line_nneg, const int* __restrict__ line_npos,
+        const double2* __restrict__ twz, const double2* __restrict__ psi, const double2* __restrict__ fnl,
+        double2* __restrict__ force, const double* __restrict__ g2, const double* __restrict__ occ, int ng, int s0,
+        double scale, double ecut, double* __restrict__ eke_part, int nblk, const double2* __restrict__ dyp) {
+  typedef typename CplxOf<R>::T C;
+  constexpr int N = N1 * N2;
+  typedef PencilLd<N1, N2> L;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = (C*)smem_raw;
+  C* s1 = tw + align_up(N, 2);
+  double* sred = (double*)(s1 + align_up((size_t)OA_LB * L::ps1, 2));
+  const int s = s0 + blockIdx.y;
+  const int l0 = blockIdx.x * OA_LB;
+  const int nb = min(OA_LB, nlines - l0);
+  load_twiddles(tw, twz, N);
+  __syncthreads();
+  const C* in = zbuf + (size_t)s * N * ldl + l0;
+  for (int it = threadIdx.x; it < N2 * OA_LB; it += blockDim.x) {
+    const int n2 = it / OA_LB, lb = it - n2 * OA_LB;
+    if (lb >= nb) continue;
+    C u[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) u[n1] = in[(size_t)(N2 * n1 + n2) * ldl + lb];
+    pass_a<N1, N2, +1>(u, n2, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) s1[lb * L::ps1 + k1 * L::ls1 + n2] = u[k1];
+  }
+  __syncthreads();
+  const double2* ps = psi + (size_t)s * ng;
+  double2* fs = force + (size_t)s * ng;
+  const double2* fn = fnl ? fnl + (size_t)s * ng : nullptr;
+  const double o = occ[s];
+  double ek = 0.0;
+  for (int it = threadIdx.x; it < nb * N1; it += blockDim.x) {
+    const int lb = it / N1, k1 = it - lb * N1;
+    const int l = l0 + lb;
+    const int off = line_off[l], nn = line_nneg[l], np = line_npos[l];
+    const double w = (line_kx[l] == 0) ? 1.0 : 2.0;
+    const double sc = scale * w;
+    const double wt = o * w;
+    C v[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) v[n2] = s1[lb * L::ps1 + k1 * L::ls1 + n2];
+    RDft<N2, +1>::run(v);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+      const int i = line_slot(k1 + N1 * k2, N, nn, np);
+      if (i < 0) continue;
+      const int idx = off + i;
+      if (dyp) {
+        const double2 d = dyp[idx];
+        const double px = (double)v[k2].x;
+        const double py = (g2[idx] == 0.0) ? 0.0 : (double)v[k2].y;
+        fs[idx] = make_double2(-w * (d.x * px - d.y * py), w * (d.y * px + d.x * py));
+        continue;
+      }
+      double2 f = make_double2((double)v[k2].x * sc, (double)v[k2].y * sc);
+      if (fn) { const double2 q = fn[idx]; f.x += q.x; f.y += q.y; }
+      const double gg = g2[idx];
+      if (gg <= ecut) {
+        const double2 p = ps[idx];
+        const double t = wt * gg;
+        f.x -= p.x * t; f.y -= p.y * t;
+        ek += t * (p.x * p.x + p.y * p.y);
+      } else {
+        f.x = 0.0; f.y = 0.0;
+      }
+      fs[idx] = f;
+    }
+  }
+  const double tot = block_sum(ek, sred);
+  if (threadIdx.x == 0) eke_part[(size_t)s * nblk + blockIdx.x] = tot;
+}
+
+// ---------------------------------------------------------------------------
+// plane pass, nx = ny = N, for one z-plane and one group of states.
+//   MODE 0: zbuf row -> P[kx][y] -> y FFT(-) -> x FFT(-) of row pairs
+//           (two-for-one c2r) -> tile += occ psi(r)^2
+//   MODE 1: ... x FFT(-) -> psi(r) V_KS occ -> x FFT(+) -> r2c unpack -> y FFT(+)
+//           -> zbuf row (in place)
+//   MODE 2: as MODE 0 but tile = psi(r) (nonlocal grid), then the EES Z gather
+//   MODE 3: EES scatter -> tile -> x FFT(+) -> r2c unpack -> y FFT(+) -> zbuf row
+// Pencils (y columns, x row pairs) go through in chunks of G; the block
+// synchronises between the passes.  In MODE 1 the forward DFT_N2, the V_KS
+// product and the backward DFT_N2 of an x pencil run back to back in the
+// registers of one thread (pass B, then pass B' of the inverse).
+// ---------------------------------------------------------------------------
+struct Plane2Smem {
+  size_t tw, P, tile, s1, s2, total;
+  int G;
+};
+
+template <typename R, int MODE, int N1, int N2>
+__global__ void __launch_bounds__(OA_PLANE_THREADS)
+k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlines,
+         const int* __restrict__ line_kx, const int* __restrict__ line_ky, int nkx,
+         const double2* __restrict__ twg, const double* __restrict__ occ, const R* __restrict__ vks,
+         double* __restrict__ rho_part, int ngroup, Plane2Smem L, EesArgs E) {
+  typedef typename CplxOf<R>::T C;
+  constexpr int N = N1 * N2;
+  constexpr int LDY = N + 1;
+  typedef PencilLd<N1, N2> LD;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = (C*)(smem_raw + L.tw);
+  C* P = (C*)(smem_raw + L.P);
+  R* tile = (R*)(smem_raw + L.tile);
+  C* s1 = (C*)(smem_raw + L.s1);
+  C* s2 = (C*)(smem_raw + L.s2);
+  const int G = L.G;
+  const int z = blockIdx.x, g = blockIdx.y;
+  const int nper = (nstate + ngroup - 1) / ngroup;
+  const int sb = g * nper, se = min(nstate, sb + nper);
+  constexpr int npairs = (N + 1) / 2;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  load_twiddles(tw, twg, N);
+  if (MODE == 0) {
+    for (int i = threadIdx.x; i < N * N; i += blockDim.x) tile[i] = (R)0;
+  } else if (MODE == 1) {
+    const R* vz = vks + (size_t)z * N * N;
+    for (int i = threadIdx.x; i < N * N; i += blockDim.x) tile[i] = vz[i];
+  }
+  __syncthreads();
+  for (int s = sb; s < se; ++s) {
+    C* row = zbuf + ((size_t)s * N + z) * ldl;
+    if (MODE == 3) {
+      for (int i = threadIdx.x; i < N * N; i += blockDim.x) tile[i] = (R)0;
+      __syncthreads();
+      ees_scatter_plane(tile, N, z, s, E, warp, lane, OA_PLANE_WARPS);
+      __syncthreads();
+    } else {
+      for (int i = threadIdx.x; i < nkx * LDY; i += blockDim.x) P[i] = cmk<C>(0.0, 0.0);
+      __syncthreads();
+      for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
+        int ky = line_ky[l]; if (ky < 0) ky += N;
+        P[line_kx[l] * LDY + ky] = row[l];
+      }
+      __syncthreads();
+      // y FFT(-) over the occupied kx columns, in place in P
+      for (int c0 = 0; c0 < nkx; c0 += G) {
+        const int gc = min(G, nkx - c0);
+        for (int it = threadIdx.x; it < gc * N2; it += blockDim.x) {
+          const int cc = it / N2, n2 = it - cc * N2;
+          const C* col = P + (c0 + cc) * LDY;
+          C u[N1];
+#pragma unroll
+          for (int n1 = 0; n1 < N1; ++n1) u[n1] = col[N2 * n1 + n2];
+          pass_a<N1, N2, -1>(u, n2, tw);
+#pragma unroll
+          for (int k1 = 0; k1 < N1; ++k1) s1[cc * LD::ps1 + k1 * LD::ls1 + n2] = u[k1];
+        }
+        __syncthreads();
+        for (int it = threadIdx.x; it < gc * N1; it += blockDim.x) {
+          const int cc = it / N1, k1 = it - cc * N1;
+          C* col = P + (c0 + cc) * LDY;
+          C w[N2];
+#pragma unroll
+          for (int n2 = 0; n2 < N2; ++n2) w[n2] = s1[cc * LD::ps1 + k1 * LD::ls1 + n2];
+          RDft<N2, -1>::run(w);
+#pragma unroll
+          for (int k2 = 0; k2 < N2; ++k2) col[k1 + N1 * k2] = w[k2];
+        }
+        __syncthreads();
+      }
+    }
+    const R o = (R)occ[s];
+    // x pencils: row pairs (y1, y2) as one complex sequence
+    for (int p0 = 0; p0 < npairs; p0 += G) {
+      const int gp = min(G, npairs - p0);
+      constexpr int SA = (MODE == 3) ? +1 : -1;
+      for (int it = threadIdx.x; it < gp * N2; it += blockDim.x) {
+        const int pp = it / N2, n2 = it - pp * N2;
+        const int y1 = 2 * (p0 + pp), y2 = y1 + 1;
+        C u[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) {
+          const int k = N2 * n1 + n2;
+          C zz;
+          if (MODE == 3) {
+            zz.x = tile[y1 * N + k];
+            zz.y = (y2 < N) ? tile[y2 * N + k] : (R)0;
+          } else {
+            const C a = herm_x(P, LDY, nkx, N, k, y1);
+            C b = cmk<C>(0.0, 0.0);
+            if (y2 < N) b = herm_x(P, LDY, nkx, N, k, y2);
+            zz.x = a.x - b.y;
+            zz.y = a.y + b.x;
+          }
+          u[n1] = zz;
+        }
+        pass_a<N1, N2, SA>(u, n2, tw);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) s1[pp * LD::ps1 + k1 * LD::ls1 + n2] = u[k1];
+      }
+      __syncthreads();
+      for (int it = threadIdx.x; it < gp * N1; it += blockDim.x) {
+        const int pp = it / N1, k1 = it - pp * N1;
+        const int y1 = 2 * (p0 + pp), y2 = y1 + 1;
+        C w[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) w[n2] = s1[pp * LD::ps1 + k1 * LD::ls1 + n2];
+        RDft<N2, SA>::run(w);
+        if (MODE == 0) {
+#pragma unroll
+          for (int k2 = 0; k2 < N2; ++k2) {
+            const int x = k1 + N1 * k2;
+            tile[y1 * N + x] += o * w[k2].x * w[k2].x;
+            if (y2 < N) tile[y2 * N + x] += o * w[k2].y * w[k2].y;
+          }
+        } else if (MODE == 2) {
+#pragma unroll
+          for (int k2 = 0; k2 < N2; ++k2) {
+            const int x = k1 + N1 * k2;
+            tile[y1 * N + x] = w[k2].x;
+            if (y2 < N) tile[y2 * N + x] = w[k2].y;
+          }
+        } else if (MODE == 3) {
+#pragma unroll
+          for (int k2 = 0; k2 < N2; ++k2) s2[pp * LD::ps2 + k1 + N1 * k2] = w[k2];
+        } else {
+#pragma unroll
+          for (int k2 = 0; k2 < N2; ++k2) {
+            const int x = k1 + N1 * k2;
+            w[k2].x *= tile[y1 * N + x] * o;
+            w[k2].y = (y2 < N) ? w[k2].y * tile[y2 * N + x] * o : (R)0;
+          }
+          // inverse, first half: DFT_N2(+) over k2, twiddle exp(+2 pi i k1 m2 / N)
+          RDft<N2, +1>::run(w);
+#pragma unroll
+          for (int m2 = 0; m2 < N2; ++m2) {
+            const C t = (m2 == 0) ? w[m2] : cmul(w[m2], tw_rt<+1>(tw, k1 * m2));
+            s2[pp * LD::ps2 + m2 * LD::ls2 + k1] = t;
+          }
+        }
+      }
+      __syncthreads();
+      if (MODE == 1) {
+        // inverse, second half: DFT_N1(+) over k1 -> natural order in s1
+        for (int it = threadIdx.x; it < gp * N2; it += blockDim.x) {
+          const int pp = it / N2, m2 = it - pp * N2;
+          C u[N1];
+#pragma unroll
+          for (int k1 = 0; k1 < N1; ++k1) u[k1] = s2[pp * LD::ps2 + m2 * LD::ls2 + k1];
+          RDft<N1, +1>::run(u);
+#pragma unroll
+          for (int m1 = 0; m1 < N1; ++m1) s1[pp * LD::ps1 + m2 + N2 * m1] = u[m1];
+        }
+        __syncthreads();
+      }
+      if (MODE == 1 || MODE == 3) {
+        // two-for-one r2c unpack of the natural-order result into P[kx][y]
+        const C* nat = (MODE == 1) ? s1 : s2;
+        const int pst = (MODE == 1) ? LD::ps1 : LD::ps2;
+        for (int it = threadIdx.x; it < gp * nkx; it += blockDim.x) {
+          const int pp = it / nkx, k = it - pp * nkx;
+          const int y1 = 2 * (p0 + pp), y2 = y1 + 1;
+          const C a = nat[pp * pst + k];
+          const C b = cconj(nat[pp * pst + (k == 0 ? 0 : N - k)]);
+          C f1, f2;
+          f1.x = (a.x + b.x) * (R)0.5; f1.y = (a.y + b.y) * (R)0.5;
+          f2.x = (a.y - b.y) * (R)0.5; f2.y = -(a.x - b.x) * (R)0.5;
+          P[k * LDY + y1] = f1;
+          if (y2 < N) P[k * LDY + y2] = f2;
+        }
+        __syncthreads();
+      }
+    }
+    if (MODE == 2) {
+      ees_gather_plane(tile, N, z, s, E, warp, lane, OA_PLANE_WARPS);
+      __syncthreads();
+    }
+    if (MODE == 1 || MODE == 3) {
+      // y FFT(+) over the kx columns, in place in P
+      for (int c0 = 0; c0 < nkx; c0 += G) {
+        const int gc = min(G, nkx - c0);
+        for (int it = threadIdx.x; it < gc * N2; it += blockDim.x) {
+          const int cc = it / N2, n2 = it - cc * N2;
+          const C* col = P + (c0 + cc) * LDY;
+          C u[N1];
+#pragma unroll
+          for (int n1 = 0; n1 < N1; ++n1) u[n1] = col[N2 * n1 + n2];
+          pass_a<N1, N2, +1>(u, n2, tw);
+#pragma unroll
+          for (int k1 = 0; k1 < N1; ++k1) s1[cc * LD::ps1 + k1 * LD::ls1 + n2] = u[k1];
+        }
+        __syncthreads();
+        for (int it = threadIdx.x; it < gc * N1; it += blockDim.x) {
+          const int cc = it / N1, k1 = it - cc * N1;
+          C* col = P + (c0 + cc) * LDY;
+          C w[N2];
+#pragma unroll
+          for (int n2 = 0; n2 < N2; ++n2) w[n2] = s1[cc * LD::ps1 + k1 * LD::ls1 + n2];
+          RDft<N2, +1>::run(w);
+#pragma unroll
+          for (int k2 = 0; k2 < N2; ++k2) col[k1 + N1 * k2] = w[k2];
+        }
+        __syncthreads();
+      }
+      for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
+        int ky = line_ky[l]; if (ky < 0) ky += N;
+        row[l] = P[line_kx[l] * LDY + ky];
+      }
+      __syncthreads();
+    }
+  }
+  if (MODE == 0) {
+    double* out = rho_part + ((size_t)g * gridDim.x + z) * (size_t)N * N;
+    for (int i = threadIdx.x; i < N * N; i += blockDim.x) out[i] = (double)tile[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+template <typename C, typename R, int N1, int N2>
+static Plane2Smem plane2_layout(int nkx, bool need_s2) {
+  constexpr int N = N1 * N2;
+  typedef PencilLd<N1, N2> LD;
+  Plane2Smem L;
+  size_t o = 0;
+  L.tw = o; o += align_up(N * sizeof(C), 16);
+  L.P = o; o += align_up((size_t)nkx * (N + 1) * sizeof(C), 16);
+  L.tile = o; o += align_up((size_t)N * N * sizeof(R), 16);
+  const size_t fixed = o;
+  const size_t per = (LD::ps1 + (need_s2 ? LD::ps2 : 0)) * sizeof(C);
+  const int want = nkx > (N + 1) / 2 ? nkx : (N + 1) / 2;
+  long g = fixed + 2 * 16 < (size_t)OA_MAX_SMEM ? (long)(((size_t)OA_MAX_SMEM - fixed - 2 * 16) / per) : 0;
+  if (g > want) g = want;
+  L.G = (int)g;
+  L.s1 = o; o += align_up((size_t)L.G * LD::ps1 * sizeof(C), 16);
+  L.s2 = o; o += need_s2 ? align_up((size_t)L.G * LD::ps2 * sizeof(C), 16) : 0;
+  L.total = o;
+  return L;
+}
+
+template <int N> struct SplitOf { static constexpr int n1 = Split<N>::n1, n2 = Split<N>::n2; };
+
+#define OA_PENCIL_LENGTHS(X) X(12) X(20) X(24) X(36) X(40) X(64) X(96) X(108) X(160)
+
+int oa_pencil_supported(int n) {
+#define OA_PS_CASE(NN) if (n == NN) return 1;
+  OA_PENCIL_LENGTHS(OA_PS_CASE)
+#undef OA_PS_CASE
+  return 0;
+}
+
+#define OA_PENCIL_DISPATCH(n, CALL)                                  \
+  switch (n) {                                                       \
+    case 12: return CALL(4, 3);                                      \
+    case 20: return CALL(4, 5);                                      \
+    case 24: return CALL(6, 4);                                      \
+    case 36: return CALL(6, 6);                                      \
+    case 40: return CALL(8, 5);                                      \
+    case 64: return CALL(8, 8);                                      \
+    case 96: return CALL(12, 8);                                     \
+    case 108: return CALL(12, 9);                                    \
+    case 160: return CALL(16, 10);                                   \
+    default: break;                                                  \
+  }
+
+template <typename R, int N1, int N2>
+static size_t zpass2_smem() {
+  typedef typename CplxOf<R>::T C;
+  return (align_up(N1 * N2, 2) + align_up((size_t)OA_LB * PencilLd<N1, N2>::ps1, 2)) * sizeof(C) +
+         64 * sizeof(double);
+}
+
+template <typename R, int N1, int N2>
+static cudaError_t zfwd2_n(cudaStream_t st, const double2* psi, int ng, int s0, int ns, const int* off,
+                           const int* nneg, const int* npos, int nlines, void* zbuf, int ldl, const double2* tw,
+                           const double2* dyp) {
+  typedef typename CplxOf<R>::T C;
+  const size_t sm = zpass2_smem<R, N1, N2>();
+  cudaError_t e = cudaFuncSetAttribute(k_zfwd2<R, N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  dim3 grid((nlines + OA_LB - 1) / OA_LB, ns);
+  k_zfwd2<R, N1, N2><<<grid, OA_NTHREADS, sm, st>>>(psi, ng, s0, off, nneg, npos, nlines, (C*)zbuf, ldl, tw, dyp);
+  return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t zfwd2(cudaStream_t st, int n, const double2* psi, int ng, int s0, int ns, const int* off,
+                         const int* nneg, const int* npos, int nlines, void* zbuf, int ldl, const double2* tw,
+                         const double2* dyp) {
+#define OA_CALL(A, B) zfwd2_n<R, A, B>(st, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp)
+  OA_PENCIL_DISPATCH(n, OA_CALL)
+#undef OA_CALL
+  return cudaErrorNotSupported;
+}
+
+cudaError_t oa_pencil_zfwd(int precision, cudaStream_t st, int n, const double2* psi, int ng, int s0, int ns,
+                           const int* off, const int* nneg, const int* npos, int nlines, void* zbuf, int ldl,
+                           const double2* tw, const double2* dyp) {
+  return precision == OA_FP64 ? zfwd2<double>(st, n, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp)
+                              : zfwd2<float>(st, n, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp);
+}
+
+template <typename R, int N1, int N2>
+static cudaError_t zbwd2_n(cudaStream_t st, const void* zbuf, int ldl, int nlines, const int* lkx, const int* off,
+                           const int* nneg, const int* npos, const double2* tw, const double2* psi,
+                           const double2* fnl, double2* force, const double* g2, const double* occ, int ng, int s0,
+                           int ns, double scale, double ecut, double* eke_part, int nblk, const double2* dyp) {
+  typedef typename CplxOf<R>::T C;
+  const size_t sm = zpass2_smem<R, N1, N2>();
+  cudaError_t e = cudaFuncSetAttribute(k_zbwd2<R, N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  dim3 grid(nblk, ns);
+  k_zbwd2<R, N1, N2><<<grid, OA_NTHREADS, sm, st>>>((const C*)zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl,
+                                                     force, g2, occ, ng, s0, scale, ecut, eke_part, nblk, dyp);
+  return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t zbwd2(cudaStream_t st, int n, const void* zbuf, int ldl, int nlines, const int* lkx,
+                         const int* off, const int* nneg, const int* npos, const double2* tw, const double2* psi,
+                         const double2* fnl, double2* force, const double* g2, const double* occ, int ng, int s0,
+                         int ns, double scale, double ecut, double* eke_part, int nblk, const double2* dyp) {
+#define OA_CALL(A, B)                                                                                          \
+  zbwd2_n<R, A, B>(st, zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl, force, g2, occ, ng, s0, ns, scale, \
+                   ecut, eke_part, nblk, dyp)
+  OA_PENCIL_DISPATCH(n, OA_CALL)
+#undef OA_CALL
+  return cudaErrorNotSupported;
+}
+
+cudaError_t oa_pencil_zbwd(int precision, cudaStream_t st, int n, const void* zbuf, int ldl, int nlines,
+                           const int* lkx, const int* off, const int* nneg, const int* npos, const double2* tw,
+                           const double2* psi, const double2* fnl, double2* force, const double* g2,
+                           const double* occ, int ng, int s0, int ns, double scale, double ecut, double* eke_part,
+                           int nblk, const double2* dyp) {
+  return precision == OA_FP64
+             ? zbwd2<double>(st, n, zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl, force, g2, occ, ng, s0,
+                             ns, scale, ecut, eke_part, nblk, dyp)
+             : zbwd2<float>(st, n, zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl, force, g2, occ, ng, s0, ns,
+                            scale, ecut, eke_part, nblk, dyp);
+}
+
+template <typename R, int MODE, int N1, int N2>
+static cudaError_t plane2_n(cudaStream_t st, void* zbuf, int nstate, int ldl, int nlines, const int* lkx,
+                            const int* lky, int nz, int nkx, const double2* tw, const double* occ, const void* vks,
+                            double* rho_part, int ngroup, const EesArgs& E) {
+  typedef typename CplxOf<R>::T C;
+  const Plane2Smem L = plane2_layout<C, R, N1, N2>(nkx, MODE == 1 || MODE == 3);
+  if (L.G < 1 || L.total > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
+  cudaError_t e =
+      cudaFuncSetAttribute(k_plane2<R, MODE, N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+  if (e != cudaSuccess) return e;
+  dim3 grid(nz, ngroup);
+  k_plane2<R, MODE, N1, N2><<<grid, OA_PLANE_THREADS, L.total, st>>>((C*)zbuf, nstate, ldl, nlines, lkx, lky, nkx,
+                                                                     tw, occ, (const R*)vks, rho_part, ngroup, L, E);
+  return cudaGetLastError();
+}
+
+template <typename R, int MODE>
+static cudaError_t plane2(cudaStream_t st, int n, void* zbuf, int nstate, int ldl, int nlines, const int* lkx,
+                          const int* lky, int nz, int nkx, const double2* tw, const double* occ, const void* vks,
+                          double* rho_part, int ngroup, const EesArgs& E) {
+#define OA_CALL(A, B) \
+  plane2_n<R, MODE, A, B>(st, zbuf, nstate, ldl, nlines, lkx, lky, nz, nkx, tw, occ, vks, rho_part, ngroup, E)
+  OA_PENCIL_DISPATCH(n, OA_CALL)
+#undef OA_CALL
+  return cudaErrorNotSupported;
+}
+
+// nx = ny = n; returns cudaErrorNotSupported when n has no two-pass kernel
+// or its shared memory does not fit (the caller then uses the runtime-plan
+// kernel)
+cudaError_t oa_pencil_plane(int precision, int mode, cudaStream_t st, int n, void* zbuf, int nstate, int ldl,
+                            int nlines, const int* lkx, const int* lky, int nz, int nkx, const double2* tw,
+                            const double* occ, const void* vks, double* rho_part, int ngroup, const EesArgs& E) {
+#define OA_MODE(M)                                                                                              \
+  if (mode == M)                                                                                                \
+    return precision == OA_FP64                                                                                 \
+               ? plane2<double, M>(st, n, zbuf, nstate, ldl, nlines, lkx, lky, nz, nkx, tw, occ, vks, rho_part, \
+                                   ngroup, E)                                                                   \
+               : plane2<float, M>(st, n, zbuf, nstate, ldl, nlines, lkx, lky, nz, nkx, tw, occ, vks, rho_part,  \
+                                  ngroup, E);
+  OA_MODE(0) OA_MODE(1) OA_MODE(2) OA_MODE(3)
+#undef OA_MODE
+  return cudaErrorNotSupported;
+}
+
+// shared memory of the two-pass plane kernel (MODE 1 layout, the largest);
+// 0 when there is none for this length
+size_t oa_pencil_plane_smem(int precision, int n, int nkx) {
+#define OA_CALL(A, B)                                                                  \
+  (precision == OA_FP64 ? plane2_layout<double2, double, A, B>(nkx, true).total        \
+                        : plane2_layout<float2, float, A, B>(nkx, true).total)
+  OA_PENCIL_DISPATCH(n, OA_CALL)
+#undef OA_CALL
+  return 0;
+}

@@ -18,30 +18,7 @@
 // lines padded to ldl so each (state, z) row is one contiguous, aligned run.
 #include "oa_internal.h"
 
-template <typename R> struct CplxOf { typedef typename OaCplx<R>::T T; };
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// Deterministic block sum; result valid in thread 0.  Uses 32 doubles of smem.
-__device__ double block_sum(double v, double* sh) {
-  v = warp_sum(v);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  __syncthreads();
-  if (lane == 0) sh[wid] = v;
-  __syncthreads();
-  double r = 0.0;
-  if (wid == 0) {
-    r = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.0;
-    r = warp_sum(r);
-  }
-  return r;
-}
-
-__host__ __device__ static inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+#include "oa_state_common.cuh"
 
 // ---------------------------------------------------------------------------
 // z pass, forward: packed sphere -> zero-filled z-lines -> FFT(-) -> zbuf[s][z][l]
@@ -94,34 +71,6 @@ k_state_zfwd(const double2* __restrict__ psi, int ng, int s0,
 // ---------------------------------------------------------------------------
 // plane helpers
 // ---------------------------------------------------------------------------
-template <typename C>
-__device__ __forceinline__ C herm_x(const C* P, int ldy, int nkx, int nx, int k, int y) {
-  // value of the x-spectrum at index k of row y from the stored kx in [0, nkx)
-  // (kx < 0 from Hermitian symmetry); DC / Nyquist use the real part only,
-  // as a c2r transform does.
-  C v = cmk<C>(0.0, 0.0);
-  if (k <= nx / 2) {
-    if (k < nkx) v = P[k * ldy + y];
-    if (k == 0 || 2 * k == nx) v.y = 0;
-  } else {
-    const int kk = nx - k;
-    if (kk < nkx) v = cconj(P[kk * ldy + y]);
-  }
-  return v;
-}
-
-#define OA_PLANE_THREADS 512
-#define OA_PLANE_WARPS (OA_PLANE_THREADS / 32)
-
-// EES stencil data for the nonlocal-grid plane modes
-struct EesArgs {
-  const int* idx;       // [natm][3][order] grid index per axis (a, b, c)
-  const double* mn;     // [natm][3][order] B-spline weight per axis
-  double* zpart;        // [nstate][natm][order] MODE 2: per-plane Z contributions
-  const double* zs;     // [nstate][natm]        MODE 3: scaled Z to scatter
-  int natm, order;
-};
-
 struct PlaneSmem {
   size_t tw_x, tw_y, P, tile, wbuf, total;
   int ldw;  // per-warp buffer length (complex elements)
@@ -402,6 +351,22 @@ static size_t zpass_smem(int nz) {
   return (align_up(nz, 2) + 2 * (size_t)OA_LB * (nz + 1)) * sizeof(C) + 64 * sizeof(double);
 }
 
+// two-pass kernels (oa_pencil.cu) for the lengths with a compile-time
+// factorisation; they return cudaErrorNotSupported otherwise
+int oa_pencil_supported(int n);
+size_t oa_pencil_plane_smem(int precision, int n, int nkx);
+cudaError_t oa_pencil_zfwd(int precision, cudaStream_t st, int n, const double2* psi, int ng, int s0, int ns,
+                           const int* off, const int* nneg, const int* npos, int nlines, void* zbuf, int ldl,
+                           const double2* tw, const double2* dyp);
+cudaError_t oa_pencil_zbwd(int precision, cudaStream_t st, int n, const void* zbuf, int ldl, int nlines,
+                           const int* lkx, const int* off, const int* nneg, const int* npos, const double2* tw,
+                           const double2* psi, const double2* fnl, double2* force, const double* g2,
+                           const double* occ, int ng, int s0, int ns, double scale, double ecut, double* eke_part,
+                           int nblk, const double2* dyp);
+cudaError_t oa_pencil_plane(int precision, int mode, cudaStream_t st, int n, void* zbuf, int nstate, int ldl,
+                            int nlines, const int* lkx, const int* lky, int nz, int nkx, const double2* tw,
+                            const double* occ, const void* vks, double* rho_part, int ngroup, const EesArgs& E);
+
 template <typename R>
 static cudaError_t launch_zfwd(oa_ctx* c, cudaStream_t st, const double2* psi, int s0, int ns) {
   typedef typename CplxOf<R>::T C;
@@ -444,6 +409,10 @@ static cudaError_t launch_zbwd(oa_ctx* c, cudaStream_t st, const double2* psi, c
 }
 
 size_t oa_plane_smem_bytes(int precision, int nx, int ny, int nkx) {
+  if (nx == ny && oa_pencil_supported(nx)) {
+    const size_t p = oa_pencil_plane_smem(precision, nx, nkx);
+    if (p > 0 && p <= (size_t)OA_MAX_SMEM) return p;
+  }
   if (precision == OA_FP64) return plane_smem_layout<double2, double>(nx, ny, nkx).total;
   return plane_smem_layout<float2, float>(nx, ny, nkx).total;
 }
@@ -456,16 +425,34 @@ int oa_plane_blocks_per_sm(int precision) {
 }
 
 cudaError_t oa_launch_state_zfwd(oa_ctx* c, cudaStream_t s, const double2* psi, int s0, int ns) {
+  if (oa_pencil_supported(c->nz))
+    return oa_pencil_zfwd(c->precision, s, c->nz, psi, c->ng, s0, ns, c->line_off, c->line_nneg, c->line_npos,
+                          c->nlines, c->zbuf, c->ldl, c->tw_z, nullptr);
   return c->precision == OA_FP64 ? launch_zfwd<double>(c, s, psi, s0, ns) : launch_zfwd<float>(c, s, psi, s0, ns);
 }
+static cudaError_t pencil_plane(oa_ctx* c, cudaStream_t s, int mode) {
+  if (c->nx != c->ny || !oa_pencil_supported(c->nx)) return cudaErrorNotSupported;
+  const EesArgs E = {nullptr, nullptr, nullptr, nullptr, 0, 0};
+  return oa_pencil_plane(c->precision, mode, s, c->nx, c->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx,
+                         c->line_ky, c->nz, c->nkx_s, c->tw_x, c->occ, c->vks, c->rho_part, c->ngroup, E);
+}
+
 cudaError_t oa_launch_state_plane_density(oa_ctx* c, cudaStream_t s) {
+  const cudaError_t e = pencil_plane(c, s, 0);
+  if (e != cudaErrorNotSupported) return e;
   return c->precision == OA_FP64 ? launch_plane<double, 0>(c, s) : launch_plane<float, 0>(c, s);
 }
 cudaError_t oa_launch_state_plane_vks(oa_ctx* c, cudaStream_t s) {
+  const cudaError_t e = pencil_plane(c, s, 1);
+  if (e != cudaErrorNotSupported) return e;
   return c->precision == OA_FP64 ? launch_plane<double, 1>(c, s) : launch_plane<float, 1>(c, s);
 }
 cudaError_t oa_launch_state_zbwd(oa_ctx* c, cudaStream_t s, const double2* psi, const double2* fnl,
                                  double2* force, int s0, int ns) {
+  if (oa_pencil_supported(c->nz))
+    return oa_pencil_zbwd(c->precision, s, c->nz, c->zbuf, c->ldl, c->nlines, c->line_kx, c->line_off,
+                          c->line_nneg, c->line_npos, c->tw_z, psi, fnl, force, c->g2, c->occ, c->ng, s0, ns,
+                          -2.0 / (double)c->npts, c->ecut_psi, c->eke_part, c->nblk_z, nullptr);
   return c->precision == OA_FP64 ? launch_zbwd<double>(c, s, psi, fnl, force, s0, ns)
                                  : launch_zbwd<float>(c, s, psi, fnl, force, s0, ns);
 }
@@ -478,8 +465,13 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
   typedef typename CplxOf<R>::T C;
   oa_ees* e = c->ees;
   cudaError_t err;
+  const bool pz = oa_pencil_supported(e->nc) != 0;
   // z pass forward with conj(dyp psi)
-  {
+  if (pz) {
+    err = oa_pencil_zfwd(c->precision, st, e->nc, psi, c->ng, 0, c->nstate, c->line_off, c->line_nneg, c->line_npos,
+                         c->nlines, e->zbuf, c->ldl, e->tw_c, e->dyp);
+    if (err != cudaSuccess) return err;
+  } else {
     size_t sm = zpass_smem<R>(e->nc);
     err = cudaFuncSetAttribute(k_state_zfwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (err != cudaSuccess) return err;
@@ -491,20 +483,39 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
   PlaneSmem L = plane_smem_layout<C, R>(e->na, e->nb, c->nkx_s);
   EesArgs E = {e->idx, e->mn, e->zpart, e->zs, c->natm_nl, e->order};
   dim3 pgrid(e->nc, e->ngroup);
-  err = cudaFuncSetAttribute(k_state_plane<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+  const bool pp = e->na == e->nb && oa_pencil_supported(e->na);
+  err = cudaErrorNotSupported;
+  if (pp)
+    err = oa_pencil_plane(c->precision, 2, st, e->na, e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky,
+                          e->nc, c->nkx_s, e->tw_a, c->occ, nullptr, nullptr, e->ngroup, E);
+  if (err == cudaErrorNotSupported) {
+    err = cudaFuncSetAttribute(k_state_plane<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    if (err != cudaSuccess) return err;
+    k_state_plane<R, 2><<<pgrid, OA_PLANE_THREADS, L.total, st>>>(
+        (C*)e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky, e->na, e->nb, e->nc, c->nkx_s, e->pa,
+        e->pb, e->tw_a, e->tw_b, c->occ, nullptr, nullptr, e->ngroup, L, E);
+    err = cudaGetLastError();
+  }
   if (err != cudaSuccess) return err;
-  k_state_plane<R, 2><<<pgrid, OA_PLANE_THREADS, L.total, st>>>(
-      (C*)e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky, e->na, e->nb, e->nc, c->nkx_s, e->pa, e->pb,
-      e->tw_a, e->tw_b, c->occ, nullptr, nullptr, e->ngroup, L, E);
-  if ((err = cudaGetLastError()) != cudaSuccess) return err;
   err = oa_launch_ees_zreduce(c, st);
   if (err != cudaSuccess) return err;
-  err = cudaFuncSetAttribute(k_state_plane<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+  err = cudaErrorNotSupported;
+  if (pp)
+    err = oa_pencil_plane(c->precision, 3, st, e->na, e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky,
+                          e->nc, c->nkx_s, e->tw_a, c->occ, nullptr, nullptr, e->ngroup, E);
+  if (err == cudaErrorNotSupported) {
+    err = cudaFuncSetAttribute(k_state_plane<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    if (err != cudaSuccess) return err;
+    k_state_plane<R, 3><<<pgrid, OA_PLANE_THREADS, L.total, st>>>(
+        (C*)e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky, e->na, e->nb, e->nc, c->nkx_s, e->pa,
+        e->pb, e->tw_a, e->tw_b, c->occ, nullptr, nullptr, e->ngroup, L, E);
+    err = cudaGetLastError();
+  }
   if (err != cudaSuccess) return err;
-  k_state_plane<R, 3><<<pgrid, OA_PLANE_THREADS, L.total, st>>>(
-      (C*)e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky, e->na, e->nb, e->nc, c->nkx_s, e->pa, e->pb,
-      e->tw_a, e->tw_b, c->occ, nullptr, nullptr, e->ngroup, L, E);
-  if ((err = cudaGetLastError()) != cudaSuccess) return err;
+  if (pz)
+    return oa_pencil_zbwd(c->precision, st, e->nc, e->zbuf, c->ldl, c->nlines, c->line_kx, c->line_off,
+                          c->line_nneg, c->line_npos, e->tw_c, psi, nullptr, fnl, c->g2, c->occ, c->ng, 0, c->nstate,
+                          1.0, c->ecut_psi, c->eke_part, c->nblk_z, e->dyp);
   {
     size_t sm = zpass_smem<R>(e->nc);
     err = cudaFuncSetAttribute(k_state_zbwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

@@ -21,11 +21,11 @@ def rel(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-@pytest.fixture(scope="module", params=["w2", "w4", "w8"])
+@pytest.fixture(scope="module", params=["w2", "w4", "w8", "w32"])
 def case(request):
     import torch
     from openatom_b200.gpu import CPContext
-    nst = {"w2": None, "w4": None, "w8": 16}[request.param]
+    nst = {"w2": None, "w4": None, "w8": 16, "w32": 8}[request.param]
     s = make_system(request.param, nstate=nst, seed=7)
     ctx = CPContext(s, "fp64")
     psi = torch.from_numpy(s.psi).cuda()
