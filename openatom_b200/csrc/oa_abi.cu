@@ -247,7 +247,7 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     c->red_len = (size_t)3 * oa_rho_xc_nblk() + 3 * (size_t)oa_rho_z_nblk(c) + 64;
     TRY(cudaMalloc(&c->red, c->red_len * sizeof(double)));
     TRY(cudaMalloc(&c->eke_part, (size_t)d->nstate * c->nblk_z * sizeof(double)));
-    p->nkb = 64;
+    p->nkb = 160;  // split-K partials: about one CTA per SM for a 128 x 128 product
     TRY(cudaMalloc(&p->part, (size_t)p->nkb * d->nstate * d->nstate * sizeof(double)));
     p->ns_grid = oa_ns_grid(d->nstate, c->device);
     TRY(cudaMalloc(&p->ns_work, ((size_t)5 * d->nstate * d->nstate + p->ns_grid + 8) * sizeof(double)));

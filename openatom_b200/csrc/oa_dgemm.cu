@@ -1,0 +1,352 @@
+// Pipelined FP64 tensor-core (DMMA) forward product of the PairCalculator:
+//   C[i][j] = alpha sum_k w(k) A[i][k] B[j][k],  w(k) = w_kx0 for k < kx0_cols, else 1
+// (PairCalculator::multiplyForward, ckPairCalculator.C:821-933, with the
+// reference's DGEMM('T','N') on the 2*ng-double real view of each state).
+//
+// Split-K over slabs of 32 columns: the kx0 columns [0, kx0_cols) are shared
+// out among the first n0 CTAs of a tile and the other columns among the
+// remaining nr CTAs, slab t of a region going to CTA t mod (count), so at
+// any moment the CTAs stream neighbouring 256-byte pieces of the same rows
+// (DRAM pages are opened once, not once per CTA).  Each CTA writes an FP64
+// partial of its 128 x 128 output tile; the kx0 weight is applied to the
+// first n0 partials in the reduction, so the main loop has no per-column
+// weight and, when A and B are the same matrix (the overlap S), one shared
+// memory copy of the operand slab serves both sides.  Partials are summed in
+// a fixed order: the result does not depend on scheduling.
+//
+// Main loop: 512 threads, 16 warps of 32 x 32 (4 x 4 DMMA m8n8k4 tiles); K
+// slabs of 32 doubles move global -> shared with 16-byte cp.async into a
+// ring of STAGES slabs (4 when A and B are one matrix, else 3: 144 / 216 KB),
+// so the loads of the next slabs overlap the DMMAs of the current one.
+#include "oa_internal.h"
+
+#define DG_TM 128
+#define DG_KS 32
+#define DG_LD (DG_KS + 4)          // doubles per smem row: conflict-free fragment loads
+#define DG_THREADS 512
+#define DG_SLAB (DG_TM * DG_LD)    // doubles per operand slab
+
+__device__ __forceinline__ void dg_dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void dg_cp16(void* smem, const void* gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 16 : 0;  // src-size 0: the 16 bytes are zero-filled
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" :: "r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void dg_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void dg_wait() { asm volatile("cp.async.wait_group %0;\n" :: "n"(N)); }
+
+// one operand slab: rows [r0, r0 + 128) of X (row stride K), columns [k0, k0 + 32)
+// clipped to [k0, kend) and rows < nrows; 2048 16-byte pieces, 4 per thread
+__device__ __forceinline__ void dg_load_slab(double* dst, const double* __restrict__ X, int r0, int nrows, long K,
+                                             long k0, long kend) {
+#pragma unroll
+  for (int q = 0; q < (DG_TM * DG_KS / 2) / DG_THREADS; ++q) {
+    const int piece = threadIdx.x + q * DG_THREADS;
+    const int r = piece >> 4;            // 16 pieces per row
+    const int kk = (piece & 15) * 2;
+    const long k = k0 + kk;
+    const bool valid = (r0 + r < nrows) && (k < kend);
+    const double* src = valid ? X + (size_t)(r0 + r) * K + k : X;
+    dg_cp16(dst + r * DG_LD + kk, src, valid);
+  }
+}
+
+template <bool SAME, int DG_STAGES>
+__global__ void __launch_bounds__(DG_THREADS, 1)
+k_dgemm_fwd(const double* __restrict__ A, const double* __restrict__ B, int m, int n, long K, long kx0_cols,
+            int n0, int nr, double* __restrict__ part) {
+  extern __shared__ __align__(16) double dg_smem[];
+  double* As = dg_smem;
+  double* Bs = SAME ? dg_smem : dg_smem + DG_STAGES * DG_SLAB;
+  const int i0 = blockIdx.x * DG_TM, j0 = blockIdx.y * DG_TM;
+  const int kb = blockIdx.z;
+  // region and slab sequence of this CTA: slabs first, first + stride, ...
+  const bool in0 = kb < n0;
+  const long rbeg = in0 ? 0 : kx0_cols, rend = in0 ? kx0_cols : K;
+  const int first = in0 ? kb : kb - n0, stride = in0 ? n0 : nr;
+  const long rslabs = (rend - rbeg + DG_KS - 1) / DG_KS;
+  const int nslab = rslabs > first ? (int)((rslabs - first + stride - 1) / stride) : 0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wi = (warp >> 2) * 32, wj = (warp & 3) * 32;
+  const bool active = (i0 + wi < m) && (j0 + wj < n);
+  double acc[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) { acc[a][b][0] = 0.0; acc[a][b][1] = 0.0; }
+  // prologue: slabs 0 .. STAGES-2
+#pragma unroll
+  for (int s = 0; s < DG_STAGES - 1; ++s) {
+    if (s < nslab) {
+      const long k0 = rbeg + ((long)first + (long)s * stride) * DG_KS;
+      dg_load_slab(As + s * DG_SLAB, A, i0, m, K, k0, rend);
+      if (!SAME) dg_load_slab(Bs + s * DG_SLAB, B, j0, n, K, k0, rend);
+    }
+    dg_commit();
+  }
+  for (int s = 0; s < nslab; ++s) {
+    dg_wait<DG_STAGES - 2>();
+    __syncthreads();
+    // refill the stage freed by slab s - 1
+    {
+      const int sn = s + DG_STAGES - 1;
+      if (sn < nslab) {
+        const int st = sn % DG_STAGES;
+        const long k0 = rbeg + ((long)first + (long)sn * stride) * DG_KS;
+        dg_load_slab(As + st * DG_SLAB, A, i0, m, K, k0, rend);
+        if (!SAME) dg_load_slab(Bs + st * DG_SLAB, B, j0, n, K, k0, rend);
+      }
+      dg_commit();
+    }
+    const double* as = As + (s % DG_STAGES) * DG_SLAB;
+    const double* bs = Bs + (s % DG_STAGES) * DG_SLAB;
+    if (active) {
+#pragma unroll
+      for (int k4 = 0; k4 < DG_KS; k4 += 4) {
+        double af[4], bf[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) af[q] = as[(wi + q * 8 + (lane >> 2)) * DG_LD + k4 + (lane & 3)];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) bf[q] = bs[(wj + q * 8 + (lane >> 2)) * DG_LD + k4 + (lane & 3)];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) dg_dmma(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+      }
+    }
+  }
+  dg_wait<0>();
+  if (!active) return;
+  double* out = part + (size_t)kb * m * n;
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = i0 + wi + a * 8 + (lane >> 2);
+      const int j = j0 + wj + b * 8 + 2 * (lane & 3);
+      if (i < m && j < n) out[(size_t)i * n + j] = acc[a][b][0];
+      if (i < m && j + 1 < n) out[(size_t)i * n + j + 1] = acc[a][b][1];
+    }
+}
+
+// C = alpha (w0 sum_{kb < n0} part[kb] + sum_{kb >= n0} part[kb]), fixed order
+__global__ void k_dgemm_fwd_reduce(const double* __restrict__ part, int n0, int nkb, size_t nn, double w0,
+                                   double alpha, double* __restrict__ C) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (size_t)gridDim.x * blockDim.x) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int k = 0; k < n0; ++k) s0 += part[(size_t)k * nn + i];
+    for (int k = n0; k < nkb; ++k) s1 += part[(size_t)k * nn + i];
+    C[i] = alpha * (w0 * s0 + s1);
+  }
+}
+
+#define DG_STAGES_SAME 4
+#define DG_STAGES_TWO 3
+size_t oa_dgemm_fwd_smem(bool same) {
+  return same ? (size_t)DG_STAGES_SAME * DG_SLAB * sizeof(double) : (size_t)2 * DG_STAGES_TWO * DG_SLAB * sizeof(double);
+}
+
+// Returns cudaErrorNotSupported when the operands do not allow 16-byte
+// copies (odd K, odd kx0_cols or unaligned pointers); the caller then uses
+// the element-wise kernel.  nkb bounds the partials the caller provides
+// (part holds nkb * m * n doubles).
+cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m, int n, long K, long kx0_cols,
+                         double w_kx0, double alpha, double* part, int nkb, double* C) {
+  if ((K & 1) || (kx0_cols & 1) || (((uintptr_t)A | (uintptr_t)B) & 15) || kx0_cols > K || nkb < 2)
+    return cudaErrorNotSupported;
+  static const int nsm = [] {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    return v;
+  }();
+  const int ti = (m + DG_TM - 1) / DG_TM, tj = (n + DG_TM - 1) / DG_TM;
+  // about one CTA per SM; the kx0 region gets CTAs in proportion to its slabs
+  const long s0 = (kx0_cols + DG_KS - 1) / DG_KS, sr = (K - kx0_cols + DG_KS - 1) / DG_KS;
+  int nk = nsm / (ti * tj);
+  if (nk > nkb) nk = nkb;
+  if (nk < 2) nk = 2;
+  int n0 = s0 > 0 ? (int)((nk * s0 + s0 + sr - 1) / (s0 + sr)) : 0;  // rounded up: no straggler
+  if (s0 > 0 && n0 < 1) n0 = 1;
+  if (n0 > s0) n0 = (int)s0;
+  int nr = nk - n0;
+  if (nr > sr) nr = (int)sr;
+  if (sr > 0 && nr < 1) return cudaErrorNotSupported;
+  const int nkb_eff = n0 + nr;
+  if (nkb_eff < 1 || nkb_eff > nkb) return cudaErrorNotSupported;
+  // one shared slab serves both operands only when the single output tile
+  // is diagonal (A == B and m, n <= 128)
+  const bool same = (A == B) && ti == 1 && tj == 1;
+  const size_t sm = oa_dgemm_fwd_smem(same);
+  dim3 grid(ti, tj, nkb_eff);
+  cudaError_t e;
+  if (same) {
+    e = cudaFuncSetAttribute(k_dgemm_fwd<true, DG_STAGES_SAME>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_dgemm_fwd<true, DG_STAGES_SAME><<<grid, DG_THREADS, sm, s>>>(A, B, m, n, K, kx0_cols, n0, nr, part);
+  } else {
+    e = cudaFuncSetAttribute(k_dgemm_fwd<false, DG_STAGES_TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_dgemm_fwd<false, DG_STAGES_TWO><<<grid, DG_THREADS, sm, s>>>(A, B, m, n, K, kx0_cols, n0, nr, part);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const size_t mn = (size_t)m * n;
+  k_dgemm_fwd_reduce<<<(unsigned)((mn + 255) / 256), 256, 0, s>>>(part, n0, nkb_eff, mn, w_kx0, alpha, C);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Backward product (PairCalculator::multiplyResult / bwMultiplyHelper /
+// bwMultiplyDynOrthoT, ckPairCalculator.C:1201-1468, 1710-2031):
+//   out[j][c] = a1(c) sum_k M1[k][j] X1[k][c] + a2 sum_k M2[k][j] X2[k][c]
+//   a1(c) = a1_kx0 for c < kx0_cols, else a1_rest
+// CTA tile: 128 rows j x 64 columns c, all k; 8 warps of 32 x 32.  The M and
+// X slabs of 16 k rows move through a 4-stage cp.async ring; the two terms
+// run as one slab sequence.  The first term's sum is scaled by a1(c) in
+// registers once it is complete; the second term's M fragments are scaled
+// by a2 as they are read, so one accumulator set serves both terms.
+// ---------------------------------------------------------------------------
+#define DB_TJ 128
+#define DB_TC 64
+#define DB_KS 16
+#define DB_LDM (DB_TJ + 4)
+#define DB_LDX (DB_TC + 4)
+#define DB_STAGES 4
+#define DB_THREADS 256
+#define DB_MSLAB (DB_KS * DB_LDM)
+#define DB_XSLAB (DB_KS * DB_LDX)
+
+__device__ __forceinline__ void db_load_slab(double* ms, double* xs, const double* __restrict__ M,
+                                             const double* __restrict__ X, int nj, int nk, long ncol, int k0,
+                                             long c0) {
+  // M rows k0..k0+15, all 128 j: 16 x 64 pieces of 16 B = 1024 -> 4 per thread
+#pragma unroll
+  for (int q = 0; q < (DB_KS * DB_TJ / 2) / DB_THREADS; ++q) {
+    const int piece = threadIdx.x + q * DB_THREADS;
+    const int kk = piece >> 6, jj = (piece & 63) * 2;
+    const int k = k0 + kk;
+    const bool valid = (k < nk) && (jj < nj);
+    dg_cp16(ms + kk * DB_LDM + jj, valid ? M + (size_t)k * nj + jj : M, valid);
+  }
+  // X rows k0..k0+15, columns c0..c0+63: 16 x 32 pieces = 512 -> 2 per thread
+#pragma unroll
+  for (int q = 0; q < (DB_KS * DB_TC / 2) / DB_THREADS; ++q) {
+    const int piece = threadIdx.x + q * DB_THREADS;
+    const int kk = piece >> 5, cc = (piece & 31) * 2;
+    const int k = k0 + kk;
+    const long c = c0 + cc;
+    const bool valid = (k < nk) && (c < ncol);
+    dg_cp16(xs + kk * DB_LDX + cc, valid ? X + (size_t)k * ncol + c : X, valid);
+  }
+}
+
+template <bool TWO>
+__global__ void __launch_bounds__(DB_THREADS, 2)
+k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double a1_kx0, double a1_rest,
+            const double* __restrict__ M2, const double* __restrict__ X2, double a2, int nj, int nk, long ncol,
+            long kx0_cols, double* __restrict__ out) {
+  extern __shared__ __align__(16) double db_smem[];
+  double* Ms = db_smem;
+  double* Xs = db_smem + DB_STAGES * DB_MSLAB;
+  const long c0 = (long)blockIdx.x * DB_TC;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wj = (warp >> 1) * 32, wc = (warp & 1) * 32;
+  const int nsl = (nk + DB_KS - 1) / DB_KS;
+  const int ntot = TWO ? 2 * nsl : nsl;
+  double acc[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) { acc[a][b][0] = 0.0; acc[a][b][1] = 0.0; }
+  auto issue = [&](int s) {
+    const int st = s % DB_STAGES;
+    const bool second = TWO && s >= nsl;
+    const int k0 = (second ? s - nsl : s) * DB_KS;
+    db_load_slab(Ms + st * DB_MSLAB, Xs + st * DB_XSLAB, second ? M2 : M1, second ? X2 : X1, nj, nk, ncol, k0, c0);
+  };
+  // a1(c) for this thread's output columns
+  auto scale_a1 = [&]() {
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const long c = c0 + wc + b * 8 + 2 * (lane & 3) + e;
+        const double a1 = (c < kx0_cols) ? a1_kx0 : a1_rest;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) acc[a][b][e] *= a1;
+      }
+  };
+#pragma unroll
+  for (int s = 0; s < DB_STAGES - 1; ++s) {
+    if (s < ntot) issue(s);
+    dg_commit();
+  }
+  for (int s = 0; s < ntot; ++s) {
+    dg_wait<DB_STAGES - 2>();
+    __syncthreads();
+    if (s + DB_STAGES - 1 < ntot) issue(s + DB_STAGES - 1);
+    dg_commit();
+    if (TWO && s == nsl) scale_a1();
+    const double sa = (TWO && s >= nsl) ? a2 : 1.0;
+    const double* ms = Ms + (s % DB_STAGES) * DB_MSLAB;
+    const double* xs = Xs + (s % DB_STAGES) * DB_XSLAB;
+#pragma unroll
+    for (int k4 = 0; k4 < DB_KS; k4 += 4) {
+      double af[4], bf[4];
+      // A[j][k] = M[k][j] (row-major 8 x 4 fragment), B[k][c] = X[k][c]
+#pragma unroll
+      for (int q = 0; q < 4; ++q) af[q] = ms[(k4 + (lane & 3)) * DB_LDM + wj + q * 8 + (lane >> 2)] * sa;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bf[q] = xs[(k4 + (lane & 3)) * DB_LDX + wc + q * 8 + (lane >> 2)];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) dg_dmma(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+    }
+  }
+  dg_wait<0>();
+  if (!TWO) scale_a1();
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int j = wj + a * 8 + (lane >> 2);
+    if (j >= nj) continue;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const long c = c0 + wc + b * 8 + 2 * (lane & 3);
+      if (c + 1 < ncol) {
+        *(double2*)(out + (size_t)j * ncol + c) = make_double2(acc[a][b][0], acc[a][b][1]);
+      } else if (c < ncol) {
+        out[(size_t)j * ncol + c] = acc[a][b][0];
+      }
+    }
+  }
+}
+
+// Returns cudaErrorNotSupported when the shapes or pointers do not allow the
+// 16-byte copies (nj > 128, odd nj or ncol, unaligned pointers).
+cudaError_t oa_dgemm_bwd(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
+                         const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
+                         double* out) {
+  const uintptr_t al = (uintptr_t)M1 | (uintptr_t)X1 | (uintptr_t)out | (uintptr_t)(M2 ? M2 : M1) |
+                       (uintptr_t)(X2 ? X2 : X1);
+  if (nj > DB_TJ || (nj & 1) || (ncol & 1) || (al & 15) || nk <= 0 || (M2 && !X2)) return cudaErrorNotSupported;
+  const size_t sm = (size_t)DB_STAGES * (DB_MSLAB + DB_XSLAB) * sizeof(double);
+  dim3 grid((unsigned)((ncol + DB_TC - 1) / DB_TC));
+  cudaError_t e;
+  if (M2) {
+    e = cudaFuncSetAttribute(k_dgemm_bwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_dgemm_bwd<true><<<grid, DB_THREADS, sm, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out);
+  } else {
+    e = cudaFuncSetAttribute(k_dgemm_bwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_dgemm_bwd<false><<<grid, DB_THREADS, sm, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols,
+                                                     out);
+  }
+  return cudaGetLastError();
+}
