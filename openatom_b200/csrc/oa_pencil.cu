@@ -20,13 +20,26 @@
 #include "oa_rdft.cuh"
 #include "oa_state_common.cuh"
 
-// shared-memory strides (complex elements) of the pass-A -> pass-B buffer
-// ([k1][n2] per pencil) and of the inverse B' -> A' buffer ([m2][k1])
+// Smallest odd stride >= minv, congruent to want (odd) modulo 16 when want >= 0.
+__host__ __device__ constexpr int pencil_stride(int minv, int want) {
+  int p = minv | 1;
+  if (want >= 0)
+    while ((p & 15) != want) p += 2;
+  return p;
+}
+
+// Shared-memory strides (complex elements) of the pass-A -> pass-B buffer
+// ([k1][n2] per pencil, row ls1, pencil ps1) and of the inverse B' -> A'
+// buffer ([m2][k1], row ls2, pencil ps2).  Bank rule (8-byte elements, 16
+// threads per conflict domain): all strides are odd, so 16 threads that
+// walk consecutive pencils at the same offset hit 16 distinct banks; and,
+// for odd N2, ps1 = N2 and ps2 = N2 ls2 (mod 16), so threads that walk
+// (pencil, n2) with n2 fastest address ps1 pencil + n2 = thread (mod 16).
 template <int N1, int N2> struct PencilLd {
   static constexpr int ls1 = odd_ld(N2);
-  static constexpr int ps1 = odd_ld(N1 * ls1);
   static constexpr int ls2 = odd_ld(N1);
-  static constexpr int ps2 = odd_ld(N2 * ls2);
+  static constexpr int ps1 = pencil_stride(N1 * ls1, (N2 & 1) ? (N2 & 15) : -1);
+  static constexpr int ps2 = pencil_stride(N2 * ls2, (N2 & 1) ? ((N2 * ls2) & 15) : -1);
 };
 
 // packed index of z-slot z on a line with nn negative and np non-negative kz
@@ -182,13 +195,17 @@ k_zbwd2(const typename CplxOf<R>::T* __restrict__ zbuf, int ldl, int nlines, con
 //   MODE 0: zbuf row -> P[kx][y] -> y FFT(-) -> x FFT(-) of row pairs
 //           (two-for-one c2r) -> tile += occ psi(r)^2
 //   MODE 1: ... x FFT(-) -> psi(r) V_KS occ -> x FFT(+) -> r2c unpack -> y FFT(+)
-//           -> zbuf row (in place)
+//           -> zbuf row (in place); V_KS is read from global memory (L2)
 //   MODE 2: as MODE 0 but tile = psi(r) (nonlocal grid), then the EES Z gather
 //   MODE 3: EES scatter -> tile -> x FFT(+) -> r2c unpack -> y FFT(+) -> zbuf row
-// Pencils (y columns, x row pairs) go through in chunks of G; the block
-// synchronises between the passes.  In MODE 1 the forward DFT_N2, the V_KS
-// product and the backward DFT_N2 of an x pencil run back to back in the
-// registers of one thread (pass B, then pass B' of the inverse).
+// Pencils (y columns, x row pairs) go through in chunks of at most G; the
+// block synchronises between the passes.  In MODE 1 the forward DFT_N2, the
+// V_KS product and the backward DFT_N2 of an x pencil run back to back in
+// the registers of one thread (pass B, then pass B' of the inverse).
+// Thread mappings keep shared memory free of bank conflicts (PencilLd):
+// y passes and the x pass B walk 16 consecutive pencils (or a whole pencil
+// padded to 16 threads) per half-warp; the other passes walk (pencil, index)
+// with the index fastest.
 // ---------------------------------------------------------------------------
 struct Plane2Smem {
   size_t tw, P, tile, s1, s2, total;
@@ -196,7 +213,7 @@ struct Plane2Smem {
 };
 
 template <typename R, int MODE, int N1, int N2>
-__global__ void __launch_bounds__(OA_PLANE_THREADS)
+__global__ void __launch_bounds__(OA_PLANE_THREADS, sizeof(R) == 4 ? 2 : 1)
 k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlines,
          const int* __restrict__ line_kx, const int* __restrict__ line_ky, int nkx,
          const double2* __restrict__ twg, const double* __restrict__ occ, const R* __restrict__ vks,
@@ -204,6 +221,7 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
   typedef typename CplxOf<R>::T C;
   constexpr int N = N1 * N2;
   constexpr int LDY = N + 1;
+  static_assert(N1 <= 16, "pass B pads a pencil to 16 threads");
   typedef PencilLd<N1, N2> LD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = (C*)(smem_raw + L.tw);
@@ -217,14 +235,45 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
   const int sb = g * nper, se = min(nstate, sb + nper);
   constexpr int npairs = (N + 1) / 2;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const R* vz = (MODE == 1) ? vks + (size_t)z * N * N : nullptr;
   load_twiddles(tw, twg, N);
   if (MODE == 0) {
     for (int i = threadIdx.x; i < N * N; i += blockDim.x) tile[i] = (R)0;
-  } else if (MODE == 1) {
-    const R* vz = vks + (size_t)z * N * N;
-    for (int i = threadIdx.x; i < N * N; i += blockDim.x) tile[i] = vz[i];
   }
   __syncthreads();
+  // y FFT over the kx columns [0, nkx), in place in P; pencil-fastest
+  // mapping padded to 16 columns
+  auto y_fft = [&](auto sign_c) {
+    constexpr int SG = decltype(sign_c)::value;
+    for (int c0 = 0; c0 < nkx; c0 += G) {
+      const int gc = min(G, nkx - c0);
+      const int gcp = (gc + 15) & ~15;
+      for (int it = threadIdx.x; it < gcp * N2; it += blockDim.x) {
+        const int n2 = it / gcp, cc = it - n2 * gcp;
+        if (cc >= gc) continue;
+        const C* col = P + (c0 + cc) * LDY;
+        C u[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) u[n1] = col[N2 * n1 + n2];
+        pass_a<N1, N2, SG>(u, n2, tw);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) s1[cc * LD::ps1 + k1 * LD::ls1 + n2] = u[k1];
+      }
+      __syncthreads();
+      for (int it = threadIdx.x; it < gcp * N1; it += blockDim.x) {
+        const int k1 = it / gcp, cc = it - k1 * gcp;
+        if (cc >= gc) continue;
+        C* col = P + (c0 + cc) * LDY;
+        C w[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) w[n2] = s1[cc * LD::ps1 + k1 * LD::ls1 + n2];
+        RDft<N2, SG>::run(w);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) col[k1 + N1 * k2] = w[k2];
+      }
+      __syncthreads();
+    }
+  };
   for (int s = sb; s < se; ++s) {
     C* row = zbuf + ((size_t)s * N + z) * ldl;
     if (MODE == 3) {
@@ -240,37 +289,14 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
         P[line_kx[l] * LDY + ky] = row[l];
       }
       __syncthreads();
-      // y FFT(-) over the occupied kx columns, in place in P
-      for (int c0 = 0; c0 < nkx; c0 += G) {
-        const int gc = min(G, nkx - c0);
-        for (int it = threadIdx.x; it < gc * N2; it += blockDim.x) {
-          const int cc = it / N2, n2 = it - cc * N2;
-          const C* col = P + (c0 + cc) * LDY;
-          C u[N1];
-#pragma unroll
-          for (int n1 = 0; n1 < N1; ++n1) u[n1] = col[N2 * n1 + n2];
-          pass_a<N1, N2, -1>(u, n2, tw);
-#pragma unroll
-          for (int k1 = 0; k1 < N1; ++k1) s1[cc * LD::ps1 + k1 * LD::ls1 + n2] = u[k1];
-        }
-        __syncthreads();
-        for (int it = threadIdx.x; it < gc * N1; it += blockDim.x) {
-          const int cc = it / N1, k1 = it - cc * N1;
-          C* col = P + (c0 + cc) * LDY;
-          C w[N2];
-#pragma unroll
-          for (int n2 = 0; n2 < N2; ++n2) w[n2] = s1[cc * LD::ps1 + k1 * LD::ls1 + n2];
-          RDft<N2, -1>::run(w);
-#pragma unroll
-          for (int k2 = 0; k2 < N2; ++k2) col[k1 + N1 * k2] = w[k2];
-        }
-        __syncthreads();
-      }
+      y_fft(std::integral_constant<int, -1>{});
     }
     const R o = (R)occ[s];
-    // x pencils: row pairs (y1, y2) as one complex sequence
-    for (int p0 = 0; p0 < npairs; p0 += G) {
-      const int gp = min(G, npairs - p0);
+    // x pencils: row pairs (y1, y2) as one complex sequence, in balanced chunks
+    const int nch = (npairs + G - 1) / G;
+    const int gsz = (npairs + nch - 1) / nch;
+    for (int p0 = 0; p0 < npairs; p0 += gsz) {
+      const int gp = min(gsz, npairs - p0);
       constexpr int SA = (MODE == 3) ? +1 : -1;
       for (int it = threadIdx.x; it < gp * N2; it += blockDim.x) {
         const int pp = it / N2, n2 = it - pp * N2;
@@ -297,8 +323,10 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
         for (int k1 = 0; k1 < N1; ++k1) s1[pp * LD::ps1 + k1 * LD::ls1 + n2] = u[k1];
       }
       __syncthreads();
-      for (int it = threadIdx.x; it < gp * N1; it += blockDim.x) {
-        const int pp = it / N1, k1 = it - pp * N1;
+      // pass B: one pencil per 16 threads (k1 < N1 active)
+      for (int it = threadIdx.x; it < gp * 16; it += blockDim.x) {
+        const int pp = it >> 4, k1 = it & 15;
+        if (k1 >= N1) continue;
         const int y1 = 2 * (p0 + pp), y2 = y1 + 1;
         C w[N2];
 #pragma unroll
@@ -325,8 +353,8 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
 #pragma unroll
           for (int k2 = 0; k2 < N2; ++k2) {
             const int x = k1 + N1 * k2;
-            w[k2].x *= tile[y1 * N + x] * o;
-            w[k2].y = (y2 < N) ? w[k2].y * tile[y2 * N + x] * o : (R)0;
+            w[k2].x *= __ldg(vz + y1 * N + x) * o;
+            w[k2].y = (y2 < N) ? w[k2].y * __ldg(vz + y2 * N + x) * o : (R)0;
           }
           // inverse, first half: DFT_N2(+) over k2, twiddle exp(+2 pi i k1 m2 / N)
           RDft<N2, +1>::run(w);
@@ -374,32 +402,7 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
       __syncthreads();
     }
     if (MODE == 1 || MODE == 3) {
-      // y FFT(+) over the kx columns, in place in P
-      for (int c0 = 0; c0 < nkx; c0 += G) {
-        const int gc = min(G, nkx - c0);
-        for (int it = threadIdx.x; it < gc * N2; it += blockDim.x) {
-          const int cc = it / N2, n2 = it - cc * N2;
-          const C* col = P + (c0 + cc) * LDY;
-          C u[N1];
-#pragma unroll
-          for (int n1 = 0; n1 < N1; ++n1) u[n1] = col[N2 * n1 + n2];
-          pass_a<N1, N2, +1>(u, n2, tw);
-#pragma unroll
-          for (int k1 = 0; k1 < N1; ++k1) s1[cc * LD::ps1 + k1 * LD::ls1 + n2] = u[k1];
-        }
-        __syncthreads();
-        for (int it = threadIdx.x; it < gc * N1; it += blockDim.x) {
-          const int cc = it / N1, k1 = it - cc * N1;
-          C* col = P + (c0 + cc) * LDY;
-          C w[N2];
-#pragma unroll
-          for (int n2 = 0; n2 < N2; ++n2) w[n2] = s1[cc * LD::ps1 + k1 * LD::ls1 + n2];
-          RDft<N2, +1>::run(w);
-#pragma unroll
-          for (int k2 = 0; k2 < N2; ++k2) col[k1 + N1 * k2] = w[k2];
-        }
-        __syncthreads();
-      }
+      y_fft(std::integral_constant<int, +1>{});
       for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
         int ky = line_ky[l]; if (ky < 0) ky += N;
         row[l] = P[line_kx[l] * LDY + ky];
@@ -416,20 +419,32 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+// Shared-memory layout of k_plane2 for one mode.  With a per-CTA budget
+// that lets two CTAs share an SM (FP32 form) when at least 16 pencils fit,
+// else the whole 227 KB; G pencils per chunk.
 template <typename C, typename R, int N1, int N2>
-static Plane2Smem plane2_layout(int nkx, bool need_s2) {
+static Plane2Smem plane2_layout(int nkx, int mode) {
   constexpr int N = N1 * N2;
   typedef PencilLd<N1, N2> LD;
+  const bool need_tile = mode != 1;
+  const bool need_s2 = mode == 1 || mode == 3;
   Plane2Smem L;
   size_t o = 0;
   L.tw = o; o += align_up(N * sizeof(C), 16);
   L.P = o; o += align_up((size_t)nkx * (N + 1) * sizeof(C), 16);
-  L.tile = o; o += align_up((size_t)N * N * sizeof(R), 16);
-  const size_t fixed = o;
+  L.tile = o; o += need_tile ? align_up((size_t)N * N * sizeof(R), 16) : 0;
+  const size_t fixed = o + 32;
   const size_t per = (LD::ps1 + (need_s2 ? LD::ps2 : 0)) * sizeof(C);
   const int want = nkx > (N + 1) / 2 ? nkx : (N + 1) / 2;
-  long g = fixed + 2 * 16 < (size_t)OA_MAX_SMEM ? (long)(((size_t)OA_MAX_SMEM - fixed - 2 * 16) / per) : 0;
+  const size_t two = (size_t)(228 * 1024) / 2 - 1024;
+  long g = 0;
+  if (sizeof(R) == 4 && fixed < two) g = (long)((two - fixed) / per);
+  if (g < 16 && g < want) g = fixed < (size_t)OA_MAX_SMEM ? (long)(((size_t)OA_MAX_SMEM - fixed) / per) : 0;
   if (g > want) g = want;
+  if (g > 0) {  // balanced chunks
+    const long nch = (want + g - 1) / g;
+    g = (want + nch - 1) / nch;
+  }
   L.G = (int)g;
   L.s1 = o; o += align_up((size_t)L.G * LD::ps1 * sizeof(C), 16);
   L.s2 = o; o += need_s2 ? align_up((size_t)L.G * LD::ps2 * sizeof(C), 16) : 0;
@@ -544,7 +559,7 @@ static cudaError_t plane2_n(cudaStream_t st, void* zbuf, int nstate, int ldl, in
                             const int* lky, int nz, int nkx, const double2* tw, const double* occ, const void* vks,
                             double* rho_part, int ngroup, const EesArgs& E) {
   typedef typename CplxOf<R>::T C;
-  const Plane2Smem L = plane2_layout<C, R, N1, N2>(nkx, MODE == 1 || MODE == 3);
+  const Plane2Smem L = plane2_layout<C, R, N1, N2>(nkx, MODE);
   if (L.G < 1 || L.total > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
   cudaError_t e =
       cudaFuncSetAttribute(k_plane2<R, MODE, N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
@@ -584,12 +599,22 @@ cudaError_t oa_pencil_plane(int precision, int mode, cudaStream_t st, int n, voi
   return cudaErrorNotSupported;
 }
 
-// shared memory of the two-pass plane kernel (MODE 1 layout, the largest);
-// 0 when there is none for this length
+template <typename C, typename R, int N1, int N2>
+static size_t plane2_smem_max(int nkx) {
+  size_t m = 0;
+  for (int mode = 0; mode < 4; ++mode) {
+    const size_t t = plane2_layout<C, R, N1, N2>(nkx, mode).total;
+    if (t > m) m = t;
+  }
+  return m;
+}
+
+// largest shared memory of the two-pass plane kernel over its modes; 0 when
+// there is none for this length
 size_t oa_pencil_plane_smem(int precision, int n, int nkx) {
 #define OA_CALL(A, B)                                                                  \
-  (precision == OA_FP64 ? plane2_layout<double2, double, A, B>(nkx, true).total        \
-                        : plane2_layout<float2, float, A, B>(nkx, true).total)
+  (precision == OA_FP64 ? plane2_smem_max<double2, double, A, B>(nkx)                  \
+                        : plane2_smem_max<float2, float, A, B>(nkx))
   OA_PENCIL_DISPATCH(n, OA_CALL)
 #undef OA_CALL
   return 0;
