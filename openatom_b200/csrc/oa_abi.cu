@@ -142,6 +142,8 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
   OA_ARG_CHECK(precision == OA_FP64 || precision == OA_MIXED, "precision must be OA_FP64 or OA_MIXED");
   OA_ARG_CHECK(d->nx > 0 && d->ny > 0 && d->nz > 0 && d->nstate > 0 && d->ng > 0 && d->nlines > 0, "bad sizes");
   OA_ARG_CHECK(d->ntype >= 1 && d->ntype <= 4, "ntype must be 1..4");
+  OA_ARG_CHECK(d->natm == 0 || d->atm_type, "null atm_type");
+  for (int a = 0; a < d->natm; ++a) OA_ARG_CHECK(d->atm_type[a] >= 0 && d->atm_type[a] < d->ntype, "atom type out of range");
   *out = nullptr;
   oa_ctx_full* F = (oa_ctx_full*)calloc(1, sizeof(oa_ctx_full));
   if (!F) return OA_ERR_CUDA;
@@ -217,6 +219,18 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     TRY(upload(&c->spl, d->spl, (size_t)d->ntype * d->nspl * 4));
     TRY(upload(&c->q_type, d->q_type, d->ntype));
     TRY(upload(&c->atm_type, d->atm_type, d->natm));
+    {
+      std::vector<int> perm;
+      perm.reserve(d->natm);
+      for (int t = 0; t < d->ntype; ++t) {
+        c->type_off[t] = (int)perm.size();
+        for (int a = 0; a < d->natm; ++a)
+          if (d->atm_type[a] == t) perm.push_back(a);
+      }
+      for (int t = d->ntype; t <= 4; ++t) c->type_off[t] = (int)perm.size();
+      if ((int)perm.size() != d->natm) { e = cudaErrorInvalidValue; goto fail; }
+      TRY(upload(&c->atm_perm, perm.data(), d->natm));
+    }
     TRY(upload(&c->pos, d->pos, (size_t)3 * d->natm));
     TRY(upload(&p->partner, d->red_partner, d->nkx0_red));
     TRY(upload(&c->ky, d->ky, d->ng));
@@ -298,7 +312,7 @@ extern "C" oa_status oa_gpu_destroy(oa_ctx* c) {
   ees_free(c);
   oa_ctx_pc* p = pcx(c);
   void* dev[] = {c->line_kx, c->line_ky, c->line_off, c->line_nneg, c->line_npos, c->kx, c->g2, c->tw_x, c->tw_y,
-                 c->tw_z, c->spl, c->q_type, c->atm_type, c->pos, c->phase, c->occ, c->zbuf, c->rho_part, c->rho,
+                 c->tw_z, c->spl, c->q_type, c->atm_type, c->atm_perm, c->pos, c->phase, c->occ, c->zbuf, c->rho_part, c->rho,
                  c->vks, c->vxc, c->dz, c->red, c->eke_part, p->part, p->ns_work, p->ns_status, p->ns_err,
                  p->partner, p->cmass, p->ke_part, p->dev_e, p->mat_a, p->mat_x, p->eye, p->vtmp, p->upart,
                  p->err_flag, c->ky, c->kz, c->nl_atm, c->nl_spl, c->nl_vnorm, c->nl_gz0, c->sf, c->zmat, c->zt,

@@ -49,6 +49,8 @@ struct oa_ctx {
   double *spl;            // [ntype][nspl][4]
   double *q_type;         // [ntype]
   int *atm_type;          // [natm]
+  int *atm_perm;          // [natm] atom ids grouped by type (stable)
+  int type_off[5];        // atoms of type t: atm_perm[type_off[t] .. type_off[t+1])
   double *pos;            // [natm][3]
   double2 *phase;         // [natm][3][2*kmax_tab+1] exp(i 2 pi k x / L)
   double *occ;            // [nstate]

@@ -224,13 +224,19 @@ k_rho_plane_bwd(const double2* __restrict__ dz, int ldl_d, int nx, int ny, int n
   }
 }
 
+struct RhoTypeOff { int off[5]; };
+
 // z pass: FFT(-) -> Hartree + local pseudopotential + Ewald (recip) in G -> FFT(+)
+// The structure factor S_t(g) = sum_{a in t} e^{i g.R_a} factorises per
+// z-line: pxy[line][a] = e^{i (gx x_a + gy y_a)} is formed once per block in
+// shared memory (atoms grouped by type), and each g of the line multiplies
+// it by the z phase e^{i gz z_a}.
 __global__ void __launch_bounds__(OA_NTHREADS)
 k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, int nz,
             OaFftPlan pz, const double2* __restrict__ twz,
             double tpi_l, double vol, double ecut4, double falp2, double gz_term,
-            int natm, int ntype, const int* __restrict__ atm_type, const double* __restrict__ q_type,
-            const double2* __restrict__ phase, int ktab,
+            int natm, int ntype, const int* __restrict__ atm_perm, RhoTypeOff toff,
+            const double* __restrict__ q_type, const double2* __restrict__ phase, int ktab,
             const double* __restrict__ spl, int nspl, double gmin, double dg,
             double* __restrict__ part) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -238,10 +244,24 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
   double2* tw = (double2*)smem_raw;
   double2* a = tw + align_up_r(nz, 2);
   double2* b = a + OA_LB * ldz;
+  double2* pxy = b + OA_LB * ldz;  // [OA_LB][natm], atoms in type order
   __shared__ double sh[3 * 32];
   const int l0 = blockIdx.x * OA_LB;
   const int nb = min(OA_LB, nlines_d - l0);
+  const int nt = 2 * ktab + 1;
   load_twiddles(tw, twz, nz);
+  for (int idx = threadIdx.x; idx < nb * natm; idx += blockDim.x) {
+    const int lb = idx / natm, ia = idx - lb * natm;
+    const int l = l0 + lb;
+    const int kx = l / ny;
+    int ky = l - kx * ny; if (2 * ky >= ny) ky -= ny;
+    double2 v = make_double2(0.0, 0.0);
+    if (kx <= ktab && abs(ky) <= ktab) {
+      const double2* ph = phase + (size_t)atm_perm[ia] * 3 * nt;
+      v = cmul(ph[kx + ktab], ph[nt + ky + ktab]);
+    }
+    pxy[lb * natm + ia] = v;
+  }
   for (int idx = threadIdx.x; idx < nz * OA_LB; idx += blockDim.x) {
     const int zz = idx / OA_LB, lb = idx - zz * OA_LB;
     if (lb < nb) a[lb * ldz + zz] = dz[(size_t)zz * ldl_d + l0 + lb];
@@ -250,7 +270,6 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
   double2* r = fft_pingpong<-1>(a, b, ldz, nb, pz, tw);
   const double pi = 3.14159265358979323846;
   const double fpi = 4.0 * pi;
-  const int nt = 2 * ktab + 1;
   double acc[3] = {0.0, 0.0, 0.0};
   for (int idx = threadIdx.x; idx < nb * nz; idx += blockDim.x) {
     const int lb = idx / nz, zz = idx - lb * nz;
@@ -273,13 +292,17 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
       // structure factors per type and for the Ewald charge sum
       double2 sf[4] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
       double2 sewd = make_double2(0.0, 0.0);
-      for (int at = 0; at < natm; ++at) {
-        const double2* ph = phase + (size_t)at * 3 * nt;
-        const double2 h = cmul(cmul(ph[kx + ktab], ph[nt + ky + ktab]), ph[2 * nt + kz + ktab]);
-        const int t = atm_type[at];
-        sf[t].x += h.x; sf[t].y += h.y;
+      const double2* pl = pxy + lb * natm;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        if (t >= ntype) break;
+        for (int ia = toff.off[t]; ia < toff.off[t + 1]; ++ia) {
+          const double2 hz = phase[(size_t)atm_perm[ia] * 3 * nt + 2 * nt + kz + ktab];
+          const double2 h = cmul(pl[ia], hz);
+          sf[t].x += h.x; sf[t].y += h.y;
+        }
         const double qa = q_type[t];
-        sewd.x += qa * h.x; sewd.y += qa * h.y;
+        sewd.x += qa * sf[t].x; sewd.y += qa * sf[t].y;
       }
       // spline of the local pseudopotential per type (CP_get_vpsnow, cp_hart_ext.C:433-480)
       const double g = sqrt(g2);
@@ -288,7 +311,9 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
       const double h0 = (double)(ii - 1) * dg + gmin;
       const double hh = g - h0;
       double2 vext = make_double2(0.0, 0.0);
-      for (int t = 0; t < ntype; ++t) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        if (t >= ntype) break;
         const double* cc = spl + ((size_t)t * nspl + (ii - 1)) * 4;
         const double vt = (((cc[3] * hh + cc[2]) * hh + cc[1]) * hh + cc[0]) / vol;
         vext.x += sf[t].x * vt; vext.y += sf[t].y * vt;
@@ -361,14 +386,18 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
                                                        c->plan_x, c->plan_y, c->tw_x, c->tw_y,
                                                        (double2*)c->dz, c->ldl_d, c->npair_d, c->ychunk_d, L);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  const size_t smz = (align_up_r(c->nz, 2) + 2 * (size_t)OA_LB * (c->nz + 1)) * sizeof(double2);
+  const size_t smz = (align_up_r(c->nz, 2) + 2 * (size_t)OA_LB * (c->nz + 1) + (size_t)OA_LB * c->natm) *
+                     sizeof(double2);
+  if (smz > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
+  RhoTypeOff toff;
+  for (int t = 0; t < 5; ++t) toff.off[t] = c->type_off[t];
   e = cudaFuncSetAttribute(k_rho_zpass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
   if (e != cudaSuccess) return e;
   const int nbz = oa_rho_z_nblk(c);
   k_rho_zpass<<<nbz, OA_NTHREADS, smz, s>>>((double2*)c->dz, c->ldl_d, c->nlines_d, c->nx, c->ny, c->nz,
                                             c->plan_z, c->tw_z, tpi_l, c->vol, c->ecut_rho,
                                             4.0 * c->alp_ewd * c->alp_ewd, c->gzvps_sum / c->vol,
-                                            c->natm, c->ntype, c->atm_type, c->q_type, c->phase, c->kmax_tab,
+                                            c->natm, c->ntype, c->atm_perm, toff, c->q_type, c->phase, c->kmax_tab,
                                             c->spl, c->nspl, c->spl_gmin, c->spl_dg,
                                             c->red + 3 * oa_rho_xc_nblk());
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
