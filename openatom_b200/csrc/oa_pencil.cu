@@ -212,8 +212,17 @@ struct Plane2Smem {
   int G;
 };
 
+// Threads per block and the blocks per SM that the shared-memory layout aims
+// for: the modes that keep a real-space tile (0, 2, 3) run 512 threads with
+// two FP32 / one FP64 block per SM; the V_KS mode, which has no tile, runs
+// 256 threads with three FP32 / two FP64 blocks per SM.
+template <typename R, int MODE> __host__ __device__ constexpr int p2_threads() { return MODE == 1 ? 256 : 512; }
+template <typename R, int MODE> __host__ __device__ constexpr int p2_min_blocks() {
+  return MODE == 1 ? (sizeof(R) == 4 ? 3 : 2) : (sizeof(R) == 4 ? 2 : 1);
+}
+
 template <typename R, int MODE, int N1, int N2>
-__global__ void __launch_bounds__(OA_PLANE_THREADS, sizeof(R) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(p2_threads<R, MODE>(), p2_min_blocks<R, MODE>())
 k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlines,
          const int* __restrict__ line_kx, const int* __restrict__ line_ky, int nkx,
          const double2* __restrict__ twg, const double* __restrict__ occ, const R* __restrict__ vks,
@@ -279,7 +288,7 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
     if (MODE == 3) {
       for (int i = threadIdx.x; i < N * N; i += blockDim.x) tile[i] = (R)0;
       __syncthreads();
-      ees_scatter_plane(tile, N, z, s, E, warp, lane, OA_PLANE_WARPS);
+      ees_scatter_plane(tile, N, z, s, E, warp, lane, p2_threads<R, MODE>() / 32);
       __syncthreads();
     } else {
       for (int i = threadIdx.x; i < nkx * LDY; i += blockDim.x) P[i] = cmk<C>(0.0, 0.0);
@@ -398,7 +407,7 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
       }
     }
     if (MODE == 2) {
-      ees_gather_plane(tile, N, z, s, E, warp, lane, OA_PLANE_WARPS);
+      ees_gather_plane(tile, N, z, s, E, warp, lane, p2_threads<R, MODE>() / 32);
       __syncthreads();
     }
     if (MODE == 1 || MODE == 3) {
@@ -419,9 +428,9 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-// Shared-memory layout of k_plane2 for one mode.  With a per-CTA budget
-// that lets two CTAs share an SM (FP32 form) when at least 16 pencils fit,
-// else the whole 227 KB; G pencils per chunk.
+// Shared-memory layout of k_plane2 for one mode: the per-block budget lets
+// the target number of blocks share an SM (p2_min_blocks) when at least 8
+// pencils then fit, else fewer blocks; G pencils per chunk.
 template <typename C, typename R, int N1, int N2>
 static Plane2Smem plane2_layout(int nkx, int mode) {
   constexpr int N = N1 * N2;
@@ -436,10 +445,14 @@ static Plane2Smem plane2_layout(int nkx, int mode) {
   const size_t fixed = o + 32;
   const size_t per = (LD::ps1 + (need_s2 ? LD::ps2 : 0)) * sizeof(C);
   const int want = nkx > (N + 1) / 2 ? nkx : (N + 1) / 2;
-  const size_t two = (size_t)(228 * 1024) / 2 - 1024;
+  const int target = mode == 1 ? (sizeof(R) == 4 ? 3 : 2) : (sizeof(R) == 4 ? 2 : 1);
   long g = 0;
-  if (sizeof(R) == 4 && fixed < two) g = (long)((two - fixed) / per);
-  if (g < 16 && g < want) g = fixed < (size_t)OA_MAX_SMEM ? (long)(((size_t)OA_MAX_SMEM - fixed) / per) : 0;
+  for (int k = target; k >= 1; --k) {
+    size_t budget = (size_t)(228 * 1024) / k - 1024;
+    if (budget > (size_t)OA_MAX_SMEM) budget = OA_MAX_SMEM;
+    g = fixed < budget ? (long)((budget - fixed) / per) : 0;
+    if (g >= 8 || g >= want) break;
+  }
   if (g > want) g = want;
   if (g > 0) {  // balanced chunks
     const long nch = (want + g - 1) / g;
@@ -565,7 +578,7 @@ static cudaError_t plane2_n(cudaStream_t st, void* zbuf, int nstate, int ldl, in
       cudaFuncSetAttribute(k_plane2<R, MODE, N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
   if (e != cudaSuccess) return e;
   dim3 grid(nz, ngroup);
-  k_plane2<R, MODE, N1, N2><<<grid, OA_PLANE_THREADS, L.total, st>>>((C*)zbuf, nstate, ldl, nlines, lkx, lky, nkx,
+  k_plane2<R, MODE, N1, N2><<<grid, p2_threads<R, MODE>(), L.total, st>>>((C*)zbuf, nstate, ldl, nlines, lkx, lky, nkx,
                                                                      tw, occ, (const R*)vks, rho_part, ngroup, L, E);
   return cudaGetLastError();
 }
