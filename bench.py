@@ -153,18 +153,19 @@ def run_reference(args):
 # GPU arm
 # ----------------------------------------------------------------------------
 
-def time_steps(torch, drv, state, k, before=None):
-    """K native CP steps (oa_gpu_cp_step, CUDA-graph replay) between two
-    CUDA events on the launching stream."""
+def time_steps(torch, drv, state, k, pos_host=None, sync_each=False):
+    """K native CP steps between two CUDA events on the launching stream:
+    one oa_gpu_cp_run call (steps enqueued back to back, CUDA-graph replay,
+    one synchronisation), or K oa_gpu_cp_step calls (one synchronisation per
+    step) when sync_each."""
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     ev0.record(drv.stream)
-    ens = []
-    for _ in range(k):
-        if before:
-            before()
-        ens.append(drv.step_native(state))
+    if sync_each:
+        ens = [drv.step_native(state) for _ in range(k)]
+    else:
+        ens = drv.run_native(state, k, pos_host)
     ev1.record(drv.stream)
     torch.cuda.synchronize()
     return ev0.elapsed_time(ev1) / k, ens
@@ -206,17 +207,19 @@ def run_ours(args):
         barrier()
         ms_64, en_64 = time_steps(torch, d64, st64, args.steps)
         barrier()
-        # end-to-end through the public API: host atom positions in, energies out
-        pos_host = torch.from_numpy(np.ascontiguousarray(sysm.pos)).pin_memory().numpy()
-        def h2d():
-            with torch.cuda.stream(dmx.stream):
-                dmx.ctx.set_atoms(pos_host)
-        ms_e2e, _ = time_steps(torch, dmx, stmx, args.steps, before=h2d)
+        # end-to-end through the public API: host atom positions copied in
+        # before every step, the per-step energy records copied out
+        pos_host = torch.from_numpy(np.repeat(np.ascontiguousarray(sysm.pos)[None], args.steps, axis=0)
+                                    ).pin_memory().numpy()
+        ms_e2e, _ = time_steps(torch, dmx, stmx, args.steps, pos_host=pos_host)
+        barrier()
+        # the same steps with a host synchronisation after each one
+        ms_sync, _ = time_steps(torch, dmx, stmx, args.steps, sync_each=True)
         barrier()
     if ws > 1:
-        t = torch.tensor([ms_mx, ms_64, ms_e2e], device="cuda")
+        t = torch.tensor([ms_mx, ms_64, ms_e2e, ms_sync], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_mx, ms_64, ms_e2e = [float(x) for x in t.tolist()]
+        ms_mx, ms_64, ms_e2e, ms_sync = [float(x) for x in t.tolist()]
 
     # accuracy of the mixed form against FP64 on the same trajectory start
     de = max(abs(total_energy(a) - total_energy(b)) for a, b in zip(en_mx, en_64)) / natm
@@ -253,7 +256,8 @@ def run_ours(args):
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": ws * 1e3 / ms_e2e, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * natm,
-                    "d2h_bytes_per_step": 2 * 16 * 8},
+                    "d2h_bytes_per_step": 20 * 8},
+            "sync_every_step": {"value": ws * 1e3 / ms_sync, "ms_per_step": ms_sync},
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(),
         }

@@ -232,10 +232,26 @@ typedef struct {
  * cp_state_ctrl/gspace.ci:199-324): forces, constraint force, Verlet
  * integration, orthonormalisation, in native code with one host
  * synchronisation at the end.  A PsiV reset triggered by max|S - 2I| >
- * norb_tol runs at the start of the next call.  energies_out (optional,
- * host [11]): EKE EHART EEXT EWALD_RECIP EEXC MUXC FICT_KE ENL, Newton-Schulz
- * iterations, residual, max|S - 2I|. */
+ * norb_tol (Ortho::maxCheck, ortho.C:455-475) is decided on the device and
+ * runs at the start of the next step.  energies_out (optional, host [11]):
+ * EKE EHART EEXT EWALD_RECIP EEXC MUXC FICT_KE ENL, Newton-Schulz
+ * iterations, residual, max|S - 2I|.  Coefficient arrays must be 16-byte
+ * aligned. */
 oa_status oa_gpu_cp_step(oa_ctx *ctx, void *stream, oa_cp_state *state, double *energies_out);
+
+/* nsteps CP dynamics steps enqueued back to back with one host
+ * synchronisation at the end: the loop of GSpaceDriver::computeDynamics
+ * over a trajectory (the reference's per-step energy print,
+ * InstanceController::printEnergy*, main/InstanceController.C:373-490,
+ * becomes one record per step).  pos_host (optional, host
+ * [nsteps][natm][3]) is copied to the atom positions before each step.
+ * energies_out (optional, host [nsteps][11]) as oa_gpu_cp_step's.  When the
+ * Newton-Schulz iteration fails in a step, the call still runs all nsteps
+ * and returns OA_ERR_NOT_CONVERGED or OA_ERR_NONFINITE naming the first
+ * failing step in oa_gpu_last_error(); the state is then that of the last
+ * step. */
+oa_status oa_gpu_cp_run(oa_ctx *ctx, void *stream, oa_cp_state *state, int nsteps, const double *pos_host,
+                        double *energies_out);
 
 /* Allocation-free PairCalculator forward product, for callers that cannot
  * call cudaMalloc (code running during CUDA stream capture, or inside a host

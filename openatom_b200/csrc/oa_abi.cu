@@ -505,6 +505,58 @@ __global__ void k_sym_quarter(const double* A, int n, double* X) {
   if (i < n && j < n) X[(size_t)i * n + j] = 0.25 * (A[(size_t)i * n + j] + A[(size_t)j * n + i]);
 }
 
+__global__ void k_sym_quarter_cond(const double* A, int n, double* X, const int* cond) {
+  if (*cond == 0) return;
+  const int i = blockIdx.y * 16 + threadIdx.y, j = blockIdx.x * 16 + threadIdx.x;
+  if (i < n && j < n) X[(size_t)i * n + j] = 0.25 * (A[(size_t)i * n + j] + A[(size_t)j * n + i]);
+}
+
+__global__ void k_copy_cond(double* __restrict__ dst, const double* __restrict__ src, size_t n, const int* cond) {
+  if (*cond == 0) return;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+__global__ void k_flag_clear(int* flag) { flag[0] = 0; }
+
+cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m, int n, long K, long kx0_cols,
+                         double w_kx0, double alpha, double* part, int nkb, double* C, const int* cond);
+cudaError_t oa_dgemm_bwd(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
+                         const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
+                         double* out, const int* cond);
+
+// The PsiV reset of oa_gpu_psiv_reset plus T = I, enqueued unconditionally
+// but doing its work only when the device flag cond[0] is set; it clears
+// the flag.  Lets the native step decide the reset on the device, so that
+// steps can be enqueued back to back without a host round trip.
+oa_status oa_psiv_reset_cond(oa_ctx* c, cudaStream_t s, const double* psi, double* psi_t, double* vpsi, double* T,
+                             int* cond) {
+  oa_ctx_pc* p = pcx(c);
+  const int n = c->nstate;
+  cudaError_t e = oa_dgemm_fwd(s, psi, vpsi, n, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, p->mat_a, cond);
+  if (e == cudaErrorNotSupported) {
+    oa_set_error("coefficient arrays must be 16-byte aligned for the native step", __FILE__, __LINE__);
+    return OA_ERR_BAD_ARG;
+  }
+  OA_CUDA_TRY(e);
+  dim3 grid((n + 15) / 16, (n + 15) / 16), blk(16, 16);
+  k_sym_quarter_cond<<<grid, blk, 0, s>>>(p->mat_a, n, p->mat_x, cond);
+  OA_CUDA_TRY(cudaGetLastError());
+  e = oa_dgemm_bwd(s, p->mat_x, psi, -1.0, -1.0, p->eye, vpsi, 1.0, n, n, 2L * c->ng, 2L * c->nkx0, p->vtmp, cond);
+  if (e == cudaErrorNotSupported) {
+    oa_set_error("coefficient arrays must be 16-byte aligned for the native step", __FILE__, __LINE__);
+    return OA_ERR_BAD_ARG;
+  }
+  OA_CUDA_TRY(e);
+  const size_t nd = (size_t)n * c->ng * 2;
+  k_copy_cond<<<4 * 148, 256, 0, s>>>(vpsi, p->vtmp, nd, cond);
+  k_copy_cond<<<4 * 148, 256, 0, s>>>(psi_t, psi, nd, cond);
+  k_copy_cond<<<16, 256, 0, s>>>(T, p->eye, (size_t)n * n, cond);
+  k_flag_clear<<<1, 1, 0, s>>>(cond);
+  OA_CUDA_TRY(cudaGetLastError());
+  return OA_OK;
+}
+
 extern "C" oa_status oa_gpu_psiv_reset(oa_ctx* c, void* stream, const double* psi, double* psi_t, double* vpsi) {
   OA_ARG_CHECK(c && psi && psi_t && vpsi, "null argument");
   cudaStream_t s = (cudaStream_t)stream;

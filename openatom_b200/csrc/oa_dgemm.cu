@@ -58,7 +58,8 @@ __device__ __forceinline__ void dg_load_slab(double* dst, const double* __restri
 template <bool SAME, int DG_STAGES>
 __global__ void __launch_bounds__(DG_THREADS, 1)
 k_dgemm_fwd(const double* __restrict__ A, const double* __restrict__ B, int m, int n, long K, long kx0_cols,
-            int n0, int nr, double* __restrict__ part) {
+            int n0, int nr, double* __restrict__ part, const int* __restrict__ cond) {
+  if (cond && *cond == 0) return;
   extern __shared__ __align__(16) double dg_smem[];
   double* As = dg_smem;
   double* Bs = SAME ? dg_smem : dg_smem + DG_STAGES * DG_SLAB;
@@ -135,7 +136,8 @@ k_dgemm_fwd(const double* __restrict__ A, const double* __restrict__ B, int m, i
 
 // C = alpha (w0 sum_{kb < n0} part[kb] + sum_{kb >= n0} part[kb]), fixed order
 __global__ void k_dgemm_fwd_reduce(const double* __restrict__ part, int n0, int nkb, size_t nn, double w0,
-                                   double alpha, double* __restrict__ C) {
+                                   double alpha, double* __restrict__ C, const int* __restrict__ cond) {
+  if (cond && *cond == 0) return;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (size_t)gridDim.x * blockDim.x) {
     double s0 = 0.0, s1 = 0.0;
     for (int k = 0; k < n0; ++k) s0 += part[(size_t)k * nn + i];
@@ -154,8 +156,10 @@ size_t oa_dgemm_fwd_smem(bool same) {
 // copies (odd K, odd kx0_cols or unaligned pointers); the caller then uses
 // the element-wise kernel.  nkb bounds the partials the caller provides
 // (part holds nkb * m * n doubles).
+// cond: optional device flag; when it is 0 at run time the launches do nothing
+// (the conditional PsiV reset of the native step).
 cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m, int n, long K, long kx0_cols,
-                         double w_kx0, double alpha, double* part, int nkb, double* C) {
+                         double w_kx0, double alpha, double* part, int nkb, double* C, const int* cond) {
   if ((K & 1) || (kx0_cols & 1) || (((uintptr_t)A | (uintptr_t)B) & 15) || kx0_cols > K || nkb < 2)
     return cudaErrorNotSupported;
   static const int nsm = [] {
@@ -187,16 +191,16 @@ cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m
   if (same) {
     e = cudaFuncSetAttribute(k_dgemm_fwd<true, DG_STAGES_SAME>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    k_dgemm_fwd<true, DG_STAGES_SAME><<<grid, DG_THREADS, sm, s>>>(A, B, m, n, K, kx0_cols, n0, nr, part);
+    k_dgemm_fwd<true, DG_STAGES_SAME><<<grid, DG_THREADS, sm, s>>>(A, B, m, n, K, kx0_cols, n0, nr, part, cond);
   } else {
     e = cudaFuncSetAttribute(k_dgemm_fwd<false, DG_STAGES_TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    k_dgemm_fwd<false, DG_STAGES_TWO><<<grid, DG_THREADS, sm, s>>>(A, B, m, n, K, kx0_cols, n0, nr, part);
+    k_dgemm_fwd<false, DG_STAGES_TWO><<<grid, DG_THREADS, sm, s>>>(A, B, m, n, K, kx0_cols, n0, nr, part, cond);
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const size_t mn = (size_t)m * n;
-  k_dgemm_fwd_reduce<<<(unsigned)((mn + 255) / 256), 256, 0, s>>>(part, n0, nkb_eff, mn, w_kx0, alpha, C);
+  k_dgemm_fwd_reduce<<<(unsigned)((mn + 255) / 256), 256, 0, s>>>(part, n0, nkb_eff, mn, w_kx0, alpha, C, cond);
   return cudaGetLastError();
 }
 
@@ -249,7 +253,8 @@ template <bool TWO>
 __global__ void __launch_bounds__(DB_THREADS, 2)
 k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double a1_kx0, double a1_rest,
             const double* __restrict__ M2, const double* __restrict__ X2, double a2, int nj, int nk, long ncol,
-            long kx0_cols, double* __restrict__ out) {
+            long kx0_cols, double* __restrict__ out, const int* __restrict__ cond) {
+  if (cond && *cond == 0) return;
   extern __shared__ __align__(16) double db_smem[];
   double* Ms = db_smem;
   double* Xs = db_smem + DB_STAGES * DB_MSLAB;
@@ -331,7 +336,7 @@ k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double
 // 16-byte copies (nj > 128, odd nj or ncol, unaligned pointers).
 cudaError_t oa_dgemm_bwd(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
                          const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
-                         double* out) {
+                         double* out, const int* cond) {
   const uintptr_t al = (uintptr_t)M1 | (uintptr_t)X1 | (uintptr_t)out | (uintptr_t)(M2 ? M2 : M1) |
                        (uintptr_t)(X2 ? X2 : X1);
   if (nj > DB_TJ || (nj & 1) || (ncol & 1) || (al & 15) || nk <= 0 || (M2 && !X2)) return cudaErrorNotSupported;
@@ -341,12 +346,13 @@ cudaError_t oa_dgemm_bwd(cudaStream_t s, const double* M1, const double* X1, dou
   if (M2) {
     e = cudaFuncSetAttribute(k_dgemm_bwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    k_dgemm_bwd<true><<<grid, DB_THREADS, sm, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out);
+    k_dgemm_bwd<true><<<grid, DB_THREADS, sm, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out,
+                                                    cond);
   } else {
     e = cudaFuncSetAttribute(k_dgemm_bwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     k_dgemm_bwd<false><<<grid, DB_THREADS, sm, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols,
-                                                     out);
+                                                     out, cond);
   }
   return cudaGetLastError();
 }

@@ -396,12 +396,12 @@ __global__ void k_sum_partials(const double* __restrict__ part, int n, int strid
 // launchers
 // ---------------------------------------------------------------------------
 cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m, int n, long K, long kx0_cols,
-                         double w_kx0, double alpha, double* part, int nkb, double* C);
+                         double w_kx0, double alpha, double* part, int nkb, double* C, const int* cond);
 
 cudaError_t oa_launch_pc_fwd_mn(cudaStream_t s, const double* A, const double* B, int m, int n, long K,
                                 long kx0_cols, double w_kx0, double alpha, double* part, int nkb, double* C) {
   // pipelined kernel (oa_dgemm.cu) when the operands allow 16-byte copies
-  const cudaError_t e2 = oa_dgemm_fwd(s, A, B, m, n, K, kx0_cols, w_kx0, alpha, part, nkb, C);
+  const cudaError_t e2 = oa_dgemm_fwd(s, A, B, m, n, K, kx0_cols, w_kx0, alpha, part, nkb, C, nullptr);
   if (e2 != cudaErrorNotSupported) return e2;
   const long kchunk = ((K + nkb - 1) / nkb + PC_KS - 1) / PC_KS * PC_KS;
   const int nkb_eff = (int)((K + kchunk - 1) / kchunk);
@@ -421,13 +421,13 @@ cudaError_t oa_launch_pc_fwd(cudaStream_t s, const double* A, const double* B, i
 
 cudaError_t oa_dgemm_bwd(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
                          const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
-                         double* out);
+                         double* out, const int* cond);
 
 cudaError_t oa_launch_pc_bwd_jk(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
                                 const double* M2, const double* X2, double a2, int nj, int nk, long ncol,
                                 long kx0_cols, double* out) {
   // pipelined kernel (oa_dgemm.cu) when the shapes allow 16-byte copies
-  const cudaError_t e2 = oa_dgemm_bwd(s, M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out);
+  const cudaError_t e2 = oa_dgemm_bwd(s, M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out, nullptr);
   if (e2 != cudaErrorNotSupported) return e2;
   dim3 grid((unsigned)((ncol + PC_TM - 1) / PC_TM), (nj + PC_TM - 1) / PC_TM);
   k_pc_bwd_f64<<<grid, 128, 0, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out);

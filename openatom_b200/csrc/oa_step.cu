@@ -1,12 +1,15 @@
-// One whole CP dynamics step in native code: the sequence of
+// Whole CP dynamics steps in native code: the sequence of
 // GSpaceDriver::computeDynamics (src_charm_driver/cp_state_ctrl/gspace.ci:199-324)
-// on one GPU, with a single host synchronisation at the end of the step
-// (energies, Newton-Schulz status, max|S - 2I|).  The steady-state step
-// (iteration > 1, fixed buffers) is captured once into two CUDA graphs
-// (forces .. S, and Psi T + the record copies) replayed around the
-// cooperative Newton-Schulz launch, which stream capture does not accept;
-// a PsiV tolerance reset decided at the end of a step runs eagerly at the
-// start of the next one.
+// on one GPU.  The steady-state step (iteration > 1, fixed buffers) is
+// captured once into two CUDA graphs (PsiV reset .. S, and Psi T + the
+// step record) replayed around the cooperative Newton-Schulz launch, which
+// stream capture does not accept.  Nothing in a step needs the host: the
+// PsiV tolerance check (Ortho::maxCheck, ortho.C:455-475) sets a device
+// flag that the conditional reset at the start of the next step reads, and
+// each step appends its energies and Newton-Schulz status to a device
+// record ring.  oa_gpu_cp_run therefore enqueues many steps and
+// synchronises once; oa_gpu_cp_step is the one-step case.
+#include <stdio.h>
 #include <string.h>
 #include "oa_internal.h"
 
@@ -32,22 +35,35 @@ oa_status oa_gpu_integrate(oa_ctx* ctx, void* stream, const double* force, doubl
 oa_status oa_gpu_psiv_reset(oa_ctx* ctx, void* stream, const double* psi, double* psi_t, double* vpsi);
 }
 
+oa_status oa_psiv_reset_cond(oa_ctx* c, cudaStream_t s, const double* psi, double* psi_t, double* vpsi, double* T,
+                             int* cond);
+
 cudaError_t oa_launch_ortho_ns(cudaStream_t s, const double* S, int n, double bscale, double tol, int max_iter,
                                double* work, double* T, int* status, double* errv, int grid);
 cudaError_t oa_step_ortho_args(oa_ctx* c, double** work, int** status, double** errv, int* grid, double** dev_e,
                                int** h_status, double** h_vals, double** eye);
 
+// per-step record: the 16 energy accumulators, NS iterations, converged,
+// residual, max|S - 2I|
+#define OA_REC 20
+
 struct oa_step_scratch {
   double *F, *F2, *Fnl, *S, *lam, *gam;
-  cudaGraphExec_t exec;   // forces .. S
-  cudaGraphExec_t exec2;  // Psi T + the record copies
-  const void* key[6];
+  int* flag;              // device: [0] PsiV pending, [1] steps recorded, [2] first error code, [3] its step
+  double* ring;           // device: [ring_cap][OA_REC]
+  int ring_cap;
+  double* ring_host;      // pinned copy of the ring
+  int flag_host[4];
+  cudaGraphExec_t exec;   // PsiV reset .. S
+  cudaGraphExec_t exec2;  // Psi T + the step record
+  const void* key[7];
   int key_nterm;
-  double key_dt;
-  int pending_psiv;
+  double key_dt, key_tol;
 };
 
 static oa_step_scratch* step_scratch(oa_ctx* c) { return (oa_step_scratch*)c->step; }
+
+void oa_step_free(oa_ctx* c);
 
 static oa_status ensure_scratch(oa_ctx* c) {
   if (c->step) return OA_OK;
@@ -55,14 +71,55 @@ static oa_status ensure_scratch(oa_ctx* c) {
   if (!s) return OA_ERR_CUDA;
   const size_t cb = (size_t)c->nstate * c->ng * sizeof(double2);
   const size_t mb = (size_t)c->nstate * c->nstate * sizeof(double);
+  c->step = s;  // freed by oa_step_free on failure below or at destroy
   if (cudaMalloc(&s->F, cb) != cudaSuccess || cudaMalloc(&s->F2, cb) != cudaSuccess ||
       cudaMalloc(&s->Fnl, cb) != cudaSuccess || cudaMalloc(&s->S, mb) != cudaSuccess ||
-      cudaMalloc(&s->lam, mb) != cudaSuccess || cudaMalloc(&s->gam, mb) != cudaSuccess) {
+      cudaMalloc(&s->lam, mb) != cudaSuccess || cudaMalloc(&s->gam, mb) != cudaSuccess ||
+      cudaMalloc(&s->flag, 4 * sizeof(int)) != cudaSuccess || cudaMemset(s->flag, 0, 4 * sizeof(int)) != cudaSuccess) {
     oa_set_error("cudaMalloc failed for the step scratch", __FILE__, __LINE__);
+    oa_step_free(c);
     return OA_ERR_CUDA;
   }
-  c->step = s;
   return OA_OK;
+}
+
+// record ring of at least n steps (reallocating drops the captured graphs)
+static oa_status ensure_ring(oa_ctx* c, int n) {
+  oa_step_scratch* s = step_scratch(c);
+  if (s->ring_cap >= n) return OA_OK;
+  int cap = s->ring_cap > 0 ? s->ring_cap : 64;
+  while (cap < n) cap *= 2;
+  if (s->ring) cudaFree(s->ring);
+  if (s->ring_host) cudaFreeHost(s->ring_host);
+  s->ring = nullptr; s->ring_host = nullptr; s->ring_cap = 0;
+  if (s->exec) { cudaGraphExecDestroy(s->exec); s->exec = nullptr; }
+  if (s->exec2) { cudaGraphExecDestroy(s->exec2); s->exec2 = nullptr; }
+  if (cudaMalloc(&s->ring, (size_t)cap * OA_REC * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&s->ring_host, (size_t)cap * OA_REC * sizeof(double)) != cudaSuccess) {
+    oa_set_error("allocation of the step record ring failed", __FILE__, __LINE__);
+    return OA_ERR_CUDA;
+  }
+  s->ring_cap = cap;
+  return OA_OK;
+}
+
+// After Newton-Schulz: the PsiV flag (max|S - 2I| > norb_tol on a good step),
+// the first failing step, and the step record.  One thread.
+__global__ void k_step_check(const int* __restrict__ status, const double* __restrict__ errv,
+                             const double* __restrict__ dev_e, double norb_tol, int* __restrict__ flag,
+                             double* __restrict__ ring, int ring_cap) {
+  const int k = flag[1];
+  const double err = errv[0], smax = errv[1];
+  const int code = (!(err == err) || !(smax == smax)) ? 2 : (status[1] ? 0 : 1);
+  if (code == 0 && smax > norb_tol) flag[0] = 1;
+  if (code != 0 && flag[2] == 0) { flag[2] = code; flag[3] = k; }
+  double* r = ring + (size_t)(k % ring_cap) * OA_REC;
+  for (int i = 0; i < 16; ++i) r[i] = dev_e[i];
+  r[16] = (double)status[0];
+  r[17] = (double)status[1];
+  r[18] = err;
+  r[19] = smax;
+  flag[1] = k + 1;
 }
 
 void oa_step_free(oa_ctx* c) {
@@ -70,8 +127,9 @@ void oa_step_free(oa_ctx* c) {
   if (!s) return;
   if (s->exec) cudaGraphExecDestroy(s->exec);
   if (s->exec2) cudaGraphExecDestroy(s->exec2);
-  void* p[] = {s->F, s->F2, s->Fnl, s->S, s->lam, s->gam};
+  void* p[] = {s->F, s->F2, s->Fnl, s->S, s->lam, s->gam, s->flag, s->ring};
   for (void* q : p) if (q) cudaFree(q);
+  if (s->ring_host) cudaFreeHost(s->ring_host);
   free(s);
   c->step = nullptr;
 }
@@ -82,6 +140,8 @@ void oa_step_free(oa_ctx* c) {
 static oa_status launch_step_a(oa_ctx* c, cudaStream_t s, oa_cp_state* st, int complete_prev) {
   oa_step_scratch* w = step_scratch(c);
   const int nt = st->mixed_nterm;
+  // PsiV reset requested by the previous step's check (no-op otherwise)
+  OA_STEP_TRY(oa_psiv_reset_cond(c, s, st->psi, st->psi_t, st->vpsi, st->T, w->flag));
   // forces on the orthonormal psi (computePsiFandVKS, ParticlePlane, combineForcesGetEke)
   OA_STEP_TRY(oa_gpu_state_fft_fwd(c, s, st->psi, nullptr));
   OA_STEP_TRY(oa_gpu_vks_build(c, s, nullptr));
@@ -115,22 +175,22 @@ static oa_status launch_step_ns(oa_ctx* c, cudaStream_t s, oa_cp_state* st) {
   return OA_OK;
 }
 
-// psi = psi_t T (FP64) and the record copies (part B)
+// psi = psi_t T (FP64), the PsiV check and the step record (part B)
 static oa_status launch_step_b(oa_ctx* c, cudaStream_t s, oa_cp_state* st) {
+  oa_step_scratch* w = step_scratch(c);
   double *work, *errv, *dev_e, *hv, *eye;
   int *status, *hs, grid;
   OA_CUDA_TRY(oa_step_ortho_args(c, &work, &status, &errv, &grid, &dev_e, &hs, &hv, &eye));
+  k_step_check<<<1, 1, 0, s>>>(status, errv, dev_e, st->norb_tol, w->flag, w->ring, w->ring_cap);
+  OA_CUDA_TRY(cudaGetLastError());
   OA_STEP_TRY(oa_gpu_pc_backward(c, s, st->T, st->psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, st->psi));
-  // one record back to the host: energies [16], NS status [2], errv [2]
-  OA_CUDA_TRY(cudaMemcpyAsync(hv, dev_e, 16 * sizeof(double), cudaMemcpyDeviceToHost, s));
-  OA_CUDA_TRY(cudaMemcpyAsync(hs, status, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-  OA_CUDA_TRY(cudaMemcpyAsync(hv + 10, errv, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
   return OA_OK;
 }
 
-extern "C" oa_status oa_gpu_cp_step(oa_ctx* c, void* stream, oa_cp_state* st, double* energies_out) {
-  if (!c || !st || !st->psi || !st->psi_t || !st->vpsi || !st->T) {
-    oa_set_error("null argument", __FILE__, __LINE__);
+static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps, const double* pos_host,
+                           double* energies_out) {
+  if (!c || !st || !st->psi || !st->psi_t || !st->vpsi || !st->T || nsteps < 1) {
+    oa_set_error("null argument or nsteps < 1", __FILE__, __LINE__);
     return OA_ERR_BAD_ARG;
   }
   if (!(st->mixed_nterm == 0 || st->mixed_nterm == 2 || st->mixed_nterm == 3)) {
@@ -138,78 +198,94 @@ extern "C" oa_status oa_gpu_cp_step(oa_ctx* c, void* stream, oa_cp_state* st, do
     return OA_ERR_BAD_ARG;
   }
   OA_STEP_TRY(ensure_scratch(c));
+  OA_STEP_TRY(ensure_ring(c, nsteps));
   cudaStream_t s = (cudaStream_t)stream;
   oa_step_scratch* w = step_scratch(c);
-  double *work, *errv, *dev_e, *hv, *eye;
-  int *status, *hs, grid;
-  OA_CUDA_TRY(oa_step_ortho_args(c, &work, &status, &errv, &grid, &dev_e, &hs, &hv, &eye));
-  if (w->pending_psiv) {
-    OA_STEP_TRY(oa_gpu_psiv_reset(c, s, st->psi, st->psi_t, st->vpsi));
-    OA_CUDA_TRY(cudaMemcpyAsync(st->T, eye, (size_t)c->nstate * c->nstate * sizeof(double),
-                                cudaMemcpyDeviceToDevice, s));
-    w->pending_psiv = 0;
-  }
-  st->iteration += 1;
-  const int complete_prev = st->iteration > 1;
-  const void* key[6] = {st->psi, st->psi_t, st->vpsi, st->T, stream, nullptr};
+  // restart the record count and the error slot; keep a pending PsiV flag
+  OA_CUDA_TRY(cudaMemsetAsync(w->flag + 1, 0, 3 * sizeof(int), s));
+  const void* key[7] = {st->psi, st->psi_t, st->vpsi, st->T, stream, w->ring, nullptr};
   // the legacy default stream cannot be captured: launch eagerly there
   const bool capturable = s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread;
-  bool use_graph = st->use_graph && complete_prev && capturable;
-  if (use_graph) {
-    const bool same = w->exec && w->exec2 && memcmp(key, w->key, sizeof(key)) == 0 &&
-                      w->key_nterm == st->mixed_nterm && w->key_dt == st->dt;
-    if (!same) {
-      if (w->exec) { cudaGraphExecDestroy(w->exec); w->exec = nullptr; }
-      if (w->exec2) { cudaGraphExecDestroy(w->exec2); w->exec2 = nullptr; }
-      for (int part = 0; part < 2; ++part) {
-        cudaGraph_t g = nullptr;
-        OA_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        oa_status r = part == 0 ? launch_step_a(c, s, st, 1) : launch_step_b(c, s, st);
-        cudaError_t ce = cudaStreamEndCapture(s, &g);
-        if (r != OA_OK) { if (g) cudaGraphDestroy(g); return r; }
-        if (ce != cudaSuccess) { oa_set_error(cudaGetErrorString(ce), __FILE__, __LINE__); return OA_ERR_CUDA; }
-        ce = cudaGraphInstantiate(part == 0 ? &w->exec : &w->exec2, g, 0);
-        cudaGraphDestroy(g);
-        if (ce != cudaSuccess) { oa_set_error(cudaGetErrorString(ce), __FILE__, __LINE__); return OA_ERR_CUDA; }
+  for (int k = 0; k < nsteps; ++k) {
+    if (pos_host)
+      OA_CUDA_TRY(cudaMemcpyAsync(c->pos, pos_host + (size_t)k * 3 * c->natm, (size_t)3 * c->natm * sizeof(double),
+                                  cudaMemcpyHostToDevice, s));
+    st->iteration += 1;
+    const int complete_prev = st->iteration > 1;
+    const bool use_graph = st->use_graph && complete_prev && capturable;
+    if (use_graph) {
+      const bool same = w->exec && w->exec2 && memcmp(key, w->key, sizeof(key)) == 0 &&
+                        w->key_nterm == st->mixed_nterm && w->key_dt == st->dt && w->key_tol == st->norb_tol;
+      if (!same) {
+        if (w->exec) { cudaGraphExecDestroy(w->exec); w->exec = nullptr; }
+        if (w->exec2) { cudaGraphExecDestroy(w->exec2); w->exec2 = nullptr; }
+        for (int part = 0; part < 2; ++part) {
+          cudaGraph_t g = nullptr;
+          OA_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+          oa_status r = part == 0 ? launch_step_a(c, s, st, 1) : launch_step_b(c, s, st);
+          cudaError_t ce = cudaStreamEndCapture(s, &g);
+          if (r != OA_OK) { if (g) cudaGraphDestroy(g); return r; }
+          if (ce != cudaSuccess) { oa_set_error(cudaGetErrorString(ce), __FILE__, __LINE__); return OA_ERR_CUDA; }
+          ce = cudaGraphInstantiate(part == 0 ? &w->exec : &w->exec2, g, 0);
+          cudaGraphDestroy(g);
+          if (ce != cudaSuccess) { oa_set_error(cudaGetErrorString(ce), __FILE__, __LINE__); return OA_ERR_CUDA; }
+        }
+        memcpy(w->key, key, sizeof(key));
+        w->key_nterm = st->mixed_nterm;
+        w->key_dt = st->dt;
+        w->key_tol = st->norb_tol;
       }
-      memcpy(w->key, key, sizeof(key));
-      w->key_nterm = st->mixed_nterm;
-      w->key_dt = st->dt;
+      OA_CUDA_TRY(cudaGraphLaunch(w->exec, s));
+      OA_STEP_TRY(launch_step_ns(c, s, st));
+      OA_CUDA_TRY(cudaGraphLaunch(w->exec2, s));
+    } else {
+      OA_STEP_TRY(launch_step_a(c, s, st, complete_prev));
+      OA_STEP_TRY(launch_step_ns(c, s, st));
+      OA_STEP_TRY(launch_step_b(c, s, st));
     }
-    OA_CUDA_TRY(cudaGraphLaunch(w->exec, s));
-    OA_STEP_TRY(launch_step_ns(c, s, st));
-    OA_CUDA_TRY(cudaGraphLaunch(w->exec2, s));
-  } else {
-    OA_STEP_TRY(launch_step_a(c, s, st, complete_prev));
-    OA_STEP_TRY(launch_step_ns(c, s, st));
-    OA_STEP_TRY(launch_step_b(c, s, st));
   }
+  OA_CUDA_TRY(cudaMemcpyAsync(w->ring_host, w->ring, (size_t)nsteps * OA_REC * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+  OA_CUDA_TRY(cudaMemcpyAsync(w->flag_host, w->flag, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
   OA_CUDA_TRY(cudaStreamSynchronize(s));
   // energies: EKE EHART EEXT EWALD EEXC MUXC FICT ENL, then NS iters, residual, smax
-  if (energies_out) {
-    energies_out[0] = hv[OA_E_EKE];
-    energies_out[1] = hv[OA_E_EHART];
-    energies_out[2] = hv[OA_E_EEXT];
-    energies_out[3] = hv[OA_E_EWALD];
-    energies_out[4] = hv[8] + hv[9];
-    energies_out[5] = hv[OA_E_MUXC];
-    energies_out[6] = hv[OA_E_FICT];
-    energies_out[7] = hv[OA_E_ENL];
-    energies_out[8] = (double)hs[0];
-    energies_out[9] = hv[10];
-    energies_out[10] = hv[11];
+  for (int k = 0; k < nsteps; ++k) {
+    const double* hv = w->ring_host + (size_t)k * OA_REC;
+    if (energies_out) {
+      double* eo = energies_out + (size_t)k * 11;
+      eo[0] = hv[OA_E_EKE];
+      eo[1] = hv[OA_E_EHART];
+      eo[2] = hv[OA_E_EEXT];
+      eo[3] = hv[OA_E_EWALD];
+      eo[4] = hv[8] + hv[9];
+      eo[5] = hv[OA_E_MUXC];
+      eo[6] = hv[OA_E_FICT];
+      eo[7] = hv[OA_E_ENL];
+      eo[8] = hv[16];
+      eo[9] = hv[18];
+      eo[10] = hv[19];
+    }
   }
-  st->last_ns_iters = hs[0];
-  st->last_ns_err = hv[10];
-  st->last_smax = hv[11];
-  if (!(hv[10] == hv[10]) || !(hv[11] == hv[11])) {
-    oa_set_error("Newton-Schulz residual is not finite", __FILE__, __LINE__);
-    return OA_ERR_NONFINITE;
+  const double* last = w->ring_host + (size_t)(nsteps - 1) * OA_REC;
+  st->last_ns_iters = (int)last[16];
+  st->last_ns_err = last[18];
+  st->last_smax = last[19];
+  if (w->flag_host[2] != 0) {
+    char msg[160];
+    snprintf(msg, sizeof(msg), "%s in step %d of %d",
+             w->flag_host[2] == 2 ? "Newton-Schulz residual is not finite" : "Newton-Schulz reached max_iter",
+             w->flag_host[3] + 1, nsteps);
+    oa_set_error(msg, __FILE__, __LINE__);
+    return w->flag_host[2] == 2 ? OA_ERR_NONFINITE : OA_ERR_NOT_CONVERGED;
   }
-  if (!hs[1]) {
-    oa_set_error("Newton-Schulz reached max_iter", __FILE__, __LINE__);
-    return OA_ERR_NOT_CONVERGED;
-  }
-  if (hv[11] > st->norb_tol) w->pending_psiv = 1;
   return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_cp_step(oa_ctx* c, void* stream, oa_cp_state* st, double* energies_out) {
+  return run_steps(c, stream, st, 1, nullptr, energies_out);
+}
+
+extern "C" oa_status oa_gpu_cp_run(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps, const double* pos_host,
+                                   double* energies_out) {
+  return run_steps(c, stream, st, nsteps, pos_host, energies_out);
 }

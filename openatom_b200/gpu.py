@@ -46,6 +46,10 @@ class SystemDesc(C.Structure):
     ]
 
 
+STEP_KEYS = ("EKE", "EHART", "EEXT", "EWALD_RECIP", "EEXC", "MUXC", "FICT_KE", "ENL", "ORTHO_ITERS",
+             "ORTHO_ERR", "SMAX")
+
+
 class CPState(C.Structure):
     _fields_ = [
         ("psi_t", _dp), ("psi", _dp), ("vpsi", _dp), ("T", _dp),
@@ -82,6 +86,7 @@ SIGNATURES = {
     "oa_gpu_check": (C.c_int, [_vp, _vp]),
     "oa_gpu_nl_sf": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp]),
     "oa_gpu_cp_step": (C.c_int, [_vp, _vp, C.POINTER(CPState), _dp]),
+    "oa_gpu_cp_run": (C.c_int, [_vp, _vp, C.POINTER(CPState), C.c_int, _dp, _dp]),
     "oa_gpu_ees_init": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp]),
     "oa_gpu_nl_ees": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "oa_gpu_pc_forward_noalloc": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
@@ -316,9 +321,22 @@ class CPContext:
     def cp_step(self, state: CPState) -> dict:
         out = (C.c_double * 11)()
         _check(self._lib.oa_gpu_cp_step(self._h, self._stream(), C.byref(state), out))
-        keys = ("EKE", "EHART", "EEXT", "EWALD_RECIP", "EEXC", "MUXC", "FICT_KE", "ENL", "ORTHO_ITERS",
-                "ORTHO_ERR", "SMAX")
-        return {k: float(v) for k, v in zip(keys, out)}
+        return {k: float(v) for k, v in zip(STEP_KEYS, out)}
+
+    def cp_run(self, state: CPState, nsteps: int, pos_host=None) -> list:
+        """nsteps CP steps enqueued back to back with one synchronisation
+        (oa_gpu_cp_run); pos_host: optional host array [nsteps][natm][3]
+        copied in before each step.  Returns one record per step."""
+        out = np.zeros((nsteps, 11))
+        pp = None
+        if pos_host is not None:
+            pp = np.ascontiguousarray(pos_host, dtype=np.float64)
+            if pp.shape != (nsteps, self.sys.natm, 3):
+                raise ValueError("pos_host must have shape (nsteps, natm, 3)")
+            pp = pp.ctypes.data_as(_dp)
+        _check(self._lib.oa_gpu_cp_run(self._h, self._stream(), C.byref(state), int(nsteps), pp,
+                                       out.ctypes.data_as(_dp)))
+        return [{k: float(v) for k, v in zip(STEP_KEYS, row)} for row in out]
 
     def ees_init(self, scale: float = 1.2, order: int = 6):
         """Enable the EES nonlocal path (grid and dyp from openatom_b200.ees)."""
@@ -408,6 +426,15 @@ class CPDriver:
         self.iteration = state.iteration
         self.last_ortho = (int(en["ORTHO_ITERS"]), en["ORTHO_ERR"], True)
         return en
+
+    def run_native(self, state: CPState, nsteps: int, pos_host=None) -> list:
+        """nsteps native CP steps with one synchronisation (oa_gpu_cp_run),
+        on the driver's own stream."""
+        with self.torch.cuda.stream(self.stream):
+            ens = self.ctx.cp_run(state, nsteps, pos_host)
+        self.iteration = state.iteration
+        self.last_ortho = (int(ens[-1]["ORTHO_ITERS"]), ens[-1]["ORTHO_ERR"], True)
+        return ens
 
     def launches_per_step(self) -> int:
         return self.ctx.sizes()["launches_per_step"]

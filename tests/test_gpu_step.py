@@ -41,3 +41,58 @@ def test_native_step_matches_host_runner(use_graph):
         for k in ("EKE", "EHART", "EEXT", "EEXC", "ENL", "FICT_KE"):
             assert eb[k] == ea[k], (k, ea[k], eb[k])
         assert np.array_equal(a.psi.cpu().numpy(), b.psi.cpu().numpy())
+
+
+def test_native_run_matches_steps_and_psiv():
+    """oa_gpu_cp_run (steps enqueued back to back, one synchronisation)
+    reproduces single steps and the host runner bit for bit, with the PsiV
+    reset decided on the device: norb_tol is set so low that every step
+    triggers it."""
+    from openatom_b200.gpu import CPDriver
+    s = make_system("w8", nstate=16, seed=13, dt=0.5)
+    a = CPDriver(s, "fp64", norb_tol=1e-14)
+    b = CPDriver(s, "fp64", norb_tol=1e-14)
+    c = CPDriver(s, "fp64", norb_tol=1e-14)
+    sb = b.native_state(use_graph=True)
+    sc = c.native_state(use_graph=True)
+    ea = [a.step() for _ in range(5)]
+    eb = [b.step_native(sb) for _ in range(5)]
+    ec = c.run_native(sc, 5)
+    assert a.n_psiv == 5
+    for i in range(5):
+        for k in ("EKE", "EHART", "EEXT", "EEXC", "ENL", "FICT_KE", "SMAX"):
+            assert eb[i][k] == ea[i][k], (i, k, ea[i][k], eb[i][k])
+            assert ec[i][k] == ea[i][k], (i, k, ea[i][k], ec[i][k])
+    for d in (b, c):
+        assert np.array_equal(a.psi.cpu().numpy(), d.psi.cpu().numpy())
+    # the host runner resets psi_t and v at the end of a step, the native
+    # step at the start of the next one: compare the two native runs
+    assert np.array_equal(b.psi_t.cpu().numpy(), c.psi_t.cpu().numpy())
+    assert np.array_equal(b.v.cpu().numpy(), c.v.cpu().numpy())
+
+
+def test_native_run_positions_and_failure():
+    """Per-step host atom positions are copied in before each step; a
+    Newton-Schulz failure is reported with the first failing step."""
+    from openatom_b200.gpu import CPDriver, OaError
+    s = make_system("w2", seed=14, dt=0.5)
+    a = CPDriver(s, "fp64")
+    b = CPDriver(s, "fp64")
+    sa = a.native_state()
+    sb = b.native_state()
+    pos = np.repeat(s.pos[None], 3, axis=0)
+    ea = a.run_native(sa, 3)
+    eb = b.run_native(sb, 3, pos_host=pos)
+    assert [e["EEXT"] for e in ea] == [e["EEXT"] for e in eb]
+    # a moved atom changes the external energy of that step only from then on
+    pos2 = pos.copy()
+    pos2[2, 0, 0] += 0.05
+    c = CPDriver(s, "fp64")
+    ec = c.run_native(c.native_state(), 3, pos_host=pos2)
+    assert ec[1]["EEXT"] == eb[1]["EEXT"]
+    assert abs(ec[2]["EEXT"] - eb[2]["EEXT"]) > 1e-8
+    # one Newton-Schulz iteration cannot reach 1e-15: every step fails, the first is named
+    d = CPDriver(s, "fp64", max_iter=1)
+    sd = d.native_state()
+    with pytest.raises(OaError, match="step 1 of 2"):
+        d.run_native(sd, 2)
