@@ -19,6 +19,7 @@ cudaError_t oa_launch_pc_bwd(cudaStream_t s, const double* M1, const double* X1,
                              double* out);
 cudaError_t oa_launch_small_gemm(cudaStream_t s, const double* A, const double* B, int n, double alpha, double* C);
 int oa_ns_grid(int n, int device);
+int oa_ns_cluster_size(int n);
 cudaError_t oa_launch_ortho_ns(cudaStream_t s, const double* S, int n, double bscale, double tol, int max_iter,
                                double* work, double* T, int* status, double* errv, int grid);
 cudaError_t oa_launch_integrate(cudaStream_t s, const double2* F, double2* V, double2* P, const double* cmass,
@@ -65,7 +66,8 @@ struct oa_ctx_pc {
   double* part;      // split-K partials
   int nkb;
   double* ns_work;   // 5 n^2 + grid
-  int ns_grid;
+  int ns_grid;        // cooperative Newton-Schulz blocks
+  int ns_cluster;     // cluster Newton-Schulz size (0: use the cooperative kernel)
   int* ns_status;    // [2] device
   double* ns_err;    // [1] device
   int* partner;      // [nkx0_red]
@@ -93,6 +95,13 @@ struct oa_ctx_full {
 };
 
 static oa_ctx_pc* pcx(oa_ctx* c) { return &reinterpret_cast<oa_ctx_full*>(c)->pc; }
+
+// launch grid argument of oa_launch_ortho_ns: -cluster size for the cluster
+// kernel, else the cooperative grid
+static int ns_launch_grid(const oa_ctx_pc* p) { return p->ns_cluster > 0 ? -p->ns_cluster : p->ns_grid; }
+
+// whether the Newton-Schulz launch can be captured in a CUDA graph
+int oa_ns_capturable(oa_ctx* c) { return pcx(c)->ns_cluster > 0; }
 
 static bool make_plan(int n, OaFftPlan* p) {
   p->n = n;
@@ -264,7 +273,8 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     p->nkb = 160;  // split-K partials: about one CTA per SM for a 128 x 128 product
     TRY(cudaMalloc(&p->part, (size_t)p->nkb * d->nstate * d->nstate * sizeof(double)));
     p->ns_grid = oa_ns_grid(d->nstate, c->device);
-    TRY(cudaMalloc(&p->ns_work, ((size_t)5 * d->nstate * d->nstate + p->ns_grid + 8) * sizeof(double)));
+    p->ns_cluster = oa_ns_cluster_size(d->nstate);
+    TRY(cudaMalloc(&p->ns_work, ((size_t)5 * d->nstate * d->nstate + p->ns_grid + 32) * sizeof(double)));
     TRY(cudaMalloc(&p->ns_status, 4 * sizeof(int)));
     TRY(cudaMalloc(&p->ns_err, 2 * sizeof(double)));
     p->ke_nblk = 2 * nsm;
@@ -431,7 +441,7 @@ extern "C" oa_status oa_gpu_ortho_invsqrt(oa_ctx* c, void* stream, const double*
   cudaStream_t s = (cudaStream_t)stream;
   oa_ctx_pc* p = pcx(c);
   OA_CUDA_TRY(oa_launch_ortho_ns(s, S, c->nstate, 0.5, tol, max_iter, p->ns_work, T, p->ns_status, p->ns_err,
-                                 p->ns_grid));
+                                 ns_launch_grid(p)));
   OA_CUDA_TRY(cudaMemcpyAsync(p->h_status, p->ns_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
   OA_CUDA_TRY(cudaMemcpyAsync(p->h_vals, p->ns_err, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
   OA_CUDA_TRY(cudaStreamSynchronize(s));
@@ -614,7 +624,8 @@ extern "C" oa_status oa_gpu_time_kernels(oa_ctx* c, void* stream, const double* 
     OA_TIME(6, oa_launch_pc_fwd(s, psi, psi, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, S));
     OA_TIME(7, oa_launch_pc_bwd(s, p->eye, psi, -0.5, -1.0, p->eye, psi, 1.0, n, 2L * c->ng, 2L * c->nkx0,
                                 p->vtmp));
-    OA_TIME(8, oa_launch_ortho_ns(s, S, n, 0.5, 1e-15, 1000, p->ns_work, T, p->ns_status, p->ns_err, p->ns_grid));
+    OA_TIME(8, oa_launch_ortho_ns(s, S, n, 0.5, 1e-15, 1000, p->ns_work, T, p->ns_status, p->ns_err,
+                                  ns_launch_grid(p)));
 #undef OA_TIME
   }
   for (int k = 0; k < 9; ++k) ms_out[k] = acc[k] / reps;
@@ -710,7 +721,7 @@ extern "C" oa_status oa_gpu_nl_sf(oa_ctx* c, void* stream, const double* psi, in
 cudaError_t oa_step_ortho_args(oa_ctx* c, double** work, int** status, double** errv, int* grid, double** dev_e,
                                int** h_status, double** h_vals, double** eye) {
   oa_ctx_pc* p = pcx(c);
-  *work = p->ns_work; *status = p->ns_status; *errv = p->ns_err; *grid = p->ns_grid; *dev_e = p->dev_e;
+  *work = p->ns_work; *status = p->ns_status; *errv = p->ns_err; *grid = ns_launch_grid(p); *dev_e = p->dev_e;
   *h_status = p->h_status; *h_vals = p->h_vals; *eye = p->eye;
   return cudaSuccess;
 }

@@ -1,0 +1,225 @@
+// Newton-Schulz S^-1/2 on one thread-block cluster (Ortho, ortho.C:109-266,
+// 848-971; cp_lowdin.C:180-265), for up to 128 states:
+//   B = S bscale, A = I; repeat { C = 3I - A B; B <- B C / 2; A <- C A / 2;
+//   err = sqrt(sum (A_old - A_new)^2 / n^2) } until err <= tol or max_iter.
+// The cluster's CTAs own row blocks of A, B and C (global memory, L2
+// resident); each product is a row block times a whole matrix, staged in
+// shared memory and multiplied with FP64 tensor-core MMAs (m8n8k4).  The
+// phases are separated by cluster barriers, so the kernel is an ordinary
+// (graph-capturable) launch; every CTA takes the same convergence decision
+// from the same partial sums in the same order.
+#include <cooperative_groups.h>
+#include "oa_internal.h"
+
+namespace cg = cooperative_groups;
+
+#define NSC_THREADS 256
+#define NSC_MAXN 128
+
+__device__ __forceinline__ void nsc_dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void nsc_cp16(void* smem, const void* gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int nb = valid ? 16 : 0;  // src-size 0: zero fill
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" :: "r"(sa), "l"(gmem), "r"(nb));
+}
+
+// Z[r0 .. r0+R) = alpha X[r0 .. r0+R) Y + diag I, n x n row-major in global
+// memory; rows and columns padded to npad (multiple of 8) with zeros in
+// shared memory.  err (optional): sum over the block of (Aold - Z)^2.
+__device__ void nsc_gemm_rows(const double* __restrict__ X, const double* __restrict__ Y, int n, int npad, int r0,
+                              int R, double alpha, double diag, double* __restrict__ Z, double* Xs, double* Ys,
+                              const double* __restrict__ Aold, double* err) {
+  const int ld = npad + 4;
+  __syncthreads();  // the previous product is done with Xs / Ys
+  // 16-byte asynchronous copies (n even), zero-filled outside n x n
+  const int pr = npad / 2;
+  const int rx = (R + 7) & ~7;
+  for (int i = threadIdx.x; i < rx * pr; i += blockDim.x) {
+    const int r = i / pr, k = (i - r * pr) * 2;
+    const bool v = (r < R) && (r0 + r < n) && (k < n);
+    nsc_cp16(Xs + r * ld + k, v ? X + (size_t)(r0 + r) * n + k : X, v);
+  }
+  for (int i = threadIdx.x; i < npad * pr; i += blockDim.x) {
+    const int k = i / pr, j = (i - k * pr) * 2;
+    const bool v = (k < n) && (j < n);
+    nsc_cp16(Ys + k * ld + j, v ? Y + (size_t)k * n + j : Y, v);
+  }
+  asm volatile("cp.async.commit_group;\n" ::);
+  asm volatile("cp.async.wait_group 0;\n" ::);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rt_n = (R + 7) / 8, ct_n = npad / 8;
+  double e = 0.0;
+  for (int t = warp; t < rt_n * ct_n; t += NSC_THREADS / 32) {
+    const int rt = t % rt_n, ct = t / rt_n;
+    double d0 = 0.0, d1 = 0.0;
+    for (int k4 = 0; k4 < npad; k4 += 4) {
+      const double a = Xs[(rt * 8 + (lane >> 2)) * ld + k4 + (lane & 3)];
+      const double b = Ys[(k4 + (lane & 3)) * ld + ct * 8 + (lane >> 2)];
+      nsc_dmma(d0, d1, a, b);
+    }
+    const int i = r0 + rt * 8 + (lane >> 2);
+    const int j = ct * 8 + 2 * (lane & 3);
+    if (rt * 8 + (lane >> 2) < R && i < n) {
+      if (j < n) {
+        const double v = alpha * d0 + (i == j ? diag : 0.0);
+        if (Aold) { const double d = __ldcg(Aold + (size_t)i * n + j) - v; e += d * d; }
+        Z[(size_t)i * n + j] = v;
+      }
+      if (j + 1 < n) {
+        const double v = alpha * d1 + (i == j + 1 ? diag : 0.0);
+        if (Aold) { const double d = __ldcg(Aold + (size_t)i * n + j + 1) - v; e += d * d; }
+        Z[(size_t)i * n + j + 1] = v;
+      }
+    }
+  }
+  if (err) *err += e;
+}
+
+// deterministic block sum (valid in every thread)
+__device__ double nsc_block_sum(double v, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < NSC_THREADS / 32; ++w) s += sh[w];
+  return s;
+}
+
+__device__ double nsc_block_max(double v, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < NSC_THREADS / 32; ++w) s = fmax(s, sh[w]);
+  return s;
+}
+
+__global__ void __launch_bounds__(NSC_THREADS)
+k_ortho_ns_cluster(const double* __restrict__ S, int n, double bscale, double tol, int max_iter,
+                   double* __restrict__ A0, double* __restrict__ A1, double* __restrict__ B0,
+                   double* __restrict__ B1, double* __restrict__ Cm, double* __restrict__ errpart,
+                   double* __restrict__ T, int* __restrict__ status, double* __restrict__ errv) {
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) double nsc_smem[];
+  __shared__ double sh[NSC_THREADS / 32];
+  const int ncta = (int)cl.num_blocks();
+  const int me = (int)cl.block_rank();
+  const int npad = (n + 7) & ~7;
+  const int R = (((n + ncta - 1) / ncta) + 7) & ~7;  // rows per CTA, multiple of 8
+  const int r0 = me * R;
+  const int nr = max(0, min(R, n - r0));
+  double* Xs = nsc_smem;
+  double* Ys = nsc_smem + (size_t)R * (npad + 4);
+  const size_t nn = (size_t)n * n;
+  // init: A = I, B = S bscale on the own rows; max |S - I/bscale|
+  double dmax = 0.0;
+  for (int i = threadIdx.x; i < nr * n; i += blockDim.x) {
+    const int r = r0 + i / n, c = i % n;
+    const size_t o = (size_t)r * n + c;
+    A0[o] = (r == c) ? 1.0 : 0.0;
+    B0[o] = S[o] * bscale;
+    dmax = fmax(dmax, fabs(S[o] - ((r == c) ? 1.0 / bscale : 0.0)));
+  }
+  dmax = nsc_block_max(dmax, sh);
+  if (threadIdx.x == 0) errpart[me] = dmax;
+  __threadfence();
+  cl.sync();
+  if (me == 0 && threadIdx.x == 0) {
+    double m = 0.0;
+    for (int b = 0; b < ncta; ++b) m = fmax(m, __ldcg(errpart + b));
+    errv[1] = m;
+  }
+  __threadfence();
+  cl.sync();  // errpart is reused below
+  double* A = A0; double* An = A1; double* B = B0; double* Bn = B1;
+  int it = 0;
+  double err = 1.0;
+  while (true) {
+    // C = 3I - A B (own rows)
+    nsc_gemm_rows(A, B, n, npad, r0, nr, -1.0, 3.0, Cm, Xs, Ys, nullptr, nullptr);
+    __threadfence();
+    cl.sync();
+    // Bn = B C / 2 ; An = C A / 2 (own rows), with the error partial
+    double e = 0.0;
+    nsc_gemm_rows(B, Cm, n, npad, r0, nr, 0.5, 0.0, Bn, Xs, Ys, nullptr, nullptr);
+    nsc_gemm_rows(Cm, A, n, npad, r0, nr, 0.5, 0.0, An, Xs, Ys, A, &e);
+    e = nsc_block_sum(e, sh);
+    if (threadIdx.x == 0) errpart[me] = e;
+    __threadfence();
+    cl.sync();
+    ++it;
+    double ssum = 0.0;
+    for (int b = 0; b < ncta; ++b) ssum += __ldcg(errpart + b);
+    err = sqrt(ssum / (double)nn);
+    const bool done = !(err > tol && it < max_iter);
+    { double* t = A; A = An; An = t; t = B; B = Bn; Bn = t; }
+    if (done) break;
+    // errpart is rewritten only after the next cluster barrier (after the
+    // C product), by which time every CTA has read it
+  }
+  for (int i = threadIdx.x; i < nr * n; i += blockDim.x) {
+    const size_t o = (size_t)r0 * n + i;
+    T[o] = A[o];
+  }
+  if (me == 0 && threadIdx.x == 0) {
+    status[0] = it;
+    status[1] = (err <= tol) ? 1 : 0;
+    errv[0] = err;
+  }
+}
+
+// Cluster size for the Newton-Schulz kernel on this device (16 where the
+// device allows non-portable clusters of 16 with the shared memory needed,
+// else 8); 0 when n is too large for it.
+int oa_ns_cluster_size(int n) {
+  if (n < 2 || n > NSC_MAXN || (n & 1)) return 0;  // 16-byte row copies need even n
+  const int npad = (n + 7) & ~7;
+  for (int cs = 16; cs >= 8; cs /= 2) {
+    const int R = (((n + cs - 1) / cs) + 7) & ~7;
+    const size_t sm = ((size_t)R * (npad + 4) + (size_t)npad * (npad + 4)) * sizeof(double);
+    if (cudaFuncSetAttribute(k_ortho_ns_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+      continue;
+    if (cs > 8 && cudaFuncSetAttribute(k_ortho_ns_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                      cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(cs); cfg.blockDim = dim3(NSC_THREADS); cfg.dynamicSmemBytes = sm;
+    cfg.attrs = at; cfg.numAttrs = 1;
+    int ncl = 0;
+    if (cudaOccupancyMaxActiveClusters(&ncl, (void*)k_ortho_ns_cluster, &cfg) == cudaSuccess && ncl >= 1) return cs;
+    cudaGetLastError();
+  }
+  return 0;
+}
+
+cudaError_t oa_launch_ortho_ns_cluster(cudaStream_t s, const double* S, int n, double bscale, double tol,
+                                       int max_iter, double* work, double* T, int* status, double* errv, int cs) {
+  const size_t nn = (size_t)n * n;
+  double* A0 = work; double* A1 = A0 + nn; double* B0 = A1 + nn; double* B1 = B0 + nn; double* Cm = B1 + nn;
+  double* errpart = Cm + nn;
+  const int npad = (n + 7) & ~7;
+  const int R = (((n + cs - 1) / cs) + 7) & ~7;
+  const size_t sm = ((size_t)R * (npad + 4) + (size_t)npad * (npad + 4)) * sizeof(double);
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cs; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(cs); cfg.blockDim = dim3(NSC_THREADS); cfg.dynamicSmemBytes = sm; cfg.stream = s;
+  cfg.attrs = at; cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_ortho_ns_cluster, S, n, bscale, tol, max_iter, A0, A1, B0, B1, Cm, errpart, T,
+                            status, errv);
+}

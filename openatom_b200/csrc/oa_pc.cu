@@ -459,8 +459,14 @@ int oa_ns_grid(int n, int device) {
   return g;
 }
 
+cudaError_t oa_launch_ortho_ns_cluster(cudaStream_t s, const double* S, int n, double bscale, double tol,
+                                       int max_iter, double* work, double* T, int* status, double* errv, int cs);
+
+// grid > 0: cooperative kernel on grid blocks; grid < 0: the cluster kernel
+// (oa_ns.cu) on a cluster of -grid blocks
 cudaError_t oa_launch_ortho_ns(cudaStream_t s, const double* S, int n, double bscale, double tol, int max_iter,
                                double* work /* 5 n^2 + grid */, double* T, int* status, double* errv, int grid) {
+  if (grid < 0) return oa_launch_ortho_ns_cluster(s, S, n, bscale, tol, max_iter, work, T, status, errv, -grid);
   const size_t nn = (size_t)n * n;
   double* A0 = work; double* A1 = A0 + nn; double* B0 = A1 + nn; double* B1 = B0 + nn; double* Cm = B1 + nn;
   double* errpart = Cm + nn;

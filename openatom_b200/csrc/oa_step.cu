@@ -1,9 +1,10 @@
 // Whole CP dynamics steps in native code: the sequence of
 // GSpaceDriver::computeDynamics (src_charm_driver/cp_state_ctrl/gspace.ci:199-324)
 // on one GPU.  The steady-state step (iteration > 1, fixed buffers) is
-// captured once into two CUDA graphs (PsiV reset .. S, and Psi T + the
-// step record) replayed around the cooperative Newton-Schulz launch, which
-// stream capture does not accept.  Nothing in a step needs the host: the
+// captured once into one CUDA graph; with more states than the cluster
+// Newton-Schulz kernel takes, into two graphs (PsiV reset .. S, and Psi T +
+// the step record) replayed around the cooperative Newton-Schulz launch,
+// which stream capture does not accept.  Nothing in a step needs the host: the
 // PsiV tolerance check (Ortho::maxCheck, ortho.C:455-475) sets a device
 // flag that the conditional reset at the start of the next step reads, and
 // each step appends its energies and Newton-Schulz status to a device
@@ -35,6 +36,7 @@ oa_status oa_gpu_integrate(oa_ctx* ctx, void* stream, const double* force, doubl
 oa_status oa_gpu_psiv_reset(oa_ctx* ctx, void* stream, const double* psi, double* psi_t, double* vpsi);
 }
 
+int oa_ns_capturable(oa_ctx* c);
 oa_status oa_psiv_reset_cond(oa_ctx* c, cudaStream_t s, const double* psi, double* psi_t, double* vpsi, double* T,
                              int* cond);
 
@@ -206,6 +208,9 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
   const void* key[7] = {st->psi, st->psi_t, st->vpsi, st->T, stream, w->ring, nullptr};
   // the legacy default stream cannot be captured: launch eagerly there
   const bool capturable = s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread;
+  // the cluster Newton-Schulz kernel is an ordinary launch: then the whole
+  // step is one graph; the cooperative one splits it in two
+  const bool ns_in_graph = oa_ns_capturable(c) != 0;
   for (int k = 0; k < nsteps; ++k) {
     if (pos_host)
       OA_CUDA_TRY(cudaMemcpyAsync(c->pos, pos_host + (size_t)k * 3 * c->natm, (size_t)3 * c->natm * sizeof(double),
@@ -214,15 +219,22 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
     const int complete_prev = st->iteration > 1;
     const bool use_graph = st->use_graph && complete_prev && capturable;
     if (use_graph) {
-      const bool same = w->exec && w->exec2 && memcmp(key, w->key, sizeof(key)) == 0 &&
+      const bool same = w->exec && (ns_in_graph || w->exec2) && memcmp(key, w->key, sizeof(key)) == 0 &&
                         w->key_nterm == st->mixed_nterm && w->key_dt == st->dt && w->key_tol == st->norb_tol;
       if (!same) {
         if (w->exec) { cudaGraphExecDestroy(w->exec); w->exec = nullptr; }
         if (w->exec2) { cudaGraphExecDestroy(w->exec2); w->exec2 = nullptr; }
-        for (int part = 0; part < 2; ++part) {
+        for (int part = 0; part < (ns_in_graph ? 1 : 2); ++part) {
           cudaGraph_t g = nullptr;
           OA_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-          oa_status r = part == 0 ? launch_step_a(c, s, st, 1) : launch_step_b(c, s, st);
+          oa_status r = OA_OK;
+          if (ns_in_graph) {
+            r = launch_step_a(c, s, st, 1);
+            if (r == OA_OK) r = launch_step_ns(c, s, st);
+            if (r == OA_OK) r = launch_step_b(c, s, st);
+          } else {
+            r = part == 0 ? launch_step_a(c, s, st, 1) : launch_step_b(c, s, st);
+          }
           cudaError_t ce = cudaStreamEndCapture(s, &g);
           if (r != OA_OK) { if (g) cudaGraphDestroy(g); return r; }
           if (ce != cudaSuccess) { oa_set_error(cudaGetErrorString(ce), __FILE__, __LINE__); return OA_ERR_CUDA; }
@@ -236,8 +248,10 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
         w->key_tol = st->norb_tol;
       }
       OA_CUDA_TRY(cudaGraphLaunch(w->exec, s));
-      OA_STEP_TRY(launch_step_ns(c, s, st));
-      OA_CUDA_TRY(cudaGraphLaunch(w->exec2, s));
+      if (!ns_in_graph) {
+        OA_STEP_TRY(launch_step_ns(c, s, st));
+        OA_CUDA_TRY(cudaGraphLaunch(w->exec2, s));
+      }
     } else {
       OA_STEP_TRY(launch_step_a(c, s, st, complete_prev));
       OA_STEP_TRY(launch_step_ns(c, s, st));
