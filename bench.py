@@ -251,7 +251,10 @@ def run_ours(args):
             "fp64": {"value": ws * 1e3 / ms_64, "ms_per_step": ms_64},
             "mixed_over_fp64": ms_64 / ms_mx,
             "dE_per_atom_max": de,
-            "ortho": {"iters": s_err[0], "residual": s_err[1], "psiv_resets_fp64": None},
+            "ortho": {"iters": s_err[0], "residual": s_err[1],
+                      "smax_max": max(e["SMAX"] for e in en_mx),
+                      "psiv_resets": sum(1 for e in en_mx if e["SMAX"] > dmx.norb_tol),
+                      "psiv_resets_fp64": sum(1 for e in en_64 if e["SMAX"] > d64.norb_tol)},
             "kernel_ms": kt, "kernel_ms_fp64": kt64,
             "roofline": roof,
             "cpu_baseline": cpu,

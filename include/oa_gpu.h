@@ -231,9 +231,9 @@ typedef struct {
 /* One whole CP dynamics step (GSpaceDriver::computeDynamics,
  * cp_state_ctrl/gspace.ci:199-324): forces, constraint force, Verlet
  * integration, orthonormalisation, in native code with one host
- * synchronisation at the end.  A PsiV reset triggered by max|S - 2I| >
+ * synchronisation at the end.  The PsiV reset triggered by max|S - 2I| >
  * norb_tol (Ortho::maxCheck, ortho.C:455-475) is decided on the device and
- * runs at the start of the next step.  energies_out (optional, host [11]):
+ * runs at the end of the step, as oa_gpu_psiv_reset would.  energies_out (optional, host [11]):
  * EKE EHART EEXT EWALD_RECIP EEXC MUXC FICT_KE ENL, Newton-Schulz
  * iterations, residual, max|S - 2I|.  Coefficient arrays must be 16-byte
  * aligned. */

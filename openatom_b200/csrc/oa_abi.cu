@@ -516,7 +516,7 @@ __global__ void k_sym_quarter(const double* A, int n, double* X) {
 }
 
 __global__ void k_sym_quarter_cond(const double* A, int n, double* X, const int* cond) {
-  if (*cond == 0) return;
+  if (cond && *cond == 0) return;
   const int i = blockIdx.y * 16 + threadIdx.y, j = blockIdx.x * 16 + threadIdx.x;
   if (i < n && j < n) X[(size_t)i * n + j] = 0.25 * (A[(size_t)i * n + j] + A[(size_t)j * n + i]);
 }
@@ -531,38 +531,52 @@ __global__ void k_flag_clear(int* flag) { flag[0] = 0; }
 
 cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m, int n, long K, long kx0_cols,
                          double w_kx0, double alpha, double* part, int nkb, double* C, const int* cond);
-cudaError_t oa_dgemm_bwd(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
-                         const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
-                         double* out, const int* cond);
+cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
+                            const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
+                            double* out, const int* cond, const double* yadd, double* out2, const int* cond2);
 
-// The PsiV reset of oa_gpu_psiv_reset plus T = I, enqueued unconditionally
-// but doing its work only when the device flag cond[0] is set; it clears
-// the flag.  Lets the native step decide the reset on the device, so that
-// steps can be enqueued back to back without a host round trip.
-oa_status oa_psiv_reset_cond(oa_ctx* c, cudaStream_t s, const double* psi, double* psi_t, double* vpsi, double* T,
-                             int* cond) {
+#define OA_STEP_CHECK(x) do { const oa_status st_ = (x); if (st_ != OA_OK) return st_; } while (0)
+
+#define OA_ALIGN_TRY(x)                                                                       \
+  do {                                                                                        \
+    const cudaError_t e_ = (x);                                                               \
+    if (e_ == cudaErrorNotSupported) {                                                        \
+      oa_set_error("coefficient arrays must be 16-byte aligned", __FILE__, __LINE__);         \
+      return OA_ERR_BAD_ARG;                                                                  \
+    }                                                                                         \
+    OA_CUDA_TRY(e_);                                                                          \
+  } while (0)
+
+// Velocity part of the PsiV reset (CP_State_GSpacePlane.C:3590-3600,
+// 3750-3760 with the orthoT velocity projection): X = sym(psi v^T) / 4 with
+// the S weights, v <- v - X psi (in place).  cond: optional device flag; the
+// launches do nothing when it is 0.
+static oa_status psiv_velocity(oa_ctx* c, cudaStream_t s, const double* psi, double* vpsi, const int* cond) {
   oa_ctx_pc* p = pcx(c);
   const int n = c->nstate;
-  cudaError_t e = oa_dgemm_fwd(s, psi, vpsi, n, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, p->mat_a, cond);
-  if (e == cudaErrorNotSupported) {
-    oa_set_error("coefficient arrays must be 16-byte aligned for the native step", __FILE__, __LINE__);
-    return OA_ERR_BAD_ARG;
-  }
-  OA_CUDA_TRY(e);
+  OA_ALIGN_TRY(oa_dgemm_fwd(s, psi, vpsi, n, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, p->mat_a, cond));
   dim3 grid((n + 15) / 16, (n + 15) / 16), blk(16, 16);
   k_sym_quarter_cond<<<grid, blk, 0, s>>>(p->mat_a, n, p->mat_x, cond);
   OA_CUDA_TRY(cudaGetLastError());
-  e = oa_dgemm_bwd(s, p->mat_x, psi, -1.0, -1.0, p->eye, vpsi, 1.0, n, n, 2L * c->ng, 2L * c->nkx0, p->vtmp, cond);
-  if (e == cudaErrorNotSupported) {
-    oa_set_error("coefficient arrays must be 16-byte aligned for the native step", __FILE__, __LINE__);
-    return OA_ERR_BAD_ARG;
-  }
-  OA_CUDA_TRY(e);
-  const size_t nd = (size_t)n * c->ng * 2;
-  k_copy_cond<<<4 * 148, 256, 0, s>>>(vpsi, p->vtmp, nd, cond);
-  k_copy_cond<<<4 * 148, 256, 0, s>>>(psi_t, psi, nd, cond);
-  k_copy_cond<<<16, 256, 0, s>>>(T, p->eye, (size_t)n * n, cond);
-  k_flag_clear<<<1, 1, 0, s>>>(cond);
+  OA_ALIGN_TRY(oa_dgemm_bwd_ex(s, p->mat_x, psi, -1.0, -1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0,
+                               vpsi, cond, vpsi, nullptr, nullptr));
+  return OA_OK;
+}
+
+// psi = psi_t T (FP64), also written to psi_t when the PsiV flag is set;
+// then, under the flag, the velocity projection and T = I, and the flag is
+// cleared.  The native step's orthonormalisation and PsiV reset
+// (Ortho::maxCheck, ortho.C:455-475): same results as oa_gpu_pc_backward
+// followed by oa_gpu_psiv_reset, decided on the device.
+oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* psi_t, double* psi, double* vpsi,
+                            double* Tout, int* flag) {
+  oa_ctx_pc* p = pcx(c);
+  const int n = c->nstate;
+  OA_ALIGN_TRY(oa_dgemm_bwd_ex(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, psi,
+                               nullptr, nullptr, psi_t, flag));
+  OA_STEP_CHECK(psiv_velocity(c, s, psi, vpsi, flag));
+  k_copy_cond<<<16, 256, 0, s>>>(Tout, p->eye, (size_t)n * n, flag);
+  k_flag_clear<<<1, 1, 0, s>>>(flag);
   OA_CUDA_TRY(cudaGetLastError());
   return OA_OK;
 }
@@ -570,16 +584,8 @@ oa_status oa_psiv_reset_cond(oa_ctx* c, cudaStream_t s, const double* psi, doubl
 extern "C" oa_status oa_gpu_psiv_reset(oa_ctx* c, void* stream, const double* psi, double* psi_t, double* vpsi) {
   OA_ARG_CHECK(c && psi && psi_t && vpsi, "null argument");
   cudaStream_t s = (cudaStream_t)stream;
-  oa_ctx_pc* p = pcx(c);
-  const int n = c->nstate;
-  OA_CUDA_TRY(oa_launch_pc_fwd(s, psi, vpsi, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, p->mat_a));
-  dim3 grid((n + 15) / 16, (n + 15) / 16), blk(16, 16);
-  k_sym_quarter<<<grid, blk, 0, s>>>(p->mat_a, n, p->mat_x);
-  OA_CUDA_TRY(cudaGetLastError());
-  OA_CUDA_TRY(oa_launch_pc_bwd(s, p->mat_x, psi, -1.0, -1.0, p->eye, vpsi, 1.0, n, 2L * c->ng, 2L * c->nkx0,
-                               p->vtmp));
-  const size_t bytes = (size_t)n * c->ng * sizeof(double2);
-  OA_CUDA_TRY(cudaMemcpyAsync(vpsi, p->vtmp, bytes, cudaMemcpyDeviceToDevice, s));
+  OA_STEP_CHECK(psiv_velocity(c, s, psi, vpsi, nullptr));
+  const size_t bytes = (size_t)c->nstate * c->ng * sizeof(double2);
   OA_CUDA_TRY(cudaMemcpyAsync(psi_t, psi, bytes, cudaMemcpyDeviceToDevice, s));
   return OA_OK;
 }

@@ -249,12 +249,18 @@ __device__ __forceinline__ void db_load_slab(double* ms, double* xs, const doubl
   }
 }
 
+// Epilogue options: yadd (optional) adds yadd[j][c] to the result (it may
+// be the output array itself: each element is read and written by one
+// thread); out2 (optional) receives a second copy of the result when
+// *cond2 != 0.
 template <bool TWO>
 __global__ void __launch_bounds__(DB_THREADS, 2)
 k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double a1_kx0, double a1_rest,
             const double* __restrict__ M2, const double* __restrict__ X2, double a2, int nj, int nk, long ncol,
-            long kx0_cols, double* __restrict__ out, const int* __restrict__ cond) {
+            long kx0_cols, double* out, const int* __restrict__ cond, const double* yadd, double* __restrict__ out2,
+            const int* __restrict__ cond2) {
   if (cond && *cond == 0) return;
+  const bool dual = out2 && *cond2 != 0;
   extern __shared__ __align__(16) double db_smem[];
   double* Ms = db_smem;
   double* Xs = db_smem + DB_STAGES * DB_MSLAB;
@@ -323,10 +329,17 @@ k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
       const long c = c0 + wc + b * 8 + 2 * (lane & 3);
+      const size_t o = (size_t)j * ncol + c;
       if (c + 1 < ncol) {
-        *(double2*)(out + (size_t)j * ncol + c) = make_double2(acc[a][b][0], acc[a][b][1]);
+        double2 v = make_double2(acc[a][b][0], acc[a][b][1]);
+        if (yadd) { const double2 y = *(const double2*)(yadd + o); v.x += y.x; v.y += y.y; }
+        *(double2*)(out + o) = v;
+        if (dual) *(double2*)(out2 + o) = v;
       } else if (c < ncol) {
-        out[(size_t)j * ncol + c] = acc[a][b][0];
+        double v = acc[a][b][0];
+        if (yadd) v += yadd[o];
+        out[o] = v;
+        if (dual) out2[o] = v;
       }
     }
   }
@@ -334,11 +347,12 @@ k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double
 
 // Returns cudaErrorNotSupported when the shapes or pointers do not allow the
 // 16-byte copies (nj > 128, odd nj or ncol, unaligned pointers).
-cudaError_t oa_dgemm_bwd(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
-                         const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
-                         double* out, const int* cond) {
+cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
+                            const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
+                            double* out, const int* cond, const double* yadd, double* out2, const int* cond2) {
   const uintptr_t al = (uintptr_t)M1 | (uintptr_t)X1 | (uintptr_t)out | (uintptr_t)(M2 ? M2 : M1) |
-                       (uintptr_t)(X2 ? X2 : X1);
+                       (uintptr_t)(X2 ? X2 : X1) | (uintptr_t)yadd | (uintptr_t)out2;
+  if (out2 && !cond2) return cudaErrorInvalidValue;
   if (nj > DB_TJ || (nj & 1) || (ncol & 1) || (al & 15) || nk <= 0 || (M2 && !X2)) return cudaErrorNotSupported;
   const size_t sm = (size_t)DB_STAGES * (DB_MSLAB + DB_XSLAB) * sizeof(double);
   dim3 grid((unsigned)((ncol + DB_TC - 1) / DB_TC));
@@ -347,12 +361,19 @@ cudaError_t oa_dgemm_bwd(cudaStream_t s, const double* M1, const double* X1, dou
     e = cudaFuncSetAttribute(k_dgemm_bwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     k_dgemm_bwd<true><<<grid, DB_THREADS, sm, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out,
-                                                    cond);
+                                                    cond, yadd, out2, cond2);
   } else {
     e = cudaFuncSetAttribute(k_dgemm_bwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     k_dgemm_bwd<false><<<grid, DB_THREADS, sm, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols,
-                                                     out, cond);
+                                                     out, cond, yadd, out2, cond2);
   }
   return cudaGetLastError();
+}
+
+cudaError_t oa_dgemm_bwd(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
+                         const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
+                         double* out, const int* cond) {
+  return oa_dgemm_bwd_ex(s, M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out, cond, nullptr, nullptr,
+                         nullptr);
 }

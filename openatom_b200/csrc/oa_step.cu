@@ -1,14 +1,14 @@
 // Whole CP dynamics steps in native code: the sequence of
 // GSpaceDriver::computeDynamics (src_charm_driver/cp_state_ctrl/gspace.ci:199-324)
-// on one GPU.  The steady-state step (iteration > 1, fixed buffers) is
+// on one GPU, ending with the PsiV tolerance reset when max|S - 2I| exceeds
+// norb_tol.  The steady-state step (iteration > 1, fixed buffers) is
 // captured once into one CUDA graph; with more states than the cluster
 // Newton-Schulz kernel takes, into two graphs (PsiV reset .. S, and Psi T +
 // the step record) replayed around the cooperative Newton-Schulz launch,
 // which stream capture does not accept.  Nothing in a step needs the host: the
 // PsiV tolerance check (Ortho::maxCheck, ortho.C:455-475) sets a device
-// flag that the conditional reset at the start of the next step reads, and
-// each step appends its energies and Newton-Schulz status to a device
-// record ring.  oa_gpu_cp_run therefore enqueues many steps and
+// flag that the conditional reset after Psi T reads, and each step appends
+// its energies and Newton-Schulz status to a device record ring.  oa_gpu_cp_run therefore enqueues many steps and
 // synchronises once; oa_gpu_cp_step is the one-step case.
 #include <stdio.h>
 #include <string.h>
@@ -37,8 +37,8 @@ oa_status oa_gpu_psiv_reset(oa_ctx* ctx, void* stream, const double* psi, double
 }
 
 int oa_ns_capturable(oa_ctx* c);
-oa_status oa_psiv_reset_cond(oa_ctx* c, cudaStream_t s, const double* psi, double* psi_t, double* vpsi, double* T,
-                             int* cond);
+oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* psi_t, double* psi, double* vpsi,
+                            double* Tout, int* flag);
 
 cudaError_t oa_launch_ortho_ns(cudaStream_t s, const double* S, int n, double bscale, double tol, int max_iter,
                                double* work, double* T, int* status, double* errv, int grid);
@@ -142,8 +142,6 @@ void oa_step_free(oa_ctx* c) {
 static oa_status launch_step_a(oa_ctx* c, cudaStream_t s, oa_cp_state* st, int complete_prev) {
   oa_step_scratch* w = step_scratch(c);
   const int nt = st->mixed_nterm;
-  // PsiV reset requested by the previous step's check (no-op otherwise)
-  OA_STEP_TRY(oa_psiv_reset_cond(c, s, st->psi, st->psi_t, st->vpsi, st->T, w->flag));
   // forces on the orthonormal psi (computePsiFandVKS, ParticlePlane, combineForcesGetEke)
   OA_STEP_TRY(oa_gpu_state_fft_fwd(c, s, st->psi, nullptr));
   OA_STEP_TRY(oa_gpu_vks_build(c, s, nullptr));
@@ -185,7 +183,8 @@ static oa_status launch_step_b(oa_ctx* c, cudaStream_t s, oa_cp_state* st) {
   OA_CUDA_TRY(oa_step_ortho_args(c, &work, &status, &errv, &grid, &dev_e, &hs, &hv, &eye));
   k_step_check<<<1, 1, 0, s>>>(status, errv, dev_e, st->norb_tol, w->flag, w->ring, w->ring_cap);
   OA_CUDA_TRY(cudaGetLastError());
-  OA_STEP_TRY(oa_gpu_pc_backward(c, s, st->T, st->psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, st->psi));
+  // psi = psi_t T, and the PsiV reset when the check asked for it
+  OA_STEP_TRY(oa_psi_t_and_psiv(c, s, st->T, st->psi_t, st->psi, st->vpsi, st->T, w->flag));
   return OA_OK;
 }
 
@@ -203,8 +202,8 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
   OA_STEP_TRY(ensure_ring(c, nsteps));
   cudaStream_t s = (cudaStream_t)stream;
   oa_step_scratch* w = step_scratch(c);
-  // restart the record count and the error slot; keep a pending PsiV flag
-  OA_CUDA_TRY(cudaMemsetAsync(w->flag + 1, 0, 3 * sizeof(int), s));
+  // restart the PsiV flag, the record count and the error slot
+  OA_CUDA_TRY(cudaMemsetAsync(w->flag, 0, 4 * sizeof(int), s));
   const void* key[7] = {st->psi, st->psi_t, st->vpsi, st->T, stream, w->ring, nullptr};
   // the legacy default stream cannot be captured: launch eagerly there
   const bool capturable = s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread;

@@ -65,10 +65,9 @@ def test_native_run_matches_steps_and_psiv():
             assert ec[i][k] == ea[i][k], (i, k, ea[i][k], ec[i][k])
     for d in (b, c):
         assert np.array_equal(a.psi.cpu().numpy(), d.psi.cpu().numpy())
-    # the host runner resets psi_t and v at the end of a step, the native
-    # step at the start of the next one: compare the two native runs
-    assert np.array_equal(b.psi_t.cpu().numpy(), c.psi_t.cpu().numpy())
-    assert np.array_equal(b.v.cpu().numpy(), c.v.cpu().numpy())
+        assert np.array_equal(a.psi_t.cpu().numpy(), d.psi_t.cpu().numpy())
+        assert np.array_equal(a.v.cpu().numpy(), d.v.cpu().numpy())
+        assert np.array_equal(a.T.cpu().numpy(), d.T.cpu().numpy())
 
 
 def test_native_run_positions_and_failure():
