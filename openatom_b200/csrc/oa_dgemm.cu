@@ -134,15 +134,40 @@ k_dgemm_fwd(const double* __restrict__ A, const double* __restrict__ B, int m, i
     }
 }
 
-// C = alpha (w0 sum_{kb < n0} part[kb] + sum_{kb >= n0} part[kb]), fixed order
-__global__ void k_dgemm_fwd_reduce(const double* __restrict__ part, int n0, int nkb, size_t nn, double w0,
-                                   double alpha, double* __restrict__ C, const int* __restrict__ cond) {
+// C = alpha (w0 sum_{kb < n0} part[kb] + sum_{kb >= n0} part[kb]).  Block =
+// 64 outputs x 4 partial groups (group g sums the partials kb = g mod 4 of
+// each range); the groups are combined in a fixed order, so the result does
+// not depend on scheduling.
+#define DR_COLS 64
+#define DR_GROUPS 4
+__global__ void __launch_bounds__(DR_COLS * DR_GROUPS)
+k_dgemm_fwd_reduce(const double* __restrict__ part, int n0, int nkb, size_t nn, double w0, double alpha,
+                   double* __restrict__ C, const int* __restrict__ cond) {
   if (cond && *cond == 0) return;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (size_t)gridDim.x * blockDim.x) {
-    double s0 = 0.0, s1 = 0.0;
-    for (int k = 0; k < n0; ++k) s0 += part[(size_t)k * nn + i];
-    for (int k = n0; k < nkb; ++k) s1 += part[(size_t)k * nn + i];
-    C[i] = alpha * (w0 * s0 + s1);
+  __shared__ double s0s[DR_GROUPS][DR_COLS], s1s[DR_GROUPS][DR_COLS];
+  const int col = threadIdx.x % DR_COLS, g = threadIdx.x / DR_COLS;
+  const size_t i = (size_t)blockIdx.x * DR_COLS + col;
+  double s0 = 0.0, s1 = 0.0;
+  if (i < nn) {
+    for (int k = g; k < n0; k += DR_GROUPS) s0 += __ldcs(part + (size_t)k * nn + i);
+    int k = n0 + g;
+    for (; k + 3 * DR_GROUPS < nkb; k += 4 * DR_GROUPS) {
+      const double a = __ldcs(part + (size_t)k * nn + i);
+      const double b = __ldcs(part + (size_t)(k + DR_GROUPS) * nn + i);
+      const double c = __ldcs(part + (size_t)(k + 2 * DR_GROUPS) * nn + i);
+      const double d = __ldcs(part + (size_t)(k + 3 * DR_GROUPS) * nn + i);
+      s1 += a; s1 += b; s1 += c; s1 += d;
+    }
+    for (; k < nkb; k += DR_GROUPS) s1 += __ldcs(part + (size_t)k * nn + i);
+  }
+  s0s[g][col] = s0;
+  s1s[g][col] = s1;
+  __syncthreads();
+  if (g == 0 && i < nn) {
+    double t0 = 0.0, t1 = 0.0;
+#pragma unroll
+    for (int q = 0; q < DR_GROUPS; ++q) { t0 += s0s[q][col]; t1 += s1s[q][col]; }
+    C[i] = alpha * (w0 * t0 + t1);
   }
 }
 
@@ -200,7 +225,8 @@ cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const size_t mn = (size_t)m * n;
-  k_dgemm_fwd_reduce<<<(unsigned)((mn + 255) / 256), 256, 0, s>>>(part, n0, nkb_eff, mn, w_kx0, alpha, C, cond);
+  k_dgemm_fwd_reduce<<<(unsigned)((mn + DR_COLS - 1) / DR_COLS), DR_COLS * DR_GROUPS, 0, s>>>(part, n0, nkb_eff, mn,
+                                                                                               w_kx0, alpha, C, cond);
   return cudaGetLastError();
 }
 

@@ -300,13 +300,28 @@ k_umma_fwd(const double* __restrict__ A, const double* __restrict__ B, int m, in
   if (warp == 0) tmem_dealloc(tmem, ncols);
 }
 
-__global__ void k_umma_fwd_reduce(const float* __restrict__ part, int nkb, size_t nn, double alpha,
-                                  double* __restrict__ C) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (size_t)gridDim.x * blockDim.x) {
-    double s = 0.0;
-    for (int k = 0; k < nkb; ++k) s += (double)part[(size_t)k * nn + i];
-    C[i] = alpha * s;
+// C = alpha sum_kb part[kb] in FP64; 64 outputs x 4 partial groups per
+// block, groups combined in a fixed order (deterministic)
+__global__ void __launch_bounds__(256)
+k_umma_fwd_reduce(const float* __restrict__ part, int nkb, size_t nn, double alpha, double* __restrict__ C) {
+  __shared__ double ss[4][64];
+  const int col = threadIdx.x & 63, g = threadIdx.x >> 6;
+  const size_t i = (size_t)blockIdx.x * 64 + col;
+  double s = 0.0;
+  if (i < nn) {
+    int k = g;
+    for (; k + 12 < nkb; k += 16) {
+      const float a = __ldcs(part + (size_t)k * nn + i);
+      const float b = __ldcs(part + (size_t)(k + 4) * nn + i);
+      const float c = __ldcs(part + (size_t)(k + 8) * nn + i);
+      const float d = __ldcs(part + (size_t)(k + 12) * nn + i);
+      s += (double)a; s += (double)b; s += (double)c; s += (double)d;
+    }
+    for (; k < nkb; k += 4) s += (double)__ldcs(part + (size_t)k * nn + i);
   }
+  ss[g][col] = s;
+  __syncthreads();
+  if (g == 0 && i < nn) C[i] = alpha * (((ss[0][col] + ss[1][col]) + ss[2][col]) + ss[3][col]);
 }
 
 // ---------------------------------------------------------------------------
@@ -485,7 +500,7 @@ cudaError_t oa_launch_umma_fwd(cudaStream_t s, int nterm, const double* A, const
   }
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const size_t mn = (size_t)m * n;
-  k_umma_fwd_reduce<<<(unsigned)((mn + 255) / 256), 256, 0, s>>>(part, kb, mn, alpha, C);
+  k_umma_fwd_reduce<<<(unsigned)((mn + 63) / 64), 256, 0, s>>>(part, kb, mn, alpha, C);
   return cudaGetLastError();
 }
 
