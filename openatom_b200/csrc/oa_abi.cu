@@ -4,6 +4,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <vector>
+#include <cuda_bf16.h>
 #include "oa_internal.h"
 
 // launchers from the other translation units
@@ -36,6 +37,14 @@ cudaError_t oa_launch_umma_bwd(cudaStream_t s, int nterm, const double* M1, cons
                                double a1_rest, const double* M2, const double* X2, double a2, int nj, int nk,
                                long ncol, long kx0_cols, double* out, int* err_flag);
 int oa_umma_max_kb(int m, int n, int nsm);
+long oa_plane_ld(long K);
+cudaError_t oa_split_planes(cudaStream_t s, int nt, const double* X, int rows, long K, long ldx, long kx0_cols,
+                            double w_kx0, __nv_bfloat16* P, long ldp);
+cudaError_t oa_pfwd(cudaStream_t s, int nt, const __nv_bfloat16* PA, const __nv_bfloat16* PB, int m, int n, long K,
+                    long ldp, double alpha, float* part, int max_kb, double* C, int* err_flag, int nsm);
+cudaError_t oa_pbwd(cudaStream_t s, int nt, const __nv_bfloat16* PM1, const __nv_bfloat16* PX1, double a1_kx0,
+                    double a1_rest, const __nv_bfloat16* PM2, const __nv_bfloat16* PX2, double a2, int nj, int nk,
+                    long ncol, long ldx, long kx0_cols, double* out, int* err_flag);
 cudaError_t oa_launch_pc_fwd_mn(cudaStream_t s, const double* A, const double* B, int m, int n, long K,
                                 long kx0_cols, double w_kx0, double alpha, double* part, int nkb, double* C);
 cudaError_t oa_launch_pc_bwd_jk(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
@@ -83,6 +92,13 @@ struct oa_ctx_pc {
   double* vtmp;      // [nstate][ng] complex scratch
   float* upart;      // split-K FP32 partials of the tensor-core forward GEMM
   int umax_kb;
+  void* pl_big[3];   // bf16 planes [3][mx][pl_ld] of the big operands (slots below)
+  void* pl_ma;       // bf16 planes [3][mx][mx] of the small matrices
+  void* pl_mb;
+  long pl_ld;
+  // what each big slot holds, for reuse inside one native step (pl_cache)
+  struct { const double* src; int rows, nt; long K, kx0; double w; bool valid; } pl_key[3];
+  int pl_cache;
   int* err_flag;     // device: set by a kernel whose bounded wait ran out
   int nsm;
 };
@@ -300,6 +316,13 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     }
     TRY(cudaMalloc(&p->err_flag, sizeof(int)));
     TRY(cudaMemset(p->err_flag, 0, sizeof(int)));
+    {
+      const int mx = d->nstate > d->natm_nl ? d->nstate : d->natm_nl;
+      p->pl_ld = oa_plane_ld(2L * d->ng);
+      for (int q = 0; q < 3; ++q) TRY(cudaMalloc(&p->pl_big[q], (size_t)3 * mx * p->pl_ld * 2));
+      TRY(cudaMalloc(&p->pl_ma, (size_t)3 * mx * mx * 2));
+      TRY(cudaMalloc(&p->pl_mb, (size_t)3 * mx * mx * 2));
+    }
     TRY(cudaMallocHost(&p->h_status, 4 * sizeof(int)));
     TRY(cudaMallocHost(&p->h_vals, 16 * sizeof(double)));
     TRY(cudaDeviceSynchronize());
@@ -325,6 +348,7 @@ extern "C" oa_status oa_gpu_destroy(oa_ctx* c) {
                  c->tw_z, c->spl, c->q_type, c->atm_type, c->atm_perm, c->pos, c->phase, c->occ, c->zbuf, c->rho_part, c->rho,
                  c->vks, c->vxc, c->dz, c->red, c->eke_part, p->part, p->ns_work, p->ns_status, p->ns_err,
                  p->partner, p->cmass, p->ke_part, p->dev_e, p->mat_a, p->mat_x, p->eye, p->vtmp, p->upart,
+                 p->pl_big[0], p->pl_big[1], p->pl_big[2], p->pl_ma, p->pl_mb,
                  p->err_flag, c->ky, c->kz, c->nl_atm, c->nl_spl, c->nl_vnorm, c->nl_gz0, c->sf, c->zmat, c->zt,
                  c->enl, c->enl_eke};
   for (void* q : dev) if (q) cudaFree(q);
@@ -653,13 +677,90 @@ extern "C" oa_status oa_gpu_sizes(const oa_ctx* c, long* out) {
   return OA_OK;
 }
 
+typedef __nv_bfloat16 bf16;
+
+// Plane slots of the big operands: the state coefficients, the force or
+// second operand, the nonlocal structure factor.
+enum { PL_PSI = 0, PL_OTHER = 1, PL_SF = 2 };
+
+// bf16 planes of X [rows][K] (kx0 columns weighted) in a big slot.  Inside a
+// native step (pl_cache set) a slot that already holds the same source with
+// the same weighting is reused; the step clears the slots whenever the
+// sources may have changed.
+static cudaError_t ensure_planes(oa_ctx* c, cudaStream_t s, int nt, int slot, const double* X, int rows, long K,
+                                 long kx0_cols, double w_kx0) {
+  oa_ctx_pc* p = pcx(c);
+  if (kx0_cols == 0) w_kx0 = 1.0;
+  if (w_kx0 == 1.0) kx0_cols = 0;
+  auto& k = p->pl_key[slot];
+  if (p->pl_cache && k.valid && k.src == X && k.rows == rows && k.nt == nt && k.K == K && k.kx0 == kx0_cols &&
+      k.w == w_kx0)
+    return cudaSuccess;
+  const cudaError_t e = oa_split_planes(s, nt, X, rows, K, K, kx0_cols, w_kx0, (bf16*)p->pl_big[slot], p->pl_ld);
+  k.src = X; k.rows = rows; k.nt = nt; k.K = K; k.kx0 = kx0_cols; k.w = w_kx0;
+  k.valid = e == cudaSuccess;
+  return e;
+}
+
+void oa_planes_reuse(oa_ctx* c, int on) {
+  oa_ctx_pc* p = pcx(c);
+  p->pl_cache = on;
+  for (int q = 0; q < 3; ++q) p->pl_key[q].valid = false;
+}
+
+// Split-BF16 forward product through bf16 planes (oa_umma2.cu); the
+// element-wise-staging kernels (oa_umma.cu) for shapes the planes path does
+// not take.  A: [m][K] (kx0 columns weighted by w_kx0), B: [n][K], in
+// plane slots sa and sb.
+static cudaError_t mixed_fwd(oa_ctx* c, cudaStream_t s, int nt, const double* A, const double* B, int m, int n,
+                             long K, long kx0_cols, double w_kx0, double alpha, double* C, int sa, int sb) {
+  oa_ctx_pc* p = pcx(c);
+  const int mx = c->nstate > c->natm_nl ? c->nstate : c->natm_nl;
+  if (m <= mx && n <= mx && K <= p->pl_ld) {
+    cudaError_t e = ensure_planes(c, s, nt, sa, A, m, K, kx0_cols, w_kx0);
+    if (e != cudaSuccess) return e;
+    const bf16* pb = (const bf16*)p->pl_big[sa];
+    if (!(B == A && (w_kx0 == 1.0 || kx0_cols == 0))) {
+      if ((e = ensure_planes(c, s, nt, sb, B, n, K, 0, 1.0)) != cudaSuccess) return e;
+      pb = (const bf16*)p->pl_big[sb];
+    }
+    e = oa_pfwd(s, nt, (const bf16*)p->pl_big[sa], pb, m, n, K, p->pl_ld, alpha, p->upart, p->umax_kb, C,
+                p->err_flag, p->nsm);
+    if (e != cudaErrorNotSupported) return e;
+  }
+  return oa_launch_umma_fwd(s, nt, A, B, m, n, K, kx0_cols, w_kx0, alpha, p->upart, p->umax_kb, C, p->err_flag,
+                            p->nsm);
+}
+
+// Split-BF16 backward product through bf16 planes, with the same fallback;
+// X1, X2 in plane slots s1, s2.
+static cudaError_t mixed_bwd(oa_ctx* c, cudaStream_t s, int nt, const double* M1, const double* X1, double a1_kx0,
+                             double a1_rest, const double* M2, const double* X2, double a2, int nj, int nk, long ncol,
+                             long kx0_cols, double* out, int s1, int s2) {
+  oa_ctx_pc* p = pcx(c);
+  const int mx = c->nstate > c->natm_nl ? c->nstate : c->natm_nl;
+  if (nj <= mx && nk <= mx && ncol <= p->pl_ld && nj <= 128 && (nj & 7) == 0 && (!M2 || s1 != s2)) {
+    bf16 *pm1 = (bf16*)p->pl_ma, *pm2 = (bf16*)p->pl_mb;
+    cudaError_t e = ensure_planes(c, s, nt, s1, X1, nk, ncol, 0, 1.0);
+    if (e == cudaSuccess) e = oa_split_planes(s, nt, M1, nk, nj, nj, 0, 1.0, pm1, nj);
+    if (e == cudaSuccess && M2) e = ensure_planes(c, s, nt, s2, X2, nk, ncol, 0, 1.0);
+    if (e == cudaSuccess && M2) e = oa_split_planes(s, nt, M2, nk, nj, nj, 0, 1.0, pm2, nj);
+    if (e != cudaSuccess) return e;
+    e = oa_pbwd(s, nt, pm1, (const bf16*)p->pl_big[s1], a1_kx0, a1_rest, M2 ? pm2 : nullptr,
+                M2 ? (const bf16*)p->pl_big[s2] : nullptr, a2, nj, nk, ncol, p->pl_ld, kx0_cols, out, p->err_flag);
+    if (e != cudaErrorNotSupported) return e;
+  }
+  return oa_launch_umma_bwd(s, nt, M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out, p->err_flag);
+}
+
 extern "C" oa_status oa_gpu_pc_forward_mixed(oa_ctx* c, void* stream, const double* left, const double* right,
                                              double alpha, double w_kx0, int nterm, double* C) {
   OA_ARG_CHECK(c && left && right && C, "null argument");
   OA_ARG_CHECK(nterm == 2 || nterm == 3, "nterm must be 2 or 3");
   oa_ctx_pc* p = pcx(c);
-  OA_CUDA_TRY(oa_launch_umma_fwd((cudaStream_t)stream, nterm, left, right, c->nstate, c->nstate, 2L * c->ng,
-                                 2L * c->nkx0, w_kx0, alpha, p->upart, p->umax_kb, C, p->err_flag, p->nsm));
+  (void)p;
+  OA_CUDA_TRY(mixed_fwd(c, (cudaStream_t)stream, nterm, left, right, c->nstate, c->nstate, 2L * c->ng, 2L * c->nkx0,
+                        w_kx0, alpha, C, PL_PSI, PL_OTHER));
   return OA_OK;
 }
 
@@ -670,8 +771,8 @@ extern "C" oa_status oa_gpu_pc_backward_mixed(oa_ctx* c, void* stream, const dou
   OA_ARG_CHECK((M2 == nullptr) == (X2 == nullptr), "M2 and X2 must both be given or both be NULL");
   OA_ARG_CHECK(out != X1 && out != X2, "out must not alias an input");
   OA_ARG_CHECK(nterm == 2 || nterm == 3, "nterm must be 2 or 3");
-  OA_CUDA_TRY(oa_launch_umma_bwd((cudaStream_t)stream, nterm, M1, X1, a1_kx0, a1_rest, M2, X2, a2, c->nstate,
-                                 c->nstate, 2L * c->ng, 2L * c->nkx0, out, pcx(c)->err_flag));
+  OA_CUDA_TRY(mixed_bwd(c, (cudaStream_t)stream, nterm, M1, X1, a1_kx0, a1_rest, M2, X2, a2, c->nstate, c->nstate,
+                        2L * c->ng, 2L * c->nkx0, out, PL_PSI, PL_OTHER));
   return OA_OK;
 }
 
@@ -709,16 +810,15 @@ extern "C" oa_status oa_gpu_nl_sf(oa_ctx* c, void* stream, const double* psi, in
   if (nterm == 0)
     OA_CUDA_TRY(oa_launch_pc_fwd_mn(s, psi, (const double*)c->sf, n, na, K, 0, 1.0, 1.0, p->part, p->nkb, c->zmat));
   else
-    OA_CUDA_TRY(oa_launch_umma_fwd(s, nterm, psi, (const double*)c->sf, n, na, K, 0, 1.0, 1.0, p->upart, p->umax_kb,
-                                   c->zmat, p->err_flag, p->nsm));
+    OA_CUDA_TRY(mixed_fwd(c, s, nterm, psi, (const double*)c->sf, n, na, K, 0, 1.0, 1.0, c->zmat, PL_PSI, PL_SF));
   OA_CUDA_TRY(oa_launch_nl_zscale(s, c->zmat, n, na, c->nl_atm, c->atm_type, c->nl_vnorm, 1.0 / c->vol, c->occ,
                                   c->zt, c->enl));
   if (nterm == 0)
     OA_CUDA_TRY(oa_launch_pc_bwd_jk(s, c->zt, (const double*)c->sf, 1.0, 1.0, nullptr, nullptr, 0.0, n, na, K, 0,
                                     fnl_out));
   else
-    OA_CUDA_TRY(oa_launch_umma_bwd(s, nterm, c->zt, (const double*)c->sf, 1.0, 1.0, nullptr, nullptr, 0.0, n, na, K,
-                                   0, fnl_out, p->err_flag));
+    OA_CUDA_TRY(mixed_bwd(c, s, nterm, c->zt, (const double*)c->sf, 1.0, 1.0, nullptr, nullptr, 0.0, n, na, K, 0,
+                          fnl_out, PL_SF, PL_OTHER));
   OA_CUDA_TRY(oa_launch_sum_partials(s, c->enl, n, 1, 0, 1.0, p->dev_e + OA_E_ENL));
   if (enl_out) OA_CUDA_TRY(cudaMemcpyAsync(enl_out, c->enl, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   return OA_OK;

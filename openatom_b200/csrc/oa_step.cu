@@ -139,7 +139,19 @@ void oa_step_free(oa_ctx* c) {
 #define OA_STEP_TRY(x) do { oa_status st_ = (x); if (st_ != OA_OK) return st_; } while (0)
 
 // Launches of one step up to S (part A); no host synchronisation.
+void oa_planes_reuse(oa_ctx* c, int on);
+
+// force phase with bf16-plane reuse: psi, the structure factor and F are
+// each split once (psi and F do not change until the step ends)
+static oa_status launch_step_a_body(oa_ctx* c, cudaStream_t s, oa_cp_state* st, int complete_prev);
 static oa_status launch_step_a(oa_ctx* c, cudaStream_t s, oa_cp_state* st, int complete_prev) {
+  oa_planes_reuse(c, 1);
+  const oa_status r = launch_step_a_body(c, s, st, complete_prev);
+  oa_planes_reuse(c, 0);
+  return r;
+}
+
+static oa_status launch_step_a_body(oa_ctx* c, cudaStream_t s, oa_cp_state* st, int complete_prev) {
   oa_step_scratch* w = step_scratch(c);
   const int nt = st->mixed_nterm;
   // forces on the orthonormal psi (computePsiFandVKS, ParticlePlane, combineForcesGetEke)
