@@ -37,12 +37,14 @@ cudaError_t oa_launch_umma_bwd(cudaStream_t s, int nterm, const double* M1, cons
                                double a1_rest, const double* M2, const double* X2, double a2, int nj, int nk,
                                long ncol, long kx0_cols, double* out, int* err_flag);
 int oa_umma_max_kb(int m, int n, int nsm);
-long oa_plane_ld(long K);
-cudaError_t oa_split_planes(cudaStream_t s, int nt, const double* X, int rows, long K, long ldx, long kx0_cols,
-                            double w_kx0, __nv_bfloat16* P, long ldp);
-cudaError_t oa_pfwd(cudaStream_t s, int nt, const __nv_bfloat16* PA, const __nv_bfloat16* PB, int m, int n, long K,
-                    long ldp, double alpha, float* part, int max_kb, double* C, int* err_flag, int nsm);
-cudaError_t oa_pbwd(cudaStream_t s, int nt, const __nv_bfloat16* PM1, const __nv_bfloat16* PX1, double a1_kx0,
+cudaError_t oa_split_kc(cudaStream_t s, int nt, const double* X, int rows, int rows_pad, long K, long ldx,
+                        long kx0_cols, double w_kx0, __nv_bfloat16* P, long ldp);
+int oa_tg_rows_pad(int rows, int box);
+int oa_tg_nb(int n);
+cudaError_t oa_tfwd(cudaStream_t s, int nt, const __nv_bfloat16* PA, int rows_a, const __nv_bfloat16* PB, int rows_b,
+                    int m, int n, long K, long ldp, double alpha, float* part, int max_kb, double* C, int* err_flag,
+                    int nsm);
+cudaError_t oa_tbwd(cudaStream_t s, int nt, const __nv_bfloat16* PM1, const __nv_bfloat16* PX1, double a1_kx0,
                     double a1_rest, const __nv_bfloat16* PM2, const __nv_bfloat16* PX2, double a2, int nj, int nk,
                     long ncol, long ldx, long kx0_cols, double* out, int* err_flag);
 cudaError_t oa_launch_pc_fwd_mn(cudaStream_t s, const double* A, const double* B, int m, int n, long K,
@@ -97,7 +99,8 @@ struct oa_ctx_pc {
   void* pl_mb;
   long pl_ld;
   // what each big slot holds, for reuse inside one native step (pl_cache)
-  struct { const double* src; int rows, nt; long K, kx0; double w; bool valid; } pl_key[3];
+  struct { const double* src; int rows, rows_pad, nt; long K, kx0; double w; bool valid; } pl_key[3];
+  int pl_rows;       // row capacity of the big and small plane buffers
   int pl_cache;
   int* err_flag;     // device: set by a kernel whose bounded wait ran out
   int nsm;
@@ -318,10 +321,11 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     TRY(cudaMemset(p->err_flag, 0, sizeof(int)));
     {
       const int mx = d->nstate > d->natm_nl ? d->nstate : d->natm_nl;
-      p->pl_ld = oa_plane_ld(2L * d->ng);
-      for (int q = 0; q < 3; ++q) TRY(cudaMalloc(&p->pl_big[q], (size_t)3 * mx * p->pl_ld * 2));
-      TRY(cudaMalloc(&p->pl_ma, (size_t)3 * mx * mx * 2));
-      TRY(cudaMalloc(&p->pl_mb, (size_t)3 * mx * mx * 2));
+      p->pl_ld = (2L * d->ng + 63) / 64 * 64;
+      p->pl_rows = oa_tg_rows_pad(mx, 128);
+      for (int q = 0; q < 3; ++q) TRY(cudaMalloc(&p->pl_big[q], (size_t)3 * p->pl_rows * p->pl_ld * 2));
+      TRY(cudaMalloc(&p->pl_ma, (size_t)3 * p->pl_rows * p->pl_rows * 2));
+      TRY(cudaMalloc(&p->pl_mb, (size_t)3 * p->pl_rows * p->pl_rows * 2));
     }
     TRY(cudaMallocHost(&p->h_status, 4 * sizeof(int)));
     TRY(cudaMallocHost(&p->h_vals, 16 * sizeof(double)));
@@ -687,17 +691,18 @@ enum { PL_PSI = 0, PL_OTHER = 1, PL_SF = 2 };
 // native step (pl_cache set) a slot that already holds the same source with
 // the same weighting is reused; the step clears the slots whenever the
 // sources may have changed.
-static cudaError_t ensure_planes(oa_ctx* c, cudaStream_t s, int nt, int slot, const double* X, int rows, long K,
-                                 long kx0_cols, double w_kx0) {
+static cudaError_t ensure_planes(oa_ctx* c, cudaStream_t s, int nt, int slot, const double* X, int rows,
+                                 int rows_pad, long K, long kx0_cols, double w_kx0) {
   oa_ctx_pc* p = pcx(c);
   if (kx0_cols == 0) w_kx0 = 1.0;
   if (w_kx0 == 1.0) kx0_cols = 0;
   auto& k = p->pl_key[slot];
-  if (p->pl_cache && k.valid && k.src == X && k.rows == rows && k.nt == nt && k.K == K && k.kx0 == kx0_cols &&
-      k.w == w_kx0)
+  if (p->pl_cache && k.valid && k.src == X && k.rows == rows && k.rows_pad == rows_pad && k.nt == nt && k.K == K &&
+      k.kx0 == kx0_cols && k.w == w_kx0)
     return cudaSuccess;
-  const cudaError_t e = oa_split_planes(s, nt, X, rows, K, K, kx0_cols, w_kx0, (bf16*)p->pl_big[slot], p->pl_ld);
-  k.src = X; k.rows = rows; k.nt = nt; k.K = K; k.kx0 = kx0_cols; k.w = w_kx0;
+  const cudaError_t e =
+      oa_split_kc(s, nt, X, rows, rows_pad, K, K, kx0_cols, w_kx0, (bf16*)p->pl_big[slot], p->pl_ld);
+  k.src = X; k.rows = rows; k.rows_pad = rows_pad; k.nt = nt; k.K = K; k.kx0 = kx0_cols; k.w = w_kx0;
   k.valid = e == cudaSuccess;
   return e;
 }
@@ -708,7 +713,7 @@ void oa_planes_reuse(oa_ctx* c, int on) {
   for (int q = 0; q < 3; ++q) p->pl_key[q].valid = false;
 }
 
-// Split-BF16 forward product through bf16 planes (oa_umma2.cu); the
+// Split-BF16 forward product through bf16 planes (oa_tgemm.cu); the
 // element-wise-staging kernels (oa_umma.cu) for shapes the planes path does
 // not take.  A: [m][K] (kx0 columns weighted by w_kx0), B: [n][K], in
 // plane slots sa and sb.
@@ -716,15 +721,20 @@ static cudaError_t mixed_fwd(oa_ctx* c, cudaStream_t s, int nt, const double* A,
                              long K, long kx0_cols, double w_kx0, double alpha, double* C, int sa, int sb) {
   oa_ctx_pc* p = pcx(c);
   const int mx = c->nstate > c->natm_nl ? c->nstate : c->natm_nl;
-  if (m <= mx && n <= mx && K <= p->pl_ld) {
-    cudaError_t e = ensure_planes(c, s, nt, sa, A, m, K, kx0_cols, w_kx0);
+  const int nb = oa_tg_nb(n);
+  const int ra = oa_tg_rows_pad(m, 128), rb = nb ? oa_tg_rows_pad(n, nb) : 0;
+  if (nb && m <= mx && n <= mx && K <= p->pl_ld && ra <= p->pl_rows && rb <= p->pl_rows) {
+    const bool same = B == A && (w_kx0 == 1.0 || kx0_cols == 0) && ra % nb == 0;
+    cudaError_t e = ensure_planes(c, s, nt, sa, A, m, ra, K, kx0_cols, w_kx0);
     if (e != cudaSuccess) return e;
     const bf16* pb = (const bf16*)p->pl_big[sa];
-    if (!(B == A && (w_kx0 == 1.0 || kx0_cols == 0))) {
-      if ((e = ensure_planes(c, s, nt, sb, B, n, K, 0, 1.0)) != cudaSuccess) return e;
+    int rows_b = ra;
+    if (!same) {
+      if ((e = ensure_planes(c, s, nt, sb, B, n, rb, K, 0, 1.0)) != cudaSuccess) return e;
       pb = (const bf16*)p->pl_big[sb];
+      rows_b = rb;
     }
-    e = oa_pfwd(s, nt, (const bf16*)p->pl_big[sa], pb, m, n, K, p->pl_ld, alpha, p->upart, p->umax_kb, C,
+    e = oa_tfwd(s, nt, (const bf16*)p->pl_big[sa], ra, pb, rows_b, m, n, K, p->pl_ld, alpha, p->upart, p->umax_kb, C,
                 p->err_flag, p->nsm);
     if (e != cudaErrorNotSupported) return e;
   }
@@ -739,15 +749,16 @@ static cudaError_t mixed_bwd(oa_ctx* c, cudaStream_t s, int nt, const double* M1
                              long kx0_cols, double* out, int s1, int s2) {
   oa_ctx_pc* p = pcx(c);
   const int mx = c->nstate > c->natm_nl ? c->nstate : c->natm_nl;
-  if (nj <= mx && nk <= mx && ncol <= p->pl_ld && nj <= 128 && (nj & 7) == 0 && (!M2 || s1 != s2)) {
+  const int nkp = oa_tg_rows_pad(nk, 32);
+  if (nj <= mx && nk <= mx && ncol <= p->pl_ld && oa_tg_nb(nj) == nj && nkp <= p->pl_rows && (!M2 || s1 != s2)) {
     bf16 *pm1 = (bf16*)p->pl_ma, *pm2 = (bf16*)p->pl_mb;
-    cudaError_t e = ensure_planes(c, s, nt, s1, X1, nk, ncol, 0, 1.0);
-    if (e == cudaSuccess) e = oa_split_planes(s, nt, M1, nk, nj, nj, 0, 1.0, pm1, nj);
-    if (e == cudaSuccess && M2) e = ensure_planes(c, s, nt, s2, X2, nk, ncol, 0, 1.0);
-    if (e == cudaSuccess && M2) e = oa_split_planes(s, nt, M2, nk, nj, nj, 0, 1.0, pm2, nj);
+    cudaError_t e = ensure_planes(c, s, nt, s1, X1, nk, nkp, ncol, 0, 1.0);
+    if (e == cudaSuccess) e = oa_split_kc(s, nt, M1, nk, nkp, nj, nj, 0, 1.0, pm1, nj);
+    if (e == cudaSuccess && M2) e = ensure_planes(c, s, nt, s2, X2, nk, nkp, ncol, 0, 1.0);
+    if (e == cudaSuccess && M2) e = oa_split_kc(s, nt, M2, nk, nkp, nj, nj, 0, 1.0, pm2, nj);
     if (e != cudaSuccess) return e;
-    e = oa_pbwd(s, nt, pm1, (const bf16*)p->pl_big[s1], a1_kx0, a1_rest, M2 ? pm2 : nullptr,
-                M2 ? (const bf16*)p->pl_big[s2] : nullptr, a2, nj, nk, ncol, p->pl_ld, kx0_cols, out, p->err_flag);
+    e = oa_tbwd(s, nt, pm1, (const bf16*)p->pl_big[s1], a1_kx0, a1_rest, M2 ? pm2 : nullptr,
+                M2 ? (const bf16*)p->pl_big[s2] : nullptr, a2, nj, nkp, ncol, p->pl_ld, kx0_cols, out, p->err_flag);
     if (e != cudaErrorNotSupported) return e;
   }
   return oa_launch_umma_bwd(s, nt, M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out, p->err_flag);
