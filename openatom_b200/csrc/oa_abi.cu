@@ -20,6 +20,7 @@ cudaError_t oa_launch_pc_bwd(cudaStream_t s, const double* M1, const double* X1,
                              double* out);
 cudaError_t oa_launch_small_gemm(cudaStream_t s, const double* A, const double* B, int n, double alpha, double* C);
 int oa_ns_grid(int n, int device);
+int oa_pencil_supported(int n);
 int oa_ns_cluster_size(int n);
 cudaError_t oa_launch_ortho_ns(cudaStream_t s, const double* S, int n, double bscale, double tol, int max_iter,
                                double* work, double* T, int* status, double* errv, int grid);
@@ -282,6 +283,7 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     c->zbuf_bytes = (size_t)d->nstate * d->nz * c->ldl * csz;
     TRY(cudaMalloc(&c->zbuf, c->zbuf_bytes));
     TRY(cudaMalloc(&c->rho_part, (size_t)c->ngroup * c->npts * sizeof(double)));
+    if (d->nx == d->ny && oa_pencil_supported(d->nx)) TRY(cudaMalloc(&c->psir, (size_t)d->nstate * c->npts * rsz));
     TRY(cudaMalloc(&c->rho, (size_t)c->npts * sizeof(double)));
     TRY(cudaMalloc(&c->vxc, (size_t)c->npts * sizeof(double)));
     TRY(cudaMalloc(&c->vks, (size_t)c->npts * rsz));
@@ -349,7 +351,7 @@ extern "C" oa_status oa_gpu_destroy(oa_ctx* c) {
   ees_free(c);
   oa_ctx_pc* p = pcx(c);
   void* dev[] = {c->line_kx, c->line_ky, c->line_off, c->line_nneg, c->line_npos, c->kx, c->g2, c->tw_x, c->tw_y,
-                 c->tw_z, c->spl, c->q_type, c->atm_type, c->atm_perm, c->pos, c->phase, c->occ, c->zbuf, c->rho_part, c->rho,
+                 c->tw_z, c->spl, c->q_type, c->atm_type, c->atm_perm, c->pos, c->psir, c->phase, c->occ, c->zbuf, c->rho_part, c->rho,
                  c->vks, c->vxc, c->dz, c->red, c->eke_part, p->part, p->ns_work, p->ns_status, p->ns_err,
                  p->partner, p->cmass, p->ke_part, p->dev_e, p->mat_a, p->mat_x, p->eye, p->vtmp, p->upart,
                  p->pl_big[0], p->pl_big[1], p->pl_big[2], p->pl_ma, p->pl_mb,
@@ -444,7 +446,10 @@ extern "C" oa_status oa_gpu_vks_apply_fft_bwd(oa_ctx* c, void* stream, const dou
                                               const double* fnl, double* force, double* eke_out) {
   OA_ARG_CHECK(c && psi && force, "null argument");
   cudaStream_t s = (cudaStream_t)stream;
-  if (recompute_fwd) OA_CUDA_TRY(oa_launch_state_zfwd(c, s, (const double2*)psi, 0, c->nstate));
+  if (recompute_fwd) {
+    OA_CUDA_TRY(oa_launch_state_zfwd(c, s, (const double2*)psi, 0, c->nstate));
+    c->psir_valid = 0;  // the z-line buffer is newer than psi(r)
+  }
   OA_CUDA_TRY(oa_launch_state_plane_vks(c, s));
   OA_CUDA_TRY(oa_launch_state_zbwd(c, s, (const double2*)psi, (const double2*)fnl, (double2*)force, 0, c->nstate));
   double* es = eke_out ? eke_out : c->enl_eke;

@@ -36,6 +36,8 @@ struct oa_ctx {
   int nkx_d;              // density half-spectrum columns (nx/2 + 1)
   int nlines_d, ldl_d;    // density z-lines (nkx_d * ny) and padded stride
   int ngroup;             // state groups in the plane kernels
+  void* psir;             // [nstate][nz][ny][nx] psi(r), compute precision (two-pass kernels)
+  int psir_valid;         // the last density pass stored psir
   double box, vol, ecut_psi, ecut_rho, alp_ewd;
   double gzvps_sum;
   int nspl; double spl_gmin, spl_dg;

@@ -198,6 +198,9 @@ k_zbwd2(const typename CplxOf<R>::T* __restrict__ zbuf, int ldl, int nlines, con
 //           -> zbuf row (in place); V_KS is read from global memory (L2)
 //   MODE 2: as MODE 0 but tile = psi(r) (nonlocal grid), then the EES Z gather
 //   MODE 3: EES scatter -> tile -> x FFT(+) -> r2c unpack -> y FFT(+) -> zbuf row
+//   MODE 4: as MODE 1 from psi(r) stored by MODE 0 (psir) instead of the
+//           gather, y FFT(-) and x FFT(-); the zbuf row is output only
+// MODE 0 also stores psi(r) to psir when it is given.
 // Pencils (y columns, x row pairs) go through in chunks of at most G; the
 // block synchronises between the passes.  In MODE 1 the forward DFT_N2, the
 // V_KS product and the backward DFT_N2 of an x pencil run back to back in
@@ -216,9 +219,11 @@ struct Plane2Smem {
 // for: the modes that keep a real-space tile (0, 2, 3) run 512 threads with
 // two FP32 / one FP64 block per SM; the V_KS mode, which has no tile, runs
 // 256 threads with three FP32 / two FP64 blocks per SM.
-template <typename R, int MODE> __host__ __device__ constexpr int p2_threads() { return MODE == 1 ? 256 : 512; }
+template <typename R, int MODE> __host__ __device__ constexpr int p2_threads() {
+  return (MODE == 1 || MODE == 4) ? 256 : 512;
+}
 template <typename R, int MODE> __host__ __device__ constexpr int p2_min_blocks() {
-  return MODE == 1 ? (sizeof(R) == 4 ? 3 : 2) : (sizeof(R) == 4 ? 2 : 1);
+  return (MODE == 1 || MODE == 4) ? (sizeof(R) == 4 ? 3 : 2) : (sizeof(R) == 4 ? 2 : 1);
 }
 
 template <typename R, int MODE, int N1, int N2>
@@ -226,10 +231,11 @@ __global__ void __launch_bounds__(p2_threads<R, MODE>(), p2_min_blocks<R, MODE>(
 k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlines,
          const int* __restrict__ line_kx, const int* __restrict__ line_ky, int nkx,
          const double2* __restrict__ twg, const double* __restrict__ occ, const R* __restrict__ vks,
-         double* __restrict__ rho_part, int ngroup, Plane2Smem L, EesArgs E) {
+         double* __restrict__ rho_part, int ngroup, Plane2Smem L, EesArgs E, R* __restrict__ psir) {
   typedef typename CplxOf<R>::T C;
   constexpr int N = N1 * N2;
   constexpr int LDY = N + 1;
+  constexpr bool VKS = MODE == 1 || MODE == 4;
   static_assert(N1 <= 16, "pass B pads a pencil to 16 threads");
   typedef PencilLd<N1, N2> LD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -244,7 +250,7 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
   const int sb = g * nper, se = min(nstate, sb + nper);
   constexpr int npairs = (N + 1) / 2;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const R* vz = (MODE == 1) ? vks + (size_t)z * N * N : nullptr;
+  const R* vz = VKS ? vks + (size_t)z * N * N : nullptr;
   load_twiddles(tw, twg, N);
   if (MODE == 0) {
     for (int i = threadIdx.x; i < N * N; i += blockDim.x) tile[i] = (R)0;
@@ -285,12 +291,13 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
   };
   for (int s = sb; s < se; ++s) {
     C* row = zbuf + ((size_t)s * N + z) * ldl;
+    R* pr = psir ? psir + ((size_t)s * N + z) * N * N : nullptr;  // psi(r) of this plane, [y][x]
     if (MODE == 3) {
       for (int i = threadIdx.x; i < N * N; i += blockDim.x) tile[i] = (R)0;
       __syncthreads();
       ees_scatter_plane(tile, N, z, s, E, warp, lane, p2_threads<R, MODE>() / 32);
       __syncthreads();
-    } else {
+    } else if (MODE != 4) {
       for (int i = threadIdx.x; i < nkx * LDY; i += blockDim.x) P[i] = cmk<C>(0.0, 0.0);
       __syncthreads();
       for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
@@ -307,7 +314,7 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
     for (int p0 = 0; p0 < npairs; p0 += gsz) {
       const int gp = min(gsz, npairs - p0);
       constexpr int SA = (MODE == 3) ? +1 : -1;
-      for (int it = threadIdx.x; it < gp * N2; it += blockDim.x) {
+      for (int it = threadIdx.x; MODE != 4 && it < gp * N2; it += blockDim.x) {
         const int pp = it / N2, n2 = it - pp * N2;
         const int y1 = 2 * (p0 + pp), y2 = y1 + 1;
         C u[N1];
@@ -331,22 +338,36 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
 #pragma unroll
         for (int k1 = 0; k1 < N1; ++k1) s1[pp * LD::ps1 + k1 * LD::ls1 + n2] = u[k1];
       }
-      __syncthreads();
+      if (MODE != 4) __syncthreads();
       // pass B: one pencil per 16 threads (k1 < N1 active)
       for (int it = threadIdx.x; it < gp * 16; it += blockDim.x) {
         const int pp = it >> 4, k1 = it & 15;
         if (k1 >= N1) continue;
         const int y1 = 2 * (p0 + pp), y2 = y1 + 1;
         C w[N2];
+        if (MODE == 4) {
+          // psi(r) of the row pair at x = k1 + N1 k2
 #pragma unroll
-        for (int n2 = 0; n2 < N2; ++n2) w[n2] = s1[pp * LD::ps1 + k1 * LD::ls1 + n2];
-        RDft<N2, SA>::run(w);
+          for (int k2 = 0; k2 < N2; ++k2) {
+            const int x = k1 + N1 * k2;
+            w[k2].x = __ldcs(pr + y1 * N + x);
+            w[k2].y = (y2 < N) ? __ldcs(pr + y2 * N + x) : (R)0;
+          }
+        } else {
+#pragma unroll
+          for (int n2 = 0; n2 < N2; ++n2) w[n2] = s1[pp * LD::ps1 + k1 * LD::ls1 + n2];
+          RDft<N2, SA>::run(w);
+        }
         if (MODE == 0) {
 #pragma unroll
           for (int k2 = 0; k2 < N2; ++k2) {
             const int x = k1 + N1 * k2;
             tile[y1 * N + x] += o * w[k2].x * w[k2].x;
             if (y2 < N) tile[y2 * N + x] += o * w[k2].y * w[k2].y;
+            if (pr) {
+              pr[y1 * N + x] = w[k2].x;
+              if (y2 < N) pr[y2 * N + x] = w[k2].y;
+            }
           }
         } else if (MODE == 2) {
 #pragma unroll
@@ -375,7 +396,7 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
         }
       }
       __syncthreads();
-      if (MODE == 1) {
+      if (VKS) {
         // inverse, second half: DFT_N1(+) over k1 -> natural order in s1
         for (int it = threadIdx.x; it < gp * N2; it += blockDim.x) {
           const int pp = it / N2, m2 = it - pp * N2;
@@ -388,10 +409,10 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
         }
         __syncthreads();
       }
-      if (MODE == 1 || MODE == 3) {
+      if (VKS || MODE == 3) {
         // two-for-one r2c unpack of the natural-order result into P[kx][y]
-        const C* nat = (MODE == 1) ? s1 : s2;
-        const int pst = (MODE == 1) ? LD::ps1 : LD::ps2;
+        const C* nat = VKS ? s1 : s2;
+        const int pst = VKS ? LD::ps1 : LD::ps2;
         for (int it = threadIdx.x; it < gp * nkx; it += blockDim.x) {
           const int pp = it / nkx, k = it - pp * nkx;
           const int y1 = 2 * (p0 + pp), y2 = y1 + 1;
@@ -410,7 +431,7 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
       ees_gather_plane(tile, N, z, s, E, warp, lane, p2_threads<R, MODE>() / 32);
       __syncthreads();
     }
-    if (MODE == 1 || MODE == 3) {
+    if (VKS || MODE == 3) {
       y_fft(std::integral_constant<int, +1>{});
       for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
         int ky = line_ky[l]; if (ky < 0) ky += N;
@@ -435,8 +456,8 @@ template <typename C, typename R, int N1, int N2>
 static Plane2Smem plane2_layout(int nkx, int mode) {
   constexpr int N = N1 * N2;
   typedef PencilLd<N1, N2> LD;
-  const bool need_tile = mode != 1;
-  const bool need_s2 = mode == 1 || mode == 3;
+  const bool need_tile = mode != 1 && mode != 4;
+  const bool need_s2 = mode == 1 || mode == 3 || mode == 4;
   Plane2Smem L;
   size_t o = 0;
   L.tw = o; o += align_up(N * sizeof(C), 16);
@@ -445,7 +466,7 @@ static Plane2Smem plane2_layout(int nkx, int mode) {
   const size_t fixed = o + 32;
   const size_t per = (LD::ps1 + (need_s2 ? LD::ps2 : 0)) * sizeof(C);
   const int want = nkx > (N + 1) / 2 ? nkx : (N + 1) / 2;
-  const int target = mode == 1 ? (sizeof(R) == 4 ? 3 : 2) : (sizeof(R) == 4 ? 2 : 1);
+  const int target = (mode == 1 || mode == 4) ? (sizeof(R) == 4 ? 3 : 2) : (sizeof(R) == 4 ? 2 : 1);
   long g = 0;
   for (int k = target; k >= 1; --k) {
     size_t budget = (size_t)(228 * 1024) / k - 1024;
@@ -570,7 +591,7 @@ cudaError_t oa_pencil_zbwd(int precision, cudaStream_t st, int n, const void* zb
 template <typename R, int MODE, int N1, int N2>
 static cudaError_t plane2_n(cudaStream_t st, void* zbuf, int nstate, int ldl, int nlines, const int* lkx,
                             const int* lky, int nz, int nkx, const double2* tw, const double* occ, const void* vks,
-                            double* rho_part, int ngroup, const EesArgs& E) {
+                            double* rho_part, int ngroup, const EesArgs& E, void* psir) {
   typedef typename CplxOf<R>::T C;
   const Plane2Smem L = plane2_layout<C, R, N1, N2>(nkx, MODE);
   if (L.G < 1 || L.total > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
@@ -578,17 +599,17 @@ static cudaError_t plane2_n(cudaStream_t st, void* zbuf, int nstate, int ldl, in
       cudaFuncSetAttribute(k_plane2<R, MODE, N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
   if (e != cudaSuccess) return e;
   dim3 grid(nz, ngroup);
-  k_plane2<R, MODE, N1, N2><<<grid, p2_threads<R, MODE>(), L.total, st>>>((C*)zbuf, nstate, ldl, nlines, lkx, lky, nkx,
-                                                                     tw, occ, (const R*)vks, rho_part, ngroup, L, E);
+  k_plane2<R, MODE, N1, N2><<<grid, p2_threads<R, MODE>(), L.total, st>>>(
+      (C*)zbuf, nstate, ldl, nlines, lkx, lky, nkx, tw, occ, (const R*)vks, rho_part, ngroup, L, E, (R*)psir);
   return cudaGetLastError();
 }
 
 template <typename R, int MODE>
 static cudaError_t plane2(cudaStream_t st, int n, void* zbuf, int nstate, int ldl, int nlines, const int* lkx,
                           const int* lky, int nz, int nkx, const double2* tw, const double* occ, const void* vks,
-                          double* rho_part, int ngroup, const EesArgs& E) {
+                          double* rho_part, int ngroup, const EesArgs& E, void* psir) {
 #define OA_CALL(A, B) \
-  plane2_n<R, MODE, A, B>(st, zbuf, nstate, ldl, nlines, lkx, lky, nz, nkx, tw, occ, vks, rho_part, ngroup, E)
+  plane2_n<R, MODE, A, B>(st, zbuf, nstate, ldl, nlines, lkx, lky, nz, nkx, tw, occ, vks, rho_part, ngroup, E, psir)
   OA_PENCIL_DISPATCH(n, OA_CALL)
 #undef OA_CALL
   return cudaErrorNotSupported;
@@ -599,15 +620,16 @@ static cudaError_t plane2(cudaStream_t st, int n, void* zbuf, int nstate, int ld
 // kernel)
 cudaError_t oa_pencil_plane(int precision, int mode, cudaStream_t st, int n, void* zbuf, int nstate, int ldl,
                             int nlines, const int* lkx, const int* lky, int nz, int nkx, const double2* tw,
-                            const double* occ, const void* vks, double* rho_part, int ngroup, const EesArgs& E) {
+                            const double* occ, const void* vks, double* rho_part, int ngroup, const EesArgs& E,
+                            void* psir) {
 #define OA_MODE(M)                                                                                              \
   if (mode == M)                                                                                                \
     return precision == OA_FP64                                                                                 \
                ? plane2<double, M>(st, n, zbuf, nstate, ldl, nlines, lkx, lky, nz, nkx, tw, occ, vks, rho_part, \
-                                   ngroup, E)                                                                   \
+                                   ngroup, E, psir)                                                             \
                : plane2<float, M>(st, n, zbuf, nstate, ldl, nlines, lkx, lky, nz, nkx, tw, occ, vks, rho_part,  \
-                                  ngroup, E);
-  OA_MODE(0) OA_MODE(1) OA_MODE(2) OA_MODE(3)
+                                  ngroup, E, psir);
+  OA_MODE(0) OA_MODE(1) OA_MODE(2) OA_MODE(3) OA_MODE(4)
 #undef OA_MODE
   return cudaErrorNotSupported;
 }
@@ -615,7 +637,7 @@ cudaError_t oa_pencil_plane(int precision, int mode, cudaStream_t st, int n, voi
 template <typename C, typename R, int N1, int N2>
 static size_t plane2_smem_max(int nkx) {
   size_t m = 0;
-  for (int mode = 0; mode < 4; ++mode) {
+  for (int mode = 0; mode < 5; ++mode) {
     const size_t t = plane2_layout<C, R, N1, N2>(nkx, mode).total;
     if (t > m) m = t;
   }

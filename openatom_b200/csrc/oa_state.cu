@@ -365,7 +365,8 @@ cudaError_t oa_pencil_zbwd(int precision, cudaStream_t st, int n, const void* zb
                            int nblk, const double2* dyp);
 cudaError_t oa_pencil_plane(int precision, int mode, cudaStream_t st, int n, void* zbuf, int nstate, int ldl,
                             int nlines, const int* lkx, const int* lky, int nz, int nkx, const double2* tw,
-                            const double* occ, const void* vks, double* rho_part, int ngroup, const EesArgs& E);
+                            const double* occ, const void* vks, double* rho_part, int ngroup, const EesArgs& E,
+                            void* psir);
 
 template <typename R>
 static cudaError_t launch_zfwd(oa_ctx* c, cudaStream_t st, const double2* psi, int s0, int ns) {
@@ -430,20 +431,25 @@ cudaError_t oa_launch_state_zfwd(oa_ctx* c, cudaStream_t s, const double2* psi, 
                           c->nlines, c->zbuf, c->ldl, c->tw_z, nullptr);
   return c->precision == OA_FP64 ? launch_zfwd<double>(c, s, psi, s0, ns) : launch_zfwd<float>(c, s, psi, s0, ns);
 }
-static cudaError_t pencil_plane(oa_ctx* c, cudaStream_t s, int mode) {
+static cudaError_t pencil_plane(oa_ctx* c, cudaStream_t s, int mode, void* psir) {
   if (c->nx != c->ny || !oa_pencil_supported(c->nx)) return cudaErrorNotSupported;
   const EesArgs E = {nullptr, nullptr, nullptr, nullptr, 0, 0};
   return oa_pencil_plane(c->precision, mode, s, c->nx, c->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx,
-                         c->line_ky, c->nz, c->nkx_s, c->tw_x, c->occ, c->vks, c->rho_part, c->ngroup, E);
+                         c->line_ky, c->nz, c->nkx_s, c->tw_x, c->occ, c->vks, c->rho_part, c->ngroup, E, psir);
 }
 
+// The density pass also stores psi(r) (c->psir) when the two-pass kernels
+// run; the V_KS pass then starts from it (MODE 4) instead of redoing the
+// forward y and x transforms.  c->psir_valid marks that the last density
+// pass stored it.
 cudaError_t oa_launch_state_plane_density(oa_ctx* c, cudaStream_t s) {
-  const cudaError_t e = pencil_plane(c, s, 0);
+  const cudaError_t e = pencil_plane(c, s, 0, c->psir);
+  c->psir_valid = (e == cudaSuccess && c->psir) ? 1 : 0;
   if (e != cudaErrorNotSupported) return e;
   return c->precision == OA_FP64 ? launch_plane<double, 0>(c, s) : launch_plane<float, 0>(c, s);
 }
 cudaError_t oa_launch_state_plane_vks(oa_ctx* c, cudaStream_t s) {
-  const cudaError_t e = pencil_plane(c, s, 1);
+  const cudaError_t e = c->psir_valid ? pencil_plane(c, s, 4, c->psir) : pencil_plane(c, s, 1, nullptr);
   if (e != cudaErrorNotSupported) return e;
   return c->precision == OA_FP64 ? launch_plane<double, 1>(c, s) : launch_plane<float, 1>(c, s);
 }
@@ -487,7 +493,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
   err = cudaErrorNotSupported;
   if (pp)
     err = oa_pencil_plane(c->precision, 2, st, e->na, e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky,
-                          e->nc, c->nkx_s, e->tw_a, c->occ, nullptr, nullptr, e->ngroup, E);
+                          e->nc, c->nkx_s, e->tw_a, c->occ, nullptr, nullptr, e->ngroup, E, nullptr);
   if (err == cudaErrorNotSupported) {
     err = cudaFuncSetAttribute(k_state_plane<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
     if (err != cudaSuccess) return err;
@@ -502,7 +508,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
   err = cudaErrorNotSupported;
   if (pp)
     err = oa_pencil_plane(c->precision, 3, st, e->na, e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky,
-                          e->nc, c->nkx_s, e->tw_a, c->occ, nullptr, nullptr, e->ngroup, E);
+                          e->nc, c->nkx_s, e->tw_a, c->occ, nullptr, nullptr, e->ngroup, E, nullptr);
   if (err == cudaErrorNotSupported) {
     err = cudaFuncSetAttribute(k_state_plane<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
     if (err != cudaSuccess) return err;

@@ -78,6 +78,27 @@ def test_forces_eke(case):
     assert rel(eke.cpu().numpy(), ek) < E_TOL
 
 
+def test_forces_from_stored_psi_r(case):
+    """vks_apply_fft_bwd without recompute_fwd starts from the psi(r) the
+    density pass stored; same forces as the recomputing path."""
+    import torch
+    s, ctx, psi = case
+    nx, ny, nz = s.nfft
+    rng = np.random.default_rng(6)
+    v = rng.standard_normal((nz, ny, nx)) * 0.3
+    ctx.state_fft_fwd(psi)
+    ctx.set_vks(torch.from_numpy(v).cuda())
+    f = torch.zeros_like(psi)
+    eke = torch.zeros(s.nstate, dtype=torch.float64, device="cuda")
+    ctx.vks_apply_fft_bwd(psi, f, recompute_fwd=False, eke_out=eke)
+    torch.cuda.synchronize()
+    psir = O.state_g_to_r(s.psi, s)
+    fr = O.add_forces(O.vks_forces(psir, v, s), None, s)
+    fr, ek = O.eke(s.psi, fr, s)
+    assert rel(f.cpu().numpy(), fr) < F_TOL
+    assert rel(eke.cpu().numpy(), ek) < E_TOL
+
+
 def test_forces_with_nonlocal_input(case):
     import torch
     s, ctx, psi = case
