@@ -228,7 +228,7 @@ def run_ours(args):
     # per-kernel timing (CUDA events on the launch stream) for the roofline
     kt = dmx.ctx.time_kernels(dmx.psi, reps=5)
     kt64 = d64.ctx.time_kernels(d64.psi, reps=5)
-    roof = roofline(sysm, dmx, kt)
+    roof = roofline(sysm, dmx, kt, args.config)
 
     cpu = None
     if rk == 0 and not args.no_cpu:
@@ -270,7 +270,13 @@ def run_ours(args):
     return 0
 
 
-def roofline(sysm, drv, kt):
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
+# the plane kernels on the w32 workload, from one ncu capture
+# (profiles/k_plane2_w32.md); None for other workloads.
+TRAFFIC_W32 = {"state_plane_density": 793.9e6, "state_plane_vks": 725.9e6}
+
+
+def roofline(sysm, drv, kt, config=None):
     """Roofline of the dominant kernel from its algorithmic bytes and its
     CUDA-event time (see DESIGN.md for the per-kernel byte formulas)."""
     peaks = {}
@@ -288,8 +294,9 @@ def roofline(sysm, drv, kt):
         return {"kernel": name, "bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
                 "traffic": None, "peak_source": src}
     ach = b / (kt[name] * 1e-3) / 1e9
+    traffic = TRAFFIC_W32.get(name) if config == "w32" else None
     return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-            "traffic": None, "algorithmic_bytes": b, "peak_source": src}
+            "traffic": traffic, "algorithmic_bytes": b, "peak_source": src}
 
 
 def main():

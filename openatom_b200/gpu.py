@@ -302,12 +302,15 @@ class CPContext:
         cb = 2 * z["rbytes"]
         zrow = n * nz * nl * cb          # the z-line buffer
         coef = n * ng * 16               # one coefficient array
+        psir = n * npts * z["rbytes"]    # psi(r) of all states
         return {
             "state_zfwd": coef + zrow,
-            "state_plane_density": zrow + g * npts * 8,
+            # reads the z-line buffer, writes the density partials and psi(r)
+            "state_plane_density": zrow + g * npts * 8 + psir,
             "rho_xc": g * npts * 8 + 2 * npts * 8,
             "vks_build": npts * 8 * 2 + npts * z["rbytes"],
-            "state_plane_vks": 2 * zrow + g * npts * z["rbytes"],
+            # reads psi(r) and V_KS, writes the z-line buffer
+            "state_plane_vks": psir + npts * z["rbytes"] + zrow,
             "state_zbwd": zrow + 2 * coef + ng * 8,
             "pc_forward_S": coef + n * n * 8,
             "pc_backward": 3 * coef,
