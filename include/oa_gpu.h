@@ -195,7 +195,7 @@ oa_status oa_gpu_set_atoms(oa_ctx *ctx, void *stream, const double *pos_host);
  * e.g. CP_State_GSpacePlane.C:1407-1409). */
 oa_status oa_gpu_time_kernels(oa_ctx *ctx, void *stream, const double *psi, int reps, double *ms_out);
 
-/* Sizes for byte/flop accounting (see oa_abi.cu): out[0..9]. */
+/* Sizes for byte/flop accounting (see oa_abi.cu): out[0..11]. */
 oa_status oa_gpu_sizes(const oa_ctx *ctx, long *out);
 
 /* Nonlocal energy and coefficient forces by the structure-factor method

@@ -24,6 +24,8 @@ int oa_pencil_supported(int n);
 int oa_ns_cluster_size(int n);
 cudaError_t oa_launch_ortho_ns(cudaStream_t s, const double* S, int n, double bscale, double tol, int max_iter,
                                double* work, double* T, int* status, double* errv, int grid);
+int oa_integrate_nblk(int ng, int nstate);
+int oa_pair_plane_supported(int n, int nkx, int nlines, int ldl);
 cudaError_t oa_launch_integrate(cudaStream_t s, const double2* F, double2* V, double2* P, const double* cmass,
                                 int ng, int nstate, int r0, int r1, int iend, double dt, int complete_prev,
                                 double* kepart, int nblk);
@@ -154,6 +156,31 @@ static cudaError_t upload(T** dst, const T* src, size_t n) {
   return e;
 }
 
+// Per kx column of the state sphere: the run of z-lines {first line, ky of
+// the first line, line count, 0} when the lines of every column are
+// consecutive with ky rising by one (the reference's line order) and
+// |ky| < ny / 2; false otherwise (the state-pair plane kernels then stay off).
+static bool column_runs(const oa_system_desc* d, int nkx, std::vector<int>* out) {
+  std::vector<int>& r = *out;
+  r.assign((size_t)4 * nkx, 0);
+  std::vector<char> seen(nkx, 0);
+  int l = 0;
+  while (l < d->nlines) {
+    const int kx = d->line_kx[l];
+    if (kx < 0 || kx >= nkx || seen[kx]) return false;
+    seen[kx] = 1;
+    int e = l + 1;
+    while (e < d->nlines && d->line_kx[e] == kx) {
+      if (d->line_ky[e] != d->line_ky[e - 1] + 1) return false;
+      ++e;
+    }
+    if (2 * d->line_ky[l] <= -d->ny || 2 * d->line_ky[e - 1] >= d->ny) return false;
+    r[4 * kx] = l; r[4 * kx + 1] = d->line_ky[l]; r[4 * kx + 2] = e - l;
+    l = e;
+  }
+  return true;
+}
+
 static int pick_groups(int nz, int nstate, int bps, int nsm) {
   // minimise ceil(nz g / (nsm bps)) * ceil(nstate / g)
   int best = 1;
@@ -224,6 +251,8 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     if (bps < 1) bps = 1;
   }
   c->ngroup = pick_groups(d->nz, d->nstate, bps, nsm);
+  c->ngroup_pair = pick_groups(d->nz, (d->nstate + 1) / 2, 1, nsm);
+  c->rho_ngroup = c->ngroup;
   c->nblk_z = (d->nlines + OA_LB - 1) / OA_LB;
 
   const size_t csz = precision == OA_FP64 ? sizeof(double2) : sizeof(float2);
@@ -282,8 +311,18 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     TRY(cudaMalloc(&c->phase, (size_t)d->natm * 3 * (2 * c->kmax_tab + 1) * sizeof(double2)));
     c->zbuf_bytes = (size_t)d->nstate * d->nz * c->ldl * csz;
     TRY(cudaMalloc(&c->zbuf, c->zbuf_bytes));
-    TRY(cudaMalloc(&c->rho_part, (size_t)c->ngroup * c->npts * sizeof(double)));
-    if (d->nx == d->ny && oa_pencil_supported(d->nx)) TRY(cudaMalloc(&c->psir, (size_t)d->nstate * c->npts * rsz));
+    {
+      std::vector<int> runs;
+      if (precision == OA_MIXED && d->nx == d->ny &&
+          oa_pair_plane_supported(d->nx, c->nkx_s, d->nlines, c->ldl) && column_runs(d, c->nkx_s, &runs))
+        TRY(upload(&c->pair_cols, runs.data(), runs.size()));
+    }
+    {
+      const int ng = c->ngroup > c->ngroup_pair ? c->ngroup : c->ngroup_pair;
+      TRY(cudaMalloc(&c->rho_part, (size_t)ng * c->npts * sizeof(double)));
+    }
+    if (d->nx == d->ny && oa_pencil_supported(d->nx))
+      TRY(cudaMalloc(&c->psir, (size_t)(d->nstate + 1) / 2 * 2 * c->npts * rsz));
     TRY(cudaMalloc(&c->rho, (size_t)c->npts * sizeof(double)));
     TRY(cudaMalloc(&c->vxc, (size_t)c->npts * sizeof(double)));
     TRY(cudaMalloc(&c->vks, (size_t)c->npts * rsz));
@@ -298,7 +337,7 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     TRY(cudaMalloc(&p->ns_work, ((size_t)5 * d->nstate * d->nstate + p->ns_grid + 32) * sizeof(double)));
     TRY(cudaMalloc(&p->ns_status, 4 * sizeof(int)));
     TRY(cudaMalloc(&p->ns_err, 2 * sizeof(double)));
-    p->ke_nblk = 2 * nsm;
+    p->ke_nblk = oa_integrate_nblk(d->ng, d->nstate);
     TRY(cudaMalloc(&p->ke_part, p->ke_nblk * sizeof(double)));
     TRY(cudaMalloc(&p->dev_e, 16 * sizeof(double)));
     TRY(cudaMemset(p->dev_e, 0, 16 * sizeof(double)));
@@ -351,7 +390,7 @@ extern "C" oa_status oa_gpu_destroy(oa_ctx* c) {
   ees_free(c);
   oa_ctx_pc* p = pcx(c);
   void* dev[] = {c->line_kx, c->line_ky, c->line_off, c->line_nneg, c->line_npos, c->kx, c->g2, c->tw_x, c->tw_y,
-                 c->tw_z, c->spl, c->q_type, c->atm_type, c->atm_perm, c->pos, c->psir, c->phase, c->occ, c->zbuf, c->rho_part, c->rho,
+                 c->tw_z, c->spl, c->q_type, c->atm_type, c->atm_perm, c->pos, c->psir, c->pair_cols, c->phase, c->occ, c->zbuf, c->rho_part, c->rho,
                  c->vks, c->vxc, c->dz, c->red, c->eke_part, p->part, p->ns_work, p->ns_status, p->ns_err,
                  p->partner, p->cmass, p->ke_part, p->dev_e, p->mat_a, p->mat_x, p->eye, p->vtmp, p->upart,
                  p->pl_big[0], p->pl_big[1], p->pl_big[2], p->pl_ma, p->pl_mb,
@@ -367,7 +406,8 @@ extern "C" oa_status oa_gpu_destroy(oa_ctx* c) {
 extern "C" size_t oa_gpu_scratch_bytes(const oa_ctx* c) {
   if (!c) return 0;
   const size_t rsz = c->precision == OA_FP64 ? 8 : 4;
-  return c->zbuf_bytes + (size_t)c->ngroup * c->npts * 8 + (size_t)c->npts * (16 + rsz) +
+  const int ng = c->ngroup > c->ngroup_pair ? c->ngroup : c->ngroup_pair;
+  return c->zbuf_bytes + (size_t)ng * c->npts * 8 + (size_t)c->npts * (16 + rsz) +
          (size_t)c->nz * c->ldl_d * 16;
 }
 
@@ -683,6 +723,8 @@ extern "C" oa_status oa_gpu_sizes(const oa_ctx* c, long* out) {
   // kernels of oa_gpu_cp_step: state_fft_fwd 3 + vks_build 10 + nl_sf 7 + vks_apply 4 + lambda 4 +
   // integrate 3 + S 2 + Newton-Schulz 1 + Psi T 1
   out[9] = 3 + 10 + 7 + 4 + 4 + 3 + 2 + 1 + 1;
+  out[10] = c->pair_cols ? 1 : 0;  // state-pair plane kernels in use (mixed form)
+  out[11] = c->ngroup_pair;
   return OA_OK;
 }
 

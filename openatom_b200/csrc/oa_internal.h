@@ -36,8 +36,12 @@ struct oa_ctx {
   int nkx_d;              // density half-spectrum columns (nx/2 + 1)
   int nlines_d, ldl_d;    // density z-lines (nkx_d * ny) and padded stride
   int ngroup;             // state groups in the plane kernels
-  void* psir;             // [nstate][nz][ny][nx] psi(r), compute precision (two-pass kernels)
-  int psir_valid;         // the last density pass stored psir
+  int ngroup_pair;        // pair groups in the state-pair plane kernels
+  int rho_ngroup;         // groups summed in rho_part by the last density pass
+  int* pair_cols;         // [nkx_s] {first line, ky of the first line, lines, 0}: FP32 pair kernels
+  void* psir;             // psi(r), compute precision: [nstate][nz][ny][nx] (two-pass kernels)
+                          // or [nstate/2][nz][ny][nx] pairs (state-pair kernels)
+  int psir_valid;         // the last density pass stored psir: 1 per state, 2 per pair
   double box, vol, ecut_psi, ecut_rho, alp_ewd;
   double gzvps_sum;
   int nspl; double spl_gmin, spl_dg;

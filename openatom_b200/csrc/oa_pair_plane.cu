@@ -1,0 +1,419 @@
+// State-pair plane kernels of the FP32 state FFT path: the density pass
+// (psi(r) of two states per x transform, |psi|^2 summed into registers,
+// psi(r) stored) and the V_KS pass that starts from that stored psi(r).
+// They do the same work as k_plane2 MODE 0 and MODE 4 (oa_pencil.cu), with
+// the two real states of a pair packed into one complex x transform
+// (psi_a + i psi_b) instead of two rows of one state, so that
+//   - one block moves one plane of two states per iteration with four block
+//     barriers (y pass A, y pass B, x pass A, x pass B);
+//   - each thread keeps a fixed set of x pass B outputs, so the density of a
+//     plane sums in registers over all states of the block, and the inverse
+//     twiddles of those outputs sit in registers;
+//   - the y pass reads the z-line rows (copied to shared memory with
+//     cp.async one pair ahead) through the per-column line runs instead of
+//     a zero-filled scatter, and writes the result rows straight back;
+//   - every shared-memory access pattern is free of bank conflicts: pass A
+//     walks consecutive pencils (odd pencil strides), pass B walks one pencil
+//     per 16 lanes (odd element strides).
+// psi(r) is stored per pair, [pair][z][y][x] float2 (psi_a, psi_b).
+//
+// Reference work replaced (as k_plane2):
+//   FFTcache::doStpFFTGtoR_Rchare (fftCache.C:1167) + the density part of
+//     CP_State_RealSpacePlane::doFFT / doReduction (:349-363, 450-517)     -> k_pair_density
+//   CP_State_RealSpacePlane::unpackVks (:530-597) + doStpFFTRtoG_Rchare
+//     (fftCache.C:1252-1319)                                               -> k_pair_vks
+#include "oa_rdft.cuh"
+#include "oa_state_common.cuh"
+
+// x pass B slots (16 lanes per row, N rows) per thread: the smallest count
+// that gives a warp-multiple block of at most 640 threads
+__host__ __device__ constexpr int pair_xb_waves(int n) {
+  for (int w = 1; w <= 8; ++w)
+    if ((16 * n) % w == 0 && ((16 * n) / w) % 32 == 0 && (16 * n) / w <= 640) return w;
+  return 0;
+}
+
+template <int N1, int N2> struct PairCfg {
+  static constexpr int N = N1 * N2;
+  static constexpr int XBW = pair_xb_waves(N);
+  static constexpr int NT = XBW ? 16 * N / XBW : 32;
+  static constexpr int LDY = N | 1;           // P[st][kx][LDY]
+  static constexpr int LS1 = N2 | 1;          // pass A -> B buffer [pencil][k1][n2]
+  static constexpr int PS1 = (N1 * LS1) | 1;
+  static constexpr int LS2 = N1;              // inverse B' -> A' buffer [row][m2][k1]
+  static constexpr int PS2 = (N2 * N1) | 1;
+  static constexpr int NJ = N2 / 2 + 1;       // m2 classes {j, N2 - j}
+};
+
+struct PairSmem {
+  size_t tw, col, rows, P, S, total;
+  int lr;  // z-line row length in shared memory (float2, even)
+};
+
+static __device__ __forceinline__ void pp_cp16(void* sdst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc));
+}
+static __device__ __forceinline__ void pp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int K> static __device__ __forceinline__ void pp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(K));
+}
+
+// x-spectrum value at index k of row y (Hermitian extension of kx in [0, nkx))
+template <int N, int LDY>
+static __device__ __forceinline__ float2 pp_herm(const float2* P, int nkx, int k, int y) {
+  float2 v = make_float2(0.f, 0.f);
+  if (k <= N / 2) {
+    if (k < nkx) v = P[k * LDY + y];
+    if (k == 0 || 2 * k == N) v.y = 0.f;
+  } else {
+    const int kk = N - k;
+    if (kk < nkx) { v = P[kk * LDY + y]; v.y = -v.y; }
+  }
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// density pass: block (z, group) runs the pairs of its group through plane z
+// ---------------------------------------------------------------------------
+template <int N1, int N2>
+__global__ void __launch_bounds__(PairCfg<N1, N2>::NT, 1)
+k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int nlines,
+               const int4* __restrict__ cols, int nkx, const double2* __restrict__ twg,
+               const double* __restrict__ occ, double* __restrict__ rho_part, int ngroup,
+               float2* __restrict__ psir, PairSmem L) {
+  typedef PairCfg<N1, N2> CF;
+  constexpr int N = CF::N, NT = CF::NT, XBW = CF::XBW;
+  constexpr int LDY = CF::LDY, LS1 = CF::LS1, PS1 = CF::PS1;
+  static_assert(N1 <= 16 && XBW > 0, "pair plane: unsupported factorisation");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tw = (float2*)(smem_raw + L.tw);
+  int4* col = (int4*)(smem_raw + L.col);
+  float2* rb = (float2*)(smem_raw + L.rows);
+  float2* P = (float2*)(smem_raw + L.P);
+  float2* S = (float2*)(smem_raw + L.S);
+  const int tid = threadIdx.x;
+  const int z = blockIdx.x, g = blockIdx.y;
+  const int npair = (nstate + 1) / 2;
+  const int nper = (npair + ngroup - 1) / ngroup;
+  const int qb = g * nper, qe = min(npair, qb + nper);
+  const int lr = L.lr, nch = lr / 2;
+  const int npc = 2 * nkx;
+  for (int i = tid; i < N; i += NT) tw[i] = make_float2((float)twg[i].x, (float)twg[i].y);
+  for (int i = tid; i < nkx; i += NT) col[i] = cols[i];
+  float dens[XBW][N2];
+#pragma unroll
+  for (int j = 0; j < XBW; ++j)
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) dens[j][k2] = 0.f;
+  auto prefetch = [&](int q, int buf) {
+    for (int it = tid; it < 2 * nch; it += NT) {
+      const int st = it >= nch ? 1 : 0, ch = it - st * nch;
+      const int s = 2 * q + st;
+      if (s < nstate) pp_cp16(rb + (size_t)(2 * buf + st) * lr + 2 * ch, zbuf + ((size_t)s * nz + z) * ldl + 2 * ch);
+    }
+    pp_commit();
+  };
+  if (qb < qe) prefetch(qb, 0);
+  for (int q = qb; q < qe; ++q) {
+    const int buf = (q - qb) & 1;
+    if (q + 1 < qe) {
+      prefetch(q + 1, buf ^ 1);
+      pp_wait<1>();
+    } else {
+      pp_wait<0>();
+    }
+    const bool has1 = 2 * q + 1 < nstate;
+    __syncthreads();
+    // y pass A: pencil (state, column) fastest; zero outside the column's run
+    for (int it = tid; it < N2 * npc; it += NT) {
+      const int n2 = it / npc, pc = it - n2 * npc;
+      const int st = pc >= nkx ? 1 : 0, cx = pc - st * nkx;
+      const int4 cr = col[cx];
+      const float2* r = rb + (size_t)(2 * buf + st) * lr + cr.x;
+      const bool live = st == 0 || has1;
+      float2 u[N1];
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) {
+        const int i = N2 * n1 + n2;
+        const int ky = (2 * i <= N) ? i : i - N;
+        const int l = ky - cr.y;
+        u[n1] = (live && l >= 0 && l < cr.z) ? r[l] : make_float2(0.f, 0.f);
+      }
+      pass_a<N1, N2, -1>(u, n2, tw);
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) S[pc * PS1 + k1 * LS1 + n2] = u[k1];
+    }
+    __syncthreads();
+    // y pass B: one pencil per 16 lanes -> P[st][kx][y]
+    for (int it = tid; it < 16 * npc; it += NT) {
+      const int pc = it >> 4, k1 = it & 15;
+      if (k1 >= N1) continue;
+      float2 w[N2];
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) w[n2] = S[pc * PS1 + k1 * LS1 + n2];
+      RDft<N2, -1>::run(w);
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) P[pc * LDY + k1 + N1 * k2] = w[k2];
+    }
+    __syncthreads();
+    // x pass A: rows fastest; the pair packs as psi_a + i psi_b
+    for (int it = tid; it < N2 * N; it += NT) {
+      const int n2 = it / N, y = it - n2 * N;
+      float2 u[N1];
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) {
+        const int k = N2 * n1 + n2;
+        const float2 a = pp_herm<N, LDY>(P, nkx, k, y);
+        const float2 b = pp_herm<N, LDY>(P + nkx * LDY, nkx, k, y);
+        u[n1] = make_float2(a.x - b.y, a.y + b.x);
+      }
+      pass_a<N1, N2, -1>(u, n2, tw);
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) S[y * PS1 + k1 * LS1 + n2] = u[k1];
+    }
+    __syncthreads();
+    // x pass B: fixed slots per thread; density and psi(r)
+    const float o0 = (float)occ[2 * q];
+    const float o1 = has1 ? (float)occ[2 * q + 1] : 0.f;
+    float2* pq = psir + ((size_t)q * nz + z) * N * N;
+#pragma unroll
+    for (int j = 0; j < XBW; ++j) {
+      const int it = tid + NT * j;
+      const int y = it >> 4, k1 = it & 15;
+      if (k1 < N1) {
+        float2 w[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) w[n2] = S[y * PS1 + k1 * LS1 + n2];
+        RDft<N2, -1>::run(w);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+          dens[j][k2] += o0 * w[k2].x * w[k2].x + o1 * w[k2].y * w[k2].y;
+          __stcs(pq + y * N + k1 + N1 * k2, w[k2]);
+        }
+      }
+    }
+  }
+  double* out = rho_part + ((size_t)g * nz + z) * N * N;
+#pragma unroll
+  for (int j = 0; j < XBW; ++j) {
+    const int it = tid + NT * j;
+    const int y = it >> 4, k1 = it & 15;
+    if (k1 < N1) {
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) out[y * N + k1 + N1 * k2] = (double)dens[j][k2];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// V_KS pass from the stored psi(r): psi V_KS occ -> x FFT(+) with the r2c
+// unpack of the pair -> y FFT(+) -> the z-line rows of both states
+// ---------------------------------------------------------------------------
+template <int N1, int N2>
+__global__ void __launch_bounds__(PairCfg<N1, N2>::NT, 1)
+k_pair_vks(float2* __restrict__ zbuf, int nstate, int nz, int ldl, const int4* __restrict__ cols, int nkx,
+           const double2* __restrict__ twg, const double* __restrict__ occ, const float* __restrict__ vks,
+           int ngroup, const float2* __restrict__ psir, PairSmem L) {
+  typedef PairCfg<N1, N2> CF;
+  constexpr int N = CF::N, NT = CF::NT, XBW = CF::XBW, NJ = CF::NJ;
+  constexpr int LDY = CF::LDY, LS1 = CF::LS1, PS1 = CF::PS1, LS2 = CF::LS2, PS2 = CF::PS2;
+  static_assert(N1 <= 16 && XBW > 0 && NT % 16 == 0, "pair plane: unsupported factorisation");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tw = (float2*)(smem_raw + L.tw);
+  int4* col = (int4*)(smem_raw + L.col);
+  float2* P = (float2*)(smem_raw + L.P);
+  float2* S = (float2*)(smem_raw + L.S);
+  const int tid = threadIdx.x;
+  const int z = blockIdx.x, g = blockIdx.y;
+  const int npair = (nstate + 1) / 2;
+  const int nper = (npair + ngroup - 1) / ngroup;
+  const int qb = g * nper, qe = min(npair, qb + nper);
+  const int npc = 2 * nkx;
+  const int kf = tid & 15;  // this thread's k1 in x pass B' (NT is a multiple of 16)
+  for (int i = tid; i < N; i += NT) tw[i] = make_float2((float)twg[i].x, (float)twg[i].y);
+  for (int i = tid; i < nkx; i += NT) col[i] = cols[i];
+  __syncthreads();
+  float2 tk[N2];
+  const float* vz = vks + (size_t)z * N * N;
+  if (kf < N1) {
+#pragma unroll
+    for (int m2 = 0; m2 < N2; ++m2) tk[m2] = tw_rt<+1>(tw, kf * m2);
+  }
+  for (int q = qb; q < qe; ++q) {
+    const bool has1 = 2 * q + 1 < nstate;
+    const float o0 = (float)occ[2 * q];
+    const float o1 = has1 ? (float)occ[2 * q + 1] : 0.f;
+    const float2* pq = psir + ((size_t)q * nz + z) * N * N;
+    __syncthreads();
+    // x pass B' (inverse, first half): DFT_N2(+) over k2, twiddle -> S[y][m2][k1]
+    if (kf < N1) {
+#pragma unroll
+      for (int j = 0; j < XBW; ++j) {
+        const int y = (tid + NT * j) >> 4;
+        float2 w[N2];
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+          const float2 p = __ldcs(pq + y * N + kf + N1 * k2);
+          const float v = __ldg(vz + y * N + kf + N1 * k2);
+          w[k2] = make_float2(p.x * v * o0, p.y * v * o1);
+        }
+        RDft<N2, +1>::run(w);
+        S[y * PS2 + kf] = w[0];
+#pragma unroll
+        for (int m2 = 1; m2 < N2; ++m2) S[y * PS2 + m2 * LS2 + kf] = cmul(w[m2], tk[m2]);
+      }
+    }
+    __syncthreads();
+    // x pass A' (inverse, second half) on the classes {j, N2 - j}, then the
+    // two-for-one unpack of the pair into P[st][kx][y] for kx < nkx
+    for (int it = tid; it < NJ * N; it += NT) {
+      const int jj = it / N, y = it - jj * N;
+      const int ma = jj, mb = (N2 - jj) % N2;
+      const bool two = ma != mb;
+      float2 za[N1], zb[N1];
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) za[k1] = S[y * PS2 + ma * LS2 + k1];
+      RDft<N1, +1>::run(za);
+      if (two) {
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) zb[k1] = S[y * PS2 + mb * LS2 + k1];
+        RDft<N1, +1>::run(zb);
+      }
+      auto put = [&](int K, float2 a, float2 bp) {
+        const float2 b = make_float2(bp.x, -bp.y);
+        P[K * LDY + y] = make_float2((a.x + b.x) * 0.5f, (a.y + b.y) * 0.5f);
+        P[(nkx + K) * LDY + y] = make_float2((a.y - b.y) * 0.5f, -(a.x - b.x) * 0.5f);
+      };
+#pragma unroll
+      for (int m1 = 0; m1 < N1; ++m1) {
+        const int K = ma + N2 * m1;
+        if (K < nkx) {
+          const float2 pa = (jj == 0) ? za[(N1 - m1) % N1] : (two ? zb[N1 - 1 - m1] : za[N1 - 1 - m1]);
+          put(K, za[m1], pa);
+        }
+        if (two) {
+          const int Kb = mb + N2 * m1;
+          if (Kb < nkx) put(Kb, zb[m1], za[N1 - 1 - m1]);
+        }
+      }
+    }
+    __syncthreads();
+    // y pass A' (+): pencils fastest
+    for (int it = tid; it < N2 * npc; it += NT) {
+      const int n2 = it / npc, pc = it - n2 * npc;
+      float2 u[N1];
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) u[n1] = P[pc * LDY + N2 * n1 + n2];
+      pass_a<N1, N2, +1>(u, n2, tw);
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) S[pc * PS1 + k1 * LS1 + n2] = u[k1];
+    }
+    __syncthreads();
+    // y pass B' (+) -> the column's z-line run of each state
+    for (int it = tid; it < 16 * npc; it += NT) {
+      const int pc = it >> 4, k1 = it & 15;
+      if (k1 >= N1) continue;
+      const int st = pc >= nkx ? 1 : 0, cx = pc - st * nkx;
+      if (st == 1 && !has1) continue;
+      float2 w[N2];
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) w[n2] = S[pc * PS1 + k1 * LS1 + n2];
+      RDft<N2, +1>::run(w);
+      const int4 cr = col[cx];
+      float2* row = zbuf + ((size_t)(2 * q + st) * nz + z) * ldl + cr.x;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) {
+        const int i = k1 + N1 * k2;
+        const int ky = (2 * i <= N) ? i : i - N;
+        const int l = ky - cr.y;
+        if (l >= 0 && l < cr.z) row[l] = w[k2];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+template <int N1, int N2>
+static PairSmem pair_layout(int nkx, int nlines, int mode) {
+  typedef PairCfg<N1, N2> CF;
+  PairSmem L;
+  size_t o = 0;
+  L.lr = (nlines + 1) & ~1;
+  L.tw = o; o += align_up((size_t)CF::N * sizeof(float2), 16);
+  L.col = o; o += align_up((size_t)nkx * sizeof(int4), 16);
+  L.rows = o; o += mode == 0 ? (size_t)4 * L.lr * sizeof(float2) : 0;
+  L.P = o; o += align_up((size_t)2 * nkx * CF::LDY * sizeof(float2), 16);
+  size_t s = (size_t)(CF::N > 2 * nkx ? CF::N : 2 * nkx) * CF::PS1;
+  if (mode != 0 && (size_t)CF::N * CF::PS2 > s) s = (size_t)CF::N * CF::PS2;
+  L.S = o; o += align_up(s * sizeof(float2), 16);
+  L.total = o;
+  return L;
+}
+
+template <int N1, int N2>
+static cudaError_t pair_launch(int mode, cudaStream_t st, void* zbuf, int nstate, int nz, int ldl, int nlines,
+                               const int* cols, int nkx, const double2* tw, const double* occ, const void* vks,
+                               double* rho_part, int ngroup, void* psir) {
+  typedef PairCfg<N1, N2> CF;
+  if (CF::XBW == 0 || N1 > 16 || 2 * nkx > CF::N + 2 || (ldl & 1)) return cudaErrorNotSupported;
+  const PairSmem L = pair_layout<N1, N2>(nkx, nlines, mode);
+  if (L.total > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
+  const dim3 grid(nz, ngroup);
+  cudaError_t e;
+  if (mode == 0) {
+    e = cudaFuncSetAttribute(k_pair_density<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    if (e != cudaSuccess) return e;
+    k_pair_density<N1, N2><<<grid, CF::NT, L.total, st>>>((const float2*)zbuf, nstate, nz, ldl, nlines,
+                                                          (const int4*)cols, nkx, tw, occ, rho_part, ngroup,
+                                                          (float2*)psir, L);
+  } else {
+    e = cudaFuncSetAttribute(k_pair_vks<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    if (e != cudaSuccess) return e;
+    k_pair_vks<N1, N2><<<grid, CF::NT, L.total, st>>>((float2*)zbuf, nstate, nz, ldl, (const int4*)cols, nkx, tw,
+                                                      occ, (const float*)vks, ngroup, (const float2*)psir, L);
+  }
+  return cudaGetLastError();
+}
+
+#define OA_PAIR_DISPATCH(n, CALL)                                    \
+  switch (n) {                                                       \
+    case 12: return CALL(4, 3);                                      \
+    case 20: return CALL(4, 5);                                      \
+    case 24: return CALL(6, 4);                                      \
+    case 36: return CALL(6, 6);                                      \
+    case 40: return CALL(8, 5);                                      \
+    case 64: return CALL(8, 8);                                      \
+    case 96: return CALL(12, 8);                                     \
+    case 108: return CALL(12, 9);                                    \
+    case 160: return CALL(16, 10);                                   \
+    default: break;                                                  \
+  }
+
+// mode 0: density pass (rho_part[group][z][y][x], psi(r) pairs stored);
+// mode 4: V_KS pass from those psi(r) pairs.  nx = ny = n; cols = per kx
+// column {first line, ky of the first line, line count, 0}.  Returns
+// cudaErrorNotSupported when n or the shared memory has no pair kernel.
+cudaError_t oa_pair_plane(int mode, cudaStream_t st, int n, void* zbuf, int nstate, int nz, int ldl, int nlines,
+                          const int* cols, int nkx, const double2* tw, const double* occ, const void* vks,
+                          double* rho_part, int ngroup, void* psir) {
+#define OA_CALL(A, B) \
+  pair_launch<A, B>(mode, st, zbuf, nstate, nz, ldl, nlines, cols, nkx, tw, occ, vks, rho_part, ngroup, psir)
+  OA_PAIR_DISPATCH(n, OA_CALL)
+#undef OA_CALL
+  return cudaErrorNotSupported;
+}
+
+// whether the pair kernels cover length n with these sizes (both modes)
+int oa_pair_plane_supported(int n, int nkx, int nlines, int ldl) {
+#define OA_CALL(A, B)                                                                                     \
+  (PairCfg<A, B>::XBW > 0 && 2 * nkx <= PairCfg<A, B>::N + 2 && !(ldl & 1) &&                             \
+   pair_layout<A, B>(nkx, nlines, 0).total <= (size_t)OA_MAX_SMEM &&                                      \
+   pair_layout<A, B>(nkx, nlines, 4).total <= (size_t)OA_MAX_SMEM)                                        \
+      ? 1 : 0
+  OA_PAIR_DISPATCH(n, OA_CALL)
+#undef OA_CALL
+  return 0;
+}

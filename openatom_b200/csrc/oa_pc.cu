@@ -327,29 +327,45 @@ k_ortho_ns(const double* __restrict__ S, int n, double bscale, double tol, int m
 // ---------------------------------------------------------------------------
 // integrator
 // ---------------------------------------------------------------------------
-__global__ void k_integrate(const double2* __restrict__ F, double2* __restrict__ V, double2* __restrict__ P,
-                            const double* __restrict__ cmass, int ng, int nstate, int r0, int r1, int iend,
-                            double dt, int complete_prev, double* __restrict__ kepart) {
-  __shared__ double sh[32];
-  const size_t total = (size_t)nstate * ng;
+// One block per (chunk of OA_INT_CHUNK coefficients, state): every thread
+// loads its OA_INT_UNROLL coefficients before it updates them, and writes one
+// kinetic-energy partial per block (kepart[state * gridDim.x + chunk]).
+#define OA_INT_UNROLL 4
+#define OA_INT_CHUNK (256 * OA_INT_UNROLL)
+__global__ void __launch_bounds__(256)
+k_integrate(const double2* __restrict__ F, double2* __restrict__ V, double2* __restrict__ P,
+            const double* __restrict__ cmass, int ng, int nstate, int r0, int r1, int iend,
+            double dt, int complete_prev, double* __restrict__ kepart) {
+  __shared__ double sh[8];
   const double dt2 = 0.5 * dt;
+  const size_t base = (size_t)blockIdx.y * ng;
+  const int i0 = blockIdx.x * OA_INT_CHUNK + threadIdx.x;
+  double2 f[OA_INT_UNROLL], v[OA_INT_UNROLL], p[OA_INT_UNROLL];
+  double m[OA_INT_UNROLL];
+#pragma unroll
+  for (int u = 0; u < OA_INT_UNROLL; ++u) {
+    const int i = i0 + 256 * u;
+    if (i >= r0 && i < ng) {
+      f[u] = F[base + i]; v[u] = V[base + i]; p[u] = P[base + i]; m[u] = __ldg(cmass + i);
+    }
+  }
   double ke = 0.0;
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(t % ng);
-    if (i < r0) continue;
-    double2 f = F[t], v = V[t];
-    const double m = cmass[i];
+#pragma unroll
+  for (int u = 0; u < OA_INT_UNROLL; ++u) {
+    const int i = i0 + 256 * u;
+    if (i < r0 || i >= ng) continue;
+    double2 ff = f[u], vv = v[u], pp = p[u];
+    const double h = dt2 / m[u];
     const bool g0 = (i < r1);
-    if (g0) { f.y = 0.0; v.y = 0.0; }
-    if (complete_prev) { v.x += f.x * (dt2 / m); v.y += f.y * (dt2 / m); if (g0) v.y = 0.0; }
-    const double mk = (i >= r1 && i < iend) ? 2.0 * m : m;
-    ke += mk * (v.x * v.x + v.y * v.y);
-    v.x += f.x * (dt2 / m); v.y += f.y * (dt2 / m);
-    if (g0) v.y = 0.0;
-    V[t] = v;
-    double2 p = P[t];
-    p.x += v.x * dt; p.y += v.y * dt;
-    P[t] = p;
+    if (g0) { ff.y = 0.0; vv.y = 0.0; }
+    if (complete_prev) { vv.x += ff.x * h; vv.y += ff.y * h; if (g0) vv.y = 0.0; }
+    const double mk = (i >= r1 && i < iend) ? 2.0 * m[u] : m[u];
+    ke += mk * (vv.x * vv.x + vv.y * vv.y);
+    vv.x += ff.x * h; vv.y += ff.y * h;
+    if (g0) vv.y = 0.0;
+    V[base + i] = vv;
+    pp.x += vv.x * dt; pp.y += vv.y * dt;
+    P[base + i] = pp;
   }
   double w = ke;
 #pragma unroll
@@ -358,10 +374,13 @@ __global__ void k_integrate(const double2* __restrict__ F, double2* __restrict__
   __syncthreads();
   if (threadIdx.x == 0) {
     double s = 0.0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += sh[k];
-    kepart[blockIdx.x] = 0.5 * s;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += sh[k];
+    kepart[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = 0.5 * s;
   }
 }
+
+int oa_integrate_nblk(int ng, int nstate) { return nstate * ((ng + OA_INT_CHUNK - 1) / OA_INT_CHUNK); }
 
 __global__ void k_sync_redundant(double2* __restrict__ P, double2* __restrict__ V, const int* __restrict__ partner,
                                  int nred, int ng, int nstate) {
@@ -478,7 +497,9 @@ cudaError_t oa_launch_ortho_ns(cudaStream_t s, const double* S, int n, double bs
 cudaError_t oa_launch_integrate(cudaStream_t s, const double2* F, double2* V, double2* P, const double* cmass,
                                 int ng, int nstate, int r0, int r1, int iend, double dt, int complete_prev,
                                 double* kepart, int nblk) {
-  k_integrate<<<nblk, 256, 0, s>>>(F, V, P, cmass, ng, nstate, r0, r1, iend, dt, complete_prev, kepart);
+  if (nblk != oa_integrate_nblk(ng, nstate)) return cudaErrorInvalidValue;
+  const dim3 grid((ng + OA_INT_CHUNK - 1) / OA_INT_CHUNK, nstate);
+  k_integrate<<<grid, 256, 0, s>>>(F, V, P, cmass, ng, nstate, r0, r1, iend, dt, complete_prev, kepart);
   return cudaGetLastError();
 }
 

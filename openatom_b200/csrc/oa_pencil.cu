@@ -290,8 +290,8 @@ k_plane2(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int nlin
     }
   };
   for (int s = sb; s < se; ++s) {
-    C* row = zbuf + ((size_t)s * N + z) * ldl;
-    R* pr = psir ? psir + ((size_t)s * N + z) * N * N : nullptr;  // psi(r) of this plane, [y][x]
+    C* row = zbuf + ((size_t)s * gridDim.x + z) * ldl;
+    R* pr = psir ? psir + ((size_t)s * gridDim.x + z) * N * N : nullptr;  // psi(r) of this plane, [y][x]
     if (MODE == 3) {
       for (int i = threadIdx.x; i < N * N; i += blockDim.x) tile[i] = (R)0;
       __syncthreads();

@@ -360,7 +360,7 @@ size_t oa_rho_plane_smem_bytes(int nx, int ny, int nkx, int npair, int ychunk) {
 
 cudaError_t oa_launch_rho_xc(oa_ctx* c, cudaStream_t s) {
   const int nblk = 4 * 148;
-  k_rho_xc<<<nblk, OA_NTHREADS, 0, s>>>(c->rho_part, c->ngroup, (size_t)c->npts, 1.0 / c->vol, c->rho, c->vxc, c->red);
+  k_rho_xc<<<nblk, OA_NTHREADS, 0, s>>>(c->rho_part, c->rho_ngroup, (size_t)c->npts, 1.0 / c->vol, c->rho, c->vxc, c->red);
   return cudaGetLastError();
 }
 

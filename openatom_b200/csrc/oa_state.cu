@@ -363,6 +363,9 @@ cudaError_t oa_pencil_zbwd(int precision, cudaStream_t st, int n, const void* zb
                            const double2* psi, const double2* fnl, double2* force, const double* g2,
                            const double* occ, int ng, int s0, int ns, double scale, double ecut, double* eke_part,
                            int nblk, const double2* dyp);
+cudaError_t oa_pair_plane(int mode, cudaStream_t st, int n, void* zbuf, int nstate, int nz, int ldl, int nlines,
+                          const int* cols, int nkx, const double2* tw, const double* occ, const void* vks,
+                          double* rho_part, int ngroup, void* psir);
 cudaError_t oa_pencil_plane(int precision, int mode, cudaStream_t st, int n, void* zbuf, int nstate, int ldl,
                             int nlines, const int* lkx, const int* lky, int nz, int nkx, const double2* tw,
                             const double* occ, const void* vks, double* rho_part, int ngroup, const EesArgs& E,
@@ -442,13 +445,27 @@ static cudaError_t pencil_plane(oa_ctx* c, cudaStream_t s, int mode, void* psir)
 // run; the V_KS pass then starts from it (MODE 4) instead of redoing the
 // forward y and x transforms.  c->psir_valid marks that the last density
 // pass stored it.
+// In the mixed form with the state-pair kernels (c->pair_cols set) both
+// passes run two states per x transform and psi(r) is stored per pair
+// (psir_valid 2).
 cudaError_t oa_launch_state_plane_density(oa_ctx* c, cudaStream_t s) {
+  if (c->pair_cols && c->psir) {
+    const cudaError_t e = oa_pair_plane(0, s, c->nx, c->zbuf, c->nstate, c->nz, c->ldl, c->nlines, c->pair_cols,
+                                        c->nkx_s, c->tw_x, c->occ, nullptr, c->rho_part, c->ngroup_pair, c->psir);
+    c->psir_valid = e == cudaSuccess ? 2 : 0;
+    c->rho_ngroup = c->ngroup_pair;
+    if (e != cudaErrorNotSupported) return e;
+  }
+  c->rho_ngroup = c->ngroup;
   const cudaError_t e = pencil_plane(c, s, 0, c->psir);
   c->psir_valid = (e == cudaSuccess && c->psir) ? 1 : 0;
   if (e != cudaErrorNotSupported) return e;
   return c->precision == OA_FP64 ? launch_plane<double, 0>(c, s) : launch_plane<float, 0>(c, s);
 }
 cudaError_t oa_launch_state_plane_vks(oa_ctx* c, cudaStream_t s) {
+  if (c->psir_valid == 2)
+    return oa_pair_plane(4, s, c->nx, c->zbuf, c->nstate, c->nz, c->ldl, c->nlines, c->pair_cols, c->nkx_s,
+                         c->tw_x, c->occ, c->vks, nullptr, c->ngroup_pair, c->psir);
   const cudaError_t e = c->psir_valid ? pencil_plane(c, s, 4, c->psir) : pencil_plane(c, s, 1, nullptr);
   if (e != cudaErrorNotSupported) return e;
   return c->precision == OA_FP64 ? launch_plane<double, 1>(c, s) : launch_plane<float, 1>(c, s);

@@ -284,9 +284,10 @@ class CPContext:
         _check(self._lib.oa_gpu_set_atoms(self._h, self._stream(), a.ctypes.data_as(_dp)))
 
     def sizes(self) -> dict:
-        out = (C.c_long * 10)()
+        out = (C.c_long * 12)()
         _check(self._lib.oa_gpu_sizes(self._h, out))
-        keys = ("nstate", "ng", "nlines", "nz", "ldl", "ngroup", "npts", "rbytes", "nlines_d", "launches_per_step")
+        keys = ("nstate", "ng", "nlines", "nz", "ldl", "ngroup", "npts", "rbytes", "nlines_d", "launches_per_step",
+                "pair_planes", "ngroup_pair")
         return {k: int(v) for k, v in zip(keys, out)}
 
     def time_kernels(self, psi, reps: int = 5) -> dict:
