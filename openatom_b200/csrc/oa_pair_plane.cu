@@ -46,7 +46,7 @@ template <int N1, int N2> struct PairCfg {
 };
 
 struct PairSmem {
-  size_t tw, col, rows, P, S, total;
+  size_t tw, col, xh, rows, P, S, total;
   int lr;  // z-line row length in shared memory (float2, even)
 };
 
@@ -99,8 +99,26 @@ k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int
   const int qb = g * nper, qe = min(npair, qb + nper);
   const int lr = L.lr, nch = lr / 2;
   const int npc = 2 * nkx;
+  int lp = 0;
+  while ((1 << lp) < npc) ++lp;
+  int2* xh = (int2*)(smem_raw + L.xh);
   for (int i = tid; i < N; i += NT) tw[i] = make_float2((float)twg[i].x, (float)twg[i].y);
   for (int i = tid; i < nkx; i += NT) col[i] = cols[i];
+  // Hermitian table of x pass A, entry n2 * N1 + n1 for kx index k = N2 n1 + n2:
+  // {P offset of the stored column (k or N - k), imaginary sign}: +1 stored
+  // column, -1 its conjugate, 0 for the real DC / Nyquist terms; offset -1
+  // where the spectrum is zero
+  for (int i = tid; i < N; i += NT) {
+    const int n2 = i / N1, n1 = i - n2 * N1, k = N2 * n1 + n2;
+    int off = -1;
+    float sg = 0.f;
+    if (2 * k <= N) {
+      if (k < nkx) { off = k * LDY; sg = (k == 0 || 2 * k == N) ? 0.f : 1.f; }
+    } else if (N - k < nkx) {
+      off = (N - k) * LDY; sg = -1.f;
+    }
+    xh[i] = make_int2(off, __float_as_int(sg));
+  }
   float dens[XBW][N2];
 #pragma unroll
   for (int j = 0; j < XBW; ++j)
@@ -125,9 +143,11 @@ k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int
     }
     const bool has1 = 2 * q + 1 < nstate;
     __syncthreads();
-    // y pass A: pencil (state, column) fastest; zero outside the column's run
-    for (int it = tid; it < N2 * npc; it += NT) {
-      const int n2 = it / npc, pc = it - n2 * npc;
+    // y pass A: pencil (state, column) fastest in slots of 2^lp per n2;
+    // zero outside the column's run
+    for (int it = tid; it < (N2 << lp); it += NT) {
+      const int n2 = it >> lp, pc = it & ((1 << lp) - 1);
+      if (pc >= npc) continue;
       const int st = pc >= nkx ? 1 : 0, cx = pc - st * nkx;
       const int4 cr = col[cx];
       const float2* r = rb + (size_t)(2 * buf + st) * lr + cr.x;
@@ -157,16 +177,22 @@ k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int
       for (int k2 = 0; k2 < N2; ++k2) P[pc * LDY + k1 + N1 * k2] = w[k2];
     }
     __syncthreads();
-    // x pass A: rows fastest; the pair packs as psi_a + i psi_b
+    // x pass A: rows fastest (n2 warp-uniform); the pair packs as
+    // psi_a + i psi_b, read through the Hermitian table
     for (int it = tid; it < N2 * N; it += NT) {
       const int n2 = it / N, y = it - n2 * N;
+      const int2* hx = xh + n2 * N1;
       float2 u[N1];
 #pragma unroll
       for (int n1 = 0; n1 < N1; ++n1) {
-        const int k = N2 * n1 + n2;
-        const float2 a = pp_herm<N, LDY>(P, nkx, k, y);
-        const float2 b = pp_herm<N, LDY>(P + nkx * LDY, nkx, k, y);
-        u[n1] = make_float2(a.x - b.y, a.y + b.x);
+        const int2 t = hx[n1];
+        float2 v = make_float2(0.f, 0.f);
+        if (t.x >= 0) {
+          const float2 a = P[t.x + y], b = P[t.x + nkx * LDY + y];
+          const float sg = __int_as_float(t.y);
+          v = make_float2(fmaf(-sg, b.y, a.x), fmaf(sg, a.y, b.x));
+        }
+        u[n1] = v;
       }
       pass_a<N1, N2, -1>(u, n2, tw);
 #pragma unroll
@@ -217,6 +243,11 @@ k_pair_vks(float2* __restrict__ zbuf, int nstate, int nz, int ldl, const int4* _
            int ngroup, const float2* __restrict__ psir, PairSmem L) {
   typedef PairCfg<N1, N2> CF;
   constexpr int N = CF::N, NT = CF::NT, XBW = CF::XBW, NJ = CF::NJ;
+  // L2 prefetch of a psi(r) pair plane (N^2 float2) in PF_PARTS pieces of
+  // PF_BYTES (multiples of 16 bytes)
+  constexpr int PF_PARTS = (N * N * 8) % (16 * 8) == 0 ? 8 : ((N * N * 8) % (16 * 4) == 0 ? 4 : 1);
+  constexpr int PF_BYTES = N * N * 8 / PF_PARTS;
+  static_assert(PF_BYTES % 16 == 0, "psi(r) plane prefetch needs 16-byte pieces");
   constexpr int LDY = CF::LDY, LS1 = CF::LS1, PS1 = CF::PS1, LS2 = CF::LS2, PS2 = CF::PS2;
   static_assert(N1 <= 16 && XBW > 0 && NT % 16 == 0, "pair plane: unsupported factorisation");
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -230,6 +261,8 @@ k_pair_vks(float2* __restrict__ zbuf, int nstate, int nz, int ldl, const int4* _
   const int nper = (npair + ngroup - 1) / ngroup;
   const int qb = g * nper, qe = min(npair, qb + nper);
   const int npc = 2 * nkx;
+  int lp = 0;
+  while ((1 << lp) < npc) ++lp;
   const int kf = tid & 15;  // this thread's k1 in x pass B' (NT is a multiple of 16)
   for (int i = tid; i < N; i += NT) tw[i] = make_float2((float)twg[i].x, (float)twg[i].y);
   for (int i = tid; i < nkx; i += NT) col[i] = cols[i];
@@ -245,6 +278,11 @@ k_pair_vks(float2* __restrict__ zbuf, int nstate, int nz, int ldl, const int4* _
     const float o0 = (float)occ[2 * q];
     const float o1 = has1 ? (float)occ[2 * q + 1] : 0.f;
     const float2* pq = psir + ((size_t)q * nz + z) * N * N;
+    if (q + 1 < qe && tid < PF_PARTS) {
+      // the next pair's psi(r) plane heads for L2 while this pair computes
+      const char* nxt = (const char*)(pq + (size_t)nz * N * N) + (size_t)tid * PF_BYTES;
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(nxt), "r"(PF_BYTES) : "memory");
+    }
     __syncthreads();
     // x pass B' (inverse, first half): DFT_N2(+) over k2, twiddle -> S[y][m2][k1]
     if (kf < N1) {
@@ -299,9 +337,10 @@ k_pair_vks(float2* __restrict__ zbuf, int nstate, int nz, int ldl, const int4* _
       }
     }
     __syncthreads();
-    // y pass A' (+): pencils fastest
-    for (int it = tid; it < N2 * npc; it += NT) {
-      const int n2 = it / npc, pc = it - n2 * npc;
+    // y pass A' (+): pencils fastest in slots of 2^lp per n2
+    for (int it = tid; it < (N2 << lp); it += NT) {
+      const int n2 = it >> lp, pc = it & ((1 << lp) - 1);
+      if (pc >= npc) continue;
       float2 u[N1];
 #pragma unroll
       for (int n1 = 0; n1 < N1; ++n1) u[n1] = P[pc * LDY + N2 * n1 + n2];
@@ -344,6 +383,7 @@ static PairSmem pair_layout(int nkx, int nlines, int mode) {
   L.lr = (nlines + 1) & ~1;
   L.tw = o; o += align_up((size_t)CF::N * sizeof(float2), 16);
   L.col = o; o += align_up((size_t)nkx * sizeof(int4), 16);
+  L.xh = o; o += align_up((size_t)CF::N * sizeof(int2), 16);
   L.rows = o; o += mode == 0 ? (size_t)4 * L.lr * sizeof(float2) : 0;
   L.P = o; o += align_up((size_t)2 * nkx * CF::LDY * sizeof(float2), 16);
   size_t s = (size_t)(CF::N > 2 * nkx ? CF::N : 2 * nkx) * CF::PS1;
