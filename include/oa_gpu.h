@@ -181,6 +181,13 @@ oa_status oa_gpu_integrate(oa_ctx *ctx, void *stream, const double *force, doubl
  * its T to the identity. */
 oa_status oa_gpu_psiv_reset(oa_ctx *ctx, void *stream, const double *psi, double *psi_t, double *vpsi);
 
+/* The same reset in the mixed-precision form: both products (A and X psi)
+ * as split-BF16 tensor-core GEMMs with nterm (2 or 3) bf16 planes and FP32
+ * accumulation; v is updated in FP64.  Same reference work as
+ * oa_gpu_psiv_reset. */
+oa_status oa_gpu_psiv_reset_mixed(oa_ctx *ctx, void *stream, const double *psi, double *psi_t, double *vpsi,
+                                  int nterm);
+
 /* Copy new atom positions (host [natm][3], bohr) for the next vks_build
  * (the structure-factor phases are rebuilt from them every call). */
 oa_status oa_gpu_set_atoms(oa_ctx *ctx, void *stream, const double *pos_host);
@@ -233,7 +240,8 @@ typedef struct {
  * integration, orthonormalisation, in native code with one host
  * synchronisation at the end.  The PsiV reset triggered by max|S - 2I| >
  * norb_tol (Ortho::maxCheck, ortho.C:455-475) is decided on the device and
- * runs at the end of the step, as oa_gpu_psiv_reset would.  energies_out (optional, host [11]):
+ * runs at the end of the step, as oa_gpu_psiv_reset would (oa_gpu_psiv_reset_mixed
+ * with state->mixed_nterm planes when that is nonzero).  energies_out (optional, host [11]):
  * EKE EHART EEXT EWALD_RECIP EEXC MUXC FICT_KE ENL, Newton-Schulz
  * iterations, residual, max|S - 2I|.  Coefficient arrays must be 16-byte
  * aligned. */

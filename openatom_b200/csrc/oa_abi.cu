@@ -41,15 +41,16 @@ cudaError_t oa_launch_umma_bwd(cudaStream_t s, int nterm, const double* M1, cons
                                long ncol, long kx0_cols, double* out, int* err_flag);
 int oa_umma_max_kb(int m, int n, int nsm);
 cudaError_t oa_split_kc(cudaStream_t s, int nt, const double* X, int rows, int rows_pad, long K, long ldx,
-                        long kx0_cols, double w_kx0, __nv_bfloat16* P, long ldp);
+                        long kx0_cols, double w_kx0, __nv_bfloat16* P, long ldp, const int* cond = nullptr);
 int oa_tg_rows_pad(int rows, int box);
 int oa_tg_nb(int n);
 cudaError_t oa_tfwd(cudaStream_t s, int nt, const __nv_bfloat16* PA, int rows_a, const __nv_bfloat16* PB, int rows_b,
                     int m, int n, long K, long ldp, double alpha, float* part, int max_kb, double* C, int* err_flag,
-                    int nsm);
+                    int nsm, const int* cond = nullptr);
 cudaError_t oa_tbwd(cudaStream_t s, int nt, const __nv_bfloat16* PM1, const __nv_bfloat16* PX1, double a1_kx0,
                     double a1_rest, const __nv_bfloat16* PM2, const __nv_bfloat16* PX2, double a2, int nj, int nk,
-                    long ncol, long ldx, long kx0_cols, double* out, int* err_flag);
+                    long ncol, long ldx, long kx0_cols, double* out, int* err_flag, const double* yadd = nullptr,
+                    const int* cond = nullptr);
 cudaError_t oa_launch_pc_fwd_mn(cudaStream_t s, const double* A, const double* B, int m, int n, long K,
                                 long kx0_cols, double w_kx0, double alpha, double* part, int nkb, double* C);
 cudaError_t oa_launch_pc_bwd_jk(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
@@ -620,49 +621,6 @@ cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, 
     OA_CUDA_TRY(e_);                                                                          \
   } while (0)
 
-// Velocity part of the PsiV reset (CP_State_GSpacePlane.C:3590-3600,
-// 3750-3760 with the orthoT velocity projection): X = sym(psi v^T) / 4 with
-// the S weights, v <- v - X psi (in place).  cond: optional device flag; the
-// launches do nothing when it is 0.
-static oa_status psiv_velocity(oa_ctx* c, cudaStream_t s, const double* psi, double* vpsi, const int* cond) {
-  oa_ctx_pc* p = pcx(c);
-  const int n = c->nstate;
-  OA_ALIGN_TRY(oa_dgemm_fwd(s, psi, vpsi, n, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, p->mat_a, cond));
-  dim3 grid((n + 15) / 16, (n + 15) / 16), blk(16, 16);
-  k_sym_quarter_cond<<<grid, blk, 0, s>>>(p->mat_a, n, p->mat_x, cond);
-  OA_CUDA_TRY(cudaGetLastError());
-  OA_ALIGN_TRY(oa_dgemm_bwd_ex(s, p->mat_x, psi, -1.0, -1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0,
-                               vpsi, cond, vpsi, nullptr, nullptr));
-  return OA_OK;
-}
-
-// psi = psi_t T (FP64), also written to psi_t when the PsiV flag is set;
-// then, under the flag, the velocity projection and T = I, and the flag is
-// cleared.  The native step's orthonormalisation and PsiV reset
-// (Ortho::maxCheck, ortho.C:455-475): same results as oa_gpu_pc_backward
-// followed by oa_gpu_psiv_reset, decided on the device.
-oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* psi_t, double* psi, double* vpsi,
-                            double* Tout, int* flag) {
-  oa_ctx_pc* p = pcx(c);
-  const int n = c->nstate;
-  OA_ALIGN_TRY(oa_dgemm_bwd_ex(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, psi,
-                               nullptr, nullptr, psi_t, flag));
-  OA_STEP_CHECK(psiv_velocity(c, s, psi, vpsi, flag));
-  k_copy_cond<<<16, 256, 0, s>>>(Tout, p->eye, (size_t)n * n, flag);
-  k_flag_clear<<<1, 1, 0, s>>>(flag);
-  OA_CUDA_TRY(cudaGetLastError());
-  return OA_OK;
-}
-
-extern "C" oa_status oa_gpu_psiv_reset(oa_ctx* c, void* stream, const double* psi, double* psi_t, double* vpsi) {
-  OA_ARG_CHECK(c && psi && psi_t && vpsi, "null argument");
-  cudaStream_t s = (cudaStream_t)stream;
-  OA_STEP_CHECK(psiv_velocity(c, s, psi, vpsi, nullptr));
-  const size_t bytes = (size_t)c->nstate * c->ng * sizeof(double2);
-  OA_CUDA_TRY(cudaMemcpyAsync(psi_t, psi, bytes, cudaMemcpyDeviceToDevice, s));
-  return OA_OK;
-}
-
 extern "C" oa_status oa_gpu_set_atoms(oa_ctx* c, void* stream, const double* pos_host) {
   OA_ARG_CHECK(c && pos_host, "null argument");
   OA_CUDA_TRY(cudaMemcpyAsync(c->pos, pos_host, (size_t)3 * c->natm * sizeof(double), cudaMemcpyHostToDevice,
@@ -739,7 +697,7 @@ enum { PL_PSI = 0, PL_OTHER = 1, PL_SF = 2 };
 // the same weighting is reused; the step clears the slots whenever the
 // sources may have changed.
 static cudaError_t ensure_planes(oa_ctx* c, cudaStream_t s, int nt, int slot, const double* X, int rows,
-                                 int rows_pad, long K, long kx0_cols, double w_kx0) {
+                                 int rows_pad, long K, long kx0_cols, double w_kx0, const int* cond = nullptr) {
   oa_ctx_pc* p = pcx(c);
   if (kx0_cols == 0) w_kx0 = 1.0;
   if (w_kx0 == 1.0) kx0_cols = 0;
@@ -748,7 +706,7 @@ static cudaError_t ensure_planes(oa_ctx* c, cudaStream_t s, int nt, int slot, co
       k.kx0 == kx0_cols && k.w == w_kx0)
     return cudaSuccess;
   const cudaError_t e =
-      oa_split_kc(s, nt, X, rows, rows_pad, K, K, kx0_cols, w_kx0, (bf16*)p->pl_big[slot], p->pl_ld);
+      oa_split_kc(s, nt, X, rows, rows_pad, K, K, kx0_cols, w_kx0, (bf16*)p->pl_big[slot], p->pl_ld, cond);
   k.src = X; k.rows = rows; k.rows_pad = rows_pad; k.nt = nt; k.K = K; k.kx0 = kx0_cols; k.w = w_kx0;
   k.valid = e == cudaSuccess;
   return e;
@@ -765,26 +723,28 @@ void oa_planes_reuse(oa_ctx* c, int on) {
 // not take.  A: [m][K] (kx0 columns weighted by w_kx0), B: [n][K], in
 // plane slots sa and sb.
 static cudaError_t mixed_fwd(oa_ctx* c, cudaStream_t s, int nt, const double* A, const double* B, int m, int n,
-                             long K, long kx0_cols, double w_kx0, double alpha, double* C, int sa, int sb) {
+                             long K, long kx0_cols, double w_kx0, double alpha, double* C, int sa, int sb,
+                             const int* cond = nullptr) {
   oa_ctx_pc* p = pcx(c);
   const int mx = c->nstate > c->natm_nl ? c->nstate : c->natm_nl;
   const int nb = oa_tg_nb(n);
   const int ra = oa_tg_rows_pad(m, 128), rb = nb ? oa_tg_rows_pad(n, nb) : 0;
   if (nb && m <= mx && n <= mx && K <= p->pl_ld && ra <= p->pl_rows && rb <= p->pl_rows) {
     const bool same = B == A && (w_kx0 == 1.0 || kx0_cols == 0) && ra % nb == 0;
-    cudaError_t e = ensure_planes(c, s, nt, sa, A, m, ra, K, kx0_cols, w_kx0);
+    cudaError_t e = ensure_planes(c, s, nt, sa, A, m, ra, K, kx0_cols, w_kx0, cond);
     if (e != cudaSuccess) return e;
     const bf16* pb = (const bf16*)p->pl_big[sa];
     int rows_b = ra;
     if (!same) {
-      if ((e = ensure_planes(c, s, nt, sb, B, n, rb, K, 0, 1.0)) != cudaSuccess) return e;
+      if ((e = ensure_planes(c, s, nt, sb, B, n, rb, K, 0, 1.0, cond)) != cudaSuccess) return e;
       pb = (const bf16*)p->pl_big[sb];
       rows_b = rb;
     }
     e = oa_tfwd(s, nt, (const bf16*)p->pl_big[sa], ra, pb, rows_b, m, n, K, p->pl_ld, alpha, p->upart, p->umax_kb, C,
-                p->err_flag, p->nsm);
+                p->err_flag, p->nsm, cond);
     if (e != cudaErrorNotSupported) return e;
   }
+  if (cond) return cudaErrorNotSupported;  // the fallback kernels have no device flag
   return oa_launch_umma_fwd(s, nt, A, B, m, n, K, kx0_cols, w_kx0, alpha, p->upart, p->umax_kb, C, p->err_flag,
                             p->nsm);
 }
@@ -793,22 +753,97 @@ static cudaError_t mixed_fwd(oa_ctx* c, cudaStream_t s, int nt, const double* A,
 // X1, X2 in plane slots s1, s2.
 static cudaError_t mixed_bwd(oa_ctx* c, cudaStream_t s, int nt, const double* M1, const double* X1, double a1_kx0,
                              double a1_rest, const double* M2, const double* X2, double a2, int nj, int nk, long ncol,
-                             long kx0_cols, double* out, int s1, int s2) {
+                             long kx0_cols, double* out, int s1, int s2, const double* yadd = nullptr,
+                             const int* cond = nullptr) {
   oa_ctx_pc* p = pcx(c);
   const int mx = c->nstate > c->natm_nl ? c->nstate : c->natm_nl;
   const int nkp = oa_tg_rows_pad(nk, 32);
   if (nj <= mx && nk <= mx && ncol <= p->pl_ld && oa_tg_nb(nj) == nj && nkp <= p->pl_rows && (!M2 || s1 != s2)) {
     bf16 *pm1 = (bf16*)p->pl_ma, *pm2 = (bf16*)p->pl_mb;
-    cudaError_t e = ensure_planes(c, s, nt, s1, X1, nk, nkp, ncol, 0, 1.0);
-    if (e == cudaSuccess) e = oa_split_kc(s, nt, M1, nk, nkp, nj, nj, 0, 1.0, pm1, nj);
-    if (e == cudaSuccess && M2) e = ensure_planes(c, s, nt, s2, X2, nk, nkp, ncol, 0, 1.0);
-    if (e == cudaSuccess && M2) e = oa_split_kc(s, nt, M2, nk, nkp, nj, nj, 0, 1.0, pm2, nj);
+    cudaError_t e = ensure_planes(c, s, nt, s1, X1, nk, nkp, ncol, 0, 1.0, cond);
+    if (e == cudaSuccess) e = oa_split_kc(s, nt, M1, nk, nkp, nj, nj, 0, 1.0, pm1, nj, cond);
+    if (e == cudaSuccess && M2) e = ensure_planes(c, s, nt, s2, X2, nk, nkp, ncol, 0, 1.0, cond);
+    if (e == cudaSuccess && M2) e = oa_split_kc(s, nt, M2, nk, nkp, nj, nj, 0, 1.0, pm2, nj, cond);
     if (e != cudaSuccess) return e;
     e = oa_tbwd(s, nt, pm1, (const bf16*)p->pl_big[s1], a1_kx0, a1_rest, M2 ? pm2 : nullptr,
-                M2 ? (const bf16*)p->pl_big[s2] : nullptr, a2, nj, nkp, ncol, p->pl_ld, kx0_cols, out, p->err_flag);
+                M2 ? (const bf16*)p->pl_big[s2] : nullptr, a2, nj, nkp, ncol, p->pl_ld, kx0_cols, out, p->err_flag,
+                yadd, cond);
     if (e != cudaErrorNotSupported) return e;
   }
+  if (cond || yadd) return cudaErrorNotSupported;  // the fallback kernels have neither
   return oa_launch_umma_bwd(s, nt, M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out, p->err_flag);
+}
+
+// Velocity part of the PsiV reset (CP_State_GSpacePlane.C:3590-3600,
+// 3750-3760 with the orthoT velocity projection): X = sym(psi v^T) / 4 with
+// the S weights, v <- v - X psi (in place).  cond: optional device flag; the
+// launches do nothing when it is 0.
+static oa_status psiv_velocity(oa_ctx* c, cudaStream_t s, const double* psi, double* vpsi, const int* cond,
+                               int nterm) {
+  oa_ctx_pc* p = pcx(c);
+  const int n = c->nstate;
+  dim3 grid((n + 15) / 16, (n + 15) / 16), blk(16, 16);
+  if (nterm) {
+    // split-BF16: A = v carries the S weights (sym(v psi^T) = sym(psi v^T)),
+    // so the psi planes serve both products; v -= X psi with v added in FP64
+    cudaError_t e = mixed_fwd(c, s, nterm, vpsi, psi, n, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->mat_a, PL_OTHER,
+                              PL_PSI, cond);
+    if (e == cudaSuccess) {
+      k_sym_quarter_cond<<<grid, blk, 0, s>>>(p->mat_a, n, p->mat_x, cond);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+      e = mixed_bwd(c, s, nterm, p->mat_x, psi, -1.0, -1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0,
+                    vpsi, PL_PSI, PL_OTHER, vpsi, cond);
+    if (e != cudaErrorNotSupported) {
+      OA_CUDA_TRY(e);
+      return OA_OK;
+    }
+  }
+  OA_ALIGN_TRY(oa_dgemm_fwd(s, psi, vpsi, n, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, p->mat_a, cond));
+  k_sym_quarter_cond<<<grid, blk, 0, s>>>(p->mat_a, n, p->mat_x, cond);
+  OA_CUDA_TRY(cudaGetLastError());
+  OA_ALIGN_TRY(oa_dgemm_bwd_ex(s, p->mat_x, psi, -1.0, -1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0,
+                               vpsi, cond, vpsi, nullptr, nullptr));
+  return OA_OK;
+}
+
+// psi = psi_t T (FP64), also written to psi_t when the PsiV flag is set;
+// then, under the flag, the velocity projection and T = I, and the flag is
+// cleared.  The native step's orthonormalisation and PsiV reset
+// (Ortho::maxCheck, ortho.C:455-475): same results as oa_gpu_pc_backward
+// followed by oa_gpu_psiv_reset, decided on the device.
+oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* psi_t, double* psi, double* vpsi,
+                            double* Tout, int* flag, int nterm) {
+  oa_ctx_pc* p = pcx(c);
+  const int n = c->nstate;
+  OA_ALIGN_TRY(oa_dgemm_bwd_ex(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, psi,
+                               nullptr, nullptr, psi_t, flag));
+  OA_STEP_CHECK(psiv_velocity(c, s, psi, vpsi, flag, nterm));
+  k_copy_cond<<<16, 256, 0, s>>>(Tout, p->eye, (size_t)n * n, flag);
+  k_flag_clear<<<1, 1, 0, s>>>(flag);
+  OA_CUDA_TRY(cudaGetLastError());
+  return OA_OK;
+}
+
+static oa_status psiv_reset(oa_ctx* c, void* stream, const double* psi, double* psi_t, double* vpsi, int nterm) {
+  cudaStream_t s = (cudaStream_t)stream;
+  OA_STEP_CHECK(psiv_velocity(c, s, psi, vpsi, nullptr, nterm));
+  const size_t bytes = (size_t)c->nstate * c->ng * sizeof(double2);
+  OA_CUDA_TRY(cudaMemcpyAsync(psi_t, psi, bytes, cudaMemcpyDeviceToDevice, s));
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_psiv_reset(oa_ctx* c, void* stream, const double* psi, double* psi_t, double* vpsi) {
+  OA_ARG_CHECK(c && psi && psi_t && vpsi, "null argument");
+  return psiv_reset(c, stream, psi, psi_t, vpsi, 0);
+}
+
+extern "C" oa_status oa_gpu_psiv_reset_mixed(oa_ctx* c, void* stream, const double* psi, double* psi_t, double* vpsi,
+                                             int nterm) {
+  OA_ARG_CHECK(c && psi && psi_t && vpsi, "null argument");
+  OA_ARG_CHECK(nterm == 2 || nterm == 3, "nterm must be 2 or 3");
+  return psiv_reset(c, stream, psi, psi_t, vpsi, nterm);
 }
 
 extern "C" oa_status oa_gpu_pc_forward_mixed(oa_ctx* c, void* stream, const double* left, const double* right,

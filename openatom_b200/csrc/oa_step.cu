@@ -38,7 +38,7 @@ oa_status oa_gpu_psiv_reset(oa_ctx* ctx, void* stream, const double* psi, double
 
 int oa_ns_capturable(oa_ctx* c);
 oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* psi_t, double* psi, double* vpsi,
-                            double* Tout, int* flag);
+                            double* Tout, int* flag, int nterm);
 
 cudaError_t oa_launch_ortho_ns(cudaStream_t s, const double* S, int n, double bscale, double tol, int max_iter,
                                double* work, double* T, int* status, double* errv, int grid);
@@ -196,7 +196,7 @@ static oa_status launch_step_b(oa_ctx* c, cudaStream_t s, oa_cp_state* st) {
   k_step_check<<<1, 1, 0, s>>>(status, errv, dev_e, st->norb_tol, w->flag, w->ring, w->ring_cap);
   OA_CUDA_TRY(cudaGetLastError());
   // psi = psi_t T, and the PsiV reset when the check asked for it
-  OA_STEP_TRY(oa_psi_t_and_psiv(c, s, st->T, st->psi_t, st->psi, st->vpsi, st->T, w->flag));
+  OA_STEP_TRY(oa_psi_t_and_psiv(c, s, st->T, st->psi_t, st->psi, st->vpsi, st->T, w->flag, st->mixed_nterm));
   return OA_OK;
 }
 

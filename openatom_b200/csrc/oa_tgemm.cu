@@ -117,7 +117,8 @@ __device__ __forceinline__ void tg_tmem_ld16(uint32_t taddr, float* v) {
 // ---------------------------------------------------------------------------
 template <int NT>
 __global__ void k_split_kc(const double* __restrict__ X, int rows, int rows_pad, long K, long ldx, long kx0_cols,
-                           double w_kx0, bf16* __restrict__ P, long ldp) {
+                           double w_kx0, bf16* __restrict__ P, long ldp, const int* __restrict__ cond) {
+  if (cond && *cond == 0) return;
   const long ng = ldp / 8;
   const size_t total = (size_t)rows_pad * ng;
   const size_t pstride = (size_t)rows_pad * ldp;
@@ -169,7 +170,8 @@ __global__ void k_split_kc(const double* __restrict__ X, int rows, int rows_pad,
 template <int NT, int NB>
 __global__ void __launch_bounds__(TG_THREADS, 1)
 k_tfwd(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int m, int n, long K, int nkb,
-       int stages, float* __restrict__ part, int* __restrict__ err_flag) {
+       int stages, float* __restrict__ part, int* __restrict__ err_flag, const int* __restrict__ cond) {
+  if (cond && *cond == 0) return;
   extern __shared__ __align__(1024) unsigned char tg_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)tg_raw + 1023) & ~(uintptr_t)1023);
   constexpr uint32_t a_bytes = TG_M * TG_KS * 2, b_bytes = (uint32_t)NB * TG_KS * 2;
@@ -275,7 +277,9 @@ k_tfwd(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorM
 }
 
 __global__ void __launch_bounds__(256)
-k_tfwd_reduce(const float* __restrict__ part, int nkb, size_t nn, double alpha, double* __restrict__ C) {
+k_tfwd_reduce(const float* __restrict__ part, int nkb, size_t nn, double alpha, double* __restrict__ C,
+              const int* __restrict__ cond) {
+  if (cond && *cond == 0) return;
   __shared__ double ss[4][64];
   const int col = threadIdx.x & 63, g = threadIdx.x >> 6;
   const size_t i = (size_t)blockIdx.x * 64 + col;
@@ -303,8 +307,9 @@ template <int NT, int NB>
 __global__ void __launch_bounds__(TG_THREADS, 1)
 k_tbwd(const __grid_constant__ CUtensorMap tX1, const __grid_constant__ CUtensorMap tM1,
        const __grid_constant__ CUtensorMap tX2, const __grid_constant__ CUtensorMap tM2, int nterm, double a1_kx0,
-       double a1_rest, double a2, int nj, int nk, long ncol, long kx0_cols, int stages, double* __restrict__ out,
-       int* __restrict__ err_flag) {
+       double a1_rest, double a2, int nj, int nk, long ncol, long kx0_cols, int stages, double* out,
+       int* __restrict__ err_flag, const double* yadd, const int* __restrict__ cond) {
+  if (cond && *cond == 0) return;
   extern __shared__ __align__(1024) unsigned char tg_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)tg_raw + 1023) & ~(uintptr_t)1023);
   constexpr uint32_t a_bytes = TG_M * TG_KS * 2, b_bytes = (uint32_t)NB * TG_KS * 2;
@@ -401,13 +406,17 @@ k_tbwd(const __grid_constant__ CUtensorMap tX1, const __grid_constant__ CUtensor
       tg_tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)q0, v1);
       if (nterm == 2) tg_tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(NBP + q0), v2);
       if (c < ncol) {
+        // yadd may be out itself: all 16 reads go before the writes
+        double ya[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) ya[e] = (yadd && q0 + e < nj) ? yadd[(size_t)(q0 + e) * ncol + c] : 0.0;
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
           const int j = q0 + e;
           if (j < nj) {
             double r = a1 * (double)v1[e];
             if (nterm == 2) r += a2 * (double)v2[e];
-            out[(size_t)j * ncol + c] = r;
+            out[(size_t)j * ncol + c] = r + ya[e];
           }
         }
       }
@@ -456,12 +465,12 @@ static bool tg_map(CUtensorMap* map, const bf16* P, int nt, int rows, long ldp, 
 int oa_tgemm_available() { return tg_encoder() != nullptr; }
 
 cudaError_t oa_split_kc(cudaStream_t s, int nt, const double* X, int rows, int rows_pad, long K, long ldx,
-                        long kx0_cols, double w_kx0, bf16* P, long ldp) {
+                        long kx0_cols, double w_kx0, bf16* P, long ldp, const int* cond) {
   if (rows_pad < rows || (ldp & 7)) return cudaErrorInvalidValue;
   const size_t total = (size_t)rows_pad * (ldp / 8);
   const unsigned nblk = (unsigned)((total + 255) / 256 < 8 * 148 ? (total + 255) / 256 : 8 * 148);
-  if (nt == 2) k_split_kc<2><<<nblk, 256, 0, s>>>(X, rows, rows_pad, K, ldx, kx0_cols, w_kx0, P, ldp);
-  else k_split_kc<3><<<nblk, 256, 0, s>>>(X, rows, rows_pad, K, ldx, kx0_cols, w_kx0, P, ldp);
+  if (nt == 2) k_split_kc<2><<<nblk, 256, 0, s>>>(X, rows, rows_pad, K, ldx, kx0_cols, w_kx0, P, ldp, cond);
+  else k_split_kc<3><<<nblk, 256, 0, s>>>(X, rows, rows_pad, K, ldx, kx0_cols, w_kx0, P, ldp, cond);
   return cudaGetLastError();
 }
 
@@ -483,7 +492,8 @@ static int tg_stages(int nt, int nb) {
 // multiple of 128), PB with rows_b rows (a multiple of the N tile), both of
 // leading size ldp.  NotSupported when the shape or the TMA encoder rules it out.
 cudaError_t oa_tfwd(cudaStream_t s, int nt, const bf16* PA, int rows_a, const bf16* PB, int rows_b, int m, int n,
-                    long K, long ldp, double alpha, float* part, int max_kb, double* C, int* err_flag, int nsm) {
+                    long K, long ldp, double alpha, float* part, int max_kb, double* C, int* err_flag, int nsm,
+                    const int* cond) {
   const int nb = tg_nb(n);
   if (nb == 0 || m > rows_a || n > rows_b) return cudaErrorNotSupported;
   const int stages = tg_stages(nt, nb);
@@ -506,23 +516,25 @@ cudaError_t oa_tfwd(cudaStream_t s, int nt, const bf16* PA, int rows_a, const bf
   if (nt == NTT && nb == NBB) {                                                                             \
     e = cudaFuncSetAttribute(k_tfwd<NTT, NBB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);        \
     if (e != cudaSuccess) return e;                                                                         \
-    k_tfwd<NTT, NBB><<<grid, TG_THREADS, sm, s>>>(ta, tb, m, n, K, nkb, stages, part, err_flag);             \
+    k_tfwd<NTT, NBB><<<grid, TG_THREADS, sm, s>>>(ta, tb, m, n, K, nkb, stages, part, err_flag, cond);       \
     e = cudaGetLastError();                                                                                 \
   }
   OA_TF(2, 32) OA_TF(2, 64) OA_TF(2, 128) OA_TF(3, 32) OA_TF(3, 64) OA_TF(3, 128)
 #undef OA_TF
   if (e != cudaSuccess) return e;
   const size_t mn = (size_t)m * n;
-  k_tfwd_reduce<<<(unsigned)((mn + 63) / 64), 256, 0, s>>>(part, nkb, mn, alpha, C);
+  k_tfwd_reduce<<<(unsigned)((mn + 63) / 64), 256, 0, s>>>(part, nkb, mn, alpha, C, cond);
   return cudaGetLastError();
 }
 
-// out[j][c] = a1(c) sum_k M1[k][j] X1[k][c] + a2 sum_k M2[k][j] X2[k][c] from
-// X planes (rows nk, leading size ldx) and M planes (rows nk, leading size nj);
-// nk a multiple of 32 (planes padded with zero rows).
+// out[j][c] = a1(c) sum_k M1[k][j] X1[k][c] + a2 sum_k M2[k][j] X2[k][c]
+// (+ yadd[j][c], which may be out itself) from X planes (rows nk, leading
+// size ldx) and M planes (rows nk, leading size nj); nk a multiple of 32
+// (planes padded with zero rows).  cond: optional device flag, nothing runs
+// when it is 0.
 cudaError_t oa_tbwd(cudaStream_t s, int nt, const bf16* PM1, const bf16* PX1, double a1_kx0, double a1_rest,
                     const bf16* PM2, const bf16* PX2, double a2, int nj, int nk, long ncol, long ldx, long kx0_cols,
-                    double* out, int* err_flag) {
+                    double* out, int* err_flag, const double* yadd, const int* cond) {
   const int nb = tg_nb(nj);
   if (nb == 0 || nb != nj || ((PM2 == nullptr) != (PX2 == nullptr)) || nk < TG_KS || (nk % TG_KS)) return cudaErrorNotSupported;
   const int stages = tg_stages(nt, nb);
@@ -545,7 +557,7 @@ cudaError_t oa_tbwd(cudaStream_t s, int nt, const bf16* PM1, const bf16* PX1, do
     e = cudaFuncSetAttribute(k_tbwd<NTT, NBB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);           \
     if (e != cudaSuccess) return e;                                                                            \
     k_tbwd<NTT, NBB><<<grid, TG_THREADS, sm, s>>>(tx1, tm1, tx2, tm2, nterm, a1_kx0, a1_rest, a2, nj, nk, ncol,  \
-                                                  kx0_cols, stages, out, err_flag);                            \
+                                                  kx0_cols, stages, out, err_flag, yadd, cond);                \
     e = cudaGetLastError();                                                                                    \
   }
   OA_TB(2, 32) OA_TB(2, 64) OA_TB(2, 128) OA_TB(3, 32) OA_TB(3, 64) OA_TB(3, 128)

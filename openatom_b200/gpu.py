@@ -77,6 +77,7 @@ SIGNATURES = {
     "oa_gpu_integrate": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_double, C.c_int, _vp]),
     "oa_gpu_energies": (C.c_int, [_vp, _vp, _dp]),
     "oa_gpu_psiv_reset": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "oa_gpu_psiv_reset_mixed": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int]),
     "oa_gpu_set_atoms": (C.c_int, [_vp, _vp, _dp]),
     "oa_gpu_time_kernels": (C.c_int, [_vp, _vp, _vp, C.c_int, _dp]),
     "oa_gpu_sizes": (C.c_int, [_vp, C.POINTER(C.c_long)]),
@@ -276,8 +277,12 @@ class CPContext:
         _check(self._lib.oa_gpu_integrate(self._h, self._stream(), _ptr(force), _ptr(vpsi), _ptr(psi), float(dt),
                                           int(complete_prev), _ptr(fict_out)))
 
-    def psiv_reset(self, psi, psi_t, vpsi):
-        _check(self._lib.oa_gpu_psiv_reset(self._h, self._stream(), _ptr(psi), _ptr(psi_t), _ptr(vpsi)))
+    def psiv_reset(self, psi, psi_t, vpsi, nterm=0):
+        if nterm:
+            _check(self._lib.oa_gpu_psiv_reset_mixed(self._h, self._stream(), _ptr(psi), _ptr(psi_t), _ptr(vpsi),
+                                                     int(nterm)))
+        else:
+            _check(self._lib.oa_gpu_psiv_reset(self._h, self._stream(), _ptr(psi), _ptr(psi_t), _ptr(vpsi)))
 
     def set_atoms(self, pos_host: np.ndarray):
         a = np.ascontiguousarray(pos_host, dtype=np.float64)
@@ -445,7 +450,7 @@ class CPDriver:
 
     def psiv_reset(self):
         """PsiV tolerance reset (oracle.psiv_reset restates the reference)."""
-        self.ctx.psiv_reset(self.psi, self.psi_t, self.v)
+        self.ctx.psiv_reset(self.psi, self.psi_t, self.v, nterm=self.nterm_nl)
         self.T.copy_(self.torch.eye(self.sys.nstate, dtype=self.torch.float64, device=self.T.device))
 
     def quench(self, nsteps: int, dt: float | None = None):

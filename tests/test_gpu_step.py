@@ -95,3 +95,44 @@ def test_native_run_positions_and_failure():
     sd = d.native_state()
     with pytest.raises(OaError, match="step 1 of 2"):
         d.run_native(sd, 2)
+
+
+def test_native_run_matches_steps_mixed():
+    """Mixed form: the native run (device-decided PsiV with split-BF16
+    projection) reproduces the host runner bit for bit."""
+    from openatom_b200.gpu import CPDriver
+    s = make_system("w8", nstate=16, seed=15, dt=0.5)
+    a = CPDriver(s, "mixed", norb_tol=1e-14)
+    c = CPDriver(s, "mixed", norb_tol=1e-14)
+    sc = c.native_state(use_graph=True)
+    ea = [a.step() for _ in range(4)]
+    ec = c.run_native(sc, 4)
+    assert a.n_psiv == 4
+    for i in range(4):
+        for k in ("EKE", "EHART", "EEXT", "EEXC", "ENL", "FICT_KE", "SMAX"):
+            assert ec[i][k] == ea[i][k], (i, k, ea[i][k], ec[i][k])
+    assert np.array_equal(a.psi.cpu().numpy(), c.psi.cpu().numpy())
+    assert np.array_equal(a.v.cpu().numpy(), c.v.cpu().numpy())
+
+
+def test_psiv_reset_mixed_matches_fp64():
+    """The split-BF16 PsiV projection agrees with the FP64 one to FP32-level
+    accuracy of the projection term, and leaves v in FP64 otherwise."""
+    import torch
+    from openatom_b200.gpu import CPContext
+    s = make_system("w8", nstate=16, seed=16)
+    ctx = CPContext(s, "mixed")
+    rng = np.random.default_rng(2)
+    psi = torch.from_numpy(s.psi).cuda()
+    v0 = (rng.standard_normal(s.psi.shape) + 1j * rng.standard_normal(s.psi.shape)) * 1e-3
+    out = {}
+    for nt in (0, 3):
+        v = torch.from_numpy(v0.copy()).cuda()
+        pt = torch.zeros_like(psi)
+        ctx.psiv_reset(psi, pt, v, nterm=nt)
+        torch.cuda.synchronize()
+        assert np.array_equal(pt.cpu().numpy(), s.psi)
+        out[nt] = v.cpu().numpy()
+    d64 = out[0] - v0
+    err = np.max(np.abs(out[3] - out[0])) / np.max(np.abs(d64))
+    assert err < 1e-5, err
