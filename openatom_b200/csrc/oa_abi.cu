@@ -758,12 +758,13 @@ static cudaError_t mixed_bwd(oa_ctx* c, cudaStream_t s, int nt, const double* M1
   oa_ctx_pc* p = pcx(c);
   const int mx = c->nstate > c->natm_nl ? c->nstate : c->natm_nl;
   const int nkp = oa_tg_rows_pad(nk, 32);
-  if (nj <= mx && nk <= mx && ncol <= p->pl_ld && oa_tg_nb(nj) == nj && nkp <= p->pl_rows && (!M2 || s1 != s2)) {
+  const int ldm = oa_tg_nb(nj);  // M planes: leading size of the N tile, zero beyond nj
+  if (nj <= mx && nk <= mx && ncol <= p->pl_ld && ldm != 0 && nkp <= p->pl_rows && (!M2 || s1 != s2)) {
     bf16 *pm1 = (bf16*)p->pl_ma, *pm2 = (bf16*)p->pl_mb;
     cudaError_t e = ensure_planes(c, s, nt, s1, X1, nk, nkp, ncol, 0, 1.0, cond);
-    if (e == cudaSuccess) e = oa_split_kc(s, nt, M1, nk, nkp, nj, nj, 0, 1.0, pm1, nj, cond);
+    if (e == cudaSuccess) e = oa_split_kc(s, nt, M1, nk, nkp, nj, nj, 0, 1.0, pm1, ldm, cond);
     if (e == cudaSuccess && M2) e = ensure_planes(c, s, nt, s2, X2, nk, nkp, ncol, 0, 1.0, cond);
-    if (e == cudaSuccess && M2) e = oa_split_kc(s, nt, M2, nk, nkp, nj, nj, 0, 1.0, pm2, nj, cond);
+    if (e == cudaSuccess && M2) e = oa_split_kc(s, nt, M2, nk, nkp, nj, nj, 0, 1.0, pm2, ldm, cond);
     if (e != cudaSuccess) return e;
     e = oa_tbwd(s, nt, pm1, (const bf16*)p->pl_big[s1], a1_kx0, a1_rest, M2 ? pm2 : nullptr,
                 M2 ? (const bf16*)p->pl_big[s2] : nullptr, a2, nj, nkp, ncol, p->pl_ld, kx0_cols, out, p->err_flag,

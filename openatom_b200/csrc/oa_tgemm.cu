@@ -2,26 +2,28 @@
 //
 // Operand format ("bf16 planes"): an FP64 matrix X [rows][K] becomes NT bf16
 // planes x = P_0 + P_1 (+ P_2), P_0 = bf16(x), P_1 = bf16(x - P_0), ...,
-// stored K-chunk-major:  P[q][K/8][rows][8]  (K padded with zeros to ldp, a
-// multiple of 64).  Element (r, k) sits at ((k/8) rows + r) 16 + (k%8) 2 bytes
-// in plane q.  With this order one 3-D TMA box lands as the UMMA canonical
-// no-swizzle layout for both uses of a matrix:
-//   K-major view (forward GEMM, K = k):    box {8, R rows, 4 k-groups}
-//       -> smem [kc][r][8]: SBO 128 (8-row groups), LBO = R 16 (k groups)
-//   MN-major view (backward GEMM, MN = k): box {8, 32 rows, G k-groups}
-//       -> smem [g][r][8]:  LBO 128 (8-row K groups), SBO = 32 16 = 512 (MN groups)
-// (the TMA strides 16 B and rows 16 B grow with the dimension index).
+// stored row-major P[q][rows_pad][ldp] (K padded with zeros to ldp, a
+// multiple of 64; rows padded with zero rows).  The kernels load 128-byte
+// rows (64 contiguous elements) with the TMA's 128-byte swizzle, which
+// lands as the UMMA SWIZZLE_128B canonical layout for both uses of a plane:
+//   K-major view (forward GEMM, contiguous = K): box {64 k, R rows}
+//       -> R rows of 128 B; 8-row groups 1024 B apart (SBO); the four
+//          K = 16 steps of a box start 32 B apart
+//   MN-major view (backward GEMM, contiguous = MN): boxes {64 mn, 32 k}
+//       -> 32 k rows of 128 B per 64-wide MN chunk; chunks 4096 B apart
+//          (LBO), 8-row K groups 1024 B apart (SBO); K = 16 steps 2048 B apart
 //
 //   k_tfwd : C[x][y] = alpha sum_k A[x][k] B[y][k]            (Lambda, the nonlocal Z)
 //            PairCalculator::multiplyForward (ckPairCalculator.C:821-893)
 //   k_tbwd : out[j][c] = a1(c) sum_k M1[k][j] X1[k][c] + a2 sum_k M2[k][j] X2[k][c]
 //            bwMultiplyHelper / bwMultiplyDynOrthoT (ckPairCalculator.C:1710-2031)
 //
-// One thread issues the TMA loads (mbarrier complete_tx) and the MMAs
-// (tcgen05.commit -> mbarrier) over a ring of stages; the block reads the
-// FP32 TMEM accumulators in the epilogue.  Every wait is bounded: on timeout
-// the block sets the device error flag, waits (bounded) for the copies it
-// issued, frees its TMEM and returns.  No multicast.
+// k_tfwd: one thread issues the TMA loads (mbarrier complete_tx) and the
+// MMAs (tcgen05.commit -> mbarrier) over a ring of stages; the block reads
+// the FP32 TMEM accumulators in the epilogue.  k_tbwd is persistent and
+// warp-specialised (below).  Every wait is bounded: on timeout the block
+// sets the device error flag, waits (bounded) for the copies it issued,
+// frees its TMEM and returns.  No multicast.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <mutex>
@@ -29,19 +31,22 @@
 
 typedef __nv_bfloat16 bf16;
 
-#define TG_KS 32            // K (or k rows) per stage
+#define TG_KS 32            // k rows per stage (backward)
+#define TG_KF 64            // K per stage (forward)
 #define TG_M 128
 #define TG_THREADS 128
 #define TG_SPIN (1u << 28)
 
 __device__ __forceinline__ uint32_t tg_s32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+// UMMA shared-memory descriptor, SWIZZLE_128B layout (type 2), version 1
 __device__ __forceinline__ uint64_t tg_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
   d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
   d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-  d |= (uint64_t)1 << 46;  // sm_100 descriptor version; base offset 0, SWIZZLE_NONE
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
   return d;
 }
 __host__ __device__ constexpr uint32_t tg_idesc(int n, int a_mn, int b_mn) {
@@ -79,13 +84,12 @@ __device__ __forceinline__ bool tg_wait(uint64_t* bar, uint32_t phase) {
   }
   return false;
 }
-// 4-D tile load of a tensor map box into shared memory, completing on bar
-__device__ __forceinline__ void tg_tma4(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
-                                        uint64_t* bar) {
+// 3-D tile load of a tensor map box into shared memory, completing on bar
+__device__ __forceinline__ void tg_tma3(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar) {
   asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
-      "[%6];"
-      :: "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(tg_s32(bar))
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];"
+      :: "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(tg_s32(bar))
       : "memory");
 }
 __device__ __forceinline__ void tg_tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -111,9 +115,9 @@ __device__ __forceinline__ void tg_tmem_ld16(uint32_t taddr, float* v) {
 }
 
 // ---------------------------------------------------------------------------
-// FP64 [rows][K] (row stride ldx) -> planes P[q][ldp/8][rows_pad][8], columns
+// FP64 [rows][K] (row stride ldx) -> planes P[q][rows_pad][ldp], columns
 // k < kx0_cols scaled by w_kx0 first; padding columns [K, ldp) and rows
-// [rows, rows_pad) zero.
+// [rows, rows_pad) zero.  One thread per 8 consecutive elements of a row.
 // ---------------------------------------------------------------------------
 template <int NT>
 __global__ void k_split_kc(const double* __restrict__ X, int rows, int rows_pad, long K, long ldx, long kx0_cols,
@@ -123,10 +127,8 @@ __global__ void k_split_kc(const double* __restrict__ X, int rows, int rows_pad,
   const size_t total = (size_t)rows_pad * ng;
   const size_t pstride = (size_t)rows_pad * ldp;
   for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-    // t -> (group kg, row r) with r fastest: consecutive threads write
-    // consecutive 16-byte pieces of the plane
-    const long kg = (long)(t / rows_pad);
-    const int r = (int)(t - (size_t)kg * rows_pad);
+    const int r = (int)(t / ng);
+    const long kg = (long)(t - (size_t)r * ng);
     const long k0 = kg * 8;
     double x[8];
     const double* src = X + (size_t)r * ldx + k0;
@@ -160,7 +162,7 @@ __global__ void k_split_kc(const double* __restrict__ X, int rows, int rows_pad,
     }
 #pragma unroll
     for (int q = 0; q < NT; ++q)
-      *reinterpret_cast<uint4*>(P + q * pstride + ((size_t)kg * rows_pad + r) * 8) = *reinterpret_cast<uint4*>(&h[q][0]);
+      *reinterpret_cast<uint4*>(P + q * pstride + (size_t)r * ldp + k0) = *reinterpret_cast<uint4*>(&h[q][0]);
   }
 }
 
@@ -174,7 +176,7 @@ k_tfwd(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorM
   if (cond && *cond == 0) return;
   extern __shared__ __align__(1024) unsigned char tg_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)tg_raw + 1023) & ~(uintptr_t)1023);
-  constexpr uint32_t a_bytes = TG_M * TG_KS * 2, b_bytes = (uint32_t)NB * TG_KS * 2;
+  constexpr uint32_t a_bytes = TG_M * TG_KF * 2, b_bytes = (uint32_t)NB * TG_KF * 2;
   constexpr uint32_t stage_bytes = NT * (a_bytes + b_bytes);
   uint64_t* full = (uint64_t*)(base + (size_t)stages * stage_bytes);
   uint64_t* empty = full + stages;
@@ -183,7 +185,7 @@ k_tfwd(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorM
   const int tid = threadIdx.x, warp = tid >> 5;
   const int m0 = blockIdx.y * TG_M, n0 = blockIdx.z * NB;
   const int kb = blockIdx.x;
-  const long rslabs = (K + TG_KS - 1) / TG_KS;
+  const long rslabs = (K + TG_KF - 1) / TG_KF;
   const int nslab = rslabs > kb ? (int)((rslabs - kb + nkb - 1) / nkb) : 0;
   constexpr uint32_t ncols = NB <= 32 ? 32 : (NB <= 64 ? 64 : (NB <= 128 ? 128 : 256));
   if (tid == 0) {
@@ -199,13 +201,13 @@ k_tfwd(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorM
     constexpr uint32_t idesc = tg_idesc(NB, 0, 0);
     const uint32_t sbase = tg_s32(base);
     auto issue_loads = [&](int sl, int st) {
-      const int g0 = (kb + sl * nkb) * (TG_KS / 8);
+      const int k0 = (kb + sl * nkb) * TG_KF;
       const uint32_t sb = sbase + st * stage_bytes;
       tg_expect_tx(&full[st], stage_bytes);
 #pragma unroll
       for (int q = 0; q < NT; ++q) {
-        tg_tma4(sb + q * a_bytes, &tA, 0, m0, g0, q, &full[st]);
-        tg_tma4(sb + NT * a_bytes + q * b_bytes, &tB, 0, n0, g0, q, &full[st]);
+        tg_tma3(sb + q * a_bytes, &tA, k0, m0, q, &full[st]);
+        tg_tma3(sb + NT * a_bytes + q * b_bytes, &tB, k0, n0, q, &full[st]);
       }
     };
     bool ok = true;
@@ -218,7 +220,8 @@ k_tfwd(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorM
       if (!tg_wait(&full[st], ph)) { ok = false; break; }
       tg_tc_after();
       const uint32_t sb = sbase + st * stage_bytes;
-      constexpr uint32_t lbo_a = TG_M * 16, lbo_b = (uint32_t)NB * 16;
+      // K-major, 128-byte swizzle: rows 128 B apart, 8-row groups 1024 B
+      // apart (SBO); K steps of 16 elements 32 B apart inside the rows
       bool acc = sl > 0;
 #pragma unroll
       for (int i = 0; i < NT; ++i)
@@ -226,9 +229,9 @@ k_tfwd(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorM
         for (int j = 0; j < NT; ++j) {
           if (i + j > NT - 1) continue;
 #pragma unroll
-          for (int ks = 0; ks < TG_KS / 16; ++ks) {
-            const uint64_t da = tg_desc(sb + i * a_bytes + ks * 2 * lbo_a, lbo_a, 128);
-            const uint64_t db = tg_desc(sb + NT * a_bytes + j * b_bytes + ks * 2 * lbo_b, lbo_b, 128);
+          for (int ks = 0; ks < TG_KF / 16; ++ks) {
+            const uint64_t da = tg_desc(sb + i * a_bytes + ks * 32, 16, 1024);
+            const uint64_t db = tg_desc(sb + NT * a_bytes + j * b_bytes + ks * 32, 16, 1024);
             tg_mma(tmem, da, db, idesc, acc ? 1u : 0u);
             acc = true;
           }
@@ -301,10 +304,25 @@ k_tfwd_reduce(const float* __restrict__ part, int nkb, size_t nn, double alpha, 
 }
 
 // ---------------------------------------------------------------------------
-// backward: CTA = 128 columns c, D_t[c][j] per term t in TMEM columns t NBP ..
+// backward, persistent: CTA b takes the 128-column tiles b, b + grid, ...;
+// D_t[c][j] per term t in TMEM.  Warp roles: warp 0 lane 0 issues the TMA
+// loads over a ring of stages, warp 1 lane 0 issues the MMAs into one of
+// two TMEM accumulators (tile i uses buffer i & 1), warps 2-5 drain the
+// other accumulator (TMEM lane quarter warp & 3) to FP64 while the next
+// tile's loads and MMAs run.
+//   full[s]  : TMA bytes of stage s landed      (producer -> MMA)
+//   empty[s] : MMAs reading stage s are done    (MMA commit -> producer)
+//   accf[b]  : accumulator b complete           (MMA commit -> epilogue)
+//   acce[b]  : accumulator b read out           (4 epilogue warps -> MMA)
 // ---------------------------------------------------------------------------
+#define TB_THREADS 192
+
+__device__ __forceinline__ void tg_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(tg_s32(bar)) : "memory");
+}
+
 template <int NT, int NB>
-__global__ void __launch_bounds__(TG_THREADS, 1)
+__global__ void __launch_bounds__(TB_THREADS, 1)
 k_tbwd(const __grid_constant__ CUtensorMap tX1, const __grid_constant__ CUtensorMap tM1,
        const __grid_constant__ CUtensorMap tX2, const __grid_constant__ CUtensorMap tM2, int nterm, double a1_kx0,
        double a1_rest, double a2, int nj, int nk, long ncol, long kx0_cols, int stages, double* out,
@@ -312,20 +330,25 @@ k_tbwd(const __grid_constant__ CUtensorMap tX1, const __grid_constant__ CUtensor
   if (cond && *cond == 0) return;
   extern __shared__ __align__(1024) unsigned char tg_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)tg_raw + 1023) & ~(uintptr_t)1023);
+  static_assert(NB == 64 || NB == 128, "k_tbwd: N tile of 64 or 128");
   constexpr uint32_t a_bytes = TG_M * TG_KS * 2, b_bytes = (uint32_t)NB * TG_KS * 2;
   constexpr uint32_t stage_bytes = NT * (a_bytes + b_bytes);
+  constexpr int NBP = NB;
+  constexpr uint32_t ncols = 4 * NBP;  // two accumulators of two terms
   uint64_t* full = (uint64_t*)(base + (size_t)stages * stage_bytes);
   uint64_t* empty = full + stages;
-  uint32_t* tslot = (uint32_t*)(empty + stages);
-  int* okflag = (int*)(tslot + 1);
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const long c0 = (long)blockIdx.x * TG_M;
-  constexpr int NBP = NB <= 32 ? 32 : (NB <= 64 ? 64 : 128);
-  const uint32_t ncols = nterm == 1 ? (uint32_t)NBP : (NBP == 128 ? 256u : (uint32_t)(2 * NBP));
+  uint64_t* accf = empty + stages;
+  uint64_t* acce = accf + 2;
+  uint32_t* tslot = (uint32_t*)(acce + 2);
+  volatile int* okflag = (volatile int*)(tslot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long ntile = (ncol + TG_M - 1) / TG_M;
+  const int my_tiles = blockIdx.x < ntile ? (int)((ntile - 1 - blockIdx.x) / gridDim.x + 1) : 0;
   const int kch = (nk + TG_KS - 1) / TG_KS;
   const int nslab = nterm * kch;
   if (tid == 0) {
     for (int s = 0; s < stages; ++s) { tg_bar_init(&full[s], 1); tg_bar_init(&empty[s], 1); }
+    for (int b = 0; b < 2; ++b) { tg_bar_init(&accf[b], 1); tg_bar_init(&acce[b], 4); }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     *okflag = 1;
   }
@@ -333,98 +356,125 @@ k_tbwd(const __grid_constant__ CUtensorMap tX1, const __grid_constant__ CUtensor
   __syncthreads();
   tg_tc_after();
   const uint32_t tmem = *tslot;
-  if (tid == 0) {
-    constexpr uint32_t idesc = tg_idesc(NB, 1, 1);
-    const uint32_t sbase = tg_s32(base);
-    const int cg0 = (int)(c0 / 8);
-    auto issue_loads = [&](int sl, int st) {
-      const int term = sl / kch;
-      const int k0 = (sl - term * kch) * TG_KS;
-      const CUtensorMap* tx = term ? &tX2 : &tX1;
-      const CUtensorMap* tm = term ? &tM2 : &tM1;
-      const uint32_t sb = sbase + st * stage_bytes;
-      tg_expect_tx(&full[st], stage_bytes);
+  if (warp == 0) {
+    if (lane == 0) {
+      // TMA producer
+      const uint32_t sbase = tg_s32(base);
+      long g = 0;
+      bool ok = true;
+      for (int i = 0; i < my_tiles && ok; ++i) {
+        const int c0 = (int)(((long)blockIdx.x + (long)i * gridDim.x) * TG_M);
+        for (int sl = 0; sl < nslab; ++sl, ++g) {
+          const int st = (int)(g % stages);
+          if (!tg_wait(&empty[st], (uint32_t)((g / stages) & 1) ^ 1u) || !*okflag) { ok = false; break; }
+          const int term = sl / kch;
+          const int k0 = (sl - term * kch) * TG_KS;
+          const CUtensorMap* tx = term ? &tX2 : &tX1;
+          const CUtensorMap* tm = term ? &tM2 : &tM1;
+          const uint32_t sb = sbase + st * stage_bytes;
+          tg_expect_tx(&full[st], stage_bytes);
+          // 64-wide MN chunks of 32 k rows, 4096 B each
 #pragma unroll
-      for (int q = 0; q < NT; ++q) {
-        tg_tma4(sb + q * a_bytes, tx, 0, k0, cg0, q, &full[st]);
-        tg_tma4(sb + NT * a_bytes + q * b_bytes, tm, 0, k0, 0, q, &full[st]);
+          for (int q = 0; q < NT; ++q) {
+            tg_tma3(sb + q * a_bytes, tx, c0, k0, q, &full[st]);
+            tg_tma3(sb + q * a_bytes + 4096, tx, c0 + 64, k0, q, &full[st]);
+#pragma unroll
+            for (int h = 0; h < NB / 64; ++h) tg_tma3(sb + NT * a_bytes + q * b_bytes + h * 4096, tm, h * 64, k0, q, &full[st]);
+          }
+        }
       }
-    };
-    bool ok = true;
-    const int pre = nslab < stages ? nslab : stages;
-    for (int s = 0; s < pre; ++s) issue_loads(s, s);
-    int issued = pre;
-    for (int sl = 0; sl < nslab && ok; ++sl) {
-      const int st = sl % stages;
-      const uint32_t ph = (uint32_t)(sl / stages) & 1u;
-      if (!tg_wait(&full[st], ph)) { ok = false; break; }
+      if (!ok) {
+        *okflag = 0;
+        // let every issued load land before the block exits: the last
+        // issue on stage s is at most one phase ahead of its consumer
+        for (int s2 = 0; s2 < stages && s2 < g; ++s2) {
+          const long last = g - 1 - ((g - 1 - s2) % stages);
+          (void)tg_wait(&full[s2], (uint32_t)((last / stages) & 1));
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // MMA issuer
+      constexpr uint32_t idesc = tg_idesc(NB, 1, 1);
+      const uint32_t sbase = tg_s32(base);
+      long g = 0;
+      bool ok = true;
+      for (int i = 0; i < my_tiles && ok; ++i) {
+        const int b = i & 1;
+        if (!tg_wait(&acce[b], (uint32_t)((i >> 1) & 1) ^ 1u) || !*okflag) { ok = false; break; }
+        tg_tc_after();
+        for (int sl = 0; sl < nslab; ++sl, ++g) {
+          const int st = (int)(g % stages);
+          if (!tg_wait(&full[st], (uint32_t)((g / stages) & 1)) || !*okflag) { ok = false; break; }
+          tg_tc_after();
+          const int term = sl / kch;
+          const bool first_of_term = (sl - term * kch) == 0;
+          const uint32_t sb = sbase + st * stage_bytes;
+          // MN-major, 128-byte swizzle: 64-wide MN chunks 4096 B apart (LBO),
+          // 8-row K groups 1024 B apart (SBO); K steps of 16 rows 2048 B apart
+          const uint32_t td = tmem + (uint32_t)(b * 2 * NBP + term * NBP);
+          bool acc = !first_of_term;
+#pragma unroll
+          for (int i2 = 0; i2 < NT; ++i2)
+#pragma unroll
+            for (int j2 = 0; j2 < NT; ++j2) {
+              if (i2 + j2 > NT - 1) continue;
+#pragma unroll
+              for (int ks = 0; ks < TG_KS / 16; ++ks) {
+                const uint64_t da = tg_desc(sb + i2 * a_bytes + ks * 2048, 4096, 1024);
+                const uint64_t db = tg_desc(sb + NT * a_bytes + j2 * b_bytes + ks * 2048, 4096, 1024);
+                tg_mma(td, da, db, idesc, acc ? 1u : 0u);
+                acc = true;
+              }
+            }
+          tg_commit(&empty[st]);
+        }
+        if (!ok) break;
+        tg_commit(&accf[b]);
+      }
+      if (!ok) *okflag = 0;
+    }
+  } else {
+    // epilogue: TMEM lane quarter q = warp & 3 holds columns c0 + 32 q ..
+    const int q = warp & 3;
+    const int row = q * 32 + lane;
+    for (int i = 0; i < my_tiles; ++i) {
+      const int b = i & 1;
+      if (!tg_wait(&accf[b], (uint32_t)((i >> 1) & 1))) { *okflag = 0; break; }
       tg_tc_after();
-      const int term = sl / kch;
-      const bool first_of_term = (sl - term * kch) == 0;
-      const uint32_t sb = sbase + st * stage_bytes;
-      // MN-major: K groups of 8 rows 128 B apart (LBO), MN groups 512 B apart (SBO)
-      const uint32_t td = tmem + (uint32_t)(term * NBP);
-      bool acc = !first_of_term;
+      if (!*okflag) break;
+      const long c = ((long)blockIdx.x + (long)i * gridDim.x) * TG_M + row;
+      const double a1 = (c < kx0_cols) ? a1_kx0 : a1_rest;
+      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 2 * NBP);
+      for (int q0 = 0; q0 < NB; q0 += 16) {
+        float v1[16], v2[16];
+        tg_tmem_ld16(tbase + (uint32_t)q0, v1);
+        if (nterm == 2) tg_tmem_ld16(tbase + (uint32_t)(NBP + q0), v2);
+        if (c < ncol) {
+          // yadd may be out itself: all 16 reads go before the writes
+          double ya[16];
 #pragma unroll
-      for (int i = 0; i < NT; ++i)
+          for (int e = 0; e < 16; ++e) ya[e] = (yadd && q0 + e < nj) ? yadd[(size_t)(q0 + e) * ncol + c] : 0.0;
 #pragma unroll
-        for (int j = 0; j < NT; ++j) {
-          if (i + j > NT - 1) continue;
-#pragma unroll
-          for (int ks = 0; ks < TG_KS / 16; ++ks) {
-            const uint64_t da = tg_desc(sb + i * a_bytes + ks * 256, 128, TG_KS * 16);
-            const uint64_t db = tg_desc(sb + NT * a_bytes + j * b_bytes + ks * 256, 128, TG_KS * 16);
-            tg_mma(td, da, db, idesc, acc ? 1u : 0u);
-            acc = true;
+          for (int e = 0; e < 16; ++e) {
+            const int j = q0 + e;
+            if (j < nj) {
+              double r = a1 * (double)v1[e];
+              if (nterm == 2) r += a2 * (double)v2[e];
+              out[(size_t)j * ncol + c] = r + ya[e];
+            }
           }
         }
-      tg_commit(&empty[st]);
-      if (issued < nslab) {
-        if (!tg_wait(&empty[st], ph)) { ok = false; break; }
-        issue_loads(issued, st);
-        ++issued;
       }
-    }
-    if (ok && nslab > 0) {
-      const int sl = nslab - 1;
-      if (!tg_wait(&empty[sl % stages], (uint32_t)(sl / stages) & 1u)) ok = false;
-    }
-    if (!ok) {
-      for (int s2 = 0; s2 < stages; ++s2) (void)tg_wait(&full[s2], 0u);
-      *okflag = 0;
+      tg_tc_before();
+      __syncwarp();
+      if (lane == 0) tg_arrive(&acce[b]);
     }
   }
   __syncthreads();
+  if (!*okflag && tid == 0) atomicExch(err_flag, 1);
   tg_tc_after();
-  const bool ok = *okflag != 0;
-  const int row = warp * 32 + (tid & 31);
-  const long c = c0 + row;
-  if (ok) {
-    const double a1 = (c < kx0_cols) ? a1_kx0 : a1_rest;
-    for (int q0 = 0; q0 < NB; q0 += 16) {
-      float v1[16], v2[16];
-      tg_tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)q0, v1);
-      if (nterm == 2) tg_tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(NBP + q0), v2);
-      if (c < ncol) {
-        // yadd may be out itself: all 16 reads go before the writes
-        double ya[16];
-#pragma unroll
-        for (int e = 0; e < 16; ++e) ya[e] = (yadd && q0 + e < nj) ? yadd[(size_t)(q0 + e) * ncol + c] : 0.0;
-#pragma unroll
-        for (int e = 0; e < 16; ++e) {
-          const int j = q0 + e;
-          if (j < nj) {
-            double r = a1 * (double)v1[e];
-            if (nterm == 2) r += a2 * (double)v2[e];
-            out[(size_t)j * ncol + c] = r + ya[e];
-          }
-        }
-      }
-    }
-  }
-  if (!ok && tid == 0) atomicExch(err_flag, 1);
-  tg_tc_before();
-  __syncthreads();
   if (warp == 0) tg_tmem_dealloc(tmem, ncols);
 }
 
@@ -449,16 +499,17 @@ static EncodeTiledFn tg_encoder() {
   return fn;
 }
 
-// planes P[nt][ldp/8][rows][8] as a 4-D bf16 tensor {8, rows, ldp/8, nt}; box {8, br, bg, 1}
-static bool tg_map(CUtensorMap* map, const bf16* P, int nt, int rows, long ldp, int br, int bg) {
+// planes P[nt][rows][ldp] as a 3-D bf16 tensor {ldp, rows, nt}; box {64, br, 1}
+// (128-byte rows) with the 128-byte swizzle
+static bool tg_map(CUtensorMap* map, const bf16* P, int nt, int rows, long ldp, int br) {
   EncodeTiledFn enc = tg_encoder();
-  if (!enc || (((uintptr_t)P) & 15)) return false;
-  const cuuint64_t dims[4] = {8, (cuuint64_t)rows, (cuuint64_t)(ldp / 8), (cuuint64_t)nt};
-  const cuuint64_t strides[3] = {16, (cuuint64_t)rows * 16, (cuuint64_t)rows * (cuuint64_t)ldp * 2};
-  const cuuint32_t box[4] = {8, (cuuint32_t)br, (cuuint32_t)bg, 1};
-  const cuuint32_t es[4] = {1, 1, 1, 1};
-  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void*)P, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+  if (!enc || (((uintptr_t)P) & 15) || (ldp & 63) || br > 256) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)ldp, (cuuint64_t)rows, (cuuint64_t)nt};
+  const cuuint64_t strides[2] = {(cuuint64_t)ldp * 2, (cuuint64_t)rows * (cuuint64_t)ldp * 2};
+  const cuuint32_t box[3] = {64, (cuuint32_t)br, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void*)P, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
          CUDA_SUCCESS;
 }
 
@@ -476,15 +527,17 @@ cudaError_t oa_split_kc(cudaStream_t s, int nt, const double* X, int rows, int r
 
 // rows of the planes of an operand the kernels read in boxes of `box` rows
 int oa_tg_rows_pad(int rows, int box) { return (rows + box - 1) / box * box; }
-int oa_tg_nb(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : (n <= 128 ? 128 : 0)); }
+int oa_tg_nb(int n) { return n <= 64 ? 64 : (n <= 128 ? 128 : 0); }
 
-static int tg_nb(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : (n <= 128 ? 128 : 0)); }
-static size_t tg_smem(int nt, int nb, int stages) {
-  return (size_t)stages * nt * ((size_t)TG_M * TG_KS * 2 + (size_t)nb * TG_KS * 2) + 1024 + 256;
+static int tg_nb(int n) { return n <= 64 ? 64 : (n <= 128 ? 128 : 0); }
+// forward stages carry TG_KF columns of K, backward stages TG_KS rows of k
+static size_t tg_smem(int nt, int nb, int stages, bool fwd) {
+  const size_t kk = fwd ? TG_KF : TG_KS;
+  return (size_t)stages * nt * ((size_t)TG_M * kk * 2 + (size_t)nb * kk * 2) + 1024 + 256;
 }
-static int tg_stages(int nt, int nb) {
+static int tg_stages(int nt, int nb, bool fwd) {
   for (int st = 6; st >= 2; --st)
-    if (tg_smem(nt, nb, st) <= (size_t)OA_MAX_SMEM) return st;
+    if (tg_smem(nt, nb, st, fwd) <= (size_t)OA_MAX_SMEM) return st;
   return 0;
 }
 
@@ -496,20 +549,19 @@ cudaError_t oa_tfwd(cudaStream_t s, int nt, const bf16* PA, int rows_a, const bf
                     const int* cond) {
   const int nb = tg_nb(n);
   if (nb == 0 || m > rows_a || n > rows_b) return cudaErrorNotSupported;
-  const int stages = tg_stages(nt, nb);
+  const int stages = tg_stages(nt, nb, true);
   if (stages < 2) return cudaErrorNotSupported;
   const int mt = (m + TG_M - 1) / TG_M, ntl = (n + nb - 1) / nb;
   // the planes are padded to whole boxes of rows (oa_tg_rows_pad)
   if (rows_a % TG_M || rows_b % nb || rows_a < m || rows_b < n) return cudaErrorNotSupported;
   CUtensorMap ta, tb;
-  if (!tg_map(&ta, PA, nt, rows_a, ldp, TG_M, TG_KS / 8) || !tg_map(&tb, PB, nt, rows_b, ldp, nb, TG_KS / 8))
-    return cudaErrorNotSupported;
-  const long sr = (K + TG_KS - 1) / TG_KS;
+  if (!tg_map(&ta, PA, nt, rows_a, ldp, TG_M) || !tg_map(&tb, PB, nt, rows_b, ldp, nb)) return cudaErrorNotSupported;
+  const long sr = (K + TG_KF - 1) / TG_KF;
   int nkb = nsm / (mt * ntl);
   if (nkb > max_kb) nkb = max_kb;
   if (nkb > sr) nkb = (int)sr;
   if (nkb < 1) nkb = 1;
-  const size_t sm = tg_smem(nt, nb, stages);
+  const size_t sm = tg_smem(nt, nb, stages, true);
   dim3 grid(nkb, mt, ntl);
   cudaError_t e = cudaErrorNotSupported;
 #define OA_TF(NTT, NBB)                                                                                     \
@@ -519,7 +571,7 @@ cudaError_t oa_tfwd(cudaStream_t s, int nt, const bf16* PA, int rows_a, const bf
     k_tfwd<NTT, NBB><<<grid, TG_THREADS, sm, s>>>(ta, tb, m, n, K, nkb, stages, part, err_flag, cond);       \
     e = cudaGetLastError();                                                                                 \
   }
-  OA_TF(2, 32) OA_TF(2, 64) OA_TF(2, 128) OA_TF(3, 32) OA_TF(3, 64) OA_TF(3, 128)
+  OA_TF(2, 64) OA_TF(2, 128) OA_TF(3, 64) OA_TF(3, 128)
 #undef OA_TF
   if (e != cudaSuccess) return e;
   const size_t mn = (size_t)m * n;
@@ -529,38 +581,43 @@ cudaError_t oa_tfwd(cudaStream_t s, int nt, const bf16* PA, int rows_a, const bf
 
 // out[j][c] = a1(c) sum_k M1[k][j] X1[k][c] + a2 sum_k M2[k][j] X2[k][c]
 // (+ yadd[j][c], which may be out itself) from X planes (rows nk, leading
-// size ldx) and M planes (rows nk, leading size nj); nk a multiple of 32
-// (planes padded with zero rows).  cond: optional device flag, nothing runs
+// size ldx) and M planes (rows nk, leading size oa_tg_nb(nj), zero beyond
+// nj); nk a multiple of 32 (planes padded with zero rows).  cond: optional device flag, nothing runs
 // when it is 0.
 cudaError_t oa_tbwd(cudaStream_t s, int nt, const bf16* PM1, const bf16* PX1, double a1_kx0, double a1_rest,
                     const bf16* PM2, const bf16* PX2, double a2, int nj, int nk, long ncol, long ldx, long kx0_cols,
                     double* out, int* err_flag, const double* yadd, const int* cond) {
   const int nb = tg_nb(nj);
-  if (nb == 0 || nb != nj || ((PM2 == nullptr) != (PX2 == nullptr)) || nk < TG_KS || (nk % TG_KS)) return cudaErrorNotSupported;
-  const int stages = tg_stages(nt, nb);
+  if (nb == 0 || ((PM2 == nullptr) != (PX2 == nullptr)) || nk < TG_KS || (nk % TG_KS)) return cudaErrorNotSupported;
+  const int stages = tg_stages(nt, nb, false);
   if (stages < 2) return cudaErrorNotSupported;
   CUtensorMap tx1, tm1, tx2, tm2;
-  if (!tg_map(&tx1, PX1, nt, nk, ldx, TG_KS, TG_M / 8) || !tg_map(&tm1, PM1, nt, nk, nj, TG_KS, nb / 8))
-    return cudaErrorNotSupported;
+  if (!tg_map(&tx1, PX1, nt, nk, ldx, TG_KS) || !tg_map(&tm1, PM1, nt, nk, nb, TG_KS)) return cudaErrorNotSupported;
   const int nterm = PM2 ? 2 : 1;
   if (nterm == 2) {
-    if (!tg_map(&tx2, PX2, nt, nk, ldx, TG_KS, TG_M / 8) || !tg_map(&tm2, PM2, nt, nk, nj, TG_KS, nb / 8))
-      return cudaErrorNotSupported;
+    if (!tg_map(&tx2, PX2, nt, nk, ldx, TG_KS) || !tg_map(&tm2, PM2, nt, nk, nb, TG_KS)) return cudaErrorNotSupported;
   } else {
     tx2 = tx1; tm2 = tm1;
   }
-  const size_t sm = tg_smem(nt, nb, stages);
-  dim3 grid((unsigned)((ncol + TG_M - 1) / TG_M));
+  const size_t sm = tg_smem(nt, nb, stages, false);
+  const long ntile = (ncol + TG_M - 1) / TG_M;
+  int nsm = 148;
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  }
+  dim3 grid((unsigned)(ntile < nsm ? ntile : nsm));
   cudaError_t e = cudaErrorNotSupported;
 #define OA_TB(NTT, NBB)                                                                                        \
   if (nt == NTT && nb == NBB) {                                                                                \
     e = cudaFuncSetAttribute(k_tbwd<NTT, NBB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);           \
     if (e != cudaSuccess) return e;                                                                            \
-    k_tbwd<NTT, NBB><<<grid, TG_THREADS, sm, s>>>(tx1, tm1, tx2, tm2, nterm, a1_kx0, a1_rest, a2, nj, nk, ncol,  \
+    k_tbwd<NTT, NBB><<<grid, TB_THREADS, sm, s>>>(tx1, tm1, tx2, tm2, nterm, a1_kx0, a1_rest, a2, nj, nk, ncol,  \
                                                   kx0_cols, stages, out, err_flag, yadd, cond);                \
     e = cudaGetLastError();                                                                                    \
   }
-  OA_TB(2, 32) OA_TB(2, 64) OA_TB(2, 128) OA_TB(3, 32) OA_TB(3, 64) OA_TB(3, 128)
+  OA_TB(2, 64) OA_TB(2, 128) OA_TB(3, 64) OA_TB(3, 128)
 #undef OA_TB
   return e;
 }

@@ -18,7 +18,7 @@ def rel(a, b):
     return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
 
 
-@pytest.fixture(scope="module", params=[("w4", None), ("w8", 32), ("w8", 128), ("w8", 160)])
+@pytest.fixture(scope="module", params=[("w4", None), ("w8", 32), ("w8", 48), ("w8", 100), ("w8", 128), ("w8", 160)])
 def case(request):
     import torch
     from openatom_b200.gpu import CPContext
