@@ -237,7 +237,8 @@ def run_ours(args):
                "sample": f"1 full CP step of the FP64 oracle on this workload ({dt:.1f} s, scipy FFT workers={os.cpu_count()})"}
 
     if rk == 0:
-        launches_per_step = dmx.launches_per_step()
+        # kernel launches of one mixed step, counted in its captured CUDA graph
+        launches_per_step = stmx.last_kernels if stmx.last_kernels > 0 else dmx.launches_per_step()
         line = {
             "metric": METRIC, "value": ws * 1e3 / ms_mx, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_mx, "higher_is_better": True, "scaling": "weak",

@@ -233,6 +233,8 @@ typedef struct {
   int last_ns_iters;    /* out */
   double last_ns_err;   /* out */
   double last_smax;     /* out: max |S - 2I| of this step */
+  int last_kernels;     /* out: kernel launches of one step when it replays as a CUDA graph
+                           (counted in the captured graph), else -1 */
 } oa_cp_state;
 
 /* One whole CP dynamics step (GSpaceDriver::computeDynamics,

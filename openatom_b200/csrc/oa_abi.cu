@@ -31,6 +31,8 @@ cudaError_t oa_launch_integrate(cudaStream_t s, const double2* F, double2* V, do
                                 double* kepart, int nblk);
 cudaError_t oa_launch_sync_redundant(cudaStream_t s, double2* P, double2* V, const int* partner, int nred, int ng,
                                      int nstate);
+cudaError_t oa_launch_sum_partials_multi(cudaStream_t s, int njob, const double* const* part, const int* n,
+                                         const int* stride, const int* off, const double* scale, double* const* out);
 cudaError_t oa_launch_sum_partials(cudaStream_t s, const double* part, int n, int stride, int off, double scale,
                                    double* out);
 cudaError_t oa_launch_umma_fwd(cudaStream_t s, int nterm, const double* A, const double* B, int m, int n, long K,
@@ -437,12 +439,16 @@ extern "C" oa_status oa_gpu_vks_build(oa_ctx* c, void* stream, double* vks_out) 
   const int nx = oa_rho_xc_nblk(), nzb = oa_rho_z_nblk(c);
   const double vs = c->vol / (double)c->npts;
   // EEXC = (0.75 ex + ec) V/N ; MUXC = sum vxc rho V/N
-  OA_CUDA_TRY(oa_launch_sum_partials(s, c->red, nx, 3, 0, 0.75 * vs, p->dev_e + 8));
-  OA_CUDA_TRY(oa_launch_sum_partials(s, c->red, nx, 3, 1, vs, p->dev_e + 9));
-  OA_CUDA_TRY(oa_launch_sum_partials(s, c->red, nx, 3, 2, vs, p->dev_e + OA_E_MUXC));
-  OA_CUDA_TRY(oa_launch_sum_partials(s, c->red + 3 * nx, nzb, 3, 0, 0.5, p->dev_e + OA_E_EHART));
-  OA_CUDA_TRY(oa_launch_sum_partials(s, c->red + 3 * nx, nzb, 3, 1, 1.0, p->dev_e + OA_E_EEXT));
-  OA_CUDA_TRY(oa_launch_sum_partials(s, c->red + 3 * nx, nzb, 3, 2, 0.5, p->dev_e + OA_E_EWALD));
+  {
+    const double* part[6] = {c->red, c->red, c->red, c->red + 3 * nx, c->red + 3 * nx, c->red + 3 * nx};
+    const int n[6] = {nx, nx, nx, nzb, nzb, nzb};
+    const int stride[6] = {3, 3, 3, 3, 3, 3};
+    const int off[6] = {0, 1, 2, 0, 1, 2};
+    const double scale[6] = {0.75 * vs, vs, vs, 0.5, 1.0, 0.5};
+    double* out[6] = {p->dev_e + 8, p->dev_e + 9, p->dev_e + OA_E_MUXC, p->dev_e + OA_E_EHART,
+                      p->dev_e + OA_E_EEXT, p->dev_e + OA_E_EWALD};
+    OA_CUDA_TRY(oa_launch_sum_partials_multi(s, 6, part, n, stride, off, scale, out));
+  }
   if (vks_out) {
     if (c->precision == OA_FP64)
       OA_CUDA_TRY(cudaMemcpyAsync(vks_out, c->vks, (size_t)c->npts * 8, cudaMemcpyDeviceToDevice, s));
@@ -678,9 +684,10 @@ extern "C" oa_status oa_gpu_sizes(const oa_ctx* c, long* out) {
   OA_ARG_CHECK(c && out, "null argument");
   out[0] = c->nstate; out[1] = c->ng; out[2] = c->nlines; out[3] = c->nz; out[4] = c->ldl;
   out[5] = c->ngroup; out[6] = c->npts; out[7] = c->precision == OA_FP64 ? 8 : 4; out[8] = c->nlines_d;
-  // kernels of oa_gpu_cp_step: state_fft_fwd 3 + vks_build 10 + nl_sf 7 + vks_apply 4 + lambda 4 +
+  // kernels of the FP64 oa_gpu_cp_step (an estimate; oa_cp_state.last_kernels counts the
+  // graphed step): state_fft_fwd 3 + vks_build 5 + nl_sf 7 + vks_apply 4 + lambda 4 +
   // integrate 3 + S 2 + Newton-Schulz 1 + Psi T 1
-  out[9] = 3 + 10 + 7 + 4 + 4 + 3 + 2 + 1 + 1;
+  out[9] = 3 + 5 + 7 + 4 + 4 + 3 + 2 + 1 + 1;
   out[10] = c->pair_cols ? 1 : 0;  // state-pair plane kernels in use (mixed form)
   out[11] = c->ngroup_pair;
   return OA_OK;

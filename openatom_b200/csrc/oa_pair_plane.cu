@@ -46,7 +46,7 @@ template <int N1, int N2> struct PairCfg {
 };
 
 struct PairSmem {
-  size_t tw, col, xh, rows, P, S, total;
+  size_t tw, col, xh, rows, P, S, Sy, total;
   int lr;  // z-line row length in shared memory (float2, even)
 };
 
@@ -74,7 +74,12 @@ static __device__ __forceinline__ float2 pp_herm(const float2* P, int nkx, int k
 }
 
 // ---------------------------------------------------------------------------
-// density pass: block (z, group) runs the pairs of its group through plane z
+// density pass: block (z, group) runs the pairs of its group through plane z,
+// software-pipelined so that each block barrier separates two phases that
+// mix the x work of pair q with the y work of pair q + 1:
+//   phase a(q): x pass A (q)  [P -> Sx]   +  y pass A (q+1) [rows -> Sy]
+//   phase b(q): x pass B (q)  [Sx -> psi(r), density]  +  y pass B (q+1) [Sy -> P]
+// The z-line rows of pair q + 2 arrive by cp.async during both phases.
 // ---------------------------------------------------------------------------
 template <int N1, int N2>
 __global__ void __launch_bounds__(PairCfg<N1, N2>::NT, 1)
@@ -89,9 +94,11 @@ k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* tw = (float2*)(smem_raw + L.tw);
   int4* col = (int4*)(smem_raw + L.col);
+  int2* xh = (int2*)(smem_raw + L.xh);
   float2* rb = (float2*)(smem_raw + L.rows);
   float2* P = (float2*)(smem_raw + L.P);
-  float2* S = (float2*)(smem_raw + L.S);
+  float2* Sx = (float2*)(smem_raw + L.S);
+  float2* Sy = (float2*)(smem_raw + L.Sy);
   const int tid = threadIdx.x;
   const int z = blockIdx.x, g = blockIdx.y;
   const int npair = (nstate + 1) / 2;
@@ -101,7 +108,8 @@ k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int
   const int npc = 2 * nkx;
   int lp = 0;
   while ((1 << lp) < npc) ++lp;
-  int2* xh = (int2*)(smem_raw + L.xh);
+  const int ya_slots = N2 << lp;
+  constexpr int XA_ITEMS = N2 * N;
   for (int i = tid; i < N; i += NT) tw[i] = make_float2((float)twg[i].x, (float)twg[i].y);
   for (int i = tid; i < nkx; i += NT) col[i] = cols[i];
   // Hermitian table of x pass A, entry n2 * N1 + n1 for kx index k = N2 n1 + n2:
@@ -132,76 +140,82 @@ k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int
     }
     pp_commit();
   };
-  if (qb < qe) prefetch(qb, 0);
+  // y pass A, slot sl of pair q (rows in buffer buf): pencil (state, column)
+  // fastest in slots of 2^lp per n2; zero outside the column's run
+  auto y_a = [&](int q, int buf, int sl) {
+    const int n2 = sl >> lp, pc = sl & ((1 << lp) - 1);
+    if (pc >= npc) return;
+    const int st = pc >= nkx ? 1 : 0, cx = pc - st * nkx;
+    const int4 cr = col[cx];
+    const float2* r = rb + (size_t)(2 * buf + st) * lr + cr.x;
+    const bool live = 2 * q + st < nstate;
+    float2 u[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int i = N2 * n1 + n2;
+      const int ky = (2 * i <= N) ? i : i - N;
+      const int l = ky - cr.y;
+      u[n1] = (live && l >= 0 && l < cr.z) ? r[l] : make_float2(0.f, 0.f);
+    }
+    pass_a<N1, N2, -1>(u, n2, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) Sy[pc * PS1 + k1 * LS1 + n2] = u[k1];
+  };
+  // y pass B, slot it: one pencil per 16 lanes -> P[st][kx][y]
+  auto y_b = [&](int it) {
+    const int pc = it >> 4, k1 = it & 15;
+    if (k1 >= N1) return;
+    float2 w[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) w[n2] = Sy[pc * PS1 + k1 * LS1 + n2];
+    RDft<N2, -1>::run(w);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) P[pc * LDY + k1 + N1 * k2] = w[k2];
+  };
+  // x pass A, item it: rows fastest (n2 warp-uniform); the pair packs as
+  // psi_a + i psi_b, read through the Hermitian table
+  auto x_a = [&](int it) {
+    const int n2 = it / N, y = it - n2 * N;
+    const int2* hx = xh + n2 * N1;
+    float2 u[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int2 t = hx[n1];
+      float2 v = make_float2(0.f, 0.f);
+      if (t.x >= 0) {
+        const float2 a = P[t.x + y], b = P[t.x + nkx * LDY + y];
+        const float sg = __int_as_float(t.y);
+        v = make_float2(fmaf(-sg, b.y, a.x), fmaf(sg, a.y, b.x));
+      }
+      u[n1] = v;
+    }
+    pass_a<N1, N2, -1>(u, n2, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) Sx[y * PS1 + k1 * LS1 + n2] = u[k1];
+  };
+  if (qb < qe) {
+    prefetch(qb, 0);
+    if (qb + 1 < qe) { prefetch(qb + 1, 1); pp_wait<1>(); } else { pp_wait<0>(); }
+    __syncthreads();
+    for (int sl = tid; sl < ya_slots; sl += NT) y_a(qb, 0, sl);
+    __syncthreads();
+    for (int it = tid; it < 16 * npc; it += NT) y_b(it);
+  }
   for (int q = qb; q < qe; ++q) {
-    const int buf = (q - qb) & 1;
-    if (q + 1 < qe) {
-      prefetch(q + 1, buf ^ 1);
-      pp_wait<1>();
-    } else {
-      pp_wait<0>();
-    }
-    const bool has1 = 2 * q + 1 < nstate;
+    const bool nxt = q + 1 < qe;
+    pp_wait<0>();
     __syncthreads();
-    // y pass A: pencil (state, column) fastest in slots of 2^lp per n2;
-    // zero outside the column's run
-    for (int it = tid; it < (N2 << lp); it += NT) {
-      const int n2 = it >> lp, pc = it & ((1 << lp) - 1);
-      if (pc >= npc) continue;
-      const int st = pc >= nkx ? 1 : 0, cx = pc - st * nkx;
-      const int4 cr = col[cx];
-      const float2* r = rb + (size_t)(2 * buf + st) * lr + cr.x;
-      const bool live = st == 0 || has1;
-      float2 u[N1];
-#pragma unroll
-      for (int n1 = 0; n1 < N1; ++n1) {
-        const int i = N2 * n1 + n2;
-        const int ky = (2 * i <= N) ? i : i - N;
-        const int l = ky - cr.y;
-        u[n1] = (live && l >= 0 && l < cr.z) ? r[l] : make_float2(0.f, 0.f);
-      }
-      pass_a<N1, N2, -1>(u, n2, tw);
-#pragma unroll
-      for (int k1 = 0; k1 < N1; ++k1) S[pc * PS1 + k1 * LS1 + n2] = u[k1];
+    if (q + 2 < qe) prefetch(q + 2, (q - qb) & 1);
+    // phase a: x pass A (q) + y pass A (q + 1)
+    const int na = XA_ITEMS + (nxt ? ya_slots : 0);
+    for (int it = tid; it < na; it += NT) {
+      if (it < XA_ITEMS) x_a(it);
+      else y_a(q + 1, (q + 1 - qb) & 1, it - XA_ITEMS);
     }
     __syncthreads();
-    // y pass B: one pencil per 16 lanes -> P[st][kx][y]
-    for (int it = tid; it < 16 * npc; it += NT) {
-      const int pc = it >> 4, k1 = it & 15;
-      if (k1 >= N1) continue;
-      float2 w[N2];
-#pragma unroll
-      for (int n2 = 0; n2 < N2; ++n2) w[n2] = S[pc * PS1 + k1 * LS1 + n2];
-      RDft<N2, -1>::run(w);
-#pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) P[pc * LDY + k1 + N1 * k2] = w[k2];
-    }
-    __syncthreads();
-    // x pass A: rows fastest (n2 warp-uniform); the pair packs as
-    // psi_a + i psi_b, read through the Hermitian table
-    for (int it = tid; it < N2 * N; it += NT) {
-      const int n2 = it / N, y = it - n2 * N;
-      const int2* hx = xh + n2 * N1;
-      float2 u[N1];
-#pragma unroll
-      for (int n1 = 0; n1 < N1; ++n1) {
-        const int2 t = hx[n1];
-        float2 v = make_float2(0.f, 0.f);
-        if (t.x >= 0) {
-          const float2 a = P[t.x + y], b = P[t.x + nkx * LDY + y];
-          const float sg = __int_as_float(t.y);
-          v = make_float2(fmaf(-sg, b.y, a.x), fmaf(sg, a.y, b.x));
-        }
-        u[n1] = v;
-      }
-      pass_a<N1, N2, -1>(u, n2, tw);
-#pragma unroll
-      for (int k1 = 0; k1 < N1; ++k1) S[y * PS1 + k1 * LS1 + n2] = u[k1];
-    }
-    __syncthreads();
-    // x pass B: fixed slots per thread; density and psi(r)
+    // phase b: x pass B (q), fixed slots per thread (density, psi(r)) + y pass B (q + 1)
     const float o0 = (float)occ[2 * q];
-    const float o1 = has1 ? (float)occ[2 * q + 1] : 0.f;
+    const float o1 = 2 * q + 1 < nstate ? (float)occ[2 * q + 1] : 0.f;
     float2* pq = psir + ((size_t)q * nz + z) * N * N;
 #pragma unroll
     for (int j = 0; j < XBW; ++j) {
@@ -210,7 +224,7 @@ k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int
       if (k1 < N1) {
         float2 w[N2];
 #pragma unroll
-        for (int n2 = 0; n2 < N2; ++n2) w[n2] = S[y * PS1 + k1 * LS1 + n2];
+        for (int n2 = 0; n2 < N2; ++n2) w[n2] = Sx[y * PS1 + k1 * LS1 + n2];
         RDft<N2, -1>::run(w);
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2) {
@@ -219,6 +233,8 @@ k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int
         }
       }
     }
+    if (nxt)
+      for (int it = tid; it < 16 * npc; it += NT) y_b(it);
   }
   double* out = rho_part + ((size_t)g * nz + z) * N * N;
 #pragma unroll
@@ -234,7 +250,10 @@ k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int
 
 // ---------------------------------------------------------------------------
 // V_KS pass from the stored psi(r): psi V_KS occ -> x FFT(+) with the r2c
-// unpack of the pair -> y FFT(+) -> the z-line rows of both states
+// unpack of the pair -> y FFT(+) -> the z-line rows of both states.
+// Software-pipelined as the density pass, the y work one pair behind:
+//   phase a(q): x pass B' (q) [psi(r) -> S2]  +  y pass A' (q-1) [P -> Sy]
+//   phase b(q): x pass A' (q) [S2 -> P]       +  y pass B' (q-1) [Sy -> rows]
 // ---------------------------------------------------------------------------
 template <int N1, int N2>
 __global__ void __launch_bounds__(PairCfg<N1, N2>::NT, 1)
@@ -254,7 +273,8 @@ k_pair_vks(float2* __restrict__ zbuf, int nstate, int nz, int ldl, const int4* _
   float2* tw = (float2*)(smem_raw + L.tw);
   int4* col = (int4*)(smem_raw + L.col);
   float2* P = (float2*)(smem_raw + L.P);
-  float2* S = (float2*)(smem_raw + L.S);
+  float2* S2 = (float2*)(smem_raw + L.S);
+  float2* Sy = (float2*)(smem_raw + L.Sy);
   const int tid = threadIdx.x;
   const int z = blockIdx.x, g = blockIdx.y;
   const int npair = (nstate + 1) / 2;
@@ -263,6 +283,7 @@ k_pair_vks(float2* __restrict__ zbuf, int nstate, int nz, int ldl, const int4* _
   const int npc = 2 * nkx;
   int lp = 0;
   while ((1 << lp) < npc) ++lp;
+  const int ya_slots = N2 << lp;
   const int kf = tid & 15;  // this thread's k1 in x pass B' (NT is a multiple of 16)
   for (int i = tid; i < N; i += NT) tw[i] = make_float2((float)twg[i].x, (float)twg[i].y);
   for (int i = tid; i < nkx; i += NT) col[i] = cols[i];
@@ -273,19 +294,21 @@ k_pair_vks(float2* __restrict__ zbuf, int nstate, int nz, int ldl, const int4* _
 #pragma unroll
     for (int m2 = 0; m2 < N2; ++m2) tk[m2] = tw_rt<+1>(tw, kf * m2);
   }
-  for (int q = qb; q < qe; ++q) {
-    const bool has1 = 2 * q + 1 < nstate;
-    const float o0 = (float)occ[2 * q];
-    const float o1 = has1 ? (float)occ[2 * q + 1] : 0.f;
-    const float2* pq = psir + ((size_t)q * nz + z) * N * N;
+  for (int q = qb; q <= qe; ++q) {
+    const bool cur = q < qe, prev = q > qb;
     if (q + 1 < qe && tid < PF_PARTS) {
       // the next pair's psi(r) plane heads for L2 while this pair computes
-      const char* nxt = (const char*)(pq + (size_t)nz * N * N) + (size_t)tid * PF_BYTES;
+      const char* nxt = (const char*)(psir + ((size_t)(q + 1) * nz + z) * N * N) + (size_t)tid * PF_BYTES;
       asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(nxt), "r"(PF_BYTES) : "memory");
     }
     __syncthreads();
-    // x pass B' (inverse, first half): DFT_N2(+) over k2, twiddle -> S[y][m2][k1]
-    if (kf < N1) {
+    // phase a: x pass B' (q) (inverse, first half: DFT_N2(+) over k2,
+    // twiddle -> S2[y][m2][k1]) + y pass A' (q - 1)
+    if (cur && kf < N1) {
+      const bool has1 = 2 * q + 1 < nstate;
+      const float o0 = (float)occ[2 * q];
+      const float o1 = has1 ? (float)occ[2 * q + 1] : 0.f;
+      const float2* pq = psir + ((size_t)q * nz + z) * N * N;
 #pragma unroll
       for (int j = 0; j < XBW; ++j) {
         const int y = (tid + NT * j) >> 4;
@@ -297,76 +320,81 @@ k_pair_vks(float2* __restrict__ zbuf, int nstate, int nz, int ldl, const int4* _
           w[k2] = make_float2(p.x * v * o0, p.y * v * o1);
         }
         RDft<N2, +1>::run(w);
-        S[y * PS2 + kf] = w[0];
+        S2[y * PS2 + kf] = w[0];
 #pragma unroll
-        for (int m2 = 1; m2 < N2; ++m2) S[y * PS2 + m2 * LS2 + kf] = cmul(w[m2], tk[m2]);
+        for (int m2 = 1; m2 < N2; ++m2) S2[y * PS2 + m2 * LS2 + kf] = cmul(w[m2], tk[m2]);
+      }
+    }
+    if (prev) {
+      for (int sl = tid; sl < ya_slots; sl += NT) {
+        const int n2 = sl >> lp, pc = sl & ((1 << lp) - 1);
+        if (pc >= npc) continue;
+        float2 u[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) u[n1] = P[pc * LDY + N2 * n1 + n2];
+        pass_a<N1, N2, +1>(u, n2, tw);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) Sy[pc * PS1 + k1 * LS1 + n2] = u[k1];
       }
     }
     __syncthreads();
-    // x pass A' (inverse, second half) on the classes {j, N2 - j}, then the
-    // two-for-one unpack of the pair into P[st][kx][y] for kx < nkx
-    for (int it = tid; it < NJ * N; it += NT) {
-      const int jj = it / N, y = it - jj * N;
-      const int ma = jj, mb = (N2 - jj) % N2;
-      const bool two = ma != mb;
-      float2 za[N1], zb[N1];
+    // phase b: x pass A' (q) (inverse, second half, on the classes
+    // {j, N2 - j}; two-for-one unpack of the pair into P[st][kx][y] for
+    // kx < nkx) + y pass B' (q - 1) -> the column's z-line run of each state
+    if (cur) {
+      for (int it = tid; it < NJ * N; it += NT) {
+        const int jj = it / N, y = it - jj * N;
+        const int ma = jj, mb = (N2 - jj) % N2;
+        const bool two = ma != mb;
+        float2 za[N1], zb[N1];
 #pragma unroll
-      for (int k1 = 0; k1 < N1; ++k1) za[k1] = S[y * PS2 + ma * LS2 + k1];
-      RDft<N1, +1>::run(za);
-      if (two) {
-#pragma unroll
-        for (int k1 = 0; k1 < N1; ++k1) zb[k1] = S[y * PS2 + mb * LS2 + k1];
-        RDft<N1, +1>::run(zb);
-      }
-      auto put = [&](int K, float2 a, float2 bp) {
-        const float2 b = make_float2(bp.x, -bp.y);
-        P[K * LDY + y] = make_float2((a.x + b.x) * 0.5f, (a.y + b.y) * 0.5f);
-        P[(nkx + K) * LDY + y] = make_float2((a.y - b.y) * 0.5f, -(a.x - b.x) * 0.5f);
-      };
-#pragma unroll
-      for (int m1 = 0; m1 < N1; ++m1) {
-        const int K = ma + N2 * m1;
-        if (K < nkx) {
-          const float2 pa = (jj == 0) ? za[(N1 - m1) % N1] : (two ? zb[N1 - 1 - m1] : za[N1 - 1 - m1]);
-          put(K, za[m1], pa);
-        }
+        for (int k1 = 0; k1 < N1; ++k1) za[k1] = S2[y * PS2 + ma * LS2 + k1];
+        RDft<N1, +1>::run(za);
         if (two) {
-          const int Kb = mb + N2 * m1;
-          if (Kb < nkx) put(Kb, zb[m1], za[N1 - 1 - m1]);
+#pragma unroll
+          for (int k1 = 0; k1 < N1; ++k1) zb[k1] = S2[y * PS2 + mb * LS2 + k1];
+          RDft<N1, +1>::run(zb);
+        }
+        auto put = [&](int K, float2 a, float2 bp) {
+          const float2 b = make_float2(bp.x, -bp.y);
+          P[K * LDY + y] = make_float2((a.x + b.x) * 0.5f, (a.y + b.y) * 0.5f);
+          P[(nkx + K) * LDY + y] = make_float2((a.y - b.y) * 0.5f, -(a.x - b.x) * 0.5f);
+        };
+#pragma unroll
+        for (int m1 = 0; m1 < N1; ++m1) {
+          const int K = ma + N2 * m1;
+          if (K < nkx) {
+            const float2 pa = (jj == 0) ? za[(N1 - m1) % N1] : (two ? zb[N1 - 1 - m1] : za[N1 - 1 - m1]);
+            put(K, za[m1], pa);
+          }
+          if (two) {
+            const int Kb = mb + N2 * m1;
+            if (Kb < nkx) put(Kb, zb[m1], za[N1 - 1 - m1]);
+          }
         }
       }
     }
-    __syncthreads();
-    // y pass A' (+): pencils fastest in slots of 2^lp per n2
-    for (int it = tid; it < (N2 << lp); it += NT) {
-      const int n2 = it >> lp, pc = it & ((1 << lp) - 1);
-      if (pc >= npc) continue;
-      float2 u[N1];
+    if (prev) {
+      const int qp = q - 1;
+      const bool has1p = 2 * qp + 1 < nstate;
+      for (int it = tid; it < 16 * npc; it += NT) {
+        const int pc = it >> 4, k1 = it & 15;
+        if (k1 >= N1) continue;
+        const int st = pc >= nkx ? 1 : 0, cx = pc - st * nkx;
+        if (st == 1 && !has1p) continue;
+        float2 w[N2];
 #pragma unroll
-      for (int n1 = 0; n1 < N1; ++n1) u[n1] = P[pc * LDY + N2 * n1 + n2];
-      pass_a<N1, N2, +1>(u, n2, tw);
+        for (int n2 = 0; n2 < N2; ++n2) w[n2] = Sy[pc * PS1 + k1 * LS1 + n2];
+        RDft<N2, +1>::run(w);
+        const int4 cr = col[cx];
+        float2* row = zbuf + ((size_t)(2 * qp + st) * nz + z) * ldl + cr.x;
 #pragma unroll
-      for (int k1 = 0; k1 < N1; ++k1) S[pc * PS1 + k1 * LS1 + n2] = u[k1];
-    }
-    __syncthreads();
-    // y pass B' (+) -> the column's z-line run of each state
-    for (int it = tid; it < 16 * npc; it += NT) {
-      const int pc = it >> 4, k1 = it & 15;
-      if (k1 >= N1) continue;
-      const int st = pc >= nkx ? 1 : 0, cx = pc - st * nkx;
-      if (st == 1 && !has1) continue;
-      float2 w[N2];
-#pragma unroll
-      for (int n2 = 0; n2 < N2; ++n2) w[n2] = S[pc * PS1 + k1 * LS1 + n2];
-      RDft<N2, +1>::run(w);
-      const int4 cr = col[cx];
-      float2* row = zbuf + ((size_t)(2 * q + st) * nz + z) * ldl + cr.x;
-#pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) {
-        const int i = k1 + N1 * k2;
-        const int ky = (2 * i <= N) ? i : i - N;
-        const int l = ky - cr.y;
-        if (l >= 0 && l < cr.z) row[l] = w[k2];
+        for (int k2 = 0; k2 < N2; ++k2) {
+          const int i = k1 + N1 * k2;
+          const int ky = (2 * i <= N) ? i : i - N;
+          const int l = ky - cr.y;
+          if (l >= 0 && l < cr.z) row[l] = w[k2];
+        }
       }
     }
   }
@@ -386,9 +414,10 @@ static PairSmem pair_layout(int nkx, int nlines, int mode) {
   L.xh = o; o += align_up((size_t)CF::N * sizeof(int2), 16);
   L.rows = o; o += mode == 0 ? (size_t)4 * L.lr * sizeof(float2) : 0;
   L.P = o; o += align_up((size_t)2 * nkx * CF::LDY * sizeof(float2), 16);
-  size_t s = (size_t)(CF::N > 2 * nkx ? CF::N : 2 * nkx) * CF::PS1;
-  if (mode != 0 && (size_t)CF::N * CF::PS2 > s) s = (size_t)CF::N * CF::PS2;
-  L.S = o; o += align_up(s * sizeof(float2), 16);
+  // x buffer: Sx [N][PS1] (density) or S2 [N][PS2] (V_KS); y buffer Sy [2 nkx][PS1]
+  const size_t sx = (size_t)CF::N * (mode == 0 ? CF::PS1 : CF::PS2);
+  L.S = o; o += align_up(sx * sizeof(float2), 16);
+  L.Sy = o; o += align_up((size_t)2 * nkx * CF::PS1 * sizeof(float2), 16);
   L.total = o;
   return L;
 }

@@ -179,16 +179,50 @@ k_pc_bwd_f64(const double* __restrict__ M1, const double* __restrict__ X1, doubl
 }
 
 // ---------------------------------------------------------------------------
-// small N x N: C = alpha * A^op B  (op = none), FP64, one output per thread
+// small N x N: C = alpha * A B, FP64; 32 x 32 output tile per block of
+// 256 threads (4 outputs each), K in slabs of 32 through shared memory
 // ---------------------------------------------------------------------------
-__global__ void k_small_gemm(const double* __restrict__ A, const double* __restrict__ B, int n, double alpha,
-                             double* __restrict__ C) {
-  const int i = blockIdx.y * 16 + threadIdx.y, j = blockIdx.x * 16 + threadIdx.x;
-  if (i >= n || j >= n) return;
-  double s = 0.0;
-  for (int k = 0; k < n; ++k) s += A[(size_t)i * n + k] * B[(size_t)k * n + j];
-  C[(size_t)i * n + j] = alpha * s;
+__global__ void __launch_bounds__(256)
+k_small_gemm(const double* __restrict__ A, const double* __restrict__ B, int n, double alpha,
+             double* __restrict__ C) {
+  __shared__ double sA[32][33], sB[32][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // ty 0..7: rows ty, ty + 8, ..
+  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int k0 = 0; k0 < n; k0 += 32) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int row = ty + 8 * r;
+      const int ia = i0 + row, ka = k0 + tx;
+      sA[row][tx] = (ia < n && ka < n) ? A[(size_t)ia * n + ka] : 0.0;
+      const int kb = k0 + row, jb = j0 + tx;
+      sB[row][tx] = (kb < n && jb < n) ? B[(size_t)kb * n + jb] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) {
+      const double b = sB[k][tx];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[r] = fma(sA[ty + 8 * r][k], b, acc[r]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int i = i0 + ty + 8 * r, j = j0 + tx;
+    if (i < n && j < n) C[(size_t)i * n + j] = alpha * acc[r];
+  }
 }
+
+// Several single-block sums in one launch: block b writes
+// out[b] = scale[b] * sum_i part[b][i * stride[b] + off[b]], in the order of
+// k_sum_partials.
+struct SumJobs {
+  const double* part[8];
+  double* out[8];
+  double scale[8];
+  int n[8], stride[8], off[8];
+};
 
 // ---------------------------------------------------------------------------
 // Newton-Schulz S^-1/2 (ortho.C), one cooperative kernel, bounded iterations.
@@ -411,6 +445,24 @@ __global__ void k_sum_partials(const double* __restrict__ part, int n, int strid
   }
 }
 
+__global__ void k_sum_partials_multi(SumJobs J) {
+  __shared__ double sh[32];
+  const int b = blockIdx.x;
+  const double* part = J.part[b];
+  const int n = J.n[b], stride = J.stride[b], off = J.off[b];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += part[(size_t)i * stride + off];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+    J.out[b][0] = J.scale[b] * t;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -460,8 +512,22 @@ cudaError_t oa_launch_pc_bwd(cudaStream_t s, const double* M1, const double* X1,
 }
 
 cudaError_t oa_launch_small_gemm(cudaStream_t s, const double* A, const double* B, int n, double alpha, double* C) {
-  dim3 grid((n + 15) / 16, (n + 15) / 16), blk(16, 16);
-  k_small_gemm<<<grid, blk, 0, s>>>(A, B, n, alpha, C);
+  dim3 grid((n + 31) / 32, (n + 31) / 32);
+  k_small_gemm<<<grid, 256, 0, s>>>(A, B, n, alpha, C);
+  return cudaGetLastError();
+}
+
+// six reductions of the density / Hartree partials in one launch (see
+// oa_gpu_vks_build): entries b < njob of the arrays
+cudaError_t oa_launch_sum_partials_multi(cudaStream_t s, int njob, const double* const* part, const int* n,
+                                         const int* stride, const int* off, const double* scale, double* const* out) {
+  if (njob < 1 || njob > 8) return cudaErrorInvalidValue;
+  SumJobs J;
+  for (int b = 0; b < njob; ++b) {
+    J.part[b] = part[b]; J.out[b] = out[b]; J.scale[b] = scale[b];
+    J.n[b] = n[b]; J.stride[b] = stride[b]; J.off[b] = off[b];
+  }
+  k_sum_partials_multi<<<njob, 256, 0, s>>>(J);
   return cudaGetLastError();
 }
 

@@ -340,6 +340,11 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
   }
 }
 
+cudaError_t oa_rho2_fwd(cudaStream_t s, int n, int nz, const double* rho, double scale, const double2* tw,
+                        double2* dz, int ldl_d);
+cudaError_t oa_rho2_bwd(cudaStream_t s, int n, int nz, const double2* dz, int ldl_d, const double2* tw,
+                        const double* vxc, void* vks, int fp64);
+
 __global__ void k_phase_tables(const double* __restrict__ pos, int natm, int ktab, double tpi_l, double2* __restrict__ phase) {
   const int nt = 2 * ktab + 1;
   const int total = natm * 3 * nt;
@@ -380,12 +385,18 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
   // phase tables exp(i 2 pi k x / L)
   if ((e = oa_launch_phase_tables(c, s)) != cudaSuccess) return e;
   RhoPlaneSmem L = rho_plane_layout(c->nx, c->ny, c->nkx_d, c->npair_d, c->ychunk_d);
-  e = cudaFuncSetAttribute(k_rho_plane_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+  const bool two_pass = c->nx == c->ny;
+  e = two_pass ? oa_rho2_fwd(s, c->nx, c->nz, c->rho, c->vol / c->npts, c->tw_x, (double2*)c->dz, c->ldl_d)
+               : cudaErrorNotSupported;
+  if (e == cudaErrorNotSupported) {
+    e = cudaFuncSetAttribute(k_rho_plane_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    if (e != cudaSuccess) return e;
+    k_rho_plane_fwd<<<c->nz, OA_NTHREADS, L.total, s>>>(c->rho, c->vol / c->npts, c->nx, c->ny, c->nz, c->nkx_d,
+                                                         c->plan_x, c->plan_y, c->tw_x, c->tw_y,
+                                                         (double2*)c->dz, c->ldl_d, c->npair_d, c->ychunk_d, L);
+    e = cudaGetLastError();
+  }
   if (e != cudaSuccess) return e;
-  k_rho_plane_fwd<<<c->nz, OA_NTHREADS, L.total, s>>>(c->rho, c->vol / c->npts, c->nx, c->ny, c->nz, c->nkx_d,
-                                                       c->plan_x, c->plan_y, c->tw_x, c->tw_y,
-                                                       (double2*)c->dz, c->ldl_d, c->npair_d, c->ychunk_d, L);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const size_t smz = (align_up_r(c->nz, 2) + 2 * (size_t)OA_LB * (c->nz + 1) + (size_t)OA_LB * c->natm) *
                      sizeof(double2);
   if (smz > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
@@ -401,6 +412,11 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
                                             c->spl, c->nspl, c->spl_gmin, c->spl_dg,
                                             c->red + 3 * oa_rho_xc_nblk());
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (two_pass) {
+    e = oa_rho2_bwd(s, c->nx, c->nz, (const double2*)c->dz, c->ldl_d, c->tw_x, c->vxc, c->vks,
+                    c->precision == OA_FP64);
+    if (e != cudaErrorNotSupported) return e;
+  }
   if (c->precision == OA_FP64) {
     e = cudaFuncSetAttribute(k_rho_plane_bwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
     if (e != cudaSuccess) return e;

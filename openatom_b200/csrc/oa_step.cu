@@ -12,6 +12,7 @@
 // synchronises once; oa_gpu_cp_step is the one-step case.
 #include <stdio.h>
 #include <string.h>
+#include <vector>
 #include "oa_internal.h"
 
 // entry points of oa_abi.cu used here
@@ -61,6 +62,7 @@ struct oa_step_scratch {
   const void* key[7];
   int key_nterm;
   double key_dt, key_tol;
+  int graph_kernels;      // kernel launches of one graphed step (graph nodes + launches outside)
 };
 
 static oa_step_scratch* step_scratch(oa_ctx* c) { return (oa_step_scratch*)c->step; }
@@ -235,6 +237,7 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
       if (!same) {
         if (w->exec) { cudaGraphExecDestroy(w->exec); w->exec = nullptr; }
         if (w->exec2) { cudaGraphExecDestroy(w->exec2); w->exec2 = nullptr; }
+        int nker = ns_in_graph ? 0 : 1;  // the Newton-Schulz launch between the two graphs
         for (int part = 0; part < (ns_in_graph ? 1 : 2); ++part) {
           cudaGraph_t g = nullptr;
           OA_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -249,11 +252,23 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
           cudaError_t ce = cudaStreamEndCapture(s, &g);
           if (r != OA_OK) { if (g) cudaGraphDestroy(g); return r; }
           if (ce != cudaSuccess) { oa_set_error(cudaGetErrorString(ce), __FILE__, __LINE__); return OA_ERR_CUDA; }
+          {
+            size_t nn = 0;
+            if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn > 0) {
+              std::vector<cudaGraphNode_t> nodes(nn);
+              if (cudaGraphGetNodes(g, nodes.data(), &nn) == cudaSuccess)
+                for (size_t i = 0; i < nn; ++i) {
+                  cudaGraphNodeType t;
+                  if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nker;
+                }
+            }
+          }
           ce = cudaGraphInstantiate(part == 0 ? &w->exec : &w->exec2, g, 0);
           cudaGraphDestroy(g);
           if (ce != cudaSuccess) { oa_set_error(cudaGetErrorString(ce), __FILE__, __LINE__); return OA_ERR_CUDA; }
         }
         memcpy(w->key, key, sizeof(key));
+        w->graph_kernels = nker;
         w->key_nterm = st->mixed_nterm;
         w->key_dt = st->dt;
         w->key_tol = st->norb_tol;
@@ -292,6 +307,7 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
     }
   }
   const double* last = w->ring_host + (size_t)(nsteps - 1) * OA_REC;
+  st->last_kernels = (st->use_graph && st->iteration > 1 && w->exec) ? w->graph_kernels : -1;
   st->last_ns_iters = (int)last[16];
   st->last_ns_err = last[18];
   st->last_smax = last[19];

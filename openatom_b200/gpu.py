@@ -56,6 +56,7 @@ class CPState(C.Structure):
         ("iteration", C.c_int), ("dt", C.c_double), ("ns_tol", C.c_double), ("norb_tol", C.c_double),
         ("ns_max_iter", C.c_int), ("mixed_nterm", C.c_int), ("use_graph", C.c_int),
         ("last_ns_iters", C.c_int), ("last_ns_err", C.c_double), ("last_smax", C.c_double),
+        ("last_kernels", C.c_int),
     ]
 
 
