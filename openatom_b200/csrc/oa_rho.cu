@@ -13,6 +13,7 @@
 // backward exp(+i g.r) are the ones under which the e^{+i g.R} structure
 // factor of cp_hart_ext.C gives E_ext = integral rho V_loc.
 #include "oa_internal.h"
+#include "oa_rdft.cuh"
 
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
@@ -231,6 +232,40 @@ struct RhoTypeOff { int off[5]; };
 // z-line: pxy[line][a] = e^{i (gx x_a + gy y_a)} is formed once per block in
 // shared memory (atoms grouped by type), and each g of the line multiplies
 // it by the z phase e^{i gz z_a}.
+// In-place z transform of nb lines a[line][z] (row stride ld) for the
+// lengths with a compile-time factorisation N = N1 N2 (oa_rdft.cuh): pass A
+// (lines fastest) into b [line][k1][n2], pass B back to natural order in a.
+template <int N1, int N2> struct ZLd {
+  static constexpr int LS = N2 | 1;
+  static constexpr int PS = (N1 * LS) | 1;
+};
+template <int N1, int N2, int SIGN>
+__device__ void zfft2(double2* a, double2* b, int ld, int nb, const double2* tw) {
+  typedef ZLd<N1, N2> L;
+  for (int i = threadIdx.x; i < N2 * nb; i += blockDim.x) {
+    const int n2 = i / nb, lb = i - n2 * nb;
+    double2 u[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) u[n1] = a[lb * ld + N2 * n1 + n2];
+    pass_a<N1, N2, SIGN>(u, n2, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) b[lb * L::PS + k1 * L::LS + n2] = u[k1];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 16 * nb; i += blockDim.x) {
+    const int lb = i >> 4, k1 = i & 15;
+    if (k1 >= N1) continue;
+    double2 w[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) w[n2] = b[lb * L::PS + k1 * L::LS + n2];
+    RDft<N2, SIGN>::run(w);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) a[lb * ld + k1 + N1 * k2] = w[k2];
+  }
+  __syncthreads();
+}
+
+template <int N1, int N2>
 __global__ void __launch_bounds__(OA_NTHREADS)
 k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, int nz,
             OaFftPlan pz, const double2* __restrict__ twz,
@@ -241,10 +276,12 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
             double* __restrict__ part) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ldz = nz + 1;
+  constexpr bool TP = N1 > 0;  // two-pass compile-time transforms
+  const int ldb = TP ? (ZLd<N1, N2>::PS > ldz ? ZLd<N1, N2>::PS : ldz) : ldz;
   double2* tw = (double2*)smem_raw;
   double2* a = tw + align_up_r(nz, 2);
   double2* b = a + OA_LB * ldz;
-  double2* pxy = b + OA_LB * ldz;  // [OA_LB][natm], atoms in type order
+  double2* pxy = b + OA_LB * ldb;  // [OA_LB][natm], atoms in type order
   __shared__ double sh[3 * 32];
   const int l0 = blockIdx.x * OA_LB;
   const int nb = min(OA_LB, nlines_d - l0);
@@ -267,7 +304,13 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
     if (lb < nb) a[lb * ldz + zz] = dz[(size_t)zz * ldl_d + l0 + lb];
   }
   __syncthreads();
-  double2* r = fft_pingpong<-1>(a, b, ldz, nb, pz, tw);
+  double2* r;
+  if constexpr (TP) {
+    zfft2<N1, N2, -1>(a, b, ldz, nb, tw);
+    r = a;
+  } else {
+    r = fft_pingpong<-1>(a, b, ldz, nb, pz, tw);
+  }
   const double pi = 3.14159265358979323846;
   const double fpi = 4.0 * pi;
   double acc[3] = {0.0, 0.0, 0.0};
@@ -326,8 +369,14 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
     r[lb * ldz + zz] = out;
   }
   __syncthreads();
-  double2* other = (r == a) ? b : a;
-  double2* r2 = fft_pingpong<+1>(r, other, ldz, nb, pz, tw);
+  double2* r2;
+  if constexpr (TP) {
+    zfft2<N1, N2, +1>(a, b, ldz, nb, tw);
+    r2 = a;
+  } else {
+    double2* other = (r == a) ? b : a;
+    r2 = fft_pingpong<+1>(r, other, ldz, nb, pz, tw);
+  }
   for (int idx = threadIdx.x; idx < nz * OA_LB; idx += blockDim.x) {
     const int zz = idx / OA_LB, lb = idx - zz * OA_LB;
     if (lb < nb) dz[(size_t)zz * ldl_d + l0 + lb] = r2[lb * ldz + zz];
@@ -397,21 +446,34 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) return e;
-  const size_t smz = (align_up_r(c->nz, 2) + 2 * (size_t)OA_LB * (c->nz + 1) + (size_t)OA_LB * c->natm) *
-                     sizeof(double2);
-  if (smz > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
   RhoTypeOff toff;
   for (int t = 0; t < 5; ++t) toff.off[t] = c->type_off[t];
-  e = cudaFuncSetAttribute(k_rho_zpass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
-  if (e != cudaSuccess) return e;
   const int nbz = oa_rho_z_nblk(c);
-  k_rho_zpass<<<nbz, OA_NTHREADS, smz, s>>>((double2*)c->dz, c->ldl_d, c->nlines_d, c->nx, c->ny, c->nz,
-                                            c->plan_z, c->tw_z, tpi_l, c->vol, c->ecut_rho,
-                                            4.0 * c->alp_ewd * c->alp_ewd, c->gzvps_sum / c->vol,
-                                            c->natm, c->ntype, c->atm_perm, toff, c->q_type, c->phase, c->kmax_tab,
-                                            c->spl, c->nspl, c->spl_gmin, c->spl_dg,
-                                            c->red + 3 * oa_rho_xc_nblk());
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  auto zpass = [&](auto kern, int ldb) -> cudaError_t {
+    const size_t smz =
+        (align_up_r(c->nz, 2) + (size_t)OA_LB * (c->nz + 1) + (size_t)OA_LB * ldb + (size_t)OA_LB * c->natm) *
+        sizeof(double2);
+    if (smz > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
+    cudaError_t e2 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
+    if (e2 != cudaSuccess) return e2;
+    kern<<<nbz, OA_NTHREADS, smz, s>>>((double2*)c->dz, c->ldl_d, c->nlines_d, c->nx, c->ny, c->nz,
+                                       c->plan_z, c->tw_z, tpi_l, c->vol, c->ecut_rho,
+                                       4.0 * c->alp_ewd * c->alp_ewd, c->gzvps_sum / c->vol,
+                                       c->natm, c->ntype, c->atm_perm, toff, c->q_type, c->phase, c->kmax_tab,
+                                       c->spl, c->nspl, c->spl_gmin, c->spl_dg,
+                                       c->red + 3 * oa_rho_xc_nblk());
+    return cudaGetLastError();
+  };
+  auto ldb2 = [&](int n1, int n2) { const int p = (n1 * (n2 | 1)) | 1; return p > c->nz + 1 ? p : c->nz + 1; };
+  switch (c->nz) {
+#define OA_ZP(NN, A, B) case NN: e = zpass(k_rho_zpass<A, B>, ldb2(A, B)); break;
+    OA_ZP(12, 4, 3) OA_ZP(20, 4, 5) OA_ZP(24, 6, 4) OA_ZP(36, 6, 6) OA_ZP(40, 8, 5) OA_ZP(64, 8, 8)
+    OA_ZP(96, 12, 8) OA_ZP(108, 12, 9) OA_ZP(160, 16, 10)
+#undef OA_ZP
+    default: e = cudaErrorNotSupported; break;
+  }
+  if (e == cudaErrorNotSupported) e = zpass(k_rho_zpass<0, 0>, c->nz + 1);
+  if (e != cudaSuccess) return e;
   if (two_pass) {
     e = oa_rho2_bwd(s, c->nx, c->nz, (const double2*)c->dz, c->ldl_d, c->tw_x, c->vxc, c->vks,
                     c->precision == OA_FP64);

@@ -279,28 +279,36 @@ k_tfwd(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorM
   if (warp == 0) tg_tmem_dealloc(tmem, ncols);
 }
 
+// C = alpha sum_kb part[kb]: block of 256 threads = 16 outputs x 16 K-block
+// groups; group g sums kb = g, g + 16, ... (all loads issued together),
+// then the 16 group sums are added in a fixed order
 __global__ void __launch_bounds__(256)
 k_tfwd_reduce(const float* __restrict__ part, int nkb, size_t nn, double alpha, double* __restrict__ C,
               const int* __restrict__ cond) {
   if (cond && *cond == 0) return;
-  __shared__ double ss[4][64];
-  const int col = threadIdx.x & 63, g = threadIdx.x >> 6;
-  const size_t i = (size_t)blockIdx.x * 64 + col;
+  __shared__ double ss[16][17];
+  const int col = threadIdx.x & 15, g = threadIdx.x >> 4;
+  const size_t i = (size_t)blockIdx.x * 16 + col;
   double s = 0.0;
   if (i < nn) {
     int k = g;
-    for (; k + 12 < nkb; k += 16) {
+    for (; k + 48 < nkb; k += 64) {
       const float a = __ldcs(part + (size_t)k * nn + i);
-      const float b = __ldcs(part + (size_t)(k + 4) * nn + i);
-      const float c = __ldcs(part + (size_t)(k + 8) * nn + i);
-      const float d = __ldcs(part + (size_t)(k + 12) * nn + i);
+      const float b = __ldcs(part + (size_t)(k + 16) * nn + i);
+      const float c = __ldcs(part + (size_t)(k + 32) * nn + i);
+      const float d = __ldcs(part + (size_t)(k + 48) * nn + i);
       s += (double)a; s += (double)b; s += (double)c; s += (double)d;
     }
-    for (; k < nkb; k += 4) s += (double)__ldcs(part + (size_t)k * nn + i);
+    for (; k < nkb; k += 16) s += (double)__ldcs(part + (size_t)k * nn + i);
   }
   ss[g][col] = s;
   __syncthreads();
-  if (g == 0 && i < nn) C[i] = alpha * (((ss[0][col] + ss[1][col]) + ss[2][col]) + ss[3][col]);
+  if (g == 0 && i < nn) {
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) t += ss[q][col];
+    C[i] = alpha * t;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -575,7 +583,7 @@ cudaError_t oa_tfwd(cudaStream_t s, int nt, const bf16* PA, int rows_a, const bf
 #undef OA_TF
   if (e != cudaSuccess) return e;
   const size_t mn = (size_t)m * n;
-  k_tfwd_reduce<<<(unsigned)((mn + 63) / 64), 256, 0, s>>>(part, nkb, mn, alpha, C, cond);
+  k_tfwd_reduce<<<(unsigned)((mn + 15) / 16), 256, 0, s>>>(part, nkb, mn, alpha, C, cond);
   return cudaGetLastError();
 }
 
