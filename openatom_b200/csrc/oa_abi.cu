@@ -367,7 +367,11 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
       const int mx = d->nstate > d->natm_nl ? d->nstate : d->natm_nl;
       p->pl_ld = (2L * d->ng + 63) / 64 * 64;
       p->pl_rows = oa_tg_rows_pad(mx, 128);
-      for (int q = 0; q < 3; ++q) TRY(cudaMalloc(&p->pl_big[q], (size_t)3 * p->pl_rows * p->pl_ld * 2));
+      for (int q = 0; q < 3; ++q) {
+        TRY(cudaMalloc(&p->pl_big[q], (size_t)3 * p->pl_rows * p->pl_ld * 2));
+        // padding rows and columns stay zero: every writer of a slot writes only its rows and columns
+        TRY(cudaMemset(p->pl_big[q], 0, (size_t)3 * p->pl_rows * p->pl_ld * 2));
+      }
       TRY(cudaMalloc(&p->pl_ma, (size_t)3 * p->pl_rows * p->pl_rows * 2));
       TRY(cudaMalloc(&p->pl_mb, (size_t)3 * p->pl_rows * p->pl_rows * 2));
     }
@@ -613,7 +617,8 @@ cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m
                          double w_kx0, double alpha, double* part, int nkb, double* C, const int* cond);
 cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
                             const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
-                            double* out, const int* cond, const double* yadd, double* out2, const int* cond2);
+                            double* out, const int* cond, const double* yadd, double* out2, const int* cond2,
+                            const OaPlaneOut* po = nullptr);
 
 #define OA_STEP_CHECK(x) do { const oa_status st_ = (x); if (st_ != OA_OK) return st_; } while (0)
 
@@ -719,10 +724,61 @@ static cudaError_t ensure_planes(oa_ctx* c, cudaStream_t s, int nt, int slot, co
   return e;
 }
 
-void oa_planes_reuse(oa_ctx* c, int on) {
+// Plane reuse inside a native step.  The keys say which FP64 source each
+// slot holds planes of; inside a step (pl_cache on) a slot whose key matches
+// is not split again.  The psi slot stays valid from step to step: psi
+// changes only in Psi T, which writes its planes in the same pass (or at the
+// start of a run, oa_planes_psi_refresh).  The other slots are forgotten at
+// both ends of a step (their sources change inside it, and a split gated by
+// the PsiV flag may not have run).
+void oa_planes_step_begin(oa_ctx* c) {
   oa_ctx_pc* p = pcx(c);
-  p->pl_cache = on;
-  for (int q = 0; q < 3; ++q) p->pl_key[q].valid = false;
+  p->pl_cache = 1;
+  for (int q = 0; q < 3; ++q)
+    if (q != PL_PSI) p->pl_key[q].valid = false;
+}
+void oa_planes_step_end(oa_ctx* c) {
+  oa_ctx_pc* p = pcx(c);
+  p->pl_cache = 0;
+  for (int q = 0; q < 3; ++q)
+    if (q != PL_PSI) p->pl_key[q].valid = false;
+}
+
+// slot as the target of a fused plane write of an [rows][2 ng] operand, with
+// the padded row count the GEMMs use for it
+static bool plane_out(oa_ctx* c, int slot, int rows, int nt, OaPlaneOut* po) {
+  oa_ctx_pc* p = pcx(c);
+  const int nb = oa_tg_nb(rows);
+  if (!p->pl_big[slot] || nb == 0 || !(nt == 2 || nt == 3)) return false;
+  const int rp = oa_tg_rows_pad(rows, nb);
+  if (rp > p->pl_rows || 2L * c->ng > p->pl_ld) return false;
+  *po = OaPlaneOut{p->pl_big[slot], rp, p->pl_ld, nt};
+  return true;
+}
+static void plane_mark(oa_ctx* c, int slot, const double* src, int rows, int rows_pad, int nt) {
+  auto& k = pcx(c)->pl_key[slot];
+  k.src = src; k.rows = rows; k.rows_pad = rows_pad; k.nt = nt; k.K = 2L * c->ng; k.kx0 = 0; k.w = 1.0;
+  k.valid = true;
+}
+
+// the next force z pass (oa_launch_state_zbwd) also writes the planes of F
+void oa_planes_force_begin(oa_ctx* c, int nt) {
+  OaPlaneOut po;
+  c->zb_po = plane_out(c, PL_OTHER, c->nstate, nt, &po) ? po : OaPlaneOut{nullptr, 0, 0, 0};
+}
+void oa_planes_force_end(oa_ctx* c, const double* F) {
+  if (c->zb_po.P && c->zb_po_done) plane_mark(c, PL_OTHER, F, c->nstate, c->zb_po.rows_pad, c->zb_po.nt);
+  c->zb_po = OaPlaneOut{nullptr, 0, 0, 0};
+  c->zb_po_done = 0;
+}
+
+// psi planes split afresh (start of a native run)
+oa_status oa_planes_psi_refresh(oa_ctx* c, cudaStream_t s, const double* psi, int nt) {
+  OaPlaneOut po;
+  if (!plane_out(c, PL_PSI, c->nstate, nt, &po)) return OA_OK;
+  OA_CUDA_TRY(oa_split_kc(s, nt, psi, c->nstate, po.rows_pad, 2L * c->ng, 2L * c->ng, 0, 1.0, (bf16*)po.P, po.ldp));
+  plane_mark(c, PL_PSI, psi, c->nstate, po.rows_pad, nt);
+  return OA_OK;
 }
 
 // Split-BF16 forward product through bf16 planes (oa_tgemm.cu); the
@@ -825,8 +881,11 @@ oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* 
                             double* Tout, int* flag, int nterm) {
   oa_ctx_pc* p = pcx(c);
   const int n = c->nstate;
+  OaPlaneOut po;
+  const bool fuse = nterm > 0 && plane_out(c, PL_PSI, n, nterm, &po);
   OA_ALIGN_TRY(oa_dgemm_bwd_ex(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, psi,
-                               nullptr, nullptr, psi_t, flag));
+                               nullptr, nullptr, psi_t, flag, fuse ? &po : nullptr));
+  if (fuse) plane_mark(c, PL_PSI, psi, n, po.rows_pad, nterm);
   OA_STEP_CHECK(psiv_velocity(c, s, psi, vpsi, flag, nterm));
   k_copy_cond<<<16, 256, 0, s>>>(Tout, p->eye, (size_t)n * n, flag);
   k_flag_clear<<<1, 1, 0, s>>>(flag);

@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(DB_THREADS, 2)
 k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double a1_kx0, double a1_rest,
             const double* __restrict__ M2, const double* __restrict__ X2, double a2, int nj, int nk, long ncol,
             long kx0_cols, double* out, const int* __restrict__ cond, const double* yadd, double* __restrict__ out2,
-            const int* __restrict__ cond2) {
+            const int* __restrict__ cond2, OaPlaneOut po) {
   if (cond && *cond == 0) return;
   const bool dual = out2 && *cond2 != 0;
   extern __shared__ __align__(16) double db_smem[];
@@ -361,6 +361,7 @@ k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double
         if (yadd) { const double2 y = *(const double2*)(yadd + o); v.x += y.x; v.y += y.y; }
         *(double2*)(out + o) = v;
         if (dual) *(double2*)(out2 + o) = v;
+        if (po.P) oa_plane_put2(po, j, c, v.x, v.y);
       } else if (c < ncol) {
         double v = acc[a][b][0];
         if (yadd) v += yadd[o];
@@ -373,9 +374,12 @@ k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double
 
 // Returns cudaErrorNotSupported when the shapes or pointers do not allow the
 // 16-byte copies (nj > 128, odd nj or ncol, unaligned pointers).
+// po (optional): bf16 planes of out written in the same pass (ncol even).
 cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
                             const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
-                            double* out, const int* cond, const double* yadd, double* out2, const int* cond2) {
+                            double* out, const int* cond, const double* yadd, double* out2, const int* cond2,
+                            const OaPlaneOut* po) {
+  const OaPlaneOut pz = po ? *po : OaPlaneOut{nullptr, 0, 0, 0};
   const uintptr_t al = (uintptr_t)M1 | (uintptr_t)X1 | (uintptr_t)out | (uintptr_t)(M2 ? M2 : M1) |
                        (uintptr_t)(X2 ? X2 : X1) | (uintptr_t)yadd | (uintptr_t)out2;
   if (out2 && !cond2) return cudaErrorInvalidValue;
@@ -387,12 +391,12 @@ cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, 
     e = cudaFuncSetAttribute(k_dgemm_bwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     k_dgemm_bwd<true><<<grid, DB_THREADS, sm, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out,
-                                                    cond, yadd, out2, cond2);
+                                                    cond, yadd, out2, cond2, pz);
   } else {
     e = cudaFuncSetAttribute(k_dgemm_bwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     k_dgemm_bwd<false><<<grid, DB_THREADS, sm, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols,
-                                                     out, cond, yadd, out2, cond2);
+                                                     out, cond, yadd, out2, cond2, pz);
   }
   return cudaGetLastError();
 }
@@ -401,5 +405,5 @@ cudaError_t oa_dgemm_bwd(cudaStream_t s, const double* M1, const double* X1, dou
                          const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
                          double* out, const int* cond) {
   return oa_dgemm_bwd_ex(s, M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out, cond, nullptr, nullptr,
-                         nullptr);
+                         nullptr, nullptr);
 }

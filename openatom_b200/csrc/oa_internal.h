@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "oa_fft.cuh"
+#include "oa_planes.cuh"
 #include "../../include/oa_gpu.h"
 
 #define OA_NTHREADS 256
@@ -83,6 +84,8 @@ struct oa_ctx {
   void *step;             // native-step scratch and captured graph (oa_step.cu)
   oa_ees *ees;            // EES nonlocal path, after oa_gpu_ees_init
   size_t smem_plane, smem_rho_plane;
+  OaPlaneOut zb_po;       // bf16 planes the next force z pass also writes (mixed native step), P = nullptr: none
+  int zb_po_done;         // the last force z pass wrote them
   int npair_d, ychunk_d;
 };
 

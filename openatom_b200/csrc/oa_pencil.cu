@@ -19,6 +19,7 @@
 //     GStateSlab::addForces (stateSlab.C:239) + CP_eke_calc (cp_eke.C:30)  -> k_zbwd2
 #include "oa_rdft.cuh"
 #include "oa_state_common.cuh"
+#include "oa_planes.cuh"
 
 // Smallest odd stride >= minv, congruent to want (odd) modulo 16 when want >= 0.
 __host__ __device__ constexpr int pencil_stride(int minv, int want) {
@@ -119,7 +120,8 @@ k_zbwd2(const typename CplxOf<R>::T* __restrict__ zbuf, int ldl, int nlines, con
         const int* __restrict__ line_off, const int* __restrict__ line_nneg, const int* __restrict__ line_npos,
         const double2* __restrict__ twz, const double2* __restrict__ psi, const double2* __restrict__ fnl,
         double2* __restrict__ force, const double* __restrict__ g2, const double* __restrict__ occ, int ng, int s0,
-        double scale, double ecut, double* __restrict__ eke_part, int nblk, const double2* __restrict__ dyp) {
+        double scale, double ecut, double* __restrict__ eke_part, int nblk, const double2* __restrict__ dyp,
+        OaPlaneOut po) {
   typedef typename CplxOf<R>::T C;
   constexpr int N = N1 * N2;
   typedef PencilLd<N1, N2> L;
@@ -184,6 +186,7 @@ k_zbwd2(const typename CplxOf<R>::T* __restrict__ zbuf, int ldl, int nlines, con
         f.x = 0.0; f.y = 0.0;
       }
       fs[idx] = f;
+      if (po.P) oa_plane_put2(po, s, 2L * idx, f.x, f.y);
     }
   }
   const double tot = block_sum(ek, sred);
@@ -552,14 +555,16 @@ template <typename R, int N1, int N2>
 static cudaError_t zbwd2_n(cudaStream_t st, const void* zbuf, int ldl, int nlines, const int* lkx, const int* off,
                            const int* nneg, const int* npos, const double2* tw, const double2* psi,
                            const double2* fnl, double2* force, const double* g2, const double* occ, int ng, int s0,
-                           int ns, double scale, double ecut, double* eke_part, int nblk, const double2* dyp) {
+                           int ns, double scale, double ecut, double* eke_part, int nblk, const double2* dyp,
+                           OaPlaneOut po) {
   typedef typename CplxOf<R>::T C;
   const size_t sm = zpass2_smem<R, N1, N2>();
   cudaError_t e = cudaFuncSetAttribute(k_zbwd2<R, N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   dim3 grid(nblk, ns);
   k_zbwd2<R, N1, N2><<<grid, OA_NTHREADS, sm, st>>>((const C*)zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl,
-                                                     force, g2, occ, ng, s0, scale, ecut, eke_part, nblk, dyp);
+                                                     force, g2, occ, ng, s0, scale, ecut, eke_part, nblk, dyp,
+                                                     po);
   return cudaGetLastError();
 }
 
@@ -567,10 +572,11 @@ template <typename R>
 static cudaError_t zbwd2(cudaStream_t st, int n, const void* zbuf, int ldl, int nlines, const int* lkx,
                          const int* off, const int* nneg, const int* npos, const double2* tw, const double2* psi,
                          const double2* fnl, double2* force, const double* g2, const double* occ, int ng, int s0,
-                         int ns, double scale, double ecut, double* eke_part, int nblk, const double2* dyp) {
+                         int ns, double scale, double ecut, double* eke_part, int nblk, const double2* dyp,
+                         OaPlaneOut po) {
 #define OA_CALL(A, B)                                                                                          \
   zbwd2_n<R, A, B>(st, zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl, force, g2, occ, ng, s0, ns, scale, \
-                   ecut, eke_part, nblk, dyp)
+                   ecut, eke_part, nblk, dyp, po)
   OA_PENCIL_DISPATCH(n, OA_CALL)
 #undef OA_CALL
   return cudaErrorNotSupported;
@@ -580,12 +586,12 @@ cudaError_t oa_pencil_zbwd(int precision, cudaStream_t st, int n, const void* zb
                            const int* lkx, const int* off, const int* nneg, const int* npos, const double2* tw,
                            const double2* psi, const double2* fnl, double2* force, const double* g2,
                            const double* occ, int ng, int s0, int ns, double scale, double ecut, double* eke_part,
-                           int nblk, const double2* dyp) {
+                           int nblk, const double2* dyp, OaPlaneOut po) {
   return precision == OA_FP64
              ? zbwd2<double>(st, n, zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl, force, g2, occ, ng, s0,
-                             ns, scale, ecut, eke_part, nblk, dyp)
+                             ns, scale, ecut, eke_part, nblk, dyp, po)
              : zbwd2<float>(st, n, zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl, force, g2, occ, ng, s0, ns,
-                            scale, ecut, eke_part, nblk, dyp);
+                            scale, ecut, eke_part, nblk, dyp, po);
 }
 
 template <typename R, int MODE, int N1, int N2>

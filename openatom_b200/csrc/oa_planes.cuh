@@ -1,0 +1,42 @@
+// bf16 "planes" of an FP64 matrix for the split-BF16 tensor-core GEMMs
+// (oa_tgemm.cu): x = P_0 + P_1 (+ P_2), P_0 = bf16(x), P_1 = bf16(x - P_0),
+// ..., stored row-major P[q][rows_pad][ldp].  Kernels that produce such a
+// matrix in FP64 can write its planes in the same pass (OaPlaneOut); the
+// digits are the ones k_split_kc computes.
+#pragma once
+#include <cuda_bf16.h>
+
+struct OaPlaneOut {
+  void* P;        // bf16 planes, nullptr = none
+  int rows_pad;   // rows per plane
+  long ldp;       // leading size (a multiple of 64)
+  int nt;         // planes: 2 or 3
+};
+
+// the nt bf16 digits of v (nt <= 3)
+__device__ __forceinline__ void oa_bf16_digits(double v, int nt, __nv_bfloat16* h) {
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    if (q >= nt) break;
+    const __nv_bfloat16 b = __float2bfloat16_rn((float)v);
+    h[q] = b;
+    v -= (double)__bfloat162float(b);
+  }
+}
+
+// planes of the pair (x, y) at row r, columns c and c + 1 (c even)
+__device__ __forceinline__ void oa_plane_put2(const OaPlaneOut& po, int r, long c, double x, double y) {
+  __nv_bfloat16 hx[3], hy[3];
+  oa_bf16_digits(x, po.nt, hx);
+  oa_bf16_digits(y, po.nt, hy);
+  __nv_bfloat16* base = (__nv_bfloat16*)po.P + (size_t)r * po.ldp + c;
+  const size_t pstride = (size_t)po.rows_pad * po.ldp;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    if (q >= po.nt) break;
+    __nv_bfloat162 v;
+    v.x = hx[q];
+    v.y = hy[q];
+    *reinterpret_cast<__nv_bfloat162*>(base + q * pstride) = v;
+  }
+}

@@ -362,7 +362,7 @@ cudaError_t oa_pencil_zbwd(int precision, cudaStream_t st, int n, const void* zb
                            const int* lkx, const int* off, const int* nneg, const int* npos, const double2* tw,
                            const double2* psi, const double2* fnl, double2* force, const double* g2,
                            const double* occ, int ng, int s0, int ns, double scale, double ecut, double* eke_part,
-                           int nblk, const double2* dyp);
+                           int nblk, const double2* dyp, OaPlaneOut po);
 cudaError_t oa_pair_plane(int mode, cudaStream_t st, int n, void* zbuf, int nstate, int nz, int ldl, int nlines,
                           const int* cols, int nkx, const double2* tw, const double* occ, const void* vks,
                           double* rho_part, int ngroup, void* psir);
@@ -472,10 +472,15 @@ cudaError_t oa_launch_state_plane_vks(oa_ctx* c, cudaStream_t s) {
 }
 cudaError_t oa_launch_state_zbwd(oa_ctx* c, cudaStream_t s, const double2* psi, const double2* fnl,
                                  double2* force, int s0, int ns) {
-  if (oa_pencil_supported(c->nz))
-    return oa_pencil_zbwd(c->precision, s, c->nz, c->zbuf, c->ldl, c->nlines, c->line_kx, c->line_off,
-                          c->line_nneg, c->line_npos, c->tw_z, psi, fnl, force, c->g2, c->occ, c->ng, s0, ns,
-                          -2.0 / (double)c->npts, c->ecut_psi, c->eke_part, c->nblk_z, nullptr);
+  c->zb_po_done = 0;
+  if (oa_pencil_supported(c->nz)) {
+    const cudaError_t e = oa_pencil_zbwd(c->precision, s, c->nz, c->zbuf, c->ldl, c->nlines, c->line_kx,
+                                         c->line_off, c->line_nneg, c->line_npos, c->tw_z, psi, fnl, force, c->g2,
+                                         c->occ, c->ng, s0, ns, -2.0 / (double)c->npts, c->ecut_psi, c->eke_part,
+                                         c->nblk_z, nullptr, c->zb_po);
+    c->zb_po_done = (e == cudaSuccess && c->zb_po.P) ? 1 : 0;
+    return e;
+  }
   return c->precision == OA_FP64 ? launch_zbwd<double>(c, s, psi, fnl, force, s0, ns)
                                  : launch_zbwd<float>(c, s, psi, fnl, force, s0, ns);
 }
@@ -538,7 +543,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
   if (pz)
     return oa_pencil_zbwd(c->precision, st, e->nc, e->zbuf, c->ldl, c->nlines, c->line_kx, c->line_off,
                           c->line_nneg, c->line_npos, e->tw_c, psi, nullptr, fnl, c->g2, c->occ, c->ng, 0, c->nstate,
-                          1.0, c->ecut_psi, c->eke_part, c->nblk_z, e->dyp);
+                          1.0, c->ecut_psi, c->eke_part, c->nblk_z, e->dyp, OaPlaneOut{nullptr, 0, 0, 0});
   {
     size_t sm = zpass_smem<R>(e->nc);
     err = cudaFuncSetAttribute(k_state_zbwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

@@ -140,27 +140,26 @@ void oa_step_free(oa_ctx* c) {
 
 #define OA_STEP_TRY(x) do { oa_status st_ = (x); if (st_ != OA_OK) return st_; } while (0)
 
-// Launches of one step up to S (part A); no host synchronisation.
-void oa_planes_reuse(oa_ctx* c, int on);
+void oa_planes_step_begin(oa_ctx* c);
+void oa_planes_step_end(oa_ctx* c);
+void oa_planes_force_begin(oa_ctx* c, int nt);
+void oa_planes_force_end(oa_ctx* c, const double* F);
+oa_status oa_planes_psi_refresh(oa_ctx* c, cudaStream_t s, const double* psi, int nt);
 
-// force phase with bf16-plane reuse: psi, the structure factor and F are
-// each split once (psi and F do not change until the step ends)
-static oa_status launch_step_a_body(oa_ctx* c, cudaStream_t s, oa_cp_state* st, int complete_prev);
+// Launches of one step up to S (part A); no host synchronisation.  In the
+// mixed form the bf16 planes of psi come from the previous step's Psi T and
+// those of F from the force z pass; the structure factor is split once.
 static oa_status launch_step_a(oa_ctx* c, cudaStream_t s, oa_cp_state* st, int complete_prev) {
-  oa_planes_reuse(c, 1);
-  const oa_status r = launch_step_a_body(c, s, st, complete_prev);
-  oa_planes_reuse(c, 0);
-  return r;
-}
-
-static oa_status launch_step_a_body(oa_ctx* c, cudaStream_t s, oa_cp_state* st, int complete_prev) {
   oa_step_scratch* w = step_scratch(c);
   const int nt = st->mixed_nterm;
   // forces on the orthonormal psi (computePsiFandVKS, ParticlePlane, combineForcesGetEke)
   OA_STEP_TRY(oa_gpu_state_fft_fwd(c, s, st->psi, nullptr));
   OA_STEP_TRY(oa_gpu_vks_build(c, s, nullptr));
   OA_STEP_TRY(oa_gpu_nl_sf(c, s, st->psi, nt, w->Fnl, nullptr));
-  OA_STEP_TRY(oa_gpu_vks_apply_fft_bwd(c, s, st->psi, 0, w->Fnl, w->F, nullptr));
+  if (nt) oa_planes_force_begin(c, nt);
+  const oa_status rf = oa_gpu_vks_apply_fft_bwd(c, s, st->psi, 0, w->Fnl, w->F, nullptr);
+  oa_planes_force_end(c, w->F);
+  OA_STEP_TRY(rf);
   // constraint force (computeLambdaAndCg): Lambda, Gamma = T Lambda, F' = F T - Psi Gamma
   if (nt) {
     OA_STEP_TRY(oa_gpu_pc_forward_mixed(c, s, st->psi, w->F, 1.0, 1.0, nt, w->lam));
@@ -218,6 +217,8 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
   oa_step_scratch* w = step_scratch(c);
   // restart the PsiV flag, the record count and the error slot
   OA_CUDA_TRY(cudaMemsetAsync(w->flag, 0, 4 * sizeof(int), s));
+  // the psi planes of the mixed products, from the psi the caller hands in
+  if (st->mixed_nterm) OA_STEP_TRY(oa_planes_psi_refresh(c, s, st->psi, st->mixed_nterm));
   const void* key[7] = {st->psi, st->psi_t, st->vpsi, st->T, stream, w->ring, nullptr};
   // the legacy default stream cannot be captured: launch eagerly there
   const bool capturable = s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread;
@@ -242,6 +243,7 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
           cudaGraph_t g = nullptr;
           OA_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
           oa_status r = OA_OK;
+          if (part == 0) oa_planes_step_begin(c);
           if (ns_in_graph) {
             r = launch_step_a(c, s, st, 1);
             if (r == OA_OK) r = launch_step_ns(c, s, st);
@@ -249,6 +251,7 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
           } else {
             r = part == 0 ? launch_step_a(c, s, st, 1) : launch_step_b(c, s, st);
           }
+          if (ns_in_graph || part == 1 || r != OA_OK) oa_planes_step_end(c);
           cudaError_t ce = cudaStreamEndCapture(s, &g);
           if (r != OA_OK) { if (g) cudaGraphDestroy(g); return r; }
           if (ce != cudaSuccess) { oa_set_error(cudaGetErrorString(ce), __FILE__, __LINE__); return OA_ERR_CUDA; }
@@ -279,9 +282,12 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
         OA_CUDA_TRY(cudaGraphLaunch(w->exec2, s));
       }
     } else {
-      OA_STEP_TRY(launch_step_a(c, s, st, complete_prev));
-      OA_STEP_TRY(launch_step_ns(c, s, st));
-      OA_STEP_TRY(launch_step_b(c, s, st));
+      oa_planes_step_begin(c);
+      oa_status r = launch_step_a(c, s, st, complete_prev);
+      if (r == OA_OK) r = launch_step_ns(c, s, st);
+      if (r == OA_OK) r = launch_step_b(c, s, st);
+      oa_planes_step_end(c);
+      OA_STEP_TRY(r);
     }
   }
   OA_CUDA_TRY(cudaMemcpyAsync(w->ring_host, w->ring, (size_t)nsteps * OA_REC * sizeof(double),
