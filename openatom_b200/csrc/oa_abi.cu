@@ -60,7 +60,8 @@ cudaError_t oa_launch_pc_bwd_jk(cudaStream_t s, const double* M1, const double* 
                                 long kx0_cols, double* out);
 cudaError_t oa_launch_nl_sf(cudaStream_t s, const int* kx, const int* ky, const int* kz, int ng, const int* nl_atm,
                             int natm_nl, const int* atm_type, const double2* phase, int ktab, const double* spl,
-                            int nspl, double gmin, double dg, const double* gz0, double tpi_l, double2* sf);
+                            int nspl, double gmin, double dg, const double* gz0, double tpi_l, double2* sf,
+                            const OaPlaneOut* po);
 cudaError_t oa_launch_nl_zscale(cudaStream_t s, const double* Z, int nstate, int natm_nl, const int* nl_atm,
                                 const int* atm_type, const double* vnorm, double rvol, const double* occ, double* zt,
                                 double* enl);
@@ -820,7 +821,14 @@ static cudaError_t mixed_bwd(oa_ctx* c, cudaStream_t s, int nt, const double* M1
                              const int* cond = nullptr) {
   oa_ctx_pc* p = pcx(c);
   const int mx = c->nstate > c->natm_nl ? c->nstate : c->natm_nl;
-  const int nkp = oa_tg_rows_pad(nk, 32);
+  int nkp = oa_tg_rows_pad(nk, 32);
+  {
+    // planes of X1 already held with more zero rows (a multiple of 32) serve as they are
+    const auto& k = p->pl_key[s1];
+    if (p->pl_cache && k.valid && k.src == X1 && k.rows == nk && k.nt == nt && k.K == ncol && k.kx0 == 0 &&
+        k.rows_pad > nkp && k.rows_pad % 32 == 0 && k.rows_pad <= p->pl_rows)
+      nkp = k.rows_pad;
+  }
   const int ldm = oa_tg_nb(nj);  // M planes: leading size of the N tile, zero beyond nj
   if (nj <= mx && nk <= mx && ncol <= p->pl_ld && ldm != 0 && nkp <= p->pl_rows && (!M2 || s1 != s2)) {
     bf16 *pm1 = (bf16*)p->pl_ma, *pm2 = (bf16*)p->pl_mb;
@@ -963,9 +971,15 @@ extern "C" oa_status oa_gpu_nl_sf(oa_ctx* c, void* stream, const double* psi, in
     return OA_OK;
   }
   const double tpi_l = 2.0 * M_PI / c->box;
-  OA_CUDA_TRY(oa_launch_phase_tables(c, s));
+  // inside a native step the phase tables are this step's (vks_build made
+  // them from the same positions), and the SF kernel also writes its planes
+  if (!p->pl_cache) OA_CUDA_TRY(oa_launch_phase_tables(c, s));
+  OaPlaneOut po;
+  const bool fuse = nterm > 0 && p->pl_cache && plane_out(c, PL_SF, na, nterm, &po);
   OA_CUDA_TRY(oa_launch_nl_sf(s, c->kx, c->ky, c->kz, c->ng, c->nl_atm, na, c->atm_type, c->phase, c->kmax_tab,
-                              c->nl_spl, c->nspl, c->spl_gmin, c->spl_dg, c->nl_gz0, tpi_l, c->sf));
+                              c->nl_spl, c->nspl, c->spl_gmin, c->spl_dg, c->nl_gz0, tpi_l, c->sf,
+                              fuse ? &po : nullptr));
+  if (fuse) plane_mark(c, PL_SF, (const double*)c->sf, na, po.rows_pad, nterm);
   const long K = 2L * c->ng;
   if (nterm == 0)
     OA_CUDA_TRY(oa_launch_pc_fwd_mn(s, psi, (const double*)c->sf, n, na, K, 0, 1.0, 1.0, p->part, p->nkb, c->zmat));

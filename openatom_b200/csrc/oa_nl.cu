@@ -10,14 +10,15 @@
 //
 // SF[a][g] = w_g p_t(|g|) y00 conj(exp(i g.R_a)) is built in FP64 from the
 // per-axis phase tables exp(i 2 pi k x_a / L) (the reference's incremental
-// e^{i g.R} recursion becomes one product of three table entries).
+// e^{i g.R} recursion becomes one product of three table entries).  In the
+// mixed form the kernel also writes the bf16 planes of SF (oa_planes.cuh).
 #include "oa_internal.h"
 
 __global__ void k_nl_sf(const int* __restrict__ kx, const int* __restrict__ ky, const int* __restrict__ kz, int ng,
                         const int* __restrict__ nl_atm, int natm_nl, const int* __restrict__ atm_type,
                         const double2* __restrict__ phase, int ktab, const double* __restrict__ spl, int nspl,
                         double gmin, double dg, const double* __restrict__ gz0, double tpi_l,
-                        double2* __restrict__ sf) {
+                        double2* __restrict__ sf, OaPlaneOut po) {
   const int a = blockIdx.y;
   const int at = nl_atm[a];
   const int t = atm_type[at];
@@ -42,6 +43,7 @@ __global__ void k_nl_sf(const int* __restrict__ kx, const int* __restrict__ ky, 
     const double2 h = cmul(cmul(ph[x + ktab], ph[nt + y + ktab]), ph[2 * nt + z + ktab]);
     const double s = w * p * y00;
     sf[(size_t)a * ng + i] = make_double2(h.x * s, -h.y * s);
+    if (po.P) oa_plane_put2(po, a, 2L * i, h.x * s, -h.y * s);
   }
 }
 
@@ -64,11 +66,12 @@ __global__ void k_nl_zscale(const double* __restrict__ Z, int nstate, int natm_n
 
 cudaError_t oa_launch_nl_sf(cudaStream_t s, const int* kx, const int* ky, const int* kz, int ng, const int* nl_atm,
                             int natm_nl, const int* atm_type, const double2* phase, int ktab, const double* spl,
-                            int nspl, double gmin, double dg, const double* gz0, double tpi_l, double2* sf) {
+                            int nspl, double gmin, double dg, const double* gz0, double tpi_l, double2* sf,
+                            const OaPlaneOut* po) {
   if (natm_nl == 0) return cudaSuccess;
   dim3 grid((ng + 255) / 256 < 64 ? (ng + 255) / 256 : 64, natm_nl);
   k_nl_sf<<<grid, 256, 0, s>>>(kx, ky, kz, ng, nl_atm, natm_nl, atm_type, phase, ktab, spl, nspl, gmin, dg, gz0,
-                               tpi_l, sf);
+                               tpi_l, sf, po ? *po : OaPlaneOut{nullptr, 0, 0, 0});
   return cudaGetLastError();
 }
 
