@@ -72,8 +72,18 @@ k_dgemm_fwd(const double* __restrict__ A, const double* __restrict__ B, int m, i
   const long rslabs = (rend - rbeg + DG_KS - 1) / DG_KS;
   const int nslab = rslabs > first ? (int)((rslabs - first + stride - 1) / stride) : 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wi = (warp >> 2) * 32, wj = (warp & 3) * 32;
-  const bool active = (i0 + wi < m) && (j0 + wj < n);
+  // A == B (the overlap, one diagonal tile): the 32 x 32 blocks below the
+  // diagonal are the transposes of those above, which the reduction mirrors.
+  // The ten blocks on and above it go to warps 0-9, so that each SM
+  // sub-partition (warp mod 4) issues the DMMAs of at most three.
+  int wi = (warp >> 2) * 32, wj = (warp & 3) * 32;
+  if (SAME) {
+    // 4 bi + bj of the upper blocks 0, 1, 2, 3, 5, 6, 7, 10, 11, 15, one hex digit per warp
+    const int u = warp < 10 ? (int)((0xFBA7653210ull >> (4 * warp)) & 15u) : 0;
+    wi = (u >> 2) * 32;
+    wj = (u & 3) * 32;
+  }
+  const bool active = (i0 + wi < m) && (j0 + wj < n) && (!SAME || warp < 10);
   double acc[4][4][2];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
@@ -142,23 +152,30 @@ k_dgemm_fwd(const double* __restrict__ A, const double* __restrict__ B, int m, i
 #define DR_GROUPS 4
 __global__ void __launch_bounds__(DR_COLS * DR_GROUPS)
 k_dgemm_fwd_reduce(const double* __restrict__ part, int n0, int nkb, size_t nn, double w0, double alpha,
-                   double* __restrict__ C, const int* __restrict__ cond) {
+                   double* __restrict__ C, const int* __restrict__ cond, int sym_n) {
   if (cond && *cond == 0) return;
   __shared__ double s0s[DR_GROUPS][DR_COLS], s1s[DR_GROUPS][DR_COLS];
   const int col = threadIdx.x % DR_COLS, g = threadIdx.x / DR_COLS;
   const size_t i = (size_t)blockIdx.x * DR_COLS + col;
+  // sym_n > 0: symmetric n x n result whose partials hold only the 32 x 32
+  // blocks on and above the diagonal; (r, c) below reads (c, r)
+  size_t src = i;
+  if (sym_n > 0 && i < nn) {
+    const int r = (int)(i / sym_n), c = (int)(i - (size_t)r * sym_n);
+    if ((r >> 5) > (c >> 5)) src = (size_t)c * sym_n + r;
+  }
   double s0 = 0.0, s1 = 0.0;
   if (i < nn) {
-    for (int k = g; k < n0; k += DR_GROUPS) s0 += __ldcs(part + (size_t)k * nn + i);
+    for (int k = g; k < n0; k += DR_GROUPS) s0 += __ldcs(part + (size_t)k * nn + src);
     int k = n0 + g;
     for (; k + 3 * DR_GROUPS < nkb; k += 4 * DR_GROUPS) {
-      const double a = __ldcs(part + (size_t)k * nn + i);
-      const double b = __ldcs(part + (size_t)(k + DR_GROUPS) * nn + i);
-      const double c = __ldcs(part + (size_t)(k + 2 * DR_GROUPS) * nn + i);
-      const double d = __ldcs(part + (size_t)(k + 3 * DR_GROUPS) * nn + i);
+      const double a = __ldcs(part + (size_t)k * nn + src);
+      const double b = __ldcs(part + (size_t)(k + DR_GROUPS) * nn + src);
+      const double c = __ldcs(part + (size_t)(k + 2 * DR_GROUPS) * nn + src);
+      const double d = __ldcs(part + (size_t)(k + 3 * DR_GROUPS) * nn + src);
       s1 += a; s1 += b; s1 += c; s1 += d;
     }
-    for (; k < nkb; k += DR_GROUPS) s1 += __ldcs(part + (size_t)k * nn + i);
+    for (; k < nkb; k += DR_GROUPS) s1 += __ldcs(part + (size_t)k * nn + src);
   }
   s0s[g][col] = s0;
   s1s[g][col] = s1;
@@ -225,8 +242,8 @@ cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const size_t mn = (size_t)m * n;
-  k_dgemm_fwd_reduce<<<(unsigned)((mn + DR_COLS - 1) / DR_COLS), DR_COLS * DR_GROUPS, 0, s>>>(part, n0, nkb_eff, mn,
-                                                                                               w_kx0, alpha, C, cond);
+  k_dgemm_fwd_reduce<<<(unsigned)((mn + DR_COLS - 1) / DR_COLS), DR_COLS * DR_GROUPS, 0, s>>>(
+      part, n0, nkb_eff, mn, w_kx0, alpha, C, cond, same ? n : 0);
   return cudaGetLastError();
 }
 
