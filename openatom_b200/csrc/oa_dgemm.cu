@@ -378,13 +378,47 @@ k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double
         if (yadd) { const double2 y = *(const double2*)(yadd + o); v.x += y.x; v.y += y.y; }
         *(double2*)(out + o) = v;
         if (dual) *(double2*)(out2 + o) = v;
-        if (po.P) oa_plane_put2(po, j, c, v.x, v.y);
       } else if (c < ncol) {
         double v = acc[a][b][0];
         if (yadd) v += yadd[o];
         out[o] = v;
         if (dual) out2[o] = v;
       }
+    }
+  }
+  if (po.P) {
+    // bf16 planes of the tile staged in the (now idle) slab ring, then
+    // written as whole 16-byte pieces of 128-byte rows
+    constexpr int SPLD = DB_TC + 8;
+    __nv_bfloat16* sp = reinterpret_cast<__nv_bfloat16*>(db_smem);
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int jl = wj + a * 8 + (lane >> 2);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int cl = wc + b * 8 + 2 * (lane & 3);
+        __nv_bfloat16 hx[3], hy[3];
+        oa_bf16_digits(acc[a][b][0], po.nt, hx);
+        oa_bf16_digits(acc[a][b][1], po.nt, hy);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          if (q >= po.nt) break;
+          __nv_bfloat162 v2;
+          v2.x = hx[q];
+          v2.y = hy[q];
+          *reinterpret_cast<__nv_bfloat162*>(sp + ((size_t)q * DB_TJ + jl) * SPLD + cl) = v2;
+        }
+      }
+    }
+    __syncthreads();
+    const size_t pstride = (size_t)po.rows_pad * po.ldp;
+    for (int i = threadIdx.x; i < po.nt * DB_TJ * (DB_TC / 8); i += DB_THREADS) {
+      const int q = i / (DB_TJ * (DB_TC / 8)), rem = i - q * (DB_TJ * (DB_TC / 8));
+      const int jl = rem / (DB_TC / 8), ch = rem - jl * (DB_TC / 8);
+      if (jl >= nj || c0 + ch * 8 >= po.ldp) continue;
+      *reinterpret_cast<uint4*>((__nv_bfloat16*)po.P + q * pstride + (size_t)jl * po.ldp + c0 + ch * 8) =
+          *reinterpret_cast<const uint4*>(sp + ((size_t)q * DB_TJ + jl) * SPLD + ch * 8);
     }
   }
 }
@@ -397,6 +431,8 @@ cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, 
                             double* out, const int* cond, const double* yadd, double* out2, const int* cond2,
                             const OaPlaneOut* po) {
   const OaPlaneOut pz = po ? *po : OaPlaneOut{nullptr, 0, 0, 0};
+  // plane tiles are whole 64-column pieces inside the plane rows
+  if (pz.P && ((pz.ldp % DB_TC) || ncol > pz.ldp || nj > pz.rows_pad || pz.nt > 3)) return cudaErrorInvalidValue;
   const uintptr_t al = (uintptr_t)M1 | (uintptr_t)X1 | (uintptr_t)out | (uintptr_t)(M2 ? M2 : M1) |
                        (uintptr_t)(X2 ? X2 : X1) | (uintptr_t)yadd | (uintptr_t)out2;
   if (out2 && !cond2) return cudaErrorInvalidValue;
