@@ -273,13 +273,14 @@ def run_ours(args):
 
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
 # the plane kernels on the w32 workload, from one ncu capture
-# (profiles/k_plane2_w32.md); None for other workloads.
-TRAFFIC_W32 = {"state_plane_density": 793.9e6, "state_plane_vks": 725.9e6}
+# (profiles/k_pair_plane_w32.md); None for other workloads.
+TRAFFIC_W32 = {"state_plane_density": 755.4e6, "state_plane_vks": 747.1e6}
 
 
 def roofline(sysm, drv, kt, config=None):
-    """Roofline of the dominant kernel from its algorithmic bytes and its
-    CUDA-event time (see DESIGN.md for the per-kernel byte formulas)."""
+    """Roofline of the dominant kernel from its algorithmic bytes
+    (CPContext.algorithmic_bytes states the per-kernel formulas) and its
+    CUDA-event time."""
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:

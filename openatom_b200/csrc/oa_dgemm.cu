@@ -417,7 +417,7 @@ k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double
       const int q = i / (DB_TJ * (DB_TC / 8)), rem = i - q * (DB_TJ * (DB_TC / 8));
       const int jl = rem / (DB_TC / 8), ch = rem - jl * (DB_TC / 8);
       if (jl >= nj || c0 + ch * 8 >= po.ldp) continue;
-      *reinterpret_cast<uint4*>((__nv_bfloat16*)po.P + q * pstride + (size_t)jl * po.ldp + c0 + ch * 8) =
+      *reinterpret_cast<uint4*>((__nv_bfloat16*)po.P + q * pstride + oa_plane_at(jl, c0 + ch * 8, po.rows_pad)) =
           *reinterpret_cast<const uint4*>(sp + ((size_t)q * DB_TJ + jl) * SPLD + ch * 8);
     }
   }

@@ -2,9 +2,10 @@
 //
 // Operand format ("bf16 planes"): an FP64 matrix X [rows][K] becomes NT bf16
 // planes x = P_0 + P_1 (+ P_2), P_0 = bf16(x), P_1 = bf16(x - P_0), ...,
-// stored row-major P[q][rows_pad][ldp] (K padded with zeros to ldp, a
-// multiple of 64; rows padded with zero rows).  The kernels load 128-byte
-// rows (64 contiguous elements) with the TMA's 128-byte swizzle, which
+// stored in 64-column chunks P[q][ldp/64][rows_pad][64] (K padded with
+// zeros to ldp, a multiple of 64; rows padded with zero rows;
+// oa_planes.cuh).  Every TMA box is 64 columns (128 bytes) by a run of rows,
+// one contiguous piece of memory, loaded with the 128-byte swizzle, which
 // lands as the UMMA SWIZZLE_128B canonical layout for both uses of a plane:
 //   K-major view (forward GEMM, contiguous = K): box {64 k, R rows}
 //       -> R rows of 128 B; 8-row groups 1024 B apart (SBO); the four
@@ -84,12 +85,14 @@ __device__ __forceinline__ bool tg_wait(uint64_t* bar, uint32_t phase) {
   }
   return false;
 }
-// 3-D tile load of a tensor map box into shared memory, completing on bar
-__device__ __forceinline__ void tg_tma3(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar) {
+// box of 64 columns x the map's rows starting at (row, column chunk ch) of
+// plane q, into shared memory, completing on bar (4-D tile load)
+__device__ __forceinline__ void tg_tma_box(uint32_t dst, const CUtensorMap* map, int row, int ch, int q,
+                                           uint64_t* bar) {
   asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-      "[%5];"
-      :: "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(tg_s32(bar))
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];"
+      :: "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(row), "r"(ch), "r"(q), "r"(tg_s32(bar))
       : "memory");
 }
 __device__ __forceinline__ void tg_tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -115,21 +118,24 @@ __device__ __forceinline__ void tg_tmem_ld16(uint32_t taddr, float* v) {
 }
 
 // ---------------------------------------------------------------------------
-// FP64 [rows][K] (row stride ldx) -> planes P[q][rows_pad][ldp], columns
-// k < kx0_cols scaled by w_kx0 first; padding columns [K, ldp) and rows
-// [rows, rows_pad) zero.  One thread per 8 consecutive elements of a row.
+// FP64 [rows][K] (row stride ldx) -> planes P[q][ldp/64][rows_pad][64],
+// columns k < kx0_cols scaled by w_kx0 first; padding columns [K, ldp) and
+// rows [rows, rows_pad) zero.  One thread per 8 consecutive elements of a row.
 // ---------------------------------------------------------------------------
 template <int NT>
 __global__ void k_split_kc(const double* __restrict__ X, int rows, int rows_pad, long K, long ldx, long kx0_cols,
                            double w_kx0, bf16* __restrict__ P, long ldp, const int* __restrict__ cond) {
   if (cond && *cond == 0) return;
-  const long ng = ldp / 8;
-  const size_t total = (size_t)rows_pad * ng;
+  const size_t total = (size_t)rows_pad * (ldp / 8);
   const size_t pstride = (size_t)rows_pad * ldp;
   for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-    const int r = (int)(t / ng);
-    const long kg = (long)(t - (size_t)r * ng);
-    const long k0 = kg * 8;
+    // t -> (64-column chunk, row, 8-column piece), piece fastest: consecutive
+    // threads write consecutive 16-byte pieces of the chunked plane
+    const size_t per_chunk = (size_t)rows_pad * 8;
+    const long ch = (long)(t / per_chunk);
+    const int rem = (int)(t - (size_t)ch * per_chunk);
+    const int r = rem >> 3;
+    const long k0 = ch * 64 + (rem & 7) * 8;
     double x[8];
     const double* src = X + (size_t)r * ldx + k0;
     if (r >= rows) {
@@ -162,7 +168,7 @@ __global__ void k_split_kc(const double* __restrict__ X, int rows, int rows_pad,
     }
 #pragma unroll
     for (int q = 0; q < NT; ++q)
-      *reinterpret_cast<uint4*>(P + q * pstride + (size_t)r * ldp + k0) = *reinterpret_cast<uint4*>(&h[q][0]);
+      *reinterpret_cast<uint4*>(P + q * pstride + oa_plane_at(r, k0, rows_pad)) = *reinterpret_cast<uint4*>(&h[q][0]);
   }
 }
 
@@ -206,8 +212,8 @@ k_tfwd(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorM
       tg_expect_tx(&full[st], stage_bytes);
 #pragma unroll
       for (int q = 0; q < NT; ++q) {
-        tg_tma3(sb + q * a_bytes, &tA, k0, m0, q, &full[st]);
-        tg_tma3(sb + NT * a_bytes + q * b_bytes, &tB, k0, n0, q, &full[st]);
+        tg_tma_box(sb + q * a_bytes, &tA, m0, k0 / 64, q, &full[st]);
+        tg_tma_box(sb + NT * a_bytes + q * b_bytes, &tB, n0, k0 / 64, q, &full[st]);
       }
     };
     bool ok = true;
@@ -384,10 +390,10 @@ k_tbwd(const __grid_constant__ CUtensorMap tX1, const __grid_constant__ CUtensor
           // 64-wide MN chunks of 32 k rows, 4096 B each
 #pragma unroll
           for (int q = 0; q < NT; ++q) {
-            tg_tma3(sb + q * a_bytes, tx, c0, k0, q, &full[st]);
-            tg_tma3(sb + q * a_bytes + 4096, tx, c0 + 64, k0, q, &full[st]);
+            tg_tma_box(sb + q * a_bytes, tx, k0, c0 / 64, q, &full[st]);
+            tg_tma_box(sb + q * a_bytes + 4096, tx, k0, c0 / 64 + 1, q, &full[st]);
 #pragma unroll
-            for (int h = 0; h < NB / 64; ++h) tg_tma3(sb + NT * a_bytes + q * b_bytes + h * 4096, tm, h * 64, k0, q, &full[st]);
+            for (int h = 0; h < NB / 64; ++h) tg_tma_box(sb + NT * a_bytes + q * b_bytes + h * 4096, tm, k0, h, q, &full[st]);
           }
         }
       }
@@ -507,16 +513,16 @@ static EncodeTiledFn tg_encoder() {
   return fn;
 }
 
-// planes P[nt][rows][ldp] as a 3-D bf16 tensor {ldp, rows, nt}; box {64, br, 1}
-// (128-byte rows) with the 128-byte swizzle
+// planes P[nt][ldp/64][rows][64] as a 4-D bf16 tensor {64, rows, ldp/64, nt};
+// box {64, br, 1, 1} (128-byte rows, one contiguous piece) with the 128-byte swizzle
 static bool tg_map(CUtensorMap* map, const bf16* P, int nt, int rows, long ldp, int br) {
   EncodeTiledFn enc = tg_encoder();
   if (!enc || (((uintptr_t)P) & 15) || (ldp & 63) || br > 256) return false;
-  const cuuint64_t dims[3] = {(cuuint64_t)ldp, (cuuint64_t)rows, (cuuint64_t)nt};
-  const cuuint64_t strides[2] = {(cuuint64_t)ldp * 2, (cuuint64_t)rows * (cuuint64_t)ldp * 2};
-  const cuuint32_t box[3] = {64, (cuuint32_t)br, 1};
-  const cuuint32_t es[3] = {1, 1, 1};
-  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void*)P, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+  const cuuint64_t dims[4] = {64, (cuuint64_t)rows, (cuuint64_t)(ldp / 64), (cuuint64_t)nt};
+  const cuuint64_t strides[3] = {128, (cuuint64_t)rows * 128, (cuuint64_t)rows * (cuuint64_t)ldp * 2};
+  const cuuint32_t box[4] = {64, (cuuint32_t)br, 1, 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void*)P, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
          CUDA_SUCCESS;
 }
@@ -525,7 +531,7 @@ int oa_tgemm_available() { return tg_encoder() != nullptr; }
 
 cudaError_t oa_split_kc(cudaStream_t s, int nt, const double* X, int rows, int rows_pad, long K, long ldx,
                         long kx0_cols, double w_kx0, bf16* P, long ldp, const int* cond) {
-  if (rows_pad < rows || (ldp & 7)) return cudaErrorInvalidValue;
+  if (rows_pad < rows || (ldp & 63)) return cudaErrorInvalidValue;
   const size_t total = (size_t)rows_pad * (ldp / 8);
   const unsigned nblk = (unsigned)((total + 255) / 256 < 8 * 148 ? (total + 255) / 256 : 8 * 148);
   if (nt == 2) k_split_kc<2><<<nblk, 256, 0, s>>>(X, rows, rows_pad, K, ldx, kx0_cols, w_kx0, P, ldp, cond);

@@ -305,7 +305,9 @@ class CPContext:
         """Compulsory HBM bytes per launch of each kernel (inputs read once,
         outputs written once) -- the numerator of the roofline."""
         z = self.sizes()
-        n, ng, nl, nz, npts, g = z["nstate"], z["ng"], z["nlines"], z["nz"], z["npts"], z["ngroup"]
+        n, ng, nl, nz, npts = z["nstate"], z["ng"], z["nlines"], z["nz"], z["npts"]
+        # density partials: one per state group of the plane kernels (state pairs in the mixed form)
+        g = z["ngroup_pair"] if z["pair_planes"] else z["ngroup"]
         cb = 2 * z["rbytes"]
         zrow = n * nz * nl * cb          # the z-line buffer
         coef = n * ng * 16               # one coefficient array
