@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--quench", type=int, default=60)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--batch", type=int, default=48,
+                    help="systems of the batching form measured beside the headline (0: skip)")
     return ap.parse_args()
 
 
@@ -58,6 +60,61 @@ def dist_env():
 def make_sys(cfg, seed):
     from openatom_b200.system import make_system
     return make_system(cfg, seed=seed, ecut_mass=2.0, cmass0=400.0, dt=5.0)
+
+
+def batch_systems(seed, nsys):
+    """Seeded set of uneven water systems for the batching form: 8-32 H2O at
+    about 1 g/cc, 4 states per molecule (32-128), 60/70/80 Ry, each on the
+    smallest two-pass grid that holds its density sphere (4 kmax)."""
+    from openatom_b200.system import make_system
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(nsys):
+        nmol = int(rng.integers(8, 33))
+        ecut = float(rng.choice([60.0, 70.0, 80.0]))
+        box = 18.6 * (nmol / 32.0) ** (1.0 / 3.0)
+        kmax = int(math.floor(math.sqrt(ecut) / (2.0 * math.pi / box))) + 1
+        grid = next(g for g in (64, 96, 108, 160) if g >= 4 * kmax)
+        out.append(make_system("w32", seed=seed + 101 * i, nmol=nmol, box=box, ecut_ry=ecut,
+                               nfft=(grid, grid, grid), ecut_mass=2.0, cmass0=400.0, dt=5.0))
+    return out
+
+
+def batch_form(torch, args):
+    """Batching form: args.batch independent systems advanced together, one
+    CUDA graph per step (oa_gpu_cp_run_batch), against the same systems run
+    one after the other (oa_gpu_cp_run each)."""
+    from openatom_b200.gpu import CPDriver, run_batch
+    syss = batch_systems(args.seed + 7, args.batch)
+    drv = [CPDriver(s, "mixed") for s in syss]
+    for d in drv:
+        d.quench(3)
+    sts = [d.native_state(use_graph=True) for d in drv]
+    stream = torch.cuda.Stream()
+    run_batch(drv, sts, 3, stream)
+    k = max(args.steps // 2, 3)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    run_batch(drv, sts, k, stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms_batch = ev0.elapsed_time(ev1) / k
+    batch_kernels = sts[0].last_kernels
+    for d, st in zip(drv, sts):
+        d.run_native(st, 2)
+    ms_seq = 0.0
+    for d, st in zip(drv, sts):
+        ms, _ = time_steps(torch, d, st, k)
+        ms_seq += ms
+    n = len(drv)
+    out = {"systems": n, "states": [min(s.nstate for s in syss), max(s.nstate for s in syss)],
+           "grids": sorted({s.nfft[0] for s in syss}), "ecut_ry": sorted({s.ecut_ry for s in syss}),
+           "steps": k, "ms_per_batch_step": ms_batch, "system_steps_per_s": n * 1e3 / ms_batch,
+           "sequential_ms_per_batch_step": ms_seq, "speedup_vs_sequential": ms_seq / ms_batch,
+           "graph_kernels_per_step": batch_kernels, "precision": "mixed"}
+    del drv
+    return out
 
 
 class ClockSampler:
@@ -236,6 +293,8 @@ def run_ours(args):
         cpu = {"value": rate, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
                "sample": f"1 full CP step of the FP64 oracle on this workload ({dt:.1f} s, scipy FFT workers={os.cpu_count()})"}
 
+    batch = batch_form(torch, args) if (rk == 0 and args.batch > 0) else None
+
     if rk == 0:
         # kernel launches of one mixed step, counted in its captured CUDA graph
         launches_per_step = stmx.last_kernels if stmx.last_kernels > 0 else dmx.launches_per_step()
@@ -264,6 +323,7 @@ def run_ours(args):
             "sync_every_step": {"value": ws * 1e3 / ms_sync, "ms_per_step": ms_sync},
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(),
+            "batch": batch,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:

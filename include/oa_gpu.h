@@ -263,6 +263,20 @@ oa_status oa_gpu_cp_step(oa_ctx *ctx, void *stream, oa_cp_state *state, double *
 oa_status oa_gpu_cp_run(oa_ctx *ctx, void *stream, oa_cp_state *state, int nsteps, const double *pos_host,
                         double *energies_out);
 
+/* Batching form: nsys independent systems (replicas, PIMD beads, tempering
+ * systems; any sizes, one context and one state each) advanced nsteps CP
+ * steps each.  After each system's first step, one step of all systems is
+ * one CUDA graph: the systems' launches fork from `stream` (a created
+ * stream, not the legacy default) onto one stream per system and join
+ * back.  Results are those of oa_gpu_cp_run on each system alone.  The
+ * reference runs such sets as separate instances (UberCollection /
+ * InstanceController, main/InstanceController.C).  energies_out (optional,
+ * host [nsys][nsteps][11]).  Needs at most 128 states per system (the whole
+ * step captured); a Newton-Schulz failure names the first failing system
+ * and step. */
+oa_status oa_gpu_cp_run_batch(oa_ctx **ctxs, oa_cp_state **states, int nsys, void *stream, int nsteps,
+                              double *energies_out);
+
 /* Allocation-free PairCalculator forward product, for callers that cannot
  * call cudaMalloc (code running during CUDA stream capture, or inside a host
  * framework whose memory pool already holds the device memory).  Same

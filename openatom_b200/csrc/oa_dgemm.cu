@@ -36,6 +36,11 @@ __device__ __forceinline__ void dg_cp16(void* smem, const void* gmem, bool valid
   const int n = valid ? 16 : 0;  // src-size 0: the 16 bytes are zero-filled
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" :: "r"(s), "l"(gmem), "r"(n));
 }
+__device__ __forceinline__ void dg_cp8(void* smem, const void* gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" :: "r"(s), "l"(gmem), "r"(n));
+}
 __device__ __forceinline__ void dg_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N> __device__ __forceinline__ void dg_wait() { asm volatile("cp.async.wait_group %0;\n" :: "n"(N)); }
 
@@ -231,11 +236,11 @@ cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m
   dim3 grid(ti, tj, nkb_eff);
   cudaError_t e;
   if (same) {
-    e = cudaFuncSetAttribute(k_dgemm_fwd<true, DG_STAGES_SAME>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    e = oa_smem_limit(k_dgemm_fwd<true, DG_STAGES_SAME>);
     if (e != cudaSuccess) return e;
     k_dgemm_fwd<true, DG_STAGES_SAME><<<grid, DG_THREADS, sm, s>>>(A, B, m, n, K, kx0_cols, n0, nr, part, cond);
   } else {
-    e = cudaFuncSetAttribute(k_dgemm_fwd<false, DG_STAGES_TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    e = oa_smem_limit(k_dgemm_fwd<false, DG_STAGES_TWO>);
     if (e != cudaSuccess) return e;
     k_dgemm_fwd<false, DG_STAGES_TWO><<<grid, DG_THREADS, sm, s>>>(A, B, m, n, K, kx0_cols, n0, nr, part, cond);
   }
@@ -271,14 +276,26 @@ cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m
 __device__ __forceinline__ void db_load_slab(double* ms, double* xs, const double* __restrict__ M,
                                              const double* __restrict__ X, int nj, int nk, long ncol, int k0,
                                              long c0) {
-  // M rows k0..k0+15, all 128 j: 16 x 64 pieces of 16 B = 1024 -> 4 per thread
+  if (nj & 1) {
+    // odd nj: the rows of M are not 16-byte aligned; 8-byte pieces, 8 per thread
 #pragma unroll
-  for (int q = 0; q < (DB_KS * DB_TJ / 2) / DB_THREADS; ++q) {
-    const int piece = threadIdx.x + q * DB_THREADS;
-    const int kk = piece >> 6, jj = (piece & 63) * 2;
-    const int k = k0 + kk;
-    const bool valid = (k < nk) && (jj < nj);
-    dg_cp16(ms + kk * DB_LDM + jj, valid ? M + (size_t)k * nj + jj : M, valid);
+    for (int q = 0; q < (DB_KS * DB_TJ) / DB_THREADS; ++q) {
+      const int piece = threadIdx.x + q * DB_THREADS;
+      const int kk = piece >> 7, jj = piece & 127;
+      const int k = k0 + kk;
+      const bool valid = (k < nk) && (jj < nj);
+      dg_cp8(ms + kk * DB_LDM + jj, valid ? M + (size_t)k * nj + jj : M, valid);
+    }
+  } else {
+    // M rows k0..k0+15, all 128 j: 16 x 64 pieces of 16 B = 1024 -> 4 per thread
+#pragma unroll
+    for (int q = 0; q < (DB_KS * DB_TJ / 2) / DB_THREADS; ++q) {
+      const int piece = threadIdx.x + q * DB_THREADS;
+      const int kk = piece >> 6, jj = (piece & 63) * 2;
+      const int k = k0 + kk;
+      const bool valid = (k < nk) && (jj < nj);
+      dg_cp16(ms + kk * DB_LDM + jj, valid ? M + (size_t)k * nj + jj : M, valid);
+    }
   }
   // X rows k0..k0+15, columns c0..c0+63: 16 x 32 pieces = 512 -> 2 per thread
 #pragma unroll
@@ -424,7 +441,8 @@ k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double
 }
 
 // Returns cudaErrorNotSupported when the shapes or pointers do not allow the
-// 16-byte copies (nj > 128, odd nj or ncol, unaligned pointers).
+// copies (nj > 128, odd ncol, unaligned pointers); an odd nj moves M in
+// 8-byte pieces.
 // po (optional): bf16 planes of out written in the same pass (ncol even).
 cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
                             const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
@@ -436,17 +454,17 @@ cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, 
   const uintptr_t al = (uintptr_t)M1 | (uintptr_t)X1 | (uintptr_t)out | (uintptr_t)(M2 ? M2 : M1) |
                        (uintptr_t)(X2 ? X2 : X1) | (uintptr_t)yadd | (uintptr_t)out2;
   if (out2 && !cond2) return cudaErrorInvalidValue;
-  if (nj > DB_TJ || (nj & 1) || (ncol & 1) || (al & 15) || nk <= 0 || (M2 && !X2)) return cudaErrorNotSupported;
+  if (nj > DB_TJ || (ncol & 1) || (al & 15) || nk <= 0 || (M2 && !X2)) return cudaErrorNotSupported;
   const size_t sm = (size_t)DB_STAGES * (DB_MSLAB + DB_XSLAB) * sizeof(double);
   dim3 grid((unsigned)((ncol + DB_TC - 1) / DB_TC));
   cudaError_t e;
   if (M2) {
-    e = cudaFuncSetAttribute(k_dgemm_bwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    e = oa_smem_limit(k_dgemm_bwd<true>);
     if (e != cudaSuccess) return e;
     k_dgemm_bwd<true><<<grid, DB_THREADS, sm, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out,
                                                     cond, yadd, out2, cond2, pz);
   } else {
-    e = cudaFuncSetAttribute(k_dgemm_bwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    e = oa_smem_limit(k_dgemm_bwd<false>);
     if (e != cudaSuccess) return e;
     k_dgemm_bwd<false><<<grid, DB_THREADS, sm, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols,
                                                      out, cond, yadd, out2, cond2, pz);

@@ -11,6 +11,19 @@
 #define OA_LB 16          // z-lines per block in the z passes
 #define OA_MAX_SMEM (227 * 1024)
 
+// Raise a kernel's dynamic shared-memory limit to the most a block can have
+// beside its static shared memory.  The limit is a per-function setting that
+// all launches share (graphs holding systems of several sizes included), so
+// it is never lowered to one launch's need.
+template <typename K>
+static inline cudaError_t oa_smem_limit(K kernel) {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, (const void*)kernel);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(OA_MAX_SMEM - a.sharedSizeBytes));
+}
+
 // EES nonlocal path (nonlocal grid na x nb x nc, B-spline order)
 struct oa_ees {
   int na, nb, nc, order, ngroup;

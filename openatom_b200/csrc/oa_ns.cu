@@ -186,7 +186,7 @@ int oa_ns_cluster_size(int n) {
   for (int cs = 16; cs >= 8; cs /= 2) {
     const int R = (((n + cs - 1) / cs) + 7) & ~7;
     const size_t sm = ((size_t)R * (npad + 4) + (size_t)npad * (npad + 4)) * sizeof(double);
-    if (cudaFuncSetAttribute(k_ortho_ns_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+    if (oa_smem_limit(k_ortho_ns_cluster) != cudaSuccess)
       continue;
     if (cs > 8 && cudaFuncSetAttribute(k_ortho_ns_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
                       cudaSuccess) {
@@ -220,6 +220,10 @@ cudaError_t oa_launch_ortho_ns_cluster(cudaStream_t s, const double* S, int n, d
   at[0].val.clusterDim.x = cs; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
   cfg.gridDim = dim3(cs); cfg.blockDim = dim3(NSC_THREADS); cfg.dynamicSmemBytes = sm; cfg.stream = s;
   cfg.attrs = at; cfg.numAttrs = 1;
+  // the shared-memory limit is a per-function setting: contexts of other
+  // sizes in the same process may have changed it since this one was sized
+  const cudaError_t e = oa_smem_limit(k_ortho_ns_cluster);
+  if (e != cudaSuccess) return e;
   return cudaLaunchKernelEx(&cfg, k_ortho_ns_cluster, S, n, bscale, tol, max_iter, A0, A1, B0, B1, Cm, errpart, T,
                             status, errv);
 }

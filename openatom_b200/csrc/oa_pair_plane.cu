@@ -433,13 +433,13 @@ static cudaError_t pair_launch(int mode, cudaStream_t st, void* zbuf, int nstate
   const dim3 grid(nz, ngroup);
   cudaError_t e;
   if (mode == 0) {
-    e = cudaFuncSetAttribute(k_pair_density<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    e = oa_smem_limit(k_pair_density<N1, N2>);
     if (e != cudaSuccess) return e;
     k_pair_density<N1, N2><<<grid, CF::NT, L.total, st>>>((const float2*)zbuf, nstate, nz, ldl, nlines,
                                                           (const int4*)cols, nkx, tw, occ, rho_part, ngroup,
                                                           (float2*)psir, L);
   } else {
-    e = cudaFuncSetAttribute(k_pair_vks<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    e = oa_smem_limit(k_pair_vks<N1, N2>);
     if (e != cudaSuccess) return e;
     k_pair_vks<N1, N2><<<grid, CF::NT, L.total, st>>>((float2*)zbuf, nstate, nz, ldl, (const int4*)cols, nkx, tw,
                                                       occ, (const float*)vks, ngroup, (const float2*)psir, L);

@@ -527,7 +527,7 @@ static cudaError_t zfwd2_n(cudaStream_t st, const double2* psi, int ng, int s0, 
                            const double2* dyp) {
   typedef typename CplxOf<R>::T C;
   const size_t sm = zpass2_smem<R, N1, N2>();
-  cudaError_t e = cudaFuncSetAttribute(k_zfwd2<R, N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = oa_smem_limit(k_zfwd2<R, N1, N2>);
   if (e != cudaSuccess) return e;
   dim3 grid((nlines + OA_LB - 1) / OA_LB, ns);
   k_zfwd2<R, N1, N2><<<grid, OA_NTHREADS, sm, st>>>(psi, ng, s0, off, nneg, npos, nlines, (C*)zbuf, ldl, tw, dyp);
@@ -559,7 +559,7 @@ static cudaError_t zbwd2_n(cudaStream_t st, const void* zbuf, int ldl, int nline
                            OaPlaneOut po) {
   typedef typename CplxOf<R>::T C;
   const size_t sm = zpass2_smem<R, N1, N2>();
-  cudaError_t e = cudaFuncSetAttribute(k_zbwd2<R, N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = oa_smem_limit(k_zbwd2<R, N1, N2>);
   if (e != cudaSuccess) return e;
   dim3 grid(nblk, ns);
   k_zbwd2<R, N1, N2><<<grid, OA_NTHREADS, sm, st>>>((const C*)zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl,
@@ -602,7 +602,7 @@ static cudaError_t plane2_n(cudaStream_t st, void* zbuf, int nstate, int ldl, in
   const Plane2Smem L = plane2_layout<C, R, N1, N2>(nkx, MODE);
   if (L.G < 1 || L.total > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
   cudaError_t e =
-      cudaFuncSetAttribute(k_plane2<R, MODE, N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+      oa_smem_limit(k_plane2<R, MODE, N1, N2>);
   if (e != cudaSuccess) return e;
   dim3 grid(nz, ngroup);
   k_plane2<R, MODE, N1, N2><<<grid, p2_threads<R, MODE>(), L.total, st>>>(

@@ -438,7 +438,7 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
   e = two_pass ? oa_rho2_fwd(s, c->nx, c->nz, c->rho, c->vol / c->npts, c->tw_x, (double2*)c->dz, c->ldl_d)
                : cudaErrorNotSupported;
   if (e == cudaErrorNotSupported) {
-    e = cudaFuncSetAttribute(k_rho_plane_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    e = oa_smem_limit(k_rho_plane_fwd);
     if (e != cudaSuccess) return e;
     k_rho_plane_fwd<<<c->nz, OA_NTHREADS, L.total, s>>>(c->rho, c->vol / c->npts, c->nx, c->ny, c->nz, c->nkx_d,
                                                          c->plan_x, c->plan_y, c->tw_x, c->tw_y,
@@ -454,7 +454,7 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
         (align_up_r(c->nz, 2) + (size_t)OA_LB * (c->nz + 1) + (size_t)OA_LB * ldb + (size_t)OA_LB * c->natm) *
         sizeof(double2);
     if (smz > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
-    cudaError_t e2 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
+    cudaError_t e2 = oa_smem_limit(kern);
     if (e2 != cudaSuccess) return e2;
     kern<<<nbz, OA_NTHREADS, smz, s>>>((double2*)c->dz, c->ldl_d, c->nlines_d, c->nx, c->ny, c->nz,
                                        c->plan_z, c->tw_z, tpi_l, c->vol, c->ecut_rho,
@@ -480,13 +480,13 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
     if (e != cudaErrorNotSupported) return e;
   }
   if (c->precision == OA_FP64) {
-    e = cudaFuncSetAttribute(k_rho_plane_bwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    e = oa_smem_limit(k_rho_plane_bwd<double>);
     if (e != cudaSuccess) return e;
     k_rho_plane_bwd<double><<<c->nz, OA_NTHREADS, L.total, s>>>((const double2*)c->dz, c->ldl_d, c->nx, c->ny, c->nz,
                                                                 c->nkx_d, c->plan_x, c->plan_y, c->tw_x, c->tw_y,
                                                                 c->vxc, (double*)c->vks, c->npair_d, c->ychunk_d, L);
   } else {
-    e = cudaFuncSetAttribute(k_rho_plane_bwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    e = oa_smem_limit(k_rho_plane_bwd<float>);
     if (e != cudaSuccess) return e;
     k_rho_plane_bwd<float><<<c->nz, OA_NTHREADS, L.total, s>>>((const double2*)c->dz, c->ldl_d, c->nx, c->ny, c->nz,
                                                                c->nkx_d, c->plan_x, c->plan_y, c->tw_x, c->tw_y,

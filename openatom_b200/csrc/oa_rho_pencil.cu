@@ -218,7 +218,7 @@ static cudaError_t rho2_fwd_n(cudaStream_t s, int nz, const double* rho, double 
                               int ldl_d) {
   const size_t sm = rho2_smem<N1, N2>();
   if (sm > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
-  cudaError_t e = cudaFuncSetAttribute(k_rho2_fwd<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = oa_smem_limit(k_rho2_fwd<N1, N2>);
   if (e != cudaSuccess) return e;
   k_rho2_fwd<N1, N2><<<nz, 512, sm, s>>>(rho, scale, tw, dz, ldl_d);
   return cudaGetLastError();
@@ -231,11 +231,11 @@ static cudaError_t rho2_bwd_n(cudaStream_t s, int nz, const double2* dz, int ldl
   if (sm > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
   cudaError_t e;
   if (fp64) {
-    e = cudaFuncSetAttribute(k_rho2_bwd<N1, N2, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    e = oa_smem_limit(k_rho2_bwd<N1, N2, double>);
     if (e != cudaSuccess) return e;
     k_rho2_bwd<N1, N2, double><<<nz, 512, sm, s>>>(dz, ldl_d, tw, vxc, (double*)vks);
   } else {
-    e = cudaFuncSetAttribute(k_rho2_bwd<N1, N2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    e = oa_smem_limit(k_rho2_bwd<N1, N2, float>);
     if (e != cudaSuccess) return e;
     k_rho2_bwd<N1, N2, float><<<nz, 512, sm, s>>>(dz, ldl_d, tw, vxc, (float*)vks);
   }

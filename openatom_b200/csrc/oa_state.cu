@@ -375,7 +375,7 @@ template <typename R>
 static cudaError_t launch_zfwd(oa_ctx* c, cudaStream_t st, const double2* psi, int s0, int ns) {
   typedef typename CplxOf<R>::T C;
   size_t sm = zpass_smem<R>(c->nz);
-  cudaError_t e = cudaFuncSetAttribute(k_state_zfwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = oa_smem_limit(k_state_zfwd<R>);
   if (e != cudaSuccess) return e;
   dim3 grid((c->nlines + OA_LB - 1) / OA_LB, ns);
   k_state_zfwd<R><<<grid, OA_NTHREADS, sm, st>>>(psi, c->ng, s0, c->line_off, c->line_nneg, c->line_npos,
@@ -387,7 +387,7 @@ template <typename R, int MODE>
 static cudaError_t launch_plane(oa_ctx* c, cudaStream_t st) {
   typedef typename CplxOf<R>::T C;
   PlaneSmem L = plane_smem_layout<C, R>(c->nx, c->ny, c->nkx_s);
-  cudaError_t e = cudaFuncSetAttribute(k_state_plane<R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+  cudaError_t e = oa_smem_limit(k_state_plane<R, MODE>);
   if (e != cudaSuccess) return e;
   dim3 grid(c->nz, c->ngroup);
   EesArgs E = {nullptr, nullptr, nullptr, nullptr, 0, 0};
@@ -402,7 +402,7 @@ static cudaError_t launch_zbwd(oa_ctx* c, cudaStream_t st, const double2* psi, c
                                double2* force, int s0, int ns) {
   typedef typename CplxOf<R>::T C;
   size_t sm = zpass_smem<R>(c->nz);
-  cudaError_t e = cudaFuncSetAttribute(k_state_zbwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = oa_smem_limit(k_state_zbwd<R>);
   if (e != cudaSuccess) return e;
   dim3 grid(c->nblk_z, ns);
   k_state_zbwd<R><<<grid, OA_NTHREADS, sm, st>>>(
@@ -501,7 +501,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
     if (err != cudaSuccess) return err;
   } else {
     size_t sm = zpass_smem<R>(e->nc);
-    err = cudaFuncSetAttribute(k_state_zfwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    err = oa_smem_limit(k_state_zfwd<R>);
     if (err != cudaSuccess) return err;
     dim3 grid((c->nlines + OA_LB - 1) / OA_LB, c->nstate);
     k_state_zfwd<R><<<grid, OA_NTHREADS, sm, st>>>(psi, c->ng, 0, c->line_off, c->line_nneg, c->line_npos, c->nlines,
@@ -517,7 +517,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
     err = oa_pencil_plane(c->precision, 2, st, e->na, e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky,
                           e->nc, c->nkx_s, e->tw_a, c->occ, nullptr, nullptr, e->ngroup, E, nullptr);
   if (err == cudaErrorNotSupported) {
-    err = cudaFuncSetAttribute(k_state_plane<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    err = oa_smem_limit(k_state_plane<R, 2>);
     if (err != cudaSuccess) return err;
     k_state_plane<R, 2><<<pgrid, OA_PLANE_THREADS, L.total, st>>>(
         (C*)e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky, e->na, e->nb, e->nc, c->nkx_s, e->pa,
@@ -532,7 +532,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
     err = oa_pencil_plane(c->precision, 3, st, e->na, e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky,
                           e->nc, c->nkx_s, e->tw_a, c->occ, nullptr, nullptr, e->ngroup, E, nullptr);
   if (err == cudaErrorNotSupported) {
-    err = cudaFuncSetAttribute(k_state_plane<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    err = oa_smem_limit(k_state_plane<R, 3>);
     if (err != cudaSuccess) return err;
     k_state_plane<R, 3><<<pgrid, OA_PLANE_THREADS, L.total, st>>>(
         (C*)e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky, e->na, e->nb, e->nc, c->nkx_s, e->pa,
@@ -546,7 +546,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
                           1.0, c->ecut_psi, c->eke_part, c->nblk_z, e->dyp, OaPlaneOut{nullptr, 0, 0, 0});
   {
     size_t sm = zpass_smem<R>(e->nc);
-    err = cudaFuncSetAttribute(k_state_zbwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    err = oa_smem_limit(k_state_zbwd<R>);
     if (err != cudaSuccess) return err;
     dim3 grid(c->nblk_z, c->nstate);
     k_state_zbwd<R><<<grid, OA_NTHREADS, sm, st>>>(

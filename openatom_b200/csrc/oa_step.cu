@@ -328,6 +328,176 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
   return OA_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Batching form: nsys independent systems (replicas, beads, tempering
+// systems of any sizes), nsteps CP steps each.  After each system's first
+// step, one step of every system is one CUDA graph: the systems' launches
+// fork from `stream` onto one stream per system and join back, so the
+// kernels of different systems fill the GPU together.
+// ---------------------------------------------------------------------------
+static void fill_energies(const double* hv, double* eo) {
+  eo[0] = hv[OA_E_EKE]; eo[1] = hv[OA_E_EHART]; eo[2] = hv[OA_E_EEXT]; eo[3] = hv[OA_E_EWALD];
+  eo[4] = hv[8] + hv[9]; eo[5] = hv[OA_E_MUXC]; eo[6] = hv[OA_E_FICT]; eo[7] = hv[OA_E_ENL];
+  eo[8] = hv[16]; eo[9] = hv[18]; eo[10] = hv[19];
+}
+
+static oa_status batch_launch_one(oa_ctx* c, cudaStream_t s, oa_cp_state* st, int complete_prev) {
+  oa_planes_step_begin(c);
+  oa_status r = launch_step_a(c, s, st, complete_prev);
+  if (r == OA_OK) r = launch_step_ns(c, s, st);
+  if (r == OA_OK) r = launch_step_b(c, s, st);
+  oa_planes_step_end(c);
+  return r;
+}
+
+extern "C" oa_status oa_gpu_cp_run_batch(oa_ctx** ctxs, oa_cp_state** states, int nsys, void* stream, int nsteps,
+                                         double* energies_out) {
+  if (!ctxs || !states || nsys < 1 || nsteps < 1) {
+    oa_set_error("null argument, nsys < 1 or nsteps < 1", __FILE__, __LINE__);
+    return OA_ERR_BAD_ARG;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  if (s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread) {
+    oa_set_error("the batched run needs a created stream (it is captured into a CUDA graph)", __FILE__, __LINE__);
+    return OA_ERR_BAD_ARG;
+  }
+  for (int i = 0; i < nsys; ++i) {
+    oa_ctx* c = ctxs[i];
+    oa_cp_state* st = states[i];
+    if (!c || !st || !st->psi || !st->psi_t || !st->vpsi || !st->T) {
+      oa_set_error("null context or state in the batch", __FILE__, __LINE__);
+      return OA_ERR_BAD_ARG;
+    }
+    if (!(st->mixed_nterm == 0 || st->mixed_nterm == 2 || st->mixed_nterm == 3)) {
+      oa_set_error("mixed_nterm must be 0, 2 or 3", __FILE__, __LINE__);
+      return OA_ERR_BAD_ARG;
+    }
+    for (int j = 0; j < i; ++j)
+      if (ctxs[j] == c) {
+        oa_set_error("a context appears twice in the batch", __FILE__, __LINE__);
+        return OA_ERR_BAD_ARG;
+      }
+    // the whole step must be capturable: the cluster Newton-Schulz kernel
+    if (!oa_ns_capturable(c)) {
+      oa_set_error("the batched run needs the cluster Newton-Schulz kernel (at most 128 states)", __FILE__,
+                   __LINE__);
+      return OA_ERR_UNSUPPORTED;
+    }
+  }
+  for (int i = 0; i < nsys; ++i) {
+    OA_STEP_TRY(ensure_scratch(ctxs[i]));
+    OA_STEP_TRY(ensure_ring(ctxs[i], nsteps));
+  }
+  std::vector<cudaStream_t> side(nsys, nullptr);
+  std::vector<cudaEvent_t> join(nsys, nullptr);
+  cudaEvent_t fork = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  oa_status ret = OA_OK;
+  auto fail = [&](cudaError_t e, int line) {
+    oa_set_error(cudaGetErrorString(e), __FILE__, line);
+    ret = OA_ERR_CUDA;
+  };
+  cudaError_t ce = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+  for (int i = 0; i < nsys && ce == cudaSuccess; ++i) {
+    ce = cudaStreamCreateWithFlags(&side[i], cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming);
+  }
+  if (ce != cudaSuccess) fail(ce, __LINE__);
+  // per system: restart the PsiV flag and record count, psi planes from the handed-in psi
+  for (int i = 0; i < nsys && ret == OA_OK; ++i) {
+    oa_step_scratch* w = step_scratch(ctxs[i]);
+    ce = cudaMemsetAsync(w->flag, 0, 4 * sizeof(int), s);
+    if (ce != cudaSuccess) { fail(ce, __LINE__); break; }
+    if (states[i]->mixed_nterm) ret = oa_planes_psi_refresh(ctxs[i], s, states[i]->psi, states[i]->mixed_nterm);
+  }
+  int graph_kernels = 0;
+  // one step of all systems, launched on the side streams (fork .. join)
+  auto step_all = [&](bool steady) -> oa_status {
+    cudaError_t e = cudaEventRecord(fork, s);
+    if (e != cudaSuccess) { fail(e, __LINE__); return ret; }
+    for (int i = 0; i < nsys; ++i) {
+      if ((e = cudaStreamWaitEvent(side[i], fork, 0)) != cudaSuccess) { fail(e, __LINE__); return ret; }
+      oa_cp_state* st = states[i];
+      const int complete_prev = steady ? 1 : (st->iteration > 0);
+      const oa_status r = batch_launch_one(ctxs[i], side[i], st, complete_prev);
+      if (r != OA_OK) return r;
+      if ((e = cudaEventRecord(join[i], side[i])) != cudaSuccess) { fail(e, __LINE__); return ret; }
+      if ((e = cudaStreamWaitEvent(s, join[i], 0)) != cudaSuccess) { fail(e, __LINE__); return ret; }
+    }
+    return OA_OK;
+  };
+  for (int k = 0; k < nsteps && ret == OA_OK; ++k) {
+    bool all_steady = true;
+    for (int i = 0; i < nsys; ++i) all_steady = all_steady && states[i]->iteration > 0;
+    if (!all_steady) {
+      // first steps (no previous half kick) run eagerly
+      ret = step_all(false);
+    } else {
+      if (!exec) {
+        cudaGraph_t g = nullptr;
+        if ((ce = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+          fail(ce, __LINE__);
+          break;
+        }
+        const oa_status r = step_all(true);
+        ce = cudaStreamEndCapture(s, &g);
+        if (r != OA_OK) { if (g) cudaGraphDestroy(g); ret = r; break; }
+        if (ce != cudaSuccess) { fail(ce, __LINE__); break; }
+        size_t nn = 0;
+        if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn > 0) {
+          std::vector<cudaGraphNode_t> nodes(nn);
+          if (cudaGraphGetNodes(g, nodes.data(), &nn) == cudaSuccess)
+            for (size_t q = 0; q < nn; ++q) {
+              cudaGraphNodeType t;
+              if (cudaGraphNodeGetType(nodes[q], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++graph_kernels;
+            }
+        }
+        ce = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) { fail(ce, __LINE__); break; }
+      }
+      if ((ce = cudaGraphLaunch(exec, s)) != cudaSuccess) { fail(ce, __LINE__); break; }
+    }
+    for (int i = 0; i < nsys; ++i) states[i]->iteration += 1;
+  }
+  // records and flags of every system, one synchronisation
+  for (int i = 0; i < nsys && ret == OA_OK; ++i) {
+    oa_step_scratch* w = step_scratch(ctxs[i]);
+    ce = cudaMemcpyAsync(w->ring_host, w->ring, (size_t)nsteps * OA_REC * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(w->flag_host, w->flag, 4 * sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (ce != cudaSuccess) fail(ce, __LINE__);
+  }
+  if (ret == OA_OK && (ce = cudaStreamSynchronize(s)) != cudaSuccess) fail(ce, __LINE__);
+  if (exec) cudaGraphExecDestroy(exec);
+  for (int i = 0; i < nsys; ++i) {
+    if (join[i]) cudaEventDestroy(join[i]);
+    if (side[i]) cudaStreamDestroy(side[i]);
+  }
+  if (fork) cudaEventDestroy(fork);
+  if (ret != OA_OK) return ret;
+  for (int i = 0; i < nsys; ++i) {
+    oa_step_scratch* w = step_scratch(ctxs[i]);
+    oa_cp_state* st = states[i];
+    if (energies_out)
+      for (int k = 0; k < nsteps; ++k)
+        fill_energies(w->ring_host + (size_t)k * OA_REC, energies_out + ((size_t)i * nsteps + k) * 11);
+    const double* last = w->ring_host + (size_t)(nsteps - 1) * OA_REC;
+    st->last_kernels = graph_kernels > 0 ? graph_kernels : -1;
+    st->last_ns_iters = (int)last[16];
+    st->last_ns_err = last[18];
+    st->last_smax = last[19];
+    if (w->flag_host[2] != 0) {
+      char msg[200];
+      snprintf(msg, sizeof(msg), "system %d of the batch: %s in step %d of %d", i,
+               w->flag_host[2] == 2 ? "Newton-Schulz residual is not finite" : "Newton-Schulz reached max_iter",
+               w->flag_host[3] + 1, nsteps);
+      oa_set_error(msg, __FILE__, __LINE__);
+      return w->flag_host[2] == 2 ? OA_ERR_NONFINITE : OA_ERR_NOT_CONVERGED;
+    }
+  }
+  return OA_OK;
+}
+
 extern "C" oa_status oa_gpu_cp_step(oa_ctx* c, void* stream, oa_cp_state* st, double* energies_out) {
   return run_steps(c, stream, st, 1, nullptr, energies_out);
 }

@@ -580,7 +580,7 @@ cudaError_t oa_tfwd(cudaStream_t s, int nt, const bf16* PA, int rows_a, const bf
   cudaError_t e = cudaErrorNotSupported;
 #define OA_TF(NTT, NBB)                                                                                     \
   if (nt == NTT && nb == NBB) {                                                                             \
-    e = cudaFuncSetAttribute(k_tfwd<NTT, NBB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);        \
+    e = oa_smem_limit(k_tfwd<NTT, NBB>);        \
     if (e != cudaSuccess) return e;                                                                         \
     k_tfwd<NTT, NBB><<<grid, TG_THREADS, sm, s>>>(ta, tb, m, n, K, nkb, stages, part, err_flag, cond);       \
     e = cudaGetLastError();                                                                                 \
@@ -625,7 +625,7 @@ cudaError_t oa_tbwd(cudaStream_t s, int nt, const bf16* PM1, const bf16* PX1, do
   cudaError_t e = cudaErrorNotSupported;
 #define OA_TB(NTT, NBB)                                                                                        \
   if (nt == NTT && nb == NBB) {                                                                                \
-    e = cudaFuncSetAttribute(k_tbwd<NTT, NBB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);           \
+    e = oa_smem_limit(k_tbwd<NTT, NBB>);           \
     if (e != cudaSuccess) return e;                                                                            \
     k_tbwd<NTT, NBB><<<grid, TB_THREADS, sm, s>>>(tx1, tm1, tx2, tm2, nterm, a1_kx0, a1_rest, a2, nj, nk, ncol,  \
                                                   kx0_cols, stages, out, err_flag, yadd, cond);                \

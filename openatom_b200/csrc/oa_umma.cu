@@ -490,11 +490,11 @@ cudaError_t oa_launch_umma_fwd(cudaStream_t s, int nterm, const double* A, const
   dim3 grid(kb, mtiles, ntiles);
   cudaError_t e;
   if (nterm == 2) {
-    e = cudaFuncSetAttribute(k_umma_fwd<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    e = oa_smem_limit(k_umma_fwd<2>);
     if (e != cudaSuccess) return e;
     k_umma_fwd<2><<<grid, UM_THREADS, L.total, s>>>(A, B, m, n, K, kx0_cols, w_kx0, nb, per, part, err_flag);
   } else {
-    e = cudaFuncSetAttribute(k_umma_fwd<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    e = oa_smem_limit(k_umma_fwd<3>);
     if (e != cudaSuccess) return e;
     k_umma_fwd<3><<<grid, UM_THREADS, L.total, s>>>(A, B, m, n, K, kx0_cols, w_kx0, nb, per, part, err_flag);
   }
@@ -513,12 +513,12 @@ cudaError_t oa_launch_umma_bwd(cudaStream_t s, int nterm, const double* M1, cons
   dim3 grid((unsigned)((ncol + UM_M - 1) / UM_M), (nj + nb - 1) / nb);
   cudaError_t e;
   if (nterm == 2) {
-    e = cudaFuncSetAttribute(k_umma_bwd<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    e = oa_smem_limit(k_umma_bwd<2>);
     if (e != cudaSuccess) return e;
     k_umma_bwd<2><<<grid, UM_THREADS, L.total, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, nb,
                                                      out, err_flag);
   } else {
-    e = cudaFuncSetAttribute(k_umma_bwd<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    e = oa_smem_limit(k_umma_bwd<3>);
     if (e != cudaSuccess) return e;
     k_umma_bwd<3><<<grid, UM_THREADS, L.total, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, nb,
                                                      out, err_flag);

@@ -79,6 +79,8 @@ SIGNATURES = {
     "oa_gpu_energies": (C.c_int, [_vp, _vp, _dp]),
     "oa_gpu_psiv_reset": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "oa_gpu_psiv_reset_mixed": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int]),
+    "oa_gpu_cp_run_batch": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int, _vp, C.c_int,
+                                      C.POINTER(C.c_double)]),
     "oa_gpu_set_atoms": (C.c_int, [_vp, _vp, _dp]),
     "oa_gpu_time_kernels": (C.c_int, [_vp, _vp, _vp, C.c_int, _dp]),
     "oa_gpu_sizes": (C.c_int, [_vp, C.POINTER(C.c_long)]),
@@ -502,3 +504,26 @@ class CPDriver:
         en["ORTHO_ERR"] = err
         en["SMAX"] = smax
         return en
+
+
+def run_batch(drivers, states, nsteps: int, stream=None) -> list:
+    """nsteps CP steps of several independent systems in one call
+    (oa_gpu_cp_run_batch): after each system's first step, one step of all
+    systems is one CUDA graph with the systems on concurrent streams.
+    drivers: CPDriver per system; states: their native_state().  Returns,
+    per system, one record per step (as CPContext.cp_run)."""
+    import torch
+    n = len(drivers)
+    if n != len(states) or n < 1:
+        raise ValueError("one state per driver")
+    lib = load_library()
+    ctxs = (C.c_void_p * n)(*[d.ctx._h.value for d in drivers])
+    sts = (C.c_void_p * n)(*[C.cast(C.pointer(s), C.c_void_p).value for s in states])
+    out = np.zeros((n, nsteps, 11))
+    st = stream if stream is not None else drivers[0].stream
+    torch.cuda.synchronize()
+    _check(lib.oa_gpu_cp_run_batch(ctxs, sts, n, C.c_void_p(st.cuda_stream), int(nsteps),
+                                   out.ctypes.data_as(_dp)))
+    for d, s in zip(drivers, states):
+        d.iteration = s.iteration
+    return [[{k: float(v) for k, v in zip(STEP_KEYS, row)} for row in sysrows] for sysrows in out]

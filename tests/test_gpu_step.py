@@ -136,3 +136,20 @@ def test_psiv_reset_mixed_matches_fp64():
     d64 = out[0] - v0
     err = np.max(np.abs(out[3] - out[0])) / np.max(np.abs(d64))
     assert err < 1e-5, err
+
+
+def test_native_run_odd_state_count():
+    """An odd number of states takes the 8-byte operand path of the FP64
+    backward product and the two-graph step (cooperative Newton-Schulz):
+    same results as the host runner."""
+    from openatom_b200.gpu import CPDriver
+    s = make_system("w2", nstate=7, seed=26, dt=0.5)
+    a = CPDriver(s, "fp64")
+    b = CPDriver(s, "fp64")
+    sb = b.native_state(use_graph=True)
+    ea = [a.step() for _ in range(3)]
+    eb = b.run_native(sb, 3)
+    for i in range(3):
+        for k in ("EKE", "EHART", "EEXT", "EEXC", "ENL", "FICT_KE"):
+            assert eb[i][k] == ea[i][k], (i, k, ea[i][k], eb[i][k])
+    assert np.array_equal(a.psi.cpu().numpy(), b.psi.cpu().numpy())
