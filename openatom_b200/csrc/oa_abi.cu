@@ -256,6 +256,11 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
   }
   c->ngroup = pick_groups(d->nz, d->nstate, bps, nsm);
   c->ngroup_pair = pick_groups(d->nz, (d->nstate + 1) / 2, 1, nsm);
+  c->pair_kymax = 0;
+  for (int l = 0; l < d->nlines; ++l) {
+    const int a = d->line_ky[l] < 0 ? -d->line_ky[l] : d->line_ky[l];
+    c->pair_kymax = a > c->pair_kymax ? a : c->pair_kymax;
+  }
   c->rho_ngroup = c->ngroup;
   c->nblk_z = (d->nlines + OA_LB - 1) / OA_LB;
 
@@ -612,7 +617,6 @@ __global__ void k_copy_cond(double* __restrict__ dst, const double* __restrict__
     dst[i] = src[i];
 }
 
-__global__ void k_flag_clear(int* flag) { flag[0] = 0; }
 
 cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m, int n, long K, long kx0_cols,
                          double w_kx0, double alpha, double* part, int nkb, double* C, const int* cond);
@@ -881,8 +885,8 @@ static oa_status psiv_velocity(oa_ctx* c, cudaStream_t s, const double* psi, dou
 }
 
 // psi = psi_t T (FP64), also written to psi_t when the PsiV flag is set;
-// then, under the flag, the velocity projection and T = I, and the flag is
-// cleared.  The native step's orthonormalisation and PsiV reset
+// then, under the flag, the velocity projection and T = I (the next step's
+// check sets or clears the flag).  The native step's orthonormalisation and PsiV reset
 // (Ortho::maxCheck, ortho.C:455-475): same results as oa_gpu_pc_backward
 // followed by oa_gpu_psiv_reset, decided on the device.
 oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* psi_t, double* psi, double* vpsi,
@@ -896,7 +900,6 @@ oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* 
   if (fuse) plane_mark(c, PL_PSI, psi, n, po.rows_pad, nterm);
   OA_STEP_CHECK(psiv_velocity(c, s, psi, vpsi, flag, nterm));
   k_copy_cond<<<16, 256, 0, s>>>(Tout, p->eye, (size_t)n * n, flag);
-  k_flag_clear<<<1, 1, 0, s>>>(flag);
   OA_CUDA_TRY(cudaGetLastError());
   return OA_OK;
 }

@@ -81,7 +81,7 @@ static __device__ __forceinline__ float2 pp_herm(const float2* P, int nkx, int k
 //   phase b(q): x pass B (q)  [Sx -> psi(r), density]  +  y pass B (q+1) [Sy -> P]
 // The z-line rows of pair q + 2 arrive by cp.async during both phases.
 // ---------------------------------------------------------------------------
-template <int N1, int N2>
+template <int N1, int N2, bool BAND>
 __global__ void __launch_bounds__(PairCfg<N1, N2>::NT, 1)
 k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int nlines,
                const int4* __restrict__ cols, int nkx, const double2* __restrict__ twg,
@@ -152,12 +152,16 @@ k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int
     float2 u[N1];
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1) {
+      if (BAND && n1 >= N1 / 4 && n1 < 3 * N1 / 4) {  // |ky| >= N/4: outside every column run
+        u[n1] = make_float2(0.f, 0.f);
+        continue;
+      }
       const int i = N2 * n1 + n2;
       const int ky = (2 * i <= N) ? i : i - N;
       const int l = ky - cr.y;
       u[n1] = (live && l >= 0 && l < cr.z) ? r[l] : make_float2(0.f, 0.f);
     }
-    pass_a<N1, N2, -1>(u, n2, tw);
+    pass_a_band<N1, N2, -1, BAND>(u, n2, tw);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) Sy[pc * PS1 + k1 * LS1 + n2] = u[k1];
   };
@@ -180,6 +184,10 @@ k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int
     float2 u[N1];
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1) {
+      if (BAND && n1 >= N1 / 4 && n1 < 3 * N1 / 4) {  // N/4 <= kx < 3N/4: zero spectrum
+        u[n1] = make_float2(0.f, 0.f);
+        continue;
+      }
       const int2 t = hx[n1];
       float2 v = make_float2(0.f, 0.f);
       if (t.x >= 0) {
@@ -189,7 +197,7 @@ k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int
       }
       u[n1] = v;
     }
-    pass_a<N1, N2, -1>(u, n2, tw);
+    pass_a_band<N1, N2, -1, BAND>(u, n2, tw);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) Sx[y * PS1 + k1 * LS1 + n2] = u[k1];
   };
@@ -425,7 +433,7 @@ static PairSmem pair_layout(int nkx, int nlines, int mode) {
 template <int N1, int N2>
 static cudaError_t pair_launch(int mode, cudaStream_t st, void* zbuf, int nstate, int nz, int ldl, int nlines,
                                const int* cols, int nkx, const double2* tw, const double* occ, const void* vks,
-                               double* rho_part, int ngroup, void* psir) {
+                               double* rho_part, int ngroup, void* psir, int kymax) {
   typedef PairCfg<N1, N2> CF;
   if (CF::XBW == 0 || N1 > 16 || 2 * nkx > CF::N + 2 || (ldl & 1)) return cudaErrorNotSupported;
   const PairSmem L = pair_layout<N1, N2>(nkx, nlines, mode);
@@ -433,11 +441,21 @@ static cudaError_t pair_launch(int mode, cudaStream_t st, void* zbuf, int nstate
   const dim3 grid(nz, ngroup);
   cudaError_t e;
   if (mode == 0) {
-    e = oa_smem_limit(k_pair_density<N1, N2>);
-    if (e != cudaSuccess) return e;
-    k_pair_density<N1, N2><<<grid, CF::NT, L.total, st>>>((const float2*)zbuf, nstate, nz, ldl, nlines,
-                                                          (const int4*)cols, nkx, tw, occ, rho_part, ngroup,
-                                                          (float2*)psir, L);
+    // the forward DFT_N1 inputs in [N1/4, 3 N1/4) are zero when the sphere's
+    // kx columns and ky runs stay inside |k| < N/4
+    constexpr int N = CF::N;
+    const bool band = (N1 % 4 == 0) && 4 * nkx <= N && 4 * (kymax + 1) <= N;
+    auto launch = [&](auto kern) -> cudaError_t {
+      cudaError_t e2 = oa_smem_limit(kern);
+      if (e2 != cudaSuccess) return e2;
+      kern<<<grid, CF::NT, L.total, st>>>((const float2*)zbuf, nstate, nz, ldl, nlines, (const int4*)cols, nkx, tw,
+                                          occ, rho_part, ngroup, (float2*)psir, L);
+      return cudaGetLastError();
+    };
+    if constexpr (N1 % 4 == 0) {
+      if (band) return launch(k_pair_density<N1, N2, true>);
+    }
+    return launch(k_pair_density<N1, N2, false>);
   } else {
     e = oa_smem_limit(k_pair_vks<N1, N2>);
     if (e != cudaSuccess) return e;
@@ -463,13 +481,14 @@ static cudaError_t pair_launch(int mode, cudaStream_t st, void* zbuf, int nstate
 
 // mode 0: density pass (rho_part[group][z][y][x], psi(r) pairs stored);
 // mode 4: V_KS pass from those psi(r) pairs.  nx = ny = n; cols = per kx
-// column {first line, ky of the first line, line count, 0}.  Returns
+// column {first line, ky of the first line, line count, 0}; kymax = the
+// largest |ky| of the lines.  Returns
 // cudaErrorNotSupported when n or the shared memory has no pair kernel.
 cudaError_t oa_pair_plane(int mode, cudaStream_t st, int n, void* zbuf, int nstate, int nz, int ldl, int nlines,
                           const int* cols, int nkx, const double2* tw, const double* occ, const void* vks,
-                          double* rho_part, int ngroup, void* psir) {
+                          double* rho_part, int ngroup, void* psir, int kymax) {
 #define OA_CALL(A, B) \
-  pair_launch<A, B>(mode, st, zbuf, nstate, nz, ldl, nlines, cols, nkx, tw, occ, vks, rho_part, ngroup, psir)
+  pair_launch<A, B>(mode, st, zbuf, nstate, nz, ldl, nlines, cols, nkx, tw, occ, vks, rho_part, ngroup, psir, kymax)
   OA_PAIR_DISPATCH(n, OA_CALL)
 #undef OA_CALL
   return cudaErrorNotSupported;

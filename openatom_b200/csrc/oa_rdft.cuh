@@ -153,3 +153,44 @@ OA_HD void pass_a(C* u, int n2, const C* tw) {
 #pragma unroll
   for (int k1 = 1; k1 < N1; ++k1) u[k1] = cmul(u[k1], tw_rt<SIGN>(tw, n2 * k1));
 }
+
+// DFT of length N (N % 4 == 0) whose inputs n in [N/4, 3N/4) are zero (the
+// sphere of a state occupies |k| < N/4 of its density-sized grid).  Same
+// Cooley-Tukey split as RDft<N> (P = 4, Q = N/4, n = Q p + q): every DFT_4
+// over p has inputs at p = 0 and p = 3 only, X[kp] = x0 + x3 W^{3 kp}.
+template <int N, int SIGN> struct RDftBand {
+  static_assert(N % 4 == 0, "RDftBand: N must be a multiple of 4");
+  static constexpr int Q = N / 4;
+  template <typename C>
+  OA_HD static void run(C* v) {
+    C t[N];
+    sfor<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      const C a = v[q], b = v[3 * Q + q];
+      C u[4];
+      u[0] = cadd(a, b);
+      u[1] = cadd(a, cmul_si<-SIGN>(b));
+      u[2] = csub(a, b);
+      u[3] = cadd(a, cmul_si<SIGN>(b));
+      sfor<0, 4>([&](auto kc) {
+        constexpr int kp = decltype(kc)::value;
+        t[kp * Q + q] = twc<N, SIGN, q * kp>(u[kp]);
+      });
+    });
+#pragma unroll
+    for (int kp = 0; kp < 4; ++kp) {
+      RDft<Q, SIGN>::run(t + kp * Q);
+#pragma unroll
+      for (int kq = 0; kq < Q; ++kq) v[kp + 4 * kq] = t[kp * Q + kq];
+    }
+  }
+};
+
+// pass A with the middle band of inputs zero (BAND) or general
+template <int N1, int N2, int SIGN, bool BAND, typename C>
+OA_HD void pass_a_band(C* u, int n2, const C* tw) {
+  if constexpr (BAND) RDftBand<N1, SIGN>::run(u);
+  else RDft<N1, SIGN>::run(u);
+#pragma unroll
+  for (int k1 = 1; k1 < N1; ++k1) u[k1] = cmul(u[k1], tw_rt<SIGN>(tw, n2 * k1));
+}

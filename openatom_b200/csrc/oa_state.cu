@@ -365,7 +365,7 @@ cudaError_t oa_pencil_zbwd(int precision, cudaStream_t st, int n, const void* zb
                            int nblk, const double2* dyp, OaPlaneOut po);
 cudaError_t oa_pair_plane(int mode, cudaStream_t st, int n, void* zbuf, int nstate, int nz, int ldl, int nlines,
                           const int* cols, int nkx, const double2* tw, const double* occ, const void* vks,
-                          double* rho_part, int ngroup, void* psir);
+                          double* rho_part, int ngroup, void* psir, int kymax);
 cudaError_t oa_pencil_plane(int precision, int mode, cudaStream_t st, int n, void* zbuf, int nstate, int ldl,
                             int nlines, const int* lkx, const int* lky, int nz, int nkx, const double2* tw,
                             const double* occ, const void* vks, double* rho_part, int ngroup, const EesArgs& E,
@@ -451,7 +451,8 @@ static cudaError_t pencil_plane(oa_ctx* c, cudaStream_t s, int mode, void* psir)
 cudaError_t oa_launch_state_plane_density(oa_ctx* c, cudaStream_t s) {
   if (c->pair_cols && c->psir) {
     const cudaError_t e = oa_pair_plane(0, s, c->nx, c->zbuf, c->nstate, c->nz, c->ldl, c->nlines, c->pair_cols,
-                                        c->nkx_s, c->tw_x, c->occ, nullptr, c->rho_part, c->ngroup_pair, c->psir);
+                                        c->nkx_s, c->tw_x, c->occ, nullptr, c->rho_part, c->ngroup_pair, c->psir,
+                                        c->pair_kymax);
     c->psir_valid = e == cudaSuccess ? 2 : 0;
     c->rho_ngroup = c->ngroup_pair;
     if (e != cudaErrorNotSupported) return e;
@@ -465,7 +466,7 @@ cudaError_t oa_launch_state_plane_density(oa_ctx* c, cudaStream_t s) {
 cudaError_t oa_launch_state_plane_vks(oa_ctx* c, cudaStream_t s) {
   if (c->psir_valid == 2)
     return oa_pair_plane(4, s, c->nx, c->zbuf, c->nstate, c->nz, c->ldl, c->nlines, c->pair_cols, c->nkx_s,
-                         c->tw_x, c->occ, c->vks, nullptr, c->ngroup_pair, c->psir);
+                         c->tw_x, c->occ, c->vks, nullptr, c->ngroup_pair, c->psir, c->pair_kymax);
   const cudaError_t e = c->psir_valid ? pencil_plane(c, s, 4, c->psir) : pencil_plane(c, s, 1, nullptr);
   if (e != cudaErrorNotSupported) return e;
   return c->precision == OA_FP64 ? launch_plane<double, 1>(c, s) : launch_plane<float, 1>(c, s);

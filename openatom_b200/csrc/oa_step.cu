@@ -115,7 +115,8 @@ __global__ void k_step_check(const int* __restrict__ status, const double* __res
   const int k = flag[1];
   const double err = errv[0], smax = errv[1];
   const int code = (!(err == err) || !(smax == smax)) ? 2 : (status[1] ? 0 : 1);
-  if (code == 0 && smax > norb_tol) flag[0] = 1;
+  // set or clear: the flag of the previous step's PsiV reset ends here
+  flag[0] = (code == 0 && smax > norb_tol) ? 1 : 0;
   if (code != 0 && flag[2] == 0) { flag[2] = code; flag[3] = k; }
   double* r = ring + (size_t)(k % ring_cap) * OA_REC;
   for (int i = 0; i < 16; ++i) r[i] = dev_e[i];
