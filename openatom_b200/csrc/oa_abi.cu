@@ -3,6 +3,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <algorithm>
 #include <vector>
 #include <cuda_bf16.h>
 #include "oa_internal.h"
@@ -263,6 +264,19 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
   }
   c->rho_ngroup = c->ngroup;
   c->nblk_z = (d->nlines + OA_LB - 1) / OA_LB;
+  c->zseg = 0;
+  {
+    bool packed = d->nlines > 0;
+    for (int l = 0; l < d->nlines && packed; ++l) {
+      const int end = d->line_off[l] + d->line_nneg[l] + d->line_npos[l];
+      packed = end == (l + 1 < d->nlines ? d->line_off[l + 1] : d->ng);
+    }
+    for (int l0 = 0; l0 < d->nlines && packed; l0 += OA_LB) {
+      const int g1 = l0 + OA_LB < d->nlines ? d->line_off[l0 + OA_LB] : d->ng;
+      c->zseg = std::max(c->zseg, g1 - d->line_off[l0]);
+    }
+    if (c->zseg > 2048) c->zseg = 0;  // keeps the staged runs within 64 KB
+  }
 
   const size_t csz = precision == OA_FP64 ? sizeof(double2) : sizeof(float2);
   const size_t rsz = precision == OA_FP64 ? sizeof(double) : sizeof(float);

@@ -94,6 +94,9 @@ struct oa_ctx {
   size_t red_len;
   double *eke_part;       // [nstate][nblk_z]
   int nblk_z;
+  int zseg;               // longest coefficient run of one z-pass block of
+                          // OA_LB lines when the lines are packed back to
+                          // back (staged in shared memory), else 0
   double energies[8];
   void *step;             // native-step scratch and captured graph (oa_step.cu)
   oa_ees *ees;            // EES nonlocal path, after oa_gpu_ees_init

@@ -43,6 +43,12 @@ template <int N1, int N2> struct PencilLd {
   static constexpr int ps2 = pencil_stride(N2 * ls2, (N2 & 1) ? ((N2 * ls2) & 15) : -1);
 };
 
+// 16-byte global -> shared copy that completes in the background
+__device__ __forceinline__ void zp_cp16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+}
+
 // packed index of z-slot z on a line with nn negative and np non-negative kz
 // (negative kz first, as the reference's run pairs); -1 outside the sphere
 __device__ __forceinline__ int line_slot(int z, int n, int nn, int np) {
@@ -60,19 +66,27 @@ __global__ void __launch_bounds__(OA_NTHREADS)
 k_zfwd2(const double2* __restrict__ psi, int ng, int s0, const int* __restrict__ line_off,
         const int* __restrict__ line_nneg, const int* __restrict__ line_npos, int nlines,
         typename CplxOf<R>::T* __restrict__ zbuf, int ldl, const double2* __restrict__ twz,
-        const double2* __restrict__ dyp) {
+        const double2* __restrict__ dyp, int zseg) {
   typedef typename CplxOf<R>::T C;
   constexpr int N = N1 * N2;
   typedef PencilLd<N1, N2> L;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = (C*)smem_raw;
   C* s1 = tw + align_up(N, 2);
+  // zseg > 0: the block's lines are one contiguous run of the coefficients,
+  // staged with coalesced loads before pass A gathers from it
+  double2* seg = (double2*)(s1 + align_up((size_t)OA_LB * L::ps1, 2));
   const int s = s0 + blockIdx.y;
   const int l0 = blockIdx.x * OA_LB;
   const int nb = min(OA_LB, nlines - l0);
+  const double2* ps = psi + (size_t)s * ng;
+  const int g0 = zseg > 0 ? line_off[l0] : 0;
+  if (zseg > 0) {
+    const int g1 = (l0 + nb < nlines) ? line_off[l0 + nb] : ng;
+    for (int i = threadIdx.x; i < g1 - g0; i += blockDim.x) seg[i] = ps[g0 + i];
+  }
   load_twiddles(tw, twz, N);
   __syncthreads();
-  const double2* ps = psi + (size_t)s * ng;
   for (int it = threadIdx.x; it < nb * N2; it += blockDim.x) {
     const int lb = it / N2, n2 = it - lb * N2;
     const int l = l0 + lb;
@@ -83,7 +97,7 @@ k_zfwd2(const double2* __restrict__ psi, int ng, int s0, const int* __restrict__
       const int i = line_slot(N2 * n1 + n2, N, nn, np);
       double2 v = make_double2(0.0, 0.0);
       if (i >= 0) {
-        v = ps[off + i];
+        v = zseg > 0 ? seg[off - g0 + i] : ps[off + i];
         if (dyp) {  // EES projector: projPsiG = conj(dyp psi) (eesProjGchare)
           const double2 d = dyp[off + i];
           v = make_double2(d.x * v.x - d.y * v.y, -(d.y * v.x + d.x * v.y));
@@ -121,7 +135,7 @@ k_zbwd2(const typename CplxOf<R>::T* __restrict__ zbuf, int ldl, int nlines, con
         const double2* __restrict__ twz, const double2* __restrict__ psi, const double2* __restrict__ fnl,
         double2* __restrict__ force, const double* __restrict__ g2, const double* __restrict__ occ, int ng, int s0,
         double scale, double ecut, double* __restrict__ eke_part, int nblk, const double2* __restrict__ dyp,
-        OaPlaneOut po) {
+        OaPlaneOut po, int zseg) {
   typedef typename CplxOf<R>::T C;
   constexpr int N = N1 * N2;
   typedef PencilLd<N1, N2> L;
@@ -129,9 +143,24 @@ k_zbwd2(const typename CplxOf<R>::T* __restrict__ zbuf, int ldl, int nlines, con
   C* tw = (C*)smem_raw;
   C* s1 = tw + align_up(N, 2);
   double* sred = (double*)(s1 + align_up((size_t)OA_LB * L::ps1, 2));
+  // zseg > 0: psi and F_NL of the block's lines (one contiguous run) staged
+  // with coalesced loads while the z transform runs
+  double2* segp = (double2*)(sred + 64);
+  double2* segf = segp + zseg;
   const int s = s0 + blockIdx.y;
   const int l0 = blockIdx.x * OA_LB;
   const int nb = min(OA_LB, nlines - l0);
+  const int g0 = zseg > 0 ? line_off[l0] : 0;
+  if (zseg > 0 && !dyp) {
+    const int g1 = (l0 + nb < nlines) ? line_off[l0 + nb] : ng;
+    const double2* ps0 = psi + (size_t)s * ng + g0;
+    const double2* fn0 = fnl ? fnl + (size_t)s * ng + g0 : nullptr;
+    for (int i = threadIdx.x; i < g1 - g0; i += blockDim.x) {
+      zp_cp16(segp + i, ps0 + i);
+      if (fn0) zp_cp16(segf + i, fn0 + i);
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+  }
   load_twiddles(tw, twz, N);
   __syncthreads();
   const C* in = zbuf + (size_t)s * N * ldl + l0;
@@ -145,6 +174,7 @@ k_zbwd2(const typename CplxOf<R>::T* __restrict__ zbuf, int ldl, int nlines, con
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) s1[lb * L::ps1 + k1 * L::ls1 + n2] = u[k1];
   }
+  if (zseg > 0 && !dyp) asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   const double2* ps = psi + (size_t)s * ng;
   double2* fs = force + (size_t)s * ng;
@@ -175,10 +205,10 @@ k_zbwd2(const typename CplxOf<R>::T* __restrict__ zbuf, int ldl, int nlines, con
         continue;
       }
       double2 f = make_double2((double)v[k2].x * sc, (double)v[k2].y * sc);
-      if (fn) { const double2 q = fn[idx]; f.x += q.x; f.y += q.y; }
+      if (fn) { const double2 q = zseg > 0 ? segf[idx - g0] : fn[idx]; f.x += q.x; f.y += q.y; }
       const double gg = g2[idx];
       if (gg <= ecut) {
-        const double2 p = ps[idx];
+        const double2 p = zseg > 0 ? segp[idx - g0] : ps[idx];
         const double t = wt * gg;
         f.x -= p.x * t; f.y -= p.y * t;
         ek += t * (p.x * p.x + p.y * p.y);
@@ -514,31 +544,34 @@ int oa_pencil_supported(int n) {
     default: break;                                                  \
   }
 
+// shared memory of the z passes: twiddles, the pass buffer, 64 doubles of
+// reduction scratch, and nseg staged coefficient segments of zseg elements
 template <typename R, int N1, int N2>
-static size_t zpass2_smem() {
+static size_t zpass2_smem(int zseg, int nseg) {
   typedef typename CplxOf<R>::T C;
   return (align_up(N1 * N2, 2) + align_up((size_t)OA_LB * PencilLd<N1, N2>::ps1, 2)) * sizeof(C) +
-         64 * sizeof(double);
+         64 * sizeof(double) + (size_t)nseg * zseg * sizeof(double2);
 }
 
 template <typename R, int N1, int N2>
 static cudaError_t zfwd2_n(cudaStream_t st, const double2* psi, int ng, int s0, int ns, const int* off,
                            const int* nneg, const int* npos, int nlines, void* zbuf, int ldl, const double2* tw,
-                           const double2* dyp) {
+                           const double2* dyp, int zseg) {
   typedef typename CplxOf<R>::T C;
-  const size_t sm = zpass2_smem<R, N1, N2>();
+  const size_t sm = zpass2_smem<R, N1, N2>(zseg, 1);
   cudaError_t e = oa_smem_limit(k_zfwd2<R, N1, N2>);
   if (e != cudaSuccess) return e;
   dim3 grid((nlines + OA_LB - 1) / OA_LB, ns);
-  k_zfwd2<R, N1, N2><<<grid, OA_NTHREADS, sm, st>>>(psi, ng, s0, off, nneg, npos, nlines, (C*)zbuf, ldl, tw, dyp);
+  k_zfwd2<R, N1, N2><<<grid, OA_NTHREADS, sm, st>>>(psi, ng, s0, off, nneg, npos, nlines, (C*)zbuf, ldl, tw, dyp,
+                                                     zseg);
   return cudaGetLastError();
 }
 
 template <typename R>
 static cudaError_t zfwd2(cudaStream_t st, int n, const double2* psi, int ng, int s0, int ns, const int* off,
                          const int* nneg, const int* npos, int nlines, void* zbuf, int ldl, const double2* tw,
-                         const double2* dyp) {
-#define OA_CALL(A, B) zfwd2_n<R, A, B>(st, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp)
+                         const double2* dyp, int zseg) {
+#define OA_CALL(A, B) zfwd2_n<R, A, B>(st, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg)
   OA_PENCIL_DISPATCH(n, OA_CALL)
 #undef OA_CALL
   return cudaErrorNotSupported;
@@ -546,9 +579,10 @@ static cudaError_t zfwd2(cudaStream_t st, int n, const double2* psi, int ng, int
 
 cudaError_t oa_pencil_zfwd(int precision, cudaStream_t st, int n, const double2* psi, int ng, int s0, int ns,
                            const int* off, const int* nneg, const int* npos, int nlines, void* zbuf, int ldl,
-                           const double2* tw, const double2* dyp) {
-  return precision == OA_FP64 ? zfwd2<double>(st, n, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp)
-                              : zfwd2<float>(st, n, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp);
+                           const double2* tw, const double2* dyp, int zseg) {
+  return precision == OA_FP64
+             ? zfwd2<double>(st, n, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg)
+             : zfwd2<float>(st, n, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg);
 }
 
 template <typename R, int N1, int N2>
@@ -556,15 +590,16 @@ static cudaError_t zbwd2_n(cudaStream_t st, const void* zbuf, int ldl, int nline
                            const int* nneg, const int* npos, const double2* tw, const double2* psi,
                            const double2* fnl, double2* force, const double* g2, const double* occ, int ng, int s0,
                            int ns, double scale, double ecut, double* eke_part, int nblk, const double2* dyp,
-                           OaPlaneOut po) {
+                           OaPlaneOut po, int zseg) {
   typedef typename CplxOf<R>::T C;
-  const size_t sm = zpass2_smem<R, N1, N2>();
+  if (dyp) zseg = 0;
+  const size_t sm = zpass2_smem<R, N1, N2>(zseg, fnl ? 2 : 1);
   cudaError_t e = oa_smem_limit(k_zbwd2<R, N1, N2>);
   if (e != cudaSuccess) return e;
   dim3 grid(nblk, ns);
   k_zbwd2<R, N1, N2><<<grid, OA_NTHREADS, sm, st>>>((const C*)zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl,
                                                      force, g2, occ, ng, s0, scale, ecut, eke_part, nblk, dyp,
-                                                     po);
+                                                     po, zseg);
   return cudaGetLastError();
 }
 
@@ -573,10 +608,10 @@ static cudaError_t zbwd2(cudaStream_t st, int n, const void* zbuf, int ldl, int 
                          const int* off, const int* nneg, const int* npos, const double2* tw, const double2* psi,
                          const double2* fnl, double2* force, const double* g2, const double* occ, int ng, int s0,
                          int ns, double scale, double ecut, double* eke_part, int nblk, const double2* dyp,
-                         OaPlaneOut po) {
+                         OaPlaneOut po, int zseg) {
 #define OA_CALL(A, B)                                                                                          \
   zbwd2_n<R, A, B>(st, zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl, force, g2, occ, ng, s0, ns, scale, \
-                   ecut, eke_part, nblk, dyp, po)
+                   ecut, eke_part, nblk, dyp, po, zseg)
   OA_PENCIL_DISPATCH(n, OA_CALL)
 #undef OA_CALL
   return cudaErrorNotSupported;
@@ -586,12 +621,12 @@ cudaError_t oa_pencil_zbwd(int precision, cudaStream_t st, int n, const void* zb
                            const int* lkx, const int* off, const int* nneg, const int* npos, const double2* tw,
                            const double2* psi, const double2* fnl, double2* force, const double* g2,
                            const double* occ, int ng, int s0, int ns, double scale, double ecut, double* eke_part,
-                           int nblk, const double2* dyp, OaPlaneOut po) {
+                           int nblk, const double2* dyp, OaPlaneOut po, int zseg) {
   return precision == OA_FP64
              ? zbwd2<double>(st, n, zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl, force, g2, occ, ng, s0,
-                             ns, scale, ecut, eke_part, nblk, dyp, po)
+                             ns, scale, ecut, eke_part, nblk, dyp, po, zseg)
              : zbwd2<float>(st, n, zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl, force, g2, occ, ng, s0, ns,
-                            scale, ecut, eke_part, nblk, dyp, po);
+                            scale, ecut, eke_part, nblk, dyp, po, zseg);
 }
 
 template <typename R, int MODE, int N1, int N2>

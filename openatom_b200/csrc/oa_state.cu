@@ -357,12 +357,12 @@ int oa_pencil_supported(int n);
 size_t oa_pencil_plane_smem(int precision, int n, int nkx);
 cudaError_t oa_pencil_zfwd(int precision, cudaStream_t st, int n, const double2* psi, int ng, int s0, int ns,
                            const int* off, const int* nneg, const int* npos, int nlines, void* zbuf, int ldl,
-                           const double2* tw, const double2* dyp);
+                           const double2* tw, const double2* dyp, int zseg);
 cudaError_t oa_pencil_zbwd(int precision, cudaStream_t st, int n, const void* zbuf, int ldl, int nlines,
                            const int* lkx, const int* off, const int* nneg, const int* npos, const double2* tw,
                            const double2* psi, const double2* fnl, double2* force, const double* g2,
                            const double* occ, int ng, int s0, int ns, double scale, double ecut, double* eke_part,
-                           int nblk, const double2* dyp, OaPlaneOut po);
+                           int nblk, const double2* dyp, OaPlaneOut po, int zseg);
 cudaError_t oa_pair_plane(int mode, cudaStream_t st, int n, void* zbuf, int nstate, int nz, int ldl, int nlines,
                           const int* cols, int nkx, const double2* tw, const double* occ, const void* vks,
                           double* rho_part, int ngroup, void* psir, int kymax);
@@ -431,7 +431,7 @@ int oa_plane_blocks_per_sm(int precision) {
 cudaError_t oa_launch_state_zfwd(oa_ctx* c, cudaStream_t s, const double2* psi, int s0, int ns) {
   if (oa_pencil_supported(c->nz))
     return oa_pencil_zfwd(c->precision, s, c->nz, psi, c->ng, s0, ns, c->line_off, c->line_nneg, c->line_npos,
-                          c->nlines, c->zbuf, c->ldl, c->tw_z, nullptr);
+                          c->nlines, c->zbuf, c->ldl, c->tw_z, nullptr, c->zseg);
   return c->precision == OA_FP64 ? launch_zfwd<double>(c, s, psi, s0, ns) : launch_zfwd<float>(c, s, psi, s0, ns);
 }
 static cudaError_t pencil_plane(oa_ctx* c, cudaStream_t s, int mode, void* psir) {
@@ -478,7 +478,7 @@ cudaError_t oa_launch_state_zbwd(oa_ctx* c, cudaStream_t s, const double2* psi, 
     const cudaError_t e = oa_pencil_zbwd(c->precision, s, c->nz, c->zbuf, c->ldl, c->nlines, c->line_kx,
                                          c->line_off, c->line_nneg, c->line_npos, c->tw_z, psi, fnl, force, c->g2,
                                          c->occ, c->ng, s0, ns, -2.0 / (double)c->npts, c->ecut_psi, c->eke_part,
-                                         c->nblk_z, nullptr, c->zb_po);
+                                         c->nblk_z, nullptr, c->zb_po, c->zseg);
     c->zb_po_done = (e == cudaSuccess && c->zb_po.P) ? 1 : 0;
     return e;
   }
@@ -498,7 +498,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
   // z pass forward with conj(dyp psi)
   if (pz) {
     err = oa_pencil_zfwd(c->precision, st, e->nc, psi, c->ng, 0, c->nstate, c->line_off, c->line_nneg, c->line_npos,
-                         c->nlines, e->zbuf, c->ldl, e->tw_c, e->dyp);
+                         c->nlines, e->zbuf, c->ldl, e->tw_c, e->dyp, c->zseg);
     if (err != cudaSuccess) return err;
   } else {
     size_t sm = zpass_smem<R>(e->nc);
@@ -544,7 +544,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
   if (pz)
     return oa_pencil_zbwd(c->precision, st, e->nc, e->zbuf, c->ldl, c->nlines, c->line_kx, c->line_off,
                           c->line_nneg, c->line_npos, e->tw_c, psi, nullptr, fnl, c->g2, c->occ, c->ng, 0, c->nstate,
-                          1.0, c->ecut_psi, c->eke_part, c->nblk_z, e->dyp, OaPlaneOut{nullptr, 0, 0, 0});
+                          1.0, c->ecut_psi, c->eke_part, c->nblk_z, e->dyp, OaPlaneOut{nullptr, 0, 0, 0}, 0);
   {
     size_t sm = zpass_smem<R>(e->nc);
     err = oa_smem_limit(k_state_zbwd<R>);
