@@ -27,9 +27,9 @@ cudaError_t oa_launch_ortho_ns(cudaStream_t s, const double* S, int n, double bs
                                double* work, double* T, int* status, double* errv, int grid);
 int oa_integrate_nblk(int ng, int nstate);
 int oa_pair_plane_supported(int n, int nkx, int nlines, int ldl);
-cudaError_t oa_launch_integrate(cudaStream_t s, const double2* F, double2* V, double2* P, const double* cmass,
-                                int ng, int nstate, int r0, int r1, int iend, double dt, int complete_prev,
-                                double* kepart, int nblk);
+cudaError_t oa_launch_integrate(cudaStream_t s, const double2* F, double2* V, double2* P, const double2* P_in,
+                                const int* sel, const double* cmass, int ng, int nstate, int r0, int r1, int iend,
+                                double dt, int complete_prev, double* kepart, int nblk);
 cudaError_t oa_launch_sync_redundant(cudaStream_t s, double2* P, double2* V, const int* partner, int nred, int ng,
                                      int nstate);
 cudaError_t oa_launch_sum_partials_multi(cudaStream_t s, int njob, const double* const* part, const int* n,
@@ -575,19 +575,27 @@ extern "C" oa_status oa_gpu_small_gemm(oa_ctx* c, void* stream, const double* A,
   return OA_OK;
 }
 
-extern "C" oa_status oa_gpu_integrate(oa_ctx* c, void* stream, const double* force, double* vpsi, double* psi,
-                                      double dt, int complete_prev, double* fict_ke_out) {
-  OA_ARG_CHECK(c && force && vpsi && psi, "null argument");
-  cudaStream_t s = (cudaStream_t)stream;
+// psi_in / sel (optional): the coefficients are read from psi_in instead of
+// psi when *sel != 0 (the native step's deferred PsiV copy)
+oa_status oa_integrate_sel(oa_ctx* c, cudaStream_t s, const double* force, double* vpsi, double* psi,
+                           const double* psi_in, const int* sel, double dt, int complete_prev, double* fict_ke_out) {
   oa_ctx_pc* p = pcx(c);
   const int r0 = c->nkx0_red, r1 = c->nkx0_red + c->nkx0_zero, iend = c->nkx0_red + c->nkx0_uni;
-  OA_CUDA_TRY(oa_launch_integrate(s, (const double2*)force, (double2*)vpsi, (double2*)psi, p->cmass, c->ng,
-                                  c->nstate, r0, r1, iend, dt, complete_prev, p->ke_part, p->ke_nblk));
+  OA_CUDA_TRY(oa_launch_integrate(s, (const double2*)force, (double2*)vpsi, (double2*)psi, (const double2*)psi_in,
+                                  sel, p->cmass, c->ng, c->nstate, r0, r1, iend, dt, complete_prev, p->ke_part,
+                                  p->ke_nblk));
   OA_CUDA_TRY(oa_launch_sum_partials(s, p->ke_part, p->ke_nblk, 1, 0, 1.0, p->dev_e + OA_E_FICT));
   if (fict_ke_out)
     OA_CUDA_TRY(cudaMemcpyAsync(fict_ke_out, p->dev_e + OA_E_FICT, sizeof(double), cudaMemcpyDeviceToDevice, s));
   OA_CUDA_TRY(oa_launch_sync_redundant(s, (double2*)psi, (double2*)vpsi, p->partner, c->nkx0_red, c->ng, c->nstate));
   return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_integrate(oa_ctx* c, void* stream, const double* force, double* vpsi, double* psi,
+                                      double dt, int complete_prev, double* fict_ke_out) {
+  OA_ARG_CHECK(c && force && vpsi && psi, "null argument");
+  return oa_integrate_sel(c, (cudaStream_t)stream, force, vpsi, psi, nullptr, nullptr, dt, complete_prev,
+                          fict_ke_out);
 }
 
 __global__ void k_energy_combine(double* e) {
@@ -898,11 +906,12 @@ static oa_status psiv_velocity(oa_ctx* c, cudaStream_t s, const double* psi, dou
   return OA_OK;
 }
 
-// psi = psi_t T (FP64), also written to psi_t when the PsiV flag is set;
-// then, under the flag, the velocity projection and T = I (the next step's
-// check sets or clears the flag).  The native step's orthonormalisation and PsiV reset
-// (Ortho::maxCheck, ortho.C:455-475): same results as oa_gpu_pc_backward
-// followed by oa_gpu_psiv_reset, decided on the device.
+// psi = psi_t T (FP64); then, under the PsiV flag, the velocity projection
+// and T = I (the next step's check sets or clears the flag).  The reset's
+// psi_t = psi is deferred: the next integration reads psi under the flag,
+// and a run ends with oa_psi_t_settle.  The native step's orthonormalisation
+// and PsiV reset (Ortho::maxCheck, ortho.C:455-475): same results as
+// oa_gpu_pc_backward followed by oa_gpu_psiv_reset, decided on the device.
 oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* psi_t, double* psi, double* vpsi,
                             double* Tout, int* flag, int nterm) {
   oa_ctx_pc* p = pcx(c);
@@ -910,10 +919,20 @@ oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* 
   OaPlaneOut po;
   const bool fuse = nterm > 0 && plane_out(c, PL_PSI, n, nterm, &po);
   OA_ALIGN_TRY(oa_dgemm_bwd_ex(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, psi,
-                               nullptr, nullptr, psi_t, flag, fuse ? &po : nullptr));
+                               nullptr, nullptr, nullptr, nullptr, fuse ? &po : nullptr));
   if (fuse) plane_mark(c, PL_PSI, psi, n, po.rows_pad, nterm);
   OA_STEP_CHECK(psiv_velocity(c, s, psi, vpsi, flag, nterm));
   k_copy_cond<<<16, 256, 0, s>>>(Tout, p->eye, (size_t)n * n, flag);
+  OA_CUDA_TRY(cudaGetLastError());
+  return OA_OK;
+}
+
+// psi_t = psi when the last step's PsiV flag is set: the native steps leave
+// that copy to the next integration (which reads psi under the flag), so a
+// run ends with it
+oa_status oa_psi_t_settle(oa_ctx* c, cudaStream_t s, const double* psi, double* psi_t, const int* flag) {
+  const size_t n = (size_t)c->nstate * c->ng * 2;
+  k_copy_cond<<<4 * 148, 256, 0, s>>>(psi_t, psi, n, flag);
   OA_CUDA_TRY(cudaGetLastError());
   return OA_OK;
 }

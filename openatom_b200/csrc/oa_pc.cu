@@ -366,13 +366,16 @@ k_ortho_ns(const double* __restrict__ S, int n, double bscale, double tol, int m
 // kinetic-energy partial per block (kepart[state * gridDim.x + chunk]).
 #define OA_INT_UNROLL 4
 #define OA_INT_CHUNK (256 * OA_INT_UNROLL)
+// P_in (optional) replaces P as the coefficients read when *sel != 0 (the
+// PsiV reset of the previous step: psi(t) = the orthonormal psi).
 __global__ void __launch_bounds__(256)
-k_integrate(const double2* __restrict__ F, double2* __restrict__ V, double2* __restrict__ P,
-            const double* __restrict__ cmass, int ng, int nstate, int r0, int r1, int iend,
-            double dt, int complete_prev, double* __restrict__ kepart) {
+k_integrate(const double2* __restrict__ F, double2* __restrict__ V, double2* P, const double2* P_in,
+            const int* __restrict__ sel, const double* __restrict__ cmass, int ng, int nstate, int r0, int r1,
+            int iend, double dt, int complete_prev, double* __restrict__ kepart) {
   __shared__ double sh[8];
   const double dt2 = 0.5 * dt;
   const size_t base = (size_t)blockIdx.y * ng;
+  const double2* src = (P_in && *sel != 0) ? P_in : P;
   const int i0 = blockIdx.x * OA_INT_CHUNK + threadIdx.x;
   double2 f[OA_INT_UNROLL], v[OA_INT_UNROLL], p[OA_INT_UNROLL];
   double m[OA_INT_UNROLL];
@@ -380,7 +383,7 @@ k_integrate(const double2* __restrict__ F, double2* __restrict__ V, double2* __r
   for (int u = 0; u < OA_INT_UNROLL; ++u) {
     const int i = i0 + 256 * u;
     if (i >= r0 && i < ng) {
-      f[u] = F[base + i]; v[u] = V[base + i]; p[u] = P[base + i]; m[u] = __ldg(cmass + i);
+      f[u] = F[base + i]; v[u] = V[base + i]; p[u] = src[base + i]; m[u] = __ldg(cmass + i);
     }
   }
   double ke = 0.0;
@@ -560,12 +563,12 @@ cudaError_t oa_launch_ortho_ns(cudaStream_t s, const double* S, int n, double bs
   return cudaLaunchCooperativeKernel((void*)k_ortho_ns, dim3(grid), dim3(256), args, 0, s);
 }
 
-cudaError_t oa_launch_integrate(cudaStream_t s, const double2* F, double2* V, double2* P, const double* cmass,
-                                int ng, int nstate, int r0, int r1, int iend, double dt, int complete_prev,
-                                double* kepart, int nblk) {
-  if (nblk != oa_integrate_nblk(ng, nstate)) return cudaErrorInvalidValue;
+cudaError_t oa_launch_integrate(cudaStream_t s, const double2* F, double2* V, double2* P, const double2* P_in,
+                                const int* sel, const double* cmass, int ng, int nstate, int r0, int r1, int iend,
+                                double dt, int complete_prev, double* kepart, int nblk) {
+  if (nblk != oa_integrate_nblk(ng, nstate) || (P_in && !sel)) return cudaErrorInvalidValue;
   const dim3 grid((ng + OA_INT_CHUNK - 1) / OA_INT_CHUNK, nstate);
-  k_integrate<<<grid, 256, 0, s>>>(F, V, P, cmass, ng, nstate, r0, r1, iend, dt, complete_prev, kepart);
+  k_integrate<<<grid, 256, 0, s>>>(F, V, P, P_in, sel, cmass, ng, nstate, r0, r1, iend, dt, complete_prev, kepart);
   return cudaGetLastError();
 }
 

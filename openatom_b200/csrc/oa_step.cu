@@ -38,6 +38,9 @@ oa_status oa_gpu_psiv_reset(oa_ctx* ctx, void* stream, const double* psi, double
 }
 
 int oa_ns_capturable(oa_ctx* c);
+oa_status oa_integrate_sel(oa_ctx* c, cudaStream_t s, const double* force, double* vpsi, double* psi,
+                           const double* psi_in, const int* sel, double dt, int complete_prev, double* fict_ke_out);
+oa_status oa_psi_t_settle(oa_ctx* c, cudaStream_t s, const double* psi, double* psi_t, const int* flag);
 oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* psi_t, double* psi, double* vpsi,
                             double* Tout, int* flag, int nterm);
 
@@ -171,8 +174,8 @@ static oa_status launch_step_a(oa_ctx* c, cudaStream_t s, oa_cp_state* st, int c
     OA_STEP_TRY(oa_gpu_small_gemm(c, s, st->T, w->lam, 1.0, w->gam));
     OA_STEP_TRY(oa_gpu_pc_backward(c, s, w->gam, st->psi, -0.5, -1.0, st->T, w->F, 1.0, w->F2));
   }
-  // integrateModForce
-  OA_STEP_TRY(oa_gpu_integrate(c, s, w->F2, st->vpsi, st->psi_t, st->dt, complete_prev, nullptr));
+  // integrateModForce; psi(t) is psi itself after the previous step's PsiV reset
+  OA_STEP_TRY(oa_integrate_sel(c, s, w->F2, st->vpsi, st->psi_t, st->psi, w->flag, st->dt, complete_prev, nullptr));
   // computeNewPsi: S (FP64)
   OA_STEP_TRY(oa_gpu_pc_forward(c, s, st->psi_t, st->psi_t, 2.0, 0.5, w->S));
   return OA_OK;
@@ -291,6 +294,7 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
       OA_STEP_TRY(r);
     }
   }
+  OA_STEP_TRY(oa_psi_t_settle(c, s, st->psi, st->psi_t, w->flag));
   OA_CUDA_TRY(cudaMemcpyAsync(w->ring_host, w->ring, (size_t)nsteps * OA_REC * sizeof(double),
                               cudaMemcpyDeviceToHost, s));
   OA_CUDA_TRY(cudaMemcpyAsync(w->flag_host, w->flag, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -464,6 +468,8 @@ extern "C" oa_status oa_gpu_cp_run_batch(oa_ctx** ctxs, oa_cp_state** states, in
   // records and flags of every system, one synchronisation
   for (int i = 0; i < nsys && ret == OA_OK; ++i) {
     oa_step_scratch* w = step_scratch(ctxs[i]);
+    ret = oa_psi_t_settle(ctxs[i], s, states[i]->psi, states[i]->psi_t, w->flag);
+    if (ret != OA_OK) break;
     ce = cudaMemcpyAsync(w->ring_host, w->ring, (size_t)nsteps * OA_REC * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (ce == cudaSuccess) ce = cudaMemcpyAsync(w->flag_host, w->flag, 4 * sizeof(int), cudaMemcpyDeviceToHost, s);
     if (ce != cudaSuccess) fail(ce, __LINE__);

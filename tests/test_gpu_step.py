@@ -70,6 +70,35 @@ def test_native_run_matches_steps_and_psiv():
         assert np.array_equal(a.T.cpu().numpy(), d.T.cpu().numpy())
 
 
+def test_native_run_some_psiv_resets():
+    """Steps with and without a PsiV reset in one native run: psi_t, whose
+    reset copy the native steps defer to the next integration, matches the
+    host runner bit for bit after every run length."""
+    from openatom_b200.gpu import CPDriver
+    s = make_system("w8", nstate=16, seed=16, dt=0.5)
+    nsteps = 6
+    tol = None
+    for cand in (1e-4, 3e-4, 1e-3, 3e-3, 1e-2, 3e-2):
+        a = CPDriver(s, "fp64", norb_tol=cand)
+        for _ in range(nsteps):
+            a.step()
+        if 0 < a.n_psiv < nsteps:
+            tol = cand
+            break
+    assert tol is not None, "no tolerance gives a mix of reset and plain steps"
+    for n in (1, 3, nsteps):
+        a = CPDriver(s, "fp64", norb_tol=tol)
+        c = CPDriver(s, "fp64", norb_tol=tol)
+        sc = c.native_state(use_graph=True)
+        ea = [a.step() for _ in range(n)]
+        ec = c.run_native(sc, n)
+        for i in range(n):
+            assert ec[i]["EKE"] == ea[i]["EKE"] and ec[i]["SMAX"] == ea[i]["SMAX"], i
+        assert np.array_equal(a.psi.cpu().numpy(), c.psi.cpu().numpy())
+        assert np.array_equal(a.psi_t.cpu().numpy(), c.psi_t.cpu().numpy())
+        assert np.array_equal(a.v.cpu().numpy(), c.v.cpu().numpy())
+
+
 def test_native_run_positions_and_failure():
     """Per-step host atom positions are copied in before each step; a
     Newton-Schulz failure is reported with the first failing step."""
