@@ -930,9 +930,28 @@ oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* 
 // psi_t = psi when the last step's PsiV flag is set: the native steps leave
 // that copy to the next integration (which reads psi under the flag), so a
 // run ends with it
+// dst = src (n 16-byte pieces) when *cond != 0; four pieces in flight per thread
+__global__ void __launch_bounds__(256) k_copy_cond16(uint4* __restrict__ dst, const uint4* __restrict__ src, size_t n,
+                                                     const int* __restrict__ cond) {
+  if (*cond == 0) return;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    uint4 v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v[u] = __ldcs(src + i + u * stride);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) __stcs(dst + i + u * stride, v[u]);
+  }
+  for (; i < n; i += stride) __stcs(dst + i, __ldcs(src + i));
+}
+
 oa_status oa_psi_t_settle(oa_ctx* c, cudaStream_t s, const double* psi, double* psi_t, const int* flag) {
-  const size_t n = (size_t)c->nstate * c->ng * 2;
-  k_copy_cond<<<4 * 148, 256, 0, s>>>(psi_t, psi, n, flag);
+  const size_t n = (size_t)c->nstate * c->ng;  // double2 coefficients
+  if ((((uintptr_t)psi | (uintptr_t)psi_t) & 15) == 0)
+    k_copy_cond16<<<8 * 148, 256, 0, s>>>((uint4*)psi_t, (const uint4*)psi, n, flag);
+  else
+    k_copy_cond<<<8 * 148, 256, 0, s>>>(psi_t, psi, 2 * n, flag);
   OA_CUDA_TRY(cudaGetLastError());
   return OA_OK;
 }

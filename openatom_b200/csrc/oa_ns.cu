@@ -2,9 +2,10 @@
 // 848-971; cp_lowdin.C:180-265), for up to 128 states:
 //   B = S bscale, A = I; repeat { C = 3I - A B; B <- B C / 2; A <- C A / 2;
 //   err = sqrt(sum (A_old - A_new)^2 / n^2) } until err <= tol or max_iter.
-// The cluster's CTAs own row blocks of A, B and C (global memory, L2
-// resident); each product is a row block times a whole matrix, staged in
-// shared memory and multiplied with FP64 tensor-core MMAs (m8n8k4).  The
+// The cluster's CTAs own the blocks of a 4 x (cs/4) grid over A, B and C
+// (global memory, L2 resident); each product block is a row block times a
+// column block, staged in shared memory and multiplied with FP64
+// tensor-core MMAs (m8n8k4).  The
 // phases are separated by cluster barriers, so the kernel is an ordinary
 // (graph-capturable) launch; every CTA takes the same convergence decision
 // from the same partial sums in the same order.
@@ -27,44 +28,60 @@ __device__ __forceinline__ void nsc_cp16(void* smem, const void* gmem, bool vali
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" :: "r"(sa), "l"(gmem), "r"(nb));
 }
 
-// Z[r0 .. r0+R) = alpha X[r0 .. r0+R) Y + diag I, n x n row-major in global
-// memory; rows and columns padded to npad (multiple of 8) with zeros in
-// shared memory.  err (optional): sum over the block of (Aold - Z)^2.
-__device__ void nsc_gemm_rows(const double* __restrict__ X, const double* __restrict__ Y, int n, int npad, int r0,
-                              int R, double alpha, double diag, double* __restrict__ Z, double* Xs, double* Ys,
-                              const double* __restrict__ Aold, double* err) {
-  const int ld = npad + 4;
+// output blocks of the cluster: rows padded to a multiple of 32, a grid of
+// gr = 4 block rows by gc = cs / 4 block columns (blocks of BR x BC)
+struct NscGeom { int npad, gc, BR, BC; };
+__host__ __device__ inline NscGeom nsc_geom(int n, int cs) {
+  NscGeom g;
+  g.npad = (n + 31) & ~31;
+  g.gc = cs / 4;
+  g.BR = g.npad / 4;
+  g.BC = g.npad / g.gc;
+  return g;
+}
+static inline size_t nsc_smem_bytes(int n, int cs) {
+  const NscGeom g = nsc_geom(n, cs);
+  return ((size_t)g.BR * (g.npad + 4) + (size_t)g.npad * (g.BC + 4)) * sizeof(double);
+}
+
+// Z[r0 .. r0+BR)[c0 .. c0+BC) = alpha X[r0 .. r0+BR)[:] Y[:][c0 .. c0+BC)
+// + diag I, n x n row-major in global memory, zero-padded to npad in shared
+// memory.  err (optional): sum over the block of (Aold - Z)^2.
+__device__ void nsc_gemm_blk(const double* __restrict__ X, const double* __restrict__ Y, int n, const NscGeom& G,
+                             int r0, int c0, double alpha, double diag, double* __restrict__ Z, double* Xs,
+                             double* Ys, const double* __restrict__ Aold, double* err) {
+  const int ldx = G.npad + 4, ldy = G.BC + 4;
   __syncthreads();  // the previous product is done with Xs / Ys
   // 16-byte asynchronous copies (n even), zero-filled outside n x n
-  const int pr = npad / 2;
-  const int rx = (R + 7) & ~7;
-  for (int i = threadIdx.x; i < rx * pr; i += blockDim.x) {
+  const int pr = G.npad / 2;
+  for (int i = threadIdx.x; i < G.BR * pr; i += blockDim.x) {
     const int r = i / pr, k = (i - r * pr) * 2;
-    const bool v = (r < R) && (r0 + r < n) && (k < n);
-    nsc_cp16(Xs + r * ld + k, v ? X + (size_t)(r0 + r) * n + k : X, v);
+    const bool v = (r0 + r < n) && (k < n);
+    nsc_cp16(Xs + r * ldx + k, v ? X + (size_t)(r0 + r) * n + k : X, v);
   }
-  for (int i = threadIdx.x; i < npad * pr; i += blockDim.x) {
-    const int k = i / pr, j = (i - k * pr) * 2;
-    const bool v = (k < n) && (j < n);
-    nsc_cp16(Ys + k * ld + j, v ? Y + (size_t)k * n + j : Y, v);
+  const int pc = G.BC / 2;
+  for (int i = threadIdx.x; i < G.npad * pc; i += blockDim.x) {
+    const int k = i / pc, j = (i - k * pc) * 2;
+    const bool v = (k < n) && (c0 + j < n);
+    nsc_cp16(Ys + k * ldy + j, v ? Y + (size_t)k * n + c0 + j : Y, v);
   }
   asm volatile("cp.async.commit_group;\n" ::);
   asm volatile("cp.async.wait_group 0;\n" ::);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int rt_n = (R + 7) / 8, ct_n = npad / 8;
+  const int rt_n = G.BR / 8, ct_n = G.BC / 8;
   double e = 0.0;
   for (int t = warp; t < rt_n * ct_n; t += NSC_THREADS / 32) {
     const int rt = t % rt_n, ct = t / rt_n;
     double d0 = 0.0, d1 = 0.0;
-    for (int k4 = 0; k4 < npad; k4 += 4) {
-      const double a = Xs[(rt * 8 + (lane >> 2)) * ld + k4 + (lane & 3)];
-      const double b = Ys[(k4 + (lane & 3)) * ld + ct * 8 + (lane >> 2)];
+    for (int k4 = 0; k4 < G.npad; k4 += 4) {
+      const double a = Xs[(rt * 8 + (lane >> 2)) * ldx + k4 + (lane & 3)];
+      const double b = Ys[(k4 + (lane & 3)) * ldy + ct * 8 + (lane >> 2)];
       nsc_dmma(d0, d1, a, b);
     }
     const int i = r0 + rt * 8 + (lane >> 2);
-    const int j = ct * 8 + 2 * (lane & 3);
-    if (rt * 8 + (lane >> 2) < R && i < n) {
+    const int j = c0 + ct * 8 + 2 * (lane & 3);
+    if (i < n) {
       if (j < n) {
         const double v = alpha * d0 + (i == j ? diag : 0.0);
         if (Aold) { const double d = __ldcg(Aold + (size_t)i * n + j) - v; e += d * d; }
@@ -113,17 +130,16 @@ k_ortho_ns_cluster(const double* __restrict__ S, int n, double bscale, double to
   __shared__ double sh[NSC_THREADS / 32];
   const int ncta = (int)cl.num_blocks();
   const int me = (int)cl.block_rank();
-  const int npad = (n + 7) & ~7;
-  const int R = (((n + ncta - 1) / ncta) + 7) & ~7;  // rows per CTA, multiple of 8
-  const int r0 = me * R;
-  const int nr = max(0, min(R, n - r0));
+  const NscGeom G = nsc_geom(n, ncta);
+  const int r0 = (me / G.gc) * G.BR, c0 = (me % G.gc) * G.BC;
   double* Xs = nsc_smem;
-  double* Ys = nsc_smem + (size_t)R * (npad + 4);
+  double* Ys = nsc_smem + (size_t)G.BR * (G.npad + 4);
   const size_t nn = (size_t)n * n;
-  // init: A = I, B = S bscale on the own rows; max |S - I/bscale|
+  // init: A = I, B = S bscale on the own block; max |S - I/bscale|
   double dmax = 0.0;
-  for (int i = threadIdx.x; i < nr * n; i += blockDim.x) {
-    const int r = r0 + i / n, c = i % n;
+  for (int i = threadIdx.x; i < G.BR * G.BC; i += blockDim.x) {
+    const int r = r0 + i / G.BC, c = c0 + i % G.BC;
+    if (r >= n || c >= n) continue;
     const size_t o = (size_t)r * n + c;
     A0[o] = (r == c) ? 1.0 : 0.0;
     B0[o] = S[o] * bscale;
@@ -145,13 +161,13 @@ k_ortho_ns_cluster(const double* __restrict__ S, int n, double bscale, double to
   double err = 1.0;
   while (true) {
     // C = 3I - A B (own rows)
-    nsc_gemm_rows(A, B, n, npad, r0, nr, -1.0, 3.0, Cm, Xs, Ys, nullptr, nullptr);
+    nsc_gemm_blk(A, B, n, G, r0, c0, -1.0, 3.0, Cm, Xs, Ys, nullptr, nullptr);
     __threadfence();
     cl.sync();
     // Bn = B C / 2 ; An = C A / 2 (own rows), with the error partial
     double e = 0.0;
-    nsc_gemm_rows(B, Cm, n, npad, r0, nr, 0.5, 0.0, Bn, Xs, Ys, nullptr, nullptr);
-    nsc_gemm_rows(Cm, A, n, npad, r0, nr, 0.5, 0.0, An, Xs, Ys, A, &e);
+    nsc_gemm_blk(B, Cm, n, G, r0, c0, 0.5, 0.0, Bn, Xs, Ys, nullptr, nullptr);
+    nsc_gemm_blk(Cm, A, n, G, r0, c0, 0.5, 0.0, An, Xs, Ys, A, &e);
     e = nsc_block_sum(e, sh);
     if (threadIdx.x == 0) errpart[me] = e;
     __threadfence();
@@ -166,9 +182,9 @@ k_ortho_ns_cluster(const double* __restrict__ S, int n, double bscale, double to
     // errpart is rewritten only after the next cluster barrier (after the
     // C product), by which time every CTA has read it
   }
-  for (int i = threadIdx.x; i < nr * n; i += blockDim.x) {
-    const size_t o = (size_t)r0 * n + i;
-    T[o] = A[o];
+  for (int i = threadIdx.x; i < G.BR * G.BC; i += blockDim.x) {
+    const int r = r0 + i / G.BC, c = c0 + i % G.BC;
+    if (r < n && c < n) T[(size_t)r * n + c] = A[(size_t)r * n + c];
   }
   if (me == 0 && threadIdx.x == 0) {
     status[0] = it;
@@ -182,10 +198,8 @@ k_ortho_ns_cluster(const double* __restrict__ S, int n, double bscale, double to
 // else 8); 0 when n is too large for it.
 int oa_ns_cluster_size(int n) {
   if (n < 2 || n > NSC_MAXN || (n & 1)) return 0;  // 16-byte row copies need even n
-  const int npad = (n + 7) & ~7;
   for (int cs = 16; cs >= 8; cs /= 2) {
-    const int R = (((n + cs - 1) / cs) + 7) & ~7;
-    const size_t sm = ((size_t)R * (npad + 4) + (size_t)npad * (npad + 4)) * sizeof(double);
+    const size_t sm = nsc_smem_bytes(n, cs);
     if (oa_smem_limit(k_ortho_ns_cluster) != cudaSuccess)
       continue;
     if (cs > 8 && cudaFuncSetAttribute(k_ortho_ns_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
@@ -211,9 +225,8 @@ cudaError_t oa_launch_ortho_ns_cluster(cudaStream_t s, const double* S, int n, d
   const size_t nn = (size_t)n * n;
   double* A0 = work; double* A1 = A0 + nn; double* B0 = A1 + nn; double* B1 = B0 + nn; double* Cm = B1 + nn;
   double* errpart = Cm + nn;
-  const int npad = (n + 7) & ~7;
-  const int R = (((n + cs - 1) / cs) + 7) & ~7;
-  const size_t sm = ((size_t)R * (npad + 4) + (size_t)npad * (npad + 4)) * sizeof(double);
+  if (cs != 8 && cs != 16) return cudaErrorInvalidValue;
+  const size_t sm = nsc_smem_bytes(n, cs);
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
