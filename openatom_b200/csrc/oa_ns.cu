@@ -14,7 +14,7 @@
 
 namespace cg = cooperative_groups;
 
-#define NSC_THREADS 256
+#define NSC_THREADS 512
 #define NSC_MAXN 128
 
 __device__ __forceinline__ void nsc_dmma(double& d0, double& d1, double a, double b) {
@@ -39,31 +39,45 @@ __host__ __device__ inline NscGeom nsc_geom(int n, int cs) {
   g.BC = g.npad / g.gc;
   return g;
 }
+// two staged products
 static inline size_t nsc_smem_bytes(int n, int cs) {
   const NscGeom g = nsc_geom(n, cs);
-  return ((size_t)g.BR * (g.npad + 4) + (size_t)g.npad * (g.BC + 4)) * sizeof(double);
+  return 2 * ((size_t)g.BR * (g.npad + 4) + (size_t)g.npad * (g.BC + 4)) * sizeof(double);
 }
 
-// Z[r0 .. r0+BR)[c0 .. c0+BC) = alpha X[r0 .. r0+BR)[:] Y[:][c0 .. c0+BC)
-// + diag I, n x n row-major in global memory, zero-padded to npad in shared
-// memory.  err (optional): sum over the block of (Aold - Z)^2.
-__device__ void nsc_gemm_blk(const double* __restrict__ X, const double* __restrict__ Y, int n, const NscGeom& G,
-                             int r0, int c0, double alpha, double diag, double* __restrict__ Z, double* Xs,
-                             double* Ys, const double* __restrict__ Aold, double* err) {
+// One or two block products, staged together:
+//   Z_p[r0 .. r0+BR)[c0 .. c0+BC) = alpha_p X_p[r0 .. r0+BR)[:] Y_p[:][c0 .. c0+BC) + diag_p I,
+// n x n row-major in global memory, zero-padded to npad in shared memory
+// (the operands of product p at stage p of Xs / Ys).  err (optional): sum
+// over the block of (Aold - Z_p)^2 for the last product.
+struct NscProd {
+  const double* X;
+  const double* Y;
+  double* Z;
+  double alpha, diag;
+};
+__device__ __forceinline__ void nsc_gemm_blk(NscProd p0, NscProd p1, int np, int n, const NscGeom& G, int r0, int c0,
+                                             double* Xs, double* Ys, const double* __restrict__ Aold, double* err) {
   const int ldx = G.npad + 4, ldy = G.BC + 4;
-  __syncthreads();  // the previous product is done with Xs / Ys
+  const size_t xstage = (size_t)G.BR * ldx, ystage = (size_t)G.npad * ldy;
+  __syncthreads();  // the previous products are done with Xs / Ys
   // 16-byte asynchronous copies (n even), zero-filled outside n x n
-  const int pr = G.npad / 2;
-  for (int i = threadIdx.x; i < G.BR * pr; i += blockDim.x) {
-    const int r = i / pr, k = (i - r * pr) * 2;
-    const bool v = (r0 + r < n) && (k < n);
-    nsc_cp16(Xs + r * ldx + k, v ? X + (size_t)(r0 + r) * n + k : X, v);
-  }
-  const int pc = G.BC / 2;
-  for (int i = threadIdx.x; i < G.npad * pc; i += blockDim.x) {
-    const int k = i / pc, j = (i - k * pc) * 2;
-    const bool v = (k < n) && (c0 + j < n);
-    nsc_cp16(Ys + k * ldy + j, v ? Y + (size_t)k * n + c0 + j : Y, v);
+  const int px = G.npad / 2, pc = G.BC / 2;
+  for (int p = 0; p < np; ++p) {
+    const double* X = p ? p1.X : p0.X;
+    const double* Y = p ? p1.Y : p0.Y;
+    double* xs = Xs + p * xstage;
+    double* ys = Ys + p * ystage;
+    for (int i = threadIdx.x; i < G.BR * px; i += blockDim.x) {
+      const int r = i / px, k = (i - r * px) * 2;
+      const bool v = (r0 + r < n) && (k < n);
+      nsc_cp16(xs + r * ldx + k, v ? X + (size_t)(r0 + r) * n + k : X, v);
+    }
+    for (int i = threadIdx.x; i < G.npad * pc; i += blockDim.x) {
+      const int k = i / pc, j = (i - k * pc) * 2;
+      const bool v = (k < n) && (c0 + j < n);
+      nsc_cp16(ys + k * ldy + j, v ? Y + (size_t)k * n + c0 + j : Y, v);
+    }
   }
   asm volatile("cp.async.commit_group;\n" ::);
   asm volatile("cp.async.wait_group 0;\n" ::);
@@ -71,25 +85,27 @@ __device__ void nsc_gemm_blk(const double* __restrict__ X, const double* __restr
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int rt_n = G.BR / 8, ct_n = G.BC / 8;
   double e = 0.0;
-  for (int t = warp; t < rt_n * ct_n; t += NSC_THREADS / 32) {
-    const int rt = t % rt_n, ct = t / rt_n;
+  for (int t = warp; t < np * rt_n * ct_n; t += NSC_THREADS / 32) {
+    const int p = t / (rt_n * ct_n), tt = t - p * (rt_n * ct_n);
+    const int rt = tt % rt_n, ct = tt / rt_n;
+    const double* xr = Xs + p * xstage + (rt * 8 + (lane >> 2)) * ldx + (lane & 3);
+    const double* yc = Ys + p * ystage + (lane & 3) * ldy + ct * 8 + (lane >> 2);
     double d0 = 0.0, d1 = 0.0;
-    for (int k4 = 0; k4 < G.npad; k4 += 4) {
-      const double a = Xs[(rt * 8 + (lane >> 2)) * ldx + k4 + (lane & 3)];
-      const double b = Ys[(k4 + (lane & 3)) * ldy + ct * 8 + (lane >> 2)];
-      nsc_dmma(d0, d1, a, b);
-    }
+    for (int k4 = 0; k4 < G.npad; k4 += 4) nsc_dmma(d0, d1, xr[k4], yc[k4 * ldy]);
+    const double alpha = p ? p1.alpha : p0.alpha, diag = p ? p1.diag : p0.diag;
+    double* Z = p ? p1.Z : p0.Z;
+    const bool chk = Aold && p == np - 1;
     const int i = r0 + rt * 8 + (lane >> 2);
     const int j = c0 + ct * 8 + 2 * (lane & 3);
     if (i < n) {
       if (j < n) {
         const double v = alpha * d0 + (i == j ? diag : 0.0);
-        if (Aold) { const double d = __ldcg(Aold + (size_t)i * n + j) - v; e += d * d; }
+        if (chk) { const double d = __ldcg(Aold + (size_t)i * n + j) - v; e += d * d; }
         Z[(size_t)i * n + j] = v;
       }
       if (j + 1 < n) {
         const double v = alpha * d1 + (i == j + 1 ? diag : 0.0);
-        if (Aold) { const double d = __ldcg(Aold + (size_t)i * n + j + 1) - v; e += d * d; }
+        if (chk) { const double d = __ldcg(Aold + (size_t)i * n + j + 1) - v; e += d * d; }
         Z[(size_t)i * n + j + 1] = v;
       }
     }
@@ -133,7 +149,7 @@ k_ortho_ns_cluster(const double* __restrict__ S, int n, double bscale, double to
   const NscGeom G = nsc_geom(n, ncta);
   const int r0 = (me / G.gc) * G.BR, c0 = (me % G.gc) * G.BC;
   double* Xs = nsc_smem;
-  double* Ys = nsc_smem + (size_t)G.BR * (G.npad + 4);
+  double* Ys = nsc_smem + 2 * (size_t)G.BR * (G.npad + 4);
   const size_t nn = (size_t)n * n;
   // init: A = I, B = S bscale on the own block; max |S - I/bscale|
   double dmax = 0.0;
@@ -161,13 +177,13 @@ k_ortho_ns_cluster(const double* __restrict__ S, int n, double bscale, double to
   double err = 1.0;
   while (true) {
     // C = 3I - A B (own rows)
-    nsc_gemm_blk(A, B, n, G, r0, c0, -1.0, 3.0, Cm, Xs, Ys, nullptr, nullptr);
+    nsc_gemm_blk(NscProd{A, B, Cm, -1.0, 3.0}, NscProd{A, B, Cm, -1.0, 3.0}, 1, n, G, r0, c0, Xs, Ys, nullptr,
+                 nullptr);
     __threadfence();
     cl.sync();
     // Bn = B C / 2 ; An = C A / 2 (own rows), with the error partial
     double e = 0.0;
-    nsc_gemm_blk(B, Cm, n, G, r0, c0, 0.5, 0.0, Bn, Xs, Ys, nullptr, nullptr);
-    nsc_gemm_blk(Cm, A, n, G, r0, c0, 0.5, 0.0, An, Xs, Ys, A, &e);
+    nsc_gemm_blk(NscProd{B, Cm, Bn, 0.5, 0.0}, NscProd{Cm, A, An, 0.5, 0.0}, 2, n, G, r0, c0, Xs, Ys, A, &e);
     e = nsc_block_sum(e, sh);
     if (threadIdx.x == 0) errpart[me] = e;
     __threadfence();
