@@ -898,11 +898,32 @@ static oa_status psiv_velocity(oa_ctx* c, cudaStream_t s, const double* psi, dou
       return OA_OK;
     }
   }
-  OA_ALIGN_TRY(oa_dgemm_fwd(s, psi, vpsi, n, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, p->mat_a, cond));
+  cudaError_t e =
+      oa_dgemm_fwd(s, psi, vpsi, n, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, p->mat_a, cond);
+  // above 128 states the general kernels, which know no device flag, run
+  // unconditionally; what they produce is used only under the flag
+  if (e == cudaErrorNotSupported)
+    e = oa_launch_pc_fwd(s, psi, vpsi, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, p->mat_a);
+  OA_ALIGN_TRY(e);
   k_sym_quarter_cond<<<grid, blk, 0, s>>>(p->mat_a, n, p->mat_x, cond);
   OA_CUDA_TRY(cudaGetLastError());
-  OA_ALIGN_TRY(oa_dgemm_bwd_ex(s, p->mat_x, psi, -1.0, -1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0,
-                               vpsi, cond, vpsi, nullptr, nullptr));
+  e = oa_dgemm_bwd_ex(s, p->mat_x, psi, -1.0, -1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, vpsi,
+                      cond, vpsi, nullptr, nullptr);
+  if (e == cudaErrorNotSupported) {
+    // v - X psi as the two-term product (-X) psi + I v into scratch, then
+    // copied over v (under the flag)
+    OA_CUDA_TRY(oa_launch_pc_bwd(s, p->mat_x, psi, -1.0, -1.0, p->eye, vpsi, 1.0, n, 2L * c->ng, 2L * c->nkx0,
+                                 p->vtmp));
+    const size_t nd = (size_t)n * c->ng * 2;
+    if (cond) {
+      k_copy_cond<<<8 * 148, 256, 0, s>>>(vpsi, p->vtmp, nd, cond);
+      OA_CUDA_TRY(cudaGetLastError());
+    } else {
+      OA_CUDA_TRY(cudaMemcpyAsync(vpsi, p->vtmp, nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    return OA_OK;
+  }
+  OA_ALIGN_TRY(e);
   return OA_OK;
 }
 
@@ -918,9 +939,18 @@ oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* 
   const int n = c->nstate;
   OaPlaneOut po;
   const bool fuse = nterm > 0 && plane_out(c, PL_PSI, n, nterm, &po);
-  OA_ALIGN_TRY(oa_dgemm_bwd_ex(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, psi,
-                               nullptr, nullptr, nullptr, nullptr, fuse ? &po : nullptr));
-  if (fuse) plane_mark(c, PL_PSI, psi, n, po.rows_pad, nterm);
+  cudaError_t e = oa_dgemm_bwd_ex(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, psi,
+                                  nullptr, nullptr, nullptr, nullptr, fuse ? &po : nullptr);
+  if (e == cudaErrorNotSupported) {
+    // above 128 states: the general kernel, and the psi planes are split
+    // again when a product needs them
+    e = oa_launch_pc_bwd(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, 2L * c->ng, 2L * c->nkx0, psi);
+    OA_CUDA_TRY(e);
+    pcx(c)->pl_key[PL_PSI].valid = false;
+  } else {
+    OA_ALIGN_TRY(e);
+    if (fuse) plane_mark(c, PL_PSI, psi, n, po.rows_pad, nterm);
+  }
   OA_STEP_CHECK(psiv_velocity(c, s, psi, vpsi, flag, nterm));
   k_copy_cond<<<16, 256, 0, s>>>(Tout, p->eye, (size_t)n * n, flag);
   OA_CUDA_TRY(cudaGetLastError());

@@ -431,39 +431,45 @@ __global__ void k_sync_redundant(double2* __restrict__ P, double2* __restrict__ 
   }
 }
 
-__global__ void k_sum_partials(const double* __restrict__ part, int n, int stride, int off, double scale,
-                               double* __restrict__ out) {
-  // one block: out[0] = scale * sum_i part[i*stride + off]
-  __shared__ double sh[32];
-  double s = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s += part[(size_t)i * stride + off];
+// sum of part[i * stride + off] over i < n in one block: each thread keeps
+// four partial sums with four loads in flight, combined in a fixed order
+__device__ __forceinline__ double sum_strided_block(const double* __restrict__ part, int n, int stride, int off,
+                                                    double* sh) {
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  const int nb = blockDim.x;
+  int i = threadIdx.x;
+  for (; i + 3 * nb < n; i += 4 * nb) {
+    const double v0 = part[(size_t)i * stride + off];
+    const double v1 = part[(size_t)(i + nb) * stride + off];
+    const double v2 = part[(size_t)(i + 2 * nb) * stride + off];
+    const double v3 = part[(size_t)(i + 3 * nb) * stride + off];
+    a0 += v0; a1 += v1; a2 += v2; a3 += v3;
+  }
+  for (; i < n; i += nb) a0 += part[(size_t)i * stride + off];
+  double s = (a0 + a1) + (a2 + a3);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
+  double t = 0.0;
+  if (threadIdx.x == 0)
     for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
-    out[0] = scale * t;
-  }
+  return t;
+}
+
+__global__ void k_sum_partials(const double* __restrict__ part, int n, int stride, int off, double scale,
+                               double* __restrict__ out) {
+  // one block: out[0] = scale * sum_i part[i*stride + off]
+  __shared__ double sh[32];
+  const double t = sum_strided_block(part, n, stride, off, sh);
+  if (threadIdx.x == 0) out[0] = scale * t;
 }
 
 __global__ void k_sum_partials_multi(SumJobs J) {
   __shared__ double sh[32];
   const int b = blockIdx.x;
-  const double* part = J.part[b];
-  const int n = J.n[b], stride = J.stride[b], off = J.off[b];
-  double s = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s += part[(size_t)i * stride + off];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
-    J.out[b][0] = J.scale[b] * t;
-  }
+  const double t = sum_strided_block(J.part[b], J.n[b], J.stride[b], J.off[b], sh);
+  if (threadIdx.x == 0) J.out[b][0] = J.scale[b] * t;
 }
 
 // ---------------------------------------------------------------------------
@@ -530,7 +536,7 @@ cudaError_t oa_launch_sum_partials_multi(cudaStream_t s, int njob, const double*
     J.part[b] = part[b]; J.out[b] = out[b]; J.scale[b] = scale[b];
     J.n[b] = n[b]; J.stride[b] = stride[b]; J.off[b] = off[b];
   }
-  k_sum_partials_multi<<<njob, 256, 0, s>>>(J);
+  k_sum_partials_multi<<<njob, 512, 0, s>>>(J);
   return cudaGetLastError();
 }
 
@@ -583,6 +589,6 @@ cudaError_t oa_launch_sync_redundant(cudaStream_t s, double2* P, double2* V, con
 
 cudaError_t oa_launch_sum_partials(cudaStream_t s, const double* part, int n, int stride, int off, double scale,
                                    double* out) {
-  k_sum_partials<<<1, 256, 0, s>>>(part, n, stride, off, scale, out);
+  k_sum_partials<<<1, 512, 0, s>>>(part, n, stride, off, scale, out);
   return cudaGetLastError();
 }

@@ -467,9 +467,11 @@ k_umma_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double 
 }
 
 // ---------------------------------------------------------------------------
+// N tile: the whole N up to 160 (one tile; the two-stage ring of three
+// planes still fits shared memory), else tiles of 128
 static int umma_nb(int n) {
   int nb = (n + 15) / 16 * 16;
-  if (nb > 256) nb = 256;
+  if (nb > 160) nb = 128;
   if (nb < 16) nb = 16;
   return nb;
 }

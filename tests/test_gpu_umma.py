@@ -3,7 +3,9 @@
 Tolerances (max |err| / max |ref|): 3-term split (6 products) 1e-5,
 2-term split (3 products) 2e-4 -- the split depth sets the operand accuracy
 (2^-24 / 2^-16); FP32 accumulation inside each K block adds up to a few
-1e-6 when a CTA accumulates a long K range (few K blocks per output tile)."""
+1e-6 when a CTA accumulates a long K range (few K blocks per output tile).
+Above 160 states the output has 16 tiles or more sharing the SMs, so each
+CTA sums a K range several times longer in FP32: twice the tolerance."""
 import numpy as np
 import pytest
 
@@ -18,7 +20,12 @@ def rel(a, b):
     return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
 
 
-@pytest.fixture(scope="module", params=[("w4", None), ("w8", 32), ("w8", 48), ("w8", 100), ("w8", 128), ("w8", 160)])
+def tol(nterm, n):
+    return TOL[nterm] * (2.0 if n > 160 else 1.0)
+
+
+@pytest.fixture(scope="module", params=[("w4", None), ("w8", 32), ("w8", 48), ("w8", 100), ("w8", 128), ("w8", 160),
+                                              ("w8", 512)])
 def case(request):
     import torch
     from openatom_b200.gpu import CPContext
@@ -50,7 +57,7 @@ def test_forward_mixed(case, nterm):
         ctx.pc_forward(a, b, al, w, ref)
         ctx.pc_forward_mixed(a, b, al, w, got, nterm=nterm)
         ctx.check()
-        assert rel(got.cpu().numpy(), ref.cpu().numpy()) < TOL[nterm]
+        assert rel(got.cpu().numpy(), ref.cpu().numpy()) < tol(nterm, n)
 
 
 @pytest.mark.parametrize("nterm", [3, 2])
@@ -70,11 +77,11 @@ def test_backward_mixed(case, nterm):
     ctx.pc_backward(Gg, P, -0.5, -1.0, ref, M2=Tg, X2=Fg, a2=1.0)
     ctx.pc_backward_mixed(Gg, P, -0.5, -1.0, got, M2=Tg, X2=Fg, a2=1.0, nterm=nterm)
     ctx.check()
-    assert rel(got.cpu().numpy(), ref.cpu().numpy()) < TOL[nterm]
+    assert rel(got.cpu().numpy(), ref.cpu().numpy()) < tol(nterm, n)
     ctx.pc_backward(Tg, P, 1.0, 1.0, ref)
     ctx.pc_backward_mixed(Tg, P, 1.0, 1.0, got, nterm=nterm)
     ctx.check()
-    assert rel(got.cpu().numpy(), ref.cpu().numpy()) < TOL[nterm]
+    assert rel(got.cpu().numpy(), ref.cpu().numpy()) < tol(nterm, n)
 
 
 def test_nonlocal_mixed(case):
