@@ -802,7 +802,11 @@ void oa_planes_force_end(oa_ctx* c, const double* F) {
 // psi planes split afresh (start of a native run)
 oa_status oa_planes_psi_refresh(oa_ctx* c, cudaStream_t s, const double* psi, int nt) {
   OaPlaneOut po;
-  if (!plane_out(c, PL_PSI, c->nstate, nt, &po)) return OA_OK;
+  if (!plane_out(c, PL_PSI, c->nstate, nt, &po)) {
+    // no fused psi planes at this size: whatever the slot holds is stale
+    pcx(c)->pl_key[PL_PSI].valid = false;
+    return OA_OK;
+  }
   OA_CUDA_TRY(oa_split_kc(s, nt, psi, c->nstate, po.rows_pad, 2L * c->ng, 2L * c->ng, 0, 1.0, (bf16*)po.P, po.ldp));
   plane_mark(c, PL_PSI, psi, c->nstate, po.rows_pad, nt);
   return OA_OK;
@@ -938,7 +942,7 @@ oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* 
   oa_ctx_pc* p = pcx(c);
   const int n = c->nstate;
   OaPlaneOut po;
-  const bool fuse = nterm > 0 && plane_out(c, PL_PSI, n, nterm, &po);
+  bool fuse = nterm > 0 && plane_out(c, PL_PSI, n, nterm, &po);
   cudaError_t e = oa_dgemm_bwd_ex(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, psi,
                                   nullptr, nullptr, nullptr, nullptr, fuse ? &po : nullptr);
   if (e == cudaErrorNotSupported) {
@@ -946,11 +950,14 @@ oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* 
     // again when a product needs them
     e = oa_launch_pc_bwd(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, 2L * c->ng, 2L * c->nkx0, psi);
     OA_CUDA_TRY(e);
-    pcx(c)->pl_key[PL_PSI].valid = false;
+    fuse = false;
   } else {
     OA_ALIGN_TRY(e);
-    if (fuse) plane_mark(c, PL_PSI, psi, n, po.rows_pad, nterm);
   }
+  // psi changed: its planes are current only when this pass wrote them (the
+  // nonlocal products split psi again otherwise)
+  if (fuse) plane_mark(c, PL_PSI, psi, n, po.rows_pad, nterm);
+  else pcx(c)->pl_key[PL_PSI].valid = false;
   OA_STEP_CHECK(psiv_velocity(c, s, psi, vpsi, flag, nterm));
   k_copy_cond<<<16, 256, 0, s>>>(Tout, p->eye, (size_t)n * n, flag);
   OA_CUDA_TRY(cudaGetLastError());

@@ -275,7 +275,7 @@ cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m
 
 __device__ __forceinline__ void db_load_slab(double* ms, double* xs, const double* __restrict__ M,
                                              const double* __restrict__ X, int nj, int nk, long ncol, int k0,
-                                             long c0) {
+                                             long c0, int j0) {
   if (nj & 1) {
     // odd nj: the rows of M are not 16-byte aligned; 8-byte pieces, 8 per thread
 #pragma unroll
@@ -283,8 +283,8 @@ __device__ __forceinline__ void db_load_slab(double* ms, double* xs, const doubl
       const int piece = threadIdx.x + q * DB_THREADS;
       const int kk = piece >> 7, jj = piece & 127;
       const int k = k0 + kk;
-      const bool valid = (k < nk) && (jj < nj);
-      dg_cp8(ms + kk * DB_LDM + jj, valid ? M + (size_t)k * nj + jj : M, valid);
+      const bool valid = (k < nk) && (j0 + jj < nj);
+      dg_cp8(ms + kk * DB_LDM + jj, valid ? M + (size_t)k * nj + j0 + jj : M, valid);
     }
   } else {
     // M rows k0..k0+15, all 128 j: 16 x 64 pieces of 16 B = 1024 -> 4 per thread
@@ -293,8 +293,8 @@ __device__ __forceinline__ void db_load_slab(double* ms, double* xs, const doubl
       const int piece = threadIdx.x + q * DB_THREADS;
       const int kk = piece >> 6, jj = (piece & 63) * 2;
       const int k = k0 + kk;
-      const bool valid = (k < nk) && (jj < nj);
-      dg_cp16(ms + kk * DB_LDM + jj, valid ? M + (size_t)k * nj + jj : M, valid);
+      const bool valid = (k < nk) && (j0 + jj < nj);
+      dg_cp16(ms + kk * DB_LDM + jj, valid ? M + (size_t)k * nj + j0 + jj : M, valid);
     }
   }
   // X rows k0..k0+15, columns c0..c0+63: 16 x 32 pieces = 512 -> 2 per thread
@@ -325,6 +325,7 @@ k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double
   double* Ms = db_smem;
   double* Xs = db_smem + DB_STAGES * DB_MSLAB;
   const long c0 = (long)blockIdx.x * DB_TC;
+  const int j0 = blockIdx.y * DB_TJ;  // rows j0 .. j0 + 127 of the output
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wj = (warp >> 1) * 32, wc = (warp & 1) * 32;
   const int nsl = (nk + DB_KS - 1) / DB_KS;
@@ -338,7 +339,8 @@ k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double
     const int st = s % DB_STAGES;
     const bool second = TWO && s >= nsl;
     const int k0 = (second ? s - nsl : s) * DB_KS;
-    db_load_slab(Ms + st * DB_MSLAB, Xs + st * DB_XSLAB, second ? M2 : M1, second ? X2 : X1, nj, nk, ncol, k0, c0);
+    db_load_slab(Ms + st * DB_MSLAB, Xs + st * DB_XSLAB, second ? M2 : M1, second ? X2 : X1, nj, nk, ncol, k0, c0,
+                 j0);
   };
   // a1(c) for this thread's output columns
   auto scale_a1 = [&]() {
@@ -384,7 +386,7 @@ k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double
   if (!TWO) scale_a1();
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
-    const int j = wj + a * 8 + (lane >> 2);
+    const int j = j0 + wj + a * 8 + (lane >> 2);
     if (j >= nj) continue;
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
@@ -433,16 +435,17 @@ k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double
     for (int i = threadIdx.x; i < po.nt * DB_TJ * (DB_TC / 8); i += DB_THREADS) {
       const int q = i / (DB_TJ * (DB_TC / 8)), rem = i - q * (DB_TJ * (DB_TC / 8));
       const int jl = rem / (DB_TC / 8), ch = rem - jl * (DB_TC / 8);
-      if (jl >= nj || c0 + ch * 8 >= po.ldp) continue;
-      *reinterpret_cast<uint4*>((__nv_bfloat16*)po.P + q * pstride + oa_plane_at(jl, c0 + ch * 8, po.rows_pad)) =
+      if (j0 + jl >= nj || c0 + ch * 8 >= po.ldp) continue;
+      *reinterpret_cast<uint4*>((__nv_bfloat16*)po.P + q * pstride +
+                                oa_plane_at(j0 + jl, c0 + ch * 8, po.rows_pad)) =
           *reinterpret_cast<const uint4*>(sp + ((size_t)q * DB_TJ + jl) * SPLD + ch * 8);
     }
   }
 }
 
 // Returns cudaErrorNotSupported when the shapes or pointers do not allow the
-// copies (nj > 128, odd ncol, unaligned pointers); an odd nj moves M in
-// 8-byte pieces.
+// copies (odd ncol, unaligned pointers); an odd nj moves M in 8-byte pieces.
+// Outputs of more than 128 rows run as row tiles of 128 (grid y).
 // po (optional): bf16 planes of out written in the same pass (ncol even).
 cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
                             const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
@@ -454,9 +457,10 @@ cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, 
   const uintptr_t al = (uintptr_t)M1 | (uintptr_t)X1 | (uintptr_t)out | (uintptr_t)(M2 ? M2 : M1) |
                        (uintptr_t)(X2 ? X2 : X1) | (uintptr_t)yadd | (uintptr_t)out2;
   if (out2 && !cond2) return cudaErrorInvalidValue;
-  if (nj > DB_TJ || (ncol & 1) || (al & 15) || nk <= 0 || (M2 && !X2)) return cudaErrorNotSupported;
+  if (nj <= 0 || (ncol & 1) || (al & 15) || nk <= 0 || (M2 && !X2)) return cudaErrorNotSupported;
   const size_t sm = (size_t)DB_STAGES * (DB_MSLAB + DB_XSLAB) * sizeof(double);
-  dim3 grid((unsigned)((ncol + DB_TC - 1) / DB_TC));
+  // column tiles of 64 by row tiles of 128
+  dim3 grid((unsigned)((ncol + DB_TC - 1) / DB_TC), (unsigned)((nj + DB_TJ - 1) / DB_TJ));
   cudaError_t e;
   if (M2) {
     e = oa_smem_limit(k_dgemm_bwd<true>);

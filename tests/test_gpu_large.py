@@ -1,7 +1,7 @@
 """State counts of the large single-system configuration (up to 512
 states): the cooperative Newton-Schulz kernel that runs above 128 states,
-against an eigendecomposition in FP64, and the native step's general-kernel
-path above 128 states against the host runner."""
+against an eigendecomposition in FP64, the native step above 128 states
+against the host runner, and the mixed form against FP64 at 256 states."""
 import numpy as np
 import pytest
 
@@ -43,10 +43,9 @@ def test_ortho_invsqrt_many_states(nst):
 
 
 def test_native_run_many_states():
-    """Above 128 states the native step runs Psi T and the PsiV projection
-    through the general FP64 kernels (the projection computed whole and kept
-    under the device flag): it reproduces the host runner bit for bit, with
-    a reset in every step."""
+    """Above 128 states (the cooperative Newton-Schulz kernel between two
+    graphs, FP64 products in row tiles of 128) the native step reproduces
+    the host runner bit for bit, with a reset in every step."""
     from openatom_b200.gpu import CPDriver
     s = make_system("w8", nstate=130, seed=22, dt=0.5)
     a = CPDriver(s, "fp64", norb_tol=1e-14)
