@@ -47,6 +47,7 @@ cudaError_t oa_split_kc(cudaStream_t s, int nt, const double* X, int rows, int r
                         long kx0_cols, double w_kx0, __nv_bfloat16* P, long ldp, const int* cond = nullptr);
 int oa_tg_rows_pad(int rows, int box);
 int oa_tg_nb(int n);
+int oa_tg_nb_fwd(int n);
 cudaError_t oa_tfwd(cudaStream_t s, int nt, const __nv_bfloat16* PA, int rows_a, const __nv_bfloat16* PB, int rows_b,
                     int m, int n, long K, long ldp, double alpha, float* part, int max_kb, double* C, int* err_flag,
                     int nsm, const int* cond = nullptr);
@@ -821,7 +822,7 @@ static cudaError_t mixed_fwd(oa_ctx* c, cudaStream_t s, int nt, const double* A,
                              const int* cond = nullptr) {
   oa_ctx_pc* p = pcx(c);
   const int mx = c->nstate > c->natm_nl ? c->nstate : c->natm_nl;
-  const int nb = oa_tg_nb(n);
+  const int nb = oa_tg_nb_fwd(n);
   const int ra = oa_tg_rows_pad(m, 128), rb = nb ? oa_tg_rows_pad(n, nb) : 0;
   if (nb && m <= mx && n <= mx && K <= p->pl_ld && ra <= p->pl_rows && rb <= p->pl_rows) {
     const bool same = B == A && (w_kx0 == 1.0 || kx0_cols == 0) && ra % nb == 0;
@@ -885,8 +886,9 @@ static oa_status psiv_velocity(oa_ctx* c, cudaStream_t s, const double* psi, dou
   oa_ctx_pc* p = pcx(c);
   const int n = c->nstate;
   dim3 grid((n + 15) / 16, (n + 15) / 16), blk(16, 16);
-  if (nterm) {
-    // split-BF16: A = v carries the S weights (sym(v psi^T) = sym(psi v^T)),
+  if (nterm && oa_tg_nb(n)) {
+    // split-BF16 (up to 128 states, where both products run on the planes):
+    // A = v carries the S weights (sym(v psi^T) = sym(psi v^T)),
     // so the psi planes serve both products; v -= X psi with v added in FP64
     cudaError_t e = mixed_fwd(c, s, nterm, vpsi, psi, n, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->mat_a, PL_OTHER,
                               PL_PSI, cond);

@@ -542,6 +542,8 @@ cudaError_t oa_split_kc(cudaStream_t s, int nt, const double* X, int rows, int r
 // rows of the planes of an operand the kernels read in boxes of `box` rows
 int oa_tg_rows_pad(int rows, int box) { return (rows + box - 1) / box * box; }
 int oa_tg_nb(int n) { return n <= 64 ? 64 : (n <= 128 ? 128 : 0); }
+// N tile of the forward product: whole N up to 128, else tiles of 128
+int oa_tg_nb_fwd(int n) { return n <= 128 ? oa_tg_nb(n) : 128; }
 
 static int tg_nb(int n) { return n <= 64 ? 64 : (n <= 128 ? 128 : 0); }
 // forward stages carry TG_KF columns of K, backward stages TG_KS rows of k
@@ -561,7 +563,7 @@ static int tg_stages(int nt, int nb, bool fwd) {
 cudaError_t oa_tfwd(cudaStream_t s, int nt, const bf16* PA, int rows_a, const bf16* PB, int rows_b, int m, int n,
                     long K, long ldp, double alpha, float* part, int max_kb, double* C, int* err_flag, int nsm,
                     const int* cond) {
-  const int nb = tg_nb(n);
+  const int nb = oa_tg_nb_fwd(n);
   if (nb == 0 || m > rows_a || n > rows_b) return cudaErrorNotSupported;
   const int stages = tg_stages(nt, nb, true);
   if (stages < 2) return cudaErrorNotSupported;
