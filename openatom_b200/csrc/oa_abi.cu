@@ -886,19 +886,23 @@ static oa_status psiv_velocity(oa_ctx* c, cudaStream_t s, const double* psi, dou
   oa_ctx_pc* p = pcx(c);
   const int n = c->nstate;
   dim3 grid((n + 15) / 16, (n + 15) / 16), blk(16, 16);
-  if (nterm && oa_tg_nb(n)) {
-    // split-BF16 (up to 128 states, where both products run on the planes):
-    // A = v carries the S weights (sym(v psi^T) = sym(psi v^T)),
-    // so the psi planes serve both products; v -= X psi with v added in FP64
+  if (nterm) {
+    // split-BF16: A = v carries the S weights (sym(v psi^T) = sym(psi v^T)),
+    // so the psi planes serve both products; v -= X psi with v added in FP64.
+    // Above 128 states the backward product (on the planes only up to 128)
+    // runs in FP64 with the same flag and in-place add.
     cudaError_t e = mixed_fwd(c, s, nterm, vpsi, psi, n, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->mat_a, PL_OTHER,
                               PL_PSI, cond);
     if (e == cudaSuccess) {
       k_sym_quarter_cond<<<grid, blk, 0, s>>>(p->mat_a, n, p->mat_x, cond);
       e = cudaGetLastError();
     }
-    if (e == cudaSuccess)
+    if (e == cudaSuccess && oa_tg_nb(n))
       e = mixed_bwd(c, s, nterm, p->mat_x, psi, -1.0, -1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0,
                     vpsi, PL_PSI, PL_OTHER, vpsi, cond);
+    else if (e == cudaSuccess)
+      e = oa_dgemm_bwd_ex(s, p->mat_x, psi, -1.0, -1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, vpsi,
+                          cond, vpsi, nullptr, nullptr);
     if (e != cudaErrorNotSupported) {
       OA_CUDA_TRY(e);
       return OA_OK;
