@@ -44,13 +44,15 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="w32")
-    ap.add_argument("--quench", type=int, default=60)
+    ap.add_argument("--quench", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--batch", type=int, default=48,
                     help="systems of the batching form measured beside the headline (0: skip)")
     ap.add_argument("--large", type=int, default=1,
                     help="also time the 128 H2O / 512-state / 160^3 system in the mixed form (0: skip)")
+    ap.add_argument("--drift-steps", type=int, default=1000,
+                    help="steps of the 8-water precision run (energy drift, mixed vs FP64; 0: skip)")
     return ap.parse_args()
 
 
@@ -188,8 +190,29 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+TERMS = ("EKE", "EHART", "EEXT", "EEXC", "ENL")
+NORB_TOL = 0.003
+
+
 def total_energy(en):
-    return en["EKE"] + en["EHART"] + en["EEXT"] + en["EEXC"]
+    """E_KS + E_NL of the orthonormal states (the Ewald energy of the fixed
+    ions is a constant and left out)."""
+    return sum(en[k] for k in TERMS)
+
+
+def conserved_energy(en):
+    """The CP constant of motion with fixed ions: E_KS + E_NL + fictitious KE."""
+    return total_energy(en) + en["FICT_KE"]
+
+
+def workload_config(args, sysm):
+    """The config object both arms print for the headline workload."""
+    return {"workload": f"{args.config}: {sysm.natm // 3} H2O, {sysm.nstate} states, {sysm.ecut_ry:g} Ry, "
+                        f"{sysm.nfft[0]}^3, ng={sysm.ng}",
+            "nstate": sysm.nstate, "grid": list(sysm.nfft), "dt": sysm.dt, "fict_mass": sysm.cmass0,
+            "quench_steps": args.quench, "norb_tol": NORB_TOL, "seed": args.seed,
+            "l2": "per-step working set > 126 MB L2 (z-line buffer alone 244 MB in FP32); no explicit flush",
+            "parallelism": f"replicas x{args.gpus}"}
 
 
 # ----------------------------------------------------------------------------
@@ -197,37 +220,83 @@ def total_energy(en):
 # arm does bench.py execute oracle code)
 # ----------------------------------------------------------------------------
 
-def cpu_step_rate(sysm, nsteps, warm):
+def cpu_info():
+    model = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "threads": os.cpu_count() or 1,
+            "fft": "scipy.fft (pocketfft/ducc, r2c/c2r) with all host threads", "gemm": "numpy BLAS"}
+
+
+def oracle_steps(sysm, psi0, nsteps, warm=0):
+    """nsteps oracle CP steps from psi0 (None: the seeded start) with the
+    PsiV tolerance of the GPU arm.  Returns (steps/s, seconds, records)."""
     from oracle import cp_oracle as O
     O.set_fft_workers(os.cpu_count() or 1)
     st = O.CPState(sysm)
+    if psi0 is not None:
+        st.psi_t = psi0.copy()
+        st.psi = psi0.copy()
     for _ in range(warm):
-        O.cp_step(st, sysm)
+        O.cp_step(st, sysm, norb_tol=NORB_TOL)
     t0 = time.perf_counter()
-    for _ in range(nsteps):
-        O.cp_step(st, sysm)
+    recs = [O.cp_step(st, sysm, norb_tol=NORB_TOL) for _ in range(nsteps)]
     dt = time.perf_counter() - t0
-    return nsteps / dt, dt
+    return nsteps / dt, dt, recs
+
+
+def per_term_errors(got, ref, natm):
+    """max over steps of |got - ref| per energy term (Ha) and of the total per atom."""
+    out = {k: max(abs(g[k] - r[k]) for g, r in zip(got, ref)) for k in TERMS}
+    out["total_per_atom"] = max(abs(total_energy(g) - total_energy(r)) for g, r in zip(got, ref)) / natm
+    out["steps"] = min(len(got), len(ref))
+    return out
 
 
 def run_reference(args):
+    """The reference arm: the FP64 oracle port of the CP step on the host
+    cores, from the same seeded start quenched the same way (damped CP,
+    args.quench steps), then W + K CPMD steps with the same PsiV tolerance."""
     ws, rk, lr = dist_env()
     if rk != 0:
         return 0
+    from oracle import cp_oracle as O
     sysm = make_sys(args.config, args.seed)
-    k = max(1, min(args.steps, 3))
-    w = min(args.warmup, 1)
-    rate, dt = cpu_step_rate(sysm, k, w)
-    cores = os.cpu_count() or 1
+    O.set_fft_workers(os.cpu_count() or 1)
+    st = O.CPState(sysm)
+    tq = time.perf_counter()
+    O.quench(st, sysm, args.quench)
+    tq = time.perf_counter() - tq
+    for _ in range(args.warmup):
+        O.cp_step(st, sysm, norb_tol=NORB_TOL)
+    t0 = time.perf_counter()
+    recs = [O.cp_step(st, sysm, norb_tol=NORB_TOL) for _ in range(args.steps)]
+    dt = time.perf_counter() - t0
+    finite = all(math.isfinite(r[k]) for r in recs for k in TERMS + ("FICT_KE", "SMAX"))
+    if not finite:
+        print(json.dumps({"impl": "reference", "unavailable": "the oracle produced non-finite energies"}))
+        return 0
+    rate = args.steps / dt
+    info = cpu_info()
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": k, "warmup": w, "ms_per_step": 1e3 * dt / k, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water box, random Loewdin-orthonormal start)",
-        "config": {"workload": f"{args.config}: 32 H2O, 128 states, 80 Ry, 108^3, ng={sysm.ng}",
-                   "nstate": sysm.nstate, "grid": list(sysm.nfft)},
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{k} full CP steps of the FP64 oracle (numpy/scipy FFT, {cores} FFT workers)"},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded water box, random Loewdin start quenched by damped CP)",
+        "config": workload_config(args, sysm),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": info["threads"], "kind": "port",
+                         "sample": f"{args.steps} full CPMD steps of the FP64 oracle after {args.warmup} warm-up "
+                                   f"steps and a {args.quench}-step damped quench ({tq:.0f} s, untimed)",
+                         **info},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "energies_last": {k: recs[-1][k] for k in TERMS + ("FICT_KE", "SMAX")},
+        "psiv_resets": sum(1 for r in recs if r["SMAX"] > NORB_TOL),
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -255,6 +324,50 @@ def time_steps(torch, drv, state, k, pos_host=None, sync_each=False):
     return ev0.elapsed_time(ev1) / k, ens
 
 
+def quenched_start(sysm, nq):
+    """The random start after nq damped FP64 CP steps on the GPU (host array)."""
+    from openatom_b200.gpu import CPDriver
+    d = CPDriver(sysm, "fp64")
+    d.quench(nq)
+    psi0 = d.psi.cpu().numpy()
+    d.ctx.close()
+    return psi0
+
+
+def native_records(sysm, psi0, prec, nsteps):
+    from openatom_b200.gpu import CPDriver
+    d = CPDriver(sysm, prec, psi0=psi0, norb_tol=NORB_TOL)
+    recs = d.run_native(d.native_state(use_graph=True), nsteps)
+    d.ctx.close()
+    return recs
+
+
+def drift_form(torch, args, want_oracle):
+    """The precision configuration on 8 H2O (32 states, 70 Ry, 64^3, dt = 5,
+    mu = 400): the mixed and the FP64 form for args.drift_steps CPMD steps
+    from the same quenched start.  Reports the drift of the CP constant of
+    motion of each form, each energy term's largest difference between the
+    two forms over the run, and (CPU leg) each term against the FP64 oracle
+    over the first 20 steps."""
+    sysm = make_sys("w8", args.seed + 3)
+    psi0 = quenched_start(sysm, args.quench)
+    n = args.drift_steps
+    recs = {p: native_records(sysm, psi0, p, n) for p in ("fp64", "mixed")}
+    out = {"workload": f"w8: 8 H2O, {sysm.nstate} states, 70 Ry, 64^3, ng={sysm.ng}", "steps": n}
+    for p, r in recs.items():
+        e = np.array([conserved_energy(x) for x in r])
+        out[f"drift_{p}_per_atom"] = float(e[-1] - e[0]) / sysm.natm
+        out[f"drift_{p}_max_per_atom"] = float(np.max(np.abs(e - e[0]))) / sysm.natm
+        out[f"psiv_resets_{p}"] = sum(1 for x in r if x["SMAX"] > NORB_TOL)
+    out["mixed_vs_fp64"] = per_term_errors(recs["mixed"], recs["fp64"], sysm.natm)
+    if want_oracle:
+        k = min(20, n)
+        _, _, ref = oracle_steps(sysm, psi0, k)
+        out["fp64_vs_oracle"] = per_term_errors(recs["fp64"][:k], ref, sysm.natm)
+        out["mixed_vs_oracle"] = per_term_errors(recs["mixed"][:k], ref, sysm.natm)
+    return out
+
+
 def run_ours(args):
     import torch
     from openatom_b200.gpu import CPDriver
@@ -268,12 +381,10 @@ def run_ours(args):
     natm = sysm.natm
 
     # quench the random start (untimed), FP64
-    d64 = CPDriver(sysm, "fp64")
-    d64.quench(args.quench)
-    psi0 = d64.psi.cpu().numpy()
+    psi0 = quenched_start(sysm, args.quench)
     # two drivers from the same quenched state
-    d64 = CPDriver(sysm, "fp64", psi0=psi0)
-    dmx = CPDriver(sysm, "mixed", psi0=psi0)
+    d64 = CPDriver(sysm, "fp64", psi0=psi0, norb_tol=NORB_TOL)
+    dmx = CPDriver(sysm, "mixed", psi0=psi0, norb_tol=NORB_TOL)
     st64 = d64.native_state(use_graph=True)
     stmx = dmx.native_state(use_graph=True)
     for _ in range(args.warmup):
@@ -313,36 +424,48 @@ def run_ours(args):
     kt = dmx.ctx.time_kernels(dmx.psi, reps=5)
     kt64 = d64.ctx.time_kernels(d64.psi, reps=5)
     roof = roofline(sysm, dmx, kt, args.config)
+    d64.ctx.close()
+    dmx.ctx.close()
+    del d64, dmx
+    torch.cuda.empty_cache()
 
     cpu = None
+    per_term = None
     if rk == 0 and not args.no_cpu:
-        rate, dt = cpu_step_rate(sysm, 1, 0)
-        cpu = {"value": rate, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
-               "sample": f"1 full CP step of the FP64 oracle on this workload ({dt:.1f} s, scipy FFT workers={os.cpu_count()})"}
+        # the first steps from the quenched start in both GPU forms and in the
+        # oracle on the host cores: per-term errors against the FP64 oracle,
+        # and the oracle's rate (cpu_baseline)
+        k = 2
+        g64 = native_records(sysm, psi0, "fp64", k)
+        gmx = native_records(sysm, psi0, "mixed", k)
+        rate, dt, ref = oracle_steps(sysm, psi0, k)
+        per_term = {"steps": k, "fp64_vs_oracle": per_term_errors(g64, ref, natm),
+                    "mixed_vs_oracle": per_term_errors(gmx, ref, natm)}
+        info = cpu_info()
+        cpu = {"value": rate, "unit": UNIT, "cores": info["threads"], "kind": "port",
+               "sample": f"{k} full CPMD steps of the FP64 oracle from the quenched start ({dt:.1f} s)", **info}
 
+    drift = drift_form(torch, args, rk == 0 and not args.no_cpu) if (rk == 0 and args.drift_steps > 0) else None
     batch = batch_form(torch, args) if (rk == 0 and args.batch > 0) else None
     large = large_form(torch, args) if (rk == 0 and args.large > 0) else None
 
     if rk == 0:
         # kernel launches of one mixed step, counted in its captured CUDA graph
-        launches_per_step = stmx.last_kernels if stmx.last_kernels > 0 else dmx.launches_per_step()
+        launches_per_step = stmx.last_kernels
         line = {
             "metric": METRIC, "value": ws * 1e3 / ms_mx, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_mx, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 FFT path + f64 GEMM/ortho/energies (mixed form)",
             "data": "synthetic (seeded water box, random Loewdin start quenched by damped CP)",
-            "config": {"workload": f"{args.config}: 32 H2O, 128 states, 80 Ry, 108^3, ng={sysm.ng}",
-                       "nstate": sysm.nstate, "grid": list(sysm.nfft), "dt": sysm.dt, "quench_steps": args.quench,
-                       "l2": "per-step working set > 126 MB L2 (z-line buffer alone "
-                             f"{dmx.ctx.scratch_bytes() / 1e6:.0f} MB); no explicit flush",
-                       "parallelism": f"replicas x{ws}"},
+            "config": workload_config(args, sysm),
             "fp64": {"value": ws * 1e3 / ms_64, "ms_per_step": ms_64},
             "mixed_over_fp64": ms_64 / ms_mx,
             "dE_per_atom_max": de,
+            "per_term_err": per_term,
             "ortho": {"iters": s_err[0], "residual": s_err[1],
                       "smax_max": max(e["SMAX"] for e in en_mx),
-                      "psiv_resets": sum(1 for e in en_mx if e["SMAX"] > dmx.norb_tol),
-                      "psiv_resets_fp64": sum(1 for e in en_64 if e["SMAX"] > d64.norb_tol)},
+                      "psiv_resets": sum(1 for e in en_mx if e["SMAX"] > NORB_TOL),
+                      "psiv_resets_fp64": sum(1 for e in en_64 if e["SMAX"] > NORB_TOL)},
             "kernel_ms": kt, "kernel_ms_fp64": kt64,
             "roofline": roof,
             "cpu_baseline": cpu,
@@ -351,6 +474,7 @@ def run_ours(args):
             "sync_every_step": {"value": ws * 1e3 / ms_sync, "ms_per_step": ms_sync},
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(),
+            "drift_1000": drift,
             "batch": batch,
             "large": large,
         }
@@ -361,8 +485,9 @@ def run_ours(args):
 
 
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
-# the plane kernels on the w32 workload, from one ncu capture
-# (profiles/k_pair_plane_w32.md); None for other workloads.
+# the plane kernels on the 32-water workload, copied from one ncu capture of
+# the same kernels (the run itself cannot read DRAM counters); None for other
+# workloads.
 TRAFFIC_W32 = {"state_plane_density": 755.4e6, "state_plane_vks": 747.1e6}
 
 
@@ -387,7 +512,8 @@ def roofline(sysm, drv, kt, config=None):
     ach = b / (kt[name] * 1e-3) / 1e9
     traffic = TRAFFIC_W32.get(name) if config == "w32" else None
     return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-            "traffic": traffic, "algorithmic_bytes": b, "peak_source": src}
+            "traffic": traffic, "traffic_source": "copied from an ncu capture of this kernel on this workload"
+            if traffic is not None else None, "algorithmic_bytes": b, "peak_source": src}
 
 
 def main():

@@ -51,6 +51,20 @@ def _ifftn(a, axes=None):
     return np.fft.ifftn(a, axes=axes)
 
 
+def _rfftn(a, axes=None):
+    if _FFT_WORKERS > 1:
+        import scipy.fft as sf
+        return sf.rfftn(a, axes=axes, workers=_FFT_WORKERS)
+    return np.fft.rfftn(a, axes=axes)
+
+
+def _irfftn(a, s, axes=None):
+    if _FFT_WORKERS > 1:
+        import scipy.fft as sf
+        return sf.irfftn(a, s=s, axes=axes, workers=_FFT_WORKERS)
+    return np.fft.irfftn(a, s=s, axes=axes)
+
+
 # ----------------------------------------------------------------------------
 # sphere <-> grid
 # ----------------------------------------------------------------------------
@@ -84,34 +98,47 @@ def _full_grid(coef, kx, ky, kz, nfft, hermitian_partner=True):
     return out
 
 
+def _half_grid(coef, kx, ky, kz, nfft):
+    """Scatter half-sphere coefficients (kx >= 0, the whole kx = 0 plane) onto
+    the r2c half grid [.., nz, ny, nx/2 + 1]."""
+    nx, ny, nz = nfft
+    out = np.zeros(coef.shape[:-1] + (nz, ny, nx // 2 + 1), dtype=np.complex128)
+    out[..., kz % nz, ky % ny, kx] = coef
+    return out
+
+
 def state_g_to_r(psi, sysm):
     """G-sphere -> real space for each state: the composition of
     ``doStpFFTGtoR_Gchare`` (expand + z FFT, ``fftCache.C:1133-1159``), the
     z->R transpose (``CP_State_GSpacePlane.C:1448-1517``,
     ``CP_State_RealSpacePlane.C:186-271``) and ``doStpFFTGtoR_Rchare``
     (y FFT, conjugate, c2r x FFT, ``fftCache.C:1167-1243``).
+    psi(r) = sum_{full sphere} c(g) exp(-i g.r) is real, so it equals
+    N * c2r[conj(c)] on the kx >= 0 half grid (the Hermitian partners
+    c(-g) = conj(c(g)) are implied, as in the reference's c2r x transform).
     Returns psi(r) as float64 [nstate, nz, ny, nx]."""
     nx, ny, nz = sysm.nfft
+    npts = nx * ny * nz
     out = np.empty(psi.shape[:-1] + (nz, ny, nx))
     flat_in = psi.reshape(-1, psi.shape[-1])
     flat_out = out.reshape(-1, nz, ny, nx)
     for c0 in range(0, flat_in.shape[0], 16):
-        full = _full_grid(flat_in[c0:c0 + 16], sysm.kx, sysm.ky, sysm.kz, sysm.nfft)
-        flat_out[c0:c0 + 16] = _fftn(full, axes=(-3, -2, -1)).real
+        half = _half_grid(np.conj(flat_in[c0:c0 + 16]), sysm.kx, sysm.ky, sysm.kz, sysm.nfft)
+        flat_out[c0:c0 + 16] = _irfftn(half, s=(nz, ny, nx), axes=(-3, -2, -1)) * npts
     return out
 
 
 def state_r_to_g(fr, sysm):
     """Real space -> g-sphere, unnormalised exp(+i g.r): ``doStpFFTRtoG_Rchare``
     (r2c x, conjugate, y FFT, ``fftCache.C:1252-1319``), transpose back, and
-    ``doStpFFTRtoG_Gchare`` (z FFT + pack, ``fftCache.C:1099-1123``)."""
-    n = fr.shape[-1] * fr.shape[-2] * fr.shape[-3]
+    ``doStpFFTRtoG_Gchare`` (z FFT + pack, ``fftCache.C:1099-1123``).
+    For real f(r), sum_r f(r) exp(+i g.r) = conj(r2c[f](g)) on kx >= 0."""
     nx, ny, nz = sysm.nfft
     flat = fr.reshape(-1, nz, ny, nx)
     out = np.empty((flat.shape[0], sysm.ng), dtype=np.complex128)
     for c0 in range(0, flat.shape[0], 16):
-        full = _ifftn(flat[c0:c0 + 16], axes=(-3, -2, -1)) * n
-        out[c0:c0 + 16] = full[:, sysm.kz % nz, sysm.ky % ny, sysm.kx % nx]
+        half = _rfftn(flat[c0:c0 + 16], axes=(-3, -2, -1))
+        out[c0:c0 + 16] = np.conj(half[:, sysm.kz % nz, sysm.ky % ny, sysm.kx])
     return out.reshape(fr.shape[:-3] + (sysm.ng,))
 
 
@@ -172,6 +199,25 @@ def rho_sphere(sysm):
     return KX[m], KY[m], KZ[m], g2[m]
 
 
+def _phase_sums(sysm, kx, ky, kz, weights):
+    """sum_a weights[k, a] exp(i g.R_a) at the g-points (kx, ky, kz), one row
+    per weight vector, with the phase factorised per axis
+    exp(i g.R) = exp(i gx x) exp(i gy y) exp(i gz z): the (kx, ky) products of
+    the atoms times the kz phases is one complex GEMM per weight vector."""
+    f = TWO_PI / sysm.box
+    pos = sysm.pos
+    ax = [np.arange(int(k.min()), int(k.max()) + 1) for k in (kx, ky, kz)]
+    ex, ey, ez = (np.exp(1j * f * np.outer(pos[:, d], ax[d])) for d in range(3))
+    nxy = ax[0].size * ax[1].size
+    exy = (ex[:, :, None] * ey[:, None, :]).reshape(pos.shape[0], nxy)
+    ix, iy, iz = kx - ax[0][0], ky - ax[1][0], kz - ax[2][0]
+    out = []
+    for w in weights:
+        full = ((exy * w[:, None]).T @ ez).reshape(ax[0].size, ax[1].size, ax[2].size)
+        out.append(full[ix, iy, iz])
+    return out
+
+
 def hart_eext(rho_r, sysm, want_forces=False):
     """``CPLOCAL::CP_hart_eext_calc`` (``abinito_physics/cp_local/cp_hart_ext.C:56-431``)
     on rho(g) = FFT_-[rho(r) V/N] (``CP_Rho_RealSpacePlane.C:846-851``).
@@ -179,9 +225,9 @@ def hart_eext(rho_r, sysm, want_forces=False):
     nx, ny, nz = sysm.nfft
     n = nx * ny * nz
     vol = sysm.vol
-    rhog_full = _fftn(rho_r * (vol / n))
+    rhog_half = _rfftn(rho_r * (vol / n))
     kx, ky, kz, g2 = rho_sphere(sysm)
-    rho = rhog_full[kz % nz, ky % ny, kx % nx]
+    rho = rhog_half[kz % nz, ky % ny, kx]
     f = TWO_PI / sysm.box
     gx, gy, gz = f * kx, f * ky, f * kz
     nz0 = g2 != 0
@@ -191,14 +237,15 @@ def hart_eext(rho_r, sysm, want_forces=False):
     hf[nz0] = 4.0 * math.pi / (g2[nz0] * vol)
     ehart = float(np.sum(hf * np.abs(rho) ** 2 * w)) / 2.0
     vks = rho * hf
-    # structure factor h = exp(i g.R) and local pseudopotential
-    arg = np.outer(gx, sysm.pos[:, 0]) + np.outer(gy, sysm.pos[:, 1]) + np.outer(gz, sysm.pos[:, 2])
-    h = np.exp(1j * arg)                                  # [ng, natm]
+    # structure factors sum_a exp(i g.R_a) per atom type and with the ion
+    # charges, and the local pseudopotential
     g = np.sqrt(g2)
-    vtyp = np.stack([sysm.vloc.eval(np.full(g.shape, t), g) for t in range(len(sysm.type_names))], axis=1) / vol
-    vtemp = vtyp[:, sysm.atm_type]                        # [ng, natm]
-    vext = np.sum(h * vtemp, axis=1)
-    sewd = h @ sysm.q
+    ntyp = len(sysm.type_names)
+    vtyp = np.stack([sysm.vloc.eval(np.full(g.shape, t), g) for t in range(ntyp)], axis=1) / vol
+    sums = _phase_sums(sysm, kx, ky, kz,
+                       [(sysm.atm_type == t).astype(np.float64) for t in range(ntyp)] + [np.asarray(sysm.q, float)])
+    vext = sum(vtyp[:, t] * sums[t] for t in range(ntyp))
+    sewd = sums[ntyp]
     falp2 = 4.0 * sysm.alp_ewd ** 2
     ewf = np.zeros_like(g2)
     ewf[nz0] = 4.0 * math.pi * np.exp(-g2[nz0] / falp2) / (g2[nz0] * vol)
@@ -207,6 +254,9 @@ def hart_eext(rho_r, sysm, want_forces=False):
     eext = float(np.sum(np.where(nz0, (rho * vext).real * w, 0.0)))
     fatm = None
     if want_forces:
+        arg = np.outer(gx, sysm.pos[:, 0]) + np.outer(gy, sysm.pos[:, 1]) + np.outer(gz, sysm.pos[:, 2])
+        h = np.exp(1j * arg)                                  # [ng, natm]
+        vtemp = vtyp[:, sysm.atm_type]                        # [ng, natm]
         rr = (rho.real * w)[:, None] * vtemp + ((sewd.real * ewf * w)[:, None] * sysm.q[None, :])
         ri = (-rho.imag * w)[:, None] * vtemp + ((sewd.imag * ewf * w)[:, None] * sysm.q[None, :])
         comp = rr * h.imag - ri * h.real
@@ -217,12 +267,11 @@ def hart_eext(rho_r, sysm, want_forces=False):
         v0 = float(np.sum(sysm.gzvps[sysm.atm_type])) / vol
         vks[iz[0]] = v0
         eext += v0 * rho[iz[0]].real
-    # V(r) = sum_{full sphere} vks(g) exp(+i g.r)
-    full = np.zeros((nz, ny, nx), dtype=np.complex128)
-    full[kz % nz, ky % ny, kx % nx] = vks
-    m = kx > 0
-    full[(-kz[m]) % nz, (-ky[m]) % ny, (-kx[m]) % nx] = np.conj(vks[m])
-    vr = (_ifftn(full) * n).real
+    # V(r) = sum_{full sphere} vks(g) exp(+i g.r): c2r of the kx >= 0 half
+    # (the whole kx = 0 plane is in the density sphere)
+    half = np.zeros((nz, ny, nx // 2 + 1), dtype=np.complex128)
+    half[kz % nz, ky % ny, kx] = vks
+    vr = _irfftn(half, s=(nz, ny, nx), axes=(0, 1, 2)) * n
     out = (vr, ehart, eext, ewald)
     return out + (fatm,) if want_forces else out
 
@@ -693,3 +742,23 @@ def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl="auto", norb_tol=None):
     if norb_tol is not None and en["SMAX"] > norb_tol:
         psiv_reset(st, sysm)
     return en
+
+
+def quench(st, sysm, nsteps, tol=1e-15, max_iter=1000):
+    """Damped CP from a random start: each step is ``cp_step`` with the
+    velocities zeroed after the integration and the non-orthogonal set reset
+    to the orthonormal one (``psiv_reset`` with v = 0), the iteration count
+    restarting every step -- steepest descent on the orthonormal states with
+    step dt^2 / (2 m).  The same procedure as ``CPDriver.quench`` on the GPU;
+    it brings the start near the Born-Oppenheimer surface before CPMD.
+    Returns the energy record of every step."""
+    out = []
+    for _ in range(nsteps):
+        st.iteration = 0
+        st.v = np.zeros_like(st.v)
+        en = cp_step(st, sysm, tol, max_iter)
+        st.v = np.zeros_like(st.v)
+        psiv_reset(st, sysm)
+        out.append(en)
+    st.iteration = 0
+    return out

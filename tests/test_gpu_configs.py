@@ -1,0 +1,114 @@
+"""Parity of the native graphed CP step (oa_gpu_cp_run: the call the
+benchmark times) with the oracle at the configured sizes:
+
+* the 8-water system with all 32 states, 20 CPMD steps at dt = 5 a.u. and
+  fictitious mass 400 a.u. from the seeded Loewdin start, with the PsiV
+  tolerance reset decided on the device (cp_norb_tol 0.003) -- the 20-step
+  CPMD run of the FP64 configuration;
+* the 32-water system with all 128 states on the 108^3 grid, three steps, so
+  the paths only 128 states take (the symmetric 128 x 128 overlap tile, the
+  4 x 4 Newton-Schulz cluster grid, the state-pair plane kernels at full
+  occupancy) are checked against the oracle;
+* the mixed form on the 32-water system from a quenched start: every energy
+  term against the FP64 oracle, the total within 1e-6 Ha/atom.
+
+FP64 form: each energy term to 1e-10 relative, coefficients to 1e-9
+(max abs error over max abs value)."""
+import numpy as np
+import pytest
+
+from openatom_b200.system import make_system
+from oracle import cp_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TERMS = ("EKE", "EHART", "EEXT", "EEXC", "ENL")
+E_TOL = 1e-10
+C_TOL = 1e-9
+NORB_TOL = 0.003
+
+
+def _cfg_system(preset, seed):
+    return make_system(preset, seed=seed, ecut_mass=2.0, cmass0=400.0, dt=5.0)
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def _oracle_run(s, psi0, nsteps, workers=None):
+    import os
+    O.set_fft_workers(workers or os.cpu_count() or 1)
+    st = O.CPState(s)
+    if psi0 is not None:
+        st.psi_t = psi0.copy()
+        st.psi = psi0.copy()
+    recs = [O.cp_step(st, s, norb_tol=NORB_TOL) for _ in range(nsteps)]
+    return st, recs
+
+
+def _check_fp64(got, ref, st, drv):
+    for i, (g, r) in enumerate(zip(got, ref)):
+        for k in TERMS + ("FICT_KE",):
+            tol = E_TOL * max(1.0, abs(r[k]))
+            assert abs(g[k] - r[k]) <= tol, (i, k, g[k], r[k])
+        assert int(g["ORTHO_ITERS"]) == r["ORTHO_ITERS"], (i, g["ORTHO_ITERS"], r["ORTHO_ITERS"])
+        assert abs(g["SMAX"] - r["SMAX"]) <= 1e-10 * max(1.0, r["SMAX"]), (i, g["SMAX"], r["SMAX"])
+    assert _rel(drv.psi.cpu().numpy(), st.psi) < C_TOL
+    assert _rel(drv.v.cpu().numpy(), st.v) < C_TOL
+
+
+def test_w8_32_states_20_cpmd_steps_native():
+    """The FP64 configuration's 20-step CPMD run (8 H2O, 32 states, 70 Ry,
+    64^3, dt = 5, mu = 400, mass cutoff 2) through oa_gpu_cp_run in one
+    call, against 20 oracle cp_step calls with the same PsiV tolerance."""
+    from openatom_b200.gpu import CPDriver
+    s = _cfg_system("w8", 2024)
+    assert s.nstate == 32
+    st, ref = _oracle_run(s, None, 20)
+    d = CPDriver(s, "fp64", norb_tol=NORB_TOL)
+    got = d.run_native(d.native_state(use_graph=True), 20)
+    _check_fp64(got, ref, st, d)
+    # the PsiV reset fired in the same steps
+    assert [g["SMAX"] > NORB_TOL for g in got] == [r["SMAX"] > NORB_TOL for r in ref]
+    d.ctx.close()
+
+
+def test_w32_128_states_native():
+    """32 H2O, 128 states, 80 Ry, 108^3 (ng = 40115): three native graphed
+    FP64 steps from the seeded start against the oracle."""
+    from openatom_b200.gpu import CPDriver
+    s = _cfg_system("w32", 2024)
+    assert s.nstate == 128
+    st, ref = _oracle_run(s, None, 3)
+    d = CPDriver(s, "fp64", norb_tol=NORB_TOL)
+    got = d.run_native(d.native_state(use_graph=True), 3)
+    _check_fp64(got, ref, st, d)
+    d.ctx.close()
+
+
+def test_w32_mixed_terms_against_oracle():
+    """The mixed form at 128 states from a start quenched by 20 damped FP64
+    steps: each energy term of three native steps against the FP64 oracle on
+    the same start.  The target is the total energy within 1e-6 Ha/atom;
+    each term is held to the same absolute bound (96 atoms)."""
+    from openatom_b200.gpu import CPDriver
+    s = _cfg_system("w32", 2025)
+    q = CPDriver(s, "fp64")
+    q.quench(20)
+    psi0 = q.psi.cpu().numpy()
+    q.ctx.close()
+    st, ref = _oracle_run(s, psi0, 3)
+    d = CPDriver(s, "mixed", psi0=psi0, norb_tol=NORB_TOL)
+    got = d.run_native(d.native_state(use_graph=True), 3)
+    bound = 1e-6 * s.natm
+    for i, (g, r) in enumerate(zip(got, ref)):
+        for k in TERMS:
+            assert abs(g[k] - r[k]) <= bound, (i, k, g[k] - r[k])
+        etot = sum(g[k] for k in TERMS) - sum(r[k] for k in TERMS)
+        assert abs(etot) / s.natm <= 1e-6, (i, etot / s.natm)
+    # orthonormality of the mixed result in FP64: ||S/2 - I||_max
+    psi = d.psi.cpu().numpy()
+    S = O.pc_forward(O.kx0_scale(psi, s, 2 ** -0.5), O.kx0_scale(psi, s, 2 ** -0.5), s, 2.0)
+    assert float(np.max(np.abs(S / 2.0 - np.eye(s.nstate)))) <= 1e-10
+    d.ctx.close()
