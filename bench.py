@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="w32")
-    ap.add_argument("--quench", type=int, default=20)
+    ap.add_argument("--quench", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--batch", type=int, default=48,
@@ -205,12 +205,23 @@ def conserved_energy(en):
     return total_energy(en) + en["FICT_KE"]
 
 
+QUENCH_DT = 10.0   # damped steps after the first three (steepest-descent step dt^2 / 2m)
+
+
+def quench_schedule(nq):
+    """(steps, dt) of the damped quench of the random start: three steps at
+    the system's dt, then the rest at QUENCH_DT."""
+    first = min(3, nq)
+    return [(first, None), (nq - first, QUENCH_DT)]
+
+
 def workload_config(args, sysm):
     """The config object both arms print for the headline workload."""
     return {"workload": f"{args.config}: {sysm.natm // 3} H2O, {sysm.nstate} states, {sysm.ecut_ry:g} Ry, "
                         f"{sysm.nfft[0]}^3, ng={sysm.ng}",
             "nstate": sysm.nstate, "grid": list(sysm.nfft), "dt": sysm.dt, "fict_mass": sysm.cmass0,
-            "quench_steps": args.quench, "norb_tol": NORB_TOL, "seed": args.seed,
+            "quench_steps": args.quench, "quench_dt": [sysm.dt, QUENCH_DT], "norb_tol": NORB_TOL,
+            "seed": args.seed,
             "l2": "per-step working set > 126 MB L2 (z-line buffer alone 244 MB in FP32); no explicit flush",
             "parallelism": f"replicas x{args.gpus}"}
 
@@ -271,7 +282,8 @@ def run_reference(args):
     O.set_fft_workers(os.cpu_count() or 1)
     st = O.CPState(sysm)
     tq = time.perf_counter()
-    O.quench(st, sysm, args.quench)
+    for n, dtq in quench_schedule(args.quench):
+        O.quench(st, sysm, n, dt=dtq)
     tq = time.perf_counter() - tq
     for _ in range(args.warmup):
         O.cp_step(st, sysm, norb_tol=NORB_TOL)
@@ -328,7 +340,8 @@ def quenched_start(sysm, nq):
     """The random start after nq damped FP64 CP steps on the GPU (host array)."""
     from openatom_b200.gpu import CPDriver
     d = CPDriver(sysm, "fp64")
-    d.quench(nq)
+    for n, dtq in quench_schedule(nq):
+        d.quench(n, dt=dtq)
     psi0 = d.psi.cpu().numpy()
     d.ctx.close()
     return psi0

@@ -157,9 +157,17 @@ oa_status oa_gpu_pc_backward_mixed(oa_ctx *ctx, void *stream, const double *M1, 
                                    double a1_kx0, double a1_rest, const double *M2, const double *X2, double a2,
                                    int nterm, double *out);
 
-/* Synchronise the stream and report whether any kernel's bounded wait ran
- * out (OA_ERR_CUDA with a message) since the context was created. */
+/* Synchronise the stream and report whether any kernel's time-bounded wait
+ * (200 ms) ran out (OA_ERR_CUDA with a message) since the last check; the
+ * device flag is cleared when it is reported. */
 oa_status oa_gpu_check(oa_ctx *ctx, void *stream);
+
+/* Failure-detection test hook, no counterpart in the reference (its
+ * failures end in CkAbort / EXIT).  kind 1: the next split-BF16 forward
+ * product skips the loads of one pipeline stage in one block, so that
+ * block's bounded wait runs out and oa_gpu_check reports it; kind 0 clears
+ * the hook.  Acts on the current device. */
+oa_status oa_gpu_fault_inject(oa_ctx *ctx, int kind);
 
 /* Small dense C = alpha A B (N x N), e.g. Gamma = T Lambda (ortho.C:565-570). */
 oa_status oa_gpu_small_gemm(oa_ctx *ctx, void *stream, const double *A, const double *B, double alpha,

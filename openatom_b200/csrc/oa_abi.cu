@@ -1049,7 +1049,11 @@ extern "C" oa_status oa_gpu_check(oa_ctx* c, void* stream) {
   OA_CUDA_TRY(cudaMemcpyAsync(p->h_status + 2, p->err_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
   OA_CUDA_TRY(cudaStreamSynchronize(s));
   if (p->h_status[2]) {
-    oa_set_error("a device wait reached its iteration limit", __FILE__, __LINE__);
+    // reported once: the flag is cleared for the calls that follow
+    OA_CUDA_TRY(cudaMemsetAsync(p->err_flag, 0, sizeof(int), s));
+    OA_CUDA_TRY(cudaStreamSynchronize(s));
+    oa_set_error("a device wait ran out of time (200 ms) in a tcgen05 product; its output is zero", __FILE__,
+                 __LINE__);
     return OA_ERR_CUDA;
   }
   return OA_OK;

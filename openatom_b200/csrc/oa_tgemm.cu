@@ -29,6 +29,7 @@
 #include <cuda_bf16.h>
 #include <mutex>
 #include "oa_internal.h"
+#include "oa_wait.cuh"
 
 typedef __nv_bfloat16 bf16;
 
@@ -36,7 +37,6 @@ typedef __nv_bfloat16 bf16;
 #define TG_KF 64            // K per stage (forward)
 #define TG_M 128
 #define TG_THREADS 128
-#define TG_SPIN (1u << 28)
 
 __device__ __forceinline__ uint32_t tg_s32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -73,17 +73,7 @@ __device__ __forceinline__ void tg_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(tg_s32(bar)), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ bool tg_wait(uint64_t* bar, uint32_t phase) {
-  const uint32_t a = tg_s32(bar);
-  for (uint32_t it = 0; it < TG_SPIN; ++it) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok) : "r"(a), "r"(phase) : "memory");
-    if (ok) return true;
-  }
-  return false;
+  return oa_mbar_wait_bounded(tg_s32(bar), phase);
 }
 // box of 64 columns x the map's rows starting at (row, column chunk ch) of
 // plane q, into shared memory, completing on bar (4-D tile load)
@@ -172,6 +162,21 @@ __global__ void k_split_kc(const double* __restrict__ X, int rows, int rows_pad,
   }
 }
 
+// Failure-detection test hook (oa_gpu_fault_inject): when set, the first
+// k_tfwd block (0, 0, 0) to read it takes it back and skips the TMA loads of
+// its first stage, so its wait on that stage runs out of time.
+__device__ int g_oa_inject_skip_load = 0;
+
+extern "C" oa_status oa_gpu_fault_inject(oa_ctx* c, int kind) {
+  if (!c || (kind != 0 && kind != 1)) {
+    oa_set_error("kind must be 0 (clear) or 1 (skip one stage's loads)", __FILE__, __LINE__);
+    return OA_ERR_BAD_ARG;
+  }
+  const int v = kind;
+  OA_CUDA_TRY(cudaMemcpyToSymbol(g_oa_inject_skip_load, &v, sizeof(int)));
+  return OA_OK;
+}
+
 // ---------------------------------------------------------------------------
 // forward: part[kb][x][y] (FP32) over the K slabs kb, kb + nkb, ... of this CTA
 // ---------------------------------------------------------------------------
@@ -206,7 +211,9 @@ k_tfwd(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorM
   if (tid == 0) {
     constexpr uint32_t idesc = tg_idesc(NB, 0, 0);
     const uint32_t sbase = tg_s32(base);
+    const bool skip0 = (blockIdx.x | blockIdx.y | blockIdx.z) == 0 && atomicExch(&g_oa_inject_skip_load, 0) != 0;
     auto issue_loads = [&](int sl, int st) {
+      if (skip0 && sl == 0) return;  // injected failure: stage 0 never fills
       const int k0 = (kb + sl * nkb) * TG_KF;
       const uint32_t sb = sbase + st * stage_bytes;
       tg_expect_tx(&full[st], stage_bytes);
@@ -220,6 +227,7 @@ k_tfwd(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorM
     const int pre = nslab < stages ? nslab : stages;
     for (int s = 0; s < pre; ++s) issue_loads(s, s);
     int issued = pre;
+    int committed = -1;  // last slab whose MMAs were committed
     for (int sl = 0; sl < nslab && ok; ++sl) {
       const int st = sl % stages;
       const uint32_t ph = (uint32_t)(sl / stages) & 1u;
@@ -243,6 +251,7 @@ k_tfwd(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorM
           }
         }
       tg_commit(&empty[st]);
+      committed = sl;
       if (issued < nslab) {
         // stage st is free once these MMAs are done
         if (!tg_wait(&empty[st], ph)) { ok = false; break; }
@@ -256,8 +265,16 @@ k_tfwd(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorM
       if (!tg_wait(&empty[sl % stages], (uint32_t)(sl / stages) & 1u)) ok = false;
     }
     if (!ok) {
-      // let the loads already issued land before the block exits
-      for (int s2 = 0; s2 < stages; ++s2) (void)tg_wait(&full[s2], 0u);
+      // let the loads already issued land before the block exits: wait for
+      // the phase of the last slab issued on each stage
+      for (int s2 = 0; s2 < stages && s2 < issued; ++s2) {
+        const int last = issued - 1 - ((issued - 1 - s2) % stages);
+        if (skip0 && last == 0) continue;  // never issued
+        (void)tg_wait(&full[s2], (uint32_t)(last / stages) & 1u);
+      }
+      // and the MMAs already issued finish before TMEM is freed (the last
+      // commit tracks all of them)
+      if (committed >= 0) (void)tg_wait(&empty[committed % stages], (uint32_t)(committed / stages) & 1u);
       *okflag = 0;
     }
   }

@@ -20,12 +20,12 @@
 // groups SBO = 128 B apart; K core-matrix columns LBO = rows/8 * 128 B apart.
 #include <cuda_bf16.h>
 #include "oa_internal.h"
+#include "oa_wait.cuh"
 
 #define UM_KT 64          // K elements per pipeline stage
 #define UM_M 128          // MMA M (rows per CTA tile)
 #define UM_THREADS 512
 #define UM_ITEMS_MAX 4   // staged 8-element chunks per thread per stage (nb <= 128)
-#define UM_SPIN_LIMIT (1u << 28)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -63,19 +63,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
 }
 
-// bounded wait on an mbarrier phase; returns false when the limit is hit
+// bounded wait on an mbarrier phase (oa_wait.cuh); false when the time limit is hit
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
-  const uint32_t a = smem_u32(bar);
-  for (uint32_t it = 0; it < UM_SPIN_LIMIT; ++it) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok) : "r"(a), "r"(phase) : "memory");
-    if (ok) return true;
-  }
-  return false;
+  return oa_mbar_wait_bounded(smem_u32(bar), phase);
 }
 
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }

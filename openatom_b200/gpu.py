@@ -88,6 +88,7 @@ SIGNATURES = {
     "oa_gpu_pc_backward_mixed": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_double, _vp, _vp, C.c_double,
                                            C.c_int, _vp]),
     "oa_gpu_check": (C.c_int, [_vp, _vp]),
+    "oa_gpu_fault_inject": (C.c_int, [_vp, C.c_int]),
     "oa_gpu_nl_sf": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp]),
     "oa_gpu_cp_step": (C.c_int, [_vp, _vp, C.POINTER(CPState), _dp]),
     "oa_gpu_cp_run": (C.c_int, [_vp, _vp, C.POINTER(CPState), C.c_int, _dp, _dp]),
@@ -272,6 +273,11 @@ class CPContext:
 
     def check(self):
         _check(self._lib.oa_gpu_check(self._h, self._stream()))
+
+    def fault_inject(self, kind: int):
+        """Test hook: kind 1 makes the next split-BF16 forward product skip
+        one stage's loads in one block (its bounded wait runs out); 0 clears."""
+        _check(self._lib.oa_gpu_fault_inject(self._h, int(kind)))
 
     def small_gemm(self, A, B, alpha, out):
         _check(self._lib.oa_gpu_small_gemm(self._h, self._stream(), _ptr(A), _ptr(B), float(alpha), _ptr(out)))

@@ -17,6 +17,11 @@ SRCS=(
   "$PINY/abinito_physics/cp_xc_fnctl/cp_pz_lda.C"
   "$PINY/abinito_physics/cp_local/cp_hart_ext.C"
   "$PINY/abinito_physics/cp_orthog/cp_lowdin.C"
+  "$PINY/abinito_physics/cp_nonlocal/cp_struct_fact.C"
+  "$PINY/abinito_physics/cp_nonlocal/cp_nlmat.C"
+  "$PINY/abinito_physics/cp_nonlocal/cp_nl_energy_forc.C"
+  "$PINY/abinito_physics/cp_integrate/cp_dynamics.C"
+  "$PINY/abinito_physics/cp_integrate/cp_isokin.C"
 )
 OBJS=()
 for s in "${SRCS[@]}"; do

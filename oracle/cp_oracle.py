@@ -649,6 +649,23 @@ def fict_ke(vpsi, cmass, sysm):
     return 0.5 * e
 
 
+def integrate_dyn(force, vpsi, psi_t, sysm, iteration, dt):
+    """``CPINTEGRATE::CP_integrate_dyn`` (``cp_dynamics.C:29-88``) with the
+    coefficient thermostat off: complete the previous half kick
+    (iteration > 1), the fictitious KE at time t, the next half kick, and
+    the drift psi += v dt on [nkx0_red, ng).  Returns (v, psi_t, per-state
+    fictitious KE); the inputs are not modified."""
+    v = vpsi
+    if iteration > 1:
+        v = evolve_vel(force, v, sysm.cmass, dt, sysm)
+    fict = fict_ke(v, sysm.cmass, sysm)
+    v = evolve_vel(force, v, sysm.cmass, dt, sysm)
+    r0 = sysm.nkx0_red
+    p = psi_t.copy()
+    p[:, r0:] = p[:, r0:] + v[:, r0:] * dt
+    return v, p, fict
+
+
 def sync_redundant(a, sysm):
     """Gamma redundancy sync (``gspace.ci:692-708``, ``CP_State_GSpacePlane.C:2829-2970``):
     the redundant kx=0 half is the conjugate of the unique half."""
@@ -713,7 +730,7 @@ def _nl_default(psi, sysm):
     return f, float(enl.sum())
 
 
-def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl="auto", norb_tol=None):
+def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl="auto", norb_tol=None, dt=None):
     """One CPAIMD electronic step.  Order: forces on the orthonormal psi
     (computePsiFandVKS + NL, combineForcesGetEke), constraint force
     (computeLambdaAndCg), integrate (integrateModForce ->
@@ -726,13 +743,8 @@ def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl="auto", norb_tol=None):
     fnl, enl = (None, 0.0) if nl is None else nl(st.psi, sysm)
     f, en = electronic_forces(st.psi, sysm, fnl, enl)
     f, lam = lambda_step(st.psi, f, st.T, sysm)
-    dt = sysm.dt
-    if st.iteration > 1:
-        st.v = evolve_vel(f, st.v, sysm.cmass, dt, sysm)
-    en["FICT_KE"] = float(fict_ke(st.v, sysm.cmass, sysm).sum())
-    st.v = evolve_vel(f, st.v, sysm.cmass, dt, sysm)
-    r0 = sysm.nkx0_red
-    st.psi_t[:, r0:] = st.psi_t[:, r0:] + st.v[:, r0:] * dt
+    st.v, st.psi_t, fict = integrate_dyn(f, st.v, st.psi_t, sysm, st.iteration, sysm.dt if dt is None else dt)
+    en["FICT_KE"] = float(fict.sum())
     st.psi_t = sync_redundant(st.psi_t, sysm)
     st.v = sync_redundant(st.v, sysm)
     st.psi, st.T, S, it, err = ortho_psi(st.psi_t, sysm, tol, max_iter)
@@ -744,19 +756,20 @@ def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl="auto", norb_tol=None):
     return en
 
 
-def quench(st, sysm, nsteps, tol=1e-15, max_iter=1000):
+def quench(st, sysm, nsteps, tol=1e-15, max_iter=1000, dt=None):
     """Damped CP from a random start: each step is ``cp_step`` with the
     velocities zeroed after the integration and the non-orthogonal set reset
     to the orthonormal one (``psiv_reset`` with v = 0), the iteration count
     restarting every step -- steepest descent on the orthonormal states with
-    step dt^2 / (2 m).  The same procedure as ``CPDriver.quench`` on the GPU;
-    it brings the start near the Born-Oppenheimer surface before CPMD.
-    Returns the energy record of every step."""
+    step dt^2 / (2 m) (dt: the system's time step unless given).  The same
+    procedure as ``CPDriver.quench`` on the GPU; it brings the start near the
+    Born-Oppenheimer surface before CPMD.  Returns the energy record of every
+    step."""
     out = []
     for _ in range(nsteps):
         st.iteration = 0
         st.v = np.zeros_like(st.v)
-        en = cp_step(st, sysm, tol, max_iter)
+        en = cp_step(st, sysm, tol, max_iter, dt=dt)
         st.v = np.zeros_like(st.v)
         psiv_reset(st, sysm)
         out.append(en)

@@ -127,3 +127,70 @@ def test_iter_tmat_pinned(ref):
     ref.ref_iter_tmat(_d(S), _d(T), n)
     T_or, it, err = O.newton_schulz(S, tol=1e-15, max_iter=10)
     assert np.max(np.abs(T - T_or)) < 1e-14
+
+
+def _nl_inputs(s):
+    nl = s.nl_atoms()
+    return dict(nl=np.ascontiguousarray(nl, dtype=np.int32),
+                kx=np.ascontiguousarray(s.kx, dtype=np.int32), ky=np.ascontiguousarray(s.ky, dtype=np.int32),
+                kz=np.ascontiguousarray(s.kz, dtype=np.int32), typ=np.ascontiguousarray(s.atm_type, dtype=np.int32),
+                pos=np.ascontiguousarray(s.pos), spl=np.ascontiguousarray(s.nl_proj.coef),
+                vn=np.ascontiguousarray(s.nl_vnorm, dtype=np.float64), gz=np.ascontiguousarray(s.nl_gz0, dtype=np.float64))
+
+
+def test_nl_struct_fact_pinned(ref, sysm):
+    """Structure-factor nonlocal energy and coefficient forces of every
+    state: CP_calc_Struct_Fact, CP_enl_matrix_calc, CP_enl_atm_forc_calc and
+    CP_enl_force_calc against oracle.struct_fact / nl_energy_forces."""
+    s = sysm
+    ref.ref_nl_sf.argtypes = [C.c_int, ip, ip, ip, C.c_int, dp, dp, C.c_int, dp, ip, C.c_int, C.c_int, ip, C.c_int,
+                              C.c_double, C.c_double, dp, dp, dp, C.c_double, C.c_double, dp, dp, dp, dp, dp]
+    a = _nl_inputs(s)
+    nnl = len(a["nl"])
+    assert nnl > 0
+    psi = np.ascontiguousarray(s.psi)
+    occ = np.ascontiguousarray(s.occ, dtype=np.float64)
+    sf = np.zeros((nnl, s.ng), dtype=np.complex128)
+    fnl = np.zeros((s.nstate, s.ng), dtype=np.complex128)
+    zmat = np.zeros((s.nstate, nnl))
+    enl = np.zeros(s.nstate)
+    fatm = np.zeros((s.natm, 3))
+    ref.ref_nl_sf(s.ng, _i(a["kx"]), _i(a["ky"]), _i(a["kz"]), s.nstate, _d(psi.view(np.float64)), _d(occ), s.natm,
+                  _d(a["pos"]), _i(a["typ"]), len(s.type_names), nnl, _i(a["nl"]), s.nl_proj.n, s.nl_proj.gmin,
+                  s.nl_proj.dg, _d(a["spl"]), _d(a["vn"]), _d(a["gz"]), s.ecut_ry, s.box,
+                  _d(sf.view(np.float64)), _d(fnl.view(np.float64)), _d(zmat), _d(enl), _d(fatm))
+    sf_or, _ = O.struct_fact(s)
+    f_or, e_or, z_or = O.nl_energy_forces(s.psi, s, sf_or)
+    assert np.max(np.abs(sf - sf_or)) <= 1e-13 * np.max(np.abs(sf_or))
+    assert np.max(np.abs(enl - e_or)) <= 1e-12 * np.max(np.abs(e_or))
+    assert np.max(np.abs(fnl - f_or)) <= 1e-12 * np.max(np.abs(f_or))
+    vn = s.nl_vnorm[s.atm_type[a["nl"]]] / s.vol
+    assert np.max(np.abs(zmat - 2.0 * vn[None, :] * z_or)) <= 1e-12 * np.max(np.abs(zmat))
+    assert np.all(np.isfinite(fatm))
+
+
+@pytest.mark.parametrize("iteration", [1, 2])
+def test_integrate_dyn_pinned(ref, sysm, iteration):
+    """CP_integrate_dyn (thermostat off) against oracle.integrate_dyn: the
+    half kicks with the g = 0 / kx = 0 conventions, the fictitious KE and the
+    drift, per state, bit for bit up to rounding."""
+    s = sysm
+    rng = np.random.default_rng(5 + iteration)
+    shape = s.psi.shape
+    f = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) * 0.1
+    v = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) * 1e-3
+    dt = 5.0
+    v_or, p_or, ke_or = O.integrate_dyn(f, v, s.psi, s, iteration, dt)
+    ref.ref_integrate_dyn.argtypes = [C.c_int, C.c_int, C.c_double, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int, dp]
+    cm = np.ascontiguousarray(s.cmass, dtype=np.float64)
+    for st in range(s.nstate):
+        ff = np.ascontiguousarray(f[st].copy())
+        vv = np.ascontiguousarray(v[st].copy())
+        pp = np.ascontiguousarray(s.psi[st].copy())
+        ke = C.c_double()
+        ref.ref_integrate_dyn(s.ng, iteration, dt, _d(ff.view(np.float64)), _d(vv.view(np.float64)),
+                              _d(pp.view(np.float64)), _d(cm), s.nkx0_red, s.nkx0_uni, s.nkx0_zero, C.byref(ke))
+        r0 = s.nkx0_red
+        assert np.max(np.abs(vv[r0:] - v_or[st, r0:])) <= 1e-14 * np.max(np.abs(v_or[st]))
+        assert np.max(np.abs(pp[r0:] - p_or[st, r0:])) <= 1e-14 * np.max(np.abs(p_or[st]))
+        assert abs(ke.value - ke_or[st]) <= 1e-13 * abs(ke_or[st])
