@@ -286,8 +286,9 @@ oa_status oa_gpu_cp_run_batch(oa_ctx **ctxs, oa_cp_state **states, int nsys, voi
                               double *energies_out);
 
 /* Allocation-free PairCalculator forward product, for callers that cannot
- * call cudaMalloc (code running during CUDA stream capture, or inside a host
- * framework whose memory pool already holds the device memory).  Same
+ * call cudaMalloc (a host framework whose memory pool already holds the
+ * device memory, or a latency-critical path that cannot take cudaMalloc's
+ * implicit device synchronisation).  Same
  * result as oa_gpu_pc_forward, but it needs no context: the caller passes
  * the sizes (nstate <= 128, ng g-points, nkx0 points on the kx = 0 plane),
  * the device inputs left/right [nstate][ng] complex and the device output
@@ -295,9 +296,10 @@ oa_status oa_gpu_cp_run_batch(oa_ctx **ctxs, oa_cp_state **states, int nsys, voi
  * held by every GPU that loads the library until the process exits; calls
  * whose kernels overlap on one GPU race on it (calls on one stream are
  * ordered).  Larger nstate returns OA_ERR_BAD_ARG.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture.  No counterpart in the
- * reference. */
+ * device looks up the array's device address (cudaGetSymbolAddress) and
+ * caches it for the process (no cudaDeviceReset while the library is
+ * loaded); make that first call before any stream capture.  No counterpart
+ * in the reference. */
 oa_status oa_gpu_pc_forward_noalloc(void *stream, const double *left, const double *right, int nstate, int ng,
                                     int nkx0, double alpha, double w_kx0, double *C);
 

@@ -209,12 +209,12 @@ cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m
                          double w_kx0, double alpha, double* part, int nkb, double* C, const int* cond) {
   if ((K & 1) || (kx0_cols & 1) || (((uintptr_t)A | (uintptr_t)B) & 15) || kx0_cols > K || nkb < 2)
     return cudaErrorNotSupported;
-  static const int nsm = [] {
-    int dev = 0, v = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
-    return v;
-  }();
+  // SM count of the current device (per call: processes may drive GPUs of
+  // different sizes)
+  int dev = 0, nsm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0)
+    nsm = 148;
   const int ti = (m + DG_TM - 1) / DG_TM, tj = (n + DG_TM - 1) / DG_TM;
   // about one CTA per SM; the kx0 region gets CTAs in proportion to its slabs
   const long s0 = (kx0_cols + DG_KS - 1) / DG_KS, sr = (K - kx0_cols + DG_KS - 1) / DG_KS;

@@ -1,10 +1,10 @@
 // Allocation-free PairCalculator forward product.
 //
-// Some callers cannot call cudaMalloc: code running while a CUDA stream is
-// being captured into a graph (an allocation there breaks the capture), code
-// inside a host framework whose memory pool has already reserved the device
-// memory, or latency-critical paths where cudaMalloc's implicit device-wide
-// synchronisation is not acceptable.  oa_gpu_pc_forward needs a context,
+// Some callers cannot call cudaMalloc: code inside a host framework whose
+// memory pool has already reserved the device memory (a further cudaMalloc
+// fails or fragments the pool), or latency-critical paths where
+// cudaMalloc's implicit device-wide synchronisation is not acceptable.
+// oa_gpu_pc_forward needs a context,
 // and creating a context allocates its scratch.  oa_gpu_pc_forward_noalloc
 // computes the same product with no context and no allocation: its split-K
 // partial sums live in a fixed device array declared in this file.
@@ -38,7 +38,10 @@ static std::mutex g_noalloc_mu;
 static double* g_noalloc_addr[OA_NOALLOC_MAX_DEVICES] = {};
 
 // Device address of g_pcfwd_part on the current device, looked up once per
-// device (with that device current) and cached.
+// device (with that device current) and cached for the life of the process.
+// The cache assumes the device's primary context is not reset
+// (cudaDeviceReset) while the library is loaded: after a reset the module
+// may load at another address and the cached one is stale.
 static oa_status noalloc_scratch(double** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);

@@ -1,12 +1,15 @@
 """The allocation-free PairCalculator forward product (oa_gpu_pc_forward_noalloc).
 
-Callers that cannot allocate device memory -- code running during CUDA
-stream capture, or inside a framework whose memory pool already holds the
-device -- call this entry point with their own inputs and output; it keeps
-its split-K scratch in a fixed device array.  This test calls it through the
-C ABI twice in a row with different inputs and compares each result with the
-context-based oa_gpu_pc_forward (same FP64 kernel and reduction order, so the
-tolerance is 1e-13 relative).  It lives in its own file, collected last."""
+Callers that cannot allocate device memory -- a framework whose memory pool
+already holds the device, or a latency-critical path that cannot take
+cudaMalloc's device synchronisation -- call this entry point with their own
+inputs and output; it keeps its split-K scratch in a fixed device array.
+This test calls it through the C ABI twice in a row with different inputs
+and compares each result with the context-based oa_gpu_pc_forward.  Both use
+the FP64 DMMA kernel, but with different split-K partitions of the g-vectors
+(the context path splits over about one CTA per SM, this one over 32 fixed
+partials), so the sums round differently: the tolerance is 1e-13 relative.
+It lives in its own file, collected last."""
 import ctypes as C
 
 import numpy as np
