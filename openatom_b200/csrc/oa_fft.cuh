@@ -47,17 +47,6 @@ template <int SIGN, typename C> OA_HD C cmul_si(C a) {
   return r;
 }
 template <typename C> OA_HD C cscale(C a, decltype(a.x) s) { a.x *= s; a.y *= s; return a; }
-// a * x for a real constant x: in FP32 x is applied as hi + lo (two floats),
-// so the rounding of the constant (sin(2 pi / 3) in float is 1.8e-8 low) puts
-// no systematic bias into the gain of the radix-3 and radix-5 butterflies
-template <typename C> OA_HD C cscale_x(C a, double x);
-template <> OA_HD double2 cscale_x<double2>(double2 a, double x) { a.x *= x; a.y *= x; return a; }
-template <> OA_HD float2 cscale_x<float2>(float2 a, double x) {
-  const float hi = (float)x, lo = (float)(x - (double)hi);
-  a.x = fmaf(a.x, lo, a.x * hi);
-  a.y = fmaf(a.y, lo, a.y * hi);
-  return a;
-}
 
 // ---------------------------------------------------------------------------
 // small DFTs: y_k = sum_r v_r exp(SIGN 2 pi i r k / R)
@@ -75,25 +64,26 @@ template <int SIGN, typename C> OA_HD void dft4(C* v) {
 template <int SIGN, typename C> OA_HD void dft3(C* v) {
   typedef decltype(v[0].x) R;
   const R c1 = (R)-0.5;
-  const double s1 = 0.86602540378443864676372317075294;  // sin(2 pi / 3)
+  const R s1 = (R)0.86602540378443864676372317075294;  // sin(2 pi / 3)
   C t = cadd(v[1], v[2]);
-  C u = cmul_si<SIGN>(cscale_x(csub(v[1], v[2]), s1));
+  C u = cmul_si<SIGN>(cscale(csub(v[1], v[2]), s1));
   C m = cadd(v[0], cscale(t, c1));
   v[0] = cadd(v[0], t);
   v[1] = cadd(m, u);
   v[2] = csub(m, u);
 }
 template <int SIGN, typename C> OA_HD void dft5(C* v) {
-  const double c1 = 0.30901699437494742410229341718282;   // cos(2 pi / 5)
-  const double c2 = -0.80901699437494742410229341718282;  // cos(4 pi / 5)
-  const double s1 = 0.95105651629515357211643933337938;   // sin(2 pi / 5)
-  const double s2 = 0.58778525229247312916870595463907;   // sin(4 pi / 5)
+  typedef decltype(v[0].x) R;
+  const R c1 = (R)0.30901699437494742410229341718282;   // cos(2 pi / 5)
+  const R c2 = (R)-0.80901699437494742410229341718282;  // cos(4 pi / 5)
+  const R s1 = (R)0.95105651629515357211643933337938;   // sin(2 pi / 5)
+  const R s2 = (R)0.58778525229247312916870595463907;   // sin(4 pi / 5)
   C a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
   C a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
-  C m1 = cadd(v[0], cadd(cscale_x(a1, c1), cscale_x(a2, c2)));
-  C m2 = cadd(v[0], cadd(cscale_x(a1, c2), cscale_x(a2, c1)));
-  C n1 = cmul_si<SIGN>(cadd(cscale_x(b1, s1), cscale_x(b2, s2)));
-  C n2 = cmul_si<SIGN>(csub(cscale_x(b1, s2), cscale_x(b2, s1)));
+  C m1 = cadd(v[0], cadd(cscale(a1, c1), cscale(a2, c2)));
+  C m2 = cadd(v[0], cadd(cscale(a1, c2), cscale(a2, c1)));
+  C n1 = cmul_si<SIGN>(cadd(cscale(b1, s1), cscale(b2, s2)));
+  C n2 = cmul_si<SIGN>(csub(cscale(b1, s2), cscale(b2, s1)));
   v[0] = cadd(v[0], cadd(a1, a2));
   v[1] = cadd(m1, n1);
   v[4] = csub(m1, n1);

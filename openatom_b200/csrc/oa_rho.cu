@@ -266,7 +266,7 @@ __device__ void zfft2(double2* a, double2* b, int ld, int nb, const double2* tw)
 }
 
 template <int N1, int N2>
-__global__ void __launch_bounds__(OA_NTHREADS)
+__global__ void __launch_bounds__(OA_NTHREADS, 2)
 k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, int nz,
             OaFftPlan pz, const double2* __restrict__ twz,
             double tpi_l, double vol, double ecut4, double falp2, double gz_term,
@@ -287,13 +287,15 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
   const int nb = min(OA_LB, nlines_d - l0);
   const int nt = 2 * ktab + 1;
   load_twiddles(tw, twz, nz);
-  for (int idx = threadIdx.x; idx < nb * natm; idx += blockDim.x) {
+  int* zoff = (int*)(pxy + OA_LB * natm);  // [natm]: z-phase row of atom ia (type order)
+  for (int ia = threadIdx.x; ia < natm; ia += blockDim.x) zoff[ia] = (atm_perm[ia] * 3 + 2) * nt + ktab;
+  for (int idx = threadIdx.x; idx < OA_LB * natm; idx += blockDim.x) {
     const int lb = idx / natm, ia = idx - lb * natm;
     const int l = l0 + lb;
     const int kx = l / ny;
     int ky = l - kx * ny; if (2 * ky >= ny) ky -= ny;
     double2 v = make_double2(0.0, 0.0);
-    if (kx <= ktab && abs(ky) <= ktab) {
+    if (lb < nb && kx <= ktab && abs(ky) <= ktab) {
       const double2* ph = phase + (size_t)atm_perm[ia] * 3 * nt;
       v = cmul(ph[kx + ktab], ph[nt + ky + ktab]);
     }
@@ -314,59 +316,95 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
   const double pi = 3.14159265358979323846;
   const double fpi = 4.0 * pi;
   double acc[3] = {0.0, 0.0, 0.0};
-  for (int idx = threadIdx.x; idx < nb * nz; idx += blockDim.x) {
-    const int lb = idx / nz, zz = idx - lb * nz;
-    const int l = l0 + lb;
-    const int kx = l / ny;
-    int ky = l - kx * ny; if (2 * ky >= ny) ky -= ny;
+  // One thread per (z, group of ZP_L lines): every z-phase load of the atom
+  // sums serves ZP_L g-points (the z phase depends on kz and the atom only),
+  // and the atoms' z-phase rows are addressed through zoff in shared memory.
+  constexpr int ZP_L = 2;
+  const int ngrp = (nb + ZP_L - 1) / ZP_L;
+  for (int idx = threadIdx.x; idx < ngrp * nz; idx += blockDim.x) {
+    const int grp = idx / nz, zz = idx - grp * nz;
     int kz = zz; if (2 * kz >= nz) kz -= nz;
-    const double gx = tpi_l * kx, gy = tpi_l * ky, gzv = tpi_l * kz;
-    const double g2 = gx * gx + gy * gy + gzv * gzv;
-    double2 rho = r[lb * ldz + zz];
-    double2 out = make_double2(0.0, 0.0);
-    if (g2 == 0.0) {
-      out.x = gz_term;
-      acc[1] += gz_term * rho.x;
-    } else if (g2 <= ecut4 && abs(kx) <= ktab && abs(ky) <= ktab && abs(kz) <= ktab) {
-      const double wn = (kx == 0) ? 1.0 : 2.0;
-      const double hf = fpi / (g2 * vol);
-      acc[0] += hf * (rho.x * rho.x + rho.y * rho.y) * wn;
-      out.x = rho.x * hf; out.y = rho.y * hf;
-      // structure factors per type and for the Ewald charge sum
-      double2 sf[4] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
-      double2 sewd = make_double2(0.0, 0.0);
-      const double2* pl = pxy + lb * natm;
+    const double gzv = tpi_l * kz;
+    double2 rho[ZP_L], sf_q[ZP_L], vext[ZP_L];
+    double g2v[ZP_L], hh[ZP_L], wn[ZP_L];
+    int cls[ZP_L], ii[ZP_L];  // cls: 0 outside, 1 g = 0, 2 inside the density sphere
+    bool any = false;
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        if (t >= ntype) break;
+    for (int j = 0; j < ZP_L; ++j) {
+      const int lb = grp * ZP_L + j;
+      cls[j] = 0; ii[j] = 1; hh[j] = 0.0; wn[j] = 1.0; g2v[j] = 0.0;
+      rho[j] = make_double2(0.0, 0.0);
+      sf_q[j] = make_double2(0.0, 0.0);
+      vext[j] = make_double2(0.0, 0.0);
+      if (lb >= nb) continue;
+      const int l = l0 + lb;
+      const int kx = l / ny;
+      int ky = l - kx * ny; if (2 * ky >= ny) ky -= ny;
+      const double gx = tpi_l * kx, gy = tpi_l * ky;
+      const double g2 = gx * gx + gy * gy + gzv * gzv;
+      g2v[j] = g2;
+      rho[j] = r[lb * ldz + zz];
+      if (g2 == 0.0) {
+        cls[j] = 1;
+      } else if (g2 <= ecut4 && abs(kx) <= ktab && abs(ky) <= ktab && abs(kz) <= ktab) {
+        cls[j] = 2;
+        any = true;
+        wn[j] = (kx == 0) ? 1.0 : 2.0;
+        // spline interval of the local pseudopotential (CP_get_vpsnow, cp_hart_ext.C:433-480)
+        const double g = sqrt(g2);
+        int i1 = (int)((g - gmin) / dg + 1.0);
+        i1 = min(i1, nspl); i1 = max(i1, 1);
+        ii[j] = i1;
+        hh[j] = g - ((double)(i1 - 1) * dg + gmin);
+      }
+    }
+    if (any) {
+      // structure factors per type, S_t(g) = sum_{a in t} pxy[line][a] e^{i gz z_a},
+      // then V_ext = sum_t S_t v_t(|g|) / V and the Ewald charge sum sum_t q_t S_t
+      for (int t = 0; t < ntype && t < 4; ++t) {
+        double2 st[ZP_L];
+#pragma unroll
+        for (int j = 0; j < ZP_L; ++j) st[j] = make_double2(0.0, 0.0);
+        const double2* pl = pxy + grp * ZP_L * natm;
         for (int ia = toff.off[t]; ia < toff.off[t + 1]; ++ia) {
-          const double2 hz = phase[(size_t)atm_perm[ia] * 3 * nt + 2 * nt + kz + ktab];
-          const double2 h = cmul(pl[ia], hz);
-          sf[t].x += h.x; sf[t].y += h.y;
+          const double2 hz = phase[zoff[ia] + kz];
+#pragma unroll
+          for (int j = 0; j < ZP_L; ++j) {
+            const double2 h = cmul(pl[j * natm + ia], hz);
+            st[j].x += h.x; st[j].y += h.y;
+          }
         }
         const double qa = q_type[t];
-        sewd.x += qa * sf[t].x; sewd.y += qa * sf[t].y;
-      }
-      // spline of the local pseudopotential per type (CP_get_vpsnow, cp_hart_ext.C:433-480)
-      const double g = sqrt(g2);
-      int ii = (int)((g - gmin) / dg + 1.0);
-      ii = min(ii, nspl); ii = max(ii, 1);
-      const double h0 = (double)(ii - 1) * dg + gmin;
-      const double hh = g - h0;
-      double2 vext = make_double2(0.0, 0.0);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        if (t >= ntype) break;
-        const double* cc = spl + ((size_t)t * nspl + (ii - 1)) * 4;
-        const double vt = (((cc[3] * hh + cc[2]) * hh + cc[1]) * hh + cc[0]) / vol;
-        vext.x += sf[t].x * vt; vext.y += sf[t].y * vt;
+        for (int j = 0; j < ZP_L; ++j) {
+          if (cls[j] != 2) continue;
+          sf_q[j].x += qa * st[j].x; sf_q[j].y += qa * st[j].y;
+          const double* cc = spl + ((size_t)t * nspl + (ii[j] - 1)) * 4;
+          const double vt = (((cc[3] * hh[j] + cc[2]) * hh[j] + cc[1]) * hh[j] + cc[0]) / vol;
+          vext[j].x += st[j].x * vt; vext[j].y += st[j].y * vt;
+        }
       }
-      const double ewf = fpi * exp(-g2 / falp2) / (g2 * vol);
-      acc[2] += ewf * (sewd.x * sewd.x + sewd.y * sewd.y) * wn;
-      out.x += vext.x; out.y -= vext.y;            // vks += conj(vext)
-      acc[1] += (rho.x * vext.x - rho.y * vext.y) * wn;  // Re(rho vext)
     }
-    r[lb * ldz + zz] = out;
+#pragma unroll
+    for (int j = 0; j < ZP_L; ++j) {
+      const int lb = grp * ZP_L + j;
+      if (lb >= nb) continue;
+      double2 out = make_double2(0.0, 0.0);
+      if (cls[j] == 1) {
+        out.x = gz_term;
+        acc[1] += gz_term * rho[j].x;
+      } else if (cls[j] == 2) {
+        const double g2 = g2v[j];
+        const double hf = fpi / (g2 * vol);
+        acc[0] += hf * (rho[j].x * rho[j].x + rho[j].y * rho[j].y) * wn[j];
+        out.x = rho[j].x * hf; out.y = rho[j].y * hf;
+        const double ewf = fpi * exp(-g2 / falp2) / (g2 * vol);
+        acc[2] += ewf * (sf_q[j].x * sf_q[j].x + sf_q[j].y * sf_q[j].y) * wn[j];
+        out.x += vext[j].x; out.y -= vext[j].y;            // vks += conj(vext)
+        acc[1] += (rho[j].x * vext[j].x - rho[j].y * vext[j].y) * wn[j];  // Re(rho vext)
+      }
+      r[lb * ldz + zz] = out;
+    }
   }
   __syncthreads();
   double2* r2;
@@ -452,7 +490,8 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
   auto zpass = [&](auto kern, int ldb) -> cudaError_t {
     const size_t smz =
         (align_up_r(c->nz, 2) + (size_t)OA_LB * (c->nz + 1) + (size_t)OA_LB * ldb + (size_t)OA_LB * c->natm) *
-        sizeof(double2);
+            sizeof(double2) +
+        (size_t)c->natm * sizeof(int);  // zoff
     if (smz > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
     cudaError_t e2 = oa_smem_limit(kern);
     if (e2 != cudaSuccess) return e2;
