@@ -20,6 +20,7 @@ extern "C" {
 oa_status oa_gpu_state_fft_fwd(oa_ctx* ctx, void* stream, const double* psi, double* rho_out);
 oa_status oa_gpu_vks_build(oa_ctx* ctx, void* stream, double* vks_out);
 oa_status oa_gpu_nl_sf(oa_ctx* ctx, void* stream, const double* psi, int nterm, double* fnl_out, double* enl_out);
+oa_status oa_gpu_nl_ees(oa_ctx* ctx, void* stream, const double* psi, double* fnl_out, double* enl_out);
 oa_status oa_gpu_vks_apply_fft_bwd(oa_ctx* ctx, void* stream, const double* psi, int recompute_fwd,
                                    const double* fnl, double* force, double* eke_out);
 oa_status oa_gpu_pc_forward(oa_ctx* ctx, void* stream, const double* left, const double* right, double alpha,
@@ -159,7 +160,11 @@ static oa_status launch_step_a(oa_ctx* c, cudaStream_t s, oa_cp_state* st, int c
   // forces on the orthonormal psi (computePsiFandVKS, ParticlePlane, combineForcesGetEke)
   OA_STEP_TRY(oa_gpu_state_fft_fwd(c, s, st->psi, nullptr));
   OA_STEP_TRY(oa_gpu_vks_build(c, s, nullptr));
-  OA_STEP_TRY(oa_gpu_nl_sf(c, s, st->psi, nt, w->Fnl, nullptr));
+  // nonlocal: the EES method once oa_gpu_ees_init enabled it
+  // (cp_nonloc_ees_opt; CP_State_ParticlePlane.C:867-1136), else the
+  // structure-factor method (StructureFactor.C:35-113)
+  if (c->ees) OA_STEP_TRY(oa_gpu_nl_ees(c, s, st->psi, w->Fnl, nullptr));
+  else OA_STEP_TRY(oa_gpu_nl_sf(c, s, st->psi, nt, w->Fnl, nullptr));
   if (nt) oa_planes_force_begin(c, nt);
   const oa_status rf = oa_gpu_vks_apply_fft_bwd(c, s, st->psi, 0, w->Fnl, w->F, nullptr);
   oa_planes_force_end(c, w->F);
@@ -223,7 +228,7 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
   OA_CUDA_TRY(cudaMemsetAsync(w->flag, 0, 4 * sizeof(int), s));
   // the psi planes of the mixed products, from the psi the caller hands in
   if (st->mixed_nterm) OA_STEP_TRY(oa_planes_psi_refresh(c, s, st->psi, st->mixed_nterm));
-  const void* key[7] = {st->psi, st->psi_t, st->vpsi, st->T, stream, w->ring, nullptr};
+  const void* key[7] = {st->psi, st->psi_t, st->vpsi, st->T, stream, w->ring, c->ees};
   // the legacy default stream cannot be captured: launch eagerly there
   const bool capturable = s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread;
   // the cluster Newton-Schulz kernel is an ordinary launch: then the whole

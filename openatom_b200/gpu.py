@@ -382,11 +382,20 @@ class CPDriver:
     """Host runner of the CP dynamics step on one GPU (electrons; ions fixed)."""
 
     def __init__(self, sysm, precision: str = "fp64", tol: float = 1e-15, max_iter: int = 1000,
-                 psi0=None, norb_tol: float = 0.003):
+                 psi0=None, norb_tol: float = 0.003, nl_method: str = "sf", ees_order: int = 6,
+                 ees_scale: float = 1.2):
         import torch
         self.torch = torch
         self.sys = sysm
         self.ctx = CPContext(sysm, precision)
+        # nonlocal method (cp_nonloc_ees_opt): "sf" structure factor (N^2) or
+        # "ees" (Euler exponential splines of order ees_order on the
+        # nonlocal grid); the native step follows the context's choice
+        if nl_method not in ("sf", "ees"):
+            raise ValueError("nl_method must be 'sf' or 'ees'")
+        self.nl_method = nl_method
+        if nl_method == "ees":
+            self.ctx.ees_init(ees_scale, ees_order)
         dev = torch.device("cuda")
         n, ng = sysm.nstate, sysm.ng
         p0 = sysm.psi if psi0 is None else psi0
@@ -420,7 +429,10 @@ class CPDriver:
         c = self.ctx
         c.state_fft_fwd(self.psi)
         c.vks_build()
-        c.nl_sf(self.psi, self.Fnl, nterm=self.nterm_nl)
+        if self.nl_method == "ees":
+            c.nl_ees(self.psi, self.Fnl)
+        else:
+            c.nl_sf(self.psi, self.Fnl, nterm=self.nterm_nl)
         c.vks_apply_fft_bwd(self.psi, self.F, fnl=self.Fnl)
 
     def native_state(self, use_graph: bool = True) -> CPState:
