@@ -383,7 +383,7 @@ class CPDriver:
 
     def __init__(self, sysm, precision: str = "fp64", tol: float = 1e-15, max_iter: int = 1000,
                  psi0=None, norb_tol: float = 0.003, nl_method: str = "sf", ees_order: int = 6,
-                 ees_scale: float = 1.2):
+                 ees_scale: float = 1.2, v0=None):
         import torch
         self.torch = torch
         self.sys = sysm
@@ -401,7 +401,7 @@ class CPDriver:
         p0 = sysm.psi if psi0 is None else psi0
         self.psi_t = torch.from_numpy(np.ascontiguousarray(p0)).to(dev)   # non-orthogonal, integrated
         self.psi = self.psi_t.clone()                                     # orthonormal psi_t T
-        self.v = torch.zeros_like(self.psi)
+        self.v = torch.zeros_like(self.psi) if v0 is None else torch.from_numpy(np.ascontiguousarray(v0)).to(dev)
         self.F = torch.zeros_like(self.psi)
         self.F2 = torch.zeros_like(self.psi)
         self.Fnl = torch.zeros_like(self.psi)
