@@ -122,6 +122,25 @@ oa_status oa_gpu_vks_apply_fft_bwd(oa_ctx *ctx, void *stream, const double *psi,
 oa_status oa_gpu_pc_forward(oa_ctx *ctx, void *stream, const double *left, const double *right,
                             double alpha, double w_kx0, double *C);
 
+/* The symmetric PairCalculator overlap of the mixed form on the int8 tensor
+ * cores, S = alpha * sum_k w(k) psi_t_x(k) psi_t_y(k) (the same product as
+ * oa_gpu_pc_forward(psi_t, psi_t), ckPairCalculator.C:821-893, with the
+ * reduction :938-1016), to FP64 accuracy: psi_t is split into six int8
+ * digits per value with one exponent per state and K range, the digit
+ * products are exact in int32 and combined in FP64 (relative error about
+ * 2^-42 of the largest value of a range).  The digits stay in the context
+ * for oa_gpu_pc_rotate_i8.  Mixed-precision contexts with at most 128
+ * states; OA_ERR_UNSUPPORTED otherwise. */
+oa_status oa_gpu_pc_overlap_i8(oa_ctx *ctx, void *stream, const double *psi_t, double alpha, double w_kx0,
+                               double *S);
+
+/* psi_out = psi_t T (psi_out_j = sum_i T[i][j] psi_t_i; bwMultiplyHelper
+ * 'N','N', ckPairCalculator.C:1710-1946) on the int8 tensor cores, to FP64
+ * accuracy, from the digits of psi_t taken by the last
+ * oa_gpu_pc_overlap_i8 on this context (OA_ERR_BAD_ARG if psi_t is another
+ * array).  T: device [nstate][nstate]; psi_out must not alias psi_t. */
+oa_status oa_gpu_pc_rotate_i8(oa_ctx *ctx, void *stream, const double *T, const double *psi_t, double *psi_out);
+
 /* Ortho S -> T = (S/2)^(-1/2) by Newton-Schulz (ortho.C:109-146, 153-266,
  * 848-971; same iteration as CPORTHOG::get_iter_Tmat, cp_lowdin.C:180-265).
  * S, T: device [n][n].  Synchronises the stream to return iterations,
@@ -201,16 +220,19 @@ oa_status oa_gpu_psiv_reset_mixed(oa_ctx *ctx, void *stream, const double *psi, 
 oa_status oa_gpu_set_atoms(oa_ctx *ctx, void *stream, const double *pos_host);
 
 /* Average device time (ms, CUDA events on `stream`) of each kernel of the
- * step over `reps` launches on the given orthonormal psi: ms_out[0..8] =
+ * step over `reps` launches on the given orthonormal psi: ms_out[0..10] =
  * state z pass fwd, state plane pass + density, density sum + XC, V_KS build
  * (density FFT, Hartree/local, inverse), state plane pass with V_KS,
- * state z pass bwd + EKE, PairCalculator forward (S), PairCalculator
- * backward (two-term), Newton-Schulz.  Clobbers the context's scratch.
+ * state z pass bwd + EKE, PairCalculator forward S, PairCalculator
+ * backward (two-term, the constraint force), Newton-Schulz, the rotation
+ * Psi T, the PairCalculator forward Lambda -- each as the context's form
+ * runs it in the step (mixed: S and Psi T on int8 digits, the two-term
+ * backward and Lambda split-BF16).  Clobbers the context's scratch.
  * No reference counterpart (it replaces the Projections user events of
  * e.g. CP_State_GSpacePlane.C:1407-1409). */
 oa_status oa_gpu_time_kernels(oa_ctx *ctx, void *stream, const double *psi, int reps, double *ms_out);
 
-/* Sizes for byte/flop accounting (see oa_abi.cu): out[0..11]. */
+/* Sizes for byte/flop accounting (see oa_abi.cu): out[0..12]. */
 oa_status oa_gpu_sizes(const oa_ctx *ctx, long *out);
 
 /* Nonlocal energy and coefficient forces by the structure-factor method

@@ -81,6 +81,16 @@ extern "C" const char* oa_gpu_last_error(void) { return g_err; }
     if (!(cond)) { oa_set_error(msg, __FILE__, __LINE__); return OA_ERR_BAD_ARG; } \
   } while (0)
 
+// FP64-accurate int8 tensor-core products of the mixed form (oa_ozaki.cu)
+struct oa_oz;
+oa_oz* oa_oz_create(int n, int ng, int nkx0, int nsm);
+void oa_oz_free(oa_oz* z);
+size_t oa_oz_bytes(const oa_oz* z);
+cudaError_t oa_oz_overlap(oa_oz* z, cudaStream_t s, const double* X, long ldx, double alpha, double w_kx0,
+                          double* S, int* err_flag, const int* cond);
+cudaError_t oa_oz_rotate(oa_oz* z, cudaStream_t s, const double* T, const double* X, double* out, long ldo,
+                         const OaPlaneOut* po, int* err_flag, const int* cond);
+
 // extra per-context PC/Ortho/integrator scratch lives behind the struct
 struct oa_ctx_pc {
   double* part;      // split-K partials
@@ -113,6 +123,7 @@ struct oa_ctx_pc {
   int pl_cache;
   int* err_flag;     // device: set by a kernel whose bounded wait ran out
   int nsm;
+  oa_oz* oz;         // int8 overlap / rotation (mixed form, up to 128 states)
 };
 
 static oa_ctx_pc* pcx(oa_ctx* c);
@@ -398,6 +409,9 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     }
     TRY(cudaMallocHost(&p->h_status, 4 * sizeof(int)));
     TRY(cudaMallocHost(&p->h_vals, 16 * sizeof(double)));
+    // the mixed form runs S and Psi T as int8 digit products (FP64 accuracy);
+    // without them (above 128 states) it keeps the FP64 DMMA products
+    if (c->precision == OA_MIXED) p->oz = oa_oz_create(d->nstate, d->ng, d->nkx0, nsm);
     TRY(cudaDeviceSynchronize());
   }
 #undef TRY
@@ -417,6 +431,8 @@ extern "C" oa_status oa_gpu_destroy(oa_ctx* c) {
   oa_step_free(c);
   ees_free(c);
   oa_ctx_pc* p = pcx(c);
+  oa_oz_free(p->oz);
+  p->oz = nullptr;
   void* dev[] = {c->line_kx, c->line_ky, c->line_off, c->line_nneg, c->line_npos, c->kx, c->g2, c->tw_x, c->tw_y,
                  c->tw_z, c->spl, c->q_type, c->atm_type, c->atm_perm, c->pos, c->psir, c->pair_cols, c->phase, c->occ, c->zbuf, c->rho_part, c->rho,
                  c->vks, c->vxc, c->dz, c->red, c->eke_part, p->part, p->ns_work, p->ns_status, p->ns_err,
@@ -540,6 +556,42 @@ extern "C" oa_status oa_gpu_pc_forward(oa_ctx* c, void* stream, const double* le
   return OA_OK;
 }
 
+extern "C" oa_status oa_gpu_pc_overlap_i8(oa_ctx* c, void* stream, const double* psi_t, double alpha,
+                                          double w_kx0, double* S) {
+  OA_ARG_CHECK(c && psi_t && S, "null argument");
+  oa_ctx_pc* p = pcx(c);
+  if (!p->oz) {
+    oa_set_error("the int8 overlap needs a mixed-precision context with at most 128 states", __FILE__, __LINE__);
+    return OA_ERR_UNSUPPORTED;
+  }
+  OA_CUDA_TRY(oa_oz_overlap(p->oz, (cudaStream_t)stream, psi_t, 2L * c->ng, alpha, w_kx0, S, p->err_flag, nullptr));
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_pc_rotate_i8(oa_ctx* c, void* stream, const double* T, const double* psi_t,
+                                         double* psi_out) {
+  OA_ARG_CHECK(c && T && psi_t && psi_out, "null argument");
+  OA_ARG_CHECK(psi_out != psi_t, "psi_out must not alias psi_t");
+  oa_ctx_pc* p = pcx(c);
+  if (!p->oz) {
+    oa_set_error("the int8 rotation needs a mixed-precision context with at most 128 states", __FILE__, __LINE__);
+    return OA_ERR_UNSUPPORTED;
+  }
+  const cudaError_t e = oa_oz_rotate(p->oz, (cudaStream_t)stream, T, psi_t, psi_out, 2L * c->ng, nullptr,
+                                     p->err_flag, nullptr);
+  if (e == cudaErrorNotSupported) {
+    oa_set_error("oa_gpu_pc_rotate_i8: psi_t is not the operand of the last oa_gpu_pc_overlap_i8", __FILE__,
+                 __LINE__);
+    return OA_ERR_BAD_ARG;
+  }
+  OA_CUDA_TRY(e);
+  // psi_out changed: planes of psi must be split again when a product needs them
+  p->pl_key[0].valid = false;
+  return OA_OK;
+}
+
+int oa_oz_enabled(oa_ctx* c) { return pcx(c)->oz != nullptr; }
+
 extern "C" oa_status oa_gpu_ortho_invsqrt(oa_ctx* c, void* stream, const double* S, double* T, double tol,
                                           int max_iter, int* iters_out, double* err_out, double* smax_out) {
   OA_ARG_CHECK(c && S && T && max_iter > 0, "bad argument");
@@ -652,12 +704,12 @@ cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, 
 
 #define OA_ALIGN_TRY(x)                                                                       \
   do {                                                                                        \
-    const cudaError_t e_ = (x);                                                               \
-    if (e_ == cudaErrorNotSupported) {                                                        \
+    const cudaError_t ea_ = (x);                                                              \
+    if (ea_ == cudaErrorNotSupported) {                                                       \
       oa_set_error("coefficient arrays must be 16-byte aligned", __FILE__, __LINE__);         \
       return OA_ERR_BAD_ARG;                                                                  \
     }                                                                                         \
-    OA_CUDA_TRY(e_);                                                                          \
+    OA_CUDA_TRY(ea_);                                                                          \
   } while (0)
 
 extern "C" oa_status oa_gpu_set_atoms(oa_ctx* c, void* stream, const double* pos_host) {
@@ -671,6 +723,14 @@ extern "C" oa_status oa_gpu_set_atoms(oa_ctx* c, void* stream, const double* pos
 // for the roofline: ms_out[0..8] = state_zfwd, state_plane_density, rho_xc,
 // vks_build (density FFT + Hartree/local + inverse), state_plane_vks,
 // state_zbwd, pc_forward (S), pc_backward (two-term), ortho_ns.
+static cudaError_t mixed_fwd(oa_ctx* c, cudaStream_t s, int nt, const double* A, const double* B, int m, int n,
+                             long K, long kx0_cols, double w_kx0, double alpha, double* C, int sa, int sb,
+                             const int* cond = nullptr);
+static cudaError_t mixed_bwd(oa_ctx* c, cudaStream_t s, int nt, const double* M1, const double* X1, double a1_kx0,
+                             double a1_rest, const double* M2, const double* X2, double a2, int nj, int nk, long ncol,
+                             long kx0_cols, double* out, int s1, int s2, const double* yadd = nullptr,
+                             const int* cond = nullptr);
+
 extern "C" oa_status oa_gpu_time_kernels(oa_ctx* c, void* stream, const double* psi, int reps, double* ms_out) {
   OA_ARG_CHECK(c && psi && ms_out && reps > 0, "bad argument");
   cudaStream_t s = (cudaStream_t)stream;
@@ -679,10 +739,17 @@ extern "C" oa_status oa_gpu_time_kernels(oa_ctx* c, void* stream, const double* 
   OA_CUDA_TRY(cudaEventCreate(&e0));
   OA_CUDA_TRY(cudaEventCreate(&e1));
   float ms = 0.f;
-  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double acc[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   const int n = c->nstate;
   double* S = p->mat_a;
   double* T = p->mat_x;
+  const bool mixed = c->precision == OA_MIXED;
+  // the second big operand of the timed products (F, or psi itself)
+  double* F = (double*)p->vtmp;
+  // an output of the same size: the z-line buffer (at least nstate x nz x
+  // nlines complex in the compute precision, which covers nstate x 2 ng doubles)
+  double* G = (double*)c->zbuf;
+  const long K = 2L * c->ng, K0 = 2L * c->nkx0;
   for (int r = 0; r < reps; ++r) {
 #define OA_TIME(slot, call)                                   \
     OA_CUDA_TRY(cudaEventRecord(e0, s));                      \
@@ -697,22 +764,47 @@ extern "C" oa_status oa_gpu_time_kernels(oa_ctx* c, void* stream, const double* 
     OA_TIME(3, oa_launch_rho_fft_hart(c, s));
     OA_TIME(4, oa_launch_state_plane_vks(c, s));
     OA_TIME(5, oa_launch_state_zbwd(c, s, (const double2*)psi, nullptr, (double2*)p->vtmp, 0, n));
-    OA_TIME(6, oa_launch_pc_fwd(s, psi, psi, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, S));
-    OA_TIME(7, oa_launch_pc_bwd(s, p->eye, psi, -0.5, -1.0, p->eye, psi, 1.0, n, 2L * c->ng, 2L * c->nkx0,
-                                p->vtmp));
+    if (mixed && p->oz) {
+      OA_TIME(6, oa_oz_overlap(p->oz, s, psi, K, 2.0, 0.5, S, p->err_flag, nullptr));
+    } else {
+      OA_TIME(6, oa_launch_pc_fwd(s, psi, psi, n, K, K0, 0.5, 2.0, p->part, p->nkb, S));
+    }
+    OA_CUDA_TRY(cudaMemcpyAsync(F, psi, (size_t)n * c->ng * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    if (mixed) {
+      // the bf16 planes of psi and F are made by their producers in the
+      // step: split them once, untimed, and reuse them (plane cache on)
+      p->pl_cache = 1;
+      p->pl_key[0].valid = p->pl_key[1].valid = false;
+      OA_CUDA_TRY(mixed_bwd(c, s, 3, p->eye, psi, -0.5, -1.0, p->eye, F, 1.0, n, n, K, K0, G, 0, 1));
+      OA_TIME(7, mixed_bwd(c, s, 3, p->eye, psi, -0.5, -1.0, p->eye, F, 1.0, n, n, K, K0, G, 0, 1));
+      OA_TIME(10, mixed_fwd(c, s, 3, psi, F, n, n, K, K0, 1.0, 1.0, S, 0, 1));
+      p->pl_cache = 0;
+      p->pl_key[0].valid = p->pl_key[1].valid = p->pl_key[2].valid = false;
+    } else {
+      OA_TIME(7, oa_launch_pc_bwd(s, p->eye, psi, -0.5, -1.0, p->eye, F, 1.0, n, K, K0, G));
+      OA_TIME(10, oa_launch_pc_fwd(s, psi, F, n, K, K0, 1.0, 1.0, p->part, p->nkb, S));
+    }
     OA_TIME(8, oa_launch_ortho_ns(s, S, n, 0.5, 1e-15, 1000, p->ns_work, T, p->ns_status, p->ns_err,
                                   ns_launch_grid(p)));
+    if (mixed && p->oz) {
+      // S first: the rotation uses the digits the overlap took of psi
+      OA_CUDA_TRY(oa_oz_overlap(p->oz, s, psi, K, 2.0, 0.5, S, p->err_flag, nullptr));
+      OA_TIME(9, oa_oz_rotate(p->oz, s, T, psi, G, K, nullptr, p->err_flag, nullptr));
+    } else {
+      OA_TIME(9, oa_launch_pc_bwd(s, T, psi, 1.0, 1.0, nullptr, nullptr, 0.0, n, K, K0, G));
+    }
 #undef OA_TIME
   }
-  for (int k = 0; k < 9; ++k) ms_out[k] = acc[k] / reps;
+  for (int k = 0; k < 11; ++k) ms_out[k] = acc[k] / reps;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return OA_OK;
 }
 
-// Problem sizes a caller needs for byte/flop accounting: out[0..9] =
+// Problem sizes a caller needs for byte/flop accounting: out[0..12] =
 // nstate, ng, nlines, nz, ldl, ngroup, npts, compute-precision bytes per
-// real, nlines_d, kernel launches per CP step of the host runner.
+// real, nlines_d, kernel launches per CP step of the host runner, state-pair
+// plane kernels in use, their state groups, int8 overlap / rotation in use.
 extern "C" oa_status oa_gpu_sizes(const oa_ctx* c, long* out) {
   OA_ARG_CHECK(c && out, "null argument");
   out[0] = c->nstate; out[1] = c->ng; out[2] = c->nlines; out[3] = c->nz; out[4] = c->ldl;
@@ -723,6 +815,7 @@ extern "C" oa_status oa_gpu_sizes(const oa_ctx* c, long* out) {
   out[9] = 3 + 5 + 7 + 4 + 4 + 3 + 2 + 1 + 1;
   out[10] = c->pair_cols ? 1 : 0;  // state-pair plane kernels in use (mixed form)
   out[11] = c->ngroup_pair;
+  out[12] = pcx(const_cast<oa_ctx*>(c))->oz ? 1 : 0;  // int8 overlap / rotation available
   return OA_OK;
 }
 
@@ -819,7 +912,7 @@ oa_status oa_planes_psi_refresh(oa_ctx* c, cudaStream_t s, const double* psi, in
 // plane slots sa and sb.
 static cudaError_t mixed_fwd(oa_ctx* c, cudaStream_t s, int nt, const double* A, const double* B, int m, int n,
                              long K, long kx0_cols, double w_kx0, double alpha, double* C, int sa, int sb,
-                             const int* cond = nullptr) {
+                             const int* cond) {
   oa_ctx_pc* p = pcx(c);
   const int mx = c->nstate > c->natm_nl ? c->nstate : c->natm_nl;
   const int nb = oa_tg_nb_fwd(n);
@@ -848,8 +941,8 @@ static cudaError_t mixed_fwd(oa_ctx* c, cudaStream_t s, int nt, const double* A,
 // X1, X2 in plane slots s1, s2.
 static cudaError_t mixed_bwd(oa_ctx* c, cudaStream_t s, int nt, const double* M1, const double* X1, double a1_kx0,
                              double a1_rest, const double* M2, const double* X2, double a2, int nj, int nk, long ncol,
-                             long kx0_cols, double* out, int s1, int s2, const double* yadd = nullptr,
-                             const int* cond = nullptr) {
+                             long kx0_cols, double* out, int s1, int s2, const double* yadd,
+                             const int* cond) {
   oa_ctx_pc* p = pcx(c);
   const int mx = c->nstate > c->natm_nl ? c->nstate : c->natm_nl;
   int nkp = oa_tg_rows_pad(nk, 32);
@@ -949,8 +1042,14 @@ oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* 
   const int n = c->nstate;
   OaPlaneOut po;
   bool fuse = nterm > 0 && plane_out(c, PL_PSI, n, nterm, &po);
-  cudaError_t e = oa_dgemm_bwd_ex(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, psi,
-                                  nullptr, nullptr, nullptr, nullptr, fuse ? &po : nullptr);
+  // mixed form: the int8 rotation from the digits the overlap product took
+  // of psi_t (FP64 accuracy); otherwise FP64 DMMA
+  cudaError_t e = cudaErrorNotSupported;
+  if (nterm > 0 && p->oz)
+    e = oa_oz_rotate(p->oz, s, T, psi_t, psi, 2L * c->ng, fuse ? &po : nullptr, p->err_flag, nullptr);
+  if (e == cudaErrorNotSupported)
+    e = oa_dgemm_bwd_ex(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, psi,
+                        nullptr, nullptr, nullptr, nullptr, fuse ? &po : nullptr);
   if (e == cudaErrorNotSupported) {
     // above 128 states: the general kernel, and the psi planes are split
     // again when a product needs them

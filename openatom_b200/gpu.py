@@ -72,6 +72,8 @@ SIGNATURES = {
     "oa_gpu_set_vks": (C.c_int, [_vp, _vp, _vp]),
     "oa_gpu_vks_apply_fft_bwd": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp, _vp]),
     "oa_gpu_pc_forward": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_double, _vp]),
+    "oa_gpu_pc_overlap_i8": (C.c_int, [_vp, _vp, _vp, C.c_double, C.c_double, _vp]),
+    "oa_gpu_pc_rotate_i8": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "oa_gpu_ortho_invsqrt": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_int, _ip, _dp, _dp]),
     "oa_gpu_pc_backward": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_double, _vp, _vp, C.c_double, _vp]),
     "oa_gpu_small_gemm": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, _vp]),
@@ -99,7 +101,7 @@ SIGNATURES = {
 }
 
 KERNEL_NAMES = ("state_zfwd", "state_plane_density", "rho_xc", "vks_build", "state_plane_vks",
-                "state_zbwd", "pc_forward_S", "pc_backward", "ortho_ns")
+                "state_zbwd", "pc_forward_S", "pc_backward", "ortho_ns", "pc_rotate", "pc_forward_lambda")
 
 _lib = None
 
@@ -246,6 +248,19 @@ class CPContext:
         _check(self._lib.oa_gpu_pc_forward(self._h, self._stream(), _ptr(left), _ptr(right),
                                            float(alpha), float(w_kx0), _ptr(out)))
 
+    def pc_overlap_i8(self, psi_t, alpha, w_kx0, out):
+        """S = alpha sum w psi_t psi_t^T on the int8 tensor cores (FP64 accuracy)."""
+        _check(self._lib.oa_gpu_pc_overlap_i8(self._h, self._stream(), _ptr(psi_t), float(alpha), float(w_kx0),
+                                              _ptr(out)))
+
+    def pc_rotate_i8(self, T, psi_t, out):
+        """out = psi_t T from the digits of the last pc_overlap_i8 (FP64 accuracy)."""
+        _check(self._lib.oa_gpu_pc_rotate_i8(self._h, self._stream(), _ptr(T), _ptr(psi_t), _ptr(out)))
+
+    def has_i8(self) -> bool:
+        """True when the int8 overlap / rotation are available (mixed form, <= 128 states)."""
+        return bool(self.sizes()["int8_products"])
+
     def ortho_invsqrt(self, S, T, tol=1e-15, max_iter=1000, with_smax=False):
         it = C.c_int(0)
         err = C.c_double(0.0)
@@ -298,14 +313,14 @@ class CPContext:
         _check(self._lib.oa_gpu_set_atoms(self._h, self._stream(), a.ctypes.data_as(_dp)))
 
     def sizes(self) -> dict:
-        out = (C.c_long * 12)()
+        out = (C.c_long * 13)()
         _check(self._lib.oa_gpu_sizes(self._h, out))
         keys = ("nstate", "ng", "nlines", "nz", "ldl", "ngroup", "npts", "rbytes", "nlines_d", "launches_per_step",
-                "pair_planes", "ngroup_pair")
+                "pair_planes", "ngroup_pair", "int8_products")
         return {k: int(v) for k, v in zip(keys, out)}
 
     def time_kernels(self, psi, reps: int = 5) -> dict:
-        out = (C.c_double * 9)()
+        out = (C.c_double * len(KERNEL_NAMES))()
         _check(self._lib.oa_gpu_time_kernels(self._h, self._stream(), _ptr(psi), int(reps), out))
         return {k: float(v) for k, v in zip(KERNEL_NAMES, out)}
 
@@ -507,13 +522,21 @@ class CPDriver:
         en["FICT_KE"] = c.energies()["FICT_KE"]
         if damp_velocity:
             self.v.zero_()
-        # orthonormalise: S = 2 sum w psi psi (kx0 weight 1/2), T = (S/2)^-1/2, psi = psi_t T
-        c.pc_forward(self.psi_t, self.psi_t, 2.0, 0.5, self.S)
+        # orthonormalise: S = 2 sum w psi psi (kx0 weight 1/2), T = (S/2)^-1/2, psi = psi_t T;
+        # the mixed form takes S and psi_t T on the int8 tensor cores (FP64 accuracy)
+        i8 = self.mixed and c.has_i8()
+        if i8:
+            c.pc_overlap_i8(self.psi_t, 2.0, 0.5, self.S)
+        else:
+            c.pc_forward(self.psi_t, self.psi_t, 2.0, 0.5, self.S)
         it, err, ok, smax = c.ortho_invsqrt(self.S, self.T, self.tol, self.max_iter, with_smax=True)
         self.last_ortho = (it, err, ok)
         if not ok:
             raise RuntimeError(f"Newton-Schulz did not converge: {it} iterations, residual {err:g}")
-        c.pc_backward(self.T, self.psi_t, 1.0, 1.0, self.psi)
+        if i8:
+            c.pc_rotate_i8(self.T, self.psi_t, self.psi)
+        else:
+            c.pc_backward(self.T, self.psi_t, 1.0, 1.0, self.psi)
         if smax > self.norb_tol and not damp_velocity:
             # Ortho::maxCheck -> PsiV: restart the non-orthogonal set from psi
             self.psiv_reset()
