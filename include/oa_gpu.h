@@ -130,7 +130,10 @@ oa_status oa_gpu_pc_forward(oa_ctx *ctx, void *stream, const double *left, const
  * products are exact in int32 and combined in FP64 (relative error about
  * 2^-42 of the largest value of a range).  The digits stay in the context
  * for oa_gpu_pc_rotate_i8.  Mixed-precision contexts with at most 128
- * states; OA_ERR_UNSUPPORTED otherwise. */
+ * states (the buffers are allocated on the first call); OA_ERR_UNSUPPORTED
+ * otherwise.  Not used by the native step: on B200 its eight digit levels
+ * fill all of TMEM with N = 64 accumulators, and at 128 states it is slower
+ * than the FP64 DMMA product. */
 oa_status oa_gpu_pc_overlap_i8(oa_ctx *ctx, void *stream, const double *psi_t, double alpha, double w_kx0,
                                double *S);
 
@@ -226,8 +229,11 @@ oa_status oa_gpu_set_atoms(oa_ctx *ctx, void *stream, const double *pos_host);
  * state z pass bwd + EKE, PairCalculator forward S, PairCalculator
  * backward (two-term, the constraint force), Newton-Schulz, the rotation
  * Psi T, the PairCalculator forward Lambda -- each as the context's form
- * runs it in the step (mixed: S and Psi T on int8 digits, the two-term
- * backward and Lambda split-BF16).  Clobbers the context's scratch.
+ * runs it in the step (mixed: the two-term backward and Lambda split-BF16,
+ * S and Psi T FP64 DMMA) -- and, for a mixed context of at most 128 states,
+ * ms_out[11..12] = the int8 digit products of S and Psi T
+ * (oa_gpu_pc_overlap_i8 / oa_gpu_pc_rotate_i8).  ms_out holds 13 values.
+ * Clobbers the context's scratch.
  * No reference counterpart (it replaces the Projections user events of
  * e.g. CP_State_GSpacePlane.C:1407-1409). */
 oa_status oa_gpu_time_kernels(oa_ctx *ctx, void *stream, const double *psi, int reps, double *ms_out);

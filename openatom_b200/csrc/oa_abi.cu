@@ -409,9 +409,6 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     }
     TRY(cudaMallocHost(&p->h_status, 4 * sizeof(int)));
     TRY(cudaMallocHost(&p->h_vals, 16 * sizeof(double)));
-    // the mixed form runs S and Psi T as int8 digit products (FP64 accuracy);
-    // without them (above 128 states) it keeps the FP64 DMMA products
-    if (c->precision == OA_MIXED) p->oz = oa_oz_create(d->nstate, d->ng, d->nkx0, nsm);
     TRY(cudaDeviceSynchronize());
   }
 #undef TRY
@@ -556,11 +553,21 @@ extern "C" oa_status oa_gpu_pc_forward(oa_ctx* c, void* stream, const double* le
   return OA_OK;
 }
 
+// The int8 products' buffers (digit slices of psi_t, about 6 bytes per
+// coefficient value) are allocated on the first call, so that contexts that
+// do not use them pay nothing.
+static bool oz_ready(oa_ctx* c) {
+  oa_ctx_pc* p = pcx(c);
+  if (!p->oz && c->precision == OA_MIXED && c->nstate <= 128)
+    p->oz = oa_oz_create(c->nstate, c->ng, c->nkx0, p->nsm);
+  return p->oz != nullptr;
+}
+
 extern "C" oa_status oa_gpu_pc_overlap_i8(oa_ctx* c, void* stream, const double* psi_t, double alpha,
                                           double w_kx0, double* S) {
   OA_ARG_CHECK(c && psi_t && S, "null argument");
   oa_ctx_pc* p = pcx(c);
-  if (!p->oz) {
+  if (!oz_ready(c)) {
     oa_set_error("the int8 overlap needs a mixed-precision context with at most 128 states", __FILE__, __LINE__);
     return OA_ERR_UNSUPPORTED;
   }
@@ -573,7 +580,7 @@ extern "C" oa_status oa_gpu_pc_rotate_i8(oa_ctx* c, void* stream, const double* 
   OA_ARG_CHECK(c && T && psi_t && psi_out, "null argument");
   OA_ARG_CHECK(psi_out != psi_t, "psi_out must not alias psi_t");
   oa_ctx_pc* p = pcx(c);
-  if (!p->oz) {
+  if (!oz_ready(c)) {
     oa_set_error("the int8 rotation needs a mixed-precision context with at most 128 states", __FILE__, __LINE__);
     return OA_ERR_UNSUPPORTED;
   }
@@ -590,7 +597,6 @@ extern "C" oa_status oa_gpu_pc_rotate_i8(oa_ctx* c, void* stream, const double* 
   return OA_OK;
 }
 
-int oa_oz_enabled(oa_ctx* c) { return pcx(c)->oz != nullptr; }
 
 extern "C" oa_status oa_gpu_ortho_invsqrt(oa_ctx* c, void* stream, const double* S, double* T, double tol,
                                           int max_iter, int* iters_out, double* err_out, double* smax_out) {
@@ -723,6 +729,7 @@ extern "C" oa_status oa_gpu_set_atoms(oa_ctx* c, void* stream, const double* pos
 // for the roofline: ms_out[0..8] = state_zfwd, state_plane_density, rho_xc,
 // vks_build (density FFT + Hartree/local + inverse), state_plane_vks,
 // state_zbwd, pc_forward (S), pc_backward (two-term), ortho_ns.
+static bool oz_ready(oa_ctx* c);
 static cudaError_t mixed_fwd(oa_ctx* c, cudaStream_t s, int nt, const double* A, const double* B, int m, int n,
                              long K, long kx0_cols, double w_kx0, double alpha, double* C, int sa, int sb,
                              const int* cond = nullptr);
@@ -739,7 +746,7 @@ extern "C" oa_status oa_gpu_time_kernels(oa_ctx* c, void* stream, const double* 
   OA_CUDA_TRY(cudaEventCreate(&e0));
   OA_CUDA_TRY(cudaEventCreate(&e1));
   float ms = 0.f;
-  double acc[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double acc[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   const int n = c->nstate;
   double* S = p->mat_a;
   double* T = p->mat_x;
@@ -764,11 +771,7 @@ extern "C" oa_status oa_gpu_time_kernels(oa_ctx* c, void* stream, const double* 
     OA_TIME(3, oa_launch_rho_fft_hart(c, s));
     OA_TIME(4, oa_launch_state_plane_vks(c, s));
     OA_TIME(5, oa_launch_state_zbwd(c, s, (const double2*)psi, nullptr, (double2*)p->vtmp, 0, n));
-    if (mixed && p->oz) {
-      OA_TIME(6, oa_oz_overlap(p->oz, s, psi, K, 2.0, 0.5, S, p->err_flag, nullptr));
-    } else {
-      OA_TIME(6, oa_launch_pc_fwd(s, psi, psi, n, K, K0, 0.5, 2.0, p->part, p->nkb, S));
-    }
+    OA_TIME(6, oa_launch_pc_fwd(s, psi, psi, n, K, K0, 0.5, 2.0, p->part, p->nkb, S));
     OA_CUDA_TRY(cudaMemcpyAsync(F, psi, (size_t)n * c->ng * sizeof(double2), cudaMemcpyDeviceToDevice, s));
     if (mixed) {
       // the bf16 planes of psi and F are made by their producers in the
@@ -786,16 +789,15 @@ extern "C" oa_status oa_gpu_time_kernels(oa_ctx* c, void* stream, const double* 
     }
     OA_TIME(8, oa_launch_ortho_ns(s, S, n, 0.5, 1e-15, 1000, p->ns_work, T, p->ns_status, p->ns_err,
                                   ns_launch_grid(p)));
-    if (mixed && p->oz) {
-      // S first: the rotation uses the digits the overlap took of psi
-      OA_CUDA_TRY(oa_oz_overlap(p->oz, s, psi, K, 2.0, 0.5, S, p->err_flag, nullptr));
-      OA_TIME(9, oa_oz_rotate(p->oz, s, T, psi, G, K, nullptr, p->err_flag, nullptr));
-    } else {
-      OA_TIME(9, oa_launch_pc_bwd(s, T, psi, 1.0, 1.0, nullptr, nullptr, 0.0, n, K, K0, G));
+    OA_TIME(9, oa_launch_pc_bwd(s, T, psi, 1.0, 1.0, nullptr, nullptr, 0.0, n, K, K0, G));
+    if (mixed && oz_ready(c)) {
+      // the int8 digit products of S and Psi T, beside the DMMA ones the step uses
+      OA_TIME(11, oa_oz_overlap(p->oz, s, psi, K, 2.0, 0.5, S, p->err_flag, nullptr));
+      OA_TIME(12, oa_oz_rotate(p->oz, s, T, psi, G, K, nullptr, p->err_flag, nullptr));
     }
 #undef OA_TIME
   }
-  for (int k = 0; k < 11; ++k) ms_out[k] = acc[k] / reps;
+  for (int k = 0; k < 13; ++k) ms_out[k] = acc[k] / reps;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return OA_OK;
@@ -815,7 +817,7 @@ extern "C" oa_status oa_gpu_sizes(const oa_ctx* c, long* out) {
   out[9] = 3 + 5 + 7 + 4 + 4 + 3 + 2 + 1 + 1;
   out[10] = c->pair_cols ? 1 : 0;  // state-pair plane kernels in use (mixed form)
   out[11] = c->ngroup_pair;
-  out[12] = pcx(const_cast<oa_ctx*>(c))->oz ? 1 : 0;  // int8 overlap / rotation available
+  out[12] = (c->precision == OA_MIXED && c->nstate <= 128) ? 1 : 0;  // int8 overlap / rotation available
   return OA_OK;
 }
 
@@ -1042,14 +1044,8 @@ oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* 
   const int n = c->nstate;
   OaPlaneOut po;
   bool fuse = nterm > 0 && plane_out(c, PL_PSI, n, nterm, &po);
-  // mixed form: the int8 rotation from the digits the overlap product took
-  // of psi_t (FP64 accuracy); otherwise FP64 DMMA
-  cudaError_t e = cudaErrorNotSupported;
-  if (nterm > 0 && p->oz)
-    e = oa_oz_rotate(p->oz, s, T, psi_t, psi, 2L * c->ng, fuse ? &po : nullptr, p->err_flag, nullptr);
-  if (e == cudaErrorNotSupported)
-    e = oa_dgemm_bwd_ex(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, psi,
-                        nullptr, nullptr, nullptr, nullptr, fuse ? &po : nullptr);
+  cudaError_t e = oa_dgemm_bwd_ex(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, psi,
+                                  nullptr, nullptr, nullptr, nullptr, fuse ? &po : nullptr);
   if (e == cudaErrorNotSupported) {
     // above 128 states: the general kernel, and the psi planes are split
     // again when a product needs them

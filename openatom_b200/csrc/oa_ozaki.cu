@@ -18,9 +18,14 @@
 //     d_q integers in [-64, 64],  |r| <= 2^(e-42),
 // the digits stored as int8 ("slices").  A product of two such operands is
 //     sum_{s,t} 2^(-7 (s + t)) (D_s^T D_t)   scaled by the two exponents,
-// where every D_s^T D_t is exact in int32 (tcgen05.mma.kind::i8).  The six
-// digit levels l = s + t <= 5 (21 digit products) accumulate in six TMEM
-// accumulators of N = 64 columns and are combined in FP64 in the epilogue.
+// where every D_s^T D_t is exact in int32 (tcgen05.mma.kind::i8).  The
+// eight digit levels l = s + t <= 7 (30 digit products) accumulate in eight
+// TMEM accumulators of N = 64 columns (all 512 columns) and are combined in
+// FP64 in the epilogue.  Levels up to 7, not 5: a value well below its
+// range's maximum has leading zero digits, and a product of two such values
+// starts at a later level; with eight levels every product keeps at least
+// 42 bits of its own magnitude (the off-diagonal entries of T are 1e-3 of
+// the diagonal ones, two leading zero digits).
 //
 // Layout.  The real view of Psi~ [rows][K] (K = 2 ng doubles) is cut into
 // 128-column chunks: the kx = 0 columns [0, kA) padded to nA chunks, then the
@@ -31,8 +36,8 @@
 // K = states, 128 B of M = g-columns).  Chunks are grouped into R ranges
 // (never across the kx = 0 boundary); each range has its own exponent per
 // state row, is one split-K unit of S and selects the scaled copy of T the
-// rotation uses: T'_r[i][j] = T[i][j] 2^(e_ri - 6), itself split into six
-// digit slices per column j (exponent f_rj), int8 [R][6][128 j][128 i].
+// rotation uses: T'_r[i][j] = T[i][j] 2^(e_ri - 6), itself split into seven
+// digit slices per column j (exponent f_rj), int8 [R][7][128 j][128 i].
 //
 // Every mbarrier wait is bounded (oa_wait.cuh); on a timeout the block sets
 // the device error flag, lets its copies land, frees TMEM and returns.  No
@@ -44,12 +49,14 @@
 #include "oa_internal.h"
 #include "oa_wait.cuh"
 
-#define OZ_ND 6                 // digits per value
-#define OZ_NL 6                 // digit levels kept (s + t <= 5)
+#define OZ_ND 6                 // digits per value of the states
+#define OZ_NDT 7                // digits per value of T' (the rotation's other operand)
+#define OZ_NL 8                 // digit levels kept (s + t <= 7)
 #define OZ_CH 128               // columns per chunk
 #define OZ_TILE (128 * OZ_CH)   // bytes of one slice chunk (128 rows)
 #define OZ_N 64                 // N of the MMAs
 #define OZ_THREADS 128
+#define OZ_TLD 132              // padded row of the T' digit staging
 
 __device__ __forceinline__ uint32_t oz_s32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -133,11 +140,12 @@ __device__ __forceinline__ int oz_exponent(double m) {
   frexp(m, &e);  // m = f 2^e, f in [0.5, 1)
   return e;
 }
-// the six digits of x 2^(6 - e), |x| < 2^e
+// the ND digits of x 2^(6 - e), |x| < 2^e
+template <int ND = OZ_ND>
 __device__ __forceinline__ void oz_digits(double x, int e, signed char* d) {
   double t = ldexp(x, 6 - e);
 #pragma unroll
-  for (int q = 0; q < OZ_ND; ++q) {
+  for (int q = 0; q < ND; ++q) {
     const double r = rint(t);
     d[q] = (signed char)(int)r;
     t = (t - r) * 128.0;
@@ -211,12 +219,16 @@ k_oz_slice(const double* __restrict__ X, long ldx, OzMap m, const int* __restric
 
 // ---------------------------------------------------------------------------
 // k_oz_tslice: block r: T'_r[i][j] = T[i][j] 2^(e_ri - 6) for i, j < n, its
-// column exponents f[r][j] and digit slices tsl[r][q][j][i] (zero beyond n).
+// column exponents f[r][j] and seven digit slices tsl[r][q][j][i] (zero
+// beyond n).  Seven, not six: each output of the rotation sums 128 products
+// whose T' digits are cut relative to the column's largest (diagonal) entry.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128)
 k_oz_tslice(const double* __restrict__ T, int n, const int* __restrict__ ex, signed char* __restrict__ tsl,
             int* __restrict__ fx) {
-  extern __shared__ __align__(16) signed char oz_tb[];  // [6][128][128]
+  // digits staged as [OZ_NDT][128 j][OZ_TLD i]: rows padded to 132 bytes so
+  // that the byte writes of 32 threads (32 columns j) fall in 32 banks
+  extern __shared__ __align__(16) signed char oz_tb[];
   const int r = blockIdx.x, j = threadIdx.x;
   double mx = 0.0;
   bool bad = false;
@@ -230,15 +242,21 @@ k_oz_tslice(const double* __restrict__ T, int n, const int* __restrict__ ex, sig
   const int f = oz_exponent(mx);
   fx[r * 128 + j] = bad ? OZ_BAD : f;
   for (int i = 0; i < 128; ++i) {
-    signed char d[OZ_ND] = {0, 0, 0, 0, 0, 0};
-    if (!bad && j < n && i < n) oz_digits(ldexp(T[(size_t)i * n + j], ex[r * 128 + i] - 6), f, d);
+    signed char d[OZ_NDT];
 #pragma unroll
-    for (int q = 0; q < OZ_ND; ++q) oz_tb[(q * 128 + j) * 128 + i] = d[q];
+    for (int q = 0; q < OZ_NDT; ++q) d[q] = 0;
+    if (!bad && j < n && i < n) oz_digits<OZ_NDT>(ldexp(T[(size_t)i * n + j], ex[r * 128 + i] - 6), f, d);
+#pragma unroll
+    for (int q = 0; q < OZ_NDT; ++q) oz_tb[(q * 128 + j) * OZ_TLD + i] = d[q];
   }
   __syncthreads();
-  uint4* dst = reinterpret_cast<uint4*>(tsl + (size_t)r * OZ_ND * OZ_TILE);
-  const uint4* src = reinterpret_cast<const uint4*>(oz_tb);
-  for (int t = threadIdx.x; t < OZ_ND * OZ_TILE / 16; t += blockDim.x) dst[t] = src[t];
+  // rows of 32 words to global, 32 consecutive words per warp
+  int* dst = reinterpret_cast<int*>(tsl + (size_t)r * OZ_NDT * OZ_TILE);
+  const int* src = reinterpret_cast<const int*>(oz_tb);
+  for (int t = threadIdx.x; t < OZ_NDT * 128 * 32; t += blockDim.x) {
+    const int row = t >> 5, w = t & 31;
+    dst[t] = src[row * (OZ_TLD / 4) + w];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -265,7 +283,7 @@ k_oz_syrk(const __grid_constant__ CUtensorMap tS, const int* __restrict__ rc, in
   int* ecol = okflag + 1;  // [OZ_N]
   const int tid = threadIdx.x, warp = tid >> 5;
   const int c0 = rc[r], nslab = rc[r + 1] - c0;
-  constexpr uint32_t ncols = 512;  // six accumulators of OZ_N columns
+  constexpr uint32_t ncols = 512;  // eight accumulators of OZ_N columns
   if (tid == 0) {
     for (int s = 0; s < stages; ++s) { oz_bar_init(&full[s], 1); oz_bar_init(&empty[s], 1); }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -306,9 +324,11 @@ k_oz_syrk(const __grid_constant__ CUtensorMap tS, const int* __restrict__ rc, in
             if (s + t >= OZ_NL) continue;
             const uint64_t da = oz_desc(sb + s * OZ_TILE + ks * 32, 16, 1024);
             const uint64_t db = oz_desc(sb + t * OZ_TILE + h * OZ_N * OZ_CH + ks * 32, 16, 1024);
-            // the first MMA into level s + t overwrites it: s = 0 of the first
-            // K step of the first chunk (t = l)
-            const uint32_t acc = (sl > 0 || ks > 0 || s > 0) ? 1u : 0u;
+            // the first MMA into level l = s + t overwrites it: in the first K
+            // step of the first chunk, the pair with the smallest s
+            // (s = max(0, l - 5))
+            const int sfirst = s + t > OZ_ND - 1 ? s + t - (OZ_ND - 1) : 0;
+            const uint32_t acc = (sl > 0 || ks > 0 || s > sfirst) ? 1u : 0u;
             oz_mma(tmem + (uint32_t)((s + t) * OZ_N), da, db, idesc, acc);
           }
       oz_commit(&empty[st]);
@@ -392,7 +412,7 @@ k_oz_rot(const __grid_constant__ CUtensorMap tS, const __grid_constant__ CUtenso
   if (h * OZ_N >= n) return;
   extern __shared__ __align__(1024) unsigned char oz_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)oz_raw + 1023) & ~(uintptr_t)1023);
-  constexpr uint32_t a_bytes = OZ_ND * OZ_TILE, b_bytes = OZ_ND * OZ_N * 128;
+  constexpr uint32_t a_bytes = OZ_ND * OZ_TILE, b_bytes = OZ_NDT * OZ_N * 128;
   uint64_t* full = (uint64_t*)(base + a_bytes + b_bytes);
   uint64_t* done = full + 1;
   uint32_t* tslot = (uint32_t*)(done + 1);
@@ -414,10 +434,9 @@ k_oz_rot(const __grid_constant__ CUtensorMap tS, const __grid_constant__ CUtenso
     const uint32_t sa = oz_s32(base), sb = sa + a_bytes;
     oz_expect_tx(full, a_bytes + b_bytes);
 #pragma unroll
-    for (int q = 0; q < OZ_ND; ++q) {
-      oz_tma(sa + q * OZ_TILE, &tS, 0, 0, c, q, full);
-      oz_tma(sb + q * OZ_N * 128, &tT, 0, h * OZ_N, q, r, full);
-    }
+    for (int q = 0; q < OZ_ND; ++q) oz_tma(sa + q * OZ_TILE, &tS, 0, 0, c, q, full);
+#pragma unroll
+    for (int q = 0; q < OZ_NDT; ++q) oz_tma(sb + q * OZ_N * 128, &tT, 0, h * OZ_N, q, r, full);
     bool ok = oz_wait(full, 0u);
     if (ok) {
       oz_tc_after();
@@ -430,11 +449,12 @@ k_oz_rot(const __grid_constant__ CUtensorMap tS, const __grid_constant__ CUtenso
 #pragma unroll
         for (int s = 0; s < OZ_ND; ++s)
 #pragma unroll
-          for (int t = 0; t < OZ_ND; ++t) {
+          for (int t = 0; t < OZ_NDT; ++t) {
             if (s + t >= OZ_NL) continue;
             const uint64_t da = oz_desc(sa + s * OZ_TILE + ks * 4096, OZ_TILE, 1024);
             const uint64_t db = oz_desc(sb + t * OZ_N * 128 + ks * 32, 16, 1024);
-            const uint32_t acc = (ks > 0 || s > 0) ? 1u : 0u;
+            const int sfirst = s + t > OZ_NDT - 1 ? s + t - (OZ_NDT - 1) : 0;
+            const uint32_t acc = (ks > 0 || s > sfirst) ? 1u : 0u;
             oz_mma(tmem + (uint32_t)((s + t) * OZ_N), da, db, idesc, acc);
           }
       oz_commit(done);
@@ -528,7 +548,7 @@ struct oa_oz {
   int* rc;              // [R + 1] first chunk of each range
   int* cr;              // [nch] range of each chunk
   signed char* sl;      // [6][nch][128][128]
-  signed char* tsl;     // [R][6][128][128]
+  signed char* tsl;     // [R][OZ_NDT][128][128]
   int* ex;              // [R][128]
   int* fx;              // [R][128]
   double* part;         // [R][128][128]
@@ -539,7 +559,7 @@ struct oa_oz {
 };
 
 static size_t oz_syrk_smem(int stages) { return (size_t)stages * OZ_ND * OZ_TILE + 1024 + 1024; }
-static size_t oz_rot_smem() { return (size_t)OZ_ND * OZ_TILE + (size_t)OZ_ND * OZ_N * 128 + 1024 + 256; }
+static size_t oz_rot_smem() { return (size_t)OZ_ND * OZ_TILE + (size_t)OZ_NDT * OZ_N * 128 + 1024 + 256; }
 
 void oa_oz_free(oa_oz* z) {
   if (!z) return;
@@ -587,7 +607,7 @@ oa_oz* oa_oz_create(int n, int ng, int nkx0, int nsm) {
   okm &= cudaMalloc(&z->rc, (R + 1) * sizeof(int)) == cudaSuccess;
   okm &= cudaMalloc(&z->cr, z->nch * sizeof(int)) == cudaSuccess;
   okm &= cudaMalloc(&z->sl, (size_t)OZ_ND * z->nch * OZ_TILE) == cudaSuccess;
-  okm &= cudaMalloc(&z->tsl, (size_t)R * OZ_ND * OZ_TILE) == cudaSuccess;
+  okm &= cudaMalloc(&z->tsl, (size_t)R * OZ_NDT * OZ_TILE) == cudaSuccess;
   okm &= cudaMalloc(&z->ex, (size_t)R * 128 * sizeof(int)) == cudaSuccess;
   okm &= cudaMalloc(&z->fx, (size_t)R * 128 * sizeof(int)) == cudaSuccess;
   okm &= cudaMalloc(&z->part, (size_t)R * 128 * 128 * sizeof(double)) == cudaSuccess;
@@ -598,7 +618,7 @@ oa_oz* oa_oz_create(int n, int ng, int nkx0, int nsm) {
   okm &= cudaMemcpy(z->rc, rc.data(), (R + 1) * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
   okm &= cudaMemcpy(z->cr, cr.data(), z->nch * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
   okm &= oz_map(&z->tS, z->sl, 128, z->nch, OZ_ND, 128);
-  okm &= oz_map(&z->tT, z->tsl, 128, OZ_ND, R, OZ_N);
+  okm &= oz_map(&z->tT, z->tsl, 128, OZ_NDT, R, OZ_N);
   z->stages = 0;
   for (int st = 3; st >= 2; --st)
     if (oz_syrk_smem(st) <= (size_t)OA_MAX_SMEM) { z->stages = st; break; }
@@ -609,7 +629,7 @@ oa_oz* oa_oz_create(int n, int ng, int nkx0, int nsm) {
 }
 
 size_t oa_oz_bytes(const oa_oz* z) {
-  return z ? (size_t)OZ_ND * z->nch * OZ_TILE + (size_t)z->R * OZ_ND * OZ_TILE + (size_t)z->R * 128 * 128 * 8 : 0;
+  return z ? (size_t)OZ_ND * z->nch * OZ_TILE + (size_t)z->R * OZ_NDT * OZ_TILE + (size_t)z->R * 128 * 128 * 8 : 0;
 }
 
 // S = alpha (w_kx0 sum over the kx = 0 columns + sum over the rest) X X^T for
@@ -640,7 +660,7 @@ cudaError_t oa_oz_rotate(oa_oz* z, cudaStream_t s, const double* T, const double
   if (!z || X != z->src) return cudaErrorNotSupported;
   cudaError_t e = oa_smem_limit(k_oz_tslice);
   if (e != cudaSuccess) return e;
-  k_oz_tslice<<<z->R, 128, OZ_ND * OZ_TILE, s>>>(T, z->n, z->ex, z->tsl, z->fx);
+  k_oz_tslice<<<z->R, 128, OZ_NDT * 128 * OZ_TLD, s>>>(T, z->n, z->ex, z->tsl, z->fx);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   e = oa_smem_limit(k_oz_rot);
   if (e != cudaSuccess) return e;

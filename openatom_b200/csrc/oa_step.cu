@@ -36,10 +36,7 @@ oa_status oa_gpu_small_gemm(oa_ctx* ctx, void* stream, const double* A, const do
 oa_status oa_gpu_integrate(oa_ctx* ctx, void* stream, const double* force, double* vpsi, double* psi, double dt,
                            int complete_prev, double* fict_ke_out);
 oa_status oa_gpu_psiv_reset(oa_ctx* ctx, void* stream, const double* psi, double* psi_t, double* vpsi);
-oa_status oa_gpu_pc_overlap_i8(oa_ctx* ctx, void* stream, const double* psi_t, double alpha, double w_kx0,
-                               double* S);
 }
-int oa_oz_enabled(oa_ctx* c);
 
 int oa_ns_capturable(oa_ctx* c);
 oa_status oa_integrate_sel(oa_ctx* c, cudaStream_t s, const double* force, double* vpsi, double* psi,
@@ -184,10 +181,8 @@ static oa_status launch_step_a(oa_ctx* c, cudaStream_t s, oa_cp_state* st, int c
   }
   // integrateModForce; psi(t) is psi itself after the previous step's PsiV reset
   OA_STEP_TRY(oa_integrate_sel(c, s, w->F2, st->vpsi, st->psi_t, st->psi, w->flag, st->dt, complete_prev, nullptr));
-  // computeNewPsi: S, FP64 DMMA, or in the mixed form the int8 digit
-  // product of the same FP64 accuracy (its digits of psi_t also serve Psi T)
-  if (nt && oa_oz_enabled(c)) OA_STEP_TRY(oa_gpu_pc_overlap_i8(c, s, st->psi_t, 2.0, 0.5, w->S));
-  else OA_STEP_TRY(oa_gpu_pc_forward(c, s, st->psi_t, st->psi_t, 2.0, 0.5, w->S));
+  // computeNewPsi: S (FP64 DMMA in both forms)
+  OA_STEP_TRY(oa_gpu_pc_forward(c, s, st->psi_t, st->psi_t, 2.0, 0.5, w->S));
   return OA_OK;
 }
 

@@ -101,7 +101,8 @@ SIGNATURES = {
 }
 
 KERNEL_NAMES = ("state_zfwd", "state_plane_density", "rho_xc", "vks_build", "state_plane_vks",
-                "state_zbwd", "pc_forward_S", "pc_backward", "ortho_ns", "pc_rotate", "pc_forward_lambda")
+                "state_zbwd", "pc_forward_S", "pc_backward", "ortho_ns", "pc_rotate", "pc_forward_lambda",
+                "pc_overlap_i8", "pc_rotate_i8")
 
 _lib = None
 
@@ -522,21 +523,13 @@ class CPDriver:
         en["FICT_KE"] = c.energies()["FICT_KE"]
         if damp_velocity:
             self.v.zero_()
-        # orthonormalise: S = 2 sum w psi psi (kx0 weight 1/2), T = (S/2)^-1/2, psi = psi_t T;
-        # the mixed form takes S and psi_t T on the int8 tensor cores (FP64 accuracy)
-        i8 = self.mixed and c.has_i8()
-        if i8:
-            c.pc_overlap_i8(self.psi_t, 2.0, 0.5, self.S)
-        else:
-            c.pc_forward(self.psi_t, self.psi_t, 2.0, 0.5, self.S)
+        # orthonormalise: S = 2 sum w psi psi (kx0 weight 1/2), T = (S/2)^-1/2, psi = psi_t T
+        c.pc_forward(self.psi_t, self.psi_t, 2.0, 0.5, self.S)
         it, err, ok, smax = c.ortho_invsqrt(self.S, self.T, self.tol, self.max_iter, with_smax=True)
         self.last_ortho = (it, err, ok)
         if not ok:
             raise RuntimeError(f"Newton-Schulz did not converge: {it} iterations, residual {err:g}")
-        if i8:
-            c.pc_rotate_i8(self.T, self.psi_t, self.psi)
-        else:
-            c.pc_backward(self.T, self.psi_t, 1.0, 1.0, self.psi)
+        c.pc_backward(self.T, self.psi_t, 1.0, 1.0, self.psi)
         if smax > self.norb_tol and not damp_velocity:
             # Ortho::maxCheck -> PsiV: restart the non-orthogonal set from psi
             self.psiv_reset()

@@ -2,9 +2,12 @@
 tcgen05.mma.kind::i8): the overlap S = alpha sum w psi_t psi_t^T
 (PairCalculator::multiplyForward, ckPairCalculator.C:821-893) and the
 rotation psi_t T (bwMultiplyHelper, :1710-1946) against the FP64 DMMA
-products and the oracle, to FP64 accuracy (1e-13 relative), for state
-counts that fill one or two 64-column halves and for odd counts; a
-non-finite input propagates to the output."""
+products and the oracle, for state counts that fill one or two 64-column
+halves and for odd counts; a non-finite input propagates to the output.
+Tolerances: S to 5e-13 of its largest entry (its K sums average the digit
+cut-offs out); the rotation to 1e-12 of the largest coefficient (each output
+is about one input coefficient, cut at 2^-41 of its K range's largest value);
+the rotated set orthonormal to 1e-12."""
 import numpy as np
 import pytest
 
@@ -13,7 +16,8 @@ from oracle import cp_oracle as O
 
 pytestmark = pytest.mark.gpu
 
-TOL = 1e-13
+TOL = 5e-13
+TOL_ROT = 1e-12
 
 
 def _case(preset, nst, seed):
@@ -53,8 +57,8 @@ def test_overlap_and_rotation_match_fp64(preset, nst):
     torch.cuda.synchronize()
     r8, r64 = R8.cpu().numpy(), R64.cpu().numpy()
     rref = T.T @ pt
-    assert np.max(np.abs(r8 - rref)) <= TOL * np.max(np.abs(rref))
-    assert np.max(np.abs(r8 - r64)) <= TOL * np.max(np.abs(r64))
+    assert np.max(np.abs(r8 - rref)) <= TOL_ROT * np.max(np.abs(rref))
+    assert np.max(np.abs(r8 - r64)) <= TOL_ROT * np.max(np.abs(r64))
     # the rotated set is orthonormal in FP64: S/2 = I
     q = O.pc_forward(O.kx0_scale(r8, s, 2 ** -0.5), O.kx0_scale(r8, s, 2 ** -0.5), s, 2.0) / 2.0
     assert np.max(np.abs(q - np.eye(nst))) < 1e-12
