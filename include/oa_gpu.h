@@ -144,6 +144,20 @@ oa_status oa_gpu_pc_overlap_i8(oa_ctx *ctx, void *stream, const double *psi_t, d
  * array).  T: device [nstate][nstate]; psi_out must not alias psi_t. */
 oa_status oa_gpu_pc_rotate_i8(oa_ctx *ctx, void *stream, const double *T, const double *psi_t, double *psi_out);
 
+/* Minimisation (cp_min_opt on; GSpaceDriver::computeMinimization,
+ * gspace.ci:85-196).  oa_gpu_min_fovlap: *fovlap_out = sum over every
+ * stored point of |force|^2 (CPINTEGRATE::CP_fovlap_calc, cp_min_CG.C:128;
+ * its square root is the force magnitude tested against tol_cp_min,
+ * CP_State_GSpacePlane.C:110-190); synchronises.  oa_gpu_min_step: one
+ * steepest-descent step psi += force dt / m (CP_integrate_min_STD,
+ * cp_min_std.C:17-60) when conj_grad is NULL, else one conjugate-gradient
+ * step conj = gamma conj + force on g^2 <= ecut, psi += conj dt / m
+ * (CP_integrate_min_CG, cp_min_CG.C:29-120), then the Gamma redundancy
+ * sync of psi.  force: the constraint-projected force, device [nstate][ng]. */
+oa_status oa_gpu_min_fovlap(oa_ctx *ctx, void *stream, const double *force, double *fovlap_out);
+oa_status oa_gpu_min_step(oa_ctx *ctx, void *stream, const double *force, double *conj_grad, double *psi,
+                          double gamma, double dt);
+
 /* Ortho S -> T = (S/2)^(-1/2) by Newton-Schulz (ortho.C:109-146, 153-266,
  * 848-971; same iteration as CPORTHOG::get_iter_Tmat, cp_lowdin.C:180-265).
  * S, T: device [n][n].  Synchronises the stream to return iterations,

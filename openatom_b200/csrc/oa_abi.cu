@@ -366,7 +366,8 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     TRY(cudaMalloc(&c->red, c->red_len * sizeof(double)));
     TRY(cudaMalloc(&c->eke_part, (size_t)d->nstate * c->nblk_z * sizeof(double)));
     p->nkb = 160;  // split-K partials: about one CTA per SM for a 128 x 128 product
-    TRY(cudaMalloc(&p->part, (size_t)p->nkb * d->nstate * d->nstate * sizeof(double)));
+    // split-K partials; also the block partials of the minimisation's |F|^2 (>= 1024)
+    TRY(cudaMalloc(&p->part, std::max((size_t)p->nkb * d->nstate * d->nstate, (size_t)1024) * sizeof(double)));
     p->ns_grid = oa_ns_grid(d->nstate, c->device);
     p->ns_cluster = oa_ns_cluster_size(d->nstate);
     TRY(cudaMalloc(&p->ns_work, ((size_t)5 * d->nstate * d->nstate + p->ns_grid + 32) * sizeof(double)));
@@ -597,6 +598,37 @@ extern "C" oa_status oa_gpu_pc_rotate_i8(oa_ctx* c, void* stream, const double* 
   return OA_OK;
 }
 
+
+cudaError_t oa_launch_min_fovlap(cudaStream_t s, const double2* F, size_t n, double* part);
+int oa_min_nblk();
+cudaError_t oa_launch_min_step(cudaStream_t s, const double2* F, double2* conj, double2* P, const double* cmass,
+                               const double* g2, double ecut, int ng, int nstate, double gamma, double dt);
+
+extern "C" oa_status oa_gpu_min_fovlap(oa_ctx* c, void* stream, const double* force, double* fovlap_out) {
+  OA_ARG_CHECK(c && force && fovlap_out, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  oa_ctx_pc* p = pcx(c);
+  const int nb = oa_min_nblk();
+  // block partials in the split-K partial buffer (at least nb doubles), summed in a fixed order
+  OA_CUDA_TRY(oa_launch_min_fovlap(s, (const double2*)force, (size_t)c->nstate * c->ng, p->part));
+  OA_CUDA_TRY(oa_launch_sum_partials(s, p->part, nb, 1, 0, 1.0, p->dev_e + 15));
+  OA_CUDA_TRY(cudaMemcpyAsync(p->h_vals + 15, p->dev_e + 15, sizeof(double), cudaMemcpyDeviceToHost, s));
+  OA_CUDA_TRY(cudaStreamSynchronize(s));
+  *fovlap_out = p->h_vals[15];
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_min_step(oa_ctx* c, void* stream, const double* force, double* conj_grad, double* psi,
+                                     double gamma, double dt) {
+  OA_ARG_CHECK(c && force && psi, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  oa_ctx_pc* p = pcx(c);
+  OA_CUDA_TRY(oa_launch_min_step(s, (const double2*)force, (double2*)conj_grad, (double2*)psi, p->cmass, c->g2,
+                                 c->ecut_psi, c->ng, c->nstate, gamma, dt));
+  // Gamma redundancy sync of psi (computeRedPsi, gspace.ci:692-708)
+  OA_CUDA_TRY(oa_launch_sync_redundant(s, (double2*)psi, nullptr, p->partner, c->nkx0_red, c->ng, c->nstate));
+  return OA_OK;
+}
 
 extern "C" oa_status oa_gpu_ortho_invsqrt(oa_ctx* c, void* stream, const double* S, double* T, double tol,
                                           int max_iter, int* iters_out, double* err_out, double* smax_out) {

@@ -419,6 +419,67 @@ k_integrate(const double2* __restrict__ F, double2* __restrict__ V, double2* P, 
 
 int oa_integrate_nblk(int ng, int nstate) { return nstate * ((ng + OA_INT_CHUNK - 1) / OA_INT_CHUNK); }
 
+// ---------------------------------------------------------------------------
+// Minimisation (cp_min_opt): CPINTEGRATE::CP_fovlap_calc (cp_min_CG.C:128-140)
+// -> k_min_fovlap, sum |F|^2 over every stored point; CP_integrate_min_STD
+// (cp_min_std.C:17-60, psi += F dt / m) and CP_integrate_min_CG
+// (cp_min_CG.C:29-120, conj = conj gamma + F on g^2 <= ecut, psi += conj
+// dt / m) -> k_min_step.  Block partial sums in a fixed order.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_min_fovlap(const double2* __restrict__ F, size_t n,
+                                                    double* __restrict__ part) {
+  __shared__ double sh[8];
+  double a = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 f = F[i];
+    a += f.x * f.x + f.y * f.y;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += sh[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_min_step(const double2* __restrict__ F, double2* __restrict__ conj, double2* __restrict__ P,
+                           const double* __restrict__ cmass, const double* __restrict__ g2, double ecut, int ng,
+                           size_t n, double gamma, double dt) {
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % (size_t)ng);
+    double2 d = F[t];
+    if (conj) {
+      double2 c = conj[t];
+      if (g2[i] <= ecut) { c.x = c.x * gamma + d.x; c.y = c.y * gamma + d.y; }
+      conj[t] = c;
+      d = c;
+    }
+    const double s = dt / cmass[i];
+    double2 p = P[t];
+    p.x += d.x * s;
+    p.y += d.y * s;
+    P[t] = p;
+  }
+}
+
+#define OA_MIN_NBLK 592
+
+cudaError_t oa_launch_min_fovlap(cudaStream_t s, const double2* F, size_t n, double* part) {
+  k_min_fovlap<<<OA_MIN_NBLK, 256, 0, s>>>(F, n, part);
+  return cudaGetLastError();
+}
+int oa_min_nblk() { return OA_MIN_NBLK; }
+
+cudaError_t oa_launch_min_step(cudaStream_t s, const double2* F, double2* conj, double2* P, const double* cmass,
+                               const double* g2, double ecut, int ng, int nstate, double gamma, double dt) {
+  const size_t n = (size_t)nstate * ng;
+  k_min_step<<<OA_MIN_NBLK, 256, 0, s>>>(F, conj, P, cmass, g2, ecut, ng, n, gamma, dt);
+  return cudaGetLastError();
+}
+
 __global__ void k_sync_redundant(double2* __restrict__ P, double2* __restrict__ V, const int* __restrict__ partner,
                                  int nred, int ng, int nstate) {
   const size_t total = (size_t)nstate * nred;

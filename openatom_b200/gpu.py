@@ -73,6 +73,8 @@ SIGNATURES = {
     "oa_gpu_vks_apply_fft_bwd": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp, _vp]),
     "oa_gpu_pc_forward": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_double, _vp]),
     "oa_gpu_pc_overlap_i8": (C.c_int, [_vp, _vp, _vp, C.c_double, C.c_double, _vp]),
+    "oa_gpu_min_fovlap": (C.c_int, [_vp, _vp, _vp, _dp]),
+    "oa_gpu_min_step": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_double, C.c_double]),
     "oa_gpu_pc_rotate_i8": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "oa_gpu_ortho_invsqrt": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_int, _ip, _dp, _dp]),
     "oa_gpu_pc_backward": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, C.c_double, _vp, _vp, C.c_double, _vp]),
@@ -257,6 +259,17 @@ class CPContext:
     def pc_rotate_i8(self, T, psi_t, out):
         """out = psi_t T from the digits of the last pc_overlap_i8 (FP64 accuracy)."""
         _check(self._lib.oa_gpu_pc_rotate_i8(self._h, self._stream(), _ptr(T), _ptr(psi_t), _ptr(out)))
+
+    def min_fovlap(self, force) -> float:
+        """sum |force|^2 over every stored point (CP_fovlap_calc)."""
+        out = C.c_double(0.0)
+        _check(self._lib.oa_gpu_min_fovlap(self._h, self._stream(), _ptr(force), C.byref(out)))
+        return out.value
+
+    def min_step(self, force, psi, dt, conj=None, gamma=0.0):
+        """One steepest-descent (conj None) or conjugate-gradient step on psi."""
+        _check(self._lib.oa_gpu_min_step(self._h, self._stream(), _ptr(force), _ptr(conj), _ptr(psi),
+                                         float(gamma), float(dt)))
 
     def has_i8(self) -> bool:
         """True when the int8 overlap / rotation are available (mixed form, <= 128 states)."""
@@ -538,6 +551,77 @@ class CPDriver:
         en["ORTHO_ERR"] = err
         en["SMAX"] = smax
         return en
+
+
+class CPMinimizer:
+    """Electronic minimisation at fixed ions (cp_min_opt): the loop of
+    GSpaceDriver::computeMinimization (gspace.ci:85-196).  Every iteration:
+    forces on the orthonormal psi (KS, nonlocal, EKE), the Lagrange
+    multipliers Lambda = <psi|F> and F' = F - Psi Lambda (Ortho hands Lambda
+    back unchanged in minimisation, ortho.C:497-608), |F'|^2
+    (CP_fovlap_calc), the steepest-descent or conjugate-gradient step
+    (CP_integrate_min_STD / CP_integrate_min_CG) with the reference's
+    conjugate-gradient resets (CP_State_GSpacePlane.C:2636-2660), and the
+    orthonormalisation S, Newton-Schulz, psi = psi T (computeNewPsi).  Stops
+    when |F'| = sqrt(sum |F'|^2) <= tol (tol_cp_min)."""
+
+    def __init__(self, driver: "CPDriver", method: str = "cg", dt: float | None = None):
+        if method not in ("cg", "sd"):
+            raise ValueError("method must be 'cg' or 'sd'")
+        self.d = driver
+        self.method = method
+        self.dt = driver.sys.dt if dt is None else dt
+        self.conj = driver.torch.zeros_like(driver.psi) if method == "cg" else None
+        self.iteration = 0
+        self.fovlap = 0.0
+        self.fmag = 0.0
+        self.num_reset = 0
+
+    def step(self) -> dict:
+        d, c = self.d, self.d.ctx
+        self.iteration += 1
+        d.forces()
+        en = c.energies()
+        if d.mixed:
+            c.pc_forward_mixed(d.psi, d.F, 1.0, 1.0, d.lam)
+        else:
+            c.pc_forward(d.psi, d.F, 1.0, 1.0, d.lam)
+        eye = d.torch.eye(d.sys.nstate, dtype=d.torch.float64, device=d.psi.device)
+        c.pc_backward(d.lam, d.psi, -0.5, -1.0, d.F2, M2=eye, X2=d.F, a2=1.0)
+        fov_old, fmag_old = self.fovlap, self.fmag
+        self.fovlap = c.min_fovlap(d.F2)
+        self.fmag = math.sqrt(self.fovlap)
+        gamma = 0.0
+        if self.method == "cg":
+            reset = self.iteration == 1
+            if self.iteration > 1 and ((self.fmag > 1.05 * fmag_old and self.num_reset >= 5)
+                                       or self.fmag > 2.0 * fmag_old):
+                reset = True
+            if reset:
+                self.num_reset = 0
+            else:
+                gamma = self.fovlap / fov_old
+            self.num_reset += 1
+        c.min_step(d.F2, d.psi, self.dt, conj=self.conj, gamma=gamma)
+        # computeNewPsi: S, T = (S/2)^-1/2, psi = psi_t T
+        d.psi_t.copy_(d.psi)
+        c.pc_forward(d.psi_t, d.psi_t, 2.0, 0.5, d.S)
+        it, err, ok = c.ortho_invsqrt(d.S, d.T, d.tol, d.max_iter)
+        if not ok:
+            raise RuntimeError(f"Newton-Schulz did not converge: {it} iterations, residual {err:g}")
+        c.pc_backward(d.T, d.psi_t, 1.0, 1.0, d.psi)
+        d.psi_t.copy_(d.psi)
+        en["FMAG"] = self.fmag
+        en["ORTHO_ITERS"] = it
+        return en
+
+    def run(self, max_iter: int, tol: float = 0.0) -> list:
+        out = []
+        for _ in range(max_iter):
+            out.append(self.step())
+            if self.fmag <= tol:
+                break
+        return out
 
 
 def run_batch(drivers, states, nsteps: int, stream=None) -> list:

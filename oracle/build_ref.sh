@@ -11,7 +11,7 @@ OUT="$HERE/_ref"
 if [ ! -d "$PINY" ]; then echo "reference tree not found at $REF; skipping oracle/_ref" >&2; exit 0; fi
 mkdir -p "$OUT"
 CXX="${CXX:-g++}"
-FLAGS="-O2 -fPIC -std=c++14 -DCHARM_ON -DFORTRANUNDERSCORE -w -include $HERE/ref_stubs/charm++.h -I$HERE/ref_stubs -I$PINY/include/pentium -I$PINY/include -I$REF/src_mathlib"
+FLAGS="-O2 -fPIC -std=c++14 -DCHARM_ON -DFORTRANUNDERSCORE -w -include $HERE/ref_stubs/charm++.h -I$HERE/ref_stubs -I$PINY/include/pentium -I$PINY/include -I$REF/src_mathlib -I$REF/include"
 SRCS=(
   "$PINY/abinito_physics/cp_nonlocal/cp_eke.C"
   "$PINY/abinito_physics/cp_xc_fnctl/cp_pz_lda.C"
@@ -22,6 +22,8 @@ SRCS=(
   "$PINY/abinito_physics/cp_nonlocal/cp_nl_energy_forc.C"
   "$PINY/abinito_physics/cp_integrate/cp_dynamics.C"
   "$PINY/abinito_physics/cp_integrate/cp_isokin.C"
+  "$PINY/abinito_physics/cp_integrate/cp_min_std.C"
+  "$PINY/abinito_physics/cp_integrate/cp_min_CG.C"
 )
 OBJS=()
 for s in "${SRCS[@]}"; do

@@ -775,3 +775,67 @@ def quench(st, sysm, nsteps, tol=1e-15, max_iter=1000, dt=None):
         out.append(en)
     st.iteration = 0
     return out
+
+
+# ----------------------------------------------------------------------------
+# minimisation (cp_min_opt), fixed ions
+# ----------------------------------------------------------------------------
+
+def fovlap(force):
+    """``CPINTEGRATE::CP_fovlap_calc`` (``cp_integrate/cp_min_CG.C:128-140``):
+    sum |F|^2 over every stored point of every state."""
+    return float(np.sum(force.real ** 2 + force.imag ** 2))
+
+
+def min_step(psi, force, sysm, dt, conj=None, gamma=0.0):
+    """``CP_integrate_min_STD`` (``cp_min_std.C:17-60``): psi += F dt / m, or
+    ``CP_integrate_min_CG`` (``cp_min_CG.C:29-120``): conj = conj gamma + F
+    for g^2 <= ecut, psi += conj dt / m.  Returns (psi, conj)."""
+    if conj is not None:
+        inside = (sysm.g2() <= sysm.ecut_ry)[None, :]
+        conj = np.where(inside, conj * gamma + force, conj)
+        d = conj
+    else:
+        d = force
+    return psi + d * (dt / sysm.cmass[None, :]), conj
+
+
+def minimize(st, sysm, nsteps, method="cg", dt=None, tol=1e-15, max_iter=1000, nl="auto"):
+    """Electronic minimisation at fixed ions, the loop of
+    ``GSpaceDriver::computeMinimization`` (``gspace.ci:85-196``): forces on
+    the orthonormal psi, F' = F - Psi Lambda (Lambda handed back unchanged by
+    Ortho in minimisation, ``ortho.C:497-608``), |F'|^2, the steepest-descent
+    or conjugate-gradient step with the resets of
+    ``CP_State_GSpacePlane.C:2636-2660``, the Gamma redundancy sync and the
+    orthonormalisation.  Returns one record per iteration (energies of the
+    psi the forces were evaluated on, FMAG = |F'|)."""
+    dt = sysm.dt if dt is None else dt
+    if nl == "auto":
+        nl = _nl_default if len(sysm.nl_atoms()) else None
+    conj = np.zeros_like(st.psi) if method == "cg" else None
+    out = []
+    fov = fmag = 0.0
+    nreset = 0
+    for it in range(1, nsteps + 1):
+        fnl, enl = (None, 0.0) if nl is None else nl(st.psi, sysm)
+        f, en = electronic_forces(st.psi, sysm, fnl, enl)
+        f, _ = lambda_step(st.psi, f, np.eye(sysm.nstate), sysm)
+        fov_old, fmag_old = fov, fmag
+        fov = fovlap(f)
+        fmag = math.sqrt(fov)
+        gamma = 0.0
+        if method == "cg":
+            reset = it == 1 or (fmag > 1.05 * fmag_old and nreset >= 5) or fmag > 2.0 * fmag_old
+            if reset:
+                nreset = 0
+            else:
+                gamma = fov / fov_old
+            nreset += 1
+        p, conj = min_step(st.psi, f, sysm, dt, conj, gamma)
+        p = sync_redundant(p, sysm)
+        st.psi, st.T, S, its, err = ortho_psi(p, sysm, tol, max_iter)
+        st.psi_t = st.psi.copy()
+        en["FMAG"] = fmag
+        en["ORTHO_ITERS"] = its
+        out.append(en)
+    return out

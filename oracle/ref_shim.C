@@ -320,3 +320,25 @@ extern "C" void ref_integrate_dyn(int ncoef, int iteration, double dt, double* f
                                 nullptr, nullptr, 1.0, fict_ke, nkx0_red, nkx0_uni, nkx0_zero, &ekeNhc, &potNHC,
                                 1.0, 1.0, &degfs, &istr, &iend, 1, false, 1.0, 1.0);
 }
+
+// CPINTEGRATE::CP_integrate_min_STD (cp_min_std.C:17-60) and
+// CP_integrate_min_CG (cp_min_CG.C:29-120) for one state, and
+// CP_fovlap_calc (cp_min_CG.C:128-140).
+extern "C" void ref_min_step(int ncoef, double* forces, double* conj, double* psi, const int* kx, const int* ky,
+                             const int* kz, double* cmass, double dt, double gamma, double box, double ecut_ry) {
+  set_cell(box);
+  readonly_general_data.gentimeinfo.dt = dt;
+  readonly_cp.cpcoeffs_info.ecut_psi = ecut_ry;
+  if (conj)
+    CPINTEGRATE::CP_integrate_min_CG(ncoef, 0, (complex*)forces, (complex*)conj, (complex*)psi,
+                                     const_cast<int*>(kx), const_cast<int*>(ky), const_cast<int*>(kz), cmass, gamma,
+                                     0);
+  else
+    CPINTEGRATE::CP_integrate_min_STD(ncoef, 0, (complex*)forces, (complex*)psi, const_cast<int*>(kx),
+                                      const_cast<int*>(ky), const_cast<int*>(kz), cmass, 0);
+}
+extern "C" double ref_fovlap(int ncoef, double* forces) {
+  double f = 0.0;
+  CPINTEGRATE::CP_fovlap_calc(ncoef, 0, (complex*)forces, &f);
+  return f;
+}

@@ -194,3 +194,32 @@ def test_integrate_dyn_pinned(ref, sysm, iteration):
         assert np.max(np.abs(vv[r0:] - v_or[st, r0:])) <= 1e-14 * np.max(np.abs(v_or[st]))
         assert np.max(np.abs(pp[r0:] - p_or[st, r0:])) <= 1e-14 * np.max(np.abs(p_or[st]))
         assert abs(ke.value - ke_or[st]) <= 1e-13 * abs(ke_or[st])
+
+
+@pytest.mark.parametrize("cg", [False, True])
+def test_min_step_pinned(ref, sysm, cg):
+    """CP_integrate_min_STD / CP_integrate_min_CG and CP_fovlap_calc against
+    oracle.min_step / fovlap, per state."""
+    s = sysm
+    ref.ref_min_step.argtypes = [C.c_int, dp, dp, dp, ip, ip, ip, dp, C.c_double, C.c_double, C.c_double, C.c_double]
+    ref.ref_fovlap.argtypes = [C.c_int, dp]
+    ref.ref_fovlap.restype = C.c_double
+    rng = np.random.default_rng(8)
+    shape = s.psi.shape
+    f = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) * 0.1
+    conj0 = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) * 0.05 if cg else None
+    gamma, dt = 0.37, 5.0
+    p_or, c_or = O.min_step(s.psi, f, s, dt, conj0, gamma)
+    kx, ky, kz = (np.ascontiguousarray(a, dtype=np.int32) for a in (s.kx, s.ky, s.kz))
+    cm = np.ascontiguousarray(s.cmass, dtype=np.float64)
+    for st in range(s.nstate):
+        ff = np.ascontiguousarray(f[st].copy())
+        pp = np.ascontiguousarray(s.psi[st].copy())
+        cc = np.ascontiguousarray(conj0[st].copy()) if cg else None
+        ref.ref_min_step(s.ng, _d(ff.view(np.float64)), _d(cc.view(np.float64)) if cg else None,
+                         _d(pp.view(np.float64)), _i(kx), _i(ky), _i(kz), _d(cm), dt, gamma, s.box, s.ecut_ry)
+        assert np.max(np.abs(pp - p_or[st])) <= 1e-14 * np.max(np.abs(p_or[st]))
+        if cg:
+            assert np.max(np.abs(cc - c_or[st])) <= 1e-14 * np.max(np.abs(c_or[st]))
+        fv = ref.ref_fovlap(s.ng, _d(np.ascontiguousarray(f[st]).view(np.float64)))
+        assert abs(fv - O.fovlap(f[st:st + 1])) <= 1e-13 * fv
