@@ -812,12 +812,12 @@ extern "C" oa_status oa_gpu_time_kernels(oa_ctx* c, void* stream, const double* 
       p->pl_key[0].valid = p->pl_key[1].valid = false;
       OA_CUDA_TRY(mixed_bwd(c, s, 3, p->eye, psi, -0.5, -1.0, p->eye, F, 1.0, n, n, K, K0, G, 0, 1));
       OA_TIME(7, mixed_bwd(c, s, 3, p->eye, psi, -0.5, -1.0, p->eye, F, 1.0, n, n, K, K0, G, 0, 1));
-      OA_TIME(10, mixed_fwd(c, s, 3, psi, F, n, n, K, K0, 1.0, 1.0, S, 0, 1));
+      OA_TIME(10, mixed_fwd(c, s, 3, psi, F, n, n, K, K0, 1.0, 1.0, T, 0, 1));
       p->pl_cache = 0;
       p->pl_key[0].valid = p->pl_key[1].valid = p->pl_key[2].valid = false;
     } else {
       OA_TIME(7, oa_launch_pc_bwd(s, p->eye, psi, -0.5, -1.0, p->eye, F, 1.0, n, K, K0, G));
-      OA_TIME(10, oa_launch_pc_fwd(s, psi, F, n, K, K0, 1.0, 1.0, p->part, p->nkb, S));
+      OA_TIME(10, oa_launch_pc_fwd(s, psi, F, n, K, K0, 1.0, 1.0, p->part, p->nkb, T));
     }
     OA_TIME(8, oa_launch_ortho_ns(s, S, n, 0.5, 1e-15, 1000, p->ns_work, T, p->ns_status, p->ns_err,
                                   ns_launch_grid(p)));
