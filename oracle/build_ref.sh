@@ -24,6 +24,8 @@ SRCS=(
   "$PINY/abinito_physics/cp_integrate/cp_isokin.C"
   "$PINY/abinito_physics/cp_integrate/cp_min_std.C"
   "$PINY/abinito_physics/cp_integrate/cp_min_CG.C"
+  "$PINY/abinito_physics/cp_nonlocal/cp_ees_nonlocal.C"
+  "$PINY/interface/cp_ewald/set_cp_ewald.C"
 )
 OBJS=()
 for s in "${SRCS[@]}"; do

@@ -432,10 +432,13 @@ def ees_dfactor(sysm, grid, order):
 def ees_bsplines(sysm, grid, order):
     """``eesAtmBsplineRgrp`` (``cp_ees_nonlocal.C:256-593``): for each nonlocal
     atom the order^3 grid points (ia, ib, ic) and weights M_a M_b M_c of its
-    cardinal B-spline.  Returns (idx [natm_nl, 3, order] int, mn [natm_nl, 3, order])."""
+    cardinal B-spline, and the derivative weights dM = M_{n-1}(u) - M_{n-1}(u - 1)
+    taken from the recursion at n = order - 1 (``:436-449``).  Returns
+    (idx [natm_nl, 3, order] int, mn [natm_nl, 3, order], dmn [natm_nl, 3, order])."""
     nl = sysm.nl_atoms()
     idx = np.zeros((len(nl), 3, order), dtype=np.int64)
     mn = np.zeros((len(nl), 3, order))
+    dmn = np.zeros((len(nl), 3, order))
     for ia_, a in enumerate(nl):
         for ax in range(3):
             ng = grid[ax]
@@ -454,13 +457,16 @@ def ees_bsplines(sysm, grid, order):
                 for j in range(n, 1, -1):
                     m[j] = (u[j - 1] * m[j] + (n - u[j - 1]) * m[j - 1]) / (n - 1)
                 m[1] = u[0] * m[1] / (n - 1)
+                if n == order - 1:
+                    dmn[ia_, ax, 0] = m[1]
+                    dmn[ia_, ax, 1:] = m[2:order + 1] - m[1:order]
             for j in range(1, order + 1):
                 g = it - (j - 2)
                 g = g if g > 0 else ng + g
                 g = g if g <= ng else g - ng
                 idx[ia_, ax, j - 1] = g - 1
                 mn[ia_, ax, j - 1] = m[j]
-    return idx, mn
+    return idx, mn, dmn
 
 
 def ees_setup(sysm, scale=1.2, order=6):
@@ -483,19 +489,12 @@ def _nl_grid_r_to_g(fr, sysm, grid):
     return full[..., sysm.kz % nc, sysm.ky % nb, sysm.kx % na]
 
 
-def nl_ees_energy_forces(psi, sysm, ees):
-    """EES nonlocal energy and coefficient forces, l = 0 channel:
-    ``eesProjGchare`` (``cp_ees_nonlocal.C:594-727``: dyp = d y00 p(|g|),
-    projPsiG = conj(dyp psi)), the nonlocal-grid FFT, ``eesZmatRchare``
-    (1238-1352: zmat = sum projPsiR M over the B-spline stencil),
-    ``eesEnergyAtmForcRchare`` (1480-1720: ENL = occ vnorm/V sum zmat^2,
-    zmat <- 2 vnorm/V occ zmat, scatter zmat M onto the grid), the inverse
-    nonlocal-grid FFT and ``eesPsiForcGspace`` (2000-2079:
-    F -= w conj(dyp P), w = 1 on kx = 0, 2 elsewhere; at g = 0 the
-    imaginary parts of P and dyp are dropped).  Returns (F_nl, per-state ENL, zmat)."""
-    grid, order, d = ees["grid"], ees["order"], ees["d"]
-    idx, mn = ees["bspl"]
-    na, nb, nc = grid
+def ees_dyp(sysm, ees):
+    """``eesProjGchare`` + ``eesYlmOnD`` (``cp_ees_nonlocal.C:594-735``), l = 0:
+    dyp(g) = d(g) y00 p(|g|) with y00 = 1/sqrt(4 pi), the projector spline p of
+    the nonlocal atom type and its g = 0 value (``gzvps0``) at g = 0, where
+    dyp is real."""
+    d = ees["d"]
     nl = sysm.nl_atoms()
     f = TWO_PI / sysm.box
     g = f * np.sqrt(sysm.kx.astype(np.float64) ** 2 + sysm.ky ** 2 + sysm.kz ** 2)
@@ -504,8 +503,28 @@ def nl_ees_energy_forces(psi, sysm, ees):
     p = sysm.nl_proj.eval(np.full(g.shape, t), np.where(g == 0, 1.0, g))
     p = np.where(g == 0, sysm.nl_gz0[t], p)
     dyp = d * y00 * p
-    g0 = g == 0
-    dyp = np.where(g0, dyp.real, dyp)
+    return np.where(g == 0, dyp.real, dyp)
+
+
+def nl_ees_energy_forces(psi, sysm, ees, atom_forces=False):
+    """EES nonlocal energy and coefficient forces, l = 0 channel:
+    ``eesProjGchare`` (``cp_ees_nonlocal.C:594-727``: dyp = d y00 p(|g|),
+    projPsiG = conj(dyp psi)), the nonlocal-grid FFT, ``eesZmatRchare``
+    (1238-1352: zmat = sum projPsiR M over the B-spline stencil),
+    ``eesEnergyAtmForcRchare`` (1480-1720: ENL = occ vnorm/V sum zmat^2,
+    zmat <- 2 vnorm/V occ zmat, scatter zmat M onto the grid; atom force
+    F -= zmat sum projPsiR dM, dM_x = dMa Mb Mc n_a / L and so on), the inverse
+    nonlocal-grid FFT and ``eesPsiForcGspace`` (2000-2079:
+    F -= w conj(dyp P), w = 1 on kx = 0, 2 elsewhere; at g = 0 the
+    imaginary parts of P and dyp are dropped).  Returns (F_nl, per-state ENL,
+    zmat), and the atom forces [natm, 3] as a fourth item when atom_forces."""
+    grid, order = ees["grid"], ees["order"]
+    idx, mn, dmn = ees["bspl"]
+    na, nb, nc = grid
+    nl = sysm.nl_atoms()
+    t = int(sysm.atm_type[nl[0]]) if len(nl) else 0
+    dyp = ees_dyp(sysm, ees)
+    g0 = (sysm.kx == 0) & (sysm.ky == 0) & (sysm.kz == 0)
     vn = sysm.nl_vnorm[t] / sysm.vol
     proj = np.conj(dyp[None, :] * psi)
     pr = _nl_grid_g_to_r(proj, sysm, grid)                     # [nstate, nc, nb, na]
@@ -514,6 +533,7 @@ def nl_ees_energy_forces(psi, sysm, ees):
     zmat = np.zeros((nst, len(nl)))
     scr = np.zeros_like(pr)
     w3 = []
+    subs = []
     for a in range(len(nl)):
         ia, ib, ic = idx[a]
         ma, mb, mc = mn[a]
@@ -521,6 +541,7 @@ def nl_ees_energy_forces(psi, sysm, ees):
         sub = pr[:, ic][:, :, ib][:, :, :, ia]                   # [s, jc, jb, ja]
         zmat[:, a] = np.einsum("skji,kji->s", sub, W)
         w3.append(W)
+        subs.append(sub)
     enl = sysm.occ * vn * np.sum(zmat * zmat, axis=1)
     zs = zmat * (2.0 * vn) * sysm.occ[:, None]
     for a in range(len(nl)):
@@ -531,7 +552,18 @@ def nl_ees_energy_forces(psi, sysm, ees):
     P = np.where(g0[None, :], P.real, P)
     w = np.where(sysm.kx == 0, 1.0, 2.0)
     fnl = -w[None, :] * np.conj(dyp[None, :] * P)
-    return fnl, enl, zmat
+    if not atom_forces:
+        return fnl, enl, zmat
+    fatm = np.zeros((sysm.natm, 3))
+    for a, atom in enumerate(nl):
+        ma, mb, mc = mn[a]
+        da, db, dc = dmn[a]
+        dw = (np.einsum("i,j,k->kji", da, mb, mc) * (na / sysm.box),
+              np.einsum("i,j,k->kji", ma, db, mc) * (nb / sysm.box),
+              np.einsum("i,j,k->kji", ma, mb, dc) * (nc / sysm.box))
+        for ax in range(3):
+            fatm[atom, ax] -= np.sum(zs[:, a] * np.einsum("skji,kji->s", subs[a], dw[ax]))
+    return fnl, enl, zmat, fatm
 
 
 # ----------------------------------------------------------------------------

@@ -62,15 +62,16 @@ void* cmalloc(size_t n, const char*) { return std::malloc(n ? n : 1); }
 void cfree(void* p, const char*) { std::free(p); }
 
 // Symbols the compiled files reference on paths the oracle never takes:
-// timers, the EISPACK eigen-solver of get_diag_Tmat, the EES B-spline
-// setup of the EES Hartree variant, and the wave generator's class.
+// timers, the EISPACK eigen-solver of get_diag_Tmat, the cell determinant
+// of the Ewald set-up routines (set_cp_ewald.C is linked for
+// get_bspline_wght1d only), and the wave generator's class.
 void cputime(double* t) { *t = 0.0; }
 extern "C" void rs_(int*, int*, double*, double*, int*, double*, double*, double*, int*) {
   std::fprintf(stderr, "oracle/_ref: rs_ (EISPACK) is not provided\n");
   std::abort();
 }
-void get_bspline_wght1d(int, int, double*, double*, double*, double*, double*, double*, double*, double*) {
-  std::fprintf(stderr, "oracle/_ref: EES B-spline setup is not provided\n");
+double getdeth(double*) {
+  std::fprintf(stderr, "oracle/_ref: getdeth is not provided\n");
   std::abort();
 }
 GEN_WAVE::GEN_WAVE() {}
@@ -341,4 +342,274 @@ extern "C" double ref_fovlap(int ncoef, double* forces) {
   double f = 0.0;
   CPINTEGRATE::CP_fovlap_calc(ncoef, 0, (complex*)forces, &f);
   return f;
+}
+
+// ---------------------------------------------------------------------------
+// EES nonlocal, l = 0 KB channel (cp_ees_nonlocal.C), doublePack, Gamma.
+// The test runs the routines in three phases with the oracle's nonlocal-grid
+// transforms in between (the FFT boundary has no reference implementation
+// here):
+//   ref_ees_config   the PINY nonlocal setup the routines read (kept here)
+//   ref_ees_gproj    eesSetEesWghtGgrp (60-160), eesSplProjectorGgrp
+//                    (182-250), eesProjGchare + eesYlmOnD (594-735): d(g),
+//                    dyp(g) and projPsiG = conj(dyp psi) of every state
+//   ref_ees_rspace   eesAtmBsplineRgrp (256-593), eesZmatRchare (1238-1352)
+//                    summed over the planes, eesEnergyAtmForcRchare
+//                    (1480-1720) on every plane with its own copy of the
+//                    summed zmat: ENL, the scaled zmat, the scattered grid
+//                    projPsiRScr and the atom forces
+//   ref_ees_psi_forc eesPsiForcGspace (2000-2079)
+// Grids are real [nc][nb][na + 2] (the x-padded doublePack plane layout
+// the routines index, igrid_b = (ib - 1)(na + 2)).
+namespace {
+struct EesCfg {
+  int ng = 0, na = 0, nb = 0, nc = 0, order = 0, natm = 0, natm_nl = 0, ntyp_nl = 0, ind_g0 = -1, nkx0 = 0;
+  double box = 0.0;
+  std::vector<int> kx, ky, kz, map_nl, natm_lang, iatm_str_lang, natm_typ_lang, lang_v, mang_v, ityp_v;
+  std::vector<std::vector<int>> typ_rows;
+  std::vector<int*> iatm_typ_lang;
+  std::vector<double> v0, v1, v2, v3, gz0, vpsnorm, occ_up, wkpt, kpt0, pos;
+  std::vector<double> d_re, d_im;                  // eesSetEesWghtGgrp
+  std::vector<double> h_spl;                       // eesSplProjectorGgrp
+  std::vector<int> ind_spl;
+  std::vector<double> dyp_re, dyp_im;              // [ntyp_nl][ng]
+} g_ees;
+
+void ees_apply() {
+  EesCfg& e = g_ees;
+  set_cell(e.box);
+  CP* cp = &readonly_cp;
+  CPPSEUDO* ps = &cp->cppseudo;
+  PSNONLOCAL* nl = &ps->nonlocal;
+  ps->nsplin_g = (int)(e.v0.size() - 1) / std::max(1, (int)e.gz0.size() - 1);
+  ps->n_ang_max = 0;
+  ps->n_interp_ps = e.order;
+  ps->vps0 = e.v0.data(); ps->vps1 = e.v1.data(); ps->vps2 = e.v2.data(); ps->vps3 = e.v3.data();
+  ps->gzvps0 = e.gz0.data();
+  ps->vpsnorm = e.vpsnorm.data();
+  nl->natm = e.natm_nl;
+  nl->n_interp = e.order;
+  nl->n_interp2 = e.order * e.order;
+  nl->ngrid_a = e.na; nl->ngrid_b = e.nb; nl->ngrid_c = e.nc;
+  nl->nfft = e.na * e.nb * e.nc;
+  nl->map_nl = e.map_nl.data();
+  nl->natm_lang = e.natm_lang.data();
+  nl->iatm_str_lang = e.iatm_str_lang.data();
+  nl->natm_typ_lang = e.natm_typ_lang.data();
+  nl->iatm_typ_lang = e.iatm_typ_lang.data();
+  nl->lang_v = e.lang_v.data(); nl->mang_v = e.mang_v.data(); nl->ityp_v = e.ityp_v.data();
+  cp->cpewald.doublepack = 1;
+  cp->cpewald.akpoint = cp->cpewald.bkpoint = cp->cpewald.ckpoint = e.kpt0.data();
+  cp->cpcoeffs_info.nkpoint = 1;
+  cp->cpcoeffs_info.igamma_kpt_ind = 1;
+  cp->cpcoeffs_info.occ_up = e.occ_up.data();
+  cp->cpcoeffs_info.wght_kpt = e.wkpt.data();
+  cp->cpylm_cons.rt_fpi = 1.0 / std::sqrt(4.0 * M_PI);
+}
+}  // namespace
+
+// Set up: g-points (the system's doublePack order, kx = 0 first), states'
+// occupations, atoms (nl_atm grouped by type in type order), the l = 0
+// projector spline per type [ntype][nspl][4], vnorm and g = 0 value per
+// type, the box, the EES grid and the interpolation order.
+extern "C" void ref_ees_config(int ng, const int* kx, const int* ky, const int* kz, int nstate, const double* occ,
+                               int natm, const double* pos, const int* atm_type, int ntype, int natm_nl,
+                               const int* nl_atm, int nspl, double gmin, double dg, const double* spl,
+                               const double* vnorm_typ, const double* gz0_typ, double box, int na, int nb, int nc,
+                               int order) {
+  EesCfg& e = g_ees;
+  e = EesCfg();
+  e.ng = ng; e.na = na; e.nb = nb; e.nc = nc; e.order = order; e.natm = natm; e.natm_nl = natm_nl; e.box = box;
+  e.kx.assign(kx, kx + ng); e.ky.assign(ky, ky + ng); e.kz.assign(kz, kz + ng);
+  for (int i = 0; i < ng; ++i) {
+    if (kx[i] == 0 && ky[i] == 0 && kz[i] == 0) e.ind_g0 = i;
+    if (kx[i] == 0) e.nkx0++;
+  }
+  e.pos.assign(pos, pos + 3 * natm);
+  e.occ_up.assign(nstate + 1, 0.0);
+  for (int s = 0; s < nstate; ++s) e.occ_up[s + 1] = occ[s];
+  e.wkpt.assign(2, 1.0);
+  e.kpt0.assign(2, 0.0);
+  e.v0.assign(ntype * nspl + 1, 0.0); e.v1 = e.v0; e.v2 = e.v0; e.v3 = e.v0;
+  for (int t = 0; t < ntype; ++t)
+    for (int i = 0; i < nspl; ++i) {
+      const double* c = spl + ((size_t)t * nspl + i) * 4;
+      const int idx = t * nspl + i + 1;
+      e.v0[idx] = c[0]; e.v1[idx] = c[1]; e.v2[idx] = c[2]; e.v3[idx] = c[3];
+    }
+  e.gz0.assign(ntype + 1, 0.0);
+  e.vpsnorm.assign(ntype + 1, 0.0);
+  for (int t = 0; t < ntype; ++t) { e.gz0[t + 1] = gz0_typ[t]; e.vpsnorm[t + 1] = vnorm_typ[t]; }
+  // one l = 0 iteration per atom type with a projector (iter_nl = 1, 2, ...)
+  e.map_nl.assign(natm_nl + 1, 0);
+  e.natm_lang.assign(ntype + 1, 0);
+  e.iatm_str_lang.assign(ntype + 1, 0);
+  std::vector<int> typ_list;
+  for (int i = 0; i < natm_nl; ++i) {
+    const int a = nl_atm[i], t = atm_type[a] + 1;
+    e.map_nl[i + 1] = a + 1;
+    if (e.natm_lang[t] == 0) { e.iatm_str_lang[t] = i + 1; typ_list.push_back(t); }
+    e.natm_lang[t]++;
+  }
+  e.ntyp_nl = (int)typ_list.size();
+  e.natm_typ_lang.assign(2, 0);
+  e.natm_typ_lang[1] = e.ntyp_nl;
+  e.typ_rows.assign(e.ntyp_nl + 1, std::vector<int>(2, 0));
+  for (int k = 0; k < e.ntyp_nl; ++k) e.typ_rows[k + 1][1] = typ_list[k];
+  e.iatm_typ_lang.resize(e.ntyp_nl + 1);
+  for (int k = 0; k <= e.ntyp_nl; ++k) e.iatm_typ_lang[k] = e.typ_rows[k].data();
+  e.lang_v.assign(e.ntyp_nl + 1, 0);
+  e.mang_v.assign(e.ntyp_nl + 1, 0);
+  e.ityp_v.assign(e.ntyp_nl + 1, 0);
+  for (int k = 1; k <= e.ntyp_nl; ++k) e.ityp_v[k] = k;
+  readonly_cp.cppseudo.nsplin_g = nspl;
+  readonly_cp.cppseudo.dg_spl = dg;
+  readonly_cp.cppseudo.gmin_spl = gmin;
+}
+
+// d(g) [ng] complex, dyp(g) [ntyp_nl][ng] complex and projPsiG
+// [ntyp_nl][nstate][ng] complex for the states psi [nstate][ng].
+extern "C" int ref_ees_gproj(int nstate, const double* psi, double* d, double* dyp, double* proj) {
+  EesCfg& e = g_ees;
+  ees_apply();
+  const int ng = e.ng;
+  e.d_re.assign(ng, 0.0); e.d_im.assign(ng, 0.0);
+  CPNONLOCAL::eesSetEesWghtGgrp(ng, e.kx.data(), e.ky.data(), e.kz.data(), e.d_re.data(), e.d_im.data(), e.na, e.nb,
+                                e.nc, e.order);
+  e.h_spl.assign(ng, 0.0); e.ind_spl.assign(ng, 0);
+  double* hs[1] = {e.h_spl.data()};
+  int* is[1] = {e.ind_spl.data()};
+  CPNONLOCAL::eesSplProjectorGgrp(ng, e.kx.data(), e.ky.data(), e.kz.data(), hs, is);
+  for (int i = 0; i < ng; ++i) { d[2 * i] = e.d_re[i]; d[2 * i + 1] = e.d_im[i]; }
+  e.dyp_re.assign((size_t)e.ntyp_nl * ng, 0.0); e.dyp_im = e.dyp_re;
+  const int ihave_g0 = e.ind_g0 >= 0 ? 1 : 0;
+  for (int it = 1; it <= e.ntyp_nl; ++it) {
+    double* yr = e.dyp_re.data() + (size_t)(it - 1) * ng;
+    double* yi = e.dyp_im.data() + (size_t)(it - 1) * ng;
+    for (int s = 0; s < nstate; ++s) {
+      complex* pg = (complex*)proj + ((size_t)(it - 1) * nstate + s) * ng;
+      CPNONLOCAL::eesProjGchare(ng, (complex*)const_cast<double*>(psi) + (size_t)s * ng, e.kx.data(), e.ky.data(),
+                                e.kz.data(), ihave_g0, e.ind_g0, it, e.d_re.data(), e.d_im.data(), yr, yi, pg, is, hs,
+                                s, 0, 0, 1, 0);
+    }
+    for (int i = 0; i < ng; ++i) {
+      dyp[2 * ((size_t)(it - 1) * ng + i)] = yr[i];
+      dyp[2 * ((size_t)(it - 1) * ng + i) + 1] = yi[i];
+    }
+  }
+  return e.ntyp_nl;
+}
+
+// projPsiR [ntyp_nl][nstate][nc][nb][na + 2] -> zmat (summed over planes,
+// unscaled) [ntyp_nl][nstate][natm of the type] laid out per nonlocal atom
+// [nstate][natm_nl], enl [nstate], the scattered grid projPsiRScr (same
+// shape as projPsiR) and the atom forces fatm [natm][3] (accumulated).
+extern "C" void ref_ees_rspace(int nstate, const double* prr, double* zmat, double* enl, double* scr, double* fatm) {
+  EesCfg& e = g_ees;
+  ees_apply();
+  const int n = e.order, n2 = n * n, natm = e.natm, nnl = e.natm_nl;
+  const int lda = e.na + 2;
+  const size_t plane = (size_t)lda * e.nb, grid = plane * e.nc;
+  // PSSCRATCH for the B-spline routine ([j][i] with j = 1..n)
+  std::vector<double> aj(n + 1), rn(n + 1), rn1(n + 1), fa(nnl), fb(nnl), fc(nnl);
+  std::vector<int> ixa(n + 1), ixb(n + 1), iga(n + 1), igb(n + 1), iat(nnl), ibt(nnl), ict(nnl);
+  std::vector<std::vector<int>> gi_a(n + 1, std::vector<int>(nnl)), gi_b = gi_a, gi_c = gi_a;
+  std::vector<std::vector<double>> m_a(n + 1, std::vector<double>(nnl)), m_b = m_a, m_c = m_a, u_a = m_a, u_b = m_a,
+                                   u_c = m_a, dm_a = m_a, dm_b = m_a, dm_c = m_a;
+  auto rows_i = [](std::vector<std::vector<int>>& v) {
+    std::vector<int*> p(v.size());
+    for (size_t i = 0; i < v.size(); ++i) p[i] = v[i].data();
+    return p;
+  };
+  auto rows_d = [](std::vector<std::vector<double>>& v) {
+    std::vector<double*> p(v.size());
+    for (size_t i = 0; i < v.size(); ++i) p[i] = v[i].data();
+    return p;
+  };
+  auto pga = rows_i(gi_a), pgb = rows_i(gi_b), pgc = rows_i(gi_c);
+  auto pma = rows_d(m_a), pmb = rows_d(m_b), pmc = rows_d(m_c), pua = rows_d(u_a), pub = rows_d(u_b),
+       puc = rows_d(u_c), pda = rows_d(dm_a), pdb = rows_d(dm_b), pdc = rows_d(dm_c);
+  PSSCRATCH ps;
+  ps.aj = aj.data(); ps.rn = rn.data(); ps.rn1 = rn1.data();
+  ps.index_a = ixa.data(); ps.index_b = ixb.data(); ps.igrid_at = iga.data(); ps.igrid_bt = igb.data();
+  ps.iatemp = iat.data(); ps.ibtemp = ibt.data(); ps.ictemp = ict.data();
+  ps.frac_a = fa.data(); ps.frac_b = fb.data(); ps.frac_c = fc.data();
+  ps.igrid_a = pga.data(); ps.igrid_b = pgb.data(); ps.igrid_c = pgc.data();
+  ps.mn_a = pma.data(); ps.mn_b = pmb.data(); ps.mn_c = pmc.data();
+  ps.ua = pua.data(); ps.ub = pub.data(); ps.uc = puc.data();
+  ps.dmn_a = pda.data(); ps.dmn_b = pdb.data(); ps.dmn_c = pdc.data();
+  // per-plane B-spline data (RPPDATA, [natm_nl][n^2 + 1])
+  std::vector<RPPDATA> rpp(e.nc);
+  std::vector<RPPDATA*> prpp(e.nc);
+  std::vector<std::vector<int>> pidx(e.nc, std::vector<int>(nnl));
+  std::vector<std::vector<std::vector<int>>> ig(e.nc, std::vector<std::vector<int>>(nnl, std::vector<int>(n2 + 1)));
+  std::vector<std::vector<std::vector<double>>> mn(e.nc, std::vector<std::vector<double>>(nnl, std::vector<double>(n2 + 1)));
+  auto dx = mn, dy = mn, dz = mn;
+  std::vector<std::vector<int*>> pig(e.nc);
+  std::vector<std::vector<double*>> pmn(e.nc), pdx(e.nc), pdy(e.nc), pdz(e.nc);
+  for (int p = 0; p < e.nc; ++p) {
+    pig[p] = rows_i(ig[p]);
+    pmn[p] = rows_d(mn[p]); pdx[p] = rows_d(dx[p]); pdy[p] = rows_d(dy[p]); pdz[p] = rows_d(dz[p]);
+    RPPDATA& r = rpp[p];
+    r.index = p; r.ngrid_a = e.na; r.ngrid_b = e.nb; r.ngrid_c = e.nc; r.n_interp = n; r.natm = nnl;
+    r.plane_index = pidx[p].data();
+    r.igrid = pig[p].data();
+    r.mn = pmn[p].data(); r.dmn_x = pdx[p].data(); r.dmn_y = pdy[p].data(); r.dmn_z = pdz[p].data();
+    r.nBreakJ = nullptr; r.sBreakJ = nullptr;
+    prpp[p] = &r;
+  }
+  std::vector<double> x(natm), y(natm), z(natm), fx(natm, 0.0), fy(natm, 0.0), fz(natm, 0.0);
+  for (int a = 0; a < natm; ++a) { x[a] = e.pos[3 * a]; y[a] = e.pos[3 * a + 1]; z[a] = e.pos[3 * a + 2]; }
+  FastAtoms at;
+  at.natm = natm; at.x = x.data(); at.y = y.data(); at.z = z.data();
+  at.fx = fx.data(); at.fy = fy.data(); at.fz = fz.data();
+  std::vector<int> allowed(e.nc, 1);
+  CPNONLOCAL::eesAtmBsplineRgrp(&at, allowed.data(), prpp.data(), &ps);
+  std::vector<double> zp(nnl), zsum(nnl), zcopy(nnl);
+  for (int s = 0; s < nstate; ++s) {
+    enl[s] = 0.0;
+    for (int it = 1; it <= e.ntyp_nl; ++it) {
+      const int t = e.iatm_typ_lang[it][1];
+      const int na_t = e.natm_lang[t], a0 = e.iatm_str_lang[t] - 1;
+      const double* pr = prr + ((size_t)(it - 1) * nstate + s) * grid;
+      double* sc = scr + ((size_t)(it - 1) * nstate + s) * grid;
+      std::fill(zsum.begin(), zsum.end(), 0.0);
+      for (int p = 0; p < e.nc; ++p) {
+        CPNONLOCAL::eesZmatRchare(const_cast<double*>(pr) + p * plane, it, zp.data(), rpp[p].igrid, rpp[p].mn,
+                                  rpp[p].plane_index, s, p);
+        for (int j = 0; j < na_t; ++j) zsum[j] += zp[j];
+      }
+      for (int j = 0; j < na_t; ++j) zmat[(size_t)s * nnl + a0 + j] = zsum[j];
+      for (int p = 0; p < e.nc; ++p) {
+        for (int j = 0; j < na_t; ++j) zcopy[j] = zsum[j];
+        double ep = 0.0;
+        CPNONLOCAL::eesEnergyAtmForcRchare(it, &ep, zcopy.data(), rpp[p].igrid, rpp[p].mn, rpp[p].dmn_x,
+                                           rpp[p].dmn_y, rpp[p].dmn_z, const_cast<double*>(pr) + p * plane,
+                                           sc + p * plane, rpp[p].plane_index, nullptr, nullptr, p, s, 0, &at);
+        if (p == 0) enl[s] += ep;  // every plane computes it; one (the reduction plane) reports it
+      }
+    }
+  }
+  for (int a = 0; a < natm; ++a) { fatm[3 * a] += fx[a]; fatm[3 * a + 1] += fy[a]; fatm[3 * a + 2] += fz[a]; }
+}
+
+// fPsiG [nstate][ng] complex (accumulated) from projPsiG [ntyp_nl][nstate][ng]
+// (the inverse nonlocal-grid transform of projPsiRScr, at the g-points) and
+// the dyp of ref_ees_gproj.
+extern "C" void ref_ees_psi_forc(int nstate, const double* projg, double* fpsi) {
+  EesCfg& e = g_ees;
+  ees_apply();
+  const int ng = e.ng;
+  std::vector<complex> pg(ng);
+  std::vector<double> yr(ng), yi(ng);
+  for (int it = 1; it <= e.ntyp_nl; ++it)
+    for (int s = 0; s < nstate; ++s) {
+      const complex* src = (const complex*)projg + ((size_t)(it - 1) * nstate + s) * ng;
+      std::copy(src, src + ng, pg.begin());
+      std::copy(e.dyp_re.begin() + (size_t)(it - 1) * ng, e.dyp_re.begin() + (size_t)it * ng, yr.begin());
+      std::copy(e.dyp_im.begin() + (size_t)(it - 1) * ng, e.dyp_im.begin() + (size_t)it * ng, yi.begin());
+      CPNONLOCAL::eesPsiForcGspace(ng, e.ind_g0 >= 0 ? 1 : 0, e.ind_g0, e.nkx0, pg.data(),
+                                   (complex*)fpsi + (size_t)s * ng, yr.data(), yi.data(), e.kx.data(), e.ky.data(),
+                                   e.kz.data(), s, 0, it, 1, 0);
+    }
 }

@@ -141,6 +141,24 @@ def test_ees_nonlocal_matches_structure_factor():
     assert errs[2] < 1e-5
 
 
+def test_ees_atom_forces_are_energy_gradient():
+    """EES nonlocal atom forces (eesEnergyAtmForcRchare, the B-spline
+    derivative weights of eesAtmBsplineRgrp) against a central finite
+    difference of the EES nonlocal energy in each atom coordinate."""
+    s = make_system("w4", seed=21)
+    ees = O.ees_setup(s, scale=1.2, order=4)
+    fa = O.nl_ees_energy_forces(s.psi, s, ees, atom_forces=True)[3]
+    a = int(s.nl_atoms()[0])
+    h = 1e-5
+    for ax in range(3):
+        es = []
+        for sg in (1.0, -1.0):
+            s.pos[a, ax] += sg * h
+            es.append(O.nl_ees_energy_forces(s.psi, s, O.ees_setup(s, scale=1.2, order=4))[1].sum())
+            s.pos[a, ax] -= sg * h
+        assert abs(-(es[0] - es[1]) / (2 * h) - fa[a, ax]) < 1e-7 * np.max(np.abs(fa[a]))
+
+
 def test_cg_minimisation_beats_steepest_descent():
     """The oracle's minimisation loop (computeMinimization): both methods
     lower the energy; conjugate gradients lower it further and reduce the

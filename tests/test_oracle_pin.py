@@ -3,10 +3,13 @@ compiled from the reference sources into oracle/_ref/libpiny_ref.so by
 oracle/build_ref.sh (CPU only).
 
 Pinned: CPNONLOCAL::CP_eke_calc (cp_eke.C), CPXCFNCTS::CP_exc_calc
-(cp_pz_lda.C), CPLOCAL::CP_hart_eext_calc (cp_hart_ext.C) and
-CPORTHOG::get_iter_Tmat (cp_lowdin.C).  The FFT and GEMM boundaries have no
-reference implementation here (FFTW2 / Fortran BLAS are absent) and are
-pinned by mathematics in test_oracle_cpu.py.
+(cp_pz_lda.C), CPLOCAL::CP_hart_eext_calc (cp_hart_ext.C),
+CPORTHOG::get_iter_Tmat (cp_lowdin.C), the structure-factor nonlocal path
+(cp_struct_fact.C, cp_nlmat.C, cp_nl_energy_forc.C), the EES nonlocal path
+(cp_ees_nonlocal.C with get_bspline_wght1d of set_cp_ewald.C), the CP
+integrator (cp_dynamics.C) and the minimisers (cp_min_std.C, cp_min_CG.C).
+The FFT and GEMM boundaries have no reference implementation here (FFTW2 /
+Fortran BLAS are absent) and are pinned by mathematics in test_oracle_cpu.py.
 """
 import ctypes as C
 import os
@@ -223,3 +226,58 @@ def test_min_step_pinned(ref, sysm, cg):
             assert np.max(np.abs(cc - c_or[st])) <= 1e-14 * np.max(np.abs(c_or[st]))
         fv = ref.ref_fovlap(s.ng, _d(np.ascontiguousarray(f[st]).view(np.float64)))
         assert abs(fv - O.fovlap(f[st:st + 1])) <= 1e-13 * fv
+
+
+@pytest.mark.parametrize("order", [4, 6])
+def test_ees_nonlocal_pinned(ref, sysm, order):
+    """EES nonlocal (cp_ees_nonlocal.C), l = 0 channel, in the three phases
+    the reference runs on G-space and real-space chares, with the oracle's
+    nonlocal-grid transforms in between: eesSetEesWghtGgrp (d(g)),
+    eesProjGchare / eesYlmOnD (dyp, projPsiG), eesAtmBsplineRgrp +
+    eesZmatRchare summed over planes (zmat), eesEnergyAtmForcRchare (ENL,
+    atom forces, the scattered grid) and eesPsiForcGspace (F_NL), against
+    oracle.ees_setup / ees_dyp / nl_ees_energy_forces."""
+    s = sysm
+    a = _nl_inputs(s)
+    nnl = len(a["nl"])
+    ees = O.ees_setup(s, scale=1.2, order=order)
+    na, nb, nc = ees["grid"]
+    occ = np.ascontiguousarray(s.occ, dtype=np.float64)
+    ref.ref_ees_config.argtypes = [C.c_int, ip, ip, ip, C.c_int, dp, C.c_int, dp, ip, C.c_int, C.c_int, ip, C.c_int,
+                                   C.c_double, C.c_double, dp, dp, dp, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int]
+    ref.ref_ees_gproj.argtypes = [C.c_int, dp, dp, dp, dp]
+    ref.ref_ees_gproj.restype = C.c_int
+    ref.ref_ees_rspace.argtypes = [C.c_int, dp, dp, dp, dp, dp]
+    ref.ref_ees_psi_forc.argtypes = [C.c_int, dp, dp]
+    ref.ref_ees_config(s.ng, _i(a["kx"]), _i(a["ky"]), _i(a["kz"]), s.nstate, _d(occ), s.natm, _d(a["pos"]),
+                       _i(a["typ"]), len(s.type_names), nnl, _i(a["nl"]), s.nl_proj.n, s.nl_proj.gmin, s.nl_proj.dg,
+                       _d(a["spl"]), _d(a["vn"]), _d(a["gz"]), s.box, na, nb, nc, order)
+    psi = np.ascontiguousarray(s.psi)
+    d = np.zeros(s.ng, dtype=np.complex128)
+    dyp = np.zeros((1, s.ng), dtype=np.complex128)
+    proj = np.zeros((1, s.nstate, s.ng), dtype=np.complex128)
+    assert ref.ref_ees_gproj(s.nstate, _d(psi.view(np.float64)), _d(d.view(np.float64)), _d(dyp.view(np.float64)),
+                             _d(proj.view(np.float64))) == 1
+    assert np.max(np.abs(d - ees["d"])) <= 1e-13 * np.max(np.abs(ees["d"]))
+    dyp_or = O.ees_dyp(s, ees)
+    assert np.max(np.abs(dyp[0] - dyp_or)) <= 1e-13 * np.max(np.abs(dyp_or))
+    assert np.max(np.abs(proj[0] - np.conj(dyp_or[None, :] * s.psi))) <= 1e-13 * np.max(np.abs(proj))
+    # phase 2 on the real-space grid: x padded to na + 2 as the reference stores it
+    pr = O._nl_grid_g_to_r(proj[0], s, ees["grid"])                       # [nstate, nc, nb, na]
+    prr = np.zeros((1, s.nstate, nc, nb, na + 2))
+    prr[0, ..., :na] = pr
+    zmat = np.zeros((s.nstate, nnl))
+    enl = np.zeros(s.nstate)
+    scr = np.zeros_like(prr)
+    fatm = np.zeros((s.natm, 3))
+    ref.ref_ees_rspace(s.nstate, _d(prr), _d(zmat), _d(enl), _d(scr), _d(fatm))
+    f_or, e_or, z_or, fa_or = O.nl_ees_energy_forces(s.psi, s, ees, atom_forces=True)
+    assert np.max(np.abs(zmat - z_or)) <= 1e-12 * np.max(np.abs(z_or))
+    assert np.max(np.abs(enl - e_or)) <= 1e-12 * np.max(np.abs(e_or))
+    assert np.max(np.abs(fatm - fa_or)) <= 1e-11 * np.max(np.abs(fa_or))
+    assert np.max(np.abs(scr[0, ..., na:])) == 0.0
+    # phase 3 back in G space
+    P = O._nl_grid_r_to_g(scr[0, ..., :na], s, ees["grid"])
+    fpsi = np.zeros((s.nstate, s.ng), dtype=np.complex128)
+    ref.ref_ees_psi_forc(s.nstate, _d(np.ascontiguousarray(P).view(np.float64)), _d(fpsi.view(np.float64)))
+    assert np.max(np.abs(fpsi - f_or)) <= 1e-12 * np.max(np.abs(f_or))
