@@ -96,6 +96,12 @@ class CPSystem:
     nl_proj: SplineTable | None = None
     nl_vnorm: np.ndarray | None = None
     nl_gz0: np.ndarray | None = None
+    # exchange-correlation: "pz_lda" (Perdew-Zunger LDA, cp_pz_lda.C) or
+    # "blyp" (Slater exchange + Becke 88 gradient correction + LYP
+    # correlation, cp_becke.C / cp_grad_rho_ctrl.C: \cp_ggax_typ{becke}
+    # \cp_ggac_typ{lyp}); gga_cut is \gradient_cutoff (default 5e-5)
+    xc: str = "pz_lda"
+    gga_cut: float = 5.0e-5
 
     @property
     def vol(self) -> float:
@@ -368,7 +374,9 @@ PRESETS = {
 
 def make_system(preset: str = "w8", seed: int = 1234, nstate: int | None = None,
                 ecut_mass: float = 1.0e30, cmass0: float = 400.0, dt: float = 5.0,
-                **over) -> CPSystem:
+                xc: str = "pz_lda", **over) -> CPSystem:
+    if xc not in ("pz_lda", "blyp"):
+        raise ValueError("xc must be 'pz_lda' or 'blyp'")
     p = dict(PRESETS[preset])
     p.update(over)
     nmol, box, ecut_ry, nfft = p["nmol"], p["box"], p["ecut_ry"], tuple(p["nfft"])
@@ -396,4 +404,4 @@ def make_system(preset: str = "w8", seed: int = 1234, nstate: int | None = None,
                     line_kx=lkx, line_ky=lky, line_off=loff, line_nneg=lneg, line_npos=lpos,
                     nkx0=nkx0, nkx0_red=nred, nkx0_uni=nuni, nkx0_zero=nzero,
                     occ=np.ones(nstate), cmass=cmass, psi=psi, dt=dt, cmass0=cmass0,
-                    nl_proj=nl_proj, nl_vnorm=nl_vnorm, nl_gz0=nl_gz0)
+                    nl_proj=nl_proj, nl_vnorm=nl_vnorm, nl_gz0=nl_gz0, xc=xc)

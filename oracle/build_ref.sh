@@ -15,6 +15,8 @@ FLAGS="-O2 -fPIC -std=c++14 -DCHARM_ON -DFORTRANUNDERSCORE -w -include $HERE/ref
 SRCS=(
   "$PINY/abinito_physics/cp_nonlocal/cp_eke.C"
   "$PINY/abinito_physics/cp_xc_fnctl/cp_pz_lda.C"
+  "$PINY/abinito_physics/cp_xc_fnctl/cp_becke.C"
+  "$PINY/abinito_physics/cp_xc_fnctl/cp_grad_rho_ctrl.C"
   "$PINY/abinito_physics/cp_local/cp_hart_ext.C"
   "$PINY/abinito_physics/cp_orthog/cp_lowdin.C"
   "$PINY/abinito_physics/cp_nonlocal/cp_struct_fact.C"

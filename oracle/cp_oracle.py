@@ -153,9 +153,11 @@ def density(psir, sysm):
     return np.einsum("s,szyx->zyx", sysm.occ, psir * psir) / sysm.vol
 
 
-def pz_lda(rho, vol, npts):
+def pz_lda(rho, vol, npts, lyp=False):
     """``CPXCFNCTS::CP_exc_calc`` (``abinito_physics/cp_xc_fnctl/cp_pz_lda.C:23-175``):
-    Perdew-Zunger LDA.  Returns (vxc(r), exc, muxc)."""
+    Perdew-Zunger LDA.  With LYP correlation on (``cp_lyp``, ``:66``) the PZ
+    correlation is dropped and only Slater exchange remains.  Returns
+    (vxc(r), exc, muxc)."""
     gamma, beta1, beta2 = -0.14230, 1.05290, 0.33340
     au, bu, cu, du = 0.03110, -0.0480, 0.00200, -0.01160
     power = 1.0 / 3.0
@@ -177,6 +179,9 @@ def pz_lda(rho, vol, npts):
             + power * (2.0 * du - cu) * rs)
     cfact = np.where(hi, c_hi, c_lo)
     mufact = np.where(hi, m_hi, m_lo)
+    if lyp:
+        cfact = cfact * 0.0
+        mufact = mufact * 0.0
     ex = float(np.sum(xfact * rho)) * 0.75
     ec = float(np.sum(cfact * rho))
     v = xfact + mufact
@@ -276,14 +281,141 @@ def hart_eext(rho_r, sysm, want_forces=False):
     return out + (fatm,) if want_forces else out
 
 
+BECKE_BETA = 0.0042
+LYP_A, LYP_B, LYP_C, LYP_D = 0.049180, 0.1320, 0.25330, 0.3490
+
+
+def becke88(rho, g):
+    """Becke 88 gradient correction to the LDA exchange (``becke_gcx_lda``,
+    ``cp_becke.C:21-88``), spin-unpolarised: per spin rho_s = rho / 2,
+    x = |grad rho_s| / rho_s^(4/3), b(x) = x^2 / (1 + 6 beta x asinh x),
+    f = -2 beta rho_s^(4/3) b(x).  g = |grad rho|.  Returns
+    (f, df/drho, df/dg)."""
+    beta = BECKE_BETA
+    rs = 0.5 * rho
+    r13 = np.cbrt(rs)
+    r43 = rs * r13
+    x = 0.5 * g / r43
+    root = np.sqrt(1.0 + x * x)
+    ash = np.log(x + root)
+    den = 1.0 + 6.0 * beta * x * ash
+    b = x * x / den
+    q = x / den
+    bp = 2.0 * q - 6.0 * beta * q * q * (ash + x / root)       # db/dx
+    return -2.0 * beta * r43 * b, -beta * (4.0 / 3.0) * r13 * (b - x * bp), -beta * bp
+
+
+def lyp(rho, g):
+    """Lee-Yang-Parr correlation, closed shell, with its local part
+    (``lyp_gcc``, ``cp_becke.C:91-172``): with u = rho^(-1/3), D = 1 + d u,
+    omega = exp(-c u) u^11 / D, delta = c u + d u / D and
+    A = C_F rho^(8/3) + (5/12 - 7 delta / 72) g^2 - 11 g^2 / 24,
+    f = -a rho / D - a b omega A rho^2.  Returns (f, df/drho, df/dg)."""
+    a, b, c, d = LYP_A, LYP_B, LYP_C, LYP_D
+    cf = 0.3 * (3.0 * math.pi * math.pi) ** (2.0 / 3.0)
+    u = 1.0 / np.cbrt(rho)
+    den = 1.0 + d * u
+    om = np.exp(-c * u) * u ** 11 / den
+    dl = c * u + d * u / den
+    g2 = g * g
+    A = cf * rho ** (8.0 / 3.0) + (5.0 / 12.0 - 7.0 * dl / 72.0) * g2 - 11.0 * g2 / 24.0
+    f = -a * rho / den - a * b * om * A * rho * rho
+    # derivatives in rho: du/drho = -u / (3 rho)
+    dom = om * (c * u + d * u / den - 11.0) / (3.0 * rho)
+    ddl = -(u / (3.0 * rho)) * (c + d / (den * den))
+    dA = (8.0 / 3.0) * cf * rho ** (5.0 / 3.0) - (7.0 / 72.0) * ddl * g2
+    dfr = -a * (1.0 + (4.0 / 3.0) * d * u) / (den * den) - a * b * (dom * A * rho * rho + om * (dA * rho * rho + 2.0 * A * rho))
+    dfg = -a * b * om * rho * rho * 2.0 * g * (5.0 / 12.0 - 7.0 * dl / 72.0 - 11.0 / 24.0)
+    return f, dfr, dfg
+
+
+def gga_point(rho, grad, gga_cut, becke=True, lyp_on=True):
+    """The per-point part of ``CPXCFNCTS::CP_getGGAFunctional``
+    (``cp_grad_rho_ctrl.C:32-190``) on points with rho > rho_cut = gga_cut / 10:
+    Becke and LYP times the switching function s(rho) = r^2 (3 - 2 r),
+    r = clamp((rho - rho_cut) / (3.9 gga_cut), 0, 1).  grad: [3, ...].
+    Returns (fx, fc, v = d(fx + fc)/drho, h = d(fx + fc)/d|grad rho| grad rho / |grad rho|),
+    all zero where rho <= rho_cut."""
+    rho_cut = 0.1 * gga_cut
+    heal = 1.0 / (3.9 * gga_cut)
+    on = rho > rho_cut
+    r = np.where(on, rho, 1.0)
+    g2 = grad[0] ** 2 + grad[1] ** 2 + grad[2] ** 2
+    g = np.sqrt(g2)
+    t = np.clip((r - rho_cut) * heal, 0.0, 1.0)
+    sw = t * t * (3.0 - 2.0 * t)
+    dsw = 6.0 * t * (1.0 - t) * heal
+    zero = np.zeros_like(r)
+    fx, dxr, dxg = becke88(r, g) if becke else (zero, zero, zero)
+    fc, dcr, dcg = lyp(r, g) if lyp_on else (zero, zero, zero)
+    v = (dxr + dcr) * sw + (fx + fc) * dsw
+    dg = (dxg + dcg) * sw
+    with np.errstate(divide="ignore", invalid="ignore"):
+        unit = np.where(g2 > 0.0, 1.0 / g, 0.0)
+    h = grad * (dg * unit)[None]
+    fx, fc, v = fx * sw, fc * sw, v
+    return (np.where(on, fx, 0.0), np.where(on, fc, 0.0), np.where(on, v, 0.0),
+            np.where(on[None], h, 0.0))
+
+
+def _sphere_to_r(vals, kx, ky, kz, sysm):
+    """sum over the full density sphere of vals(g) exp(+i g.r) from the
+    kx >= 0 half (the whole kx = 0 plane in it): a c2r transform."""
+    nx, ny, nz = sysm.nfft
+    half = np.zeros((nz, ny, nx // 2 + 1), dtype=np.complex128)
+    half[kz % nz, ky % ny, kx] = vals
+    return _irfftn(half, s=(nz, ny, nx), axes=(0, 1, 2)) * (nx * ny * nz)
+
+
+def density_gradient(rho_r, sysm):
+    """grad rho(r) = sum_sphere i g rho(g) / V exp(i g.r) with
+    rho(g) = FFT_-[rho(r) V/N] (``divRhoVksGspace``, ``CP_Rho_GSpacePlane.C:278-320``,
+    and its backward transforms scaled by 1/V).  Returns [3, nz, ny, nx]."""
+    nx, ny, nz = sysm.nfft
+    n = nx * ny * nz
+    kx, ky, kz, g2 = rho_sphere(sysm)
+    rhog = _rfftn(rho_r * (sysm.vol / n))[kz % nz, ky % ny, kx]
+    f = TWO_PI / sysm.box
+    return np.stack([_sphere_to_r(1j * (f * k) * rhog / sysm.vol, kx, ky, kz, sysm) for k in (kx, ky, kz)])
+
+
+def gga_blyp(rho_r, sysm):
+    """BLYP gradient correction (``CP_Rho_GSpacePlane::divRhoVksGspace``
+    ``CP_Rho_GSpacePlane.C:278-320``, ``CP_Rho_RealSpacePlane::acceptGradRhoVks``
+    ``CP_Rho_RealSpacePlane.C:1061-1215`` -> ``CP_getGGAFunctional``,
+    ``whiteByrdFFT`` 1237-1300, ``CP_Rho_GSpacePlane::acceptWhiteByrd``
+    330-380, ``CP_Rho_RealSpacePlane::acceptWhiteByrd`` 1314-1350):
+    grad rho(r) from i g rho(g) on the density sphere, the per-point
+    functional, h(g) = FFT(h(r)) / N and the white-byrd correction
+    V -= sum_sphere (i g . h(g)) exp(i g.r).  Returns (V_gga(r), EGGA)."""
+    nx, ny, nz = sysm.nfft
+    n = nx * ny * nz
+    vol = sysm.vol
+    kx, ky, kz, g2 = rho_sphere(sysm)
+    f = TWO_PI / sysm.box
+    gv = (f * kx, f * ky, f * kz)
+    grad = density_gradient(rho_r, sysm)
+    fx, fc, v, h = gga_point(rho_r, grad, sysm.gga_cut)
+    egga = float(np.sum(fx) + np.sum(fc)) * vol / n
+    hg = [_rfftn(h[a] / n)[kz % nz, ky % ny, kx] for a in range(3)]
+    div = 1j * (gv[0] * hg[0] + gv[1] * hg[1] + gv[2] * hg[2])
+    return v - _sphere_to_r(div, kx, ky, kz, sysm), egga
+
+
 def vks_build(psir, sysm):
     """Density -> V_KS(r) = V_xc + V_H + V_loc with the energy terms
     (``CP_Rho_RealSpacePlane::energyComputation`` 739-800, ``HartExtVksG``
-    ``CP_Rho_GHartExt.C:461-510``, ``acceptHartVks`` 1365-1390)."""
+    ``CP_Rho_GHartExt.C:461-510``, ``acceptHartVks`` 1365-1390), and the BLYP
+    gradient correction when the system asks for it (EGGA)."""
     rho = density(psir, sysm)
-    vxc, exc, muxc = pz_lda(rho, sysm.vol, sysm.npts)
+    blyp = getattr(sysm, "xc", "pz_lda") == "blyp"
+    vxc, exc, muxc = pz_lda(rho, sysm.vol, sysm.npts, lyp=blyp)
     vh, ehart, eext, ewald = hart_eext(rho, sysm)
-    return rho, vxc + vh, dict(EEXC=exc, MUXC=muxc, EHART=ehart, EEXT=eext, EWALD_RECIP=ewald)
+    en = dict(EEXC=exc, MUXC=muxc, EHART=ehart, EEXT=eext, EWALD_RECIP=ewald, EGGA=0.0)
+    if blyp:
+        vg, en["EGGA"] = gga_blyp(rho, sysm)
+        vxc = vxc + vg
+    return rho, vxc + vh, en
 
 
 # ----------------------------------------------------------------------------

@@ -127,12 +127,32 @@ extern "C" void ref_eke(int ncoef, const double* psi, double* forces, const int*
 }
 
 // CPXCFNCTS::CP_exc_calc (cp_pz_lda.C:23-175) on an x-padded grid
-// [nf3][nf2][2*(nf1/2+1)]
+// [nf3][nf2][2*(nf1/2+1)]; lyp = 1 drops the PZ correlation (LYP on)
 extern "C" void ref_pz_lda(int nf1, int nf2, int nf3, double* density, double* result, double box, double* exc,
-                           double* muxc) {
+                           double* muxc, int lyp) {
   set_cell(box);
-  readonly_cp.cpopts.cp_lyp = 0;
+  readonly_cp.cpopts.cp_lyp = lyp;
   CPXCFNCTS::CP_exc_calc(nf1 * nf2 * nf3, nf1, nf2, nf3, density, result, exc, muxc, 1);
+  readonly_cp.cpopts.cp_lyp = 0;
+}
+
+// CPXCFNCTS::CP_getGGAFunctional (cp_grad_rho_ctrl.C:32-190) with Becke
+// exchange and LYP correlation (cp_becke.C) on x-padded grids
+// [nf3][nf2][2*(nf1/2+1)]: vks += df/drho, grad rho (gx, gy, gz) replaced by
+// df/d|grad rho| grad rho / |grad rho|, EGGA returned.  The routine keeps
+// its healing length in a function-level static, so one process pins one
+// gga_cut.
+extern "C" double ref_gga(int nf1, int nf2, int nf3, double* density, double* gx, double* gy, double* gz,
+                          double* vks, double box, double gga_cut, int becke, int lyp) {
+  set_cell(box);
+  readonly_cp.cpopts.cp_becke = becke;
+  readonly_cp.cpopts.cp_lyp = lyp;
+  readonly_cp.cppseudo.gga_cut = gga_cut;
+  double e = 0.0;
+  CPXCFNCTS::CP_getGGAFunctional(nf1 * nf2 * nf3, nf1, nf2, nf3, density, gx, gy, gz, vks, 0, &e, 1);
+  readonly_cp.cpopts.cp_becke = 0;
+  readonly_cp.cpopts.cp_lyp = 0;
+  return e;
 }
 
 // CPLOCAL::CP_hart_eext_calc (cp_hart_ext.C:56-431) on a list of density

@@ -159,6 +159,22 @@ def test_ees_atom_forces_are_energy_gradient():
         assert abs(-(es[0] - es[1]) / (2 * h) - fa[a, ax]) < 1e-7 * np.max(np.abs(fa[a]))
 
 
+def test_gga_potential_is_energy_derivative():
+    """The BLYP gradient-correction potential (df/drho minus the white-byrd
+    divergence term) is the functional derivative of EGGA: a central
+    finite difference of EGGA along a density perturbation equals
+    sum_r V_gga(r) drho(r) V/N."""
+    s = make_system("w2", seed=3, xc="blyp")
+    rho = O.density(O.state_g_to_r(s.psi, s), s)
+    v, egga = O.gga_blyp(rho, s)
+    assert egga < 0.0
+    d = np.random.default_rng(7).standard_normal(rho.shape) * 1e-3 * rho
+    e = 1e-3
+    fd = (O.gga_blyp(rho + e * d, s)[1] - O.gga_blyp(rho - e * d, s)[1]) / (2 * e)
+    pred = float(np.sum(v * d)) * s.vol / s.npts
+    assert abs(fd - pred) < 1e-6 * abs(pred)
+
+
 def test_cg_minimisation_beats_steepest_descent():
     """The oracle's minimisation loop (computeMinimization): both methods
     lower the energy; conjugate gradients lower it further and reduce the

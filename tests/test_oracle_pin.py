@@ -37,7 +37,9 @@ def ref():
         pytest.skip("oracle/_ref not built (reference sources absent)")
     lib = C.CDLL(LIB)
     lib.ref_eke.argtypes = [C.c_int, dp, dp, ip, ip, ip, dp, C.c_double, C.c_double, C.c_int, C.c_double, dp]
-    lib.ref_pz_lda.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp, C.c_double, dp, dp]
+    lib.ref_pz_lda.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp, C.c_double, dp, dp, C.c_int]
+    lib.ref_gga.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp, dp, dp, dp, C.c_double, C.c_double, C.c_int, C.c_int]
+    lib.ref_gga.restype = C.c_double
     lib.ref_hart_eext.argtypes = [C.c_int, ip, ip, ip, dp, dp, C.c_int, dp, ip, dp, C.c_int, C.c_int, C.c_double,
                                   C.c_double, dp, dp, C.c_double, C.c_double, C.c_double, dp, dp, dp, dp]
     lib.ref_iter_tmat.argtypes = [dp, dp, C.c_int]
@@ -75,17 +77,18 @@ def test_eke_pinned(ref, sysm):
         assert np.max(np.abs(fr - f_or[st])) <= 1e-12 * np.max(np.abs(f_or[st]))
 
 
-def test_pz_lda_pinned(ref, sysm):
+@pytest.mark.parametrize("lyp", [0, 1])
+def test_pz_lda_pinned(ref, sysm, lyp):
     s = sysm
     nx, ny, nz = s.nfft
     rho = O.density(O.state_g_to_r(s.psi, s), s)
-    v_or, exc_or, muxc_or = O.pz_lda(rho, s.vol, s.npts)
+    v_or, exc_or, muxc_or = O.pz_lda(rho, s.vol, s.npts, lyp=bool(lyp))
     xl = 2 * (nx // 2 + 1)
     pad = np.zeros((nz, ny, xl))
     pad[:, :, :nx] = rho
     res = np.zeros_like(pad)
     exc, muxc = C.c_double(), C.c_double()
-    ref.ref_pz_lda(nx, ny, nz, _d(pad), _d(res), s.box, C.byref(exc), C.byref(muxc))
+    ref.ref_pz_lda(nx, ny, nz, _d(pad), _d(res), s.box, C.byref(exc), C.byref(muxc), lyp)
     assert abs(exc.value - exc_or) <= 1e-12 * abs(exc_or)
     assert abs(muxc.value - muxc_or) <= 1e-12 * abs(muxc_or)
     assert np.max(np.abs(res[:, :, :nx] - v_or)) <= 1e-13 * np.max(np.abs(v_or))
@@ -281,3 +284,37 @@ def test_ees_nonlocal_pinned(ref, sysm, order):
     fpsi = np.zeros((s.nstate, s.ng), dtype=np.complex128)
     ref.ref_ees_psi_forc(s.nstate, _d(np.ascontiguousarray(P).view(np.float64)), _d(fpsi.view(np.float64)))
     assert np.max(np.abs(fpsi - f_or)) <= 1e-12 * np.max(np.abs(f_or))
+
+
+def test_gga_functional_pinned(ref, sysm):
+    """CP_getGGAFunctional with Becke 88 and LYP (cp_grad_rho_ctrl.C,
+    cp_becke.C) on the oracle's density and density gradient, with a dilute
+    region so that the switching function and the rho_cut branch both run:
+    df/drho, the h = df/d|grad rho| unit(grad rho) fields and EGGA against
+    oracle.gga_point."""
+    s = sysm
+    nx, ny, nz = s.nfft
+    rho = O.density(O.state_g_to_r(s.psi, s), s)
+    # scale a slab down into the switching range (rho_cut = 5e-6, full on at ~2e-4)
+    rho = rho.copy()
+    slab = rho[: nz // 3]
+    rho[: nz // 3] = 2e-4 * (slab / slab.max()) ** 4
+    grad = O.density_gradient(rho, s)
+    fx, fc, v_or, h_or = O.gga_point(rho, grad, s.gga_cut)
+    e_or = float(np.sum(fx) + np.sum(fc)) * s.vol / s.npts
+    sw = (rho > 0.1 * s.gga_cut) & (rho < 0.1 * s.gga_cut + 3.9 * s.gga_cut)
+    assert sw.sum() > 100 and (rho <= 0.1 * s.gga_cut).sum() > 100
+    xl = 2 * (nx // 2 + 1)
+
+    def pad(a):
+        p = np.zeros((nz, ny, xl))
+        p[:, :, :nx] = a
+        return p
+
+    dpad, vks = pad(rho), pad(np.zeros_like(rho))
+    g = [pad(grad[a]) for a in range(3)]
+    e = ref.ref_gga(nx, ny, nz, _d(dpad), _d(g[0]), _d(g[1]), _d(g[2]), _d(vks), s.box, s.gga_cut, 1, 1)
+    assert abs(e - e_or) <= 1e-12 * abs(e_or)
+    assert np.max(np.abs(vks[:, :, :nx] - v_or)) <= 1e-12 * np.max(np.abs(v_or))
+    for a in range(3):
+        assert np.max(np.abs(g[a][:, :, :nx] - h_or[a])) <= 1e-12 * np.max(np.abs(h_or))
