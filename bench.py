@@ -51,6 +51,8 @@ def parse():
                     help="systems of the batching form measured beside the headline (0: skip)")
     ap.add_argument("--large", type=int, default=1,
                     help="also time the 128 H2O / 512-state / 160^3 system in the mixed form (0: skip)")
+    ap.add_argument("--blyp", type=int, default=1,
+                    help="also time the 32-water step with the BLYP gradient correction (0: skip)")
     ap.add_argument("--drift-steps", type=int, default=1000,
                     help="steps of the 8-water precision run (energy drift, mixed vs FP64; 0: skip)")
     return ap.parse_args()
@@ -150,6 +152,44 @@ def large_form(torch, args):
     return out
 
 
+def blyp_form(torch, args):
+    """The 32-water workload with the BLYP functional (Becke 88 + LYP
+    gradient correction, its six extra density-grid transforms per step):
+    mixed and FP64 CP steps/s from the same quenched start, the total-energy
+    difference of the two forms, EGGA, and the density path's kernel time
+    with and without the correction."""
+    from openatom_b200.gpu import CPDriver
+    sysm = make_sys(args.config, args.seed)
+    sysm.xc = "blyp"
+    psi0 = quenched_start(sysm, min(args.quench, 12))
+    res = {}
+    ens = {}
+    kt = {}
+    for prec in ("mixed", "fp64"):
+        d = CPDriver(sysm, prec, psi0=psi0, norb_tol=NORB_TOL)
+        st = d.native_state(use_graph=True)
+        d.run_native(st, 3)
+        k = 10
+        ms, en = time_steps(torch, d, st, k)
+        res[prec] = ms
+        ens[prec] = en
+        if prec == "mixed":
+            kt["blyp"] = d.ctx.time_kernels(d.psi, reps=5)["vks_build"]
+            d.ctx.set_xc("pz_lda")
+            kt["pz_lda"] = d.ctx.time_kernels(d.psi, reps=5)["vks_build"]
+        d.ctx.close()
+        del d
+    de = max(abs(total_energy(a) - total_energy(b)) for a, b in zip(ens["mixed"], ens["fp64"])) / sysm.natm
+    torch.cuda.empty_cache()
+    return {"workload": f"{args.config} with BLYP: {sysm.natm // 3} H2O, {sysm.nstate} states, "
+                        f"{sysm.ecut_ry:g} Ry, {sysm.nfft[0]}^3, gradient_cutoff {sysm.gga_cut:g}",
+            "steps": 10, "mixed": {"value": 1e3 / res["mixed"], "ms_per_step": res["mixed"]},
+            "fp64": {"value": 1e3 / res["fp64"], "ms_per_step": res["fp64"]},
+            "mixed_over_fp64": res["fp64"] / res["mixed"], "dE_per_atom_max": de,
+            "egga": ens["fp64"][-1]["EGGA"], "quench_steps": min(args.quench, 12),
+            "density_path_ms": {"blyp": kt["blyp"], "pz_lda": kt["pz_lda"]}}
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
 
@@ -194,7 +234,7 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-TERMS = ("EKE", "EHART", "EEXT", "EEXC", "ENL")
+TERMS = ("EKE", "EHART", "EEXT", "EEXC", "ENL", "EGGA")
 NORB_TOL = 0.003
 
 
@@ -471,6 +511,7 @@ def run_ours(args):
     drift = drift_form(torch, args, rk == 0 and not args.no_cpu) if (rk == 0 and args.drift_steps > 0) else None
     batch = batch_form(torch, args) if (rk == 0 and args.batch > 0) else None
     large = large_form(torch, args) if (rk == 0 and args.large > 0) else None
+    blyp = blyp_form(torch, args) if (rk == 0 and args.blyp > 0) else None
 
     if rk == 0:
         # kernel launches of one mixed step, counted in its captured CUDA graph
@@ -500,6 +541,7 @@ def run_ours(args):
             "drift_1000": drift,
             "batch": batch,
             "large": large,
+            "blyp": blyp,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -293,9 +293,9 @@ typedef struct {
  * synchronisation at the end.  The PsiV reset triggered by max|S - 2I| >
  * norb_tol (Ortho::maxCheck, ortho.C:455-475) is decided on the device and
  * runs at the end of the step, as oa_gpu_psiv_reset would (oa_gpu_psiv_reset_mixed
- * with state->mixed_nterm planes when that is nonzero).  energies_out (optional, host [11]):
+ * with state->mixed_nterm planes when that is nonzero).  energies_out (optional, host [12]):
  * EKE EHART EEXT EWALD_RECIP EEXC MUXC FICT_KE ENL, Newton-Schulz
- * iterations, residual, max|S - 2I|.  Coefficient arrays must be 16-byte
+ * iterations, residual, max|S - 2I|, EGGA (0 under PZ-LDA).  Coefficient arrays must be 16-byte
  * aligned. */
 oa_status oa_gpu_cp_step(oa_ctx *ctx, void *stream, oa_cp_state *state, double *energies_out);
 
@@ -305,7 +305,7 @@ oa_status oa_gpu_cp_step(oa_ctx *ctx, void *stream, oa_cp_state *state, double *
  * InstanceController::printEnergy*, main/InstanceController.C:373-490,
  * becomes one record per step).  pos_host (optional, host
  * [nsteps][natm][3]) is copied to the atom positions before each step.
- * energies_out (optional, host [nsteps][11]) as oa_gpu_cp_step's.  When the
+ * energies_out (optional, host [nsteps][12]) as oa_gpu_cp_step's.  When the
  * Newton-Schulz iteration fails in a step, the call still runs all nsteps
  * and returns OA_ERR_NOT_CONVERGED or OA_ERR_NONFINITE naming the first
  * failing step in oa_gpu_last_error(); the state is then that of the last
@@ -321,7 +321,7 @@ oa_status oa_gpu_cp_run(oa_ctx *ctx, void *stream, oa_cp_state *state, int nstep
  * back.  Results are those of oa_gpu_cp_run on each system alone.  The
  * reference runs such sets as separate instances (UberCollection /
  * InstanceController, main/InstanceController.C).  energies_out (optional,
- * host [nsys][nsteps][11]).  Needs at most 128 states per system (the whole
+ * host [nsys][nsteps][12]).  Needs at most 128 states per system (the whole
  * step captured); a Newton-Schulz failure names the first failing system
  * and step. */
 oa_status oa_gpu_cp_run_batch(oa_ctx **ctxs, oa_cp_state **states, int nsys, void *stream, int nsteps,
@@ -361,8 +361,21 @@ oa_status oa_gpu_ees_init(oa_ctx *ctx, int na, int nb, int nc, int order, const 
 oa_status oa_gpu_nl_ees(oa_ctx *ctx, void *stream, const double *psi, double *fnl_out, double *enl_out);
 
 /* Energies of the last vks_build / vks_apply_fft_bwd (synchronises):
- * out[0..7] = EKE, EHART, EEXT, EWALD_RECIP, EEXC, MUXC, FICT_KE, ENL. */
-oa_status oa_gpu_energies(oa_ctx *ctx, void *stream, double *out8);
+ * out[0..8] = EKE, EHART, EEXT, EWALD_RECIP, EEXC, MUXC, FICT_KE, ENL, EGGA. */
+oa_status oa_gpu_energies(oa_ctx *ctx, void *stream, double *out9);
+
+/* Exchange-correlation functional of the density path (the reference's
+ * \cp_ggax_typ / \cp_ggac_typ and \gradient_cutoff inputs,
+ * interface/sim_params/set_sim_params.C:521-585, 803-808):
+ *   functional 0: Perdew-Zunger LDA (CP_exc_calc, cp_pz_lda.C:23-175), the default;
+ *   functional 1: BLYP = Slater exchange (the PZ correlation off, cp_pz_lda.C:66)
+ *     + the Becke 88 / LYP gradient correction (CP_getGGAFunctional,
+ *     cp_grad_rho_ctrl.C:32-190, becke_gcx_lda / lyp_gcc, cp_becke.C) with its
+ *     grad rho and white-byrd divergence transforms (CP_Rho_GSpacePlane.C:278-380,
+ *     CP_Rho_RealSpacePlane.C:1061-1350); EGGA is reported separately.
+ * gradient_cutoff > 0 (the reference's default is 5e-5).  The first BLYP
+ * call allocates 3 density grids and 3 density z-line sets. */
+oa_status oa_gpu_set_xc(oa_ctx *ctx, int functional, double gradient_cutoff);
 
 #ifdef __cplusplus
 }

@@ -13,6 +13,7 @@ size_t oa_plane_smem_bytes(int precision, int nx, int ny, int nkx);
 int oa_plane_blocks_per_sm(int precision);
 size_t oa_rho_plane_smem_bytes(int nx, int ny, int nkx, int npair, int ychunk);
 int oa_rho_xc_nblk();
+size_t oa_rho_gga_red_off(const oa_ctx* c);
 int oa_rho_z_nblk(const oa_ctx* c);
 cudaError_t oa_launch_pc_fwd(cudaStream_t s, const double* A, const double* B, int n, long K, long kx0_cols,
                              double w_kx0, double alpha, double* part, int nkb, double* C);
@@ -362,7 +363,8 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     TRY(cudaMalloc(&c->vxc, (size_t)c->npts * sizeof(double)));
     TRY(cudaMalloc(&c->vks, (size_t)c->npts * rsz));
     TRY(cudaMalloc(&c->dz, (size_t)d->nz * c->ldl_d * sizeof(double2)));
-    c->red_len = (size_t)3 * oa_rho_xc_nblk() + 3 * (size_t)oa_rho_z_nblk(c) + 64;
+    c->red_len = (size_t)5 * oa_rho_xc_nblk() + 3 * (size_t)oa_rho_z_nblk(c) + 64;  // xc, z pass, GGA partials
+    c->gga_cut = 5.0e-5;
     TRY(cudaMalloc(&c->red, c->red_len * sizeof(double)));
     TRY(cudaMalloc(&c->eke_part, (size_t)d->nstate * c->nblk_z * sizeof(double)));
     p->nkb = 160;  // split-K partials: about one CTA per SM for a 128 x 128 product
@@ -437,7 +439,7 @@ extern "C" oa_status oa_gpu_destroy(oa_ctx* c) {
                  p->partner, p->cmass, p->ke_part, p->dev_e, p->mat_a, p->mat_x, p->eye, p->vtmp, p->upart,
                  p->pl_big[0], p->pl_big[1], p->pl_big[2], p->pl_ma, p->pl_mb,
                  p->err_flag, c->ky, c->kz, c->nl_atm, c->nl_spl, c->nl_vnorm, c->nl_gz0, c->sf, c->zmat, c->zt,
-                 c->enl, c->enl_eke};
+                 c->enl, c->enl_eke, c->grad, c->dzg};
   for (void* q : dev) if (q) cudaFree(q);
   if (p->h_status) cudaFreeHost(p->h_status);
   if (p->h_vals) cudaFreeHost(p->h_vals);
@@ -450,7 +452,7 @@ extern "C" size_t oa_gpu_scratch_bytes(const oa_ctx* c) {
   const size_t rsz = c->precision == OA_FP64 ? 8 : 4;
   const int ng = c->ngroup > c->ngroup_pair ? c->ngroup : c->ngroup_pair;
   return c->zbuf_bytes + (size_t)ng * c->npts * 8 + (size_t)c->npts * (16 + rsz) +
-         (size_t)c->nz * c->ldl_d * 16;
+         (size_t)c->nz * c->ldl_d * 16 + (c->grad ? (size_t)3 * c->npts * 8 + (size_t)3 * c->nz * c->ldl_d * 16 : 0);
 }
 
 extern "C" oa_status oa_gpu_state_fft_fwd(oa_ctx* c, void* stream, const double* psi, double* rho_out) {
@@ -477,16 +479,19 @@ extern "C" oa_status oa_gpu_vks_build(oa_ctx* c, void* stream, double* vks_out) 
   OA_CUDA_TRY(oa_launch_rho_fft_hart(c, s));
   const int nx = oa_rho_xc_nblk(), nzb = oa_rho_z_nblk(c);
   const double vs = c->vol / (double)c->npts;
-  // EEXC = (0.75 ex + ec) V/N ; MUXC = sum vxc rho V/N
+  // EEXC = (0.75 ex + ec) V/N ; MUXC = sum vxc rho V/N; EGGA = (ex + ec of the
+  // gradient correction) V/N, the two halves of each block's partials
   {
-    const double* part[6] = {c->red, c->red, c->red, c->red + 3 * nx, c->red + 3 * nx, c->red + 3 * nx};
-    const int n[6] = {nx, nx, nx, nzb, nzb, nzb};
-    const int stride[6] = {3, 3, 3, 3, 3, 3};
-    const int off[6] = {0, 1, 2, 0, 1, 2};
-    const double scale[6] = {0.75 * vs, vs, vs, 0.5, 1.0, 0.5};
-    double* out[6] = {p->dev_e + 8, p->dev_e + 9, p->dev_e + OA_E_MUXC, p->dev_e + OA_E_EHART,
-                      p->dev_e + OA_E_EEXT, p->dev_e + OA_E_EWALD};
-    OA_CUDA_TRY(oa_launch_sum_partials_multi(s, 6, part, n, stride, off, scale, out));
+    const double* gp = c->red + oa_rho_gga_red_off(c);
+    const double* part[8] = {c->red, c->red, c->red, c->red + 3 * nx, c->red + 3 * nx, c->red + 3 * nx, gp, gp + 1};
+    const int n[8] = {nx, nx, nx, nzb, nzb, nzb, nx, nx};
+    const int stride[8] = {3, 3, 3, 3, 3, 3, 2, 2};
+    const int off[8] = {0, 1, 2, 0, 1, 2, 0, 0};
+    const double scale[8] = {0.75 * vs, vs, vs, 0.5, 1.0, 0.5, vs, vs};
+    double* out[8] = {p->dev_e + 8, p->dev_e + 9, p->dev_e + OA_E_MUXC, p->dev_e + OA_E_EHART,
+                      p->dev_e + OA_E_EEXT, p->dev_e + OA_E_EWALD, p->dev_e + 11, p->dev_e + 12};
+    OA_CUDA_TRY(oa_launch_sum_partials_multi(s, c->gga ? 8 : 6, part, n, stride, off, scale, out));
+    if (!c->gga) OA_CUDA_TRY(cudaMemsetAsync(p->dev_e + 11, 0, 2 * sizeof(double), s));
   }
   if (vks_out) {
     if (c->precision == OA_FP64)
@@ -690,8 +695,9 @@ extern "C" oa_status oa_gpu_integrate(oa_ctx* c, void* stream, const double* for
 }
 
 __global__ void k_energy_combine(double* e) {
-  // EEXC = 0.75 ex V/N + ec V/N was stored split at [8] and [9]
+  // EEXC = 0.75 ex V/N + ec V/N was stored split at [8] and [9], EGGA at [11] and [12]
   e[OA_E_EEXC] = e[8] + e[9];
+  e[OA_E_EGGA] = e[11] + e[12];
 }
 
 extern "C" oa_status oa_gpu_energies(oa_ctx* c, void* stream, double* out7) {
@@ -710,6 +716,27 @@ extern "C" oa_status oa_gpu_energies(oa_ctx* c, void* stream, double* out7) {
   out7[5] = p->h_vals[OA_E_MUXC];
   out7[6] = p->h_vals[OA_E_FICT];
   out7[7] = p->h_vals[OA_E_ENL];
+  out7[8] = p->h_vals[OA_E_EGGA];
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_set_xc(oa_ctx* c, int functional, double gradient_cutoff) {
+  OA_ARG_CHECK(c, "null argument");
+  if (functional != 0 && functional != 1) {
+    oa_set_error("functional must be 0 (PZ-LDA) or 1 (BLYP)", __FILE__, __LINE__);
+    return OA_ERR_BAD_ARG;
+  }
+  if (!(gradient_cutoff > 0.0)) {
+    oa_set_error("gradient_cutoff must be > 0", __FILE__, __LINE__);
+    return OA_ERR_BAD_ARG;
+  }
+  if (functional == 1 && !c->grad) {
+    OA_CUDA_TRY(cudaMalloc(&c->grad, (size_t)3 * c->npts * sizeof(double)));
+    OA_CUDA_TRY(cudaMalloc(&c->dzg, (size_t)3 * c->nz * c->ldl_d * sizeof(double2)));
+  }
+  c->gga = functional;
+  c->gga_cut = gradient_cutoff;
+  c->xc_gen += 1;
   return OA_OK;
 }
 

@@ -104,9 +104,17 @@ struct oa_ctx {
   OaPlaneOut zb_po;       // bf16 planes the next force z pass also writes (mixed native step), P = nullptr: none
   int zb_po_done;         // the last force z pass wrote them
   int npair_d, ychunk_d;
+  // exchange-correlation: gga = 0 Perdew-Zunger LDA, 1 BLYP (Slater
+  // exchange + Becke 88 + LYP, oa_gpu_set_xc); gga_cut = \gradient_cutoff
+  int gga;
+  double gga_cut;
+  unsigned xc_gen;        // bumped by every oa_gpu_set_xc (captured step graphs key on it)
+  double *grad;           // [3][nz][ny][nx] grad rho, then the GGA vector h (BLYP)
+  void *dzg;              // [3][nz][ldl_d] C  z-lines of grad rho / h (BLYP)
 };
 
 enum { OA_E_EKE = 0, OA_E_EHART, OA_E_EEXT, OA_E_EWALD, OA_E_EEXC, OA_E_MUXC, OA_E_ENL, OA_E_FICT };
+#define OA_E_EGGA 10      // device energy slot of EGGA (slots 8, 9 hold the EEXC halves)
 cudaError_t oa_launch_phase_tables(oa_ctx* c, cudaStream_t s);
 
 #define OA_CUDA_TRY(x)                                  \

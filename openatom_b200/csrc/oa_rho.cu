@@ -48,8 +48,9 @@ __host__ __device__ static inline size_t align_up_r(size_t x, size_t a) { return
 // density sum + PZ-LDA
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(OA_NTHREADS)
-k_rho_xc(const double* __restrict__ rho_part, int ngroup, size_t npts, double rvol,
+k_rho_xc(const double* __restrict__ rho_part, int ngroup, size_t npts, double rvol, double cfac,
          double* __restrict__ rho, double* __restrict__ vxc, double* __restrict__ part) {
+  // cfac = 0 drops the PZ correlation (LYP correlation on, cp_pz_lda.C:66)
   __shared__ double sh[3 * 32];
   // Perdew-Zunger constants (cp_pz_lda.C:46-52)
   const double gamma = -0.14230, beta1 = 1.05290, beta2 = 0.33340;
@@ -78,6 +79,8 @@ k_rho_xc(const double* __restrict__ rho_part, int ngroup, size_t npts, double rv
       cfact = au * lnrs + bu + cu * rs * lnrs + du * rs;
       mufact = au * lnrs + (bu - power * au) + 2.0 * power * cu * rs * lnrs + power * (2.0 * du - cu) * rs;
     }
+    cfact *= cfac;
+    mufact *= cfac;
     acc[0] += xfact * r;
     acc[1] += cfact * r;
     const double v = xfact + mufact;
@@ -129,7 +132,8 @@ static RhoPlaneSmem rho_plane_layout(int nx, int ny, int nkx, int npair, int ych
 __global__ void __launch_bounds__(OA_NTHREADS)
 k_rho_plane_fwd(const double* __restrict__ rho, double scale, int nx, int ny, int nz, int nkx,
                 OaFftPlan px, OaFftPlan py, const double2* __restrict__ twx, const double2* __restrict__ twy,
-                double2* __restrict__ dz, int ldl_d, int npair, int ychunk, RhoPlaneSmem L) {
+                double2* __restrict__ dz, int ldl_d, int npair, int ychunk, RhoPlaneSmem L, size_t fin,
+                size_t fout) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* stwx = (double2*)(smem_raw + L.tw_x);
   double2* stwy = (double2*)(smem_raw + L.tw_y);
@@ -139,6 +143,8 @@ k_rho_plane_fwd(const double* __restrict__ rho, double scale, int nx, int ny, in
   const int ldx = nx + 1, ldy = ny + 1;
   const int z = blockIdx.x;
   const int npairs = (ny + 1) / 2;
+  rho += blockIdx.y * fin;
+  dz += blockIdx.y * fout;
   load_twiddles(stwx, twx, nx);
   load_twiddles(stwy, twy, ny);
   const double* rz = rho + (size_t)z * nx * ny;
@@ -178,7 +184,8 @@ template <typename R>
 __global__ void __launch_bounds__(OA_NTHREADS)
 k_rho_plane_bwd(const double2* __restrict__ dz, int ldl_d, int nx, int ny, int nz, int nkx,
                 OaFftPlan px, OaFftPlan py, const double2* __restrict__ twx, const double2* __restrict__ twy,
-                const double* __restrict__ vxc, R* __restrict__ vks, int npair, int ychunk, RhoPlaneSmem L) {
+                const double* __restrict__ vxc, R* __restrict__ vks, int npair, int ychunk, RhoPlaneSmem L,
+                size_t fin, size_t fout) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* stwx = (double2*)(smem_raw + L.tw_x);
   double2* stwy = (double2*)(smem_raw + L.tw_y);
@@ -188,6 +195,8 @@ k_rho_plane_bwd(const double2* __restrict__ dz, int ldl_d, int nx, int ny, int n
   const int ldx = nx + 1, ldy = ny + 1;
   const int z = blockIdx.x;
   const int npairs = (ny + 1) / 2;
+  dz += blockIdx.y * fin;
+  vks += blockIdx.y * fout;
   load_twiddles(stwx, twx, nx);
   load_twiddles(stwy, twy, ny);
   const double2* in = dz + (size_t)z * ldl_d;
@@ -200,7 +209,7 @@ k_rho_plane_bwd(const double2* __restrict__ dz, int ldl_d, int nx, int ny, int n
     const int nb = min(ychunk, nkx - c0);
     fft_inout<+1>(P + c0 * ldy, ldy, P + c0 * ldy, ldy, W1, W2, ldy, nb, py, stwy);
   }
-  const double* vz = vxc + (size_t)z * nx * ny;
+  const double* vz = vxc ? vxc + (size_t)z * nx * ny : nullptr;  // null: vks = V
   R* oz = vks + (size_t)z * nx * ny;
   for (int p0 = 0; p0 < npairs; p0 += npair) {
     const int np = min(npair, npairs - p0);
@@ -218,8 +227,8 @@ k_rho_plane_bwd(const double2* __restrict__ dz, int ldl_d, int nx, int ny, int n
       const int p = idx / nx, x = idx - p * nx;
       const int y1 = 2 * (p0 + p), y2 = y1 + 1;
       const double2 v = r[p * ldx + x];
-      oz[y1 * nx + x] = (R)(v.x + vz[y1 * nx + x]);
-      if (y2 < ny) oz[y2 * nx + x] = (R)(v.y + vz[y2 * nx + x]);
+      oz[y1 * nx + x] = (R)(v.x + (vz ? vz[y1 * nx + x] : 0.0));
+      if (y2 < ny) oz[y2 * nx + x] = (R)(v.y + (vz ? vz[y2 * nx + x] : 0.0));
     }
     __syncthreads();
   }
@@ -427,10 +436,247 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
   }
 }
 
+// ---------------------------------------------------------------------------
+// BLYP gradient correction (cp_grad_rho_ctrl.C, cp_becke.C; the driver's
+// divRhoVksGspace / acceptGradRhoVks / whiteByrdFFT / acceptWhiteByrd,
+// CP_Rho_GSpacePlane.C:278-380, CP_Rho_RealSpacePlane.C:1061-1350):
+//   k_rho_grad_z   rho(g) -> i g_a rho(g) / V on the density sphere, z^-1
+//   (x-y inverse)  -> grad rho(r), three fields
+//   k_rho_gga      per point: EGGA density, vxc += df/drho,
+//                  h = df/d|grad rho| grad rho / |grad rho|
+//   (x-y forward of h / N)
+//   k_rho_div_z    z forward of h, i g . h(g) on the sphere, z^-1, and
+//                  subtracted from the V_KS z-lines before their x-y inverse
+// ---------------------------------------------------------------------------
+struct GgaTerm { double f, dfr, dfg; };
+
+// Becke 88 correction to the LDA exchange, spin-unpolarised (becke_gcx_lda,
+// cp_becke.C:21-88): per spin rho_s = rho / 2, x = (g / 2) / rho_s^(4/3),
+// b = x^2 / (1 + 6 beta x asinh x), f = -2 beta rho_s^(4/3) b;
+// df/drho = -(4/3) beta rho_s^(1/3) (b - x b'), df/dg = -beta b'.
+__device__ __forceinline__ GgaTerm gga_becke88(double rho, double g) {
+  const double beta = 0.0042;
+  const double rs = 0.5 * rho;
+  const double r13 = cbrt(rs);
+  const double r43 = rs * r13;
+  const double x = 0.5 * g / r43;
+  const double root = sqrt(1.0 + x * x);
+  const double ash = log(x + root);
+  const double den = 1.0 + 6.0 * beta * x * ash;
+  const double b = x * x / den;
+  const double q = x / den;
+  const double bp = 2.0 * q - 6.0 * beta * q * q * (ash + x / root);
+  GgaTerm t;
+  t.f = -2.0 * beta * r43 * b;
+  t.dfr = -beta * (4.0 / 3.0) * r13 * (b - x * bp);
+  t.dfg = -beta * bp;
+  return t;
+}
+
+// Lee-Yang-Parr correlation, closed shell (lyp_gcc, cp_becke.C:91-172):
+// u = rho^(-1/3), D = 1 + d u, omega = exp(-c u) u^11 / D,
+// delta = c u + d u / D, A = C_F rho^(8/3) + (5/12 - 7 delta / 72) g^2 - 11 g^2 / 24,
+// f = -a rho / D - a b omega A rho^2.
+__device__ __forceinline__ GgaTerm gga_lyp(double rho, double g) {
+  const double a = 0.049180, b = 0.1320, c = 0.25330, d = 0.3490;
+  const double cf = 2.871234000188191;  // C_F = 0.3 (3 pi^2)^(2/3)
+  const double u = 1.0 / cbrt(rho);
+  const double u2 = u * u;
+  const double den = 1.0 + d * u;
+  double u11 = u2 * u2;            // u^4
+  u11 = u11 * u11 * u2 * u;        // u^11
+  const double om = exp(-c * u) * u11 / den;
+  const double dl = c * u + d * u / den;
+  const double g2 = g * g;
+  const double r2 = rho * rho;
+  const double r23i = u2;          // rho^(-2/3)
+  const double cq = 5.0 / 12.0 - 7.0 * dl / 72.0;
+  const double A = cf * r2 / r23i + cq * g2 - 11.0 * g2 / 24.0;  // C_F rho^(8/3) = C_F rho^2 / rho^(-2/3)
+  const double dom = om * (c * u + d * u / den - 11.0) / (3.0 * rho);
+  const double ddl = -(u / (3.0 * rho)) * (c + d / (den * den));
+  const double dA = (8.0 / 3.0) * cf * rho / r23i - (7.0 / 72.0) * ddl * g2;  // d/drho, rho^(5/3) = rho / rho^(-2/3)
+  GgaTerm t;
+  t.f = -a * rho / den - a * b * om * A * r2;
+  t.dfr = -a * (1.0 + (4.0 / 3.0) * d * u) / (den * den) - a * b * (dom * A * r2 + om * (dA * r2 + 2.0 * A * rho));
+  t.dfg = -a * b * om * r2 * 2.0 * g * (cq - 11.0 / 24.0);
+  return t;
+}
+
+// Per point, on rho > rho_cut = gga_cut / 10 (CP_getGGAFunctional): Becke +
+// LYP times the switching function s = t^2 (3 - 2 t), t = clamp((rho -
+// rho_cut) / (3.9 gga_cut), 0, 1); vxc += d(s f)/drho; grad <- h; block
+// partials of the exchange and correlation parts.  h is 0 where
+// |grad rho| = 0 (no direction) and below rho_cut.
+__global__ void __launch_bounds__(OA_NTHREADS)
+k_rho_gga(const double* __restrict__ rho, double* __restrict__ grad, size_t npts, double gga_cut,
+          double* __restrict__ vxc, double* __restrict__ part) {
+  __shared__ double sh[2 * 32];
+  const double rho_cut = 0.1 * gga_cut, heal = 1.0 / (3.9 * gga_cut);
+  double acc[2] = {0.0, 0.0};
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += (size_t)gridDim.x * blockDim.x) {
+    const double r = rho[i];
+    double hx = 0.0, hy = 0.0, hz = 0.0;
+    if (r > rho_cut) {
+      const double gx = grad[i], gy = grad[npts + i], gz = grad[2 * npts + i];
+      const double g2 = gx * gx + gy * gy + gz * gz;
+      const double g = sqrt(g2);
+      const double t = fmin(fmax((r - rho_cut) * heal, 0.0), 1.0);
+      const double sw = t * t * (3.0 - 2.0 * t);
+      const double dsw = 6.0 * t * (1.0 - t) * heal;
+      const GgaTerm x = gga_becke88(r, g), c = gga_lyp(r, g);
+      vxc[i] += (x.dfr + c.dfr) * sw + (x.f + c.f) * dsw;
+      acc[0] += x.f * sw;
+      acc[1] += c.f * sw;
+      if (g2 > 0.0) {
+        const double k = (x.dfg + c.dfg) * sw / g;
+        hx = gx * k; hy = gy * k; hz = gz * k;
+      }
+    }
+    grad[i] = hx;
+    grad[npts + i] = hy;
+    grad[2 * npts + i] = hz;
+  }
+  block_sum_n<2>(acc, sh);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x + 0] = acc[0];
+    part[2 * blockIdx.x + 1] = acc[1];
+  }
+}
+
+// g-vector of element (line lb, plane zz) of a z-pass block and whether it
+// is inside the density sphere (the points k_rho_zpass keeps, g = 0 out)
+__device__ __forceinline__ bool rho_sphere_g(int l, int zz, int ny, int nz, double tpi_l, double ecut4, int ktab,
+                                             double* gx, double* gy, double* gz) {
+  const int kx = l / ny;
+  int ky = l - kx * ny; if (2 * ky >= ny) ky -= ny;
+  int kz = zz; if (2 * kz >= nz) kz -= nz;
+  *gx = tpi_l * kx; *gy = tpi_l * ky; *gz = tpi_l * kz;
+  const double g2 = *gx * *gx + *gy * *gy + *gz * *gz;
+  return g2 != 0.0 && g2 <= ecut4 && abs(kx) <= ktab && abs(ky) <= ktab && abs(kz) <= ktab;
+}
+
+// z transform of nb lines in x (ld ldz) with y as scratch; returns the
+// buffer holding the result
+template <int N1, int N2, int SIGN>
+__device__ __forceinline__ double2* zfft_any(double2* x, double2* y, int ldz, int nb, const OaFftPlan& pz,
+                                             const double2* tw) {
+  if constexpr (N1 > 0) {
+    zfft2<N1, N2, SIGN>(x, y, ldz, nb, tw);
+    return x;
+  } else {
+    return fft_pingpong<SIGN>(x, y, ldz, nb, pz, tw);
+  }
+}
+
+// three buffers of OA_LB lines (row stride ldz, each sized for the
+// two-pass scratch layout) after the twiddles
+template <int N1, int N2>
+__host__ __device__ inline int gga_zbuf_ld(int nz) {
+  if constexpr (N1 > 0) {
+    const int ps = ZLd<N1, N2>::PS;
+    return ps > nz + 1 ? ps : nz + 1;
+  } else {
+    return nz + 1;
+  }
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(OA_NTHREADS, 2)
+k_rho_grad_z(const double2* __restrict__ dz, double2* __restrict__ dzg, size_t fstride, int ldl_d, int nlines_d,
+             int ny, int nz, OaFftPlan pz, const double2* __restrict__ twz, double tpi_l, double ecut4, int ktab,
+             double rvol) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ldz = nz + 1, lb_sz = OA_LB * gga_zbuf_ld<N1, N2>(nz);
+  double2* tw = (double2*)smem_raw;
+  double2* bufs[3];
+  bufs[0] = tw + align_up_r(nz, 2);
+  bufs[1] = bufs[0] + lb_sz;
+  bufs[2] = bufs[1] + lb_sz;
+  const int l0 = blockIdx.x * OA_LB;
+  const int nb = min(OA_LB, nlines_d - l0);
+  load_twiddles(tw, twz, nz);
+  for (int idx = threadIdx.x; idx < nz * OA_LB; idx += blockDim.x) {
+    const int zz = idx / OA_LB, lb = idx - zz * OA_LB;
+    if (lb < nb) bufs[0][lb * ldz + zz] = dz[(size_t)zz * ldl_d + l0 + lb];
+  }
+  __syncthreads();
+  double2* r = zfft_any<N1, N2, -1>(bufs[0], bufs[1], ldz, nb, pz, tw);
+  __syncthreads();
+  double2* x = (r == bufs[0]) ? bufs[1] : bufs[0];
+  double2* y = bufs[2];
+  for (int a = 0; a < 3; ++a) {
+    for (int idx = threadIdx.x; idx < nb * nz; idx += blockDim.x) {
+      const int lb = idx / nz, zz = idx - lb * nz;
+      double gx, gy, gz;
+      const bool in = rho_sphere_g(l0 + lb, zz, ny, nz, tpi_l, ecut4, ktab, &gx, &gy, &gz);
+      const double2 v = r[lb * ldz + zz];
+      const double f = in ? (a == 0 ? gx : (a == 1 ? gy : gz)) * rvol : 0.0;
+      x[lb * ldz + zz] = make_double2(-v.y * f, v.x * f);  // i g_a rho(g) / V
+    }
+    __syncthreads();
+    double2* q = zfft_any<N1, N2, +1>(x, y, ldz, nb, pz, tw);
+    __syncthreads();
+    double2* out = dzg + a * fstride;
+    for (int idx = threadIdx.x; idx < nz * OA_LB; idx += blockDim.x) {
+      const int zz = idx / OA_LB, lb = idx - zz * OA_LB;
+      if (lb < nb) out[(size_t)zz * ldl_d + l0 + lb] = q[lb * ldz + zz];
+    }
+    __syncthreads();
+  }
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(OA_NTHREADS, 2)
+k_rho_div_z(double2* __restrict__ dz, const double2* __restrict__ dzh, size_t fstride, int ldl_d, int nlines_d,
+            int ny, int nz, OaFftPlan pz, const double2* __restrict__ twz, double tpi_l, double ecut4, int ktab) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ldz = nz + 1, lb_sz = OA_LB * gga_zbuf_ld<N1, N2>(nz);
+  double2* tw = (double2*)smem_raw;
+  double2* a0 = tw + align_up_r(nz, 2);
+  double2* a1 = a0 + lb_sz;
+  double2* acc = a1 + lb_sz;
+  const int l0 = blockIdx.x * OA_LB;
+  const int nb = min(OA_LB, nlines_d - l0);
+  load_twiddles(tw, twz, nz);
+  for (int idx = threadIdx.x; idx < OA_LB * ldz; idx += blockDim.x) acc[idx] = make_double2(0.0, 0.0);
+  for (int a = 0; a < 3; ++a) {
+    const double2* in = dzh + a * fstride;
+    for (int idx = threadIdx.x; idx < nz * OA_LB; idx += blockDim.x) {
+      const int zz = idx / OA_LB, lb = idx - zz * OA_LB;
+      if (lb < nb) a0[lb * ldz + zz] = in[(size_t)zz * ldl_d + l0 + lb];
+    }
+    __syncthreads();
+    const double2* r = zfft_any<N1, N2, -1>(a0, a1, ldz, nb, pz, tw);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nb * nz; idx += blockDim.x) {
+      const int lb = idx / nz, zz = idx - lb * nz;
+      double gx, gy, gz;
+      if (rho_sphere_g(l0 + lb, zz, ny, nz, tpi_l, ecut4, ktab, &gx, &gy, &gz)) {
+        const double ga = a == 0 ? gx : (a == 1 ? gy : gz);
+        const double2 v = r[lb * ldz + zz];
+        acc[lb * ldz + zz].x -= v.y * ga;  // += i g_a h_a(g)
+        acc[lb * ldz + zz].y += v.x * ga;
+      }
+    }
+    __syncthreads();
+  }
+  const double2* q = zfft_any<N1, N2, +1>(acc, a0, ldz, nb, pz, tw);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < nz * OA_LB; idx += blockDim.x) {
+    const int zz = idx / OA_LB, lb = idx - zz * OA_LB;
+    if (lb < nb) {
+      double2& o = dz[(size_t)zz * ldl_d + l0 + lb];
+      const double2 w = q[lb * ldz + zz];
+      o.x -= w.x;
+      o.y -= w.y;
+    }
+  }
+}
+
 cudaError_t oa_rho2_fwd(cudaStream_t s, int n, int nz, const double* rho, double scale, const double2* tw,
-                        double2* dz, int ldl_d);
+                        double2* dz, int ldl_d, int nf, size_t fin, size_t fout);
 cudaError_t oa_rho2_bwd(cudaStream_t s, int n, int nz, const double2* dz, int ldl_d, const double2* tw,
-                        const double* vxc, void* vks, int fp64);
+                        const double* vxc, void* vks, int fp64, int nf, size_t fin, size_t fout);
 
 __global__ void k_phase_tables(const double* __restrict__ pos, int natm, int ktab, double tpi_l, double2* __restrict__ phase) {
   const int nt = 2 * ktab + 1;
@@ -452,12 +698,15 @@ size_t oa_rho_plane_smem_bytes(int nx, int ny, int nkx, int npair, int ychunk) {
 
 cudaError_t oa_launch_rho_xc(oa_ctx* c, cudaStream_t s) {
   const int nblk = 4 * 148;
-  k_rho_xc<<<nblk, OA_NTHREADS, 0, s>>>(c->rho_part, c->rho_ngroup, (size_t)c->npts, 1.0 / c->vol, c->rho, c->vxc, c->red);
+  k_rho_xc<<<nblk, OA_NTHREADS, 0, s>>>(c->rho_part, c->rho_ngroup, (size_t)c->npts, 1.0 / c->vol,
+                                        c->gga ? 0.0 : 1.0, c->rho, c->vxc, c->red);
   return cudaGetLastError();
 }
 
 int oa_rho_xc_nblk() { return 4 * 148; }
 int oa_rho_z_nblk(const oa_ctx* c) { return (c->nlines_d + OA_LB - 1) / OA_LB; }
+// offset of the GGA block partials (2 per block of k_rho_gga) in c->red
+size_t oa_rho_gga_red_off(const oa_ctx* c) { return (size_t)3 * oa_rho_xc_nblk() + 3 * (size_t)oa_rho_z_nblk(c); }
 
 cudaError_t oa_launch_phase_tables(oa_ctx* c, cudaStream_t s) {
   const double tpi_l = 2.0 * 3.14159265358979323846 / c->box;
@@ -466,24 +715,102 @@ cudaError_t oa_launch_phase_tables(oa_ctx* c, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// x-y forward transform of nf real fields (stride fin doubles) into density
+// z-lines (stride fout double2), two-pass kernels where the length has them
+static cudaError_t rho_xy_fwd(oa_ctx* c, cudaStream_t s, const double* src, double scale, double2* dst, int nf,
+                              size_t fin, size_t fout) {
+  cudaError_t e = c->nx == c->ny ? oa_rho2_fwd(s, c->nx, c->nz, src, scale, c->tw_x, dst, c->ldl_d, nf, fin, fout)
+                                 : cudaErrorNotSupported;
+  if (e != cudaErrorNotSupported) return e;
+  RhoPlaneSmem L = rho_plane_layout(c->nx, c->ny, c->nkx_d, c->npair_d, c->ychunk_d);
+  e = oa_smem_limit(k_rho_plane_fwd);
+  if (e != cudaSuccess) return e;
+  k_rho_plane_fwd<<<dim3(c->nz, nf), OA_NTHREADS, L.total, s>>>(src, scale, c->nx, c->ny, c->nz, c->nkx_d,
+                                                                 c->plan_x, c->plan_y, c->tw_x, c->tw_y, dst,
+                                                                 c->ldl_d, c->npair_d, c->ychunk_d, L, fin, fout);
+  return cudaGetLastError();
+}
+
+// x-y inverse of nf fields of density z-lines into real grids (+ vxc when
+// not null), in FP64 or the compute precision
+static cudaError_t rho_xy_bwd(oa_ctx* c, cudaStream_t s, const double2* src, const double* vxc, void* dst, int fp64,
+                              int nf, size_t fin, size_t fout) {
+  cudaError_t e = c->nx == c->ny
+                      ? oa_rho2_bwd(s, c->nx, c->nz, src, c->ldl_d, c->tw_x, vxc, dst, fp64, nf, fin, fout)
+                      : cudaErrorNotSupported;
+  if (e != cudaErrorNotSupported) return e;
+  RhoPlaneSmem L = rho_plane_layout(c->nx, c->ny, c->nkx_d, c->npair_d, c->ychunk_d);
+  const dim3 grid(c->nz, nf);
+  if (fp64) {
+    e = oa_smem_limit(k_rho_plane_bwd<double>);
+    if (e != cudaSuccess) return e;
+    k_rho_plane_bwd<double><<<grid, OA_NTHREADS, L.total, s>>>(src, c->ldl_d, c->nx, c->ny, c->nz, c->nkx_d,
+                                                               c->plan_x, c->plan_y, c->tw_x, c->tw_y, vxc,
+                                                               (double*)dst, c->npair_d, c->ychunk_d, L, fin, fout);
+  } else {
+    e = oa_smem_limit(k_rho_plane_bwd<float>);
+    if (e != cudaSuccess) return e;
+    k_rho_plane_bwd<float><<<grid, OA_NTHREADS, L.total, s>>>(src, c->ldl_d, c->nx, c->ny, c->nz, c->nkx_d,
+                                                              c->plan_x, c->plan_y, c->tw_x, c->tw_y, vxc,
+                                                              (float*)dst, c->npair_d, c->ychunk_d, L, fin, fout);
+  }
+  return cudaGetLastError();
+}
+
+// the two GGA z kernels, two-pass where nz has a factorisation
+static cudaError_t gga_z(oa_ctx* c, cudaStream_t s, int div) {
+  const double tpi_l = 2.0 * 3.14159265358979323846 / c->box;
+  const size_t fst = (size_t)c->nz * c->ldl_d;
+  const int nbz = oa_rho_z_nblk(c);
+  auto go = [&](auto grad_k, auto div_k, int ld) -> cudaError_t {
+    const size_t sm = (align_up_r(c->nz, 2) + (size_t)3 * OA_LB * ld) * sizeof(double2);
+    if (sm > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
+    cudaError_t e2;
+    if (div) {
+      if ((e2 = oa_smem_limit(div_k)) != cudaSuccess) return e2;
+      div_k<<<nbz, OA_NTHREADS, sm, s>>>((double2*)c->dz, (const double2*)c->dzg, fst, c->ldl_d, c->nlines_d, c->ny,
+                                         c->nz, c->plan_z, c->tw_z, tpi_l, c->ecut_rho, c->kmax_tab);
+    } else {
+      if ((e2 = oa_smem_limit(grad_k)) != cudaSuccess) return e2;
+      grad_k<<<nbz, OA_NTHREADS, sm, s>>>((const double2*)c->dz, (double2*)c->dzg, fst, c->ldl_d, c->nlines_d,
+                                          c->ny, c->nz, c->plan_z, c->tw_z, tpi_l, c->ecut_rho, c->kmax_tab,
+                                          1.0 / c->vol);
+    }
+    return cudaGetLastError();
+  };
+  cudaError_t e;
+  switch (c->nz) {
+#define OA_GZ(NN, A, B) \
+  case NN: e = go(k_rho_grad_z<A, B>, k_rho_div_z<A, B>, gga_zbuf_ld<A, B>(c->nz)); break;
+    OA_GZ(12, 4, 3) OA_GZ(20, 4, 5) OA_GZ(24, 6, 4) OA_GZ(36, 6, 6) OA_GZ(40, 8, 5) OA_GZ(64, 8, 8)
+    OA_GZ(96, 12, 8) OA_GZ(108, 12, 9) OA_GZ(160, 16, 10)
+#undef OA_GZ
+    default: e = cudaErrorNotSupported; break;
+  }
+  if (e == cudaErrorNotSupported) e = go(k_rho_grad_z<0, 0>, k_rho_div_z<0, 0>, c->nz + 1);
+  return e;
+}
+
+// BLYP before the Hartree z pass: grad rho, the per-point functional
+// (vxc, EGGA partials, h), and h's x-y forward transform into dzg
+static cudaError_t gga_front(oa_ctx* c, cudaStream_t s) {
+  const size_t fz = (size_t)c->nz * c->ldl_d, fr = (size_t)c->npts;
+  cudaError_t e;
+  if ((e = gga_z(c, s, 0)) != cudaSuccess) return e;
+  if ((e = rho_xy_bwd(c, s, (const double2*)c->dzg, nullptr, c->grad, 1, 3, fz, fr)) != cudaSuccess) return e;
+  k_rho_gga<<<oa_rho_xc_nblk(), OA_NTHREADS, 0, s>>>(c->rho, c->grad, fr, c->gga_cut, c->vxc,
+                                                      c->red + oa_rho_gga_red_off(c));
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return rho_xy_fwd(c, s, c->grad, 1.0 / c->npts, (double2*)c->dzg, 3, fr, fz);
+}
+
 cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
   const double tpi_l = 2.0 * 3.14159265358979323846 / c->box;
   cudaError_t e;
   // phase tables exp(i 2 pi k x / L)
   if ((e = oa_launch_phase_tables(c, s)) != cudaSuccess) return e;
-  RhoPlaneSmem L = rho_plane_layout(c->nx, c->ny, c->nkx_d, c->npair_d, c->ychunk_d);
-  const bool two_pass = c->nx == c->ny;
-  e = two_pass ? oa_rho2_fwd(s, c->nx, c->nz, c->rho, c->vol / c->npts, c->tw_x, (double2*)c->dz, c->ldl_d)
-               : cudaErrorNotSupported;
-  if (e == cudaErrorNotSupported) {
-    e = oa_smem_limit(k_rho_plane_fwd);
-    if (e != cudaSuccess) return e;
-    k_rho_plane_fwd<<<c->nz, OA_NTHREADS, L.total, s>>>(c->rho, c->vol / c->npts, c->nx, c->ny, c->nz, c->nkx_d,
-                                                         c->plan_x, c->plan_y, c->tw_x, c->tw_y,
-                                                         (double2*)c->dz, c->ldl_d, c->npair_d, c->ychunk_d, L);
-    e = cudaGetLastError();
-  }
-  if (e != cudaSuccess) return e;
+  if ((e = rho_xy_fwd(c, s, c->rho, c->vol / c->npts, (double2*)c->dz, 1, 0, 0)) != cudaSuccess) return e;
+  if (c->gga && (e = gga_front(c, s)) != cudaSuccess) return e;
   RhoTypeOff toff;
   for (int t = 0; t < 5; ++t) toff.off[t] = c->type_off[t];
   const int nbz = oa_rho_z_nblk(c);
@@ -513,23 +840,7 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
   }
   if (e == cudaErrorNotSupported) e = zpass(k_rho_zpass<0, 0>, c->nz + 1);
   if (e != cudaSuccess) return e;
-  if (two_pass) {
-    e = oa_rho2_bwd(s, c->nx, c->nz, (const double2*)c->dz, c->ldl_d, c->tw_x, c->vxc, c->vks,
-                    c->precision == OA_FP64);
-    if (e != cudaErrorNotSupported) return e;
-  }
-  if (c->precision == OA_FP64) {
-    e = oa_smem_limit(k_rho_plane_bwd<double>);
-    if (e != cudaSuccess) return e;
-    k_rho_plane_bwd<double><<<c->nz, OA_NTHREADS, L.total, s>>>((const double2*)c->dz, c->ldl_d, c->nx, c->ny, c->nz,
-                                                                c->nkx_d, c->plan_x, c->plan_y, c->tw_x, c->tw_y,
-                                                                c->vxc, (double*)c->vks, c->npair_d, c->ychunk_d, L);
-  } else {
-    e = oa_smem_limit(k_rho_plane_bwd<float>);
-    if (e != cudaSuccess) return e;
-    k_rho_plane_bwd<float><<<c->nz, OA_NTHREADS, L.total, s>>>((const double2*)c->dz, c->ldl_d, c->nx, c->ny, c->nz,
-                                                               c->nkx_d, c->plan_x, c->plan_y, c->tw_x, c->tw_y,
-                                                               c->vxc, (float*)c->vks, c->npair_d, c->ychunk_d, L);
-  }
-  return cudaGetLastError();
+  // white-byrd: V_KS z-lines -= z^-1 (i g . h(g))
+  if (c->gga && (e = gga_z(c, s, 1)) != cudaSuccess) return e;
+  return rho_xy_bwd(c, s, (const double2*)c->dz, c->vxc, c->vks, c->precision == OA_FP64, 1, 0, 0);
 }

@@ -10,6 +10,8 @@
 //             -> y pass B -> dz[z][kx ny + y]
 //   backward: dz -> A [kx][y] -> y pass A (+) -> B -> y pass B -> A [kx][y]
 //             -> c2r x pass A (+) on row pairs -> B -> x pass B -> vks = V + vxc
+// Both take several fields at once (gridDim.y, one field per y index at
+// fixed strides): the three components of grad rho and of the GGA vector h.
 //
 // Reference work replaced (as the oa_rho.cu kernels):
 //   fftRhoRtoRhoG (CP_Rho_RealSpacePlane.C:831) + the Charm forward FFT   -> k_rho2_fwd
@@ -33,7 +35,7 @@ template <int N1, int N2> struct Rho2Cfg {
 template <int N1, int N2>
 __global__ void __launch_bounds__(512, 1)
 k_rho2_fwd(const double* __restrict__ rho, double scale, const double2* __restrict__ twg,
-           double2* __restrict__ dz, int ldl_d) {
+           double2* __restrict__ dz, int ldl_d, size_t fin, size_t fout) {
   typedef Rho2Cfg<N1, N2> CF;
   constexpr int N = CF::N, NKX = CF::NKX, NPAIR = CF::NPAIR, LD = CF::LD, LS1 = CF::LS1, PS1 = CF::PS1;
   constexpr int NT = CF::NT;
@@ -43,6 +45,8 @@ k_rho2_fwd(const double* __restrict__ rho, double scale, const double2* __restri
   double2* A = tw + ((N + 1) & ~1);
   double2* B = A + CF::REGION;
   const int z = blockIdx.x, tid = threadIdx.x;
+  rho += blockIdx.y * fin;
+  dz += blockIdx.y * fout;
   for (int i = tid; i < N; i += NT) tw[i] = twg[i];
   // rows y1 = 2p, y2 = 2p + 1 as one complex sequence, scaled by V/N
   const double* rz = rho + (size_t)z * N * N;
@@ -113,7 +117,7 @@ k_rho2_fwd(const double* __restrict__ rho, double scale, const double2* __restri
 template <int N1, int N2, typename R>
 __global__ void __launch_bounds__(512, 1)
 k_rho2_bwd(const double2* __restrict__ dz, int ldl_d, const double2* __restrict__ twg,
-           const double* __restrict__ vxc, R* __restrict__ vks) {
+           const double* __restrict__ vxc, R* __restrict__ vks, size_t fin, size_t fout) {
   typedef Rho2Cfg<N1, N2> CF;
   constexpr int N = CF::N, NKX = CF::NKX, NPAIR = CF::NPAIR, LD = CF::LD, LS1 = CF::LS1, PS1 = CF::PS1;
   constexpr int NT = CF::NT;
@@ -123,6 +127,8 @@ k_rho2_bwd(const double2* __restrict__ dz, int ldl_d, const double2* __restrict_
   double2* A = tw + ((N + 1) & ~1);
   double2* B = A + CF::REGION;
   const int z = blockIdx.x, tid = threadIdx.x;
+  dz += blockIdx.y * fin;
+  vks += blockIdx.y * fout;
   for (int i = tid; i < N; i += NT) tw[i] = twg[i];
   const double2* in = dz + (size_t)z * ldl_d;
   for (int i = tid; i < NKX * N; i += NT) {
@@ -171,8 +177,8 @@ k_rho2_bwd(const double2* __restrict__ dz, int ldl_d, const double2* __restrict_
     for (int k1 = 0; k1 < N1; ++k1) B[p * PS1 + k1 * LS1 + n2] = u[k1];
   }
   __syncthreads();
-  // x pass B -> vks = V + vxc
-  const double* vz = vxc + (size_t)z * N * N;
+  // x pass B -> vks = V + vxc (vxc may be null: vks = V)
+  const double* vz = vxc ? vxc + (size_t)z * N * N : nullptr;
   R* oz = vks + (size_t)z * N * N;
   for (int i = tid; i < 16 * NPAIR; i += NT) {
     const int p = i >> 4, k1 = i & 15;
@@ -185,8 +191,8 @@ k_rho2_bwd(const double2* __restrict__ dz, int ldl_d, const double2* __restrict_
 #pragma unroll
     for (int k2 = 0; k2 < N2; ++k2) {
       const int x = k1 + N1 * k2;
-      oz[y1 * N + x] = (R)(w[k2].x + vz[y1 * N + x]);
-      if (y2 < N) oz[y2 * N + x] = (R)(w[k2].y + vz[y2 * N + x]);
+      oz[y1 * N + x] = (R)(w[k2].x + (vz ? vz[y1 * N + x] : 0.0));
+      if (y2 < N) oz[y2 * N + x] = (R)(w[k2].y + (vz ? vz[y2 * N + x] : 0.0));
     }
   }
 }
@@ -215,47 +221,48 @@ static size_t rho2_smem() {
 
 template <int N1, int N2>
 static cudaError_t rho2_fwd_n(cudaStream_t s, int nz, const double* rho, double scale, const double2* tw, double2* dz,
-                              int ldl_d) {
+                              int ldl_d, int nf, size_t fin, size_t fout) {
   const size_t sm = rho2_smem<N1, N2>();
   if (sm > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
   cudaError_t e = oa_smem_limit(k_rho2_fwd<N1, N2>);
   if (e != cudaSuccess) return e;
-  k_rho2_fwd<N1, N2><<<nz, 512, sm, s>>>(rho, scale, tw, dz, ldl_d);
+  k_rho2_fwd<N1, N2><<<dim3(nz, nf), 512, sm, s>>>(rho, scale, tw, dz, ldl_d, fin, fout);
   return cudaGetLastError();
 }
 
 template <int N1, int N2>
 static cudaError_t rho2_bwd_n(cudaStream_t s, int nz, const double2* dz, int ldl_d, const double2* tw,
-                              const double* vxc, void* vks, int fp64) {
+                              const double* vxc, void* vks, int fp64, int nf, size_t fin, size_t fout) {
   const size_t sm = rho2_smem<N1, N2>();
   if (sm > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
   cudaError_t e;
   if (fp64) {
     e = oa_smem_limit(k_rho2_bwd<N1, N2, double>);
     if (e != cudaSuccess) return e;
-    k_rho2_bwd<N1, N2, double><<<nz, 512, sm, s>>>(dz, ldl_d, tw, vxc, (double*)vks);
+    k_rho2_bwd<N1, N2, double><<<dim3(nz, nf), 512, sm, s>>>(dz, ldl_d, tw, vxc, (double*)vks, fin, fout);
   } else {
     e = oa_smem_limit(k_rho2_bwd<N1, N2, float>);
     if (e != cudaSuccess) return e;
-    k_rho2_bwd<N1, N2, float><<<nz, 512, sm, s>>>(dz, ldl_d, tw, vxc, (float*)vks);
+    k_rho2_bwd<N1, N2, float><<<dim3(nz, nf), 512, sm, s>>>(dz, ldl_d, tw, vxc, (float*)vks, fin, fout);
   }
   return cudaGetLastError();
 }
 
-// nx = ny = n; cudaErrorNotSupported when n has no two-pass kernel or the
+// nx = ny = n; nf fields at strides fin / fout (elements of the input /
+// output type); cudaErrorNotSupported when n has no two-pass kernel or the
 // plane does not fit in shared memory (the caller then uses the
 // runtime-plan kernels)
 cudaError_t oa_rho2_fwd(cudaStream_t s, int n, int nz, const double* rho, double scale, const double2* tw,
-                        double2* dz, int ldl_d) {
-#define OA_CALL(A, B) rho2_fwd_n<A, B>(s, nz, rho, scale, tw, dz, ldl_d)
+                        double2* dz, int ldl_d, int nf, size_t fin, size_t fout) {
+#define OA_CALL(A, B) rho2_fwd_n<A, B>(s, nz, rho, scale, tw, dz, ldl_d, nf, fin, fout)
   OA_RHO2_DISPATCH(n, OA_CALL)
 #undef OA_CALL
   return cudaErrorNotSupported;
 }
 
 cudaError_t oa_rho2_bwd(cudaStream_t s, int n, int nz, const double2* dz, int ldl_d, const double2* tw,
-                        const double* vxc, void* vks, int fp64) {
-#define OA_CALL(A, B) rho2_bwd_n<A, B>(s, nz, dz, ldl_d, tw, vxc, vks, fp64)
+                        const double* vxc, void* vks, int fp64, int nf, size_t fin, size_t fout) {
+#define OA_CALL(A, B) rho2_bwd_n<A, B>(s, nz, dz, ldl_d, tw, vxc, vks, fp64, nf, fin, fout)
   OA_RHO2_DISPATCH(n, OA_CALL)
 #undef OA_CALL
   return cudaErrorNotSupported;

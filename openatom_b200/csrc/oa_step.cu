@@ -53,6 +53,15 @@ cudaError_t oa_step_ortho_args(oa_ctx* c, double** work, int** status, double** 
 // per-step record: the 16 energy accumulators, NS iterations, converged,
 // residual, max|S - 2I|
 #define OA_REC 20
+#define OA_NREC_OUT 12  // values per step handed back (oa_gpu_cp_step)
+
+// one step record -> EKE EHART EEXT EWALD EEXC MUXC FICT ENL, Newton-Schulz
+// iterations, residual, max|S - 2I|, EGGA
+static void fill_energies(const double* hv, double* eo) {
+  eo[0] = hv[OA_E_EKE]; eo[1] = hv[OA_E_EHART]; eo[2] = hv[OA_E_EEXT]; eo[3] = hv[OA_E_EWALD];
+  eo[4] = hv[8] + hv[9]; eo[5] = hv[OA_E_MUXC]; eo[6] = hv[OA_E_FICT]; eo[7] = hv[OA_E_ENL];
+  eo[8] = hv[16]; eo[9] = hv[18]; eo[10] = hv[19]; eo[11] = hv[11] + hv[12];
+}
 
 struct oa_step_scratch {
   double *F, *F2, *Fnl, *S, *lam, *gam;
@@ -63,7 +72,7 @@ struct oa_step_scratch {
   int flag_host[4];
   cudaGraphExec_t exec;   // PsiV reset .. S
   cudaGraphExec_t exec2;  // Psi T + the step record
-  const void* key[7];
+  const void* key[8];
   int key_nterm;
   double key_dt, key_tol;
   int graph_kernels;      // kernel launches of one graphed step (graph nodes + launches outside)
@@ -228,7 +237,8 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
   OA_CUDA_TRY(cudaMemsetAsync(w->flag, 0, 4 * sizeof(int), s));
   // the psi planes of the mixed products, from the psi the caller hands in
   if (st->mixed_nterm) OA_STEP_TRY(oa_planes_psi_refresh(c, s, st->psi, st->mixed_nterm));
-  const void* key[7] = {st->psi, st->psi_t, st->vpsi, st->T, stream, w->ring, c->ees};
+  const void* key[8] = {st->psi, st->psi_t, st->vpsi, st->T, stream, w->ring, c->ees,
+                        (const void*)(uintptr_t)c->xc_gen};
   // the legacy default stream cannot be captured: launch eagerly there
   const bool capturable = s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread;
   // the cluster Newton-Schulz kernel is an ordinary launch: then the whole
@@ -304,24 +314,9 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
                               cudaMemcpyDeviceToHost, s));
   OA_CUDA_TRY(cudaMemcpyAsync(w->flag_host, w->flag, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
   OA_CUDA_TRY(cudaStreamSynchronize(s));
-  // energies: EKE EHART EEXT EWALD EEXC MUXC FICT ENL, then NS iters, residual, smax
-  for (int k = 0; k < nsteps; ++k) {
-    const double* hv = w->ring_host + (size_t)k * OA_REC;
-    if (energies_out) {
-      double* eo = energies_out + (size_t)k * 11;
-      eo[0] = hv[OA_E_EKE];
-      eo[1] = hv[OA_E_EHART];
-      eo[2] = hv[OA_E_EEXT];
-      eo[3] = hv[OA_E_EWALD];
-      eo[4] = hv[8] + hv[9];
-      eo[5] = hv[OA_E_MUXC];
-      eo[6] = hv[OA_E_FICT];
-      eo[7] = hv[OA_E_ENL];
-      eo[8] = hv[16];
-      eo[9] = hv[18];
-      eo[10] = hv[19];
-    }
-  }
+  // energies: EKE EHART EEXT EWALD EEXC MUXC FICT ENL, then NS iters, residual, smax, EGGA
+  if (energies_out)
+    for (int k = 0; k < nsteps; ++k) fill_energies(w->ring_host + (size_t)k * OA_REC, energies_out + (size_t)k * OA_NREC_OUT);
   const double* last = w->ring_host + (size_t)(nsteps - 1) * OA_REC;
   st->last_kernels = (st->use_graph && st->iteration > 1 && w->exec) ? w->graph_kernels : -1;
   st->last_ns_iters = (int)last[16];
@@ -345,12 +340,6 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
 // fork from `stream` onto one stream per system and join back, so the
 // kernels of different systems fill the GPU together.
 // ---------------------------------------------------------------------------
-static void fill_energies(const double* hv, double* eo) {
-  eo[0] = hv[OA_E_EKE]; eo[1] = hv[OA_E_EHART]; eo[2] = hv[OA_E_EEXT]; eo[3] = hv[OA_E_EWALD];
-  eo[4] = hv[8] + hv[9]; eo[5] = hv[OA_E_MUXC]; eo[6] = hv[OA_E_FICT]; eo[7] = hv[OA_E_ENL];
-  eo[8] = hv[16]; eo[9] = hv[18]; eo[10] = hv[19];
-}
-
 static oa_status batch_launch_one(oa_ctx* c, cudaStream_t s, oa_cp_state* st, int complete_prev) {
   oa_planes_step_begin(c);
   oa_status r = launch_step_a(c, s, st, complete_prev);
@@ -492,7 +481,7 @@ extern "C" oa_status oa_gpu_cp_run_batch(oa_ctx** ctxs, oa_cp_state** states, in
     oa_cp_state* st = states[i];
     if (energies_out)
       for (int k = 0; k < nsteps; ++k)
-        fill_energies(w->ring_host + (size_t)k * OA_REC, energies_out + ((size_t)i * nsteps + k) * 11);
+        fill_energies(w->ring_host + (size_t)k * OA_REC, energies_out + ((size_t)i * nsteps + k) * OA_NREC_OUT);
     const double* last = w->ring_host + (size_t)(nsteps - 1) * OA_REC;
     st->last_kernels = graph_kernels > 0 ? graph_kernels : -1;
     st->last_ns_iters = (int)last[16];

@@ -47,7 +47,9 @@ class SystemDesc(C.Structure):
 
 
 STEP_KEYS = ("EKE", "EHART", "EEXT", "EWALD_RECIP", "EEXC", "MUXC", "FICT_KE", "ENL", "ORTHO_ITERS",
-             "ORTHO_ERR", "SMAX")
+             "ORTHO_ERR", "SMAX", "EGGA")
+NREC = len(STEP_KEYS)
+XC_FUNCTIONALS = {"pz_lda": 0, "blyp": 1}
 
 
 class CPState(C.Structure):
@@ -81,6 +83,7 @@ SIGNATURES = {
     "oa_gpu_small_gemm": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, _vp]),
     "oa_gpu_integrate": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_double, C.c_int, _vp]),
     "oa_gpu_energies": (C.c_int, [_vp, _vp, _dp]),
+    "oa_gpu_set_xc": (C.c_int, [_vp, C.c_int, C.c_double]),
     "oa_gpu_psiv_reset": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "oa_gpu_psiv_reset_mixed": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int]),
     "oa_gpu_cp_run_batch": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int, _vp, C.c_int,
@@ -213,6 +216,16 @@ class CPContext:
         _check(lib.oa_gpu_init(C.byref(d), self.precision, C.byref(h)))
         self._h = h
         self._lib = lib
+        xc = getattr(sysm, "xc", "pz_lda")
+        if xc != "pz_lda":
+            self.set_xc(xc, getattr(sysm, "gga_cut", 5.0e-5))
+
+    def set_xc(self, functional: str, gradient_cutoff: float = 5.0e-5):
+        """Exchange-correlation of the density path: "pz_lda" or "blyp"
+        (oa_gpu_set_xc)."""
+        if functional not in XC_FUNCTIONALS:
+            raise ValueError(f"functional must be one of {sorted(XC_FUNCTIONALS)}")
+        _check(self._lib.oa_gpu_set_xc(self._h, XC_FUNCTIONALS[functional], float(gradient_cutoff)))
 
     def close(self):
         if getattr(self, "_h", None):
@@ -368,7 +381,7 @@ class CPContext:
                                       _ptr(enl_out)))
 
     def cp_step(self, state: CPState) -> dict:
-        out = (C.c_double * 11)()
+        out = (C.c_double * NREC)()
         _check(self._lib.oa_gpu_cp_step(self._h, self._stream(), C.byref(state), out))
         return {k: float(v) for k, v in zip(STEP_KEYS, out)}
 
@@ -376,7 +389,7 @@ class CPContext:
         """nsteps CP steps enqueued back to back with one synchronisation
         (oa_gpu_cp_run); pos_host: optional host array [nsteps][natm][3]
         copied in before each step.  Returns one record per step."""
-        out = np.zeros((nsteps, 11))
+        out = np.zeros((nsteps, NREC))
         pp = None
         if pos_host is not None:
             pp = np.ascontiguousarray(pos_host, dtype=np.float64)
@@ -401,9 +414,9 @@ class CPContext:
         _check(self._lib.oa_gpu_nl_ees(self._h, self._stream(), _ptr(psi), _ptr(fnl_out), _ptr(enl_out)))
 
     def energies(self) -> dict:
-        out = (C.c_double * 8)()
+        out = (C.c_double * 9)()
         _check(self._lib.oa_gpu_energies(self._h, self._stream(), out))
-        keys = ("EKE", "EHART", "EEXT", "EWALD_RECIP", "EEXC", "MUXC", "FICT_KE", "ENL")
+        keys = ("EKE", "EHART", "EEXT", "EWALD_RECIP", "EEXC", "MUXC", "FICT_KE", "ENL", "EGGA")
         return {k: float(v) for k, v in zip(keys, out)}
 
 
@@ -637,7 +650,7 @@ def run_batch(drivers, states, nsteps: int, stream=None) -> list:
     lib = load_library()
     ctxs = (C.c_void_p * n)(*[d.ctx._h.value for d in drivers])
     sts = (C.c_void_p * n)(*[C.cast(C.pointer(s), C.c_void_p).value for s in states])
-    out = np.zeros((n, nsteps, 11))
+    out = np.zeros((n, nsteps, NREC))
     st = stream if stream is not None else drivers[0].stream
     torch.cuda.synchronize()
     _check(lib.oa_gpu_cp_run_batch(ctxs, sts, n, C.c_void_p(st.cuda_stream), int(nsteps),
