@@ -8,8 +8,8 @@ cp_becke.C / cp_grad_rho_ctrl.C).
   and on one without (30^3: the runtime-plan transforms);
 * the native graphed FP64 step: 8 waters with all 32 states, five CPMD
   steps at dt = 5, each energy term to 1e-10 and the coefficients to 1e-9;
-* the mixed form on the same run: the total energy within 1e-6 Ha/atom of
-  the oracle;
+* the mixed form from a quenched start: the total energy within 1e-6
+  Ha/atom of the oracle;
 * switching the functional back to PZ-LDA re-captures the step graph."""
 import numpy as np
 import pytest
@@ -78,11 +78,21 @@ def test_blyp_native_steps_fp64():
 
 
 def test_blyp_native_steps_mixed():
+    """From a quenched start (three damped FP64 steps at dt = 5, then 27 at
+    dt = 10 on the GPU; the FP64 form is pinned above), where the energy
+    terms have their physical size, as in the mixed-form benchmark."""
     from openatom_b200.gpu import CPDriver
     s = _blyp_w8()
+    q = CPDriver(s, "fp64")
+    q.quench(3)
+    q.quench(27, dt=10.0)
+    psi0 = q.psi.cpu().numpy()
+    q.ctx.close()
     st = O.CPState(s)
+    st.psi_t = psi0.copy()
+    st.psi = psi0.copy()
     ref = [O.cp_step(st, s, norb_tol=0.003) for _ in range(5)]
-    d = CPDriver(s, "mixed", norb_tol=0.003)
+    d = CPDriver(s, "mixed", psi0=psi0, norb_tol=0.003)
     got = d.run_native(d.native_state(use_graph=True), 5)
     natm = s.natm
     for g, r in zip(got, ref):
