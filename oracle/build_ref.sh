@@ -28,6 +28,7 @@ SRCS=(
   "$PINY/abinito_physics/cp_integrate/cp_min_CG.C"
   "$PINY/abinito_physics/cp_nonlocal/cp_ees_nonlocal.C"
   "$PINY/interface/cp_ewald/set_cp_ewald.C"
+  "$PINY/abinito_physics/cp_ions/cp_rspace_ion.C"
 )
 OBJS=()
 for s in "${SRCS[@]}"; do

@@ -698,6 +698,136 @@ def nl_ees_energy_forces(psi, sysm, ees, atom_forces=False):
     return fnl, enl, zmat, fatm
 
 
+def nl_sf_atom_forces(psi, sysm, sf=None):
+    """Nonlocal atom forces of the N^2 method (``CP_enl_atm_forc_calc``,
+    ``cp_nl_energy_forc.C:178-235``, doublePack branch): with
+    Z = real_view(psi) real_view(SF)^T and dSF/dR_a = -i g SF_a
+    (``CP_calc_Struct_Fact``'s derivative structure factors,
+    ``cp_struct_fact.C:37-255``), F_a -= sum_s (2 vnorm / V Z_sa) dZ_sa/dR_a.
+    As in the reference, the occupation scales the energy, not this force
+    (the seeded systems have occupation 1).  Returns [natm, 3]."""
+    if sf is None:
+        sf, nl = struct_fact(sysm)
+    else:
+        nl = sysm.nl_atoms()
+    vn = sysm.nl_vnorm[sysm.atm_type[nl]] / sysm.vol
+    Z = real_view(psi) @ real_view(sf).T
+    Zp = 2.0 * vn[None, :] * Z
+    f = TWO_PI / sysm.box
+    fatm = np.zeros((sysm.natm, 3))
+    for ax, k in enumerate((sysm.kx, sysm.ky, sysm.kz)):
+        dsf = np.ascontiguousarray(-1j * (f * k)[None, :] * sf)
+        dZ = real_view(psi) @ real_view(dsf).T
+        np.add.at(fatm[:, ax], nl, -np.sum(Zp * dZ, axis=0))
+    return fatm
+
+
+# ----------------------------------------------------------------------------
+# ion side: real-space Ewald, atom integration
+# ----------------------------------------------------------------------------
+
+PROT_MASS = 1822.8885                         # piny_constants.h:55: amu -> electron masses
+ATOM_MASS_AMU = {"O": 15.9994, "H": 1.00794}
+# erfc(x) exp(-x^2)-form approximation of CPRSPACEION::CP_getionforce
+# (cp_ions/cp_rspace_ion.C:36-45): erfc(x) = t P(t) exp(-x^2), t = 1/(1 + p x)
+EWALD_P = 0.3614
+EWALD_E = (0.2041422096422003, 0.1997535956961481, 0.2213176596405576, 0.03360430734640255,
+           0.4732592578721755, -0.509078520069735, 0.6772631491947646, -0.369912979092217,
+           0.06965131976970335)
+
+
+def _erfc_poly(x):
+    """(erfc(x), t^2 exp(-x^2) sum_k k e_k t^(k-1)) of the reference's approximation."""
+    t = 1.0 / (1.0 + EWALD_P * x)
+    eee = np.exp(-x * x)
+    poly = 0.0
+    dpoly = 0.0
+    for k in range(len(EWALD_E), 0, -1):
+        poly = poly * t + EWALD_E[k - 1]
+        dpoly = dpoly * t + k * EWALD_E[k - 1]
+    return poly * t * eee, dpoly * t * t * eee
+
+
+def atom_masses(sysm):
+    return np.array([ATOM_MASS_AMU[sysm.type_names[t]] * PROT_MASS for t in sysm.atm_type])
+
+
+def ewald_rspace(sysm):
+    """``CPRSPACEION::CP_getionforce`` (``cp_rspace_ion.C:25-251``), cubic
+    periodic cell: pairs at the minimum image within half the box,
+    q_i q_j erfc(alpha r) / r and its force; the self term
+    -alpha sum q^2 / sqrt(pi) times erf(k_cut / 2 alpha) of the finite
+    reciprocal sum (k_cut = the density-sphere radius) and the neutralising
+    background -pi (sum q)^2 / (2 alpha^2 V).  Returns (E_real, E_self,
+    E_bgr, F [natm, 3])."""
+    pos, q, L, alp = sysm.pos, np.asarray(sysm.q, float), sysm.box, sysm.alp_ewd
+    natm = pos.shape[0]
+    F = np.zeros((natm, 3))
+    e_real = 0.0
+    palp = EWALD_P * alp
+    talp2 = 2.0 * alp * alp
+    for i in range(natm - 1):
+        d = pos[i] - pos[i + 1:]
+        d -= L * np.rint(d / L)
+        r2 = np.sum(d * d, axis=1)
+        r = np.sqrt(r2)
+        m = r <= 0.5 * L
+        qij = q[i] * q[i + 1:]
+        ge, dg = _erfc_poly(r * alp)
+        dge = dg * palp + talp2 * ge * r
+        v = np.where(m, qij * ge / r, 0.0)
+        dv = np.where(m, (ge / r2 + dge / r) * qij / r, 0.0)
+        e_real += float(np.sum(v))
+        fij = d * dv[:, None]
+        F[i] += fij.sum(0)
+        F[i + 1:] -= fij
+    kcut = math.sqrt(sysm.ecut_rho_g2)
+    self_erfc, _ = _erfc_poly(np.array(kcut / (2.0 * alp)))
+    e_self = -(float(np.sum(q * q)) * alp) / math.sqrt(math.pi) * (1.0 - float(self_erfc))
+    e_bgr = -(0.5 * float(np.sum(q)) ** 2 * math.pi) / (alp * alp * sysm.vol)
+    return e_real, e_self, e_bgr, F
+
+
+class IonState:
+    """Atom velocities and masses of a CPMD run with moving ions."""
+
+    def __init__(self, sysm, vel=None):
+        self.m = atom_masses(sysm)
+        self.v = np.zeros_like(sysm.pos) if vel is None else np.array(vel, dtype=np.float64)
+
+
+def ion_forces(psi, sysm, rho_r, nl="sf", ees=None):
+    """Forces on the ions at the current positions: local pseudopotential and
+    reciprocal Ewald (``CP_hart_eext_calc``), the nonlocal part (structure
+    factor or EES) and the real-space Ewald sum.  Returns (F [natm, 3],
+    dict of the ion-side energies)."""
+    _, _, _, _, f_loc = hart_eext(rho_r, sysm, want_forces=True)
+    if nl == "ees":
+        f_nl = nl_ees_energy_forces(psi, sysm, ees, atom_forces=True)[3]
+    elif nl == "sf":
+        f_nl = nl_sf_atom_forces(psi, sysm)
+    else:
+        f_nl = 0.0
+    e_real, e_self, e_bgr, f_r = ewald_rspace(sysm)
+    return f_loc + f_nl + f_r, {"EWALD_REAL": e_real, "EWALD_SELF": e_self, "EWALD_BGR": e_bgr}
+
+
+def integrate_ions(ions, F, sysm, iteration, dt):
+    """NVE atom integration (``ATOMINTEGRATE::integrate_nve_2nd_half`` /
+    ``integrate_nve_1st_half``, ``classical_physics/integrate/integration_drivers.C:17-85``,
+    in the order of ``ctrl_atom_integrate``, ``control_integrate.C:22-160``):
+    the second half kick of the previous step (not on the first step), the
+    kinetic energy, then the first half kick and the drift.  Moves
+    sysm.pos in place; returns the ionic kinetic energy."""
+    a = F / ions.m[:, None]
+    if iteration > 1:
+        ions.v += 0.5 * dt * a
+    ke = 0.5 * float(np.sum(ions.m[:, None] * ions.v * ions.v))
+    ions.v += 0.5 * dt * a
+    sysm.pos += dt * ions.v
+    return ke
+
+
 # ----------------------------------------------------------------------------
 # PairCalculator / Ortho
 # ----------------------------------------------------------------------------
@@ -894,18 +1024,28 @@ def _nl_default(psi, sysm):
     return f, float(enl.sum())
 
 
-def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl="auto", norb_tol=None, dt=None):
+def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl="auto", norb_tol=None, dt=None, ions=None):
     """One CPAIMD electronic step.  Order: forces on the orthonormal psi
     (computePsiFandVKS + NL, combineForcesGetEke), constraint force
     (computeLambdaAndCg), integrate (integrateModForce ->
     CPINTEGRATE::CP_integrate_dyn, cp_dynamics.C:29-88), orthonormalise
-    (computeNewPsi).  Returns the energy record of the psi the forces were
-    evaluated on."""
+    (computeNewPsi).  With ions (an IonState) the atoms move too: their
+    forces at the positions of this step (ion_forces) and the NVE atom
+    integration (integrate_ions, AtomsCompute::integrateAtoms,
+    drv/main/AtomsCompute.C:461-640), after which the next step's structure
+    factors see the new positions.  Returns the energy record of the psi the
+    forces were evaluated on."""
     st.iteration += 1
     if nl == "auto":
         nl = _nl_default if len(sysm.nl_atoms()) else None
     fnl, enl = (None, 0.0) if nl is None else nl(st.psi, sysm)
+    if ions is not None:
+        rho_r = density(state_g_to_r(st.psi, sysm), sysm)
+        fion, eion = ion_forces(st.psi, sysm, rho_r, nl="sf" if nl is not None else None)
     f, en = electronic_forces(st.psi, sysm, fnl, enl)
+    if ions is not None:
+        en.update(eion)
+        en["ION_KE"] = integrate_ions(ions, fion, sysm, st.iteration, sysm.dt if dt is None else dt)
     f, lam = lambda_step(st.psi, f, st.T, sysm)
     st.v, st.psi_t, fict = integrate_dyn(f, st.v, st.psi_t, sysm, st.iteration, sysm.dt if dt is None else dt)
     en["FICT_KE"] = float(fict.sum())

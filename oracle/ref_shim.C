@@ -18,6 +18,7 @@
 #include "../class_defs/CP_OPERATIONS/class_cplocal.h"
 #include "../class_defs/CP_OPERATIONS/class_cporthog.h"
 #include "../class_defs/CP_OPERATIONS/class_cpintegrate.h"
+#include "../class_defs/CP_OPERATIONS/class_cprspaceion.h"
 #include <vector>
 
 // y = alpha op(A) x + beta y, A column-major m x n (lda), op = 'T'/'t' or
@@ -632,4 +633,29 @@ extern "C" void ref_ees_psi_forc(int nstate, const double* projg, double* fpsi) 
                                    (complex*)fpsi + (size_t)s * ng, yr.data(), yi.data(), e.kx.data(), e.ky.data(),
                                    e.kz.data(), s, 0, it, 1, 0);
     }
+}
+
+// CPRSPACEION::CP_getionforce (cp_ions/cp_rspace_ion.C:25-251), cubic
+// periodic box (iperd 3), no Grimme dispersion: real-space Ewald energy and
+// forces, the self term with its erf factor and the background term.
+// ecut_ha: the reciprocal Ewald cutoff in Hartree (k_cut = sqrt(2 ecut_ha)).
+extern "C" void ref_rspace_ion(int natm, const double* pos, const double* q, double alp_ewd, double ecut_ha,
+                               double box, double* e_real, double* e_self, double* e_bgr, double* fatm) {
+  set_cell(box);
+  GENERAL_DATA* g = &readonly_general_data;
+  g->gencell.iperd = 3;
+  g->genewald.alp_ewd = alp_ewd;
+  g->genewald.ecut = ecut_ha;
+  MDATOMS* md = &readonly_mdatoms;
+  md->mdclatoms_info.natm_tot = natm;
+  md->mdclatoms_info.cp_grimme = 0;
+  std::vector<double> x(natm), y(natm), z(natm), qq(q, q + natm), fx(natm, 0.0), fy(natm, 0.0), fz(natm, 0.0);
+  for (int a = 0; a < natm; ++a) { x[a] = pos[3 * a]; y[a] = pos[3 * a + 1]; z[a] = pos[3 * a + 2]; }
+  FastAtoms fa;
+  fa.natm = natm; fa.x = x.data(); fa.y = y.data(); fa.z = z.data(); fa.q = qq.data();
+  fa.fx = fx.data(); fa.fy = fy.data(); fa.fz = fz.data();
+  PSSCRATCH scr;
+  double recip = 0.0, grimme = 0.0;
+  CPRSPACEION::CP_getionforce(natm, &fa, 0, 1, e_real, e_self, e_bgr, &recip, &scr, &grimme);
+  for (int a = 0; a < natm; ++a) { fatm[3 * a] = fx[a]; fatm[3 * a + 1] = fy[a]; fatm[3 * a + 2] = fz[a]; }
 }

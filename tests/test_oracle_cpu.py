@@ -175,6 +175,32 @@ def test_gga_potential_is_energy_derivative():
     assert abs(fd - pred) < 1e-6 * abs(pred)
 
 
+def test_ion_forces_are_energy_gradient():
+    """The forces on the ions (local pseudopotential and reciprocal Ewald of
+    CP_hart_eext_calc, the structure-factor nonlocal part, the real-space
+    Ewald sum) are minus the gradient of EEXT + ENL + the Ewald energy at
+    fixed coefficients, by central finite differences."""
+    s = make_system("w2", seed=3)
+    psi = s.psi
+
+    def e_ion():
+        rho = O.density(O.state_g_to_r(psi, s), s)
+        _, _, ee, ew = O.hart_eext(rho, s)
+        er, es, eb, _ = O.ewald_rspace(s)
+        return ee + ew + float(O.nl_energy_forces(psi, s)[1].sum()) + er + es + eb
+
+    F, _ = O.ion_forces(psi, s, O.density(O.state_g_to_r(psi, s), s))
+    h = 1e-5
+    for a in (0, 1, 4):
+        for ax in range(3):
+            s.pos[a, ax] += h
+            ep = e_ion()
+            s.pos[a, ax] -= 2 * h
+            em = e_ion()
+            s.pos[a, ax] += h
+            assert abs(-(ep - em) / (2 * h) - F[a, ax]) < 1e-7 * np.max(np.abs(F))
+
+
 def test_cg_minimisation_beats_steepest_descent():
     """The oracle's minimisation loop (computeMinimization): both methods
     lower the energy; conjugate gradients lower it further and reduce the

@@ -7,7 +7,9 @@ Pinned: CPNONLOCAL::CP_eke_calc (cp_eke.C), CPXCFNCTS::CP_exc_calc
 CPORTHOG::get_iter_Tmat (cp_lowdin.C), the structure-factor nonlocal path
 (cp_struct_fact.C, cp_nlmat.C, cp_nl_energy_forc.C), the EES nonlocal path
 (cp_ees_nonlocal.C with get_bspline_wght1d of set_cp_ewald.C), the CP
-integrator (cp_dynamics.C) and the minimisers (cp_min_std.C, cp_min_CG.C).
+integrator (cp_dynamics.C), the minimisers (cp_min_std.C, cp_min_CG.C), the
+BLYP functional (cp_becke.C, cp_grad_rho_ctrl.C) and the real-space Ewald
+sum (cp_rspace_ion.C).
 The FFT and GEMM boundaries have no reference implementation here (FFTW2 /
 Fortran BLAS are absent) and are pinned by mathematics in test_oracle_cpu.py.
 """
@@ -172,7 +174,8 @@ def test_nl_struct_fact_pinned(ref, sysm):
     assert np.max(np.abs(fnl - f_or)) <= 1e-12 * np.max(np.abs(f_or))
     vn = s.nl_vnorm[s.atm_type[a["nl"]]] / s.vol
     assert np.max(np.abs(zmat - 2.0 * vn[None, :] * z_or)) <= 1e-12 * np.max(np.abs(zmat))
-    assert np.all(np.isfinite(fatm))
+    fa_or = O.nl_sf_atom_forces(s.psi, s, sf_or)
+    assert np.max(np.abs(fatm - fa_or)) <= 1e-11 * np.max(np.abs(fa_or))
 
 
 @pytest.mark.parametrize("iteration", [1, 2])
@@ -318,3 +321,24 @@ def test_gga_functional_pinned(ref, sysm):
     assert np.max(np.abs(vks[:, :, :nx] - v_or)) <= 1e-12 * np.max(np.abs(v_or))
     for a in range(3):
         assert np.max(np.abs(g[a][:, :, :nx] - h_or[a])) <= 1e-12 * np.max(np.abs(h_or))
+
+
+def test_rspace_ewald_pinned(ref, sysm):
+    """CPRSPACEION::CP_getionforce (cp_rspace_ion.C): real-space Ewald energy
+    and forces at the minimum image within half the box, the self term with
+    the erf factor of the finite reciprocal sum and the background term,
+    against oracle.ewald_rspace."""
+    s = sysm
+    ref.ref_rspace_ion.argtypes = [C.c_int, dp, dp, C.c_double, C.c_double, C.c_double, dp, dp, dp, dp]
+    pos = np.ascontiguousarray(s.pos)
+    q = np.ascontiguousarray(s.q, dtype=np.float64)
+    er, es, eb = C.c_double(), C.c_double(), C.c_double()
+    fatm = np.zeros((s.natm, 3))
+    # reciprocal cutoff of the density sphere in Hartree: k_cut^2 = 2 ecut
+    ref.ref_rspace_ion(s.natm, _d(pos), _d(q), s.alp_ewd, 0.5 * s.ecut_rho_g2, s.box, C.byref(er), C.byref(es),
+                       C.byref(eb), _d(fatm))
+    e_r, e_s, e_b, f_or = O.ewald_rspace(s)
+    assert abs(er.value - e_r) <= 1e-12 * abs(e_r)
+    assert abs(es.value - e_s) <= 1e-13 * abs(e_s)
+    assert abs(eb.value - e_b) <= 1e-13 * abs(e_b)
+    assert np.max(np.abs(fatm - f_or)) <= 1e-12 * np.max(np.abs(f_or))
