@@ -293,9 +293,11 @@ typedef struct {
  * synchronisation at the end.  The PsiV reset triggered by max|S - 2I| >
  * norb_tol (Ortho::maxCheck, ortho.C:455-475) is decided on the device and
  * runs at the end of the step, as oa_gpu_psiv_reset would (oa_gpu_psiv_reset_mixed
- * with state->mixed_nterm planes when that is nonzero).  energies_out (optional, host [12]):
+ * with state->mixed_nterm planes when that is nonzero).  energies_out (optional, host [14]):
  * EKE EHART EEXT EWALD_RECIP EEXC MUXC FICT_KE ENL, Newton-Schulz
- * iterations, residual, max|S - 2I|, EGGA (0 under PZ-LDA).  Coefficient arrays must be 16-byte
+ * iterations, residual, max|S - 2I|, EGGA (0 under PZ-LDA), the ionic
+ * kinetic energy and the real-space Ewald energy with its self and
+ * background terms (both 0 unless oa_gpu_set_ions turned ion dynamics on).  Coefficient arrays must be 16-byte
  * aligned. */
 oa_status oa_gpu_cp_step(oa_ctx *ctx, void *stream, oa_cp_state *state, double *energies_out);
 
@@ -305,7 +307,7 @@ oa_status oa_gpu_cp_step(oa_ctx *ctx, void *stream, oa_cp_state *state, double *
  * InstanceController::printEnergy*, main/InstanceController.C:373-490,
  * becomes one record per step).  pos_host (optional, host
  * [nsteps][natm][3]) is copied to the atom positions before each step.
- * energies_out (optional, host [nsteps][12]) as oa_gpu_cp_step's.  When the
+ * energies_out (optional, host [nsteps][14]) as oa_gpu_cp_step's.  When the
  * Newton-Schulz iteration fails in a step, the call still runs all nsteps
  * and returns OA_ERR_NOT_CONVERGED or OA_ERR_NONFINITE naming the first
  * failing step in oa_gpu_last_error(); the state is then that of the last
@@ -321,7 +323,7 @@ oa_status oa_gpu_cp_run(oa_ctx *ctx, void *stream, oa_cp_state *state, int nstep
  * back.  Results are those of oa_gpu_cp_run on each system alone.  The
  * reference runs such sets as separate instances (UberCollection /
  * InstanceController, main/InstanceController.C).  energies_out (optional,
- * host [nsys][nsteps][12]).  Needs at most 128 states per system (the whole
+ * host [nsys][nsteps][14]).  Needs at most 128 states per system (the whole
  * step captured); a Newton-Schulz failure names the first failing system
  * and step. */
 oa_status oa_gpu_cp_run_batch(oa_ctx **ctxs, oa_cp_state **states, int nsys, void *stream, int nsteps,
@@ -361,8 +363,28 @@ oa_status oa_gpu_ees_init(oa_ctx *ctx, int na, int nb, int nc, int order, const 
 oa_status oa_gpu_nl_ees(oa_ctx *ctx, void *stream, const double *psi, double *fnl_out, double *enl_out);
 
 /* Energies of the last vks_build / vks_apply_fft_bwd (synchronises):
- * out[0..8] = EKE, EHART, EEXT, EWALD_RECIP, EEXC, MUXC, FICT_KE, ENL, EGGA. */
-oa_status oa_gpu_energies(oa_ctx *ctx, void *stream, double *out9);
+ * out[0..10] = EKE, EHART, EEXT, EWALD_RECIP, EEXC, MUXC, FICT_KE, ENL, EGGA,
+ * ION_KE, EWALD_REAL (the last two from the last native step with ions). */
+oa_status oa_gpu_energies(oa_ctx *ctx, void *stream, double *out11);
+
+/* Ion dynamics in the native step (oa_gpu_cp_step / oa_gpu_cp_run): each
+ * step computes the forces on the atoms at their current positions -- the
+ * local pseudopotential and reciprocal Ewald part of CP_hart_eext_calc
+ * (cp_hart_ext.C:56-431, in the density z pass), the structure-factor
+ * nonlocal part of CP_enl_atm_forc_calc (cp_nl_energy_forc.C:178-235) and
+ * the real-space Ewald sum of CPRSPACEION::CP_getionforce
+ * (cp_ions/cp_rspace_ion.C:25-251) -- and moves them by the NVE integrator of
+ * AtomsCompute::integrateAtoms (drv/main/AtomsCompute.C:461-640,
+ * integration_drivers.C:17-85): second half kick of the previous step
+ * (not on a run's first step), first half kick, drift.  masses: host [natm]
+ * in electron masses; vel: host [natm][3] (null: zero).  Not with the EES
+ * nonlocal path (its atom forces are not built; OA_ERR_BAD_ARG), and
+ * oa_gpu_cp_run then takes no pos_host. */
+oa_status oa_gpu_set_ions(oa_ctx *ctx, const double *masses, const double *vel);
+
+/* Current atom positions and velocities (host [natm][3] each, either may be
+ * null); synchronises. */
+oa_status oa_gpu_get_ions(oa_ctx *ctx, void *stream, double *pos_out, double *vel_out);
 
 /* Exchange-correlation functional of the density path (the reference's
  * \cp_ggax_typ / \cp_ggac_typ and \gradient_cutoff inputs,

@@ -424,12 +424,14 @@ fail:
 }
 
 void oa_step_free(oa_ctx* c);
+void oa_ions_free(oa_ctx* c);
 static void ees_free(oa_ctx* c);
 
 extern "C" oa_status oa_gpu_destroy(oa_ctx* c) {
   if (!c) return OA_OK;
   oa_step_free(c);
   ees_free(c);
+  oa_ions_free(c);
   oa_ctx_pc* p = pcx(c);
   oa_oz_free(p->oz);
   p->oz = nullptr;
@@ -717,6 +719,8 @@ extern "C" oa_status oa_gpu_energies(oa_ctx* c, void* stream, double* out7) {
   out7[6] = p->h_vals[OA_E_FICT];
   out7[7] = p->h_vals[OA_E_ENL];
   out7[8] = p->h_vals[OA_E_EGGA];
+  out7[9] = p->h_vals[OA_E_ION_KE];
+  out7[10] = p->h_vals[OA_E_EWALD_REAL];
   return OA_OK;
 }
 
@@ -1251,6 +1255,8 @@ extern "C" oa_status oa_gpu_nl_sf(oa_ctx* c, void* stream, const double* psi, in
                           fnl_out, PL_SF, PL_OTHER));
   OA_CUDA_TRY(oa_launch_sum_partials(s, c->enl, n, 1, 0, 1.0, p->dev_e + OA_E_ENL));
   if (enl_out) OA_CUDA_TRY(cudaMemcpyAsync(enl_out, c->enl, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  // ion dynamics: the nonlocal atom forces from the same Z
+  if (c->ions) OA_CUDA_TRY(oa_launch_nl_sf_force(c, s, psi));
   return OA_OK;
 }
 
@@ -1281,6 +1287,7 @@ extern "C" oa_status oa_gpu_ees_init(oa_ctx* c, int na, int nb, int nc, int orde
   OA_ARG_CHECK(order >= 4 && order <= 16 && order % 2 == 0, "EES order must be even, 4..16 (cp_pseudo_ees_order)");
   OA_ARG_CHECK(na >= order && nb >= order && nc >= order, "EES grid smaller than the interpolation order");
   OA_ARG_CHECK(c->natm_nl > 0, "no nonlocal atoms");
+  OA_ARG_CHECK(!c->ions, "ion dynamics needs the structure-factor nonlocal path (the EES atom forces are not built)");
   ees_free(c);
   oa_ees* e = (oa_ees*)calloc(1, sizeof(oa_ees));
   if (!e) return OA_ERR_CUDA;

@@ -39,6 +39,20 @@ struct oa_ees {
   double* enl;         // [nstate]
 };
 
+// Ion dynamics (oa_gpu_set_ions): masses, velocities and the force pieces of
+// one step, summed by the integrator in a fixed order
+struct oa_ions {
+  double* m;        // [natm] electron masses
+  double* v;        // [natm][3]
+  double* fpart;    // [z-pass blocks][natm][3] local pseudopotential + reciprocal Ewald
+  double* fnl;      // [natm][3] nonlocal (structure-factor method)
+  double* fr;       // [natm][3] real-space Ewald
+  double* er;       // [natm] real-space Ewald energy per atom i (pairs j > i)
+  double* y;        // [natm_nl][2 ng] sum_s Z[s][a] psi_s (nonlocal force product)
+  int nfpart;       // z-pass blocks
+  double self_bgr;  // Ewald self + background terms (constant for fixed charges and box)
+};
+
 struct oa_ctx {
   int device;
   int precision;          // OA_FP64 or OA_MIXED
@@ -111,10 +125,13 @@ struct oa_ctx {
   unsigned xc_gen;        // bumped by every oa_gpu_set_xc (captured step graphs key on it)
   double *grad;           // [3][nz][ny][nx] grad rho, then the GGA vector h (BLYP)
   void *dzg;              // [3][nz][ldl_d] C  z-lines of grad rho / h (BLYP)
+  oa_ions *ions;          // ion dynamics, after oa_gpu_set_ions
 };
 
 enum { OA_E_EKE = 0, OA_E_EHART, OA_E_EEXT, OA_E_EWALD, OA_E_EEXC, OA_E_MUXC, OA_E_ENL, OA_E_FICT };
 #define OA_E_EGGA 10      // device energy slot of EGGA (slots 8, 9 hold the EEXC halves)
+#define OA_E_ION_KE 13    // ionic kinetic energy (ion dynamics)
+#define OA_E_EWALD_REAL 14  // real-space Ewald + self + background terms (ion dynamics)
 cudaError_t oa_launch_phase_tables(oa_ctx* c, cudaStream_t s);
 
 #define OA_CUDA_TRY(x)                                  \
@@ -136,4 +153,6 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s);
 cudaError_t oa_launch_ees(oa_ctx* c, cudaStream_t s, const double2* psi, double2* fnl);
 cudaError_t oa_launch_ees_zreduce(oa_ctx* c, cudaStream_t s);
 cudaError_t oa_launch_ees_bspline(oa_ctx* c, cudaStream_t s);
+cudaError_t oa_launch_nl_sf_force(oa_ctx* c, cudaStream_t s, const double* psi);
+cudaError_t oa_launch_ion_step(oa_ctx* c, cudaStream_t s, double* dev_e, double dt, int kick2);
 size_t oa_plane_smem_bytes(int precision, int nx, int ny, int nkx);

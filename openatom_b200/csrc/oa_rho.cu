@@ -274,7 +274,14 @@ __device__ void zfft2(double2* a, double2* b, int ld, int nb, const double2* tw)
   __syncthreads();
 }
 
-template <int N1, int N2>
+// FORCES: also the atom forces of the local pseudopotential and the
+// reciprocal Ewald sum (CP_hart_eext_calc's force loop, cp_hart_ext.C:300-360):
+// per g of the block the per-type coefficients
+//   A_t = w (Re rho v_t + Re S_q ewf q_t),  B_t = w (-Im rho v_t + Im S_q ewf q_t)
+// go to shared memory, then one warp per atom sums
+//   F_a += g (A_t Im h_a - B_t Re h_a),  h_a = e^{i g.R_a},
+// over the block's g-points into fpart[block][atom][3].
+template <int N1, int N2, bool FORCES>
 __global__ void __launch_bounds__(OA_NTHREADS, 2)
 k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, int nz,
             OaFftPlan pz, const double2* __restrict__ twz,
@@ -282,7 +289,7 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
             int natm, int ntype, const int* __restrict__ atm_perm, RhoTypeOff toff,
             const double* __restrict__ q_type, const double2* __restrict__ phase, int ktab,
             const double* __restrict__ spl, int nspl, double gmin, double dg,
-            double* __restrict__ part) {
+            double* __restrict__ part, double* __restrict__ fpart) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ldz = nz + 1;
   constexpr bool TP = N1 > 0;  // two-pass compile-time transforms
@@ -297,6 +304,8 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
   const int nt = 2 * ktab + 1;
   load_twiddles(tw, twz, nz);
   int* zoff = (int*)(pxy + OA_LB * natm);  // [natm]: z-phase row of atom ia (type order)
+  // FORCES: [OA_LB * nz][ntype] per-type (A, B) coefficients after zoff
+  double2* cf = (double2*)(smem_raw + (((size_t)((char*)(zoff + natm) - (char*)smem_raw) + 15) & ~(size_t)15));
   for (int ia = threadIdx.x; ia < natm; ia += blockDim.x) zoff[ia] = (atm_perm[ia] * 3 + 2) * nt + ktab;
   for (int idx = threadIdx.x; idx < OA_LB * natm; idx += blockDim.x) {
     const int lb = idx / natm, ia = idx - lb * natm;
@@ -336,6 +345,7 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
     const double gzv = tpi_l * kz;
     double2 rho[ZP_L], sf_q[ZP_L], vext[ZP_L];
     double g2v[ZP_L], hh[ZP_L], wn[ZP_L];
+    double vtt[ZP_L][4];  // FORCES: v_t(|g|) / V per type
     int cls[ZP_L], ii[ZP_L];  // cls: 0 outside, 1 g = 0, 2 inside the density sphere
     bool any = false;
 #pragma unroll
@@ -391,6 +401,7 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
           const double* cc = spl + ((size_t)t * nspl + (ii[j] - 1)) * 4;
           const double vt = (((cc[3] * hh[j] + cc[2]) * hh[j] + cc[1]) * hh[j] + cc[0]) / vol;
           vext[j].x += st[j].x * vt; vext[j].y += st[j].y * vt;
+          if constexpr (FORCES) vtt[j][t] = vt;
         }
       }
     }
@@ -413,9 +424,53 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
         acc[1] += (rho[j].x * vext[j].x - rho[j].y * vext[j].y) * wn[j];  // Re(rho vext)
       }
       r[lb * ldz + zz] = out;
+      if constexpr (FORCES) {
+        double2* c2 = cf + ((size_t)lb * nz + zz) * ntype;
+        for (int t = 0; t < ntype && t < 4; ++t) {
+          double2 ab = make_double2(0.0, 0.0);
+          if (cls[j] == 2) {
+            const double g2 = g2v[j];
+            const double ewf = fpi * exp(-g2 / falp2) / (g2 * vol);
+            const double qt = q_type[t];
+            ab.x = wn[j] * (rho[j].x * vtt[j][t] + sf_q[j].x * ewf * qt);
+            ab.y = wn[j] * (-rho[j].y * vtt[j][t] + sf_q[j].y * ewf * qt);
+          }
+          c2[t] = ab;
+        }
+      }
     }
   }
   __syncthreads();
+  if constexpr (FORCES) {
+    // one warp per atom (type order), lanes over the block's (line, plane) points
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int ia = warp; ia < natm; ia += nwarp) {
+      int t = 0;
+      while (t + 1 < ntype && ia >= toff.off[t + 1]) ++t;
+      double fx = 0.0, fy = 0.0, fz = 0.0;
+      for (int e = lane; e < nb * nz; e += 32) {
+        const int lb = e / nz, zz = e - lb * nz;
+        const double2 ab = cf[((size_t)lb * nz + zz) * ntype + t];
+        if (ab.x == 0.0 && ab.y == 0.0) continue;
+        const int l = l0 + lb;
+        const int kx = l / ny;
+        int ky = l - kx * ny; if (2 * ky >= ny) ky -= ny;
+        int kz = zz; if (2 * kz >= nz) kz -= nz;
+        const double2 h = cmul(pxy[lb * natm + ia], phase[zoff[ia] + kz]);
+        const double comp = ab.x * h.y - ab.y * h.x;
+        fx += tpi_l * kx * comp;
+        fy += tpi_l * ky * comp;
+        fz += tpi_l * kz * comp;
+      }
+      fx = warp_sum_d(fx);
+      fy = warp_sum_d(fy);
+      fz = warp_sum_d(fz);
+      if (lane == 0) {
+        double* o = fpart + ((size_t)blockIdx.x * natm + atm_perm[ia]) * 3;
+        o[0] = fx; o[1] = fy; o[2] = fz;
+      }
+    }
+  }
   double2* r2;
   if constexpr (TP) {
     zfft2<N1, N2, +1>(a, b, ldz, nb, tw);
@@ -814,11 +869,13 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
   RhoTypeOff toff;
   for (int t = 0; t < 5; ++t) toff.off[t] = c->type_off[t];
   const int nbz = oa_rho_z_nblk(c);
+  const bool forces = c->ions != nullptr;
   auto zpass = [&](auto kern, int ldb) -> cudaError_t {
-    const size_t smz =
+    size_t smz =
         (align_up_r(c->nz, 2) + (size_t)OA_LB * (c->nz + 1) + (size_t)OA_LB * ldb + (size_t)OA_LB * c->natm) *
             sizeof(double2) +
         (size_t)c->natm * sizeof(int);  // zoff
+    if (forces) smz = align_up_r(smz, 16) + (size_t)OA_LB * c->nz * c->ntype * sizeof(double2);
     if (smz > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
     cudaError_t e2 = oa_smem_limit(kern);
     if (e2 != cudaSuccess) return e2;
@@ -827,18 +884,22 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
                                        4.0 * c->alp_ewd * c->alp_ewd, c->gzvps_sum / c->vol,
                                        c->natm, c->ntype, c->atm_perm, toff, c->q_type, c->phase, c->kmax_tab,
                                        c->spl, c->nspl, c->spl_gmin, c->spl_dg,
-                                       c->red + 3 * oa_rho_xc_nblk());
+                                       c->red + 3 * oa_rho_xc_nblk(), forces ? c->ions->fpart : nullptr);
     return cudaGetLastError();
   };
   auto ldb2 = [&](int n1, int n2) { const int p = (n1 * (n2 | 1)) | 1; return p > c->nz + 1 ? p : c->nz + 1; };
   switch (c->nz) {
-#define OA_ZP(NN, A, B) case NN: e = zpass(k_rho_zpass<A, B>, ldb2(A, B)); break;
+#define OA_ZP(NN, A, B)                                                                      \
+  case NN:                                                                                   \
+    e = forces ? zpass(k_rho_zpass<A, B, true>, ldb2(A, B)) : zpass(k_rho_zpass<A, B, false>, ldb2(A, B)); \
+    break;
     OA_ZP(12, 4, 3) OA_ZP(20, 4, 5) OA_ZP(24, 6, 4) OA_ZP(36, 6, 6) OA_ZP(40, 8, 5) OA_ZP(64, 8, 8)
     OA_ZP(96, 12, 8) OA_ZP(108, 12, 9) OA_ZP(160, 16, 10)
 #undef OA_ZP
     default: e = cudaErrorNotSupported; break;
   }
-  if (e == cudaErrorNotSupported) e = zpass(k_rho_zpass<0, 0>, c->nz + 1);
+  if (e == cudaErrorNotSupported)
+    e = forces ? zpass(k_rho_zpass<0, 0, true>, c->nz + 1) : zpass(k_rho_zpass<0, 0, false>, c->nz + 1);
   if (e != cudaSuccess) return e;
   // white-byrd: V_KS z-lines -= z^-1 (i g . h(g))
   if (c->gga && (e = gga_z(c, s, 1)) != cudaSuccess) return e;

@@ -53,14 +53,15 @@ cudaError_t oa_step_ortho_args(oa_ctx* c, double** work, int** status, double** 
 // per-step record: the 16 energy accumulators, NS iterations, converged,
 // residual, max|S - 2I|
 #define OA_REC 20
-#define OA_NREC_OUT 12  // values per step handed back (oa_gpu_cp_step)
+#define OA_NREC_OUT 14  // values per step handed back (oa_gpu_cp_step)
 
 // one step record -> EKE EHART EEXT EWALD EEXC MUXC FICT ENL, Newton-Schulz
-// iterations, residual, max|S - 2I|, EGGA
+// iterations, residual, max|S - 2I|, EGGA, ionic KE, real-space Ewald
 static void fill_energies(const double* hv, double* eo) {
   eo[0] = hv[OA_E_EKE]; eo[1] = hv[OA_E_EHART]; eo[2] = hv[OA_E_EEXT]; eo[3] = hv[OA_E_EWALD];
   eo[4] = hv[8] + hv[9]; eo[5] = hv[OA_E_MUXC]; eo[6] = hv[OA_E_FICT]; eo[7] = hv[OA_E_ENL];
   eo[8] = hv[16]; eo[9] = hv[18]; eo[10] = hv[19]; eo[11] = hv[11] + hv[12];
+  eo[12] = hv[OA_E_ION_KE]; eo[13] = hv[OA_E_EWALD_REAL];
 }
 
 struct oa_step_scratch {
@@ -190,6 +191,15 @@ static oa_status launch_step_a(oa_ctx* c, cudaStream_t s, oa_cp_state* st, int c
   }
   // integrateModForce; psi(t) is psi itself after the previous step's PsiV reset
   OA_STEP_TRY(oa_integrate_sel(c, s, w->F2, st->vpsi, st->psi_t, st->psi, w->flag, st->dt, complete_prev, nullptr));
+  // ion dynamics: real-space Ewald and the atom integration with this
+  // step's forces (AtomsCompute::integrateAtoms); the next step's phase
+  // tables, structure factors and B-splines see the new positions
+  if (c->ions) {
+    double *work, *errv, *dev_e, *hv, *eye;
+    int *status, *hs, grid;
+    OA_CUDA_TRY(oa_step_ortho_args(c, &work, &status, &errv, &grid, &dev_e, &hs, &hv, &eye));
+    OA_CUDA_TRY(oa_launch_ion_step(c, s, dev_e, st->dt, complete_prev));
+  }
   // computeNewPsi: S (FP64 DMMA in both forms)
   OA_STEP_TRY(oa_gpu_pc_forward(c, s, st->psi_t, st->psi_t, 2.0, 0.5, w->S));
   return OA_OK;
@@ -244,6 +254,10 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
   // the cluster Newton-Schulz kernel is an ordinary launch: then the whole
   // step is one graph; the cooperative one splits it in two
   const bool ns_in_graph = oa_ns_capturable(c) != 0;
+  if (pos_host && c->ions) {
+    oa_set_error("pos_host with ion dynamics on: the atoms move on the device", __FILE__, __LINE__);
+    return OA_ERR_BAD_ARG;
+  }
   for (int k = 0; k < nsteps; ++k) {
     if (pos_host)
       OA_CUDA_TRY(cudaMemcpyAsync(c->pos, pos_host + (size_t)k * 3 * c->natm, (size_t)3 * c->natm * sizeof(double),

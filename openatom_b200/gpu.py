@@ -47,7 +47,7 @@ class SystemDesc(C.Structure):
 
 
 STEP_KEYS = ("EKE", "EHART", "EEXT", "EWALD_RECIP", "EEXC", "MUXC", "FICT_KE", "ENL", "ORTHO_ITERS",
-             "ORTHO_ERR", "SMAX", "EGGA")
+             "ORTHO_ERR", "SMAX", "EGGA", "ION_KE", "EWALD_REAL")
 NREC = len(STEP_KEYS)
 XC_FUNCTIONALS = {"pz_lda": 0, "blyp": 1}
 
@@ -84,6 +84,8 @@ SIGNATURES = {
     "oa_gpu_integrate": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_double, C.c_int, _vp]),
     "oa_gpu_energies": (C.c_int, [_vp, _vp, _dp]),
     "oa_gpu_set_xc": (C.c_int, [_vp, C.c_int, C.c_double]),
+    "oa_gpu_set_ions": (C.c_int, [_vp, _dp, _dp]),
+    "oa_gpu_get_ions": (C.c_int, [_vp, _vp, _dp, _dp]),
     "oa_gpu_psiv_reset": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "oa_gpu_psiv_reset_mixed": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int]),
     "oa_gpu_cp_run_batch": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int, _vp, C.c_int,
@@ -219,6 +221,26 @@ class CPContext:
         xc = getattr(sysm, "xc", "pz_lda")
         if xc != "pz_lda":
             self.set_xc(xc, getattr(sysm, "gga_cut", 5.0e-5))
+
+    def set_ions(self, masses, vel=None):
+        """Turn on ion dynamics in the native step (oa_gpu_set_ions): masses
+        [natm] in electron masses, velocities [natm, 3] (None: zero)."""
+        m = np.ascontiguousarray(masses, dtype=np.float64)
+        if m.shape != (self.sys.natm,):
+            raise ValueError("masses must have shape (natm,)")
+        v = None
+        if vel is not None:
+            v = np.ascontiguousarray(vel, dtype=np.float64)
+            if v.shape != (self.sys.natm, 3):
+                raise ValueError("vel must have shape (natm, 3)")
+        _check(self._lib.oa_gpu_set_ions(self._h, m.ctypes.data_as(_dp), None if v is None else v.ctypes.data_as(_dp)))
+
+    def get_ions(self):
+        """(positions, velocities) of the atoms, host arrays [natm, 3]."""
+        pos = np.zeros((self.sys.natm, 3))
+        vel = np.zeros((self.sys.natm, 3))
+        _check(self._lib.oa_gpu_get_ions(self._h, self._stream(), pos.ctypes.data_as(_dp), vel.ctypes.data_as(_dp)))
+        return pos, vel
 
     def set_xc(self, functional: str, gradient_cutoff: float = 5.0e-5):
         """Exchange-correlation of the density path: "pz_lda" or "blyp"
@@ -414,9 +436,10 @@ class CPContext:
         _check(self._lib.oa_gpu_nl_ees(self._h, self._stream(), _ptr(psi), _ptr(fnl_out), _ptr(enl_out)))
 
     def energies(self) -> dict:
-        out = (C.c_double * 9)()
+        out = (C.c_double * 11)()
         _check(self._lib.oa_gpu_energies(self._h, self._stream(), out))
-        keys = ("EKE", "EHART", "EEXT", "EWALD_RECIP", "EEXC", "MUXC", "FICT_KE", "ENL", "EGGA")
+        keys = ("EKE", "EHART", "EEXT", "EWALD_RECIP", "EEXC", "MUXC", "FICT_KE", "ENL", "EGGA", "ION_KE",
+                "EWALD_REAL")
         return {k: float(v) for k, v in zip(keys, out)}
 
 
