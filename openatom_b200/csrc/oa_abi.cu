@@ -353,6 +353,15 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
           oa_pair_plane_supported(d->nx, c->nkx_s, d->nlines, c->ldl) && column_runs(d, c->nkx_s, &runs))
         TRY(upload(&c->pair_cols, runs.data(), runs.size()));
     }
+    if (c->pair_cols) {
+      // charge partials of the z forward pass (state x 16-line block) and of
+      // the pair density pass (group x plane) for the density renormalisation
+      c->nq = d->nstate * ((d->nlines + OA_LB - 1) / OA_LB);
+      c->nq2 = c->ngroup_pair * d->nz;
+      TRY(cudaMalloc(&c->qpart, (size_t)c->nq * sizeof(double)));
+      TRY(cudaMalloc(&c->qpart2, (size_t)c->nq2 * sizeof(double)));
+      TRY(cudaMalloc(&c->qscale, sizeof(double)));
+    }
     {
       const int ng = c->ngroup > c->ngroup_pair ? c->ngroup : c->ngroup_pair;
       TRY(cudaMalloc(&c->rho_part, (size_t)ng * c->npts * sizeof(double)));
@@ -441,7 +450,7 @@ extern "C" oa_status oa_gpu_destroy(oa_ctx* c) {
                  p->partner, p->cmass, p->ke_part, p->dev_e, p->mat_a, p->mat_x, p->eye, p->vtmp, p->upart,
                  p->pl_big[0], p->pl_big[1], p->pl_big[2], p->pl_ma, p->pl_mb,
                  p->err_flag, c->ky, c->kz, c->nl_atm, c->nl_spl, c->nl_vnorm, c->nl_gz0, c->sf, c->zmat, c->zt,
-                 c->enl, c->enl_eke, c->grad, c->dzg};
+                 c->enl, c->enl_eke, c->grad, c->dzg, c->qpart, c->qpart2, c->qscale};
   for (void* q : dev) if (q) cudaFree(q);
   if (p->h_status) cudaFreeHost(p->h_status);
   if (p->h_vals) cudaFreeHost(p->h_vals);

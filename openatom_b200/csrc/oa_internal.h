@@ -39,6 +39,15 @@ struct oa_ees {
   double* enl;         // [nstate]
 };
 
+// Per-block charge partials of the mixed z forward pass: sum over the
+// block's coefficients of occ_s w |c|^2 (w = 1 on the kx = 0 lines, whose
+// two halves are both stored, 2 elsewhere); part = null: none
+struct OaCharge {
+  const int* line_kx;
+  const double* occ;
+  double* part;
+};
+
 // Ion dynamics (oa_gpu_set_ions): masses, velocities and the force pieces of
 // one step, summed by the integrator in a fixed order
 struct oa_ions {
@@ -126,6 +135,11 @@ struct oa_ctx {
   double *grad;           // [3][nz][ny][nx] grad rho, then the GGA vector h (BLYP)
   void *dzg;              // [3][nz][ldl_d] C  z-lines of grad rho / h (BLYP)
   oa_ions *ions;          // ion dynamics, after oa_gpu_set_ions
+  // mixed form: the FP32 density renormalised to the exact electron count
+  // (charge partials of the z forward pass and of the pair density pass)
+  double *qpart, *qpart2, *qscale;
+  int nq, nq2;
+  int qvalid;             // the last density pass wrote both partial sets
 };
 
 enum { OA_E_EKE = 0, OA_E_EHART, OA_E_EEXT, OA_E_EWALD, OA_E_EEXC, OA_E_MUXC, OA_E_ENL, OA_E_FICT };

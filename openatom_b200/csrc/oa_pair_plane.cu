@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(PairCfg<N1, N2>::NT, 1)
 k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int nlines,
                const int4* __restrict__ cols, int nkx, const double2* __restrict__ twg,
                const double* __restrict__ occ, double* __restrict__ rho_part, int ngroup,
-               float2* __restrict__ psir, PairSmem L) {
+               float2* __restrict__ psir, PairSmem L, double* __restrict__ qpart) {
   typedef PairCfg<N1, N2> CF;
   constexpr int N = CF::N, NT = CF::NT, XBW = CF::XBW;
   constexpr int LDY = CF::LDY, LS1 = CF::LS1, PS1 = CF::PS1;
@@ -245,14 +245,23 @@ k_pair_density(const float2* __restrict__ zbuf, int nstate, int nz, int ldl, int
       for (int it = tid; it < 16 * npc; it += NT) y_b(it);
   }
   double* out = rho_part + ((size_t)g * nz + z) * N * N;
+  double q = 0.0;  // this block's share of sum_r occ |psi(r)|^2 (the FP32 charge)
 #pragma unroll
   for (int j = 0; j < XBW; ++j) {
     const int it = tid + NT * j;
     const int y = it >> 4, k1 = it & 15;
     if (k1 < N1) {
 #pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) out[y * N + k1 + N1 * k2] = (double)dens[j][k2];
+      for (int k2 = 0; k2 < N2; ++k2) {
+        out[y * N + k1 + N1 * k2] = (double)dens[j][k2];
+        q += (double)dens[j][k2];
+      }
     }
+  }
+  if (qpart) {
+    __shared__ double qsh[32];
+    q = block_sum(q, qsh);
+    if (tid == 0) qpart[(size_t)g * nz + z] = q;
   }
 }
 
@@ -433,7 +442,7 @@ static PairSmem pair_layout(int nkx, int nlines, int mode) {
 template <int N1, int N2>
 static cudaError_t pair_launch(int mode, cudaStream_t st, void* zbuf, int nstate, int nz, int ldl, int nlines,
                                const int* cols, int nkx, const double2* tw, const double* occ, const void* vks,
-                               double* rho_part, int ngroup, void* psir, int kymax) {
+                               double* rho_part, int ngroup, void* psir, int kymax, double* qpart) {
   typedef PairCfg<N1, N2> CF;
   if (CF::XBW == 0 || N1 > 16 || 2 * nkx > CF::N + 2 || (ldl & 1)) return cudaErrorNotSupported;
   const PairSmem L = pair_layout<N1, N2>(nkx, nlines, mode);
@@ -449,7 +458,7 @@ static cudaError_t pair_launch(int mode, cudaStream_t st, void* zbuf, int nstate
       cudaError_t e2 = oa_smem_limit(kern);
       if (e2 != cudaSuccess) return e2;
       kern<<<grid, CF::NT, L.total, st>>>((const float2*)zbuf, nstate, nz, ldl, nlines, (const int4*)cols, nkx, tw,
-                                          occ, rho_part, ngroup, (float2*)psir, L);
+                                          occ, rho_part, ngroup, (float2*)psir, L, qpart);
       return cudaGetLastError();
     };
     if constexpr (N1 % 4 == 0) {
@@ -479,16 +488,18 @@ static cudaError_t pair_launch(int mode, cudaStream_t st, void* zbuf, int nstate
     default: break;                                                  \
   }
 
-// mode 0: density pass (rho_part[group][z][y][x], psi(r) pairs stored);
+// mode 0: density pass (rho_part[group][z][y][x], psi(r) pairs stored;
+// qpart, when not null: [group][z] block sums of sum_r occ |psi(r)|^2);
 // mode 4: V_KS pass from those psi(r) pairs.  nx = ny = n; cols = per kx
 // column {first line, ky of the first line, line count, 0}; kymax = the
 // largest |ky| of the lines.  Returns
 // cudaErrorNotSupported when n or the shared memory has no pair kernel.
 cudaError_t oa_pair_plane(int mode, cudaStream_t st, int n, void* zbuf, int nstate, int nz, int ldl, int nlines,
                           const int* cols, int nkx, const double2* tw, const double* occ, const void* vks,
-                          double* rho_part, int ngroup, void* psir, int kymax) {
-#define OA_CALL(A, B) \
-  pair_launch<A, B>(mode, st, zbuf, nstate, nz, ldl, nlines, cols, nkx, tw, occ, vks, rho_part, ngroup, psir, kymax)
+                          double* rho_part, int ngroup, void* psir, int kymax, double* qpart) {
+#define OA_CALL(A, B)                                                                                          \
+  pair_launch<A, B>(mode, st, zbuf, nstate, nz, ldl, nlines, cols, nkx, tw, occ, vks, rho_part, ngroup, psir, kymax, \
+                    qpart)
   OA_PAIR_DISPATCH(n, OA_CALL)
 #undef OA_CALL
   return cudaErrorNotSupported;

@@ -66,11 +66,12 @@ __global__ void __launch_bounds__(OA_NTHREADS)
 k_zfwd2(const double2* __restrict__ psi, int ng, int s0, const int* __restrict__ line_off,
         const int* __restrict__ line_nneg, const int* __restrict__ line_npos, int nlines,
         typename CplxOf<R>::T* __restrict__ zbuf, int ldl, const double2* __restrict__ twz,
-        const double2* __restrict__ dyp, int zseg) {
+        const double2* __restrict__ dyp, int zseg, OaCharge qc) {
   typedef typename CplxOf<R>::T C;
   constexpr int N = N1 * N2;
   typedef PencilLd<N1, N2> L;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double qsh[32];
   C* tw = (C*)smem_raw;
   C* s1 = tw + align_up(N, 2);
   // zseg > 0: the block's lines are one contiguous run of the coefficients,
@@ -87,10 +88,12 @@ k_zfwd2(const double2* __restrict__ psi, int ng, int s0, const int* __restrict__
   }
   load_twiddles(tw, twz, N);
   __syncthreads();
+  double q = 0.0;  // charge partial (qc.part)
   for (int it = threadIdx.x; it < nb * N2; it += blockDim.x) {
     const int lb = it / N2, n2 = it - lb * N2;
     const int l = l0 + lb;
     const int off = line_off[l], nn = line_nneg[l], np = line_npos[l];
+    const double wq = (qc.part && qc.line_kx[l] != 0) ? 2.0 : 1.0;
     C u[N1];
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1) {
@@ -98,6 +101,7 @@ k_zfwd2(const double2* __restrict__ psi, int ng, int s0, const int* __restrict__
       double2 v = make_double2(0.0, 0.0);
       if (i >= 0) {
         v = zseg > 0 ? seg[off - g0 + i] : ps[off + i];
+        q += wq * (v.x * v.x + v.y * v.y);
         if (dyp) {  // EES projector: projPsiG = conj(dyp psi) (eesProjGchare)
           const double2 d = dyp[off + i];
           v = make_double2(d.x * v.x - d.y * v.y, -(d.y * v.x + d.x * v.y));
@@ -120,6 +124,10 @@ k_zfwd2(const double2* __restrict__ psi, int ng, int s0, const int* __restrict__
     RDft<N2, -1>::run(w);
 #pragma unroll
     for (int k2 = 0; k2 < N2; ++k2) out[(size_t)(k1 + N1 * k2) * ldl + lb] = w[k2];
+  }
+  if (qc.part) {
+    q = block_sum(q, qsh);
+    if (threadIdx.x == 0) qc.part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = qc.occ[s] * q;
   }
 }
 
@@ -556,22 +564,22 @@ static size_t zpass2_smem(int zseg, int nseg) {
 template <typename R, int N1, int N2>
 static cudaError_t zfwd2_n(cudaStream_t st, const double2* psi, int ng, int s0, int ns, const int* off,
                            const int* nneg, const int* npos, int nlines, void* zbuf, int ldl, const double2* tw,
-                           const double2* dyp, int zseg) {
+                           const double2* dyp, int zseg, OaCharge qc) {
   typedef typename CplxOf<R>::T C;
   const size_t sm = zpass2_smem<R, N1, N2>(zseg, 1);
   cudaError_t e = oa_smem_limit(k_zfwd2<R, N1, N2>);
   if (e != cudaSuccess) return e;
   dim3 grid((nlines + OA_LB - 1) / OA_LB, ns);
   k_zfwd2<R, N1, N2><<<grid, OA_NTHREADS, sm, st>>>(psi, ng, s0, off, nneg, npos, nlines, (C*)zbuf, ldl, tw, dyp,
-                                                     zseg);
+                                                     zseg, qc);
   return cudaGetLastError();
 }
 
 template <typename R>
 static cudaError_t zfwd2(cudaStream_t st, int n, const double2* psi, int ng, int s0, int ns, const int* off,
                          const int* nneg, const int* npos, int nlines, void* zbuf, int ldl, const double2* tw,
-                         const double2* dyp, int zseg) {
-#define OA_CALL(A, B) zfwd2_n<R, A, B>(st, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg)
+                         const double2* dyp, int zseg, OaCharge qc) {
+#define OA_CALL(A, B) zfwd2_n<R, A, B>(st, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg, qc)
   OA_PENCIL_DISPATCH(n, OA_CALL)
 #undef OA_CALL
   return cudaErrorNotSupported;
@@ -579,10 +587,10 @@ static cudaError_t zfwd2(cudaStream_t st, int n, const double2* psi, int ng, int
 
 cudaError_t oa_pencil_zfwd(int precision, cudaStream_t st, int n, const double2* psi, int ng, int s0, int ns,
                            const int* off, const int* nneg, const int* npos, int nlines, void* zbuf, int ldl,
-                           const double2* tw, const double2* dyp, int zseg) {
+                           const double2* tw, const double2* dyp, int zseg, OaCharge qc) {
   return precision == OA_FP64
-             ? zfwd2<double>(st, n, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg)
-             : zfwd2<float>(st, n, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg);
+             ? zfwd2<double>(st, n, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg, qc)
+             : zfwd2<float>(st, n, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg, qc);
 }
 
 template <typename R, int N1, int N2>

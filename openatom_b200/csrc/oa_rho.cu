@@ -49,8 +49,11 @@ __host__ __device__ static inline size_t align_up_r(size_t x, size_t a) { return
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(OA_NTHREADS)
 k_rho_xc(const double* __restrict__ rho_part, int ngroup, size_t npts, double rvol, double cfac,
-         double* __restrict__ rho, double* __restrict__ vxc, double* __restrict__ part) {
-  // cfac = 0 drops the PZ correlation (LYP correlation on, cp_pz_lda.C:66)
+         const double* __restrict__ qscale, double* __restrict__ rho, double* __restrict__ vxc,
+         double* __restrict__ part) {
+  // cfac = 0 drops the PZ correlation (LYP correlation on, cp_pz_lda.C:66);
+  // qscale (mixed form): the renormalisation to the exact electron count
+  if (qscale) rvol *= qscale[0];
   __shared__ double sh[3 * 32];
   // Perdew-Zunger constants (cp_pz_lda.C:46-52)
   const double gamma = -0.14230, beta1 = 1.05290, beta2 = 0.33340;
@@ -751,10 +754,30 @@ size_t oa_rho_plane_smem_bytes(int nx, int ny, int nkx, int npair, int ychunk) {
   return rho_plane_layout(nx, ny, nkx, npair, ychunk).total;
 }
 
+// Mixed form: the FP32 transforms scale the density by about 1 - 1.4e-7
+// (a uniform gain error); the density is renormalised to the electron count
+// of the FP64 coefficients, Q = sum_s occ_s sum_g w |c_sg|^2, against the
+// FP32 density's own sum_r rho V/N.  One block, fixed summation order.
+__global__ void k_charge_scale(const double* __restrict__ qexact, int n1, const double* __restrict__ q32, int n2,
+                               double rnpts, double* __restrict__ scale) {
+  __shared__ double sh[2 * 32];
+  double v[2] = {0.0, 0.0};
+  for (int i = threadIdx.x; i < n1; i += blockDim.x) v[0] += qexact[i];
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) v[1] += q32[i];
+  block_sum_n<2>(v, sh);
+  if (threadIdx.x == 0) scale[0] = (v[1] > 0.0) ? v[0] / (v[1] * rnpts) : 1.0;
+}
+
 cudaError_t oa_launch_rho_xc(oa_ctx* c, cudaStream_t s) {
   const int nblk = 4 * 148;
+  const bool renorm = c->qvalid == 2;
+  if (renorm) {
+    k_charge_scale<<<1, 1024, 0, s>>>(c->qpart, c->nq, c->qpart2, c->nq2, 1.0 / (double)c->npts, c->qscale);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   k_rho_xc<<<nblk, OA_NTHREADS, 0, s>>>(c->rho_part, c->rho_ngroup, (size_t)c->npts, 1.0 / c->vol,
-                                        c->gga ? 0.0 : 1.0, c->rho, c->vxc, c->red);
+                                        c->gga ? 0.0 : 1.0, renorm ? c->qscale : nullptr, c->rho, c->vxc, c->red);
   return cudaGetLastError();
 }
 

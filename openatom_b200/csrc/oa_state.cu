@@ -357,7 +357,7 @@ int oa_pencil_supported(int n);
 size_t oa_pencil_plane_smem(int precision, int n, int nkx);
 cudaError_t oa_pencil_zfwd(int precision, cudaStream_t st, int n, const double2* psi, int ng, int s0, int ns,
                            const int* off, const int* nneg, const int* npos, int nlines, void* zbuf, int ldl,
-                           const double2* tw, const double2* dyp, int zseg);
+                           const double2* tw, const double2* dyp, int zseg, OaCharge qc);
 cudaError_t oa_pencil_zbwd(int precision, cudaStream_t st, int n, const void* zbuf, int ldl, int nlines,
                            const int* lkx, const int* off, const int* nneg, const int* npos, const double2* tw,
                            const double2* psi, const double2* fnl, double2* force, const double* g2,
@@ -365,7 +365,7 @@ cudaError_t oa_pencil_zbwd(int precision, cudaStream_t st, int n, const void* zb
                            int nblk, const double2* dyp, OaPlaneOut po, int zseg);
 cudaError_t oa_pair_plane(int mode, cudaStream_t st, int n, void* zbuf, int nstate, int nz, int ldl, int nlines,
                           const int* cols, int nkx, const double2* tw, const double* occ, const void* vks,
-                          double* rho_part, int ngroup, void* psir, int kymax);
+                          double* rho_part, int ngroup, void* psir, int kymax, double* qpart);
 cudaError_t oa_pencil_plane(int precision, int mode, cudaStream_t st, int n, void* zbuf, int nstate, int ldl,
                             int nlines, const int* lkx, const int* lky, int nz, int nkx, const double2* tw,
                             const double* occ, const void* vks, double* rho_part, int ngroup, const EesArgs& E,
@@ -429,9 +429,16 @@ int oa_plane_blocks_per_sm(int precision) {
 }
 
 cudaError_t oa_launch_state_zfwd(oa_ctx* c, cudaStream_t s, const double2* psi, int s0, int ns) {
-  if (oa_pencil_supported(c->nz))
+  if (oa_pencil_supported(c->nz)) {
+    // mixed form, all states: the exact charge partials for the density
+    // renormalisation ride along
+    OaCharge qc = {nullptr, nullptr, nullptr};
+    if (c->qpart && s0 == 0 && ns == c->nstate) qc = OaCharge{c->line_kx, c->occ, c->qpart};
+    c->qvalid = qc.part ? 1 : 0;
     return oa_pencil_zfwd(c->precision, s, c->nz, psi, c->ng, s0, ns, c->line_off, c->line_nneg, c->line_npos,
-                          c->nlines, c->zbuf, c->ldl, c->tw_z, nullptr, c->zseg);
+                          c->nlines, c->zbuf, c->ldl, c->tw_z, nullptr, c->zseg, qc);
+  }
+  c->qvalid = 0;
   return c->precision == OA_FP64 ? launch_zfwd<double>(c, s, psi, s0, ns) : launch_zfwd<float>(c, s, psi, s0, ns);
 }
 static cudaError_t pencil_plane(oa_ctx* c, cudaStream_t s, int mode, void* psir) {
@@ -452,8 +459,9 @@ cudaError_t oa_launch_state_plane_density(oa_ctx* c, cudaStream_t s) {
   if (c->pair_cols && c->psir) {
     const cudaError_t e = oa_pair_plane(0, s, c->nx, c->zbuf, c->nstate, c->nz, c->ldl, c->nlines, c->pair_cols,
                                         c->nkx_s, c->tw_x, c->occ, nullptr, c->rho_part, c->ngroup_pair, c->psir,
-                                        c->pair_kymax);
+                                        c->pair_kymax, c->qvalid ? c->qpart2 : nullptr);
     c->psir_valid = e == cudaSuccess ? 2 : 0;
+    if (e == cudaSuccess && c->qvalid) c->qvalid = 2;
     c->rho_ngroup = c->ngroup_pair;
     if (e != cudaErrorNotSupported) return e;
   }
@@ -466,7 +474,7 @@ cudaError_t oa_launch_state_plane_density(oa_ctx* c, cudaStream_t s) {
 cudaError_t oa_launch_state_plane_vks(oa_ctx* c, cudaStream_t s) {
   if (c->psir_valid == 2)
     return oa_pair_plane(4, s, c->nx, c->zbuf, c->nstate, c->nz, c->ldl, c->nlines, c->pair_cols, c->nkx_s,
-                         c->tw_x, c->occ, c->vks, nullptr, c->ngroup_pair, c->psir, c->pair_kymax);
+                         c->tw_x, c->occ, c->vks, nullptr, c->ngroup_pair, c->psir, c->pair_kymax, nullptr);
   const cudaError_t e = c->psir_valid ? pencil_plane(c, s, 4, c->psir) : pencil_plane(c, s, 1, nullptr);
   if (e != cudaErrorNotSupported) return e;
   return c->precision == OA_FP64 ? launch_plane<double, 1>(c, s) : launch_plane<float, 1>(c, s);
@@ -498,7 +506,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
   // z pass forward with conj(dyp psi)
   if (pz) {
     err = oa_pencil_zfwd(c->precision, st, e->nc, psi, c->ng, 0, c->nstate, c->line_off, c->line_nneg, c->line_npos,
-                         c->nlines, e->zbuf, c->ldl, e->tw_c, e->dyp, c->zseg);
+                         c->nlines, e->zbuf, c->ldl, e->tw_c, e->dyp, c->zseg, OaCharge{nullptr, nullptr, nullptr});
     if (err != cudaSuccess) return err;
   } else {
     size_t sm = zpass_smem<R>(e->nc);

@@ -61,12 +61,24 @@ def test_ion_dynamics_fp64_matches_oracle(preset, nstate):
 
 
 def test_ion_dynamics_mixed_total_energy():
+    """Mixed form from a quenched start (30 damped FP64 steps on the GPU), as
+    in the mixed-form benchmark: the total energy within 1e-6 Ha/atom."""
     from openatom_b200.gpu import CPDriver
     s, m, vel = _start("w8", 16, 43)
-    d = CPDriver(s, "mixed", norb_tol=0.003)
+    q = CPDriver(s, "fp64")
+    q.quench(3)
+    q.quench(27, dt=10.0)
+    psi0 = q.psi.cpu().numpy()
+    q.ctx.close()
+    d = CPDriver(s, "mixed", psi0=psi0, norb_tol=0.003)
     d.ctx.set_ions(m, vel)
     got = d.run_native(d.native_state(use_graph=True), 5)
-    so, _, ions, ref = _oracle(s, vel, 5)
+    so = copy.deepcopy(s)
+    st = O.CPState(so)
+    st.psi_t = psi0.copy()
+    st.psi = psi0.copy()
+    ions = O.IonState(so, vel)
+    ref = [O.cp_step(st, so, norb_tol=0.003, ions=ions) for _ in range(5)]
     keys = ("EKE", "EHART", "EEXT", "EEXC", "ENL")
     for g, r in zip(got, ref):
         assert abs(sum(g[k] for k in keys) - sum(r[k] for k in keys)) / s.natm <= 1e-6

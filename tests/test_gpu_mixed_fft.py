@@ -52,6 +52,11 @@ def test_density_mixed(case):
     torch.cuda.synchronize()
     ref = O.density(O.state_g_to_r(s.psi, s), s)
     assert rel(rho.cpu().numpy(), ref) < 2e-6
+    # renormalised to the exact electron count of the FP64 coefficients
+    # (the FP32 transforms alone leave it about 1.4e-7 low)
+    q_exact = float(np.sum(s.occ * np.sum(s.kx_weight()[None, :] * np.abs(s.psi) ** 2, axis=1)))
+    q = rho.sum().item() * s.vol / s.npts
+    assert abs(q - q_exact) <= 1e-12 * q_exact, (q, q_exact)
 
 
 def test_forces_mixed(case):
