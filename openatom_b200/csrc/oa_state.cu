@@ -76,8 +76,11 @@ struct PlaneSmem {
   int ldw;  // per-warp buffer length (complex elements)
 };
 
+// gtile: the density / V_KS plane stays in global memory (the block's own
+// rho_part plane, or V_KS read in place) instead of shared memory: the
+// layout of planes too large for shared memory (FP64 at 160^3)
 template <typename C, typename T>
-static PlaneSmem plane_smem_layout(int nx, int ny, int nkx) {
+static PlaneSmem plane_smem_layout(int nx, int ny, int nkx, bool gtile = false) {
   PlaneSmem L;
   const int ldy = ny + 1;
   L.ldw = (nx > ny ? nx : ny) + 1;
@@ -85,7 +88,7 @@ static PlaneSmem plane_smem_layout(int nx, int ny, int nkx) {
   L.tw_x = o; o += align_up(nx * sizeof(C), 16);
   L.tw_y = o; o += align_up(ny * sizeof(C), 16);
   L.P = o; o += align_up((size_t)nkx * ldy * sizeof(C), 16);
-  L.tile = o; o += align_up((size_t)nx * ny * sizeof(T), 16);
+  L.tile = o; o += gtile ? 0 : align_up((size_t)nx * ny * sizeof(T), 16);
   L.wbuf = o; o += align_up((size_t)OA_PLANE_WARPS * 2 * L.ldw * sizeof(C), 16);
   L.total = o;
   return L;
@@ -106,13 +109,20 @@ k_state_plane(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int
               int nx, int ny, int nz, int nkx,
               OaFftPlan px, OaFftPlan py, const double2* __restrict__ twx, const double2* __restrict__ twy,
               const double* __restrict__ occ, const R* __restrict__ vks, double* __restrict__ rho_part,
-              int ngroup, PlaneSmem L, EesArgs E) {
+              int ngroup, PlaneSmem L, EesArgs E, int gtile) {
+  // gtile (MODE 0 / 1 with R = double): the tile is this block's rho_part
+  // plane (accumulated in place; each (group, plane) belongs to one block)
+  // or the V_KS plane itself
   typedef typename CplxOf<R>::T C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* stwx = (C*)(smem_raw + L.tw_x);
   C* stwy = (C*)(smem_raw + L.tw_y);
   C* P = (C*)(smem_raw + L.P);
   R* tile = (R*)(smem_raw + L.tile);
+  if (gtile) {
+    if (MODE == 0) tile = (R*)(rho_part + ((size_t)blockIdx.y * nz + blockIdx.x) * (size_t)nx * ny);
+    else tile = const_cast<R*>(vks) + (size_t)blockIdx.x * nx * ny;
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   C* wa = (C*)(smem_raw + L.wbuf) + (size_t)warp * 2 * L.ldw;
   C* wb = wa + L.ldw;
@@ -125,7 +135,7 @@ k_state_plane(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int
   load_twiddles(stwy, twy, ny);
   if (MODE == 0) {
     for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) tile[i] = (R)0;
-  } else if (MODE == 1) {
+  } else if (MODE == 1 && !gtile) {
     const R* vz = vks + (size_t)z * nx * ny;
     for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) tile[i] = vz[i];
   }
@@ -260,7 +270,7 @@ k_state_plane(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int
       __syncthreads();
     }
   }
-  if (MODE == 0) {
+  if (MODE == 0 && !gtile) {
     __syncthreads();
     double* out = rho_part + ((size_t)g * nz + z) * (size_t)nx * ny;
     for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) out[i] = (double)tile[i];
@@ -387,13 +397,17 @@ template <typename R, int MODE>
 static cudaError_t launch_plane(oa_ctx* c, cudaStream_t st) {
   typedef typename CplxOf<R>::T C;
   PlaneSmem L = plane_smem_layout<C, R>(c->nx, c->ny, c->nkx_s);
+  // FP64 planes beyond shared memory: the tile in global memory
+  const int gtile = (L.total > (size_t)OA_MAX_SMEM && sizeof(R) == 8) ? 1 : 0;
+  if (gtile) L = plane_smem_layout<C, R>(c->nx, c->ny, c->nkx_s, true);
+  if (L.total > (size_t)OA_MAX_SMEM) return cudaErrorNotSupported;
   cudaError_t e = oa_smem_limit(k_state_plane<R, MODE>);
   if (e != cudaSuccess) return e;
   dim3 grid(c->nz, c->ngroup);
   EesArgs E = {nullptr, nullptr, nullptr, nullptr, 0, 0};
   k_state_plane<R, MODE><<<grid, OA_PLANE_THREADS, L.total, st>>>(
       (C*)c->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky, c->nx, c->ny, c->nz, c->nkx_s,
-      c->plan_x, c->plan_y, c->tw_x, c->tw_y, c->occ, (const R*)c->vks, c->rho_part, c->ngroup, L, E);
+      c->plan_x, c->plan_y, c->tw_x, c->tw_y, c->occ, (const R*)c->vks, c->rho_part, c->ngroup, L, E, gtile);
   return cudaGetLastError();
 }
 
@@ -417,7 +431,10 @@ size_t oa_plane_smem_bytes(int precision, int nx, int ny, int nkx) {
     const size_t p = oa_pencil_plane_smem(precision, nx, nkx);
     if (p > 0 && p <= (size_t)OA_MAX_SMEM) return p;
   }
-  if (precision == OA_FP64) return plane_smem_layout<double2, double>(nx, ny, nkx).total;
+  if (precision == OA_FP64) {
+    const size_t t = plane_smem_layout<double2, double>(nx, ny, nkx).total;
+    return t <= (size_t)OA_MAX_SMEM ? t : plane_smem_layout<double2, double>(nx, ny, nkx, true).total;
+  }
   return plane_smem_layout<float2, float>(nx, ny, nkx).total;
 }
 
@@ -530,7 +547,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
     if (err != cudaSuccess) return err;
     k_state_plane<R, 2><<<pgrid, OA_PLANE_THREADS, L.total, st>>>(
         (C*)e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky, e->na, e->nb, e->nc, c->nkx_s, e->pa,
-        e->pb, e->tw_a, e->tw_b, c->occ, nullptr, nullptr, e->ngroup, L, E);
+        e->pb, e->tw_a, e->tw_b, c->occ, nullptr, nullptr, e->ngroup, L, E, 0);
     err = cudaGetLastError();
   }
   if (err != cudaSuccess) return err;
@@ -545,7 +562,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
     if (err != cudaSuccess) return err;
     k_state_plane<R, 3><<<pgrid, OA_PLANE_THREADS, L.total, st>>>(
         (C*)e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky, e->na, e->nb, e->nc, c->nkx_s, e->pa,
-        e->pb, e->tw_a, e->tw_b, c->occ, nullptr, nullptr, e->ngroup, L, E);
+        e->pb, e->tw_a, e->tw_b, c->occ, nullptr, nullptr, e->ngroup, L, E, 0);
     err = cudaGetLastError();
   }
   if (err != cudaSuccess) return err;

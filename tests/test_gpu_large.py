@@ -89,3 +89,22 @@ def test_mixed_matches_fp64_many_states():
     for a, b in zip(out["fp64"], out["mixed"]):
         de = abs(sum(a[k] for k in keys) - sum(b[k] for k in keys)) / (2 * s.nstate)
         assert de < per_electron, de
+
+
+def test_fp64_form_at_160():
+    """The FP64 form on the 160^3 grid of the large configuration (128 H2O,
+    70 Ry), with 32 states: its plane passes keep the density / V_KS plane
+    in global memory (an FP64 160 x 160 plane does not fit in shared memory
+    beside the y-FFT buffers).  One native step against the oracle, each
+    energy term to 1e-10 relative."""
+    from openatom_b200.gpu import CPDriver
+    from oracle import cp_oracle as O
+    s = make_system("w128", seed=5, nstate=32, ecut_mass=2.0, cmass0=400.0, dt=5.0)
+    d = CPDriver(s, "fp64", norb_tol=0.003)
+    got = d.run_native(d.native_state(use_graph=True), 2)
+    st = O.CPState(s)
+    ref = [O.cp_step(st, s, norb_tol=0.003) for _ in range(2)]
+    for i, (g, r) in enumerate(zip(got, ref)):
+        for k in ("EKE", "EHART", "EEXT", "EEXC", "ENL", "FICT_KE"):
+            assert abs(g[k] - r[k]) <= 1e-10 * max(1.0, abs(r[k])), (i, k, g[k], r[k])
+    d.ctx.close()
