@@ -378,7 +378,10 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     TRY(cudaMalloc(&c->eke_part, (size_t)d->nstate * c->nblk_z * sizeof(double)));
     p->nkb = 160;  // split-K partials: about one CTA per SM for a 128 x 128 product
     // split-K partials; also the block partials of the minimisation's |F|^2 (>= 1024)
-    TRY(cudaMalloc(&p->part, std::max((size_t)p->nkb * d->nstate * d->nstate, (size_t)1024) * sizeof(double)));
+    // (the nonlocal Z product is nstate x natm_nl: more columns than states
+    // when there are more nonlocal atoms than states)
+    TRY(cudaMalloc(&p->part, std::max((size_t)p->nkb * d->nstate * std::max(d->nstate, d->natm_nl), (size_t)1024) *
+                                 sizeof(double)));
     p->ns_grid = oa_ns_grid(d->nstate, c->device);
     p->ns_cluster = oa_ns_cluster_size(d->nstate);
     TRY(cudaMalloc(&p->ns_work, ((size_t)5 * d->nstate * d->nstate + p->ns_grid + 32) * sizeof(double)));
