@@ -374,9 +374,16 @@ PRESETS = {
 
 def make_system(preset: str = "w8", seed: int = 1234, nstate: int | None = None,
                 ecut_mass: float = 1.0e30, cmass0: float = 400.0, dt: float = 5.0,
-                xc: str = "pz_lda", **over) -> CPSystem:
+                xc: str = "pz_lda", pseudo: str = "shipped", **over) -> CPSystem:
+    """A seeded water system of a preset.  pseudo: "shipped" splines the
+    reference's O / H BLYP pseudopotentials (openatom_b200.pseudo, the
+    make_vps_splin algorithm) on this box's spline grid; "analytic" uses
+    Gaussian stand-ins (a Gaussian-smeared ion core and a Gaussian s
+    projector)."""
     if xc not in ("pz_lda", "blyp"):
         raise ValueError("xc must be 'pz_lda' or 'blyp'")
+    if pseudo not in ("shipped", "analytic"):
+        raise ValueError("pseudo must be 'shipped' or 'analytic'")
     p = dict(PRESETS[preset])
     p.update(over)
     nmol, box, ecut_ry, nfft = p["nmol"], p["box"], p["ecut_ry"], tuple(p["nfft"])
@@ -388,11 +395,17 @@ def make_system(preset: str = "w8", seed: int = 1234, nstate: int | None = None,
     (kx, ky, kz, lkx, lky, loff, lneg, lpos, nkx0, nred, nuni, nzero) = state_sphere(box, ecut_ry, nfft)
     f = TWO_PI / box
     g2 = f * f * (kx.astype(np.float64) ** 2 + ky ** 2 + kz ** 2)
-    gmax = math.sqrt(4.0 * ecut_ry) * 1.05 + 0.5
-    vloc, gz = gaussian_vloc_table([6.0, 1.0], [0.247, 0.2], gmax)
-    # O: one s-channel KB projector; H: local only (data/DATABASE/pi_md.vps)
-    nl_proj, nl_gz0 = gaussian_nl_table([12.0, 0.0], [0.35, 0.35], gmax)
-    nl_vnorm = np.array([0.9, 0.0])
+    if pseudo == "shipped":
+        # O: one s-channel KB projector (p local); H: local only (data/DATABASE/pi_md.vps)
+        from .pseudo import shipped_water_tables
+        gmin_s, dg_s, vl, gz, pj, nl_vnorm, nl_gz0 = shipped_water_tables(box, ecut_ry)
+        vloc = SplineTable(gmin=float(gmin_s), dg=float(dg_s), coef=vl)
+        nl_proj = SplineTable(gmin=float(gmin_s), dg=float(dg_s), coef=pj)
+    else:
+        gmax = math.sqrt(4.0 * ecut_ry) * 1.05 + 0.5
+        vloc, gz = gaussian_vloc_table([6.0, 1.0], [0.247, 0.2], gmax)
+        nl_proj, nl_gz0 = gaussian_nl_table([12.0, 0.0], [0.35, 0.35], gmax)
+        nl_vnorm = np.array([0.9, 0.0])
     psi = random_coefficients(nstate, kx, ky, kz, g2, rng)
     cmass = create_mass(kx, g2, cmass0, ecut_mass)
     # Ewald splitting parameter: alpha = 3.5 / (L/2) style default (screening

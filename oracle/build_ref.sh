@@ -29,6 +29,8 @@ SRCS=(
   "$PINY/abinito_physics/cp_nonlocal/cp_ees_nonlocal.C"
   "$PINY/interface/cp_ewald/set_cp_ewald.C"
   "$PINY/abinito_physics/cp_ions/cp_rspace_ion.C"
+  "$PINY/interface/vps_params/control_vps_params.C"
+  "$PINY/friend_lib/friend_lib.C"
 )
 OBJS=()
 for s in "${SRCS[@]}"; do

@@ -13,6 +13,7 @@
 #include "../class_defs/allclass_gen.h"
 #include "../class_defs/allclass_cp.h"
 #include "../class_defs/allclass_mdatoms.h"
+#include "../class_defs/typedefs_par.h"
 #include "../class_defs/CP_OPERATIONS/class_cpnonlocal.h"
 #include "../class_defs/CP_OPERATIONS/class_cpxcfnctls.h"
 #include "../class_defs/CP_OPERATIONS/class_cplocal.h"
@@ -20,6 +21,7 @@
 #include "../class_defs/CP_OPERATIONS/class_cpintegrate.h"
 #include "../class_defs/CP_OPERATIONS/class_cprspaceion.h"
 #include <vector>
+#include <cstring>
 
 // y = alpha op(A) x + beta y, A column-major m x n (lda), op = 'T'/'t' or
 // 'N'/'n': the BLAS DGEMV / ZGEMV semantics the PINY nonlocal routines call
@@ -71,6 +73,23 @@ extern "C" void rs_(int*, int*, double*, double*, int*, double*, double*, double
   std::fprintf(stderr, "oracle/_ref: rs_ (EISPACK) is not provided\n");
   std::abort();
 }
+// the input-parsing and Gauss-Hermite routines of control_vps_params.C's
+// other functions (make_vps_splin of a LOC / KB type reaches none of them)
+#define OA_SHIM_ABSENT(sig)                                                   \
+  sig {                                                                       \
+    std::fprintf(stderr, "oracle/_ref: %s is not provided\n", #sig);         \
+    std::abort();                                                             \
+  }
+OA_SHIM_ABSENT(void keyarg_barf(DICT_WORD*, char*, char*, int))
+OA_SHIM_ABSENT(int** cmall_int_mat(long, long, long, long, const char*))
+OA_SHIM_ABSENT(void search_base_vps(char*, CVPS*, DICT_WORD*, int, DICT_WORD**, DICT_WORD*, int, int*))
+OA_SHIM_ABSENT(void set_grimme_dict(DICT_WORD**, int*, int))
+OA_SHIM_ABSENT(void set_potfun_dict(DICT_WORD**, int*, int))
+OA_SHIM_ABSENT(void set_potvps_dict(DICT_WORD**, int*, int))
+OA_SHIM_ABSENT(void search_base_grimme(char*, CVPS*, DICT_WORD*, int, DICT_WORD**, DICT_WORD*, int, int*))
+OA_SHIM_ABSENT(void limit_gauss_hermite(int*, double*, double*))
+OA_SHIM_ABSENT(void weight_node_gauss_hermite(int, double*, double*))
+OA_SHIM_ABSENT(double** cmall_mat(long, long, long, long, const char*))
 double getdeth(double*) {
   std::fprintf(stderr, "oracle/_ref: getdeth is not provided\n");
   std::abort();
@@ -658,4 +677,39 @@ extern "C" void ref_rspace_ion(int natm, const double* pos, const double* q, dou
   double recip = 0.0, grimme = 0.0;
   CPRSPACEION::CP_getionforce(natm, &fa, 0, 1, e_real, e_self, e_bgr, &recip, &scr, &grimme);
   for (int a = 0; a < natm; ++a) { fatm[3 * a] = fx[a]; fatm[3 * a + 1] = fy[a]; fatm[3 * a + 2] = fz[a]; }
+}
+
+void make_vps_splin(char*, int, int, int, int, double, double, double, double, double*, double*, double*, double*,
+                    double*, double*, double*, double*, double*, double*, double*, double*, int, int, int, int, int, int,
+                    double, int, int, int*, double*, double*);
+
+// make_vps_splin (interface/vps_params/control_vps_params.C:690-1262) for
+// one LOC (ivps_label 0) or KB (1) atom type read from a .pseud file, no
+// pressure tensor, no dual grid, one radial channel per l.  Outputs per
+// angular channel l = 0..n_ang the spline [nspl][4] at vps[l][nspl][4]
+// (the local table in the loc_opt slot), gzvps, gzvps0 (l = 0 KB), q and
+// vpsnorm[l].
+extern "C" int ref_vps_splin(const char* file, int loc_opt, int n_ang, int ivps_label, int nspl, double dg,
+                             double gmin_spl, double gmax_spl, double gmin_true, double* vps, double* gzvps,
+                             double* gzvps0, double* q, double* vpsnorm) {
+  const size_t len = (size_t)(n_ang + 1) * nspl + 1;
+  std::vector<double> v0(len, 0.0), v1(len, 0.0), v2(len, 0.0), v3(len, 0.0);
+  std::vector<double> nrm(n_ang + 2, 0.0), gz0(2, 0.0);
+  double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0, gz = 0.0, qq = 0.0;
+  int ngh = 0;
+  std::vector<char> name(file, file + std::strlen(file) + 1);
+  make_vps_splin(name.data(), loc_opt, n_ang, ivps_label, nspl, dg, gmin_spl, gmax_spl, gmin_true, v0.data(),
+                 v1.data(), v2.data(), v3.data(), &d0, &d1, &d2, &d3, &gz, gz0.data(), &qq, nrm.data(), 1, 1, 1, 1, 0,
+                 0, 1.0, 1, 0, &ngh, nullptr, nullptr);
+  for (int l = 0; l <= n_ang; ++l)
+    for (int j = 0; j < nspl; ++j) {
+      const size_t i = (size_t)l * nspl + j + 1;
+      double* o = vps + ((size_t)l * nspl + j) * 4;
+      o[0] = v0[i]; o[1] = v1[i]; o[2] = v2[i]; o[3] = v3[i];
+    }
+  *gzvps = gz;
+  *gzvps0 = gz0[1];
+  *q = qq;
+  for (int l = 0; l <= n_ang; ++l) vpsnorm[l] = nrm[l + 1];
+  return 0;
 }

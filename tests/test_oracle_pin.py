@@ -342,3 +342,48 @@ def test_rspace_ewald_pinned(ref, sysm):
     assert abs(es.value - e_s) <= 1e-13 * abs(e_s)
     assert abs(eb.value - e_b) <= 1e-13 * abs(e_b)
     assert np.max(np.abs(fatm - f_or)) <= 1e-12 * np.max(np.abs(f_or))
+
+
+@pytest.mark.parametrize("name,loc_opt,n_ang,label", [("O", 1, 1, 1), ("H", 0, 0, 0)])
+def test_pseudopotential_splines_pinned(ref, name, loc_opt, n_ang, label):
+    """make_vps_splin / slow_bess_vps / spline_fit (control_vps_params.C,
+    friend_lib.C) on the shipped O (KB, s nonlocal, p local) and H (local)
+    BLYP pseudopotentials, on the spline grid of the 8-water box at 70 Ry,
+    against openatom_b200.pseudo: the tabulated values, the spline
+    evaluated between the knots, the g = 0 limits, the charge and the KB
+    norm.  Also checks that the packaged radial data equal the files."""
+    from openatom_b200 import pseudo as P
+    path = f"/root/reference/data/DATABASE/{name}_BLYP_PP30.pseud"
+    ref.ref_vps_splin.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                  C.c_double, C.c_double, dp, dp, dp, dp, dp]
+    grid = P.spline_grid(11.7, 70.0)
+    gmin, gmin_spl, dg, nspl = grid
+    vps = np.zeros((n_ang + 1, nspl, 4))
+    gz, gz0, q = C.c_double(), C.c_double(), C.c_double()
+    nrm = np.zeros(n_ang + 1)
+    ref.ref_vps_splin(path.encode(), loc_opt, n_ang, label, nspl, dg, gmin_spl, gmin_spl + dg * nspl, gmin,
+                      _d(vps), C.byref(gz), C.byref(gz0), C.byref(q), _d(nrm))
+    pp = P.read_pseud(path)
+    packed = np.load(P._DATA)
+    assert np.array_equal(packed[f"{name}_v"], pp["v"]) and np.array_equal(packed[f"{name}_rphi"], pp["rphi"])
+    tab = P.vps_tables(pp, loc_opt, label == 1, grid)
+    rng = np.random.default_rng(1)
+    gs = gmin_spl + dg * (nspl - 1) * rng.random(2000)
+
+    def ev(c):
+        i = np.clip(((gs - gmin_spl) / dg + 1.0).astype(np.int64), 1, nspl)
+        h = gs - ((i - 1) * dg + gmin_spl)
+        cc = c[i - 1]
+        return ((cc[:, 3] * h + cc[:, 2]) * h + cc[:, 1]) * h + cc[:, 0]
+
+    pairs = [(tab["vloc"], vps[loc_opt])]
+    if label == 1:
+        pairs.append((tab["proj"], vps[0]))
+        assert abs(tab["vpsnorm"] - nrm[0]) <= 1e-13 * abs(nrm[0])
+        assert abs(tab["gzvps0"] - gz0.value) <= 1e-13 * abs(gz0.value)
+    for mine, theirs in pairs:
+        scale = np.max(np.abs(theirs[:, 0]))
+        assert np.max(np.abs(mine[:, 0] - theirs[:, 0])) <= 1e-13 * scale
+        assert np.max(np.abs(ev(mine) - ev(theirs))) <= 1e-12 * scale
+    assert abs(tab["gzvps"] - gz.value) <= 1e-12 * max(1.0, abs(gz.value))
+    assert tab["q"] == q.value
