@@ -226,7 +226,10 @@ def _phase_sums(sysm, kx, ky, kz, weights):
 def hart_eext(rho_r, sysm, want_forces=False):
     """``CPLOCAL::CP_hart_eext_calc`` (``abinito_physics/cp_local/cp_hart_ext.C:56-431``)
     on rho(g) = FFT_-[rho(r) V/N] (``CP_Rho_RealSpacePlane.C:846-851``).
-    Returns (vks_hart_ext(r), ehart, eext, ewald_recip[, fatm])."""
+    Returns (vks_hart_ext(r), ehart, eext, ewald_recip[, fatm]).  A system
+    with eext_ees set takes the EES method (hart_eext_ees)."""
+    if getattr(sysm, "eext_ees", None) is not None:
+        return hart_eext_ees(rho_r, sysm, want_forces)
     nx, ny, nz = sysm.nfft
     n = nx * ny * nz
     vol = sysm.vol
@@ -567,14 +570,21 @@ def ees_bsplines(sysm, grid, order):
     cardinal B-spline, and the derivative weights dM = M_{n-1}(u) - M_{n-1}(u - 1)
     taken from the recursion at n = order - 1 (``:436-449``).  Returns
     (idx [natm_nl, 3, order] int, mn [natm_nl, 3, order], dmn [natm_nl, 3, order])."""
-    nl = sysm.nl_atoms()
-    idx = np.zeros((len(nl), 3, order), dtype=np.int64)
-    mn = np.zeros((len(nl), 3, order))
-    dmn = np.zeros((len(nl), 3, order))
-    for ia_, a in enumerate(nl):
+    return atom_bsplines(sysm.pos[sysm.nl_atoms()], sysm.box, grid, order)
+
+
+def atom_bsplines(pos, box, grid, order):
+    """Per atom and axis the B-spline stencil of ``eesAtmBsplineRgrp``
+    (nonlocal: ``cp_ees_nonlocal.C:256-593``; local: ``cp_hart_ext.C:641-860``,
+    the same recursion): grid indices, M_n and dM_n, [natm, 3, order] each."""
+    natm = pos.shape[0]
+    idx = np.zeros((natm, 3, order), dtype=np.int64)
+    mn = np.zeros((natm, 3, order))
+    dmn = np.zeros((natm, 3, order))
+    for ia_ in range(natm):
         for ax in range(3):
             ng = grid[ax]
-            t = sysm.pos[a, ax] / sysm.box
+            t = pos[ia_, ax] / box
             t -= round(t - 0.5)
             if t == 1.0:
                 t = 0.0
@@ -696,6 +706,170 @@ def nl_ees_energy_forces(psi, sysm, ees, atom_forces=False):
         for ax in range(3):
             fatm[atom, ax] -= np.sum(zs[:, a] * np.einsum("skji,kji->s", subs[a], dw[ax]))
     return fnl, enl, zmat, fatm
+
+
+# ----------------------------------------------------------------------------
+# local pseudopotential and reciprocal Ewald sum, EES method
+# (\cp_eext_ees_opt{on}: CP_Rho_RHartExt / CP_Rho_GHartExt)
+# ----------------------------------------------------------------------------
+
+def eesl_grid(sysm, scale=1.2, order=6):
+    """EES local-pseudopotential grid (``init_eext_ees``,
+    ``interface/cp_ewald/set_cp_ewald.C:1419-1500``): per axis
+    n = int(2 scale (2 kmax + 1)), one more if below 2 (2 kmax + 1), rounded
+    up to an FFT size (here: the next 2^a 3^b 5^c); kmax of the state sphere."""
+    out = []
+    for k in (sysm.kx, sysm.ky, sysm.kz):
+        nk = 2 * int(np.max(np.abs(k))) + 1
+        n = int(2.0 * scale * nk)
+        if n < 2 * nk:
+            n += 1
+        out.append(_smooth235(n))
+    if min(out) < order:
+        raise ValueError("EES grid smaller than the interpolation order")
+    return tuple(out)
+
+
+def eesl_pack(sysm, grid, order):
+    """``eesAtmBsplineRgrp`` + ``eesPackGridRchare`` (``cp_hart_ext.C:641-990``):
+    per atom type the real grid Q_t[c, b, a] = sum over the type's atoms of
+    M_a M_b M_c on their order^3 stencils.  Returns (Q [ntype, nc, nb, na],
+    (idx, mn, dmn) of atom_bsplines)."""
+    na, nb, nc = grid
+    bs = atom_bsplines(sysm.pos, sysm.box, grid, order)
+    idx, mn, _ = bs
+    ntyp = len(sysm.type_names)
+    Q = np.zeros((ntyp, nc, nb, na))
+    for a in range(sysm.natm):
+        w = np.einsum("i,j,k->kji", mn[a, 0], mn[a, 1], mn[a, 2])      # [jc, jb, ja]
+        np.add.at(Q[int(sysm.atm_type[a])], np.ix_(idx[a, 2], idx[a, 1], idx[a, 0]), w)
+    return Q, bs
+
+
+def eesl_sf(Q, kx, ky, kz):
+    """sfAtmTypG: Qhat_t(g) = sum_k Q_t(k) exp(+2 pi i m.k / n) at the density
+    g-points (the R -> G transform of ``CP_Rho_RHartExt.C:300-330``; with
+    this sign b(g) Qhat(g) approximates the structure factor
+    sum_a exp(+i g.R_a) of ``CP_hart_eext_calc``)."""
+    nc, nb, na = Q.shape[1:]
+    full = _ifftn(Q, axes=(1, 2, 3)) * (na * nb * nc)
+    return full[:, kz % nc, ky % nb, kx % na]
+
+
+def eesl_bfactor(kx, ky, kz, grid, order):
+    """``CPLOCAL::eesSetEesWghtGgrp`` (``cp_hart_ext.C:521-635``):
+    b(g) = b_a(kx) b_b(ky) b_c(kz); at g = 0 the real product."""
+    na, nb, nc = grid
+    ba, bb, bc = (bspline_weight_1d(order, n) for n in grid)
+    b = ba[kx % na] * bb[ky % nb] * bc[kz % nc]
+    g0 = (kx == 0) & (ky == 0) & (kz == 0)
+    b[g0] = (ba[0] * bb[0] * bc[0]).real
+    return b
+
+
+def eesl_gspace(rho, kx, ky, kz, g2, qhat, b, sysm):
+    """``eesHartEextGchare`` over the atom types then ``eesEwaldGchare``
+    (``cp_hart_ext.C:1005-1330``) on the density g-points.  Returns
+    (vks(g), ehart, eext, ewald, Y [ntype, npts], Ytot [npts]) with Y the
+    per-type atom-force transforms v_t conj(rho b) (g = 0: v_t(0) rho b) and
+    Ytot = prep sfAtmTotG = 4 pi e^{-g^2/4 alpha^2} / (g^2 V) |b|^2 sum_t q_t Qhat_t."""
+    vol = sysm.vol
+    ntyp = qhat.shape[0]
+    w = np.where(kx == 0, 1.0, 2.0)
+    g0 = g2 == 0.0
+    ins = (g2 <= sysm.ecut_rho_g2) & ~g0
+    hf = np.zeros_like(g2)
+    hf[ins] = 4.0 * math.pi / (g2[ins] * vol)
+    ehart = float(np.sum(hf * np.abs(rho) ** 2 * w)) / 2.0
+    vks = rho * hf
+    g = np.sqrt(g2)
+    qt = np.array([float(sysm.q[sysm.atm_type == t][0]) if np.any(sysm.atm_type == t) else 0.0 for t in range(ntyp)])
+    Y = np.zeros((ntyp, g.size), dtype=np.complex128)
+    eext = 0.0
+    for t in range(ntyp):
+        vt = np.where(ins, sysm.vloc.eval(np.full(g.shape, t), np.where(ins, g, 1.0)), 0.0) / vol
+        vext = b * qhat[t] * vt
+        eext += float(np.sum(np.where(ins, (rho * vext).real * w, 0.0)))
+        vks = vks + np.where(ins, np.conj(vext), 0.0)
+        Y[t] = np.where(ins, vt * np.conj(rho * b), 0.0)
+        if g0.any():
+            i0 = int(np.nonzero(g0)[0][0])
+            v0 = sysm.gzvps[t] / vol
+            vx = v0 * qhat[t][i0].real * b[i0].real
+            eext += rho[i0].real * vx
+            vks[i0] = vks[i0].real + vx
+            Y[t][i0] = v0 * rho[i0].real * b[i0].real
+    sq = np.where(ins, np.tensordot(qt, qhat, axes=1), 0.0)
+    falp2 = 4.0 * sysm.alp_ewd ** 2
+    preg = np.zeros_like(g2)
+    preg[ins] = 4.0 * math.pi * np.exp(-g2[ins] / falp2) / (g2[ins] * vol)
+    bmag = np.abs(b) ** 2
+    ewald = float(np.sum(bmag * np.abs(sq) ** 2 * preg * w)) / 2.0
+    vks = np.where(ins | g0, vks, 0.0)
+    return vks, ehart, eext, ewald, Y, sq * preg * bmag
+
+
+def eesl_backtransform(Y, kx, ky, kz, grid):
+    """The G -> R transform of the atom-force grids (``FFTEesFwd``,
+    ``CP_Rho_GHartExt.C:1018-1060``): P(k) = sum over the full sphere of
+    Y(g) exp(-2 pi i m.k / n), the kx > 0 half entering with its conjugate
+    partner.  Y [..., npts] -> real [..., nc, nb, na]."""
+    na, nb, nc = grid
+    lead = Y.shape[:-1]
+    full = np.zeros(lead + (nc, nb, na), dtype=np.complex128)
+    full[..., kz % nc, ky % nb, kx % na] = Y
+    h = kx > 0
+    full[..., (-kz[h]) % nc, (-ky[h]) % nb, (-kx[h]) % na] = np.conj(Y[..., h])
+    return _fftn(full, axes=(-3, -2, -1)).real
+
+
+def eesl_forces(P, Ptot, sysm, bs, grid):
+    """``eesAtmForceRchare`` (``cp_hart_ext.C:1357-1470``): for each atom
+    f -= sum over its stencil of grad(M_a M_b M_c) P_type, then with the
+    atom's charge the same with Ptot (the Ewald part)."""
+    na, nb, nc = grid
+    idx, mn, dmn = bs
+    f = np.zeros((sysm.natm, 3))
+    for a in range(sysm.natm):
+        ma, mb, mc = mn[a]
+        da, db, dc = dmn[a]
+        sl = np.ix_(idx[a, 2], idx[a, 1], idx[a, 0])
+        pt = P[int(sysm.atm_type[a])][sl]
+        pq = Ptot[sl]
+        for comp, dw in enumerate((np.einsum("i,j,k->kji", da, mb, mc) * (na / sysm.box),
+                                   np.einsum("i,j,k->kji", ma, db, mc) * (nb / sysm.box),
+                                   np.einsum("i,j,k->kji", ma, mb, dc) * (nc / sysm.box))):
+            f[a, comp] -= float(np.sum(dw * pt)) + sysm.q[a] * float(np.sum(dw * pq))
+    return f
+
+
+def hart_eext_ees(rho_r, sysm, want_forces=False):
+    """``CP_hart_eext_calc`` with the EES structure factors
+    (cp_eext_ees_opt on; ``CP_Rho_RHartExt`` -> ``CP_Rho_GHartExt``):
+    the per-type B-spline grids, their transform, b(g), the Hartree / local
+    / reciprocal Ewald terms and V_KS(g), then the atom forces by the
+    back-transformed grids.  sysm.eext_ees = (na, nb, nc, order).  Returns
+    like hart_eext."""
+    na, nb, nc, order = sysm.eext_ees
+    grid = (na, nb, nc)
+    nx, ny, nz = sysm.nfft
+    n = nx * ny * nz
+    rhog_half = _rfftn(rho_r * (sysm.vol / n))
+    kx, ky, kz, g2 = rho_sphere(sysm)
+    rho = rhog_half[kz % nz, ky % ny, kx]
+    Q, bs = eesl_pack(sysm, grid, order)
+    qhat = eesl_sf(Q, kx, ky, kz)
+    b = eesl_bfactor(kx, ky, kz, grid, order)
+    vks, ehart, eext, ewald, Y, Ytot = eesl_gspace(rho, kx, ky, kz, g2, qhat, b, sysm)
+    half = np.zeros((nz, ny, nx // 2 + 1), dtype=np.complex128)
+    half[kz % nz, ky % ny, kx] = vks
+    vr = _irfftn(half, s=(nz, ny, nx), axes=(0, 1, 2)) * n
+    out = (vr, ehart, eext, ewald)
+    if not want_forces:
+        return out
+    P = eesl_backtransform(Y, kx, ky, kz, grid)
+    Ptot = eesl_backtransform(Ytot, kx, ky, kz, grid)
+    return out + (eesl_forces(P, Ptot, sysm, bs, grid),)
 
 
 def nl_sf_atom_forces(psi, sysm, sf=None):

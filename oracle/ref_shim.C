@@ -713,3 +713,214 @@ extern "C" int ref_vps_splin(const char* file, int loc_opt, int n_ang, int ivps_
   for (int l = 0; l <= n_ang; ++l) vpsnorm[l] = nrm[l + 1];
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// EES local pseudopotential and reciprocal Ewald sum (cp_hart_ext.C:492-1470),
+// one RhoRHart chare holding the whole grid [nc][nb][lda], lda = 2 (na/2 + 1),
+// in three phases with the oracle's transforms between them:
+//   ref_eesl_pack    eesAtmBsplineRgrp (641-900) + eesPackGridRchare
+//                    (925-990) per type: the real grids sfAtmTypR
+//   ref_eesl_gspace  eesSetEesWghtGgrp (521-635), eesHartEextGchare
+//                    (1005-1225) over the types, eesEwaldGchare (1241-1340):
+//                    energies, vks(g), the per-type force transforms and
+//                    the scaled total structure factor
+//   ref_eesl_force   eesAtmForceRchare (1357-1470) per type (flag 0) and
+//                    for the Ewald grid (flag 1)
+namespace {
+struct EeslCfg {
+  int natm = 0, ntype = 0, na = 0, nb = 0, nc = 0, order = 0, lda = 0;
+  double box = 0.0;
+  std::vector<double> x, y, z, q, fx, fy, fz;
+  std::vector<int> natm_eext;
+  std::vector<std::vector<int>> map_rows;
+  std::vector<int*> map_eext;
+  std::vector<double> q_typ;
+  // RHORHARTDATA storage [nc][natm][order^2 + 1]
+  std::vector<std::vector<int>> pidx, nsub, itemp;
+  std::vector<std::vector<std::vector<int>>> ig;
+  std::vector<std::vector<std::vector<double>>> mn, dx, dy, dz;
+  std::vector<int*> ppidx, pnsub, pitemp;
+  std::vector<std::vector<int*>> pig;
+  std::vector<std::vector<double*>> pmn, pdx, pdy, pdz;
+  std::vector<int**> ppig;
+  std::vector<double**> ppmn, ppdx, ppdy, ppdz;
+  RHORHARTDATA rd;
+  FastAtoms fa;
+} g_eesl;
+
+void eesl_apply() {
+  EeslCfg& e = g_eesl;
+  set_cell(e.box);
+  CPPSEUDO* ps = &readonly_cp.cppseudo;
+  ps->n_interp_ps = e.order;
+  ps->ngrid_eext_a = e.na; ps->ngrid_eext_b = e.nb; ps->ngrid_eext_c = e.nc;
+  ps->natm_typ = e.ntype;
+  ps->natm_eext = e.natm_eext.data();
+  ps->map_eext = e.map_eext.data();
+  ps->q_typ = e.q_typ.data();
+  readonly_mdatoms.mdclatoms_info.natm_tot = e.natm;
+}
+}  // namespace
+
+// Atoms (0-based types, charges), box, EES grid na x nb x nc and order; the
+// per-type real grids sfAtmTypR [ntype][nc][nb][lda] are written.
+extern "C" void ref_eesl_pack(int natm, const double* pos, const int* atm_type, const double* q, int ntype, double box,
+                              int na, int nb, int nc, int order, double* grids) {
+  EeslCfg& e = g_eesl;
+  e = EeslCfg();
+  e.natm = natm; e.ntype = ntype; e.na = na; e.nb = nb; e.nc = nc; e.order = order; e.box = box;
+  e.lda = 2 * (na / 2 + 1);
+  e.x.resize(natm); e.y.resize(natm); e.z.resize(natm); e.q.assign(q, q + natm);
+  e.fx.assign(natm, 0.0); e.fy = e.fx; e.fz = e.fx;
+  for (int a = 0; a < natm; ++a) { e.x[a] = pos[3 * a]; e.y[a] = pos[3 * a + 1]; e.z[a] = pos[3 * a + 2]; }
+  e.natm_eext.assign(ntype + 2, 0);
+  e.map_rows.assign(ntype + 2, std::vector<int>(natm + 1, 0));
+  e.q_typ.assign(ntype + 2, 0.0);
+  for (int a = 0; a < natm; ++a) {
+    const int t = atm_type[a] + 1;
+    e.map_rows[t][++e.natm_eext[t]] = a + 1;
+    e.q_typ[t] = q[a];
+  }
+  e.natm_eext[ntype + 1] = natm;  // the Ewald pass runs over all atoms
+  for (int a = 0; a < natm; ++a) e.map_rows[ntype + 1][a + 1] = a + 1;
+  e.map_eext.resize(ntype + 2);
+  for (int t = 0; t <= ntype + 1; ++t) e.map_eext[t] = e.map_rows[t].data();
+  eesl_apply();
+  const int n = order, n2 = n * n;
+  e.pidx.assign(nc, std::vector<int>(natm, 0)); e.nsub = e.pidx;
+  e.itemp.assign(nc, std::vector<int>(n + 1, 0));
+  e.ig.assign(nc, std::vector<std::vector<int>>(natm, std::vector<int>(n2 + 1, 0)));
+  e.mn.assign(nc, std::vector<std::vector<double>>(natm, std::vector<double>(n2 + 1, 0.0)));
+  e.dx = e.mn; e.dy = e.mn; e.dz = e.mn;
+  e.ppidx.resize(nc); e.pnsub.resize(nc); e.pitemp.resize(nc);
+  e.pig.resize(nc); e.pmn.resize(nc); e.pdx.resize(nc); e.pdy.resize(nc); e.pdz.resize(nc);
+  e.ppig.resize(nc); e.ppmn.resize(nc); e.ppdx.resize(nc); e.ppdy.resize(nc); e.ppdz.resize(nc);
+  for (int c = 0; c < nc; ++c) {
+    e.ppidx[c] = e.pidx[c].data(); e.pnsub[c] = e.nsub[c].data(); e.pitemp[c] = e.itemp[c].data();
+    e.pig[c].resize(natm); e.pmn[c].resize(natm); e.pdx[c].resize(natm); e.pdy[c].resize(natm); e.pdz[c].resize(natm);
+    for (int a = 0; a < natm; ++a) {
+      e.pig[c][a] = e.ig[c][a].data(); e.pmn[c][a] = e.mn[c][a].data();
+      e.pdx[c][a] = e.dx[c][a].data(); e.pdy[c][a] = e.dy[c][a].data(); e.pdz[c][a] = e.dz[c][a].data();
+    }
+    e.ppig[c] = e.pig[c].data(); e.ppmn[c] = e.pmn[c].data();
+    e.ppdx[c] = e.pdx[c].data(); e.ppdy[c] = e.pdy[c].data(); e.ppdz[c] = e.pdz[c].data();
+  }
+  RHORHARTDATA& r = e.rd;
+  r.xindex = 0; r.yindex = 0;
+  r.gridc_start = 0; r.gridc_end = nc; r.gridb_start = 0; r.gridb_end = nb;
+  r.mygridc = nc; r.mygridb = nb;
+  r.ngrid_a = na; r.ngrid_b = nb; r.ngrid_c = nc; r.n_interp = n; r.natm = natm;
+  r.plane_index = e.ppidx.data(); r.nSub = e.pnsub.data(); r.itemp = e.pitemp.data();
+  r.igrid = e.ppig.data(); r.mn = e.ppmn.data();
+  r.dmn_x = e.ppdx.data(); r.dmn_y = e.ppdy.data(); r.dmn_z = e.ppdz.data();
+  // PSSCRATCH ([j][i], j = 1..n)
+  std::vector<double> aj(n + 1), rn(n + 1), rn1(n + 1), fa_(natm), fb(natm), fc(natm);
+  std::vector<int> iat(natm), ibt(natm), ict(natm);
+  std::vector<std::vector<int>> gi_a(n + 1, std::vector<int>(natm)), gi_b = gi_a, gi_c = gi_a;
+  std::vector<std::vector<double>> m_a(n + 1, std::vector<double>(natm)), m_b = m_a, m_c = m_a, u_a = m_a, u_b = m_a,
+                                   u_c = m_a, dm_a = m_a, dm_b = m_a, dm_c = m_a;
+  auto rows_i = [](std::vector<std::vector<int>>& v) {
+    std::vector<int*> p(v.size());
+    for (size_t i = 0; i < v.size(); ++i) p[i] = v[i].data();
+    return p;
+  };
+  auto rows_d = [](std::vector<std::vector<double>>& v) {
+    std::vector<double*> p(v.size());
+    for (size_t i = 0; i < v.size(); ++i) p[i] = v[i].data();
+    return p;
+  };
+  auto pga = rows_i(gi_a), pgb = rows_i(gi_b), pgc = rows_i(gi_c);
+  auto pma = rows_d(m_a), pmb = rows_d(m_b), pmc = rows_d(m_c), pua = rows_d(u_a), pub = rows_d(u_b),
+       puc = rows_d(u_c), pda = rows_d(dm_a), pdb = rows_d(dm_b), pdc = rows_d(dm_c);
+  PSSCRATCH ps;
+  ps.aj = aj.data(); ps.rn = rn.data(); ps.rn1 = rn1.data();
+  ps.iatemp = iat.data(); ps.ibtemp = ibt.data(); ps.ictemp = ict.data();
+  ps.frac_a = fa_.data(); ps.frac_b = fb.data(); ps.frac_c = fc.data();
+  ps.igrid_a = pga.data(); ps.igrid_b = pgb.data(); ps.igrid_c = pgc.data();
+  ps.mn_a = pma.data(); ps.mn_b = pmb.data(); ps.mn_c = pmc.data();
+  ps.ua = pua.data(); ps.ub = pub.data(); ps.uc = puc.data();
+  ps.dmn_a = pda.data(); ps.dmn_b = pdb.data(); ps.dmn_c = pdc.data();
+  FastAtoms& at = e.fa;
+  at.natm = natm; at.x = e.x.data(); at.y = e.y.data(); at.z = e.z.data(); at.q = e.q.data();
+  at.fx = e.fx.data(); at.fy = e.fy.data(); at.fz = e.fz.data();
+  std::vector<RHORHARTDATA> rv(1, r);
+  CPLOCAL::eesAtmBsplineRgrp(&at, rv, &ps);
+  const size_t gsz = (size_t)nc * nb * e.lda;
+  for (int t = 1; t <= ntype; ++t)
+    CPLOCAL::eesPackGridRchare(natm, t, grids + (size_t)(t - 1) * gsz, 0, nc, 0, nb, (int)gsz, r.igrid, r.mn,
+                               r.plane_index, r.nSub);
+  ps.aj = nullptr; ps.rn = nullptr; ps.rn1 = nullptr;
+  ps.iatemp = ps.ibtemp = ps.ictemp = nullptr;
+  ps.frac_a = ps.frac_b = ps.frac_c = nullptr;
+  ps.igrid_a = ps.igrid_b = ps.igrid_c = nullptr;
+  ps.mn_a = ps.mn_b = ps.mn_c = ps.ua = ps.ub = ps.uc = ps.dmn_a = ps.dmn_b = ps.dmn_c = nullptr;
+}
+
+// Density g-points (kx, ky, kz) with rho(g); local splines per type
+// [ntype][nspl][4], gzvps per type, alpha, the state cutoff in Ry.  In:
+// sfg [ntype][npts] complex = the transformed grids at the points.  Out:
+// vks(g), sfg overwritten by the atom-force transforms, sftot [npts] the
+// scaled total structure factor, b [npts] complex, the energies.
+extern "C" void ref_eesl_gspace(int npts, const int* kx, const int* ky, const int* kz, const double* rho, double* vks,
+                                int nspl, double gmin, double dg, const double* spl, const double* gzvps,
+                                double alp_ewd, double ecut_ry, double* sfg, double* sftot, double* b, double* ehart,
+                                double* eext, double* ewd) {
+  EeslCfg& e = g_eesl;
+  eesl_apply();
+  CP* cp = &readonly_cp;
+  CPPSEUDO* ps = &cp->cppseudo;
+  const int ntype = e.ntype;
+  ps->nsplin_g = nspl;
+  ps->n_rad_max = 1;
+  ps->n_ang_max = 0;
+  ps->dg_spl = dg;
+  ps->gmin_spl = gmin;
+  std::vector<double> v0(ntype * nspl + 1), v1(ntype * nspl + 1), v2(ntype * nspl + 1), v3(ntype * nspl + 1);
+  for (int t = 0; t < ntype; ++t)
+    for (int i = 0; i < nspl; ++i) {
+      const double* c = spl + ((size_t)t * nspl + i) * 4;
+      const int idx = t * nspl + i + 1;
+      v0[idx] = c[0]; v1[idx] = c[1]; v2[idx] = c[2]; v3[idx] = c[3];
+    }
+  ps->vps0 = v0.data(); ps->vps1 = v1.data(); ps->vps2 = v2.data(); ps->vps3 = v3.data();
+  std::vector<double> gz(ntype + 1);
+  std::vector<int> lopt(ntype + 1, 0);
+  for (int t = 0; t < ntype; ++t) gz[t + 1] = gzvps[t];
+  ps->gzvps = gz.data();
+  ps->loc_opt = lopt.data();
+  cp->cpcoeffs_info.ecut = 0.5 * ecut_ry;
+  readonly_general_data.genewald.alp_ewd = alp_ewd;
+  std::vector<gridPoint> pts(npts);
+  for (int i = 0; i < npts; ++i) { pts[i].d3 = kx[i]; pts[i].d2 = ky[i]; pts[i].d1 = kz[i]; pts[i].offset = i; }
+  std::vector<double> bre(npts), bim(npts);
+  CPLOCAL::eesSetEesWghtGgrp(npts, pts, bre.data(), bim.data(), e.na, e.nb, e.nc, e.order);
+  for (int i = 0; i < npts; ++i) { b[2 * i] = bre[i]; b[2 * i + 1] = bim[i]; }
+  for (int i = 0; i < 2 * npts; ++i) { vks[i] = 0.0; sftot[i] = 0.0; }
+  *ehart = 0.0; *eext = 0.0;
+  for (int t = 1; t <= ntype; ++t)
+    CPLOCAL::eesHartEextGchare(npts, t, (complex*)const_cast<double*>(rho), (complex*)vks,
+                               (complex*)sfg + (size_t)(t - 1) * npts, (complex*)sftot, bre.data(), bim.data(), ehart,
+                               eext, pts, nullptr, 0, 1);
+  CPLOCAL::eesEwaldGchare(npts, (complex*)sftot, bre.data(), bim.data(), ewd, pts, 0, nullptr, 0, 1);
+  ps->vps0 = ps->vps1 = ps->vps2 = ps->vps3 = nullptr;
+  ps->gzvps = nullptr;
+  ps->loc_opt = nullptr;
+}
+
+// Back-transformed grids [ntype][nc][nb][lda] (per type) and [nc][nb][lda]
+// (Ewald) -> atom forces [natm][3] (overwritten).
+extern "C" void ref_eesl_force(const double* grids, const double* grid_tot, double* fatm) {
+  EeslCfg& e = g_eesl;
+  eesl_apply();
+  std::fill(e.fx.begin(), e.fx.end(), 0.0);
+  std::fill(e.fy.begin(), e.fy.end(), 0.0);
+  std::fill(e.fz.begin(), e.fz.end(), 0.0);
+  RHORHARTDATA& r = e.rd;
+  const size_t gsz = (size_t)e.nc * e.nb * e.lda;
+  for (int t = 1; t <= e.ntype; ++t)
+    CPLOCAL::eesAtmForceRchare(e.natm, &e.fa, t, r.igrid, r.dmn_x, r.dmn_y, r.dmn_z, r.plane_index, r.nSub,
+                               const_cast<double*>(grids) + (size_t)(t - 1) * gsz, 0, e.nc, 0, e.nb, 0);
+  CPLOCAL::eesAtmForceRchare(e.natm, &e.fa, 1, r.igrid, r.dmn_x, r.dmn_y, r.dmn_z, r.plane_index, r.nSub,
+                             const_cast<double*>(grid_tot), 0, e.nc, 0, e.nb, 1);
+  for (int a = 0; a < e.natm; ++a) { fatm[3 * a] = e.fx[a]; fatm[3 * a + 1] = e.fy[a]; fatm[3 * a + 2] = e.fz[a]; }
+}

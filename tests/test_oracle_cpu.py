@@ -217,3 +217,37 @@ def test_cg_minimisation_beats_steepest_descent():
         S = O.pc_forward(O.kx0_scale(st.psi, s, 2 ** -0.5), O.kx0_scale(st.psi, s, 2 ** -0.5), s, 2.0)
         assert np.max(np.abs(S / 2.0 - np.eye(s.nstate))) < 1e-12
     assert out["cg"][0] < out["sd"][0] and out["cg"][1] < out["sd"][1] < out["sd"][2]
+
+
+def test_ees_local_converges_to_structure_factor():
+    """The EES local pseudopotential / reciprocal Ewald path approaches the
+    structure-factor path as the B-spline order grows, and its atom forces
+    are the negative gradient of E_ext + E_ewald(recip) at fixed density."""
+    import copy
+    s = make_system("w4", seed=21)
+    rho = O.density(O.state_g_to_r(s.psi, s), s)
+    ref = O.hart_eext(rho, s, want_forces=True)
+    errs = []
+    for order in (4, 8):
+        s2 = copy.copy(s)
+        s2.eext_ees = O.eesl_grid(s, 1.2, order) + (order,)
+        out = O.hart_eext(rho, s2, want_forces=True)
+        assert out[1] == ref[1]                                   # Hartree does not change
+        errs.append((abs(out[2] - ref[2]) / abs(ref[2]), abs(out[3] - ref[3]) / abs(ref[3]),
+                     np.max(np.abs(out[4] - ref[4])) / np.max(np.abs(ref[4]))))
+    assert errs[1][0] < 1e-5 and errs[1][1] < 1e-9 and errs[1][2] < 1e-5
+    assert all(b < a for a, b in zip(errs[0], errs[1]))
+    s2 = copy.copy(s)
+    s2.pos = s.pos.copy()
+    s2.eext_ees = O.eesl_grid(s, 1.2, 6) + (6,)
+    F = O.hart_eext(rho, s2, want_forces=True)[4]
+    h = 1e-4
+    for a, c in ((0, 0), (1, 2), (s.natm - 1, 1)):
+        e = []
+        for sgn in (1, -1):
+            s3 = copy.copy(s2)
+            s3.pos = s2.pos.copy()
+            s3.pos[a, c] += sgn * h
+            o = O.hart_eext(rho, s3)
+            e.append(o[2] + o[3])
+        assert abs(-(e[0] - e[1]) / (2 * h) - F[a, c]) <= 1e-6 * max(1.0, abs(F[a, c]))

@@ -8,11 +8,14 @@ CPORTHOG::get_iter_Tmat (cp_lowdin.C), the structure-factor nonlocal path
 (cp_struct_fact.C, cp_nlmat.C, cp_nl_energy_forc.C), the EES nonlocal path
 (cp_ees_nonlocal.C with get_bspline_wght1d of set_cp_ewald.C), the CP
 integrator (cp_dynamics.C), the minimisers (cp_min_std.C, cp_min_CG.C), the
-BLYP functional (cp_becke.C, cp_grad_rho_ctrl.C) and the real-space Ewald
-sum (cp_rspace_ion.C).
+BLYP functional (cp_becke.C, cp_grad_rho_ctrl.C), the real-space Ewald
+sum (cp_rspace_ion.C), the EES local pseudopotential and reciprocal Ewald
+path (cp_hart_ext.C) and the pseudopotential splines (control_vps_params.C,
+friend_lib.C).
 The FFT and GEMM boundaries have no reference implementation here (FFTW2 /
 Fortran BLAS are absent) and are pinned by mathematics in test_oracle_cpu.py.
 """
+import copy
 import ctypes as C
 import os
 import subprocess
@@ -387,3 +390,73 @@ def test_pseudopotential_splines_pinned(ref, name, loc_opt, n_ang, label):
         assert np.max(np.abs(ev(mine) - ev(theirs))) <= 1e-12 * scale
     assert abs(tab["gzvps"] - gz.value) <= 1e-12 * max(1.0, abs(gz.value))
     assert tab["q"] == q.value
+
+
+@pytest.mark.parametrize("order", [4, 6])
+def test_ees_local_pinned(ref, sysm, order):
+    """The EES local pseudopotential and reciprocal Ewald path
+    (cp_eext_ees_opt on, cp_hart_ext.C:492-1470) against the oracle's
+    eesl_* restatement, phase by phase with the oracle's transforms between:
+    the per-type B-spline grids (eesAtmBsplineRgrp + eesPackGridRchare),
+    the g-space energies / vks / force transforms (eesSetEesWghtGgrp,
+    eesHartEextGchare over the types, eesEwaldGchare), and the atom forces
+    (eesAtmForceRchare, types and Ewald)."""
+    s = sysm
+    ntyp = len(s.type_names)
+    grid = O.eesl_grid(s, 1.2, order)
+    na, nb, nc = grid
+    lda = 2 * (na // 2 + 1)
+    ref.ref_eesl_pack.argtypes = [C.c_int, dp, ip, dp, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, dp]
+    ref.ref_eesl_gspace.argtypes = [C.c_int, ip, ip, ip, dp, dp, C.c_int, C.c_double, C.c_double, dp, dp,
+                                    C.c_double, C.c_double, dp, dp, dp, dp, dp, dp]
+    ref.ref_eesl_force.argtypes = [dp, dp, dp]
+    typ = np.ascontiguousarray(s.atm_type, dtype=np.int32)
+    pos = np.ascontiguousarray(s.pos)
+    q = np.ascontiguousarray(s.q)
+    grids = np.zeros((ntyp, nc, nb, lda))
+    ref.ref_eesl_pack(s.natm, _d(pos), _i(typ), _d(q), ntyp, s.box, na, nb, nc, order, _d(grids))
+    Q, bs = O.eesl_pack(s, grid, order)
+    assert np.max(np.abs(grids[..., :na] - Q)) <= 1e-14
+    assert not np.any(grids[..., na:])
+    # g-space on the density sphere, rho of the seeded states
+    rho_r = O.density(O.state_g_to_r(s.psi, s), s)
+    kx, ky, kz, g2 = O.rho_sphere(s)
+    nx, ny, nz = s.nfft
+    rho = np.ascontiguousarray(np.fft.rfftn(rho_r * (s.vol / s.npts))[kz % nz, ky % ny, kx])
+    qhat = O.eesl_sf(Q, kx, ky, kz)
+    b_or = O.eesl_bfactor(kx, ky, kz, grid, order)
+    vks_or, eh_or, ee_or, ew_or, Y_or, Yt_or = O.eesl_gspace(rho, kx, ky, kz, g2, qhat, b_or, s)
+    kx_, ky_, kz_ = (np.ascontiguousarray(a, dtype=np.int32) for a in (kx, ky, kz))
+    sfg = np.ascontiguousarray(O.eesl_sf(grids[..., :na], kx, ky, kz))
+    vks = np.zeros_like(rho)
+    sftot = np.zeros_like(rho)
+    b = np.zeros_like(rho)
+    eh, ee, ew = C.c_double(), C.c_double(), C.c_double()
+    ref.ref_eesl_gspace(len(kx), _i(kx_), _i(ky_), _i(kz_), _d(rho.view(np.float64)), _d(vks.view(np.float64)),
+                        s.vloc.n, s.vloc.gmin, s.vloc.dg, _d(np.ascontiguousarray(s.vloc.coef)),
+                        _d(np.ascontiguousarray(s.gzvps)), s.alp_ewd, s.ecut_ry, _d(sfg.view(np.float64)),
+                        _d(sftot.view(np.float64)), _d(b.view(np.float64)), C.byref(eh), C.byref(ee), C.byref(ew))
+    assert np.max(np.abs(b - b_or)) <= 1e-13
+    assert abs(eh.value - eh_or) <= 1e-12 * abs(eh_or)
+    assert abs(ee.value - ee_or) <= 1e-12 * abs(ee_or)
+    assert abs(ew.value - ew_or) <= 1e-12 * abs(ew_or)
+    assert np.max(np.abs(vks - vks_or)) <= 1e-12 * np.max(np.abs(vks_or))
+    assert np.max(np.abs(sfg - Y_or)) <= 1e-12 * np.max(np.abs(Y_or))
+    assert np.max(np.abs(sftot - Yt_or)) <= 1e-12 * np.max(np.abs(Yt_or))
+    # forces from the back-transformed grids (x-padded for the reference)
+    P = O.eesl_backtransform(sfg, kx, ky, kz, grid)
+    Pt = O.eesl_backtransform(sftot, kx, ky, kz, grid)
+    Pg = np.zeros((ntyp, nc, nb, lda))
+    Pg[..., :na] = P
+    Ptg = np.zeros((nc, nb, lda))
+    Ptg[..., :na] = Pt
+    fatm = np.zeros((s.natm, 3))
+    ref.ref_eesl_force(_d(Pg), _d(Ptg), _d(fatm))
+    f_or = O.eesl_forces(P, Pt, s, bs, grid)
+    assert np.max(np.abs(fatm - f_or)) <= 1e-11 * np.max(np.abs(f_or))
+    # and the composed oracle path equals the pieces
+    s2 = copy.copy(s)
+    s2.eext_ees = grid + (order,)
+    _, eh2, ee2, ew2, f2 = O.hart_eext(rho_r, s2, want_forces=True)
+    assert (eh2, ee2, ew2) == (eh_or, ee_or, ew_or)
+    assert np.max(np.abs(f2 - f_or)) <= 1e-13 * np.max(np.abs(f_or))
