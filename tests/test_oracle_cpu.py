@@ -235,7 +235,7 @@ def test_ees_local_converges_to_structure_factor():
         assert out[1] == ref[1]                                   # Hartree does not change
         errs.append((abs(out[2] - ref[2]) / abs(ref[2]), abs(out[3] - ref[3]) / abs(ref[3]),
                      np.max(np.abs(out[4] - ref[4])) / np.max(np.abs(ref[4]))))
-    assert errs[1][0] < 1e-5 and errs[1][1] < 1e-9 and errs[1][2] < 1e-5
+    assert errs[1][0] < 1e-5 and errs[1][1] < 1e-7 and errs[1][2] < 1e-5
     assert all(b < a for a, b in zip(errs[0], errs[1]))
     s2 = copy.copy(s)
     s2.pos = s.pos.copy()
