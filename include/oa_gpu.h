@@ -354,6 +354,21 @@ oa_status oa_gpu_pc_forward_noalloc(void *stream, const double *left, const doub
  * eesProjGchare 594-727).  Allocates the nonlocal-grid scratch. */
 oa_status oa_gpu_ees_init(oa_ctx *ctx, int na, int nb, int nc, int order, const double *dyp);
 
+/* Switch the local pseudopotential and the reciprocal Ewald sum to the EES
+ * method (cp_eext_ees_opt on; replaces the per-step work of
+ * CP_Rho_RHartExt / CP_Rho_GHartExt: eesAtmBsplineRgrp, eesPackGridRchare,
+ * eesHartEextGchare, eesEwaldGchare, eesAtmForceRchare,
+ * cp_hart_ext.C:641-1470, with eesSetEesWghtGgrp 521-635 and
+ * get_bspline_wght1d set_cp_ewald.C:1237-1325 computed here).  Grid
+ * na x nb x nc (2^a 3^b 5^c, <= 512, each >= order and > twice the largest
+ * |k| of the density sphere; init_eext_ees set_cp_ewald.C:1419-1500 gives
+ * the reference's choice), B-spline order even 4..16.  Every later density
+ * pass (the stage entry points, oa_gpu_cp_step/run) uses it; with ion
+ * dynamics the local and reciprocal Ewald atom forces come from it too.
+ * na = nb = nc = 0 switches back to the structure-factor method.
+ * Allocates two complex grids per two atom types. */
+oa_status oa_gpu_set_ees_local(oa_ctx *ctx, int na, int nb, int nc, int order);
+
 /* Nonlocal energy and coefficient forces by the EES method:
  * eesAtmBsplineRgrp (cp_ees_nonlocal.C:256-593), eesProjGchare + the
  * nonlocal-grid FFT (CP_State_ParticlePlane.C:867-1136), eesZmatRchare

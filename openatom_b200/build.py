@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liboa_gpu.so")
-SOURCES = ["oa_state.cu", "oa_pencil.cu", "oa_pair_plane.cu", "oa_rho.cu", "oa_rho_pencil.cu", "oa_pc.cu", "oa_dgemm.cu", "oa_ns.cu", "oa_umma.cu", "oa_tgemm.cu", "oa_ozaki.cu", "oa_nl.cu", "oa_ions.cu", "oa_step.cu", "oa_noalloc.cu", "oa_abi.cu"]
+SOURCES = ["oa_state.cu", "oa_pencil.cu", "oa_pair_plane.cu", "oa_rho.cu", "oa_rho_pencil.cu", "oa_pc.cu", "oa_dgemm.cu", "oa_ns.cu", "oa_umma.cu", "oa_tgemm.cu", "oa_ozaki.cu", "oa_nl.cu", "oa_ions.cu", "oa_eesl.cu", "oa_step.cu", "oa_noalloc.cu", "oa_abi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -244,6 +244,7 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
   double gz = 0.0;
   for (int a = 0; a < d->natm; ++a) gz += d->gzvps[d->atm_type[a]];
   c->gzvps_sum = gz;
+  for (int t = 0; t < d->ntype; ++t) c->gzvps_t[t] = d->gzvps[t];
   if (!make_plan(d->nx, &c->plan_x) || !make_plan(d->ny, &c->plan_y) || !make_plan(d->nz, &c->plan_z)) {
     oa_set_error("FFT length must be 2^a 3^b 5^c with at least two radix stages and <= 512", __FILE__, __LINE__);
     free(F);
@@ -443,6 +444,7 @@ extern "C" oa_status oa_gpu_destroy(oa_ctx* c) {
   if (!c) return OA_OK;
   oa_step_free(c);
   ees_free(c);
+  oa_eesl_free(c);
   oa_ions_free(c);
   oa_ctx_pc* p = pcx(c);
   oa_oz_free(p->oz);
@@ -1337,6 +1339,76 @@ extern "C" oa_status oa_gpu_ees_init(oa_ctx* c, int na, int nb, int nc, int orde
   TRYE(cudaMalloc(&e->zs, (size_t)c->nstate * c->natm_nl * sizeof(double)));
   TRYE(cudaMalloc(&e->enl, (size_t)c->nstate * sizeof(double)));
 #undef TRYE
+  return OA_OK;
+}
+
+// get_bspline_wght1d (set_cp_ewald.C:1237-1325): for m = 0..ngrid-1
+// b(m) = exp(2 pi i (n-1) m / K) / sum_{k=1}^{n-1} M_n(k) exp(2 pi i m (k-1) / K),
+// M_n at the integers by the cardinal B-spline recursion from M_2.
+static std::vector<double2> bspline_factor_1d(int order, int ngrid) {
+  std::vector<double> mn(order + 1, 0.0), uk(order + 1, 0.0);
+  mn[1] = 1.0;
+  for (int k = 1; k <= order; ++k) uk[k] = (double)k;
+  for (int n = 3; n <= order; ++n) {
+    for (int k = n; k >= 2; --k) mn[k] = (uk[k] * mn[k] + ((double)n - uk[k]) * mn[k - 1]) / (double)(n - 1);
+    mn[1] = uk[1] * mn[1] / (double)(n - 1);
+  }
+  std::vector<double2> b(ngrid);
+  for (int m = 0; m < ngrid; ++m) {
+    double dr = 0.0, di = 0.0;
+    for (int k = 1; k < order; ++k) {
+      const double a = 2.0 * M_PI * (double)m * (double)(k - 1) / (double)ngrid;
+      dr += cos(a) * mn[k];
+      di += sin(a) * mn[k];
+    }
+    const double an = 2.0 * M_PI * (double)(order - 1) * (double)m / (double)ngrid;
+    const double nr = cos(an), ni = sin(an);
+    const double den = dr * dr + di * di;
+    b[m] = make_double2((nr * dr + ni * di) / den, (ni * dr - nr * di) / den);
+  }
+  return b;
+}
+
+extern "C" oa_status oa_gpu_set_ees_local(oa_ctx* c, int na, int nb, int nc, int order) {
+  OA_ARG_CHECK(c, "null context");
+  if (na == 0 && nb == 0 && nc == 0) {
+    oa_eesl_free(c);
+    c->eesl_gen++;
+    return OA_OK;
+  }
+  OA_ARG_CHECK(order >= 4 && order <= 16 && order % 2 == 0, "EES order must be even, 4..16 (cp_pseudo_ees_order)");
+  OA_ARG_CHECK(na >= order && nb >= order && nc >= order, "EES grid smaller than the interpolation order");
+  OA_ARG_CHECK(na > 2 * c->kmax_tab && nb > 2 * c->kmax_tab && nc > 2 * c->kmax_tab,
+               "EES local grid too small for the density sphere (n > 2 kmax_rho)");
+  OaFftPlan pa, pb, pc;
+  if (!make_plan(na, &pa) || !make_plan(nb, &pb) || !make_plan(nc, &pc)) {
+    oa_set_error("EES grid size must be 2^a 3^b 5^c with at least two radix stages and <= 512", __FILE__, __LINE__);
+    return OA_ERR_UNSUPPORTED;
+  }
+  oa_eesl_free(c);
+  c->eesl_gen++;
+  oa_eesl* L = (oa_eesl*)calloc(1, sizeof(oa_eesl));
+  if (!L) return OA_ERR_CUDA;
+  c->eesl = L;
+  L->na = na; L->nb = nb; L->nc = nc; L->order = order;
+  L->ngrid = (c->ntype + 1) / 2;
+  L->pa = pa; L->pb = pb; L->pc = pc;
+  cudaError_t err = cudaSuccess;
+#define TRYL(x) do { err = (x); if (err != cudaSuccess) { oa_eesl_free(c); oa_set_error(cudaGetErrorString(err), __FILE__, __LINE__); return OA_ERR_CUDA; } } while (0)
+  L->tw_a = make_twiddles(na);
+  L->tw_b = make_twiddles(nb);
+  L->tw_c = make_twiddles(nc);
+  if (!L->tw_a || !L->tw_b || !L->tw_c) { oa_eesl_free(c); oa_set_error("twiddle allocation failed", __FILE__, __LINE__); return OA_ERR_CUDA; }
+  const std::vector<double2> ba = bspline_factor_1d(order, na), bb = bspline_factor_1d(order, nb),
+                             bc = bspline_factor_1d(order, nc);
+  TRYL(upload(&L->ba, ba.data(), ba.size()));
+  TRYL(upload(&L->bb, bb.data(), bb.size()));
+  TRYL(upload(&L->bc, bc.data(), bc.size()));
+  TRYL(upload(&L->gzvps, c->gzvps_t, (size_t)c->ntype));
+  const size_t gbytes = (size_t)L->ngrid * na * nb * nc * sizeof(double2);
+  TRYL(cudaMalloc(&L->zq, gbytes));
+  TRYL(cudaMalloc(&L->zy, gbytes));
+#undef TRYL
   return OA_OK;
 }
 

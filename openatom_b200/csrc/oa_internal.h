@@ -39,6 +39,30 @@ struct oa_ees {
   double* enl;         // [nstate]
 };
 
+// EES local pseudopotential and reciprocal Ewald path (oa_gpu_set_ees_local,
+// cp_eext_ees_opt on): grid na x nb x nc, B-spline order; atom types 2k and
+// 2k+1 share complex grid k (real and imaginary part)
+struct oa_eesl {
+  int na, nb, nc, order, ngrid;
+  OaFftPlan pa, pb, pc;
+  double2 *tw_a, *tw_b, *tw_c;
+  double2 *ba, *bb, *bc;   // 1-D B-spline factors b(m), m = 0..n-1 (get_bspline_wght1d)
+  double2* zq;             // [ngrid][nc][nb][na]: type grids, then their transform
+  double2* zy;             // [ngrid][nc][nb][na]: force transforms, then the force grids
+  double* gzvps;           // [ntype]
+};
+
+// What the density z pass reads of the EES local path (zq = null: the
+// structure-factor path)
+struct EesLocArgs {
+  const double2* zq;
+  double2* zy;             // forces: written at the sphere points (zeroed before)
+  const double2 *ba, *bb, *bc;
+  const double* gzvps;
+  int na, nb, nc;
+  size_t gstride;          // na nb nc
+};
+
 // Per-block charge partials of the mixed z forward pass: sum over the
 // block's coefficients of occ_s w |c|^2 (w = 1 on the kx = 0 lines, whose
 // two halves are both stored, 2 elsewhere); part = null: none
@@ -135,6 +159,9 @@ struct oa_ctx {
   double *grad;           // [3][nz][ny][nx] grad rho, then the GGA vector h (BLYP)
   void *dzg;              // [3][nz][ldl_d] C  z-lines of grad rho / h (BLYP)
   oa_ions *ions;          // ion dynamics, after oa_gpu_set_ions
+  oa_eesl *eesl;          // EES local path, after oa_gpu_set_ees_local
+  int eesl_gen;           // bumped by every oa_gpu_set_ees_local (captured graphs depend on it)
+  double gzvps_t[4];      // g = 0 limit of the local part per type
   // mixed form: the FP32 density renormalised to the exact electron count
   // (charge partials of the z forward pass and of the pair density pass)
   double *qpart, *qpart2, *qscale;
@@ -168,5 +195,8 @@ cudaError_t oa_launch_ees(oa_ctx* c, cudaStream_t s, const double2* psi, double2
 cudaError_t oa_launch_ees_zreduce(oa_ctx* c, cudaStream_t s);
 cudaError_t oa_launch_ees_bspline(oa_ctx* c, cudaStream_t s);
 cudaError_t oa_launch_nl_sf_force(oa_ctx* c, cudaStream_t s, const double* psi);
+cudaError_t oa_launch_eesl_front(oa_ctx* c, cudaStream_t s);
+cudaError_t oa_launch_eesl_forces(oa_ctx* c, cudaStream_t s);
+void oa_eesl_free(oa_ctx* c);
 cudaError_t oa_launch_ion_step(oa_ctx* c, cudaStream_t s, double* dev_e, double dt, int kick2);
 size_t oa_plane_smem_bytes(int precision, int nx, int ny, int nkx);

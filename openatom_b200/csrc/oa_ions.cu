@@ -9,7 +9,9 @@
 //     ATOMINTEGRATE::integrate_nve_2nd_half / integrate_nve_1st_half
 //     (classical_physics/integrate/integration_drivers.C:17-85)             -> k_ion_integrate
 // The local pseudopotential and reciprocal Ewald forces come from the
-// density z pass (k_rho_zpass<..., true>, oa_rho.cu).
+// density z pass (k_rho_zpass<..., true>, oa_rho.cu), one partial per z-pass
+// block, or with the EES local path from k_eesl_force (oa_eesl.cu) in the
+// first partial.
 #include <stdlib.h>
 #include <string.h>
 #include <vector>
@@ -222,8 +224,8 @@ cudaError_t oa_launch_ion_step(oa_ctx* c, cudaStream_t s, double* dev_e, double 
                                          io->er);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_ion_integrate<<<1, 256, 0, s>>>(c->pos, io->v, io->m, io->fpart, io->nfpart, io->fnl, io->fr, io->er, c->natm,
-                                    dt, kick2, io->self_bgr, dev_e);
+  k_ion_integrate<<<1, 256, 0, s>>>(c->pos, io->v, io->m, io->fpart, c->eesl ? 1 : io->nfpart, io->fnl, io->fr,
+                                    io->er, c->natm, dt, kick2, io->self_bgr, dev_e);
   return cudaGetLastError();
 }
 

@@ -284,6 +284,13 @@ __device__ void zfft2(double2* a, double2* b, int ld, int nb, const double2* tw)
 // go to shared memory, then one warp per atom sums
 //   F_a += g (A_t Im h_a - B_t Re h_a),  h_a = e^{i g.R_a},
 // over the block's g-points into fpart[block][atom][3].
+// EES (ees.zq set; eesHartEextGchare / eesEwaldGchare, cp_hart_ext.C:1005-1340):
+// the per-type structure factors are b(g) Qhat_t(g), Qhat_t taken from the
+// transformed B-spline grids (types 2k, 2k+1 split from complex grid k by
+// the conjugate point -g); FORCES writes the per-type force transforms
+//   Y_t = v_t conj(rho b) + q_t ewf conj(b) S_q
+// (the Ewald part folded in by the type's charge) into ees.zy at g and, for
+// kx > 0, their conjugates at -g, instead of reducing over atoms here.
 template <int N1, int N2, bool FORCES>
 __global__ void __launch_bounds__(OA_NTHREADS, 2)
 k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, int nz,
@@ -292,9 +299,10 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
             int natm, int ntype, const int* __restrict__ atm_perm, RhoTypeOff toff,
             const double* __restrict__ q_type, const double2* __restrict__ phase, int ktab,
             const double* __restrict__ spl, int nspl, double gmin, double dg,
-            double* __restrict__ part, double* __restrict__ fpart) {
+            double* __restrict__ part, double* __restrict__ fpart, EesLocArgs ees) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ldz = nz + 1;
+  const bool use_ees = ees.zq != nullptr;
   constexpr bool TP = N1 > 0;  // two-pass compile-time transforms
   const int ldb = TP ? (ZLd<N1, N2>::PS > ldz ? ZLd<N1, N2>::PS : ldz) : ldz;
   double2* tw = (double2*)smem_raw;
@@ -310,7 +318,7 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
   // FORCES: [OA_LB * nz][ntype] per-type (A, B) coefficients after zoff
   double2* cf = (double2*)(smem_raw + (((size_t)((char*)(zoff + natm) - (char*)smem_raw) + 15) & ~(size_t)15));
   for (int ia = threadIdx.x; ia < natm; ia += blockDim.x) zoff[ia] = (atm_perm[ia] * 3 + 2) * nt + ktab;
-  for (int idx = threadIdx.x; idx < OA_LB * natm; idx += blockDim.x) {
+  for (int idx = use_ees ? OA_LB * natm : threadIdx.x; idx < OA_LB * natm; idx += blockDim.x) {
     const int lb = idx / natm, ia = idx - lb * natm;
     const int l = l0 + lb;
     const int kx = l / ny;
@@ -350,11 +358,15 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
     double g2v[ZP_L], hh[ZP_L], wn[ZP_L];
     double vtt[ZP_L][4];  // FORCES: v_t(|g|) / V per type
     int cls[ZP_L], ii[ZP_L];  // cls: 0 outside, 1 g = 0, 2 inside the density sphere
+    size_t ep[ZP_L], em[ZP_L];  // EES: grid offsets of g and -g
+    double2 bgv[ZP_L];          // EES: b(g)
     bool any = false;
 #pragma unroll
     for (int j = 0; j < ZP_L; ++j) {
       const int lb = grp * ZP_L + j;
       cls[j] = 0; ii[j] = 1; hh[j] = 0.0; wn[j] = 1.0; g2v[j] = 0.0;
+      ep[j] = 0; em[j] = 0;
+      bgv[j] = make_double2(0.0, 0.0);
       rho[j] = make_double2(0.0, 0.0);
       sf_q[j] = make_double2(0.0, 0.0);
       vext[j] = make_double2(0.0, 0.0);
@@ -362,6 +374,14 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
       const int l = l0 + lb;
       const int kx = l / ny;
       int ky = l - kx * ny; if (2 * ky >= ny) ky -= ny;
+      if (use_ees && abs(kx) <= ktab && abs(ky) <= ktab && abs(kz) <= ktab) {
+        // kx >= 0 here; |k| <= ktab < n / 2 on each axis of the EES grid
+        const int ia = kx, ib = ky < 0 ? ky + ees.nb : ky, ic = kz < 0 ? kz + ees.nc : kz;
+        const int iam = kx == 0 ? 0 : ees.na - kx, ibm = ky > 0 ? ees.nb - ky : -ky, icm = kz > 0 ? ees.nc - kz : -kz;
+        ep[j] = ((size_t)ic * ees.nb + ib) * ees.na + ia;
+        em[j] = ((size_t)icm * ees.nb + ibm) * ees.na + iam;
+        bgv[j] = cmul(cmul(ees.ba[ia], ees.bb[ib]), ees.bc[ic]);
+      }
       const double gx = tpi_l * kx, gy = tpi_l * ky;
       const double g2 = gx * gx + gy * gy + gzv * gzv;
       g2v[j] = g2;
@@ -387,13 +407,26 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
         double2 st[ZP_L];
 #pragma unroll
         for (int j = 0; j < ZP_L; ++j) st[j] = make_double2(0.0, 0.0);
-        const double2* pl = pxy + grp * ZP_L * natm;
-        for (int ia = toff.off[t]; ia < toff.off[t + 1]; ++ia) {
-          const double2 hz = phase[zoff[ia] + kz];
+        if (use_ees) {
+          // Qhat_t = (Z +- conj Z(-g)) / (2 or 2i) of grid t / 2, times b(g)
+          const double2* zg = ees.zq + (size_t)(t >> 1) * ees.gstride;
 #pragma unroll
           for (int j = 0; j < ZP_L; ++j) {
-            const double2 h = cmul(pl[j * natm + ia], hz);
-            st[j].x += h.x; st[j].y += h.y;
+            if (cls[j] != 2) continue;
+            const double2 z = zg[ep[j]], zm = zg[em[j]];
+            const double2 qh = (t & 1) ? make_double2(0.5 * (z.y + zm.y), 0.5 * (zm.x - z.x))
+                                       : make_double2(0.5 * (z.x + zm.x), 0.5 * (z.y - zm.y));
+            st[j] = cmul(bgv[j], qh);
+          }
+        } else {
+          const double2* pl = pxy + grp * ZP_L * natm;
+          for (int ia = toff.off[t]; ia < toff.off[t + 1]; ++ia) {
+            const double2 hz = phase[zoff[ia] + kz];
+#pragma unroll
+            for (int j = 0; j < ZP_L; ++j) {
+              const double2 h = cmul(pl[j * natm + ia], hz);
+              st[j].x += h.x; st[j].y += h.y;
+            }
           }
         }
         const double qa = q_type[t];
@@ -414,8 +447,23 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
       if (lb >= nb) continue;
       double2 out = make_double2(0.0, 0.0);
       if (cls[j] == 1) {
-        out.x = gz_term;
-        acc[1] += gz_term * rho[j].x;
+        double gzt = gz_term;
+        if (use_ees) {
+          // sum_t gzvps_t b(0) Qhat_t(0) / V (eesHartEextGchare's g = 0 branch)
+          const double b0 = cmul(cmul(ees.ba[0], ees.bb[0]), ees.bc[0]).x;
+          gzt = 0.0;
+          for (int t = 0; t < ntype && t < 4; ++t) {
+            const double2 z0 = ees.zq[(size_t)(t >> 1) * ees.gstride];
+            const double yt = ees.gzvps[t] / vol * b0;
+            gzt += yt * ((t & 1) ? z0.y : z0.x);
+            if constexpr (FORCES) {
+              double* w0 = (double*)(ees.zy + (size_t)(t >> 1) * ees.gstride);
+              w0[t & 1] = yt * rho[j].x;
+            }
+          }
+        }
+        out.x = gzt;
+        acc[1] += gzt * rho[j].x;
       } else if (cls[j] == 2) {
         const double g2 = g2v[j];
         const double hf = fpi / (g2 * vol);
@@ -427,7 +475,31 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
         acc[1] += (rho[j].x * vext[j].x - rho[j].y * vext[j].y) * wn[j];  // Re(rho vext)
       }
       r[lb * ldz + zz] = out;
-      if constexpr (FORCES) {
+      if (FORCES && use_ees) {
+        if (cls[j] == 2) {
+          const double g2 = g2v[j];
+          const double ewf = fpi * exp(-g2 / falp2) / (g2 * vol);
+          const double2 cb = cconj(bgv[j]);
+          const double2 rb = cconj(cmul(rho[j], bgv[j]));
+          const double2 sqe = cmul(cb, sf_q[j]);
+          const bool mirror = l0 + lb >= ny;  // kx > 0
+          for (int t0 = 0; t0 < ntype && t0 < 4; t0 += 2) {
+            double2 y[2];
+            for (int u = 0; u < 2; ++u) {
+              const int t = t0 + u;
+              y[u] = make_double2(0.0, 0.0);
+              if (t < ntype) {
+                const double qt = q_type[t] * ewf;
+                y[u].x = vtt[j][t] * rb.x + qt * sqe.x;
+                y[u].y = vtt[j][t] * rb.y + qt * sqe.y;
+              }
+            }
+            double2* w = ees.zy + (size_t)(t0 >> 1) * ees.gstride;
+            w[ep[j]] = make_double2(y[0].x - y[1].y, y[0].y + y[1].x);
+            if (mirror) w[em[j]] = make_double2(y[0].x + y[1].y, y[1].x - y[0].y);
+          }
+        }
+      } else if constexpr (FORCES) {
         double2* c2 = cf + ((size_t)lb * nz + zz) * ntype;
         for (int t = 0; t < ntype && t < 4; ++t) {
           double2 ab = make_double2(0.0, 0.0);
@@ -444,7 +516,7 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
     }
   }
   __syncthreads();
-  if constexpr (FORCES) {
+  if (FORCES && !use_ees) {
     // one warp per atom (type order), lanes over the block's (line, plane) points
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     for (int ia = warp; ia < natm; ia += nwarp) {
@@ -893,6 +965,19 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
   for (int t = 0; t < 5; ++t) toff.off[t] = c->type_off[t];
   const int nbz = oa_rho_z_nblk(c);
   const bool forces = c->ions != nullptr;
+  EesLocArgs ees{};
+  if (c->eesl) {
+    // B-spline grids of the atom types and their transform (and the force
+    // grids zeroed) before the z pass reads them
+    if ((e = oa_launch_eesl_front(c, s)) != cudaSuccess) return e;
+    const oa_eesl* L = c->eesl;
+    ees.zq = L->zq;
+    ees.zy = forces ? L->zy : nullptr;
+    ees.ba = L->ba; ees.bb = L->bb; ees.bc = L->bc;
+    ees.gzvps = L->gzvps;
+    ees.na = L->na; ees.nb = L->nb; ees.nc = L->nc;
+    ees.gstride = (size_t)L->na * L->nb * L->nc;
+  }
   auto zpass = [&](auto kern, int ldb) -> cudaError_t {
     size_t smz =
         (align_up_r(c->nz, 2) + (size_t)OA_LB * (c->nz + 1) + (size_t)OA_LB * ldb + (size_t)OA_LB * c->natm) *
@@ -907,7 +992,7 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
                                        4.0 * c->alp_ewd * c->alp_ewd, c->gzvps_sum / c->vol,
                                        c->natm, c->ntype, c->atm_perm, toff, c->q_type, c->phase, c->kmax_tab,
                                        c->spl, c->nspl, c->spl_gmin, c->spl_dg,
-                                       c->red + 3 * oa_rho_xc_nblk(), forces ? c->ions->fpart : nullptr);
+                                       c->red + 3 * oa_rho_xc_nblk(), forces ? c->ions->fpart : nullptr, ees);
     return cudaGetLastError();
   };
   auto ldb2 = [&](int n1, int n2) { const int p = (n1 * (n2 | 1)) | 1; return p > c->nz + 1 ? p : c->nz + 1; };
@@ -924,6 +1009,8 @@ cudaError_t oa_launch_rho_fft_hart(oa_ctx* c, cudaStream_t s) {
   if (e == cudaErrorNotSupported)
     e = forces ? zpass(k_rho_zpass<0, 0, true>, c->nz + 1) : zpass(k_rho_zpass<0, 0, false>, c->nz + 1);
   if (e != cudaSuccess) return e;
+  // EES: the force grids back to real space and the atom forces from them
+  if (c->eesl && forces && (e = oa_launch_eesl_forces(c, s)) != cudaSuccess) return e;
   // white-byrd: V_KS z-lines -= z^-1 (i g . h(g))
   if (c->gga && (e = gga_z(c, s, 1)) != cudaSuccess) return e;
   return rho_xy_bwd(c, s, (const double2*)c->dz, c->vxc, c->vks, c->precision == OA_FP64, 1, 0, 0);

@@ -73,7 +73,7 @@ struct oa_step_scratch {
   int flag_host[4];
   cudaGraphExec_t exec;   // PsiV reset .. S
   cudaGraphExec_t exec2;  // Psi T + the step record
-  const void* key[8];
+  const void* key[9];
   int key_nterm;
   double key_dt, key_tol;
   int graph_kernels;      // kernel launches of one graphed step (graph nodes + launches outside)
@@ -247,8 +247,8 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
   OA_CUDA_TRY(cudaMemsetAsync(w->flag, 0, 4 * sizeof(int), s));
   // the psi planes of the mixed products, from the psi the caller hands in
   if (st->mixed_nterm) OA_STEP_TRY(oa_planes_psi_refresh(c, s, st->psi, st->mixed_nterm));
-  const void* key[8] = {st->psi, st->psi_t, st->vpsi, st->T, stream, w->ring, c->ees,
-                        (const void*)(uintptr_t)c->xc_gen};
+  const void* key[9] = {st->psi, st->psi_t, st->vpsi, st->T, stream, w->ring, c->ees,
+                        (const void*)(uintptr_t)c->xc_gen, (const void*)(uintptr_t)c->eesl_gen};
   // the legacy default stream cannot be captured: launch eagerly there
   const bool capturable = s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread;
   // the cluster Newton-Schulz kernel is an ordinary launch: then the whole

@@ -8,6 +8,8 @@ complex B-spline factor of every g-vector (``get_bspline_wght1d``
 ``abinito_physics/cp_nonlocal/cp_ees_nonlocal.C:60-160``) and the l = 0
 projector factor dyp(g) = d(g) y00 p(|g|) of ``eesProjGchare`` (594-727).
 The per-step work (atom B-splines, grid FFTs, Z, ENL, forces) runs on the GPU.
+``local_grid`` gives the grid of the EES local pseudopotential path
+(``init_eext_ees``), whose setup is otherwise done by the library.
 """
 from __future__ import annotations
 
@@ -42,6 +44,24 @@ def nonlocal_grid(sysm, scale: float = 1.2, order: int = 6):
         grid.append(_fft_size(n))
     if min(grid) < order:
         raise ValueError("nonlocal grid smaller than the spline order")
+    return tuple(grid)
+
+
+def local_grid(sysm, scale: float = 1.2, order: int = 6):
+    """EES grid of the local pseudopotential (``init_eext_ees``,
+    ``set_cp_ewald.C:1419-1500``): n = int(2 scale (2 kmax + 1)) per axis, one
+    more if below 2 (2 kmax + 1), rounded up to an FFT size; kmax of the
+    state sphere.  The same scale and order keys as the nonlocal grid
+    (cp_pseudo_ees_scale, cp_pseudo_ees_order)."""
+    grid = []
+    for k in (sysm.kx, sysm.ky, sysm.kz):
+        nk = 2 * int(np.max(np.abs(k))) + 1
+        n = int(2.0 * scale * nk)
+        if n < 2 * nk:
+            n += 1
+        grid.append(_fft_size(n))
+    if min(grid) < order:
+        raise ValueError("EES local grid smaller than the spline order")
     return tuple(grid)
 
 

@@ -103,6 +103,7 @@ SIGNATURES = {
     "oa_gpu_cp_run": (C.c_int, [_vp, _vp, C.POINTER(CPState), C.c_int, _dp, _dp]),
     "oa_gpu_ees_init": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp]),
     "oa_gpu_nl_ees": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "oa_gpu_set_ees_local": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
     "oa_gpu_pc_forward_noalloc": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                             _vp]),
 }
@@ -221,6 +222,9 @@ class CPContext:
         xc = getattr(sysm, "xc", "pz_lda")
         if xc != "pz_lda":
             self.set_xc(xc, getattr(sysm, "gga_cut", 5.0e-5))
+        if getattr(sysm, "eext_ees", None) is not None:
+            na, nb, nc, order = sysm.eext_ees
+            self.set_ees_local((na, nb, nc), order)
 
     def set_ions(self, masses, vel=None):
         """Turn on ion dynamics in the native step (oa_gpu_set_ions): masses
@@ -241,6 +245,13 @@ class CPContext:
         vel = np.zeros((self.sys.natm, 3))
         _check(self._lib.oa_gpu_get_ions(self._h, self._stream(), pos.ctypes.data_as(_dp), vel.ctypes.data_as(_dp)))
         return pos, vel
+
+    def set_ees_local(self, grid, order: int = 6):
+        """Local pseudopotential and reciprocal Ewald sum by the EES method
+        (cp_eext_ees_opt on; oa_gpu_set_ees_local) on grid (na, nb, nc) with
+        B-splines of this order; grid None: the structure-factor method."""
+        na, nb, nc = (0, 0, 0) if grid is None else (int(g) for g in grid)
+        _check(self._lib.oa_gpu_set_ees_local(self._h, na, nb, nc, int(order)))
 
     def set_xc(self, functional: str, gradient_cutoff: float = 5.0e-5):
         """Exchange-correlation of the density path: "pz_lda" or "blyp"

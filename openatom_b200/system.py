@@ -102,6 +102,10 @@ class CPSystem:
     # \cp_ggac_typ{lyp}); gga_cut is \gradient_cutoff (default 5e-5)
     xc: str = "pz_lda"
     gga_cut: float = 5.0e-5
+    # local pseudopotential and reciprocal Ewald sum by the EES method
+    # (\cp_eext_ees_opt{on}): (na, nb, nc, order) of its B-spline grid, or
+    # None for the structure-factor method
+    eext_ees: tuple | None = None
 
     @property
     def vol(self) -> float:
@@ -374,12 +378,15 @@ PRESETS = {
 
 def make_system(preset: str = "w8", seed: int = 1234, nstate: int | None = None,
                 ecut_mass: float = 1.0e30, cmass0: float = 400.0, dt: float = 5.0,
-                xc: str = "pz_lda", pseudo: str = "shipped", **over) -> CPSystem:
+                xc: str = "pz_lda", pseudo: str = "shipped", eext_ees_order: int | None = None,
+                ees_scale: float = 1.2, **over) -> CPSystem:
     """A seeded water system of a preset.  pseudo: "shipped" splines the
     reference's O / H BLYP pseudopotentials (openatom_b200.pseudo, the
     make_vps_splin algorithm) on this box's spline grid; "analytic" uses
     Gaussian stand-ins (a Gaussian-smeared ion core and a Gaussian s
-    projector)."""
+    projector).  eext_ees_order: the local pseudopotential and reciprocal
+    Ewald sum by the EES method with B-splines of this order on the grid of
+    ees.local_grid(ees_scale) (cp_eext_ees_opt on); None: structure factors."""
     if xc not in ("pz_lda", "blyp"):
         raise ValueError("xc must be 'pz_lda' or 'blyp'")
     if pseudo not in ("shipped", "analytic"):
@@ -411,10 +418,14 @@ def make_system(preset: str = "w8", seed: int = 1234, nstate: int | None = None,
     # Ewald splitting parameter: alpha = 3.5 / (L/2) style default (screening
     # length well inside the box)
     alp_ewd = 7.0 / box
-    return CPSystem(name=preset, seed=seed, box=box, nfft=nfft, ecut_ry=ecut_ry,
+    sysm = CPSystem(name=preset, seed=seed, box=box, nfft=nfft, ecut_ry=ecut_ry,
                     nstate=nstate, pos=pos, atm_type=typ, q=q, type_names=("O", "H"),
                     gzvps=gz, vloc=vloc, alp_ewd=alp_ewd, kx=kx, ky=ky, kz=kz,
                     line_kx=lkx, line_ky=lky, line_off=loff, line_nneg=lneg, line_npos=lpos,
                     nkx0=nkx0, nkx0_red=nred, nkx0_uni=nuni, nkx0_zero=nzero,
                     occ=np.ones(nstate), cmass=cmass, psi=psi, dt=dt, cmass0=cmass0,
                     nl_proj=nl_proj, nl_vnorm=nl_vnorm, nl_gz0=nl_gz0, xc=xc)
+    if eext_ees_order is not None:
+        from .ees import local_grid
+        sysm.eext_ees = local_grid(sysm, ees_scale, int(eext_ees_order)) + (int(eext_ees_order),)
+    return sysm
