@@ -385,16 +385,17 @@ oa_status oa_gpu_energies(oa_ctx *ctx, void *stream, double *out11);
 /* Ion dynamics in the native step (oa_gpu_cp_step / oa_gpu_cp_run): each
  * step computes the forces on the atoms at their current positions -- the
  * local pseudopotential and reciprocal Ewald part of CP_hart_eext_calc
- * (cp_hart_ext.C:56-431, in the density z pass), the structure-factor
- * nonlocal part of CP_enl_atm_forc_calc (cp_nl_energy_forc.C:178-235) and
- * the real-space Ewald sum of CPRSPACEION::CP_getionforce
- * (cp_ions/cp_rspace_ion.C:25-251) -- and moves them by the NVE integrator of
- * AtomsCompute::integrateAtoms (drv/main/AtomsCompute.C:461-640,
- * integration_drivers.C:17-85): second half kick of the previous step
- * (not on a run's first step), first half kick, drift.  masses: host [natm]
- * in electron masses; vel: host [natm][3] (null: zero).  Not with the EES
- * nonlocal path (its atom forces are not built; OA_ERR_BAD_ARG), and
- * oa_gpu_cp_run then takes no pos_host. */
+ * (cp_hart_ext.C:56-431, in the density z pass) or of the EES local path
+ * (eesAtmForceRchare, cp_hart_ext.C:1357-1470; oa_gpu_set_ees_local), the
+ * nonlocal part by the structure-factor method (CP_enl_atm_forc_calc,
+ * cp_nl_energy_forc.C:178-235) or the EES method (eesEnergyAtmForcRchare,
+ * cp_ees_nonlocal.C:1560-1720; oa_gpu_ees_init), and the real-space Ewald
+ * sum of CPRSPACEION::CP_getionforce (cp_ions/cp_rspace_ion.C:25-251) -- and
+ * moves them by the NVE integrator of AtomsCompute::integrateAtoms
+ * (drv/main/AtomsCompute.C:461-640, integration_drivers.C:17-85): second
+ * half kick of the previous step (not on a run's first step), first half
+ * kick, drift.  masses: host [natm] in electron masses; vel: host [natm][3]
+ * (null: zero).  oa_gpu_cp_run then takes no pos_host. */
 oa_status oa_gpu_set_ions(oa_ctx *ctx, const double *masses, const double *vel);
 
 /* Current atom positions and velocities (host [natm][3] each, either may be

@@ -1288,7 +1288,8 @@ cudaError_t oa_step_ortho_args(oa_ctx* c, double** work, int** status, double** 
 static void ees_free(oa_ctx* c) {
   oa_ees* e = c->ees;
   if (!e) return;
-  void* dev[] = {e->tw_a, e->tw_b, e->tw_c, e->zbuf, e->dyp, e->idx, e->mn, e->zpart, e->zmat, e->zs, e->enl};
+  void* dev[] = {e->tw_a, e->tw_b, e->tw_c, e->zbuf, e->dyp, e->idx, e->mn, e->zpart, e->zmat, e->zs, e->enl,
+                 e->dmn, e->fpart};
   for (void* q : dev) if (q) cudaFree(q);
   free(e);
   c->ees = nullptr;
@@ -1301,7 +1302,6 @@ extern "C" oa_status oa_gpu_ees_init(oa_ctx* c, int na, int nb, int nc, int orde
   OA_ARG_CHECK(order >= 4 && order <= 16 && order % 2 == 0, "EES order must be even, 4..16 (cp_pseudo_ees_order)");
   OA_ARG_CHECK(na >= order && nb >= order && nc >= order, "EES grid smaller than the interpolation order");
   OA_ARG_CHECK(c->natm_nl > 0, "no nonlocal atoms");
-  OA_ARG_CHECK(!c->ions, "ion dynamics needs the structure-factor nonlocal path (the EES atom forces are not built)");
   ees_free(c);
   oa_ees* e = (oa_ees*)calloc(1, sizeof(oa_ees));
   if (!e) return OA_ERR_CUDA;
@@ -1338,6 +1338,8 @@ extern "C" oa_status oa_gpu_ees_init(oa_ctx* c, int na, int nb, int nc, int orde
   TRYE(cudaMalloc(&e->zmat, (size_t)c->nstate * c->natm_nl * sizeof(double)));
   TRYE(cudaMalloc(&e->zs, (size_t)c->nstate * c->natm_nl * sizeof(double)));
   TRYE(cudaMalloc(&e->enl, (size_t)c->nstate * sizeof(double)));
+  TRYE(cudaMalloc(&e->dmn, (size_t)c->natm_nl * 3 * order * sizeof(double)));
+  TRYE(cudaMalloc(&e->fpart, (size_t)c->nstate * c->natm_nl * order * 3 * sizeof(double)));
 #undef TRYE
   return OA_OK;
 }

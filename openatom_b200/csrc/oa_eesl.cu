@@ -14,41 +14,7 @@
 // one complex transform serves two real ones; the Ewald force grid is folded
 // into the per-type grids by the type's charge in g-space.
 #include "oa_internal.h"
-
-// Cardinal B-spline stencil of one coordinate (eesAtmBsplineRgrp,
-// cp_hart_ext.C:719-820): grid points it - (j - 2), j = 1..order, wrapped
-// onto [0, ngrid), weights M_n(frac + j - 1) and dM_n = M_{n-1}(u) - M_{n-1}(u - 1).
-__device__ static void eesl_axis(double x, double box, int ngrid, int order, int* idx, double* m, double* dm) {
-  double u0 = x / box;
-  u0 -= rint(u0 - 0.5);
-  if (u0 == 1.0) u0 = 0.0;
-  u0 *= (double)ngrid;
-  const int it = (int)u0;
-  const double frac = u0 - (double)it;
-  double w[17];
-  for (int j = 0; j <= order; ++j) w[j] = 0.0;
-  w[1] = 1.0 - fabs(frac - 1.0);
-  w[2] = 1.0 - fabs(frac + 1.0 - 1.0);
-  for (int n = 3; n <= order; ++n) {
-    const double rn1 = 1.0 / (double)(n - 1);
-    for (int j = n; j >= 2; --j) {
-      const double u = frac + (double)(j - 1);
-      w[j] = (u * w[j] + ((double)n - u) * w[j - 1]) * rn1;
-    }
-    w[1] = frac * w[1] * rn1;
-    if (n == order - 1 && dm) {
-      dm[0] = w[1];
-      for (int j = 2; j <= order; ++j) dm[j - 1] = w[j] - w[j - 1];
-    }
-  }
-  for (int j = 1; j <= order; ++j) {
-    int g = it - (j - 2);
-    g = g > 0 ? g : ngrid + g;
-    g = g <= ngrid ? g : g - ngrid;
-    idx[j - 1] = g - 1;
-    m[j - 1] = w[j];
-  }
-}
+#include "oa_bspline.cuh"
 
 // One warp per atom: lanes 0..2 build the axis stencils, then the warp adds
 // M_a M_b M_c over the order^3 points into the atom type's grid slot.
@@ -61,7 +27,7 @@ __global__ void __launch_bounds__(32) k_eesl_spread(const double* __restrict__ p
   if (a >= natm) return;
   if (lane < 3) {
     const int ng = lane == 0 ? na : (lane == 1 ? nb : nc);
-    eesl_axis(pos[3 * a + lane], box, ng, order, sidx[lane], sm[lane], nullptr);
+    ees_bspline_axis(pos[3 * a + lane], box, ng, order, sidx[lane], sm[lane], nullptr);
   }
   __syncwarp();
   const int t = atm_type[a];
@@ -125,7 +91,7 @@ __global__ void __launch_bounds__(32) k_eesl_force(const double* __restrict__ po
   if (a >= natm) return;
   if (lane < 3) {
     const int ng = lane == 0 ? na : (lane == 1 ? nb : nc);
-    eesl_axis(pos[3 * a + lane], box, ng, order, sidx[lane], sm[lane], sd[lane]);
+    ees_bspline_axis(pos[3 * a + lane], box, ng, order, sidx[lane], sm[lane], sd[lane]);
   }
   __syncwarp();
   const int t = atm_type[a];

@@ -37,6 +37,8 @@ struct oa_ees {
   double* zmat;        // [nstate][natm_nl]
   double* zs;          // [nstate][natm_nl]
   double* enl;         // [nstate]
+  double* dmn;         // [natm_nl][3][order] B-spline derivative weights (ion dynamics)
+  double* fpart;       // [nstate][natm_nl][order][3] per-plane atom-force sums (ion dynamics)
 };
 
 // EES local pseudopotential and reciprocal Ewald path (oa_gpu_set_ees_local,
@@ -195,6 +197,7 @@ cudaError_t oa_launch_ees(oa_ctx* c, cudaStream_t s, const double2* psi, double2
 cudaError_t oa_launch_ees_zreduce(oa_ctx* c, cudaStream_t s);
 cudaError_t oa_launch_ees_bspline(oa_ctx* c, cudaStream_t s);
 cudaError_t oa_launch_nl_sf_force(oa_ctx* c, cudaStream_t s, const double* psi);
+cudaError_t oa_launch_ees_atom_force(oa_ctx* c, cudaStream_t s);
 cudaError_t oa_launch_eesl_front(oa_ctx* c, cudaStream_t s);
 cudaError_t oa_launch_eesl_forces(oa_ctx* c, cudaStream_t s);
 void oa_eesl_free(oa_ctx* c);

@@ -4,6 +4,9 @@
 // Replaces:
 //   CPNONLOCAL::CP_enl_atm_forc_calc (cp_nl_energy_forc.C:178-235) with the
 //     derivative structure factors of CP_calc_Struct_Fact (cp_struct_fact.C)  -> GEMM + k_nl_sf_force
+//   the atom-force loop of CPNONLOCAL::eesEnergyAtmForcRchare
+//     (cp_ees_nonlocal.C:1560-1720), EES nonlocal method                      -> k_ees_atom_force
+//     (the per-plane sums come from the Z gather, ees_gather_plane)
 //   CPRSPACEION::CP_getionforce (cp_ions/cp_rspace_ion.C:25-251)              -> k_ewald_rspace
 //   AtomsCompute::integrateAtoms (drv/main/AtomsCompute.C:461-640) ->
 //     ATOMINTEGRATE::integrate_nve_2nd_half / integrate_nve_1st_half
@@ -62,6 +65,33 @@ __global__ void k_nl_sf_force(const double2* __restrict__ y, const double2* __re
     fnl[3 * at + 0] = s * f[0];
     fnl[3 * at + 1] = s * f[1];
     fnl[3 * at + 2] = s * f[2];
+  }
+}
+
+// EES nonlocal atom forces (eesEnergyAtmForcRchare's force loop,
+// cp_ees_nonlocal.C:1560-1720): F_a = -sum_s zs[s][a] sum over the stencil
+// planes of the gathered sums (x n_a / L, y n_b / L, z n_c / L), with zs the
+// scaled Z = 2 vnorm / V occ Z.  One block per nonlocal atom.
+__global__ void k_ees_atom_force(const double* __restrict__ fpart, const double* __restrict__ zs, int nstate,
+                                 int natm_nl, int order, const int* __restrict__ nl_atm, double sa, double sb,
+                                 double sc, double* __restrict__ fnl) {
+  __shared__ double sh[3 * 32];
+  const int a = blockIdx.x;
+  double f[3] = {0.0, 0.0, 0.0};
+  for (int i = threadIdx.x; i < nstate * order; i += blockDim.x) {
+    const int s = i / order, jc = i - s * order;
+    const double z = zs[(size_t)s * natm_nl + a];
+    const double* fp = fpart + (((size_t)s * natm_nl + a) * order + jc) * 3;
+    f[0] += z * fp[0];
+    f[1] += z * fp[1];
+    f[2] += z * fp[2];
+  }
+  ion_block_sum3(f, sh);
+  if (threadIdx.x == 0) {
+    const int at = nl_atm[a];
+    fnl[3 * at + 0] = -sa * f[0];
+    fnl[3 * at + 1] = -sb * f[1];
+    fnl[3 * at + 2] = -sc * f[2];
   }
 }
 
@@ -215,6 +245,18 @@ static double ewald_self_bgr(const oa_ctx* c, const double* q_host) {
   return vself * (1.0 - erfc_x) + vbgr;
 }
 
+cudaError_t oa_launch_ees_atom_force(oa_ctx* c, cudaStream_t s) {
+  oa_ions* io = c->ions;
+  const oa_ees* e = c->ees;
+  cudaError_t err = cudaMemsetAsync(io->fnl, 0, (size_t)3 * c->natm * sizeof(double), s);
+  if (err != cudaSuccess) return err;
+  if (c->natm_nl == 0) return cudaSuccess;
+  k_ees_atom_force<<<c->natm_nl, 128, 0, s>>>(e->fpart, e->zs, c->nstate, c->natm_nl, e->order, c->nl_atm,
+                                              (double)e->na / c->box, (double)e->nb / c->box, (double)e->nc / c->box,
+                                              io->fnl);
+  return cudaGetLastError();
+}
+
 // the real-space Ewald sum and the integration, at the end of a step's
 // force work (the next step's phase tables see the new positions)
 cudaError_t oa_launch_ion_step(oa_ctx* c, cudaStream_t s, double* dev_e, double dt, int kick2) {
@@ -240,11 +282,6 @@ int oa_rho_z_nblk(const oa_ctx* c);
 extern "C" oa_status oa_gpu_set_ions(oa_ctx* c, const double* masses, const double* vel) {
   if (!c || !masses) {
     oa_set_error("null argument", __FILE__, __LINE__);
-    return OA_ERR_BAD_ARG;
-  }
-  if (c->ees) {
-    oa_set_error("ion dynamics needs the structure-factor nonlocal path (the EES atom forces are not built)",
-                 __FILE__, __LINE__);
     return OA_ERR_BAD_ARG;
   }
   for (int a = 0; a < c->natm; ++a)

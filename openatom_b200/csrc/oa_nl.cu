@@ -13,6 +13,7 @@
 // e^{i g.R} recursion becomes one product of three table entries).  In the
 // mixed form the kernel also writes the bf16 planes of SF (oa_planes.cuh).
 #include "oa_internal.h"
+#include "oa_bspline.cuh"
 
 __global__ void k_nl_sf(const int* __restrict__ kx, const int* __restrict__ ky, const int* __restrict__ kz, int ng,
                         const int* __restrict__ nl_atm, int natm_nl, const int* __restrict__ atm_type,
@@ -88,38 +89,16 @@ cudaError_t oa_launch_nl_zscale(cudaStream_t s, const double* Z, int nstate, int
 
 // CPNONLOCAL::eesAtmBsplineRgrp (cp_ees_nonlocal.C:256-593): cardinal
 // B-spline of order n at the fractional grid coordinate of each nonlocal atom,
-// per axis; stencil index it - (j - 2) wrapped onto [0, ngrid).
+// per axis, and (dmn not null) its derivative weights for the atom forces.
 __global__ void k_ees_bspline(const double* __restrict__ pos, const int* __restrict__ nl_atm, int natm_nl, double box,
-                              int na, int nb, int nc, int order, int* __restrict__ idx, double* __restrict__ mn) {
+                              int na, int nb, int nc, int order, int* __restrict__ idx, double* __restrict__ mn,
+                              double* __restrict__ dmn) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= natm_nl * 3) return;
   const int a = t / 3, ax = t - a * 3;
   const int ngrid = ax == 0 ? na : (ax == 1 ? nb : nc);
-  double u0 = pos[nl_atm[a] * 3 + ax] / box;
-  u0 -= rint(u0 - 0.5);
-  if (u0 == 1.0) u0 = 0.0;
-  u0 *= (double)ngrid;
-  const int it = (int)u0;
-  const double frac = u0 - (double)it;
-  double m[17];
-  for (int j = 0; j <= order; ++j) m[j] = 0.0;
-  m[1] = 1.0 - fabs(frac - 1.0);
-  m[2] = 1.0 - fabs(frac + 1.0 - 1.0);
-  for (int n = 3; n <= order; ++n) {
-    const double rn1 = 1.0 / (double)(n - 1);
-    for (int j = n; j >= 2; --j) {
-      const double u = frac + (double)(j - 1);
-      m[j] = (u * m[j] + ((double)n - u) * m[j - 1]) * rn1;
-    }
-    m[1] = frac * m[1] * rn1;
-  }
-  for (int j = 1; j <= order; ++j) {
-    int g = it - (j - 2);
-    g = g > 0 ? g : ngrid + g;
-    g = g <= ngrid ? g : g - ngrid;
-    idx[((size_t)a * 3 + ax) * order + (j - 1)] = g - 1;
-    mn[((size_t)a * 3 + ax) * order + (j - 1)] = m[j];
-  }
+  const size_t o = ((size_t)a * 3 + ax) * order;
+  ees_bspline_axis(pos[nl_atm[a] * 3 + ax], box, ngrid, order, idx + o, mn + o, dmn ? dmn + o : nullptr);
 }
 
 // Z = sum over stencil planes; ENL = occ vnorm/V sum Z^2; zs = 2 vnorm/V occ Z
@@ -146,7 +125,7 @@ cudaError_t oa_launch_ees_bspline(oa_ctx* c, cudaStream_t s) {
   oa_ees* e = c->ees;
   const int n = c->natm_nl * 3;
   k_ees_bspline<<<(n + 127) / 128, 128, 0, s>>>(c->pos, c->nl_atm, c->natm_nl, c->box, e->na, e->nb, e->nc, e->order,
-                                                 e->idx, e->mn);
+                                                 e->idx, e->mn, c->ions ? e->dmn : nullptr);
   return cudaGetLastError();
 }
 

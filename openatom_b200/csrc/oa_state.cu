@@ -145,19 +145,7 @@ k_state_plane(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int
       // scatter Z M onto this plane (eesEnergyAtmForcRchare: projPsiRScr[igrid] += z Mn)
       for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) tile[i] = (R)0;
       __syncthreads();
-      const int o2 = E.order * E.order;
-      for (int a = warp; a < E.natm; a += OA_PLANE_WARPS) {
-        const int* ia = E.idx + (size_t)a * 3 * E.order;
-        const double* ma = E.mn + (size_t)a * 3 * E.order;
-        int jc = -1;
-        for (int j = 0; j < E.order; ++j) if (ia[2 * E.order + j] == z) jc = j;
-        if (jc < 0) continue;
-        const double zc = E.zs[(size_t)s * E.natm + a] * ma[2 * E.order + jc];
-        for (int q = lane; q < o2; q += 32) {
-          const int jb = q / E.order, ja = q - jb * E.order;
-          atomicAdd(&tile[ia[E.order + jb] * nx + ia[ja]], (R)(zc * ma[E.order + jb] * ma[ja]));
-        }
-      }
+      ees_scatter_plane<R>(tile, nx, z, s, E, warp, lane, OA_PLANE_WARPS);
       __syncthreads();
     } else {
       for (int i = threadIdx.x; i < nkx * ldy; i += blockDim.x) P[i] = cmk<C>(0.0, 0.0);
@@ -241,22 +229,7 @@ k_state_plane(typename CplxOf<R>::T* __restrict__ zbuf, int nstate, int ldl, int
     __syncthreads();
     if (MODE == 2) {
       // Z gather over the stencil points of this plane (eesZmatRchare)
-      const int o2 = E.order * E.order;
-      for (int a = warp; a < E.natm; a += OA_PLANE_WARPS) {
-        const int* ia = E.idx + (size_t)a * 3 * E.order;
-        const double* ma = E.mn + (size_t)a * 3 * E.order;
-        int jc = -1;
-        for (int j = 0; j < E.order; ++j) if (ia[2 * E.order + j] == z) jc = j;
-        if (jc < 0) continue;
-        double acc = 0.0;
-        for (int q = lane; q < o2; q += 32) {
-          const int jb = q / E.order, ja = q - jb * E.order;
-          acc += (double)tile[ia[E.order + jb] * nx + ia[ja]] * ma[E.order + jb] * ma[ja];
-        }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-        if (lane == 0) E.zpart[((size_t)s * E.natm + a) * E.order + jc] = acc * ma[2 * E.order + jc];
-      }
+      ees_gather_plane<R>(tile, nx, z, s, E, warp, lane, OA_PLANE_WARPS);
       __syncthreads();
     }
     if (MODE == 1 || MODE == 3) {
@@ -535,7 +508,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
     if ((err = cudaGetLastError()) != cudaSuccess) return err;
   }
   PlaneSmem L = plane_smem_layout<C, R>(e->na, e->nb, c->nkx_s);
-  EesArgs E = {e->idx, e->mn, e->zpart, e->zs, c->natm_nl, e->order};
+  EesArgs E = {e->idx, e->mn, e->zpart, e->zs, c->natm_nl, e->order, e->dmn, c->ions ? e->fpart : nullptr};
   dim3 pgrid(e->nc, e->ngroup);
   const bool pp = e->na == e->nb && oa_pencil_supported(e->na);
   err = cudaErrorNotSupported;
@@ -553,6 +526,8 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
   if (err != cudaSuccess) return err;
   err = oa_launch_ees_zreduce(c, st);
   if (err != cudaSuccess) return err;
+  // with ion dynamics: the nonlocal atom forces from the gathered sums and zs
+  if (c->ions && (err = oa_launch_ees_atom_force(c, st)) != cudaSuccess) return err;
   err = cudaErrorNotSupported;
   if (pp)
     err = oa_pencil_plane(c->precision, 3, st, e->na, e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky,

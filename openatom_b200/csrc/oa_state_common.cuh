@@ -55,6 +55,8 @@ struct EesArgs {
   double* zpart;        // [nstate][natm][order] MODE 2: per-plane Z contributions
   const double* zs;     // [nstate][natm]        MODE 3: scaled Z to scatter
   int natm, order;
+  const double* dmn;    // [natm][3][order] derivative weights (with fpart)
+  double* fpart;        // [nstate][natm][order][3] MODE 2, null: no atom forces
 };
 
 
@@ -82,22 +84,45 @@ __device__ __forceinline__ void ees_scatter_plane(R* tile, int nx, int z, int s,
 
 // EES Z gather on one plane (eesZmatRchare, cp_ees_nonlocal.C:1238-1352):
 // zpart[s][a][jc] = Mn_c(jc) sum over the a-b stencil of tile * Mn_a Mn_b.
+// With fpart the plane's share of the atom-force sums of
+// eesEnergyAtmForcRchare (1560-1720), before the zs and n / L factors:
+// (Mn_c sum tile dMn_a Mn_b, Mn_c sum tile Mn_a dMn_b, dMn_c sum tile Mn_a Mn_b).
 template <typename R>
 __device__ __forceinline__ void ees_gather_plane(const R* tile, int nx, int z, int s, const EesArgs& E, int warp,
                                                  int lane, int nwarp) {
   const int o2 = E.order * E.order;
+  const bool frc = E.fpart != nullptr;
   for (int a = warp; a < E.natm; a += nwarp) {
     const int* ia = E.idx + (size_t)a * 3 * E.order;
     const double* ma = E.mn + (size_t)a * 3 * E.order;
+    const double* da = frc ? E.dmn + (size_t)a * 3 * E.order : ma;
     int jc = -1;
     for (int j = 0; j < E.order; ++j) if (ia[2 * E.order + j] == z) jc = j;
     if (jc < 0) continue;
-    double acc = 0.0;
+    double acc = 0.0, fx = 0.0, fy = 0.0;
     for (int q = lane; q < o2; q += 32) {
       const int jb = q / E.order, ja = q - jb * E.order;
-      acc += (double)tile[ia[E.order + jb] * nx + ia[ja]] * ma[E.order + jb] * ma[ja];
+      const double v = (double)tile[ia[E.order + jb] * nx + ia[ja]];
+      acc += v * ma[E.order + jb] * ma[ja];
+      if (frc) {
+        fx += v * ma[E.order + jb] * da[ja];
+        fy += v * da[E.order + jb] * ma[ja];
+      }
     }
     acc = warp_sum(acc);
-    if (lane == 0) E.zpart[((size_t)s * E.natm + a) * E.order + jc] = acc * ma[2 * E.order + jc];
+    if (frc) {
+      fx = warp_sum(fx);
+      fy = warp_sum(fy);
+    }
+    if (lane == 0) {
+      const double mc = ma[2 * E.order + jc];
+      E.zpart[((size_t)s * E.natm + a) * E.order + jc] = acc * mc;
+      if (frc) {
+        double* fp = E.fpart + (((size_t)s * E.natm + a) * E.order + jc) * 3;
+        fp[0] = fx * mc;
+        fp[1] = fy * mc;
+        fp[2] = acc * da[2 * E.order + jc];
+      }
+    }
   }
 }

@@ -1198,7 +1198,7 @@ def _nl_default(psi, sysm):
     return f, float(enl.sum())
 
 
-def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl="auto", norb_tol=None, dt=None, ions=None):
+def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl="auto", norb_tol=None, dt=None, ions=None, ees=None):
     """One CPAIMD electronic step.  Order: forces on the orthonormal psi
     (computePsiFandVKS + NL, combineForcesGetEke), constraint force
     (computeLambdaAndCg), integrate (integrateModForce ->
@@ -1207,15 +1207,20 @@ def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl="auto", norb_tol=None, dt=Non
     forces at the positions of this step (ion_forces) and the NVE atom
     integration (integrate_ions, AtomsCompute::integrateAtoms,
     drv/main/AtomsCompute.C:461-640), after which the next step's structure
-    factors see the new positions.  Returns the energy record of the psi the
-    forces were evaluated on."""
+    factors see the new positions.  ees: the EES nonlocal setup (ees_setup)
+    that nl evaluates with; with ions its B-splines follow the atoms and the
+    nonlocal atom forces come from it.  Returns the energy record of the psi
+    the forces were evaluated on."""
     st.iteration += 1
+    if ees is not None and ions is not None:
+        ees["bspl"] = ees_bsplines(sysm, ees["grid"], ees["order"])
     if nl == "auto":
         nl = _nl_default if len(sysm.nl_atoms()) else None
     fnl, enl = (None, 0.0) if nl is None else nl(st.psi, sysm)
     if ions is not None:
         rho_r = density(state_g_to_r(st.psi, sysm), sysm)
-        fion, eion = ion_forces(st.psi, sysm, rho_r, nl="sf" if nl is not None else None)
+        nl_ion = None if nl is None else ("ees" if ees is not None else "sf")
+        fion, eion = ion_forces(st.psi, sysm, rho_r, nl=nl_ion, ees=ees)
     f, en = electronic_forces(st.psi, sysm, fnl, enl)
     if ions is not None:
         en.update(eion)

@@ -1,7 +1,7 @@
 """Ion dynamics in the native graphed step (oa_gpu_set_ions): the local
 pseudopotential and reciprocal Ewald atom forces of the density z pass, the
-structure-factor nonlocal atom forces, the real-space Ewald sum and the NVE
-atom integration, against the oracle's CP step with an IonState (whose
+nonlocal atom forces (structure-factor and EES methods), the real-space Ewald
+sum and the NVE atom integration, against the oracle's CP step with an IonState (whose
 forces are pinned to compiled cp_hart_ext.C, cp_nl_energy_forc.C and
 cp_rspace_ion.C).
 
@@ -88,13 +88,39 @@ def test_ion_dynamics_mixed_total_energy():
     d.ctx.close()
 
 
-def test_ion_dynamics_refuses_ees_and_host_positions():
+@pytest.mark.parametrize("preset,nstate,order", [("w2", None, 4), ("w8", 16, 6)])
+def test_ion_dynamics_ees_nonlocal_fp64(preset, nstate, order):
+    """EES nonlocal method with moving atoms: the B-splines follow the atoms
+    every step and the nonlocal atom forces come from the gathered stencil
+    sums (eesEnergyAtmForcRchare's force loop)."""
+    from openatom_b200.gpu import CPDriver
+    s, m, vel = _start(preset, nstate, 45)
+    d = CPDriver(s, "fp64", norb_tol=0.003, nl_method="ees", ees_order=order)
+    d.ctx.set_ions(m, vel)
+    got = d.run_native(d.native_state(use_graph=True), 6)
+    so = copy.deepcopy(s)
+    st = O.CPState(so)
+    ions = O.IonState(so, vel)
+    ees = O.ees_setup(so, 1.2, order)
+
+    def nl(psi, sysm):
+        f, enl, _ = O.nl_ees_energy_forces(psi, sysm, ees)
+        return f, float(enl.sum())
+
+    ref = [O.cp_step(st, so, nl=nl, norb_tol=0.003, ions=ions, ees=ees) for _ in range(6)]
+    for i, (g, r) in enumerate(zip(got, ref)):
+        for k in TERMS:
+            assert abs(g[k] - r[k]) <= 1e-10 * max(1.0, abs(r[k])), (i, k, g[k], r[k])
+    pos, v = d.ctx.get_ions()
+    assert np.max(np.abs(pos - so.pos)) <= 1e-10 * np.max(np.abs(so.pos))
+    assert np.max(np.abs(v - ions.v)) <= 1e-10 * np.max(np.abs(ions.v))
+    assert np.max(np.abs(d.psi.cpu().numpy() - st.psi)) <= 1e-9 * np.max(np.abs(st.psi))
+    d.ctx.close()
+
+
+def test_ion_dynamics_refuses_host_positions():
     from openatom_b200.gpu import CPDriver, OaError
     s, m, vel = _start("w2", None, 44)
-    d = CPDriver(s, "fp64", nl_method="ees", ees_order=4)
-    with pytest.raises(OaError):
-        d.ctx.set_ions(m, vel)
-    d.ctx.close()
     d = CPDriver(s, "fp64")
     d.ctx.set_ions(m, vel)
     with pytest.raises(OaError):
