@@ -53,6 +53,8 @@ def parse():
                     help="also time the 128 H2O / 512-state / 160^3 system in the mixed form (0: skip)")
     ap.add_argument("--blyp", type=int, default=1,
                     help="also time the 32-water step with the BLYP gradient correction (0: skip)")
+    ap.add_argument("--ions", type=int, default=1,
+                    help="also time the 32-water step with moving atoms (structure factors, EES local; 0: skip)")
     ap.add_argument("--drift-steps", type=int, default=1000,
                     help="steps of the 8-water precision run (energy drift, mixed vs FP64; 0: skip)")
     return ap.parse_args()
@@ -203,6 +205,44 @@ def blyp_form(torch, args):
             "mixed_over_fp64": res["fp64"] / res["mixed"], "dE_per_atom_max_steps_3_to_6": de,
             "egga": ens["fp64"][-1]["EGGA"], "quench_steps": min(args.quench, 12),
             "density_path_ms": {"blyp": kt["blyp"], "pz_lda": kt["pz_lda"]}}
+
+
+def ion_form(torch, args):
+    """Ion dynamics on the 32-water workload (NVE, atoms starting at 300 K):
+    mixed-form CP steps/s with the structure-factor local and nonlocal atom
+    forces and with the EES local path (order 6, cp_eext_ees_opt on), beside
+    the fixed-ion step, all from one quenched start."""
+    import copy
+    from openatom_b200.ees import local_grid
+    from openatom_b200.gpu import CPDriver
+    from openatom_b200.system import atom_masses
+    sysm = make_sys(args.config, args.seed)
+    psi0 = quenched_start(sysm, min(args.quench, 12))
+    m = atom_masses(sysm)
+    rng = np.random.default_rng(args.seed)
+    vel = rng.standard_normal(sysm.pos.shape) * np.sqrt(300.0 * 3.1668115634556e-6 / m)[:, None]
+    out = {}
+    k = 10
+    variants = (("fixed_ions", None, False), ("ions_sf", None, True), ("ions_ees_local6", 6, True))
+    for name, order, moving in variants:
+        s2 = copy.copy(sysm)
+        s2.pos = sysm.pos.copy()
+        if order:
+            s2.eext_ees = local_grid(s2, 1.2, order) + (order,)
+        d = CPDriver(s2, "mixed", psi0=psi0, norb_tol=NORB_TOL)
+        if moving:
+            d.ctx.set_ions(m, vel)
+        st = d.native_state(use_graph=True)
+        d.run_native(st, 3)
+        ms, _ = time_steps(torch, d, st, k)
+        out[name] = {"value": 1e3 / ms, "ms_per_step": ms}
+        if order:
+            out[name]["grid"] = list(s2.eext_ees[:3])
+        d.ctx.close()
+        del d
+    torch.cuda.empty_cache()
+    return {"workload": f"{args.config} with moving atoms: {sysm.natm // 3} H2O, {sysm.nstate} states, "
+                        f"NVE from 300 K", "steps": k, "precision": "mixed", **out}
 
 
 class ClockSampler:
@@ -535,6 +575,7 @@ def run_ours(args):
     batch = batch_form(torch, args) if (rk == 0 and args.batch > 0) else None
     large = large_form(torch, args) if (rk == 0 and args.large > 0) else None
     blyp = blyp_form(torch, args) if (rk == 0 and args.blyp > 0) else None
+    ions = ion_form(torch, args) if (rk == 0 and args.ions > 0) else None
 
     if rk == 0:
         # kernel launches of one mixed step, counted in its captured CUDA graph
@@ -565,6 +606,7 @@ def run_ours(args):
             "batch": batch,
             "large": large,
             "blyp": blyp,
+            "ions": ions,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -376,6 +376,17 @@ PRESETS = {
 }
 
 
+# atom masses in amu (O, H as in the reference's water examples) and the
+# amu -> electron-mass factor of PINY (piny_constants.h:55)
+ATOM_MASS_AMU = {"O": 15.9994, "H": 1.00794}
+PROT_MASS = 1822.8885
+
+
+def atom_masses(sysm) -> np.ndarray:
+    """[natm] atom masses in electron masses, for oa_gpu_set_ions."""
+    return np.array([ATOM_MASS_AMU[sysm.type_names[int(t)]] for t in sysm.atm_type]) * PROT_MASS
+
+
 def make_system(preset: str = "w8", seed: int = 1234, nstate: int | None = None,
                 ecut_mass: float = 1.0e30, cmass0: float = 400.0, dt: float = 5.0,
                 xc: str = "pz_lda", pseudo: str = "shipped", eext_ees_order: int | None = None,
