@@ -72,29 +72,12 @@ def make_sys(cfg, seed):
     return make_system(cfg, seed=seed, ecut_mass=2.0, cmass0=400.0, dt=5.0)
 
 
-def batch_systems(seed, nsys):
-    """Seeded set of uneven water systems for the batching form: 8-32 H2O at
-    about 1 g/cc, 4 states per molecule (32-128), 60/70/80 Ry, each on the
-    smallest two-pass grid that holds its density sphere (4 kmax)."""
-    from openatom_b200.system import make_system
-    rng = np.random.default_rng(seed)
-    out = []
-    for i in range(nsys):
-        nmol = int(rng.integers(8, 33))
-        ecut = float(rng.choice([60.0, 70.0, 80.0]))
-        box = 18.6 * (nmol / 32.0) ** (1.0 / 3.0)
-        kmax = int(math.floor(math.sqrt(ecut) / (2.0 * math.pi / box))) + 1
-        grid = next(g for g in (64, 96, 108, 160) if g >= 4 * kmax)
-        out.append(make_system("w32", seed=seed + 101 * i, nmol=nmol, box=box, ecut_ry=ecut,
-                               nfft=(grid, grid, grid), ecut_mass=2.0, cmass0=400.0, dt=5.0))
-    return out
-
-
 def batch_form(torch, args):
     """Batching form: args.batch independent systems advanced together, one
     CUDA graph per step (oa_gpu_cp_run_batch), against the same systems run
     one after the other (oa_gpu_cp_run each)."""
     from openatom_b200.gpu import CPDriver, run_batch
+    from openatom_b200.system import batch_systems
     syss = batch_systems(args.seed + 7, args.batch)
     drv = [CPDriver(s, "mixed") for s in syss]
     for d in drv:
@@ -122,7 +105,8 @@ def batch_form(torch, args):
            "grids": sorted({s.nfft[0] for s in syss}), "ecut_ry": sorted({s.ecut_ry for s in syss}),
            "steps": k, "ms_per_batch_step": ms_batch, "system_steps_per_s": n * 1e3 / ms_batch,
            "sequential_ms_per_batch_step": ms_seq, "speedup_vs_sequential": ms_seq / ms_batch,
-           "graph_kernels_per_step": batch_kernels, "precision": "mixed"}
+           "graph_kernels_per_step": batch_kernels, "precision": "mixed",
+           "tuned_systems": sum(1 for d in drv if d.ctx.tuning_source == "table")}
     del drv
     return out
 
@@ -550,6 +534,9 @@ def run_ours(args):
     kt = dmx.ctx.time_kernels(dmx.psi, reps=5)
     kt64 = d64.ctx.time_kernels(d64.psi, reps=5)
     roof = roofline(sysm, dmx, kt, args.config)
+    tuning = {"table": "openatom_b200/tuning/b200.json (openatom_b200.tuner)",
+              "mixed": {"source": dmx.ctx.tuning_source, **dmx.ctx.get_tuning()},
+              "fp64": {"source": d64.ctx.tuning_source, **d64.ctx.get_tuning()}}
     d64.ctx.close()
     dmx.ctx.close()
     del d64, dmx
@@ -595,6 +582,7 @@ def run_ours(args):
                       "psiv_resets": sum(1 for e in en_mx if e["SMAX"] > NORB_TOL),
                       "psiv_resets_fp64": sum(1 for e in en_64 if e["SMAX"] > NORB_TOL)},
             "kernel_ms": kt, "kernel_ms_fp64": kt64,
+            "tuning": tuning,
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": ws * 1e3 / ms_e2e, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * natm,

@@ -252,6 +252,33 @@ oa_status oa_gpu_set_atoms(oa_ctx *ctx, void *stream, const double *pos_host);
  * e.g. CP_State_GSpacePlane.C:1407-1409). */
 oa_status oa_gpu_time_kernels(oa_ctx *ctx, void *stream, const double *psi, int reps, double *ms_out);
 
+/* Runtime tile and schedule choices of a context: what the autotuner
+ * (openatom_b200/tuner.py) searches per system size.  No counterpart in the
+ * reference, whose decomposition is set by its Charm++ configuration
+ * (piny_to_driver/configure.C).  The group, dgemm and fft choices change
+ * at most the order of partial sums (results agree to rounding);
+ * tgemm_kblocks also sets how many terms each FP32 tensor-core
+ * accumulation holds (fewer blocks: longer FP32 sums, larger error), so
+ * the autotuner leaves it at the built-in choice, the most the partials
+ * allow. */
+typedef struct oa_tuning {
+  int group_state;   /* state groups of the per-state plane kernels: nz x groups blocks (1..32) */
+  int group_pair;    /* state-pair groups of the mixed state-pair plane kernels (1..32) */
+  int dgemm_kblocks; /* most split-K blocks of the FP64 tensor-core products (2..160) */
+  int tgemm_kblocks; /* most split-K blocks of the split-BF16 tcgen05 products (1..the limit set at init) */
+  int fft_path;      /* 1: two-pass register transforms where compiled; 2: runtime-plan shared-memory
+                        transforms (FP64 form only: the state-pair kernels are two-pass) */
+} oa_tuning;
+
+/* The current choices (after oa_gpu_init: the built-in heuristics). */
+oa_status oa_gpu_get_tuning(const oa_ctx *ctx, oa_tuning *out);
+
+/* Set the choices; a field of 0 keeps its value.  Out of range:
+ * OA_ERR_BAD_ARG; fft_path 2 in the mixed form: OA_ERR_UNSUPPORTED.  Grows
+ * the density partials when a group count grows (synchronising the
+ * device first); the next oa_gpu_cp_run re-makes its captured step. */
+oa_status oa_gpu_set_tuning(oa_ctx *ctx, const oa_tuning *in);
+
 /* Sizes for byte/flop accounting (see oa_abi.cu): out[0..12]. */
 oa_status oa_gpu_sizes(const oa_ctx *ctx, long *out);
 

@@ -114,6 +114,8 @@ struct oa_ctx_pc {
   double* vtmp;      // [nstate][ng] complex scratch
   float* upart;      // split-K FP32 partials of the tensor-core forward GEMM
   int umax_kb;
+  int umax_cap;      // split-K blocks upart holds
+  int nkb_cap;       // split-K blocks part holds
   void* pl_big[3];   // bf16 planes [3][mx][pl_ld] of the big operands (slots below)
   void* pl_ma;       // bf16 planes [3][mx][mx] of the small matrices
   void* pl_mb;
@@ -199,13 +201,15 @@ static bool column_runs(const oa_system_desc* d, int nkx, std::vector<int>* out)
   return true;
 }
 
-static int pick_groups(int nz, int nstate, int bps, int nsm) {
-  // minimise ceil(nz g / (nsm bps)) * ceil(nstate / g)
+static int pick_groups(int nz, int nstate, int bps, int nsm, int fixed = 0) {
+  // minimise ceil(nz g / (nsm bps)) * (ceil(nstate / g) + fixed): waves of
+  // blocks times the items each block runs, plus a fixed per-block cost in
+  // items (pipeline fill and drain, twiddle and table loads)
   int best = 1;
   long bestc = -1;
   for (int g = 1; g <= 32 && g <= nstate; ++g) {
     const long waves = (nz * (long)g + (long)nsm * bps - 1) / ((long)nsm * bps);
-    const long cost = waves * ((nstate + g - 1) / g);
+    const long cost = waves * ((nstate + g - 1) / g + fixed);
     if (bestc < 0 || cost < bestc) { bestc = cost; best = g; }
   }
   return best;
@@ -270,7 +274,10 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     if (bps < 1) bps = 1;
   }
   c->ngroup = pick_groups(d->nz, d->nstate, bps, nsm);
-  c->ngroup_pair = pick_groups(d->nz, (d->nstate + 1) / 2, 1, nsm);
+  // the state-pair kernels software-pipeline the pairs of a block: a fixed
+  // cost of about two pairs per block, which is what the autotuner's
+  // measurements over 8-32 water systems on 64^3-108^3 grids imply
+  c->ngroup_pair = pick_groups(d->nz, (d->nstate + 1) / 2, 1, nsm, 2);
   c->pair_kymax = 0;
   for (int l = 0; l < d->nlines; ++l) {
     const int a = d->line_ky[l] < 0 ? -d->line_ky[l] : d->line_ky[l];
@@ -361,11 +368,13 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
       c->nq2 = c->ngroup_pair * d->nz;
       TRY(cudaMalloc(&c->qpart, (size_t)c->nq * sizeof(double)));
       TRY(cudaMalloc(&c->qpart2, (size_t)c->nq2 * sizeof(double)));
+      c->nq2_cap = c->nq2;
       TRY(cudaMalloc(&c->qscale, sizeof(double)));
     }
     {
       const int ng = c->ngroup > c->ngroup_pair ? c->ngroup : c->ngroup_pair;
       TRY(cudaMalloc(&c->rho_part, (size_t)ng * c->npts * sizeof(double)));
+      c->rho_groups_cap = ng;
     }
     if (d->nx == d->ny && oa_pencil_supported(d->nx))
       TRY(cudaMalloc(&c->psir, (size_t)(d->nstate + 1) / 2 * 2 * c->npts * rsz));
@@ -378,6 +387,7 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
     TRY(cudaMalloc(&c->red, c->red_len * sizeof(double)));
     TRY(cudaMalloc(&c->eke_part, (size_t)d->nstate * c->nblk_z * sizeof(double)));
     p->nkb = 160;  // split-K partials: about one CTA per SM for a 128 x 128 product
+    p->nkb_cap = p->nkb;
     // split-K partials; also the block partials of the minimisation's |F|^2 (>= 1024)
     // (the nonlocal Z product is nstate x natm_nl: more columns than states
     // when there are more nonlocal atoms than states)
@@ -408,6 +418,7 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
       const size_t need = (size_t)(p->umax_kb > kbz ? p->umax_kb : kbz) * d->nstate * mx;
       TRY(cudaMalloc(&p->upart, need * sizeof(float)));
       p->umax_kb = p->umax_kb > kbz ? p->umax_kb : kbz;
+      p->umax_cap = p->umax_kb;
     }
     TRY(cudaMalloc(&p->err_flag, sizeof(int)));
     TRY(cudaMemset(p->err_flag, 0, sizeof(int)));
@@ -884,6 +895,67 @@ extern "C" oa_status oa_gpu_time_kernels(oa_ctx* c, void* stream, const double* 
 // nstate, ng, nlines, nz, ldl, ngroup, npts, compute-precision bytes per
 // real, nlines_d, kernel launches per CP step of the host runner, state-pair
 // plane kernels in use, their state groups, int8 overlap / rotation in use.
+extern "C" oa_status oa_gpu_get_tuning(const oa_ctx* c, oa_tuning* t) {
+  OA_ARG_CHECK(c && t, "null argument");
+  const oa_ctx_pc* p = pcx(const_cast<oa_ctx*>(c));
+  t->group_state = c->ngroup;
+  t->group_pair = c->ngroup_pair;
+  t->dgemm_kblocks = p->nkb;
+  t->tgemm_kblocks = p->umax_kb;
+  t->fft_path = c->fft_runtime ? 2 : 1;
+  return OA_OK;
+}
+
+extern "C" oa_status oa_gpu_set_tuning(oa_ctx* c, const oa_tuning* t) {
+  OA_ARG_CHECK(c && t, "null argument");
+  oa_ctx_pc* p = pcx(c);
+  const int npair = (c->nstate + 1) / 2;
+  OA_ARG_CHECK(t->group_state >= 0 && t->group_state <= 32 && t->group_state <= c->nstate,
+               "group_state must be 1..min(32, nstate) (0 keeps it)");
+  OA_ARG_CHECK(t->group_pair >= 0 && t->group_pair <= 32 && t->group_pair <= npair,
+               "group_pair must be 1..min(32, state pairs) (0 keeps it)");
+  OA_ARG_CHECK(t->dgemm_kblocks == 0 || (t->dgemm_kblocks >= 2 && t->dgemm_kblocks <= p->nkb_cap),
+               "dgemm_kblocks must be 2..160 (0 keeps it)");
+  OA_ARG_CHECK(t->tgemm_kblocks >= 0 && t->tgemm_kblocks <= p->umax_cap,
+               "tgemm_kblocks above the split-K partials allocated at init");
+  OA_ARG_CHECK(t->fft_path >= 0 && t->fft_path <= 2, "fft_path must be 1 or 2 (0 keeps it)");
+  if (t->fft_path == 2 && c->precision == OA_MIXED) {
+    oa_set_error("fft_path 2: the mixed form's state-pair kernels need the two-pass transforms", __FILE__, __LINE__);
+    return OA_ERR_UNSUPPORTED;
+  }
+  const int gs = t->group_state ? t->group_state : c->ngroup;
+  const int gp = t->group_pair ? t->group_pair : c->ngroup_pair;
+  const int need = gs > gp ? gs : gp;
+  if (need > c->rho_groups_cap || (c->pair_cols && gp * c->nz > c->nq2_cap)) {
+    OA_CUDA_TRY(cudaDeviceSynchronize());
+    if (need > c->rho_groups_cap) {
+      double* r = nullptr;
+      OA_CUDA_TRY(cudaMalloc(&r, (size_t)need * c->npts * sizeof(double)));
+      cudaFree(c->rho_part);
+      c->rho_part = r;
+      c->rho_groups_cap = need;
+    }
+    if (c->pair_cols && gp * c->nz > c->nq2_cap) {
+      double* q = nullptr;
+      OA_CUDA_TRY(cudaMalloc(&q, (size_t)gp * c->nz * sizeof(double)));
+      cudaFree(c->qpart2);
+      c->qpart2 = q;
+      c->nq2_cap = gp * c->nz;
+    }
+  }
+  c->ngroup = gs;
+  c->ngroup_pair = gp;
+  if (c->pair_cols) c->nq2 = gp * c->nz;
+  if (t->dgemm_kblocks) p->nkb = t->dgemm_kblocks;
+  if (t->tgemm_kblocks) p->umax_kb = t->tgemm_kblocks;
+  if (t->fft_path) c->fft_runtime = t->fft_path == 2 ? 1 : 0;
+  c->rho_ngroup = c->ngroup;
+  c->psir_valid = 0;
+  c->qvalid = 0;
+  c->xc_gen += 1;  // the captured step is re-made with the new launch shapes
+  return OA_OK;
+}
+
 extern "C" oa_status oa_gpu_sizes(const oa_ctx* c, long* out) {
   OA_ARG_CHECK(c && out, "null argument");
   out[0] = c->nstate; out[1] = c->ng; out[2] = c->nlines; out[3] = c->nz; out[4] = c->ldl;

@@ -163,6 +163,9 @@ struct oa_ctx {
   oa_ions *ions;          // ion dynamics, after oa_gpu_set_ions
   oa_eesl *eesl;          // EES local path, after oa_gpu_set_ees_local
   int eesl_gen;           // bumped by every oa_gpu_set_ees_local (captured graphs depend on it)
+  int fft_runtime;        // oa_tuning fft_path 2: runtime-plan transforms for the state path
+  int rho_groups_cap;     // groups the density partials are allocated for
+  int nq2_cap;            // entries of qpart2 allocated
   double gzvps_t[4];      // g = 0 limit of the local part per type
   // mixed form: the FP32 density renormalised to the exact electron count
   // (charge partials of the z forward pass and of the pair density pass)

@@ -419,7 +419,7 @@ int oa_plane_blocks_per_sm(int precision) {
 }
 
 cudaError_t oa_launch_state_zfwd(oa_ctx* c, cudaStream_t s, const double2* psi, int s0, int ns) {
-  if (oa_pencil_supported(c->nz)) {
+  if (!c->fft_runtime && oa_pencil_supported(c->nz)) {
     // mixed form, all states: the exact charge partials for the density
     // renormalisation ride along
     OaCharge qc = {nullptr, nullptr, nullptr};
@@ -432,7 +432,7 @@ cudaError_t oa_launch_state_zfwd(oa_ctx* c, cudaStream_t s, const double2* psi, 
   return c->precision == OA_FP64 ? launch_zfwd<double>(c, s, psi, s0, ns) : launch_zfwd<float>(c, s, psi, s0, ns);
 }
 static cudaError_t pencil_plane(oa_ctx* c, cudaStream_t s, int mode, void* psir) {
-  if (c->nx != c->ny || !oa_pencil_supported(c->nx)) return cudaErrorNotSupported;
+  if (c->fft_runtime || c->nx != c->ny || !oa_pencil_supported(c->nx)) return cudaErrorNotSupported;
   const EesArgs E = {nullptr, nullptr, nullptr, nullptr, 0, 0};
   return oa_pencil_plane(c->precision, mode, s, c->nx, c->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx,
                          c->line_ky, c->nz, c->nkx_s, c->tw_x, c->occ, c->vks, c->rho_part, c->ngroup, E, psir);
@@ -472,7 +472,7 @@ cudaError_t oa_launch_state_plane_vks(oa_ctx* c, cudaStream_t s) {
 cudaError_t oa_launch_state_zbwd(oa_ctx* c, cudaStream_t s, const double2* psi, const double2* fnl,
                                  double2* force, int s0, int ns) {
   c->zb_po_done = 0;
-  if (oa_pencil_supported(c->nz)) {
+  if (!c->fft_runtime && oa_pencil_supported(c->nz)) {
     const cudaError_t e = oa_pencil_zbwd(c->precision, s, c->nz, c->zbuf, c->ldl, c->nlines, c->line_kx,
                                          c->line_off, c->line_nneg, c->line_npos, c->tw_z, psi, fnl, force, c->g2,
                                          c->occ, c->ng, s0, ns, -2.0 / (double)c->npts, c->ecut_psi, c->eke_part,
@@ -492,7 +492,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
   typedef typename CplxOf<R>::T C;
   oa_ees* e = c->ees;
   cudaError_t err;
-  const bool pz = oa_pencil_supported(e->nc) != 0;
+  const bool pz = !c->fft_runtime && oa_pencil_supported(e->nc) != 0;
   // z pass forward with conj(dyp psi)
   if (pz) {
     err = oa_pencil_zfwd(c->precision, st, e->nc, psi, c->ng, 0, c->nstate, c->line_off, c->line_nneg, c->line_npos,
@@ -510,7 +510,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
   PlaneSmem L = plane_smem_layout<C, R>(e->na, e->nb, c->nkx_s);
   EesArgs E = {e->idx, e->mn, e->zpart, e->zs, c->natm_nl, e->order, e->dmn, c->ions ? e->fpart : nullptr};
   dim3 pgrid(e->nc, e->ngroup);
-  const bool pp = e->na == e->nb && oa_pencil_supported(e->na);
+  const bool pp = !c->fft_runtime && e->na == e->nb && oa_pencil_supported(e->na);
   err = cudaErrorNotSupported;
   if (pp)
     err = oa_pencil_plane(c->precision, 2, st, e->na, e->zbuf, c->nstate, c->ldl, c->nlines, c->line_kx, c->line_ky,

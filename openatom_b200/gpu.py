@@ -62,6 +62,15 @@ class CPState(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    """oa_tuning: the runtime tile and schedule choices of a context."""
+    _fields_ = [("group_state", C.c_int), ("group_pair", C.c_int), ("dgemm_kblocks", C.c_int),
+                ("tgemm_kblocks", C.c_int), ("fft_path", C.c_int)]
+
+
+TUNING_FIELDS = tuple(f for f, _ in Tuning._fields_)
+
+
 # name -> (restype, argtypes); the exported surface of include/oa_gpu.h
 _vp = C.c_void_p
 SIGNATURES = {
@@ -104,6 +113,8 @@ SIGNATURES = {
     "oa_gpu_ees_init": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp]),
     "oa_gpu_nl_ees": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "oa_gpu_set_ees_local": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "oa_gpu_get_tuning": (C.c_int, [_vp, C.POINTER(Tuning)]),
+    "oa_gpu_set_tuning": (C.c_int, [_vp, C.POINTER(Tuning)]),
     "oa_gpu_pc_forward_noalloc": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                             _vp]),
 }
@@ -162,7 +173,11 @@ def redundant_partner(sysm) -> np.ndarray:
 class CPContext:
     """One system on the current CUDA device (one ``oa_ctx``)."""
 
-    def __init__(self, sysm, precision: str = "fp64"):
+    def __init__(self, sysm, precision: str = "fp64", tuning: str = "table"):
+        """tuning: "table" applies the autotuner's recorded choices for this
+        system's sizes and precision when the table has them
+        (openatom_b200/tuning/b200.json, openatom_b200.tuner); "default"
+        keeps the library's built-in heuristics."""
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("CPContext needs a CUDA device; there is no CPU path")
@@ -225,6 +240,15 @@ class CPContext:
         if getattr(sysm, "eext_ees", None) is not None:
             na, nb, nc, order = sysm.eext_ees
             self.set_ees_local((na, nb, nc), order)
+        self.tuning_source = "default"
+        if tuning == "table":
+            from .tuner import lookup
+            choice = lookup(sysm, precision)
+            if choice is not None:
+                self.set_tuning(**choice)
+                self.tuning_source = "table"
+        elif tuning != "default":
+            raise ValueError("tuning must be 'table' or 'default'")
 
     def set_ions(self, masses, vel=None):
         """Turn on ion dynamics in the native step (oa_gpu_set_ions): masses
@@ -245,6 +269,20 @@ class CPContext:
         vel = np.zeros((self.sys.natm, 3))
         _check(self._lib.oa_gpu_get_ions(self._h, self._stream(), pos.ctypes.data_as(_dp), vel.ctypes.data_as(_dp)))
         return pos, vel
+
+    def get_tuning(self) -> dict:
+        """The context's tile and schedule choices (oa_gpu_get_tuning)."""
+        t = Tuning()
+        _check(self._lib.oa_gpu_get_tuning(self._h, C.byref(t)))
+        return {f: int(getattr(t, f)) for f in TUNING_FIELDS}
+
+    def set_tuning(self, **choice):
+        """Set some of the choices (oa_gpu_set_tuning); the others are kept."""
+        bad = set(choice) - set(TUNING_FIELDS)
+        if bad:
+            raise ValueError(f"unknown tuning fields {sorted(bad)}")
+        t = Tuning(**{f: int(choice.get(f, 0)) for f in TUNING_FIELDS})
+        _check(self._lib.oa_gpu_set_tuning(self._h, C.byref(t)))
 
     def set_ees_local(self, grid, order: int = 6):
         """Local pseudopotential and reciprocal Ewald sum by the EES method
@@ -459,11 +497,11 @@ class CPDriver:
 
     def __init__(self, sysm, precision: str = "fp64", tol: float = 1e-15, max_iter: int = 1000,
                  psi0=None, norb_tol: float = 0.003, nl_method: str = "sf", ees_order: int = 6,
-                 ees_scale: float = 1.2, v0=None):
+                 ees_scale: float = 1.2, v0=None, tuning: str = "table"):
         import torch
         self.torch = torch
         self.sys = sysm
-        self.ctx = CPContext(sysm, precision)
+        self.ctx = CPContext(sysm, precision, tuning=tuning)
         # nonlocal method (cp_nonloc_ees_opt): "sf" structure factor (N^2) or
         # "ees" (Euler exponential splines of order ees_order on the
         # nonlocal grid); the native step follows the context's choice

@@ -440,3 +440,20 @@ def make_system(preset: str = "w8", seed: int = 1234, nstate: int | None = None,
         from .ees import local_grid
         sysm.eext_ees = local_grid(sysm, ees_scale, int(eext_ees_order)) + (int(eext_ees_order),)
     return sysm
+
+
+def batch_systems(seed, nsys):
+    """Seeded set of uneven water systems for the batching form: 8-32 H2O at
+    about 1 g/cc, 4 states per molecule (32-128), 60/70/80 Ry, each on the
+    smallest two-pass grid that holds its density sphere (4 kmax)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(nsys):
+        nmol = int(rng.integers(8, 33))
+        ecut = float(rng.choice([60.0, 70.0, 80.0]))
+        box = 18.6 * (nmol / 32.0) ** (1.0 / 3.0)
+        kmax = int(math.floor(math.sqrt(ecut) / (2.0 * math.pi / box))) + 1
+        grid = next(g for g in (64, 96, 108, 160) if g >= 4 * kmax)
+        out.append(make_system("w32", seed=seed + 101 * i, nmol=nmol, box=box, ecut_ry=ecut,
+                               nfft=(grid, grid, grid), ecut_mass=2.0, cmass0=400.0, dt=5.0))
+    return out
