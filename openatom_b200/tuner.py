@@ -4,9 +4,10 @@ split-K blocks of the FP64 products, the FFT path) per system size and
 precision.
 
 For each system it runs coordinate descent over the knobs: every candidate
-value is set on a live context (oa_gpu_set_tuning) and timed as whole
-native CP steps (one oa_gpu_cp_run call of ``steps`` steps after a warm-up
-call, CUDA events on the context's stream, best of ``reps``).  A value is
+value is set (oa_gpu_set_tuning) on a fresh context started from the same
+quenched coefficients and timed as whole native CP steps (one
+oa_gpu_cp_run call of ``steps`` steps after a warm-up call, CUDA events on
+the context's stream, best of ``reps``).  A value is
 kept only when it beats the current choice by more than ``margin``.  The
 result is recorded in a JSON table keyed by the system's sizes and
 precision (``tuning/b200.json``), which CPContext applies at creation.
@@ -95,22 +96,47 @@ def _time_steps(torch, drv, st, steps: int, reps: int) -> float:
     return best
 
 
+def _quenched_psi(sysm, large: bool):
+    """Coefficients off the random start: damped FP64 CP, three steps at
+    the system's dt then more at dt = 10 (as the benchmark's start)."""
+    from .gpu import CPDriver
+    q = CPDriver(sysm, "fp64", tuning="default")
+    q.quench(3)
+    q.quench(3 if large else 27, dt=10.0)
+    psi0 = q.psi.cpu().numpy()
+    q.ctx.close()
+    return psi0
+
+
+def _measure(torch, sysm, precision: str, psi0, choice: dict, steps: int, reps: int) -> float:
+    """ms per native CP step with these choices, on a fresh context from psi0."""
+    from .gpu import CPDriver
+    drv = CPDriver(sysm, precision, psi0=psi0, norb_tol=0.003, tuning="default")
+    try:
+        if choice:
+            drv.ctx.set_tuning(**choice)
+        st = drv.native_state(use_graph=True)
+        drv.run_native(st, 3)
+        return _time_steps(torch, drv, st, steps, reps)
+    finally:
+        drv.ctx.close()
+
+
 def tune_system(sysm, precision: str, steps: int = 10, reps: int = 3, margin: float = 0.015, log=None) -> dict:
-    """Coordinate descent over knobs_for(precision) on one system; returns
-    the table entry {"choice", "default", "ms_default", "ms_tuned", "trials"}."""
+    """Coordinate descent over knobs_for(precision) on one system, every
+    candidate timed on a fresh context from the same quenched coefficients;
+    returns the table entry {"choice", "default", "ms_default", "ms_tuned",
+    "trials"}."""
     import torch
-    from .gpu import CPDriver, OaError
-    drv = CPDriver(sysm, precision, norb_tol=0.003, tuning="default")
-    ctx = drv.ctx
+    from .gpu import CPContext, OaError
+    ctx = CPContext(sysm, precision, tuning="default")
     default = ctx.get_tuning()
+    ctx.close()
     caps = dict(default)
     caps["dgemm_kblocks"] = 160
-    drv.quench(3)  # off the random start, as a run would be
-    st = drv.native_state(use_graph=True)
-    drv.run_native(st, 3)
-    ms_default = _time_steps(torch, drv, st, steps, reps)
-    cur = dict(default)
-    cur_ms = ms_default
+    psi0 = _quenched_psi(sysm, sysm.nstate > 128)
+    ms_default = _measure(torch, sysm, precision, psi0, {}, steps, reps)
+    cur, cur_ms = dict(default), ms_default
     trials = []
     for knob in knobs_for(precision):
         for v in candidates(knob, sysm, precision, cur, caps):
@@ -119,30 +145,19 @@ def tune_system(sysm, precision: str, steps: int = 10, reps: int = 3, margin: fl
             trial = dict(cur)
             trial[knob] = v
             try:
-                ctx.set_tuning(**{knob: v})
-                drv.run_native(st, 2)
-                ms = _time_steps(torch, drv, st, steps, reps)
+                ms = _measure(torch, sysm, precision, psi0, trial, steps, reps)
             except OaError as e:
                 trials.append({knob: v, "error": str(e)[:120]})
-                ctx.set_tuning(**{knob: cur[knob]})
                 continue
             trials.append({knob: v, "ms": ms})
             if ms < cur_ms * (1.0 - margin):
                 cur, cur_ms = trial, ms
-            else:
-                ctx.set_tuning(**{knob: cur[knob]})
         if log:
             log(f"  {knob}: {cur[knob]} ({cur_ms:.4f} ms)")
-    # confirm against the default once more, with fresh timing of both
-    ctx.set_tuning(**default)
-    drv.run_native(st, 2)
-    ms_d2 = _time_steps(torch, drv, st, steps, reps)
-    ctx.set_tuning(**cur)
-    drv.run_native(st, 2)
-    ms_t2 = _time_steps(torch, drv, st, steps, reps)
+    # confirm against the built-in choice with fresh timings of both
+    ms_d2 = _measure(torch, sysm, precision, psi0, {}, steps, reps)
+    ms_t2 = _measure(torch, sysm, precision, psi0, cur, steps, reps) if cur != default else ms_d2
     choice = cur if ms_t2 < ms_d2 * (1.0 - margin) else dict(default)
-    ctx.close()
-    del drv
     torch.cuda.empty_cache()
     return {"choice": choice, "default": default, "ms_default": min(ms_default, ms_d2),
             "ms_tuned": ms_t2 if choice != default else min(ms_default, ms_d2), "trials": trials}
@@ -160,6 +175,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--out", default=TABLE)
+    ap.add_argument("--only-missing", action="store_true", help="skip systems the table already holds")
     a = ap.parse_args(argv)
     from .system import make_system
     import torch
@@ -174,7 +190,7 @@ def main(argv=None):
     t0 = time.time()
     for sysm, prec in jobs:
         key = system_key(sysm, prec)
-        if key in tab and tab[key].get("seen_this_run"):
+        if key in tab and (tab[key].get("seen_this_run") or a.only_missing):
             continue
         print(f"{key}", flush=True)
         steps = a.steps if sysm.nstate <= 128 else max(2, a.steps // 4)
