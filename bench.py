@@ -191,6 +191,36 @@ def blyp_form(torch, args):
             "density_path_ms": {"blyp": kt["blyp"], "pz_lda": kt["pz_lda"]}}
 
 
+def force_call_form(torch, drv, k):
+    """The force half of a CP step as a chare would call it through the C
+    ABI with host buffers: psi copied in from pinned host memory,
+    state_fft_fwd + vks_build + nl_sf + vks_apply_fft_bwd (computePsiFandVKS,
+    the ParticlePlane forces, combineForcesGetEke), F copied back to pinned
+    host memory; CUDA events around k such calls."""
+    psi_h = drv.psi.cpu().pin_memory()
+    f_h = torch.empty_like(psi_h).pin_memory()
+
+    def call():
+        drv.psi.copy_(psi_h, non_blocking=True)
+        drv.forces()
+        f_h.copy_(drv.F, non_blocking=True)
+
+    for _ in range(2):
+        call()
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(k):
+        call()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / k
+    nb = psi_h.numel() * psi_h.element_size()
+    return {"value": 1e3 / ms, "unit": "force calls/s", "ms_per_call": ms, "h2d_bytes_per_call": nb,
+            "d2h_bytes_per_call": nb, "precision": "mixed"}
+
+
 def ion_form(torch, args):
     """Ion dynamics on the 32-water workload (NVE, atoms starting at 300 K):
     mixed-form CP steps/s with the structure-factor local and nonlocal atom
@@ -530,6 +560,8 @@ def run_ours(args):
     de = max(abs(total_energy(a) - total_energy(b)) for a, b in zip(en_mx, en_64)) / natm
     s_err = dmx.last_ortho
 
+    # the force half of the step with host psi in and host F out, per call
+    force_call = force_call_form(torch, dmx, args.steps)
     # per-kernel timing (CUDA events on the launch stream) for the roofline
     kt = dmx.ctx.time_kernels(dmx.psi, reps=5)
     kt64 = d64.ctx.time_kernels(d64.psi, reps=5)
@@ -588,6 +620,7 @@ def run_ours(args):
             "e2e": {"value": ws * 1e3 / ms_e2e, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * natm,
                     "d2h_bytes_per_step": 20 * 8},
             "sync_every_step": {"value": ws * 1e3 / ms_sync, "ms_per_step": ms_sync},
+            "e2e_force_call": force_call,
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(),
             "drift_1000": drift,
