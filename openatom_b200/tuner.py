@@ -179,7 +179,9 @@ def main(argv=None):
     a = ap.parse_args(argv)
     from .system import make_system
     import torch
-    jobs = [(make_system(p, seed=a.seed), prec) for p in a.presets for prec in a.precisions]
+    # the benchmark's systems: mass preconditioning at 2 Ry, mu = 400, dt = 5
+    jobs = [(make_system(p, seed=a.seed, ecut_mass=2.0, cmass0=400.0, dt=5.0), prec)
+            for p in a.presets for prec in a.precisions]
     if a.batch:
         from .system import batch_systems
         jobs += [(sy, "mixed") for sy in batch_systems(a.batch_seed, a.batch)]
