@@ -194,3 +194,40 @@ OA_HD void pass_a_band(C* u, int n2, const C* tw) {
 #pragma unroll
   for (int k1 = 1; k1 < N1; ++k1) u[k1] = cmul(u[k1], tw_rt<SIGN>(tw, n2 * k1));
 }
+
+#ifdef __CUDACC__
+// In-place transform of nb lines a[line][n] (row stride ld) for the lengths
+// with a compile-time factorisation N = N1 N2, N1 <= 16: pass A (lines
+// fastest) into b [line][k1][n2] (row stride ZLd::PS), pass B back to
+// natural order in a.  tw: the length-N table exp(-2 pi i k / N) in shared
+// memory.  Used by the density z pass and the EES local grid transforms.
+template <int N1, int N2> struct ZLd {
+  static constexpr int LS = N2 | 1;
+  static constexpr int PS = (N1 * LS) | 1;
+};
+template <int N1, int N2, int SIGN>
+__device__ void zfft2(double2* a, double2* b, int ld, int nb, const double2* tw) {
+  typedef ZLd<N1, N2> L;
+  for (int i = threadIdx.x; i < N2 * nb; i += blockDim.x) {
+    const int n2 = i / nb, lb = i - n2 * nb;
+    double2 u[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) u[n1] = a[lb * ld + N2 * n1 + n2];
+    pass_a<N1, N2, SIGN>(u, n2, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) b[lb * L::PS + k1 * L::LS + n2] = u[k1];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 16 * nb; i += blockDim.x) {
+    const int lb = i >> 4, k1 = i & 15;
+    if (k1 >= N1) continue;
+    double2 w[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) w[n2] = b[lb * L::PS + k1 * L::LS + n2];
+    RDft<N2, SIGN>::run(w);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) a[lb * ld + k1 + N1 * k2] = w[k2];
+  }
+  __syncthreads();
+}
+#endif

@@ -244,38 +244,6 @@ struct RhoTypeOff { int off[5]; };
 // z-line: pxy[line][a] = e^{i (gx x_a + gy y_a)} is formed once per block in
 // shared memory (atoms grouped by type), and each g of the line multiplies
 // it by the z phase e^{i gz z_a}.
-// In-place z transform of nb lines a[line][z] (row stride ld) for the
-// lengths with a compile-time factorisation N = N1 N2 (oa_rdft.cuh): pass A
-// (lines fastest) into b [line][k1][n2], pass B back to natural order in a.
-template <int N1, int N2> struct ZLd {
-  static constexpr int LS = N2 | 1;
-  static constexpr int PS = (N1 * LS) | 1;
-};
-template <int N1, int N2, int SIGN>
-__device__ void zfft2(double2* a, double2* b, int ld, int nb, const double2* tw) {
-  typedef ZLd<N1, N2> L;
-  for (int i = threadIdx.x; i < N2 * nb; i += blockDim.x) {
-    const int n2 = i / nb, lb = i - n2 * nb;
-    double2 u[N1];
-#pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) u[n1] = a[lb * ld + N2 * n1 + n2];
-    pass_a<N1, N2, SIGN>(u, n2, tw);
-#pragma unroll
-    for (int k1 = 0; k1 < N1; ++k1) b[lb * L::PS + k1 * L::LS + n2] = u[k1];
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < 16 * nb; i += blockDim.x) {
-    const int lb = i >> 4, k1 = i & 15;
-    if (k1 >= N1) continue;
-    double2 w[N2];
-#pragma unroll
-    for (int n2 = 0; n2 < N2; ++n2) w[n2] = b[lb * L::PS + k1 * L::LS + n2];
-    RDft<N2, SIGN>::run(w);
-#pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2) a[lb * ld + k1 + N1 * k2] = w[k2];
-  }
-  __syncthreads();
-}
 
 // FORCES: also the atom forces of the local pseudopotential and the
 // reciprocal Ewald sum (CP_hart_eext_calc's force loop, cp_hart_ext.C:300-360):
