@@ -51,6 +51,8 @@ def parse():
                     help="systems of the batching form measured beside the headline (0: skip)")
     ap.add_argument("--large", type=int, default=1,
                     help="also time the 128 H2O / 512-state / 160^3 system in the mixed form (0: skip)")
+    ap.add_argument("--large-min-iter", type=int, default=80,
+                    help="CG iterations of the large system's start")
     ap.add_argument("--blyp", type=int, default=1,
                     help="also time the 32-water step with the BLYP gradient correction (0: skip)")
     ap.add_argument("--ions", type=int, default=1,
@@ -113,20 +115,16 @@ def batch_form(torch, args):
 
 def large_form(torch, args):
     """The large single system (128 H2O, 512 states, 70 Ry, 160^3) with the
-    EES nonlocal projectors of B-spline order 4: mixed CP steps/s after a
-    short damped start, then the FP64 form from the same start (its plane
-    passes keep the FP64 density / V_KS plane in global memory at this size)
-    and the total-energy difference of the two forms per atom."""
+    EES nonlocal projectors of B-spline order 4: mixed CP steps/s from a
+    start minimised by conjugate gradients (mixed form, a capped number of
+    iterations), then the FP64 form from the same start (its plane passes
+    keep the FP64 density / V_KS plane in global memory at this size) and
+    the total-energy difference of the two forms per atom."""
     from openatom_b200.gpu import CPDriver
     sysm = make_sys("w128", args.seed + 11)
-    nq = min(args.quench, 6)
-    d = CPDriver(sysm, "mixed", nl_method="ees", ees_order=4, norb_tol=NORB_TOL)
-    for n, dtq in quench_schedule(nq):
-        d.quench(n, dt=dtq)
-    psi0 = d.psi.cpu().numpy()
-    grid = list(d.ctx.ees_grid)
-    d.ctx.close()
-    del d
+    psi0, start = minimized_start(sysm, iters=args.large_min_iter, prec="mixed", nl_method="ees", ees_order=4)
+    from openatom_b200 import ees as ees_mod
+    grid = list(ees_mod.nonlocal_grid(sysm, 1.2, 4))
     torch.cuda.empty_cache()
     k = 4
     res, ens, first = {}, {}, {}
@@ -150,19 +148,19 @@ def large_form(torch, args):
             "ms_per_step": res["mixed"], "value": 1e3 / res["mixed"], "unit": UNIT,
             "fp64": {"ms_per_step": res["fp64"], "value": 1e3 / res["fp64"]},
             "mixed_over_fp64": res["fp64"] / res["mixed"], "dE_per_atom_max_steps_3_to_6": de,
-            "ortho_residual": ortho, "smax_max": max(e["SMAX"] for e in ens["mixed"]), "quench_steps": nq}
+            "ortho_residual": ortho, "smax_max": max(e["SMAX"] for e in ens["mixed"]), "start": start}
 
 
 def blyp_form(torch, args):
     """The 32-water workload with the BLYP functional (Becke 88 + LYP
     gradient correction, its six extra density-grid transforms per step):
-    mixed and FP64 CP steps/s from the same quenched start, the total-energy
+    mixed and FP64 CP steps/s from the same CG-minimised start, the total-energy
     difference of the two forms, EGGA, and the density path's kernel time
     with and without the correction."""
     from openatom_b200.gpu import CPDriver
     sysm = make_sys(args.config, args.seed)
     sysm.xc = "blyp"
-    psi0 = quenched_start(sysm, min(args.quench, 12))
+    psi0, start = minimized_start(sysm, iters=300)
     res = {}
     ens = {}
     kt = {}
@@ -187,8 +185,31 @@ def blyp_form(torch, args):
             "steps": 10, "mixed": {"value": 1e3 / res["mixed"], "ms_per_step": res["mixed"]},
             "fp64": {"value": 1e3 / res["fp64"], "ms_per_step": res["fp64"]},
             "mixed_over_fp64": res["fp64"] / res["mixed"], "dE_per_atom_max_steps_3_to_6": de,
-            "egga": ens["fp64"][-1]["EGGA"], "quench_steps": min(args.quench, 12),
+            "egga": ens["fp64"][-1]["EGGA"], "start": start,
             "density_path_ms": {"blyp": kt["blyp"], "pz_lda": kt["pz_lda"]}}
+
+
+def ground_state_form(torch, sysm, k):
+    """Mixed and FP64 CP steps/s from the CG-minimised ground state of the
+    headline system (beside the quenched start the headline uses, which the
+    reference arm can reproduce on the host), the PsiV resets in the timed
+    steps and the largest total-energy difference of the two forms."""
+    from openatom_b200.gpu import CPDriver
+    psi0, start = minimized_start(sysm)
+    out = {"start": start, "steps": k}
+    ens = {}
+    for prec in ("mixed", "fp64"):
+        d = CPDriver(sysm, prec, psi0=psi0, norb_tol=NORB_TOL)
+        st = d.native_state(use_graph=True)
+        d.run_native(st, 5)
+        ms, en = time_steps(torch, d, st, k)
+        ens[prec] = en
+        out[prec] = {"value": 1e3 / ms, "ms_per_step": ms, "psiv_resets": sum(1 for e in en if e["SMAX"] > NORB_TOL)}
+        d.ctx.close()
+    out["mixed_over_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["dE_per_atom_max"] = max(abs(total_energy(a) - total_energy(b))
+                                 for a, b in zip(ens["mixed"], ens["fp64"])) / sysm.natm
+    return out
 
 
 def force_call_form(torch, drv, k):
@@ -225,13 +246,13 @@ def ion_form(torch, args):
     """Ion dynamics on the 32-water workload (NVE, atoms starting at 300 K):
     mixed-form CP steps/s with the structure-factor local and nonlocal atom
     forces and with the EES local path (order 6, cp_eext_ees_opt on), beside
-    the fixed-ion step, all from one quenched start."""
+    the fixed-ion step, all from one CG-minimised start."""
     import copy
     from openatom_b200.ees import local_grid
     from openatom_b200.gpu import CPDriver
     from openatom_b200.system import atom_masses
     sysm = make_sys(args.config, args.seed)
-    psi0 = quenched_start(sysm, min(args.quench, 12))
+    psi0, _ = minimized_start(sysm, iters=300)
     m = atom_masses(sysm)
     rng = np.random.default_rng(args.seed)
     vel = rng.standard_normal(sysm.pos.shape) * np.sqrt(300.0 * 3.1668115634556e-6 / m)[:, None]
@@ -460,6 +481,22 @@ def quenched_start(sysm, nq):
     return psi0
 
 
+def minimized_start(sysm, iters=600, tol=1e-3, prec="fp64", **drv_kw):
+    """The electronic ground state the reference reaches before dynamics
+    (cp_min_opt): three damped steps off the random start, then
+    conjugate-gradient minimisation (CPMinimizer, dt = 20) until |F| <= tol
+    or iters iterations.  Returns (psi, info)."""
+    from openatom_b200.gpu import CPDriver, CPMinimizer
+    d = CPDriver(sysm, prec, **drv_kw)
+    d.quench(3)
+    m = CPMinimizer(d, "cg", dt=20.0)
+    recs = m.run(iters, tol=tol)
+    psi0 = d.psi.cpu().numpy()
+    d.ctx.close()
+    return psi0, {"method": "CG minimisation (cp_min_opt), dt 20", "iterations": len(recs),
+                  "fmag": recs[-1]["FMAG"], "e_ks": total_energy(recs[-1])}
+
+
 def native_records(sysm, psi0, prec, nsteps, norb_tol=NORB_TOL):
     from openatom_b200.gpu import CPDriver
     d = CPDriver(sysm, prec, psi0=psi0, norb_tol=norb_tol)
@@ -471,12 +508,13 @@ def native_records(sysm, psi0, prec, nsteps, norb_tol=NORB_TOL):
 def drift_form(torch, args, want_oracle):
     """The precision configuration on 8 H2O (32 states, 70 Ry, 64^3, dt = 5,
     mu = 400): the mixed and the FP64 form for args.drift_steps CPMD steps
-    from the same quenched start.  Reports the drift of the CP constant of
-    motion of each form, each energy term's largest difference between the
-    two forms over the run, and (CPU leg) each term against the FP64 oracle
-    over the first 20 steps."""
+    from the same start, the electronic ground state (CG minimisation, as the
+    reference runs cp_min_opt before dynamics).  Reports the drift of the CP
+    constant of motion of each form, each energy term's largest difference
+    between the two forms over the run, and (CPU leg) each term against the
+    FP64 oracle over the first 20 steps."""
     sysm = make_sys("w8", args.seed + 3)
-    psi0 = quenched_start(sysm, args.quench)
+    psi0, start = minimized_start(sysm)
     n = args.drift_steps
     recs = {p: native_records(sysm, psi0, p, n) for p in ("fp64", "mixed")}
     # the same runs without the PsiV tolerance reset (its velocity projection
@@ -484,7 +522,8 @@ def drift_form(torch, args, want_oracle):
     # integrator and the orthonormality constraint alone
     from openatom_b200.gpu import OaError
     free = {}
-    out = {"workload": f"w8: 8 H2O, {sysm.nstate} states, 70 Ry, 64^3, ng={sysm.ng}", "steps": n}
+    out = {"workload": f"w8: 8 H2O, {sysm.nstate} states, 70 Ry, 64^3, ng={sysm.ng}", "steps": n,
+           "start": start}
     for p in ("fp64", "mixed"):
         try:
             free[p] = native_records(sysm, psi0, p, n, norb_tol=1e30)
@@ -562,6 +601,9 @@ def run_ours(args):
 
     # the force half of the step with host psi in and host F out, per call
     force_call = force_call_form(torch, dmx, args.steps)
+    # the same timing from the electronic ground state (CG minimisation):
+    # the reference's cp_min_opt start, where the PsiV reset fires rarely
+    ground = ground_state_form(torch, sysm, args.steps) if rk == 0 else None
     # per-kernel timing (CUDA events on the launch stream) for the roofline
     kt = dmx.ctx.time_kernels(dmx.psi, reps=5)
     kt64 = d64.ctx.time_kernels(d64.psi, reps=5)
@@ -621,6 +663,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": 20 * 8},
             "sync_every_step": {"value": ws * 1e3 / ms_sync, "ms_per_step": ms_sync},
             "e2e_force_call": force_call,
+            "ground_state_start": ground,
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(),
             "drift_1000": drift,
