@@ -217,20 +217,15 @@ oa_status oa_gpu_small_gemm(oa_ctx *ctx, void *stream, const double *A, const do
 oa_status oa_gpu_integrate(oa_ctx *ctx, void *stream, const double *force, double *vpsi, double *psi,
                            double dt, int complete_prev, double *fict_ke_out);
 
-/* PsiV tolerance reset (Ortho::maxCheck, ortho.C:455-475, and the
- * "replace non-ortho psi by ortho" copies of CP_State_GSpacePlane.C:3590-3600,
- * 3750-3760): psi_t <- psi and the velocities projected onto the
- * orthonormality constraint, v_j <- v_j - sum_k psi_k X_kj,
- * X = (A + A^T)/4, A_ij = <psi_i|v_j> in the S metric.  The caller resets
- * its T to the identity. */
-oa_status oa_gpu_psiv_reset(oa_ctx *ctx, void *stream, const double *psi, double *psi_t, double *vpsi);
-
-/* The same reset in the mixed-precision form: both products (A and X psi)
- * as split-BF16 tensor-core GEMMs with nterm (2 or 3) bf16 planes and FP32
- * accumulation; v is updated in FP64.  Same reference work as
- * oa_gpu_psiv_reset. */
-oa_status oa_gpu_psiv_reset_mixed(oa_ctx *ctx, void *stream, const double *psi, double *psi_t, double *vpsi,
-                                  int nterm);
+/* PsiV tolerance reset of the reference's default build (Ortho::maxCheck,
+ * ortho.C:455-475 -> computeNewPsiVFiniteDifference, gspace.ci:290-301;
+ * CP_State_GSpacePlane::finiteDifferencePsiV, CP_State_GSpacePlane.C:3741-3800,
+ * norb_fin_diff_order 0): psi_t <- psi and v <- (psi - psi_prev) / dt, with
+ * psi_prev the orthonormal states of the previous step.  The caller resets
+ * its T to the identity, and its next oa_gpu_integrate takes
+ * complete_prev = 0 (the velocity is already at t: halfStepEvolve = 0). */
+oa_status oa_gpu_psiv_reset(oa_ctx *ctx, void *stream, const double *psi, const double *psi_prev, double *psi_t,
+                            double *vpsi, double dt);
 
 /* Copy new atom positions (host [natm][3], bohr) for the next vks_build
  * (the structure-factor phases are rebuilt from them every call). */
@@ -312,6 +307,8 @@ typedef struct {
   double last_smax;     /* out: max |S - 2I| of this step */
   int last_kernels;     /* out: kernel launches of one step when it replays as a CUDA graph
                            (counted in the captured graph), else -1 */
+  int psiv_pending;     /* in/out: the last step ended with a PsiV reset, so the next step
+                           completes no half kick (halfStepEvolve = 0); 0 for a new run */
 } oa_cp_state;
 
 /* One whole CP dynamics step (GSpaceDriver::computeDynamics,
@@ -319,8 +316,9 @@ typedef struct {
  * integration, orthonormalisation, in native code with one host
  * synchronisation at the end.  The PsiV reset triggered by max|S - 2I| >
  * norb_tol (Ortho::maxCheck, ortho.C:455-475) is decided on the device and
- * runs at the end of the step, as oa_gpu_psiv_reset would (oa_gpu_psiv_reset_mixed
- * with state->mixed_nterm planes when that is nonzero).  energies_out (optional, host [14]):
+ * runs at the end of the step, as oa_gpu_psiv_reset would (the velocity
+ * from the states before and after the rotation; the next step completes
+ * no half kick).  energies_out (optional, host [14]):
  * EKE EHART EEXT EWALD_RECIP EEXC MUXC FICT_KE ENL, Newton-Schulz
  * iterations, residual, max|S - 2I|, EGGA (0 under PZ-LDA), the ionic
  * kinetic energy and the real-space Ewald energy with its self and

@@ -774,12 +774,6 @@ __global__ void k_sym_quarter(const double* A, int n, double* X) {
   if (i < n && j < n) X[(size_t)i * n + j] = 0.25 * (A[(size_t)i * n + j] + A[(size_t)j * n + i]);
 }
 
-__global__ void k_sym_quarter_cond(const double* A, int n, double* X, const int* cond) {
-  if (cond && *cond == 0) return;
-  const int i = blockIdx.y * 16 + threadIdx.y, j = blockIdx.x * 16 + threadIdx.x;
-  if (i < n && j < n) X[(size_t)i * n + j] = 0.25 * (A[(size_t)i * n + j] + A[(size_t)j * n + i]);
-}
-
 __global__ void k_copy_cond(double* __restrict__ dst, const double* __restrict__ src, size_t n, const int* cond) {
   if (*cond == 0) return;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -1125,61 +1119,6 @@ static cudaError_t mixed_bwd(oa_ctx* c, cudaStream_t s, int nt, const double* M1
 // 3750-3760 with the orthoT velocity projection): X = sym(psi v^T) / 4 with
 // the S weights, v <- v - X psi (in place).  cond: optional device flag; the
 // launches do nothing when it is 0.
-static oa_status psiv_velocity(oa_ctx* c, cudaStream_t s, const double* psi, double* vpsi, const int* cond,
-                               int nterm) {
-  oa_ctx_pc* p = pcx(c);
-  const int n = c->nstate;
-  dim3 grid((n + 15) / 16, (n + 15) / 16), blk(16, 16);
-  if (nterm) {
-    // split-BF16: A = v carries the S weights (sym(v psi^T) = sym(psi v^T)),
-    // so the psi planes serve both products; v -= X psi with v added in FP64.
-    // Above 128 states the backward product (on the planes only up to 128)
-    // runs in FP64 with the same flag and in-place add.
-    cudaError_t e = mixed_fwd(c, s, nterm, vpsi, psi, n, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->mat_a, PL_OTHER,
-                              PL_PSI, cond);
-    if (e == cudaSuccess) {
-      k_sym_quarter_cond<<<grid, blk, 0, s>>>(p->mat_a, n, p->mat_x, cond);
-      e = cudaGetLastError();
-    }
-    if (e == cudaSuccess && oa_tg_nb(n))
-      e = mixed_bwd(c, s, nterm, p->mat_x, psi, -1.0, -1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0,
-                    vpsi, PL_PSI, PL_OTHER, vpsi, cond);
-    else if (e == cudaSuccess)
-      e = oa_dgemm_bwd_ex(s, p->mat_x, psi, -1.0, -1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, vpsi,
-                          cond, vpsi, nullptr, nullptr);
-    if (e != cudaErrorNotSupported) {
-      OA_CUDA_TRY(e);
-      return OA_OK;
-    }
-  }
-  cudaError_t e =
-      oa_dgemm_fwd(s, psi, vpsi, n, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, p->mat_a, cond);
-  // above 128 states the general kernels, which know no device flag, run
-  // unconditionally; what they produce is used only under the flag
-  if (e == cudaErrorNotSupported)
-    e = oa_launch_pc_fwd(s, psi, vpsi, n, 2L * c->ng, 2L * c->nkx0, 0.5, 2.0, p->part, p->nkb, p->mat_a);
-  OA_ALIGN_TRY(e);
-  k_sym_quarter_cond<<<grid, blk, 0, s>>>(p->mat_a, n, p->mat_x, cond);
-  OA_CUDA_TRY(cudaGetLastError());
-  e = oa_dgemm_bwd_ex(s, p->mat_x, psi, -1.0, -1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, vpsi,
-                      cond, vpsi, nullptr, nullptr);
-  if (e == cudaErrorNotSupported) {
-    // v - X psi as the two-term product (-X) psi + I v into scratch, then
-    // copied over v (under the flag)
-    OA_CUDA_TRY(oa_launch_pc_bwd(s, p->mat_x, psi, -1.0, -1.0, p->eye, vpsi, 1.0, n, 2L * c->ng, 2L * c->nkx0,
-                                 p->vtmp));
-    const size_t nd = (size_t)n * c->ng * 2;
-    if (cond) {
-      k_copy_cond<<<8 * 148, 256, 0, s>>>(vpsi, p->vtmp, nd, cond);
-      OA_CUDA_TRY(cudaGetLastError());
-    } else {
-      OA_CUDA_TRY(cudaMemcpyAsync(vpsi, p->vtmp, nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    }
-    return OA_OK;
-  }
-  OA_ALIGN_TRY(e);
-  return OA_OK;
-}
 
 // psi = psi_t T (FP64); then, under the PsiV flag, the velocity projection
 // and T = I (the next step's check sets or clears the flag).  The reset's
@@ -1187,10 +1126,44 @@ static oa_status psiv_velocity(oa_ctx* c, cudaStream_t s, const double* psi, dou
 // and a run ends with oa_psi_t_settle.  The native step's orthonormalisation
 // and PsiV reset (Ortho::maxCheck, ortho.C:455-475): same results as
 // oa_gpu_pc_backward followed by oa_gpu_psiv_reset, decided on the device.
+// v = sign psi / dt under the device flag (and everywhere when cond is
+// null): the two halves of finiteDifferencePsiV's v = (psi(t) - psi(t-dt)) / dt
+// around the rotation that overwrites psi(t - dt) with psi(t)
+__global__ void __launch_bounds__(256) k_fd_velocity(const double2* __restrict__ psi, double2* __restrict__ v,
+                                                     size_t n, double scale, int accumulate,
+                                                     const int* __restrict__ cond) {
+  if (cond && *cond == 0) return;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double2 p = psi[i];
+    double2 r = make_double2(p.x * scale, p.y * scale);
+    if (accumulate) {
+      const double2 o = v[i];
+      r.x += o.x;
+      r.y += o.y;
+    }
+    v[i] = r;
+  }
+}
+
+static cudaError_t fd_velocity(oa_ctx* c, cudaStream_t s, const double* psi, double* vpsi, double scale,
+                               int accumulate, const int* cond) {
+  const size_t n = (size_t)c->nstate * c->ng;
+  k_fd_velocity<<<8 * 148, 256, 0, s>>>((const double2*)psi, (double2*)vpsi, n, scale, accumulate, cond);
+  return cudaGetLastError();
+}
+
+// psi = psi_t T and, under the device flag, the PsiV reset of the
+// reference's default build (finiteDifferencePsiV,
+// CP_State_GSpacePlane.C:3741-3800, norb_fin_diff_order 0):
+// v = (psi(t) - psi(t - dt)) / dt from the psi the rotation overwrites, and
+// T = I.  psi_t = psi is left to the next integration (which reads psi
+// under the flag, and then completes no half kick) or to oa_psi_t_settle.
 oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* psi_t, double* psi, double* vpsi,
-                            double* Tout, int* flag, int nterm) {
+                            double* Tout, int* flag, int nterm, double dt) {
   oa_ctx_pc* p = pcx(c);
   const int n = c->nstate;
+  OA_CUDA_TRY(fd_velocity(c, s, psi, vpsi, -1.0 / dt, 0, flag));
   OaPlaneOut po;
   bool fuse = nterm > 0 && plane_out(c, PL_PSI, n, nterm, &po);
   cudaError_t e = oa_dgemm_bwd_ex(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, psi,
@@ -1208,7 +1181,7 @@ oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* 
   // nonlocal products split psi again otherwise)
   if (fuse) plane_mark(c, PL_PSI, psi, n, po.rows_pad, nterm);
   else pcx(c)->pl_key[PL_PSI].valid = false;
-  OA_STEP_CHECK(psiv_velocity(c, s, psi, vpsi, flag, nterm));
+  OA_CUDA_TRY(fd_velocity(c, s, psi, vpsi, 1.0 / dt, 1, flag));
   k_copy_cond<<<16, 256, 0, s>>>(Tout, p->eye, (size_t)n * n, flag);
   OA_CUDA_TRY(cudaGetLastError());
   return OA_OK;
@@ -1243,24 +1216,15 @@ oa_status oa_psi_t_settle(oa_ctx* c, cudaStream_t s, const double* psi, double* 
   return OA_OK;
 }
 
-static oa_status psiv_reset(oa_ctx* c, void* stream, const double* psi, double* psi_t, double* vpsi, int nterm) {
+extern "C" oa_status oa_gpu_psiv_reset(oa_ctx* c, void* stream, const double* psi, const double* psi_prev,
+                                       double* psi_t, double* vpsi, double dt) {
+  OA_ARG_CHECK(c && psi && psi_prev && psi_t && vpsi && dt > 0.0, "null argument or dt <= 0");
   cudaStream_t s = (cudaStream_t)stream;
-  OA_STEP_CHECK(psiv_velocity(c, s, psi, vpsi, nullptr, nterm));
+  OA_CUDA_TRY(fd_velocity(c, s, psi_prev, vpsi, -1.0 / dt, 0, nullptr));
+  OA_CUDA_TRY(fd_velocity(c, s, psi, vpsi, 1.0 / dt, 1, nullptr));
   const size_t bytes = (size_t)c->nstate * c->ng * sizeof(double2);
   OA_CUDA_TRY(cudaMemcpyAsync(psi_t, psi, bytes, cudaMemcpyDeviceToDevice, s));
   return OA_OK;
-}
-
-extern "C" oa_status oa_gpu_psiv_reset(oa_ctx* c, void* stream, const double* psi, double* psi_t, double* vpsi) {
-  OA_ARG_CHECK(c && psi && psi_t && vpsi, "null argument");
-  return psiv_reset(c, stream, psi, psi_t, vpsi, 0);
-}
-
-extern "C" oa_status oa_gpu_psiv_reset_mixed(oa_ctx* c, void* stream, const double* psi, double* psi_t, double* vpsi,
-                                             int nterm) {
-  OA_ARG_CHECK(c && psi && psi_t && vpsi, "null argument");
-  OA_ARG_CHECK(nterm == 2 || nterm == 3, "nterm must be 2 or 3");
-  return psiv_reset(c, stream, psi, psi_t, vpsi, nterm);
 }
 
 extern "C" oa_status oa_gpu_pc_forward_mixed(oa_ctx* c, void* stream, const double* left, const double* right,

@@ -367,7 +367,9 @@ k_ortho_ns(const double* __restrict__ S, int n, double bscale, double tol, int m
 #define OA_INT_UNROLL 4
 #define OA_INT_CHUNK (256 * OA_INT_UNROLL)
 // P_in (optional) replaces P as the coefficients read when *sel != 0 (the
-// PsiV reset of the previous step: psi(t) = the orthonormal psi).
+// PsiV reset of the previous step: psi(t) = the orthonormal psi, and the
+// velocity is already at t, so no half kick is completed: halfStepEvolve = 0
+// of finiteDifferencePsiV, CP_State_GSpacePlane.C:3776).
 __global__ void __launch_bounds__(256)
 k_integrate(const double2* __restrict__ F, double2* __restrict__ V, double2* P, const double2* P_in,
             const int* __restrict__ sel, const double* __restrict__ cmass, int ng, int nstate, int r0, int r1,
@@ -375,7 +377,9 @@ k_integrate(const double2* __restrict__ F, double2* __restrict__ V, double2* P, 
   __shared__ double sh[8];
   const double dt2 = 0.5 * dt;
   const size_t base = (size_t)blockIdx.y * ng;
-  const double2* src = (P_in && *sel != 0) ? P_in : P;
+  const bool reset = P_in && *sel != 0;
+  const double2* src = reset ? P_in : P;
+  complete_prev = complete_prev && !reset;
   const int i0 = blockIdx.x * OA_INT_CHUNK + threadIdx.x;
   double2 f[OA_INT_UNROLL], v[OA_INT_UNROLL], p[OA_INT_UNROLL];
   double m[OA_INT_UNROLL];

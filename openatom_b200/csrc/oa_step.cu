@@ -35,7 +35,6 @@ oa_status oa_gpu_pc_backward_mixed(oa_ctx* ctx, void* stream, const double* M1, 
 oa_status oa_gpu_small_gemm(oa_ctx* ctx, void* stream, const double* A, const double* B, double alpha, double* C);
 oa_status oa_gpu_integrate(oa_ctx* ctx, void* stream, const double* force, double* vpsi, double* psi, double dt,
                            int complete_prev, double* fict_ke_out);
-oa_status oa_gpu_psiv_reset(oa_ctx* ctx, void* stream, const double* psi, double* psi_t, double* vpsi);
 }
 
 int oa_ns_capturable(oa_ctx* c);
@@ -43,7 +42,7 @@ oa_status oa_integrate_sel(oa_ctx* c, cudaStream_t s, const double* force, doubl
                            const double* psi_in, const int* sel, double dt, int complete_prev, double* fict_ke_out);
 oa_status oa_psi_t_settle(oa_ctx* c, cudaStream_t s, const double* psi, double* psi_t, const int* flag);
 oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* psi_t, double* psi, double* vpsi,
-                            double* Tout, int* flag, int nterm);
+                            double* Tout, int* flag, int nterm, double dt);
 
 cudaError_t oa_launch_ortho_ns(cudaStream_t s, const double* S, int n, double bscale, double tol, int max_iter,
                                double* work, double* T, int* status, double* errv, int grid);
@@ -80,6 +79,14 @@ struct oa_step_scratch {
 };
 
 static oa_step_scratch* step_scratch(oa_ctx* c) { return (oa_step_scratch*)c->step; }
+
+__global__ void k_set_flag(int* flag) { flag[0] = 1; }
+
+// flag[0] = 1: a PsiV reset is pending from the previous call
+static cudaError_t set_flag(cudaStream_t s, int* flag) {
+  k_set_flag<<<1, 1, 0, s>>>(flag);
+  return cudaGetLastError();
+}
 
 void oa_step_free(oa_ctx* c);
 
@@ -225,7 +232,7 @@ static oa_status launch_step_b(oa_ctx* c, cudaStream_t s, oa_cp_state* st) {
   k_step_check<<<1, 1, 0, s>>>(status, errv, dev_e, st->norb_tol, w->flag, w->ring, w->ring_cap);
   OA_CUDA_TRY(cudaGetLastError());
   // psi = psi_t T, and the PsiV reset when the check asked for it
-  OA_STEP_TRY(oa_psi_t_and_psiv(c, s, st->T, st->psi_t, st->psi, st->vpsi, st->T, w->flag, st->mixed_nterm));
+  OA_STEP_TRY(oa_psi_t_and_psiv(c, s, st->T, st->psi_t, st->psi, st->vpsi, st->T, w->flag, st->mixed_nterm, st->dt));
   return OA_OK;
 }
 
@@ -243,8 +250,10 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
   OA_STEP_TRY(ensure_ring(c, nsteps));
   cudaStream_t s = (cudaStream_t)stream;
   oa_step_scratch* w = step_scratch(c);
-  // restart the PsiV flag, the record count and the error slot
+  // restart the record count and the error slot; the PsiV flag carries a
+  // reset that ended the previous call
   OA_CUDA_TRY(cudaMemsetAsync(w->flag, 0, 4 * sizeof(int), s));
+  if (st->psiv_pending) OA_CUDA_TRY(set_flag(s, w->flag));
   // the psi planes of the mixed products, from the psi the caller hands in
   if (st->mixed_nterm) OA_STEP_TRY(oa_planes_psi_refresh(c, s, st->psi, st->mixed_nterm));
   const void* key[9] = {st->psi, st->psi_t, st->vpsi, st->T, stream, w->ring, c->ees,
@@ -336,6 +345,7 @@ static oa_status run_steps(oa_ctx* c, void* stream, oa_cp_state* st, int nsteps,
   st->last_ns_iters = (int)last[16];
   st->last_ns_err = last[18];
   st->last_smax = last[19];
+  st->psiv_pending = w->flag_host[0];
   if (w->flag_host[2] != 0) {
     char msg[160];
     snprintf(msg, sizeof(msg), "%s in step %d of %d",
@@ -420,6 +430,7 @@ extern "C" oa_status oa_gpu_cp_run_batch(oa_ctx** ctxs, oa_cp_state** states, in
   for (int i = 0; i < nsys && ret == OA_OK; ++i) {
     oa_step_scratch* w = step_scratch(ctxs[i]);
     ce = cudaMemsetAsync(w->flag, 0, 4 * sizeof(int), s);
+    if (ce == cudaSuccess && states[i]->psiv_pending) ce = set_flag(s, w->flag);
     if (ce != cudaSuccess) { fail(ce, __LINE__); break; }
     if (states[i]->mixed_nterm) ret = oa_planes_psi_refresh(ctxs[i], s, states[i]->psi, states[i]->mixed_nterm);
   }
@@ -501,6 +512,7 @@ extern "C" oa_status oa_gpu_cp_run_batch(oa_ctx** ctxs, oa_cp_state** states, in
     st->last_ns_iters = (int)last[16];
     st->last_ns_err = last[18];
     st->last_smax = last[19];
+    st->psiv_pending = w->flag_host[0];
     if (w->flag_host[2] != 0) {
       char msg[200];
       snprintf(msg, sizeof(msg), "system %d of the batch: %s in step %d of %d", i,

@@ -58,7 +58,7 @@ class CPState(C.Structure):
         ("iteration", C.c_int), ("dt", C.c_double), ("ns_tol", C.c_double), ("norb_tol", C.c_double),
         ("ns_max_iter", C.c_int), ("mixed_nterm", C.c_int), ("use_graph", C.c_int),
         ("last_ns_iters", C.c_int), ("last_ns_err", C.c_double), ("last_smax", C.c_double),
-        ("last_kernels", C.c_int),
+        ("last_kernels", C.c_int), ("psiv_pending", C.c_int),
     ]
 
 
@@ -95,8 +95,7 @@ SIGNATURES = {
     "oa_gpu_set_xc": (C.c_int, [_vp, C.c_int, C.c_double]),
     "oa_gpu_set_ions": (C.c_int, [_vp, _dp, _dp]),
     "oa_gpu_get_ions": (C.c_int, [_vp, _vp, _dp, _dp]),
-    "oa_gpu_psiv_reset": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
-    "oa_gpu_psiv_reset_mixed": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int]),
+    "oa_gpu_psiv_reset": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_double]),
     "oa_gpu_cp_run_batch": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int, _vp, C.c_int,
                                       C.POINTER(C.c_double)]),
     "oa_gpu_set_atoms": (C.c_int, [_vp, _vp, _dp]),
@@ -399,12 +398,10 @@ class CPContext:
         _check(self._lib.oa_gpu_integrate(self._h, self._stream(), _ptr(force), _ptr(vpsi), _ptr(psi), float(dt),
                                           int(complete_prev), _ptr(fict_out)))
 
-    def psiv_reset(self, psi, psi_t, vpsi, nterm=0):
-        if nterm:
-            _check(self._lib.oa_gpu_psiv_reset_mixed(self._h, self._stream(), _ptr(psi), _ptr(psi_t), _ptr(vpsi),
-                                                     int(nterm)))
-        else:
-            _check(self._lib.oa_gpu_psiv_reset(self._h, self._stream(), _ptr(psi), _ptr(psi_t), _ptr(vpsi)))
+    def psiv_reset(self, psi, psi_prev, psi_t, vpsi, dt: float):
+        """psi_t <- psi, v <- (psi - psi_prev) / dt (oa_gpu_psiv_reset)."""
+        _check(self._lib.oa_gpu_psiv_reset(self._h, self._stream(), _ptr(psi), _ptr(psi_prev), _ptr(psi_t),
+                                           _ptr(vpsi), float(dt)))
 
     def set_atoms(self, pos_host: np.ndarray):
         a = np.ascontiguousarray(pos_host, dtype=np.float64)
@@ -518,6 +515,8 @@ class CPDriver:
         self.v = torch.zeros_like(self.psi) if v0 is None else torch.from_numpy(np.ascontiguousarray(v0)).to(dev)
         self.F = torch.zeros_like(self.psi)
         self.F2 = torch.zeros_like(self.psi)
+        self.psi_prev = torch.zeros_like(self.psi)   # psi(t - dt) for the PsiV finite difference
+        self.half_step = True
         self.Fnl = torch.zeros_like(self.psi)
         # mixed form: split-BF16 tcgen05 GEMMs for Lambda, the constraint
         # force and the nonlocal Z / force products; FP64 for S and Psi T
@@ -562,6 +561,7 @@ class CPDriver:
         st.ns_tol, st.norb_tol, st.ns_max_iter = self.tol, self.norb_tol, self.max_iter
         st.mixed_nterm = self.nterm_nl
         st.use_graph = int(use_graph)
+        st.psiv_pending = 0 if self.half_step else 1
         return st
 
     def step_native(self, state: CPState) -> dict:
@@ -570,6 +570,7 @@ class CPDriver:
         with self.torch.cuda.stream(self.stream):
             en = self.ctx.cp_step(state)
         self.iteration = state.iteration
+        self.half_step = not state.psiv_pending
         self.last_ortho = (int(en["ORTHO_ITERS"]), en["ORTHO_ERR"], True)
         return en
 
@@ -579,16 +580,27 @@ class CPDriver:
         with self.torch.cuda.stream(self.stream):
             ens = self.ctx.cp_run(state, nsteps, pos_host)
         self.iteration = state.iteration
+        self.half_step = not state.psiv_pending
         self.last_ortho = (int(ens[-1]["ORTHO_ITERS"]), ens[-1]["ORTHO_ERR"], True)
         return ens
 
     def launches_per_step(self) -> int:
         return self.ctx.sizes()["launches_per_step"]
 
-    def psiv_reset(self):
-        """PsiV tolerance reset (oracle.psiv_reset restates the reference)."""
-        self.ctx.psiv_reset(self.psi, self.psi_t, self.v, nterm=self.nterm_nl)
+    def psiv_reset(self, dt: float):
+        """PsiV tolerance reset of the reference's default build
+        (finiteDifferencePsiV; oracle.psiv_reset restates it): psi_t = psi,
+        T = I, v = (psi - psi_prev) / dt, and the next integration completes
+        no half kick."""
+        self.ctx.psiv_reset(self.psi, self.psi_prev, self.psi_t, self.v, dt)
         self.T.copy_(self.torch.eye(self.sys.nstate, dtype=self.torch.float64, device=self.T.device))
+        self.half_step = False
+
+    def _restart_frame(self):
+        """psi_t = psi, T = I (the quench's reset, velocities zero)."""
+        self.psi_t.copy_(self.psi)
+        self.T.copy_(self.torch.eye(self.sys.nstate, dtype=self.torch.float64, device=self.T.device))
+        self.half_step = True
 
     def quench(self, nsteps: int, dt: float | None = None):
         """Damped CP (steepest descent on the orthonormal states): each step
@@ -597,7 +609,7 @@ class CPDriver:
         out = []
         for _ in range(nsteps):
             out.append(self.step(damp_velocity=True, dt=dt))
-            self.psiv_reset()
+            self._restart_frame()
             self.iteration = 0
         return out
 
@@ -616,8 +628,9 @@ class CPDriver:
             c.pc_forward(self.psi, self.F, 1.0, 1.0, self.lam)
             c.small_gemm(self.T, self.lam, 1.0, self.gam)
             c.pc_backward(self.gam, self.psi, -0.5, -1.0, self.F2, M2=self.T, X2=self.F, a2=1.0)
-        # integrate psi_t
-        c.integrate(self.F2, self.v, self.psi_t, dt, self.iteration > 1)
+        # integrate psi_t (after a PsiV reset the velocity is already at t)
+        c.integrate(self.F2, self.v, self.psi_t, dt, self.iteration > 1 and self.half_step)
+        self.half_step = True
         en["FICT_KE"] = c.energies()["FICT_KE"]
         if damp_velocity:
             self.v.zero_()
@@ -627,10 +640,11 @@ class CPDriver:
         self.last_ortho = (it, err, ok)
         if not ok:
             raise RuntimeError(f"Newton-Schulz did not converge: {it} iterations, residual {err:g}")
+        self.psi_prev.copy_(self.psi)
         c.pc_backward(self.T, self.psi_t, 1.0, 1.0, self.psi)
         if smax > self.norb_tol and not damp_velocity:
             # Ortho::maxCheck -> PsiV: restart the non-orthogonal set from psi
-            self.psiv_reset()
+            self.psiv_reset(dt)
             self.n_psiv += 1
         en["ORTHO_ITERS"] = it
         en["ORTHO_ERR"] = err
@@ -729,4 +743,5 @@ def run_batch(drivers, states, nsteps: int, stream=None) -> list:
                                    out.ctypes.data_as(_dp)))
     for d, s in zip(drivers, states):
         d.iteration = s.iteration
+        d.half_step = not s.psiv_pending
     return [[{k: float(v) for k, v in zip(STEP_KEYS, row)} for row in sysrows] for sysrows in out]

@@ -1163,6 +1163,7 @@ class CPState:
         self.T = np.eye(sysm.nstate)
         self.v = np.zeros_like(sysm.psi)
         self.iteration = 0
+        self.half_step = True    # False after a PsiV reset: v is at t, the next step completes no half kick
 
 
 def electronic_forces(psi, sysm, fnl=None, enl=0.0):
@@ -1177,20 +1178,20 @@ def electronic_forces(psi, sysm, fnl=None, enl=0.0):
     return f, en
 
 
-def psiv_reset(st, sysm):
-    """PsiV tolerance reset (``Ortho::maxCheck``, ``ortho.C:455-475``; the
-    "replace non-ortho psi by ortho" copies of ``CP_State_GSpacePlane.C:3590-3600,
-    3750-3760``): psi_t <- psi, T <- I, and the velocities projected onto the
-    orthonormality constraint, v_j <- v_j - sum_k psi_k X_kj with
-    X = (A + A^T)/4, A = <psi_i|v_j> in the S metric (alpha = 2)."""
-    r2i = 1.0 / math.sqrt(2.0)
-    ps = kx0_scale(st.psi, sysm, r2i)
-    vs = kx0_scale(st.v, sysm, r2i)
-    A = pc_forward(ps, vs, sysm, 2.0)
-    X = 0.25 * (A + A.T)
-    st.v = st.v - X.T @ st.psi
+def psiv_reset(st, sysm, psi_prev, dt):
+    """PsiV tolerance reset of the reference's default build
+    (``Ortho::maxCheck``, ``ortho.C:455-475`` -> ``computeNewPsiVFiniteDifference``,
+    ``gspace.ci:290-301``; ``CP_State_GSpacePlane::finiteDifferencePsiV``,
+    ``CP_State_GSpacePlane.C:3741-3800``, ``norb_fin_diff_order`` 0): the
+    non-orthogonal set is replaced by the orthonormal one (psi_t <- psi,
+    T <- I) and the velocities by the first-order finite difference of the
+    orthonormal states, v = (psi(t) - psi(t - dt)) / dt, taken as the
+    velocity at t (``halfStepEvolve = 0``: the next integration does not
+    complete a half kick)."""
+    st.v = (st.psi - psi_prev) / dt
     st.psi_t = st.psi.copy()
     st.T = np.eye(sysm.nstate)
+    st.half_step = False
 
 
 def _nl_default(psi, sysm):
@@ -1212,6 +1213,8 @@ def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl="auto", norb_tol=None, dt=Non
     nonlocal atom forces come from it.  Returns the energy record of the psi
     the forces were evaluated on."""
     st.iteration += 1
+    dt_now = sysm.dt if dt is None else dt
+    psi_prev = st.psi.copy()       # the orthonormal psi(t) (sendLambda keeps it, CP_State_GSpacePlane.C:1838-1858)
     if ees is not None and ions is not None:
         ees["bspl"] = ees_bsplines(sysm, ees["grid"], ees["order"])
     if nl == "auto":
@@ -1226,7 +1229,10 @@ def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl="auto", norb_tol=None, dt=Non
         en.update(eion)
         en["ION_KE"] = integrate_ions(ions, fion, sysm, st.iteration, sysm.dt if dt is None else dt)
     f, lam = lambda_step(st.psi, f, st.T, sysm)
-    st.v, st.psi_t, fict = integrate_dyn(f, st.v, st.psi_t, sysm, st.iteration, sysm.dt if dt is None else dt)
+    # after a PsiV reset the velocity is already at t (halfStepEvolve = 0)
+    it_int = st.iteration if getattr(st, "half_step", True) else 1
+    st.v, st.psi_t, fict = integrate_dyn(f, st.v, st.psi_t, sysm, it_int, dt_now)
+    st.half_step = True
     en["FICT_KE"] = float(fict.sum())
     st.psi_t = sync_redundant(st.psi_t, sysm)
     st.v = sync_redundant(st.v, sysm)
@@ -1235,14 +1241,14 @@ def cp_step(st, sysm, tol=1e-15, max_iter=1000, nl="auto", norb_tol=None, dt=Non
     en["ORTHO_ERR"] = err
     en["SMAX"] = float(np.max(np.abs(S - 2.0 * np.eye(sysm.nstate))))
     if norb_tol is not None and en["SMAX"] > norb_tol:
-        psiv_reset(st, sysm)
+        psiv_reset(st, sysm, psi_prev, dt_now)
     return en
 
 
 def quench(st, sysm, nsteps, tol=1e-15, max_iter=1000, dt=None):
     """Damped CP from a random start: each step is ``cp_step`` with the
     velocities zeroed after the integration and the non-orthogonal set reset
-    to the orthonormal one (``psiv_reset`` with v = 0), the iteration count
+    to the orthonormal one (psi_t <- psi, T <- I, v = 0), the iteration count
     restarting every step -- steepest descent on the orthonormal states with
     step dt^2 / (2 m) (dt: the system's time step unless given).  The same
     procedure as ``CPDriver.quench`` on the GPU; it brings the start near the
@@ -1254,7 +1260,9 @@ def quench(st, sysm, nsteps, tol=1e-15, max_iter=1000, dt=None):
         st.v = np.zeros_like(st.v)
         en = cp_step(st, sysm, tol, max_iter, dt=dt)
         st.v = np.zeros_like(st.v)
-        psiv_reset(st, sysm)
+        st.psi_t = st.psi.copy()
+        st.T = np.eye(sysm.nstate)
+        st.half_step = True
         out.append(en)
     st.iteration = 0
     return out

@@ -127,8 +127,8 @@ def test_native_run_positions_and_failure():
 
 
 def test_native_run_matches_steps_mixed():
-    """Mixed form: the native run (device-decided PsiV with split-BF16
-    projection) reproduces the host runner bit for bit."""
+    """Mixed form: the native run (device-decided PsiV) reproduces the host
+    runner bit for bit."""
     from openatom_b200.gpu import CPDriver
     s = make_system("w8", nstate=16, seed=15, dt=0.5)
     a = CPDriver(s, "mixed", norb_tol=1e-14)
@@ -144,27 +144,46 @@ def test_native_run_matches_steps_mixed():
     assert np.array_equal(a.v.cpu().numpy(), c.v.cpu().numpy())
 
 
-def test_psiv_reset_mixed_matches_fp64():
-    """The split-BF16 PsiV projection agrees with the FP64 one to FP32-level
-    accuracy of the projection term, and leaves v in FP64 otherwise."""
+def test_psiv_reset_finite_difference():
+    """oa_gpu_psiv_reset (finiteDifferencePsiV): psi_t = psi and
+    v = (psi - psi_prev) / dt."""
     import torch
     from openatom_b200.gpu import CPContext
     s = make_system("w8", nstate=16, seed=16)
     ctx = CPContext(s, "mixed")
     rng = np.random.default_rng(2)
+    prev = s.psi + (rng.standard_normal(s.psi.shape) + 1j * rng.standard_normal(s.psi.shape)) * 1e-3
     psi = torch.from_numpy(s.psi).cuda()
-    v0 = (rng.standard_normal(s.psi.shape) + 1j * rng.standard_normal(s.psi.shape)) * 1e-3
-    out = {}
-    for nt in (0, 3):
-        v = torch.from_numpy(v0.copy()).cuda()
-        pt = torch.zeros_like(psi)
-        ctx.psiv_reset(psi, pt, v, nterm=nt)
-        torch.cuda.synchronize()
-        assert np.array_equal(pt.cpu().numpy(), s.psi)
-        out[nt] = v.cpu().numpy()
-    d64 = out[0] - v0
-    err = np.max(np.abs(out[3] - out[0])) / np.max(np.abs(d64))
-    assert err < 1e-5, err
+    pp = torch.from_numpy(prev).cuda()
+    v = torch.zeros_like(psi)
+    pt = torch.zeros_like(psi)
+    ctx.psiv_reset(psi, pp, pt, v, 5.0)
+    torch.cuda.synchronize()
+    assert np.array_equal(pt.cpu().numpy(), s.psi)
+    ref = (s.psi - prev) / 5.0
+    assert np.max(np.abs(v.cpu().numpy() - ref)) <= 1e-15 * np.max(np.abs(s.psi)) / 5.0 * 4
+    ctx.close()
+
+
+def test_native_runs_carry_a_pending_psiv_reset():
+    """Runs split at every step reproduce one long run bit for bit, PsiV
+    resets included (the pending reset crosses the call: the next step
+    completes no half kick)."""
+    from openatom_b200.gpu import CPDriver
+    s = make_system("w8", nstate=16, seed=17, dt=0.5)
+    a = CPDriver(s, "fp64", norb_tol=1e-3)
+    b = CPDriver(s, "fp64", norb_tol=1e-3)
+    sa = a.native_state(use_graph=True)
+    sb = b.native_state(use_graph=True)
+    ea = a.run_native(sa, 6)
+    eb = []
+    for _ in range(6):
+        eb += b.run_native(sb, 1)
+    assert any(e["SMAX"] > 1e-3 for e in ea[:-1]), "no reset inside the run"
+    for i in range(6):
+        for k in ("EKE", "FICT_KE", "SMAX"):
+            assert eb[i][k] == ea[i][k], (i, k, ea[i][k], eb[i][k])
+    assert np.array_equal(a.v.cpu().numpy(), b.v.cpu().numpy())
 
 
 def test_native_run_odd_state_count():

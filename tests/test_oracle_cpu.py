@@ -100,17 +100,23 @@ def test_energy_conservation(w2):
 
 
 def test_psiv_reset_restores_orthonormal_frame(w2):
+    """finiteDifferencePsiV: psi_t = psi (orthonormal), T = I, v = (psi(t) -
+    psi(t - dt)) / dt, and the next step completes no half kick."""
     s = make_system("w2", seed=3, dt=0.5)
     st = O.CPState(s)
     for _ in range(3):
         O.cp_step(st, s)
-    O.psiv_reset(st, s)
+    prev = st.psi.copy()
+    O.cp_step(st, s)
+    O.psiv_reset(st, s, prev, s.dt)
     S = gamma_overlap(st.psi_t, s.kx)
     assert np.max(np.abs(S - 2 * np.eye(s.nstate))) < 1e-12
-    # velocities satisfy the linearised constraint <psi_i|v_j> + <v_i|psi_j> = 0
-    r2i = 1 / math.sqrt(2)
-    A = O.pc_forward(O.kx0_scale(st.psi, s, r2i), O.kx0_scale(st.v, s, r2i), s, 2.0)
-    assert np.max(np.abs(A + A.T)) < 1e-12
+    assert np.array_equal(st.T, np.eye(s.nstate))
+    assert np.allclose(st.v, (st.psi - prev) / s.dt, rtol=0, atol=1e-15)
+    # the next step's fictitious KE is that of v itself (no completing half kick)
+    v0 = st.v.copy()
+    en = O.cp_step(st, s)
+    assert abs(en["FICT_KE"] - float(O.fict_ke(v0, s.cmass, s).sum())) <= 1e-12 * en["FICT_KE"]
 
 
 def test_nonlocal_force_is_energy_gradient(w2):
