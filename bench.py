@@ -55,6 +55,8 @@ def parse():
                     help="CG iterations of the large system's start")
     ap.add_argument("--blyp", type=int, default=1,
                     help="also time the 32-water step with the BLYP gradient correction (0: skip)")
+    ap.add_argument("--ground", type=int, default=1,
+                    help="also time the headline system from its CG-minimised ground state (0: skip)")
     ap.add_argument("--ions", type=int, default=1,
                     help="also time the 32-water step with moving atoms (structure factors, EES local; 0: skip)")
     ap.add_argument("--drift-steps", type=int, default=1000,
@@ -603,7 +605,7 @@ def run_ours(args):
     force_call = force_call_form(torch, dmx, args.steps)
     # the same timing from the electronic ground state (CG minimisation):
     # the reference's cp_min_opt start, where the PsiV reset fires rarely
-    ground = ground_state_form(torch, sysm, args.steps) if rk == 0 else None
+    ground = ground_state_form(torch, sysm, args.steps) if (rk == 0 and args.ground > 0) else None
     # per-kernel timing (CUDA events on the launch stream) for the roofline
     kt = dmx.ctx.time_kernels(dmx.psi, reps=5)
     kt64 = d64.ctx.time_kernels(d64.psi, reps=5)
