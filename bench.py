@@ -519,9 +519,8 @@ def drift_form(torch, args, want_oracle):
     psi0, start = minimized_start(sysm)
     n = args.drift_steps
     recs = {p: native_records(sysm, psi0, p, n) for p in ("fp64", "mixed")}
-    # the same runs without the PsiV tolerance reset (its velocity projection
-    # removes fictitious kinetic energy): the energy conservation of the
-    # integrator and the orthonormality constraint alone
+    # the same runs without the PsiV tolerance reset: the integrator and the
+    # orthonormality constraint alone
     from openatom_b200.gpu import OaError
     free = {}
     out = {"workload": f"w8: 8 H2O, {sysm.nstate} states, 70 Ry, 64^3, ng={sysm.ng}", "steps": n,

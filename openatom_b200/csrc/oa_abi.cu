@@ -1115,17 +1115,6 @@ static cudaError_t mixed_bwd(oa_ctx* c, cudaStream_t s, int nt, const double* M1
   return oa_launch_umma_bwd(s, nt, M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out, p->err_flag);
 }
 
-// Velocity part of the PsiV reset (CP_State_GSpacePlane.C:3590-3600,
-// 3750-3760 with the orthoT velocity projection): X = sym(psi v^T) / 4 with
-// the S weights, v <- v - X psi (in place).  cond: optional device flag; the
-// launches do nothing when it is 0.
-
-// psi = psi_t T (FP64); then, under the PsiV flag, the velocity projection
-// and T = I (the next step's check sets or clears the flag).  The reset's
-// psi_t = psi is deferred: the next integration reads psi under the flag,
-// and a run ends with oa_psi_t_settle.  The native step's orthonormalisation
-// and PsiV reset (Ortho::maxCheck, ortho.C:455-475): same results as
-// oa_gpu_pc_backward followed by oa_gpu_psiv_reset, decided on the device.
 // v = sign psi / dt under the device flag (and everywhere when cond is
 // null): the two halves of finiteDifferencePsiV's v = (psi(t) - psi(t-dt)) / dt
 // around the rotation that overwrites psi(t - dt) with psi(t)
