@@ -388,7 +388,24 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
           }
         } else {
           const double2* pl = pxy + grp * ZP_L * natm;
-          for (int ia = toff.off[t]; ia < toff.off[t + 1]; ++ia) {
+          // four z-phase loads in flight per thread (the loop is bound by
+          // their latency, not by the multiply-adds)
+          // (the force variant, short of registers, takes them one at a time)
+          const int a0 = toff.off[t], a1 = toff.off[t + 1];
+          int ia = a0;
+          for (; !FORCES && ia + 4 <= a1; ia += 4) {
+            double2 hz[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) hz[u] = phase[zoff[ia + u] + kz];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+              for (int j = 0; j < ZP_L; ++j) {
+                const double2 h = cmul(pl[j * natm + ia + u], hz[u]);
+                st[j].x += h.x; st[j].y += h.y;
+              }
+          }
+          for (; ia < a1; ++ia) {
             const double2 hz = phase[zoff[ia] + kz];
 #pragma unroll
             for (int j = 0; j < ZP_L; ++j) {
