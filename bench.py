@@ -71,6 +71,24 @@ def dist_env():
     return ws, rk, lr
 
 
+def max_over_ranks(values, ws, device="cuda"):
+    """The per-rank timings reduced to their maximum over the ranks (the
+    slowest replica sets the step time); one all-reduce, every rank takes
+    part."""
+    if ws <= 1:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def replica_seed(seed, rank):
+    """Seed of a rank's independent system (replicas only: no data-path
+    collective between ranks)."""
+    return seed + rank
+
+
 def make_sys(cfg, seed):
     from openatom_b200.system import make_system
     return make_system(cfg, seed=seed, ecut_mass=2.0, cmass0=400.0, dt=5.0)
@@ -557,7 +575,7 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    sysm = make_sys(args.config, args.seed + rk)
+    sysm = make_sys(args.config, replica_seed(args.seed, rk))
     natm = sysm.natm
 
     # quench the random start (untimed), FP64
@@ -591,10 +609,7 @@ def run_ours(args):
         # the same steps with a host synchronisation after each one
         ms_sync, _ = time_steps(torch, dmx, stmx, args.steps, sync_each=True)
         barrier()
-    if ws > 1:
-        t = torch.tensor([ms_mx, ms_64, ms_e2e, ms_sync], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_mx, ms_64, ms_e2e, ms_sync = [float(x) for x in t.tolist()]
+    ms_mx, ms_64, ms_e2e, ms_sync = max_over_ranks([ms_mx, ms_64, ms_e2e, ms_sync], ws)
 
     # accuracy of the mixed form against FP64 on the same trajectory start
     de = max(abs(total_energy(a) - total_energy(b)) for a, b in zip(en_mx, en_64)) / natm
