@@ -357,6 +357,8 @@ def test_pseudopotential_splines_pinned(ref, name, loc_opt, n_ang, label):
     norm.  Also checks that the packaged radial data equal the files."""
     from openatom_b200 import pseudo as P
     path = f"/root/reference/data/DATABASE/{name}_BLYP_PP30.pseud"
+    if not os.path.exists(path):
+        pytest.skip("reference pseudopotential files absent")
     ref.ref_vps_splin.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                   C.c_double, C.c_double, dp, dp, dp, dp, dp]
     grid = P.spline_grid(11.7, 70.0)
