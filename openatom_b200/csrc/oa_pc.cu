@@ -179,39 +179,29 @@ k_pc_bwd_f64(const double* __restrict__ M1, const double* __restrict__ X1, doubl
 }
 
 // ---------------------------------------------------------------------------
-// small N x N: C = alpha * A B, FP64; 32 x 32 output tile per block of
-// 256 threads (4 outputs each), K in slabs of 32 through shared memory
+// small N x N: C = alpha * A B, FP64; 16 x 16 output tile per block of
+// 256 threads (one output each, k in ascending order), K in slabs of 16
+// through shared memory
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
 k_small_gemm(const double* __restrict__ A, const double* __restrict__ B, int n, double alpha,
              double* __restrict__ C) {
-  __shared__ double sA[32][33], sB[32][33];
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // ty 0..7: rows ty, ty + 8, ..
-  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int k0 = 0; k0 < n; k0 += 32) {
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int row = ty + 8 * r;
-      const int ia = i0 + row, ka = k0 + tx;
-      sA[row][tx] = (ia < n && ka < n) ? A[(size_t)ia * n + ka] : 0.0;
-      const int kb = k0 + row, jb = j0 + tx;
-      sB[row][tx] = (kb < n && jb < n) ? B[(size_t)kb * n + jb] : 0.0;
-    }
+  __shared__ double sA[16][17], sB[16][17];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int i0 = blockIdx.y * 16, j0 = blockIdx.x * 16;
+  double acc = 0.0;
+  for (int k0 = 0; k0 < n; k0 += 16) {
+    const int ia = i0 + ty, ka = k0 + tx;
+    sA[ty][tx] = (ia < n && ka < n) ? A[(size_t)ia * n + ka] : 0.0;
+    const int kb = k0 + ty, jb = j0 + tx;
+    sB[ty][tx] = (kb < n && jb < n) ? B[(size_t)kb * n + jb] : 0.0;
     __syncthreads();
-#pragma unroll 8
-    for (int k = 0; k < 32; ++k) {
-      const double b = sB[k][tx];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) acc[r] = fma(sA[ty + 8 * r][k], b, acc[r]);
-    }
+    for (int k = 0; k < 16; ++k) acc = fma(sA[ty][k], sB[k][tx], acc);
     __syncthreads();
   }
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const int i = i0 + ty + 8 * r, j = j0 + tx;
-    if (i < n && j < n) C[(size_t)i * n + j] = alpha * acc[r];
-  }
+  const int i = i0 + ty, j = j0 + tx;
+  if (i < n && j < n) C[(size_t)i * n + j] = alpha * acc;
 }
 
 // Several single-block sums in one launch: block b writes
@@ -586,7 +576,7 @@ cudaError_t oa_launch_pc_bwd(cudaStream_t s, const double* M1, const double* X1,
 }
 
 cudaError_t oa_launch_small_gemm(cudaStream_t s, const double* A, const double* B, int n, double alpha, double* C) {
-  dim3 grid((n + 31) / 32, (n + 31) / 32);
+  dim3 grid((n + 15) / 16, (n + 15) / 16);
   k_small_gemm<<<grid, 256, 0, s>>>(A, B, n, alpha, C);
   return cudaGetLastError();
 }
