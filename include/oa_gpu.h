@@ -367,8 +367,7 @@ oa_status oa_gpu_cp_run_batch(oa_ctx **ctxs, oa_cp_state **states, int nsys, voi
  * ordered).  Larger nstate returns OA_ERR_BAD_ARG.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) and
  * caches it for the process (no cudaDeviceReset while the library is
- * loaded); make that first call before any stream capture.  No counterpart
- * in the reference. */
+ * loaded).  No counterpart in the reference. */
 oa_status oa_gpu_pc_forward_noalloc(void *stream, const double *left, const double *right, int nstate, int ng,
                                     int nkx0, double alpha, double w_kx0, double *C);
 
