@@ -83,10 +83,13 @@ k_zfwd2(const double2* __restrict__ psi, int ng, int s0, const int* __restrict__
   const double2* ps = psi + (size_t)s * ng;
   const int g0 = zseg > 0 ? line_off[l0] : 0;
   if (zseg > 0) {
+    // every 16-byte copy of the run issued before any is waited for
     const int g1 = (l0 + nb < nlines) ? line_off[l0 + nb] : ng;
-    for (int i = threadIdx.x; i < g1 - g0; i += blockDim.x) seg[i] = ps[g0 + i];
+    for (int i = threadIdx.x; i < g1 - g0; i += blockDim.x) zp_cp16(seg + i, ps + g0 + i);
+    asm volatile("cp.async.commit_group;\n" ::);
   }
   load_twiddles(tw, twz, N);
+  if (zseg > 0) asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   double q = 0.0;  // charge partial (qc.part)
   for (int it = threadIdx.x; it < nb * N2; it += blockDim.x) {
@@ -554,6 +557,16 @@ int oa_pencil_supported(int n) {
 
 // shared memory of the z passes: twiddles, the pass buffer, 64 doubles of
 // reduction scratch, and nseg staged coefficient segments of zseg elements
+// threads of a z-pass block: one per item of the larger of the two passes
+// (N2 x OA_LB pass A items, N1 x OA_LB pass B items), in whole warps, at
+// most OA_NTHREADS; smaller blocks than OA_NTHREADS leave room for more
+// resident blocks, each with its staged coefficient run in flight
+template <int N1, int N2> constexpr int zpass_threads() {
+  constexpr int items = (N1 > N2 ? N1 : N2) * OA_LB;
+  constexpr int t = (items + 31) / 32 * 32;
+  return t < OA_NTHREADS ? t : OA_NTHREADS;
+}
+
 template <typename R, int N1, int N2>
 static size_t zpass2_smem(int zseg, int nseg) {
   typedef typename CplxOf<R>::T C;
@@ -570,7 +583,7 @@ static cudaError_t zfwd2_n(cudaStream_t st, const double2* psi, int ng, int s0, 
   cudaError_t e = oa_smem_limit(k_zfwd2<R, N1, N2>);
   if (e != cudaSuccess) return e;
   dim3 grid((nlines + OA_LB - 1) / OA_LB, ns);
-  k_zfwd2<R, N1, N2><<<grid, OA_NTHREADS, sm, st>>>(psi, ng, s0, off, nneg, npos, nlines, (C*)zbuf, ldl, tw, dyp,
+  k_zfwd2<R, N1, N2><<<grid, zpass_threads<N1, N2>(), sm, st>>>(psi, ng, s0, off, nneg, npos, nlines, (C*)zbuf, ldl, tw, dyp,
                                                      zseg, qc);
   return cudaGetLastError();
 }
@@ -605,7 +618,7 @@ static cudaError_t zbwd2_n(cudaStream_t st, const void* zbuf, int ldl, int nline
   cudaError_t e = oa_smem_limit(k_zbwd2<R, N1, N2>);
   if (e != cudaSuccess) return e;
   dim3 grid(nblk, ns);
-  k_zbwd2<R, N1, N2><<<grid, OA_NTHREADS, sm, st>>>((const C*)zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl,
+  k_zbwd2<R, N1, N2><<<grid, zpass_threads<N1, N2>(), sm, st>>>((const C*)zbuf, ldl, nlines, lkx, off, nneg, npos, tw, psi, fnl,
                                                      force, g2, occ, ng, s0, scale, ecut, eke_part, nblk, dyp,
                                                      po, zseg);
   return cudaGetLastError();

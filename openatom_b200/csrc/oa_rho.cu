@@ -44,6 +44,16 @@ __device__ void block_sum_n(double* v, double* sh /* 32*NV */) {
 
 __host__ __device__ static inline size_t align_up_r(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// 16-byte global -> shared copy without a register round trip, so that a
+// block's staging copies are all in flight together (the caller commits
+// the group and waits for it)
+__device__ __forceinline__ void rho_cp16(void* sdst, const void* gsrc) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc));
+}
+__device__ __forceinline__ void rho_cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void rho_cp_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // ---------------------------------------------------------------------------
 // density sum + PZ-LDA
 // ---------------------------------------------------------------------------
@@ -285,7 +295,14 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
   int* zoff = (int*)(pxy + OA_LB * natm);  // [natm]: z-phase row of atom ia (type order)
   // FORCES: [OA_LB * nz][ntype] per-type (A, B) coefficients after zoff
   double2* cf = (double2*)(smem_raw + (((size_t)((char*)(zoff + natm) - (char*)smem_raw) + 15) & ~(size_t)15));
+  // the line's density coefficients: every 16-byte copy issued before any is waited for
+  for (int idx = threadIdx.x; idx < nz * OA_LB; idx += blockDim.x) {
+    const int zz = idx / OA_LB, lb = idx - zz * OA_LB;
+    if (lb < nb) rho_cp16(a + lb * ldz + zz, dz + (size_t)zz * ldl_d + l0 + lb);
+  }
+  rho_cp_commit();
   for (int ia = threadIdx.x; ia < natm; ia += blockDim.x) zoff[ia] = (atm_perm[ia] * 3 + 2) * nt + ktab;
+#pragma unroll 4
   for (int idx = use_ees ? OA_LB * natm : threadIdx.x; idx < OA_LB * natm; idx += blockDim.x) {
     const int lb = idx / natm, ia = idx - lb * natm;
     const int l = l0 + lb;
@@ -298,10 +315,7 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
     }
     pxy[lb * natm + ia] = v;
   }
-  for (int idx = threadIdx.x; idx < nz * OA_LB; idx += blockDim.x) {
-    const int zz = idx / OA_LB, lb = idx - zz * OA_LB;
-    if (lb < nb) a[lb * ldz + zz] = dz[(size_t)zz * ldl_d + l0 + lb];
-  }
+  rho_cp_wait();
   __syncthreads();
   double2* r;
   if constexpr (TP) {
@@ -712,8 +726,10 @@ k_rho_grad_z(const double2* __restrict__ dz, double2* __restrict__ dzg, size_t f
   load_twiddles(tw, twz, nz);
   for (int idx = threadIdx.x; idx < nz * OA_LB; idx += blockDim.x) {
     const int zz = idx / OA_LB, lb = idx - zz * OA_LB;
-    if (lb < nb) bufs[0][lb * ldz + zz] = dz[(size_t)zz * ldl_d + l0 + lb];
+    if (lb < nb) rho_cp16(bufs[0] + lb * ldz + zz, dz + (size_t)zz * ldl_d + l0 + lb);
   }
+  rho_cp_commit();
+  rho_cp_wait();
   __syncthreads();
   double2* r = zfft_any<N1, N2, -1>(bufs[0], bufs[1], ldz, nb, pz, tw);
   __syncthreads();
@@ -758,8 +774,10 @@ k_rho_div_z(double2* __restrict__ dz, const double2* __restrict__ dzh, size_t fs
     const double2* in = dzh + a * fstride;
     for (int idx = threadIdx.x; idx < nz * OA_LB; idx += blockDim.x) {
       const int zz = idx / OA_LB, lb = idx - zz * OA_LB;
-      if (lb < nb) a0[lb * ldz + zz] = in[(size_t)zz * ldl_d + l0 + lb];
+      if (lb < nb) rho_cp16(a0 + lb * ldz + zz, in + (size_t)zz * ldl_d + l0 + lb);
     }
+    rho_cp_commit();
+    rho_cp_wait();
     __syncthreads();
     const double2* r = zfft_any<N1, N2, -1>(a0, a1, ldz, nb, pz, tw);
     __syncthreads();
