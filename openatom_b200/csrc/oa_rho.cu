@@ -71,16 +71,19 @@ k_rho_xc(const double* __restrict__ rho_part, int ngroup, size_t npts, double rv
   const double power = 1.0 / 3.0;
   const double rat1 = (7.0 / 6.0) * beta1, rat2 = (4.0 / 3.0) * beta2;
   const double pi = 3.14159265358979323846, fpi = 4.0 * pi;
+  // rs = (3 / (4 pi r))^(1/3) and -(3 r / pi)^(1/3) from one cube root of
+  // r; a negative density gives NaN as the powers do
+  const double c_rs = cbrt(3.0 / fpi), c_x = cbrt(3.0 / pi);
   double acc[3] = {0.0, 0.0, 0.0};
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += (size_t)gridDim.x * blockDim.x) {
     double r = 0.0;
     for (int g = 0; g < ngroup; ++g) r += rho_part[(size_t)g * npts + i];
     r *= rvol;
     rho[i] = r;
-    const double fpin = fpi * r;
-    const double rs = pow(3.0 / fpin, power);
+    const double cr = r >= 0.0 ? cbrt(r) : __longlong_as_double(0x7ff8000000000000LL);
+    const double rs = c_rs / cr;
     const double sqtrs = sqrt(rs);
-    const double xfact = -pow(3.0 * r / pi, power);
+    const double xfact = -c_x * cr;
     double cfact, mufact;
     if (rs >= 1.0) {
       const double cf1 = 1.0 + beta1 * sqtrs + beta2 * rs;
