@@ -279,9 +279,11 @@ extern "C" oa_status oa_gpu_init(const oa_system_desc* d, int precision, oa_ctx*
   // measurements over 8-32 water systems on 64^3-108^3 grids imply
   c->ngroup_pair = pick_groups(d->nz, (d->nstate + 1) / 2, 1, nsm, 2);
   c->pair_kymax = 0;
+  c->z_ext = 0;
   for (int l = 0; l < d->nlines; ++l) {
     const int a = d->line_ky[l] < 0 ? -d->line_ky[l] : d->line_ky[l];
     c->pair_kymax = a > c->pair_kymax ? a : c->pair_kymax;
+    c->z_ext = std::max(c->z_ext, std::max(d->line_nneg[l], d->line_npos[l]));
   }
   c->rho_ngroup = c->ngroup;
   c->nblk_z = (d->nlines + OA_LB - 1) / OA_LB;

@@ -103,6 +103,7 @@ struct oa_ctx {
   int rho_ngroup;         // groups summed in rho_part by the last density pass
   int* pair_cols;         // [nkx_s] {first line, ky of the first line, lines, 0}: FP32 pair kernels
   int pair_kymax;         // largest |ky| of the state lines
+  int z_ext;              // largest kz count of a state line on either side (max of nneg, npos)
   void* psir;             // psi(r), compute precision: [nstate][nz][ny][nx] (two-pass kernels)
                           // or [nstate/2][nz][ny][nx] pairs (state-pair kernels)
   int psir_valid;         // the last density pass stored psir: 1 per state, 2 per pair

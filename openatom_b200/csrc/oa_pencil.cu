@@ -60,8 +60,10 @@ __device__ __forceinline__ int line_slot(int z, int n, int nn, int np) {
 // ---------------------------------------------------------------------------
 // z pass forward: packed sphere (optionally conj(dyp psi)) -> FFT(-) of the
 // zero-filled z-line -> zbuf[s][z][line].  Block = OA_LB lines of one state.
+// BAND: every line's kz lie in (-N/4, N/4), so the pass-A inputs n1 in
+// [N1/4, 3 N1/4) are zero (band-pruned first DFT, RDftBand).
 // ---------------------------------------------------------------------------
-template <typename R, int N1, int N2>
+template <typename R, int N1, int N2, bool BAND>
 __global__ void __launch_bounds__(OA_NTHREADS)
 k_zfwd2(const double2* __restrict__ psi, int ng, int s0, const int* __restrict__ line_off,
         const int* __restrict__ line_nneg, const int* __restrict__ line_npos, int nlines,
@@ -100,6 +102,10 @@ k_zfwd2(const double2* __restrict__ psi, int ng, int s0, const int* __restrict__
     C u[N1];
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1) {
+      if (BAND && n1 >= N1 / 4 && n1 < 3 * N1 / 4) {
+        u[n1] = cmk<C>(0.0, 0.0);
+        continue;
+      }
       const int i = line_slot(N2 * n1 + n2, N, nn, np);
       double2 v = make_double2(0.0, 0.0);
       if (i >= 0) {
@@ -112,7 +118,7 @@ k_zfwd2(const double2* __restrict__ psi, int ng, int s0, const int* __restrict__
       }
       u[n1] = cmk<C>(v.x, v.y);
     }
-    pass_a<N1, N2, -1>(u, n2, tw);
+    pass_a_band<N1, N2, -1, BAND>(u, n2, tw);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) s1[lb * L::ps1 + k1 * L::ls1 + n2] = u[k1];
   }
@@ -577,22 +583,29 @@ static size_t zpass2_smem(int zseg, int nseg) {
 template <typename R, int N1, int N2>
 static cudaError_t zfwd2_n(cudaStream_t st, const double2* psi, int ng, int s0, int ns, const int* off,
                            const int* nneg, const int* npos, int nlines, void* zbuf, int ldl, const double2* tw,
-                           const double2* dyp, int zseg, OaCharge qc) {
+                           const double2* dyp, int zseg, OaCharge qc, int zext) {
   typedef typename CplxOf<R>::T C;
   const size_t sm = zpass2_smem<R, N1, N2>(zseg, 1);
-  cudaError_t e = oa_smem_limit(k_zfwd2<R, N1, N2>);
-  if (e != cudaSuccess) return e;
-  dim3 grid((nlines + OA_LB - 1) / OA_LB, ns);
-  k_zfwd2<R, N1, N2><<<grid, zpass_threads<N1, N2>(), sm, st>>>(psi, ng, s0, off, nneg, npos, nlines, (C*)zbuf, ldl, tw, dyp,
-                                                     zseg, qc);
-  return cudaGetLastError();
+  const dim3 grid((nlines + OA_LB - 1) / OA_LB, ns);
+  auto launch = [&](auto kern) -> cudaError_t {
+    cudaError_t e = oa_smem_limit(kern);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, zpass_threads<N1, N2>(), sm, st>>>(psi, ng, s0, off, nneg, npos, nlines, (C*)zbuf, ldl, tw, dyp,
+                                                    zseg, qc);
+    return cudaGetLastError();
+  };
+  // every line's kz within (-N/4, N/4): the band-pruned first DFT
+  if constexpr (N1 % 4 == 0) {
+    if (4 * zext <= N1 * N2) return launch(k_zfwd2<R, N1, N2, true>);
+  }
+  return launch(k_zfwd2<R, N1, N2, false>);
 }
 
 template <typename R>
 static cudaError_t zfwd2(cudaStream_t st, int n, const double2* psi, int ng, int s0, int ns, const int* off,
                          const int* nneg, const int* npos, int nlines, void* zbuf, int ldl, const double2* tw,
-                         const double2* dyp, int zseg, OaCharge qc) {
-#define OA_CALL(A, B) zfwd2_n<R, A, B>(st, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg, qc)
+                         const double2* dyp, int zseg, OaCharge qc, int zext) {
+#define OA_CALL(A, B) zfwd2_n<R, A, B>(st, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg, qc, zext)
   OA_PENCIL_DISPATCH(n, OA_CALL)
 #undef OA_CALL
   return cudaErrorNotSupported;
@@ -600,10 +613,10 @@ static cudaError_t zfwd2(cudaStream_t st, int n, const double2* psi, int ng, int
 
 cudaError_t oa_pencil_zfwd(int precision, cudaStream_t st, int n, const double2* psi, int ng, int s0, int ns,
                            const int* off, const int* nneg, const int* npos, int nlines, void* zbuf, int ldl,
-                           const double2* tw, const double2* dyp, int zseg, OaCharge qc) {
+                           const double2* tw, const double2* dyp, int zseg, OaCharge qc, int zext) {
   return precision == OA_FP64
-             ? zfwd2<double>(st, n, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg, qc)
-             : zfwd2<float>(st, n, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg, qc);
+             ? zfwd2<double>(st, n, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg, qc, zext)
+             : zfwd2<float>(st, n, psi, ng, s0, ns, off, nneg, npos, nlines, zbuf, ldl, tw, dyp, zseg, qc, zext);
 }
 
 template <typename R, int N1, int N2>

@@ -340,7 +340,7 @@ int oa_pencil_supported(int n);
 size_t oa_pencil_plane_smem(int precision, int n, int nkx);
 cudaError_t oa_pencil_zfwd(int precision, cudaStream_t st, int n, const double2* psi, int ng, int s0, int ns,
                            const int* off, const int* nneg, const int* npos, int nlines, void* zbuf, int ldl,
-                           const double2* tw, const double2* dyp, int zseg, OaCharge qc);
+                           const double2* tw, const double2* dyp, int zseg, OaCharge qc, int zext);
 cudaError_t oa_pencil_zbwd(int precision, cudaStream_t st, int n, const void* zbuf, int ldl, int nlines,
                            const int* lkx, const int* off, const int* nneg, const int* npos, const double2* tw,
                            const double2* psi, const double2* fnl, double2* force, const double* g2,
@@ -426,7 +426,7 @@ cudaError_t oa_launch_state_zfwd(oa_ctx* c, cudaStream_t s, const double2* psi, 
     if (c->qpart && s0 == 0 && ns == c->nstate) qc = OaCharge{c->line_kx, c->occ, c->qpart};
     c->qvalid = qc.part ? 1 : 0;
     return oa_pencil_zfwd(c->precision, s, c->nz, psi, c->ng, s0, ns, c->line_off, c->line_nneg, c->line_npos,
-                          c->nlines, c->zbuf, c->ldl, c->tw_z, nullptr, c->zseg, qc);
+                          c->nlines, c->zbuf, c->ldl, c->tw_z, nullptr, c->zseg, qc, c->z_ext);
   }
   c->qvalid = 0;
   return c->precision == OA_FP64 ? launch_zfwd<double>(c, s, psi, s0, ns) : launch_zfwd<float>(c, s, psi, s0, ns);
@@ -496,7 +496,7 @@ static cudaError_t launch_ees(oa_ctx* c, cudaStream_t st, const double2* psi, do
   // z pass forward with conj(dyp psi)
   if (pz) {
     err = oa_pencil_zfwd(c->precision, st, e->nc, psi, c->ng, 0, c->nstate, c->line_off, c->line_nneg, c->line_npos,
-                         c->nlines, e->zbuf, c->ldl, e->tw_c, e->dyp, c->zseg, OaCharge{nullptr, nullptr, nullptr});
+                         c->nlines, e->zbuf, c->ldl, e->tw_c, e->dyp, c->zseg, OaCharge{nullptr, nullptr, nullptr}, c->z_ext);
     if (err != cudaSuccess) return err;
   } else {
     size_t sm = zpass_smem<R>(e->nc);
