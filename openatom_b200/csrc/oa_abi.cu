@@ -788,7 +788,8 @@ cudaError_t oa_dgemm_fwd(cudaStream_t s, const double* A, const double* B, int m
 cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
                             const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
                             double* out, const int* cond, const double* yadd, double* out2, const int* cond2,
-                            const OaPlaneOut* po = nullptr);
+                            const OaPlaneOut* po = nullptr, double* vel = nullptr, double vscale = 0.0,
+                            const int* vcond = nullptr);
 
 #define OA_STEP_CHECK(x) do { const oa_status st_ = (x); if (st_ != OA_OK) return st_; } while (0)
 
@@ -1154,16 +1155,20 @@ oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* 
                             double* Tout, int* flag, int nterm, double dt) {
   oa_ctx_pc* p = pcx(c);
   const int n = c->nstate;
-  OA_CUDA_TRY(fd_velocity(c, s, psi, vpsi, -1.0 / dt, 0, flag));
   OaPlaneOut po;
   bool fuse = nterm > 0 && plane_out(c, PL_PSI, n, nterm, &po);
+  // the rotation's epilogue writes the velocity under the flag from the psi
+  // it overwrites (no separate passes)
   cudaError_t e = oa_dgemm_bwd_ex(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, n, 2L * c->ng, 2L * c->nkx0, psi,
-                                  nullptr, nullptr, nullptr, nullptr, fuse ? &po : nullptr);
+                                  nullptr, nullptr, nullptr, nullptr, fuse ? &po : nullptr, vpsi, 1.0 / dt, flag);
   if (e == cudaErrorNotSupported) {
-    // above 128 states: the general kernel, and the psi planes are split
-    // again when a product needs them
+    // shapes the tiled kernel does not take: the general kernel, and the psi
+    // planes are split again when a product needs them; the velocity in two
+    // passes around it
+    OA_CUDA_TRY(fd_velocity(c, s, psi, vpsi, -1.0 / dt, 0, flag));
     e = oa_launch_pc_bwd(s, T, psi_t, 1.0, 1.0, nullptr, nullptr, 0.0, n, 2L * c->ng, 2L * c->nkx0, psi);
     OA_CUDA_TRY(e);
+    OA_CUDA_TRY(fd_velocity(c, s, psi, vpsi, 1.0 / dt, 1, flag));
     fuse = false;
   } else {
     OA_ALIGN_TRY(e);
@@ -1172,7 +1177,6 @@ oa_status oa_psi_t_and_psiv(oa_ctx* c, cudaStream_t s, const double* T, double* 
   // nonlocal products split psi again otherwise)
   if (fuse) plane_mark(c, PL_PSI, psi, n, po.rows_pad, nterm);
   else pcx(c)->pl_key[PL_PSI].valid = false;
-  OA_CUDA_TRY(fd_velocity(c, s, psi, vpsi, 1.0 / dt, 1, flag));
   k_copy_cond<<<16, 256, 0, s>>>(Tout, p->eye, (size_t)n * n, flag);
   OA_CUDA_TRY(cudaGetLastError());
   return OA_OK;

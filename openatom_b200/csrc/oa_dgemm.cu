@@ -312,15 +312,19 @@ __device__ __forceinline__ void db_load_slab(double* ms, double* xs, const doubl
 // Epilogue options: yadd (optional) adds yadd[j][c] to the result (it may
 // be the output array itself: each element is read and written by one
 // thread); out2 (optional) receives a second copy of the result when
-// *cond2 != 0.
+// *cond2 != 0; vel (optional, when *vcond != 0) receives the finite
+// difference (result - previous out) vscale, previous out read by the
+// thread that overwrites it.
 template <bool TWO>
 __global__ void __launch_bounds__(DB_THREADS, 2)
 k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double a1_kx0, double a1_rest,
             const double* __restrict__ M2, const double* __restrict__ X2, double a2, int nj, int nk, long ncol,
             long kx0_cols, double* out, const int* __restrict__ cond, const double* yadd, double* __restrict__ out2,
-            const int* __restrict__ cond2, OaPlaneOut po) {
+            const int* __restrict__ cond2, OaPlaneOut po, double* __restrict__ vel, double vscale,
+            const int* __restrict__ vcond) {
   if (cond && *cond == 0) return;
   const bool dual = out2 && *cond2 != 0;
+  const bool velo = vel && *vcond != 0;
   extern __shared__ __align__(16) double db_smem[];
   double* Ms = db_smem;
   double* Xs = db_smem + DB_STAGES * DB_MSLAB;
@@ -395,11 +399,16 @@ k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double
       if (c + 1 < ncol) {
         double2 v = make_double2(acc[a][b][0], acc[a][b][1]);
         if (yadd) { const double2 y = *(const double2*)(yadd + o); v.x += y.x; v.y += y.y; }
+        if (velo) {
+          const double2 p = *(const double2*)(out + o);
+          *(double2*)(vel + o) = make_double2(fma(v.x, vscale, p.x * -vscale), fma(v.y, vscale, p.y * -vscale));
+        }
         *(double2*)(out + o) = v;
         if (dual) *(double2*)(out2 + o) = v;
       } else if (c < ncol) {
         double v = acc[a][b][0];
         if (yadd) v += yadd[o];
+        if (velo) vel[o] = fma(v, vscale, out[o] * -vscale);
         out[o] = v;
         if (dual) out2[o] = v;
       }
@@ -450,12 +459,13 @@ k_dgemm_bwd(const double* __restrict__ M1, const double* __restrict__ X1, double
 cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, double a1_kx0, double a1_rest,
                             const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
                             double* out, const int* cond, const double* yadd, double* out2, const int* cond2,
-                            const OaPlaneOut* po) {
+                            const OaPlaneOut* po, double* vel, double vscale, const int* vcond) {
   const OaPlaneOut pz = po ? *po : OaPlaneOut{nullptr, 0, 0, 0};
+  if (vel && (!vcond || yadd || M2)) return cudaErrorInvalidValue;
   // plane tiles are whole 64-column pieces inside the plane rows
   if (pz.P && ((pz.ldp % DB_TC) || ncol > pz.ldp || nj > pz.rows_pad || pz.nt > 3)) return cudaErrorInvalidValue;
   const uintptr_t al = (uintptr_t)M1 | (uintptr_t)X1 | (uintptr_t)out | (uintptr_t)(M2 ? M2 : M1) |
-                       (uintptr_t)(X2 ? X2 : X1) | (uintptr_t)yadd | (uintptr_t)out2;
+                       (uintptr_t)(X2 ? X2 : X1) | (uintptr_t)yadd | (uintptr_t)out2 | (uintptr_t)vel;
   if (out2 && !cond2) return cudaErrorInvalidValue;
   if (nj <= 0 || (ncol & 1) || (al & 15) || nk <= 0 || (M2 && !X2)) return cudaErrorNotSupported;
   const size_t sm = (size_t)DB_STAGES * (DB_MSLAB + DB_XSLAB) * sizeof(double);
@@ -466,12 +476,12 @@ cudaError_t oa_dgemm_bwd_ex(cudaStream_t s, const double* M1, const double* X1, 
     e = oa_smem_limit(k_dgemm_bwd<true>);
     if (e != cudaSuccess) return e;
     k_dgemm_bwd<true><<<grid, DB_THREADS, sm, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out,
-                                                    cond, yadd, out2, cond2, pz);
+                                                    cond, yadd, out2, cond2, pz, vel, vscale, vcond);
   } else {
     e = oa_smem_limit(k_dgemm_bwd<false>);
     if (e != cudaSuccess) return e;
     k_dgemm_bwd<false><<<grid, DB_THREADS, sm, s>>>(M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols,
-                                                     out, cond, yadd, out2, cond2, pz);
+                                                     out, cond, yadd, out2, cond2, pz, vel, vscale, vcond);
   }
   return cudaGetLastError();
 }
@@ -480,5 +490,5 @@ cudaError_t oa_dgemm_bwd(cudaStream_t s, const double* M1, const double* X1, dou
                          const double* M2, const double* X2, double a2, int nj, int nk, long ncol, long kx0_cols,
                          double* out, const int* cond) {
   return oa_dgemm_bwd_ex(s, M1, X1, a1_kx0, a1_rest, M2, X2, a2, nj, nk, ncol, kx0_cols, out, cond, nullptr, nullptr,
-                         nullptr, nullptr);
+                         nullptr, nullptr, nullptr, 0.0, nullptr);
 }
