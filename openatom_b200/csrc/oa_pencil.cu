@@ -167,6 +167,15 @@ k_zbwd2(const typename CplxOf<R>::T* __restrict__ zbuf, int ldl, int nlines, con
   const int s = s0 + blockIdx.y;
   const int l0 = blockIdx.x * OA_LB;
   const int nb = min(OA_LB, nlines - l0);
+  // this thread's first pass-B item (k1 fastest): its line's packing read
+  // now, so that pass B does not wait for it
+  const int itB = threadIdx.x;
+  const bool hasB = itB < nb * N1;
+  int offB = 0, nnB = 0, npB = 0, kxB = 0;
+  if (hasB) {
+    const int l = l0 + itB / N1;
+    offB = line_off[l]; nnB = line_nneg[l]; npB = line_npos[l]; kxB = line_kx[l];
+  }
   const int g0 = zseg > 0 ? line_off[l0] : 0;
   if (zseg > 0 && !dyp) {
     const int g1 = (l0 + nb < nlines) ? line_off[l0 + nb] : ng;
@@ -178,10 +187,25 @@ k_zbwd2(const typename CplxOf<R>::T* __restrict__ zbuf, int ldl, int nlines, con
     }
     asm volatile("cp.async.commit_group;\n" ::);
   }
+  const C* in = zbuf + (size_t)s * N * ldl + l0;
+  // this thread's first pass-A item: its z-line loads go out before the
+  // twiddle barrier
+  const int itA = threadIdx.x;
+  const int n2A = itA / OA_LB, lbA = itA - n2A * OA_LB;
+  const bool hasA = itA < N2 * OA_LB && lbA < nb;
+  C uA[N1];
+  if (hasA) {
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) uA[n1] = in[(size_t)(N2 * n1 + n2A) * ldl + lbA];
+  }
   load_twiddles(tw, twz, N);
   __syncthreads();
-  const C* in = zbuf + (size_t)s * N * ldl + l0;
-  for (int it = threadIdx.x; it < N2 * OA_LB; it += blockDim.x) {
+  if (hasA) {
+    pass_a<N1, N2, +1>(uA, n2A, tw);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) s1[lbA * L::ps1 + k1 * L::ls1 + n2A] = uA[k1];
+  }
+  for (int it = threadIdx.x + blockDim.x; it < N2 * OA_LB; it += blockDim.x) {
     const int n2 = it / OA_LB, lb = it - n2 * OA_LB;
     if (lb >= nb) continue;
     C u[N1];
@@ -201,8 +225,11 @@ k_zbwd2(const typename CplxOf<R>::T* __restrict__ zbuf, int ldl, int nlines, con
   for (int it = threadIdx.x; it < nb * N1; it += blockDim.x) {
     const int lb = it / N1, k1 = it - lb * N1;
     const int l = l0 + lb;
-    const int off = line_off[l], nn = line_nneg[l], np = line_npos[l];
-    const double w = (line_kx[l] == 0) ? 1.0 : 2.0;
+    const bool first = it == itB;
+    const int off = first ? offB : line_off[l];
+    const int nn = first ? nnB : line_nneg[l];
+    const int np = first ? npB : line_npos[l];
+    const double w = ((first ? kxB : line_kx[l]) == 0) ? 1.0 : 2.0;
     const double sc = scale * w;
     const double wt = o * w;
     C v[N2];
@@ -214,16 +241,16 @@ k_zbwd2(const typename CplxOf<R>::T* __restrict__ zbuf, int ldl, int nlines, con
       const int i = line_slot(k1 + N1 * k2, N, nn, np);
       if (i < 0) continue;
       const int idx = off + i;
+      const double gg = g2[idx];
       if (dyp) {
         const double2 d = dyp[idx];
         const double px = (double)v[k2].x;
-        const double py = (g2[idx] == 0.0) ? 0.0 : (double)v[k2].y;
+        const double py = (gg == 0.0) ? 0.0 : (double)v[k2].y;
         fs[idx] = make_double2(-w * (d.x * px - d.y * py), w * (d.y * px + d.x * py));
         continue;
       }
       double2 f = make_double2((double)v[k2].x * sc, (double)v[k2].y * sc);
       if (fn) { const double2 q = zseg > 0 ? segf[idx - g0] : fn[idx]; f.x += q.x; f.y += q.y; }
-      const double gg = g2[idx];
       if (gg <= ecut) {
         const double2 p = zseg > 0 ? segp[idx - g0] : ps[idx];
         const double t = wt * gg;
