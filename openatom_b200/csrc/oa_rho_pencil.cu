@@ -48,12 +48,32 @@ k_rho2_fwd(const double* __restrict__ rho, double scale, const double2* __restri
   rho += blockIdx.y * fin;
   dz += blockIdx.y * fout;
   for (int i = tid; i < N; i += NT) tw[i] = twg[i];
-  // rows y1 = 2p, y2 = 2p + 1 as one complex sequence, scaled by V/N
+  // rows y1 = 2p, y2 = 2p + 1 as one complex sequence, scaled by V/N; four
+  // items per thread have their loads in flight before any store
   const double* rz = rho + (size_t)z * N * N;
-  for (int i = tid; i < NPAIR * N; i += NT) {
-    const int p = i / N, x = i - p * N;
-    const int y1 = 2 * p, y2 = y1 + 1;
-    A[p * LD + x] = make_double2(rz[y1 * N + x] * scale, (y2 < N) ? rz[y2 * N + x] * scale : 0.0);
+  constexpr int NI = NPAIR * N;
+  for (int i0 = tid; i0 < NI; i0 += 4 * NT) {
+    double va[4], vb[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * NT;
+      va[u] = 0.0;
+      vb[u] = 0.0;
+      if (i < NI) {
+        const int p = i / N, x = i - p * N;
+        const int y1 = 2 * p, y2 = y1 + 1;
+        va[u] = rz[y1 * N + x];
+        if (y2 < N) vb[u] = rz[y2 * N + x];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * NT;
+      if (i < NI) {
+        const int p = i / N, x = i - p * N;
+        A[p * LD + x] = make_double2(va[u] * scale, vb[u] * scale);
+      }
+    }
   }
   __syncthreads();
   // x pass A (-): pairs fastest
@@ -130,11 +150,16 @@ k_rho2_bwd(const double2* __restrict__ dz, int ldl_d, const double2* __restrict_
   dz += blockIdx.y * fin;
   vks += blockIdx.y * fout;
   for (int i = tid; i < N; i += NT) tw[i] = twg[i];
+  // the plane's columns staged by cp.async: every 16-byte copy in flight
+  // before any is waited for
   const double2* in = dz + (size_t)z * ldl_d;
   for (int i = tid; i < NKX * N; i += NT) {
     const int c = i / N, y = i - c * N;
-    A[c * LD + y] = in[i];
+    const unsigned d = (unsigned)__cvta_generic_to_shared(A + c * LD + y);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(in + i));
   }
+  asm volatile("cp.async.commit_group;\n" ::);
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   // y pass A (+): columns fastest
   for (int i = tid; i < N2 * NKX; i += NT) {
