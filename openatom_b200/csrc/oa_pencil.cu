@@ -60,8 +60,8 @@ __device__ __forceinline__ int line_slot(int z, int n, int nn, int np) {
 // ---------------------------------------------------------------------------
 // z pass forward: packed sphere (optionally conj(dyp psi)) -> FFT(-) of the
 // zero-filled z-line -> zbuf[s][z][line].  Block = OA_LB lines of one state.
-// BAND: every line's kz lie in (-N/4, N/4), so the pass-A inputs n1 in
-// [N1/4, 3 N1/4) are zero (band-pruned first DFT, RDftBand).
+// BAND: the kz of every line lie in (-N/4, N/4), so the pass-A inputs n1
+// in [N1/4, 3 N1/4) are zero (band-pruned first DFT, RDftBand).
 // ---------------------------------------------------------------------------
 template <typename R, int N1, int N2, bool BAND>
 __global__ void __launch_bounds__(OA_NTHREADS)

@@ -298,7 +298,8 @@ k_rho_zpass(double2* __restrict__ dz, int ldl_d, int nlines_d, int nx, int ny, i
   int* zoff = (int*)(pxy + OA_LB * natm);  // [natm]: z-phase row of atom ia (type order)
   // FORCES: [OA_LB * nz][ntype] per-type (A, B) coefficients after zoff
   double2* cf = (double2*)(smem_raw + (((size_t)((char*)(zoff + natm) - (char*)smem_raw) + 15) & ~(size_t)15));
-  // the line's density coefficients: every 16-byte copy issued before any is waited for
+  // the density coefficients of the block's lines: every 16-byte copy
+  // issued before any is waited for
   for (int idx = threadIdx.x; idx < nz * OA_LB; idx += blockDim.x) {
     const int zz = idx / OA_LB, lb = idx - zz * OA_LB;
     if (lb < nb) rho_cp16(a + lb * ldz + zz, dz + (size_t)zz * ldl_d + l0 + lb);
